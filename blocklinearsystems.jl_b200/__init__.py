@@ -1,0 +1,21 @@
+"""blsgpu: a B200 (sm_100a) implementation of BlockLinearSystems.jl's elimination path behind a C ABI.
+
+The package directory is named `blocklinearsystems.jl_b200`; load it under the module name `blsgpu` with
+`load_package()` in __graft_entry__.py (or any importlib loader), as the directory name is not an identifier.
+
+Layout (host, integer):  SchurStructure, build_schur_pattern, build_r_to_s_map, sparse_with_map
+Device reduction:        SchurReductionWorkspace, reset_schur_sparse / reset_schur_dense,
+                         reduce_schur_sparse / reduce_schur_dense, backsubstitute, scatter_copy
+Workloads:               scenes.workload, scenes.hessian_problem
+"""
+from ._lib import ArgumentError, BlsError, DimensionMismatch
+from .layout import DEFAULT_MIN_WORK, SchurPattern, SchurStructure, build_r_to_s_map, build_schur_pattern, sparse_with_map
+from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce_schur_dense, reduce_schur_sparse,
+                        reset_schur_dense, reset_schur_sparse, scatter_copy)
+from . import scenes
+
+__all__ = [
+    "ArgumentError", "BlsError", "DimensionMismatch", "DEFAULT_MIN_WORK", "SchurPattern", "SchurStructure", "build_r_to_s_map",
+    "build_schur_pattern", "sparse_with_map", "SchurReductionWorkspace", "backsubstitute", "context", "reduce_schur_dense",
+    "reduce_schur_sparse", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes",
+]

@@ -1,0 +1,204 @@
+// C ABI of libblsgpu: contexts, errors and the host-side layout (structure, pattern, maps).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+
+namespace bls {
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace bls
+
+struct bls_structure : bls::Structure {};
+struct bls_pattern : bls::Pattern {};
+
+using namespace bls;
+
+#define BLS_GUARD(...)                         \
+  try {                                        \
+    __VA_ARGS__                                \
+  } catch (const bls::Error& e) {              \
+    bls::set_error(e.what());                  \
+    return e.code;                             \
+  } catch (const std::bad_alloc&) {            \
+    bls::set_error("out of host memory");      \
+    return BLS_ENOMEM;                         \
+  } catch (const std::exception& e) {          \
+    bls::set_error(e.what());                  \
+    return BLS_EINVAL;                         \
+  }
+
+static int64_t put(int64_t* out, const std::vector<int64_t>& v) {
+  if (out && !v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(int64_t));
+  return (int64_t)v.size();
+}
+
+extern "C" {
+
+int bls_version(void) { return 1; }
+const char* bls_last_error(void) { return bls::g_last_error.c_str(); }
+
+int bls_ctx_create(int device, bls_ctx** out) {
+  BLS_GUARD({
+    if (!out) throw Error(BLS_EINVAL, "null argument");
+    int n = 0;
+    BLS_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) throw Error(BLS_EINVAL, "no CUDA device " + std::to_string(device));
+    BLS_CUDA(cudaSetDevice(device));
+    auto* c = new bls_ctx();
+    c->device = device;
+    c->stream = nullptr;
+    *out = c;
+    return BLS_OK;
+  })
+}
+
+int bls_ctx_destroy(bls_ctx* ctx) {
+  delete ctx;
+  return BLS_OK;
+}
+
+int bls_ctx_set_stream(bls_ctx* ctx, void* stream) {
+  if (!ctx) return BLS_EINVAL;
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  return BLS_OK;
+}
+
+int bls_ctx_synchronize(bls_ctx* ctx) {
+  BLS_GUARD({
+    BLS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return BLS_OK;
+  })
+}
+
+int bls_structure_from_description(int64_t nblocks, const int64_t* blocksizes, int64_t nrowblocks, const int64_t* rowblock_ptr,
+                                   const int64_t* rowblock_idx, const uint8_t* eliminated, int64_t nchunks, int64_t min_work,
+                                   bls_structure** out) {
+  BLS_GUARD({
+    if (!out || (nblocks > 0 && (!blocksizes || !eliminated)) || (nrowblocks > 0 && (!rowblock_ptr || !rowblock_idx)))
+      throw Error(BLS_EINVAL, "null argument");
+    auto* s = new bls_structure();
+    try {
+      static_cast<Structure&>(*s) = structure_from_description(nblocks, blocksizes, nrowblocks, rowblock_ptr, rowblock_idx, eliminated, nchunks, min_work);
+    } catch (...) {
+      delete s;
+      throw;
+    }
+    *out = s;
+    return BLS_OK;
+  })
+}
+
+int bls_structure_positional(int64_t nrblocks, const int64_t* r_dims, int64_t neblocks, const int64_t* e_dims, const int64_t* coupling_ptr,
+                             const int64_t* coupling_idx, int64_t nchunks, int64_t min_work, bls_structure** out) {
+  BLS_GUARD({
+    std::vector<std::vector<int64_t>> coup(neblocks);
+    for (int64_t e = 0; e < neblocks; ++e) coup[e].assign(coupling_idx + coupling_ptr[e], coupling_idx + coupling_ptr[e + 1]);
+    auto* s = new bls_structure();
+    try {
+      static_cast<Structure&>(*s) = structure_positional(std::vector<int64_t>(r_dims, r_dims + nrblocks), std::vector<int64_t>(e_dims, e_dims + neblocks), coup, nchunks, min_work);
+    } catch (...) {
+      delete s;
+      throw;
+    }
+    *out = s;
+    return BLS_OK;
+  })
+}
+
+int64_t bls_structure_field(const bls_structure* st, const char* name, int64_t* out) {
+  if (!st || !name) return -1;
+  const std::string f(name);
+  auto scalar = [&](int64_t v) { if (out) out[0] = v; return (int64_t)1; };
+  if (f == "nr") return scalar(st->nr);
+  if (f == "ne") return scalar(st->ne);
+  if (f == "nrblocks") return scalar(st->nrblocks);
+  if (f == "neblocks") return scalar(st->neblocks);
+  if (f == "max_coupled_dim") return scalar(st->max_coupled_dim);
+  if (f == "E_length") return scalar(st->E_length);
+  if (f == "C_length") return scalar(st->C_length);
+  if (f == "nchunks") return scalar(st->nchunks);
+  if (f == "min_work") return scalar(st->min_work);
+  if (f == "r_dims") return put(out, st->r_dims);
+  if (f == "e_dims") return put(out, st->e_dims);
+  if (f == "boffsets_r") return put(out, st->boffsets_r);
+  if (f == "boffsets_e") return put(out, st->boffsets_e);
+  if (f == "eoffsets") return put(out, st->eoffsets);
+  if (f == "eliminated_ptr") return put(out, st->eliminated_ptr);
+  if (f == "entry_retained") return put(out, st->entry_retained);
+  if (f == "coffsets") return put(out, st->coffsets);
+  if (f == "order") return put(out, st->order);
+  if (f == "chunks") return put(out, st->chunks);
+  if (f == "retained_ptr") return put(out, st->retained_ptr);
+  if (f == "retained_entry") return put(out, st->retained_entry);
+  if (f == "entry_eliminated") return put(out, st->entry_eliminated);
+  if (f == "col_chunks") return put(out, st->col_chunks);
+  if (f == "retained_pairs") {
+    std::vector<int64_t> v;
+    for (auto& p : st->retained_pairs) { v.push_back(p.first); v.push_back(p.second); }
+    return put(out, v);
+  }
+  return -1;
+}
+
+int bls_structure_destroy(bls_structure* st) {
+  delete st;
+  return BLS_OK;
+}
+
+int bls_schur_pattern_build(const bls_structure* st, int64_t nextra, const int64_t* extra_pairs, bls_pattern** out) {
+  BLS_GUARD({
+    if (!st || !out) throw Error(BLS_EINVAL, "null argument");
+    std::vector<std::pair<int64_t, int64_t>> ex;
+    for (int64_t i = 0; i < nextra; ++i) ex.push_back({extra_pairs[2 * i], extra_pairs[2 * i + 1]});
+    auto* p = new bls_pattern();
+    try {
+      static_cast<Pattern&>(*p) = build_pattern(*st, ex);
+    } catch (...) {
+      delete p;
+      throw;
+    }
+    *out = p;
+    return BLS_OK;
+  })
+}
+
+int64_t bls_pattern_field(const bls_pattern* p, const char* name, int64_t* out) {
+  if (!p || !name) return -1;
+  const std::string f(name);
+  if (f == "block_colptr") return put(out, p->block_colptr);
+  if (f == "block_rowval") return put(out, p->block_rowval);
+  if (f == "block_row_offsets") return put(out, p->block_row_offsets);
+  if (f == "col_heights") return put(out, p->col_heights);
+  if (f == "S_colptr") return put(out, p->S_colptr);
+  if (f == "S_rowval") return put(out, p->S_rowval);
+  if (f == "diag_inds") return put(out, p->diag_inds);
+  if (f == "R_block_start") return put(out, p->R_block_start);
+  if (f == "R_length") { if (out) out[0] = p->R_length; return 1; }
+  return -1;
+}
+
+int bls_pattern_destroy(bls_pattern* p) {
+  delete p;
+  return BLS_OK;
+}
+
+int bls_build_r_to_s_map(const bls_structure* st, const bls_pattern* p, int64_t* out) {
+  BLS_GUARD({
+    if (!st || !p || !out) throw Error(BLS_EINVAL, "null argument");
+    std::vector<int64_t> m = build_r_to_s(*st, *p);
+    put(out, m);
+    return BLS_OK;
+  })
+}
+
+int64_t bls_sparse_indices(const bls_structure* st, const bls_pattern* p, int symmetric, int64_t* colptr, int64_t* rowval, int64_t* map) {
+  BLS_GUARD({
+    if (!st || !p) throw Error(BLS_EINVAL, "null argument");
+    return sparse_indices(*st, *p, symmetric != 0, colptr, rowval, map);
+  })
+}
+
+}  // extern "C"

@@ -1,0 +1,48 @@
+// Host-side layout types shared by the C ABI and the layout builders (0-based throughout).
+#pragma once
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/blsgpu.h"
+
+namespace bls {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// SchurStructure (src/schur_structure.jl:50-68) plus the workspace index of SchurReductionWorkspace
+// (src/schur_reduction.jl:22-25).
+struct Structure {
+  int64_t nr = 0, ne = 0, nrblocks = 0, neblocks = 0, nchunks = 1, min_work = 4096, max_coupled_dim = 0;
+  int64_t E_length = 0, C_length = 0;
+  std::vector<int64_t> r_dims, e_dims, boffsets_r, boffsets_e, eoffsets, eliminated_ptr, entry_retained, coffsets, order;
+  std::vector<std::pair<int64_t, int64_t>> retained_pairs;
+  std::vector<int64_t> e_run_first;   // first block of each run of equal e_dims, then neblocks
+  std::vector<int64_t> chunks;        // per run, nchunks half-open ranges (first, stop)
+  std::vector<int64_t> retained_ptr, retained_entry, entry_eliminated;
+  std::vector<int64_t> col_chunks;    // nchunks half-open ranges of retained blocks
+};
+
+// build_schur_pattern's result (src/schur_structure.jl:314-322) and the retained storage laid out on it.
+struct Pattern {
+  std::vector<int64_t> block_colptr, block_rowval, block_row_offsets, col_heights, S_colptr, S_rowval, diag_inds;
+  std::vector<int64_t> R_block_start;
+  int64_t R_length = 0;
+};
+
+std::vector<int64_t> partition_columns(const std::vector<int64_t>& retained_ptr, int64_t K);
+void finish_structure(Structure& st, const std::vector<std::vector<int64_t>>& couplings);
+Structure structure_positional(const std::vector<int64_t>& r_dims, const std::vector<int64_t>& e_dims,
+                               const std::vector<std::vector<int64_t>>& couplings, int64_t nchunks, int64_t min_work);
+Structure structure_from_description(int64_t n, const int64_t* blocksizes, int64_t K, const int64_t* rb_ptr,
+                                     const int64_t* rb_idx, const uint8_t* eliminated, int64_t nchunks, int64_t min_work);
+Pattern build_pattern(const Structure& st, const std::vector<std::pair<int64_t, int64_t>>& extra);
+std::vector<int64_t> build_r_to_s(const Structure& st, const Pattern& P);
+int64_t sparse_indices(const Structure& st, const Pattern& P, bool symmetric, int64_t* colptr, int64_t* rowval, int64_t* map);
+
+}  // namespace bls

@@ -1,0 +1,859 @@
+// Schur-complement elimination of the point blocks on sm_100a.
+//
+// Reference: src/schur_reduction.jl (SchurReductionWorkspace :16-92, factor_eliminated! :121-162, accumulate_entry_*!
+// :262-354, reset_schur_*! :389-436, reduce_schur_*! :465-507, backsubstitute! :519-576), src/kernels.jl:3-67
+// (inv_sym_block), src/conditioning.jl:99-150 (scaling at read).
+//
+// Device layout. Everything the reference keeps in its workspace is built once per structure into a plan:
+//   - the structure's index arrays as int32 (r_dims, boffsets, eliminated_ptr, entry_retained, coffsets, ...);
+//   - the S blocks that receive contributions, each with the base index of its (0, 0) entry and its column stride
+//     (sparse: S_colptr[boffsets_r[r2]] + block_row_offsets[k] and col_heights[r2]; dense: the column-major offset
+//     and nr), so one kernel serves reduce_schur_sparse! and reduce_schur_dense!;
+//   - for every S block (r1, r2) the list of coupling pairs (c1, c2) of the points that observe both (c1 of r1, c2 of
+//     r2, same point), in ascending point order, cut into work items of at most PAIR_CHUNK pairs.
+// A call then runs:
+//   phase 1  k_factor   one thread per point: the damped d_e x d_e inverse in FP64 (closed forms of
+//                        src/kernels.jl:14-67, same pivot tests), z = E^-1 (s_e .* b_e) in FP64;
+//   phase 2  k_pairs    one thread per work item: sum over its pairs of C_c1' (E^-1 C_c2), the 6x6 block in
+//                        registers, then one plain read-modify-write of S when the block has a single item, else
+//                        atomic adds (one per block entry per item, not per pair);
+//            k_gradient one warp per retained block: g_S = s_r .* b_r - sum C' z over its couplings.
+// The reference forms W = E^-1 C in phase 1 and reads it back in phase 2; here E^-1 C_c2 is formed in registers
+// where it is used, so nothing the size of C_data is written. W' C and C' (E^-1 C) are the same product (E^-1 is
+// symmetric); the order of the additions differs, which the tests bound by tolerance.
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <omp.h>
+#include <type_traits>
+
+#include "common.cuh"
+
+namespace bls {
+
+constexpr int PAIR_CHUNK = 32;
+constexpr long long NONE = LLONG_MAX;
+
+// ------------------------------------------------------------------------------------------------------------------
+// Plan
+// ------------------------------------------------------------------------------------------------------------------
+struct SchurPlan {
+  bls_ctx* ctx = nullptr;
+  int64_t nrblocks = 0, neblocks = 0, nr = 0, ne = 0, ncoup = 0, E_length = 0, C_length = 0;
+  int64_t nblocks = 0, npairs = 0, nitems = 0, nnzS = 0, R_length = 0;
+  bool has_sparse = false;
+  int max_de = 0, max_dr = 0;
+  bool uniform36 = false;   // every r_dim is 6 and every e_dim is 3
+  std::vector<int64_t> diag_inds_host;
+  // structure
+  DevBuf r_dims, boffsets_r, e_dims, boffsets_e, eoffsets, eliminated_ptr, entry_retained, coffsets, entry_eliminated;
+  DevBuf retained_ptr, retained_entry;
+  // blocks and pairs
+  DevBuf block_r1, block_r2, block_base_sparse, block_stride_sparse, block_base_dense;
+  DevBuf pair_c1, pair_c2, item_block, item_start, item_info;
+  // reset
+  DevBuf r_to_s, diag_inds, S_rowval, S_col;
+  // scratch: E^-1 (FP64, and FP32 for the mixed form), z, status
+  DevBuf Einv64, Einv32, z, status;
+  Status* host_status = nullptr;   // pinned
+  int last_dtype = -1;
+  ~SchurPlan() { if (host_status) cudaFreeHost(host_status); }
+};
+
+static std::vector<int32_t> to32(const int64_t* a, int64_t n, const char* what) {
+  std::vector<int32_t> v((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    if (a[i] < INT32_MIN || a[i] > INT32_MAX) throw Error(BLS_EUNSUPPORTED, std::string(what) + " exceeds the 32-bit index range of this build");
+    v[i] = (int32_t)a[i];
+  }
+  return v;
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Kernels
+// ------------------------------------------------------------------------------------------------------------------
+// which = 0: the reset's scaling_r slot; 1: the reduction's scaling_e slot
+__global__ void k_status_begin(Status* st, int which) {
+  if (which == 0) st->einval_r = NONE;
+  else st->einval_e = NONE;
+}
+// check_damping (src/utils.jl:100-107): every scaling entry finite and non-negative; the lowest bad index is kept
+__global__ void k_check_scaling(const double* __restrict__ sc, int64_t n, Status* st, int which) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x = sc[i];
+  if (!(isfinite(x) && x >= 0.0)) atomicMin(which == 0 ? &st->einval_r : &st->einval_e, (long long)i);
+}
+__device__ __forceinline__ bool args_ok(const Status* st) { return st->einval_r == NONE && st->einval_e == NONE; }
+// The reduction's failure word starts clear when the arguments are valid
+__global__ void k_arm(Status* st) {
+  if (args_ok(st)) st->failed = NONE;
+}
+
+__device__ __forceinline__ bool live(const Status* st) { return args_ok(st) && st->failed == NONE; }
+
+// --- reset_schur_sparse!: fill, scatter R by the r -> s map, scale, damp the diagonal ---
+template <class T>
+__global__ void k_fill(T* __restrict__ S, int64_t n, const Status* st) {
+  if (st->einval_r != NONE) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (; i < n; i += (int64_t)gridDim.x * blockDim.x) S[i] = T(0);
+}
+template <class T>
+__global__ void k_scatter_r(T* __restrict__ S, const T* __restrict__ R, const int64_t* __restrict__ map, int64_t n, const Status* st) {
+  if (st->einval_r != NONE) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t idx = map[i];
+    if (idx >= 0) S[idx] = R[i];
+  }
+}
+// scale_sparse! (src/conditioning.jl:144-150): nz = T(nz * s[row] * s[col]), formed in FP64
+template <class T>
+__global__ void k_scale_sparse(T* __restrict__ S, const int32_t* __restrict__ rowval, const int32_t* __restrict__ col,
+                               const double* __restrict__ s, int64_t n, const Status* st) {
+  if (st->einval_r != NONE) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (; i < n; i += (int64_t)gridDim.x * blockDim.x) S[i] = T((double)S[i] * (s[rowval[i]] * s[col[i]]));
+}
+// nzval[idx] = T(Float64(nzval[idx]) + lambda * scaling_r[i] * (s_i * s_i)) (src/schur_reduction.jl:430-433)
+template <class T>
+__global__ void k_damp_diag(T* __restrict__ S, const int64_t* __restrict__ diag_inds, int64_t dense_nr,
+                            const double* __restrict__ sc, double lambda, const double* __restrict__ s, int64_t nr, Status* st) {
+  if (st->einval_r != NONE) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nr) return;
+  double si = s ? s[i] : 1.0;
+  int64_t idx = diag_inds ? diag_inds[i] : i * (dense_nr + 1);
+  S[idx] = T((double)S[idx] + lambda * sc[i] * (si * si));
+}
+// reset_schur_dense! copy with scaling (src/schur_reduction.jl:394-400)
+template <class T>
+__global__ void k_copy_scaled_dense(T* __restrict__ S, const T* __restrict__ R, const double* __restrict__ s, int64_t nr, const Status* st) {
+  if (st->einval_r != NONE) return;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (; i < nr * nr; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = i % nr, c = i / nr;
+    S[i] = s ? T((double)R[i] * (s[r] * s[c])) : R[i];
+  }
+}
+__global__ void k_reset_done(Status* st) {
+  if (st->einval_r == NONE) st->failed = NONE;
+}
+
+// --- phase 1: damped inverse of each eliminated block (src/kernels.jl:14-67, src/schur_reduction.jl:127-147) ---
+// The closed forms are evaluated with explicitly rounded operations (no FMA contraction), as the reference's Julia
+// arithmetic is, so that the pivot tests take the reference's decisions.
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+__device__ bool inv_sym_closed(int de, const double* H, const double* damp, double* inv) {
+  const double tol = 4504.0 * 2.220446049250313e-16;   // singular_tol(Float64) = 4504 * eps(Float64)
+  if (de == 1) {
+    double h11 = add(H[0], mul(1.0, damp[0]));
+    if (!(h11 > 0.0) || !isfinite(h11)) return false;
+    inv[0] = __drcp_rn(h11);
+    return true;
+  }
+  if (de == 2) {
+    double H11 = add(H[0], damp[0]), H22 = add(H[3], damp[1]), H12 = H[2];
+    double det = sub(mul(H11, H22), mul(H12, H12));
+    if (!(H11 > 0.0) || !(det > mul(tol, mul(H11, H22))) || !isfinite(det)) return false;
+    double id = __drcp_rn(det);
+    inv[0] = mul(H22, id); inv[1] = mul(-H12, id); inv[2] = mul(-H12, id); inv[3] = mul(H11, id);
+    return true;
+  }
+  // de == 3, H column-major: H[i + 3j]
+  double H11 = add(H[0], damp[0]), H22 = add(H[4], damp[1]), H33 = add(H[8], damp[2]);
+  double H12 = H[3], H13 = H[6], H23 = H[7];
+  double c11 = sub(mul(H22, H33), mul(H23, H23));
+  double c12 = sub(mul(H13, H23), mul(H12, H33));
+  double c13 = sub(mul(H12, H23), mul(H13, H22));
+  double c22 = sub(mul(H11, H33), mul(H13, H13));
+  double c23 = sub(mul(H12, H13), mul(H11, H23));
+  double c33 = sub(mul(H11, H22), mul(H12, H12));
+  double det = add(add(mul(H11, c11), mul(H12, c12)), mul(H13, c13));
+  if (!(H11 > 0.0) || !(c33 > mul(tol, mul(H11, H22))) || !(det > mul(tol, mul(c33, H33))) || !isfinite(det)) return false;
+  double id = __drcp_rn(det);
+  inv[0] = mul(c11, id); inv[1] = mul(c12, id); inv[2] = mul(c13, id);
+  inv[3] = mul(c12, id); inv[4] = mul(c22, id); inv[5] = mul(c23, id);
+  inv[6] = mul(c13, id); inv[7] = mul(c23, id); inv[8] = mul(c33, id);
+  return true;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_factor(int64_t neb, const int32_t* __restrict__ e_dims, const int32_t* __restrict__ eoffsets,
+                                                const int32_t* __restrict__ boffsets_e, const T* __restrict__ E,
+                                                const double* __restrict__ b_e, const double* __restrict__ scaling_e, double lambda,
+                                                const double* __restrict__ s_e, double* __restrict__ Einv64, float* __restrict__ Einv32,
+                                                double* __restrict__ z, Status* st) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= neb) return;
+  if (!args_ok(st)) return;
+  const int de = e_dims[e], eo = eoffsets[e], so = boffsets_e[e];
+  double se[3], damp[3], H[9], inv[9];
+  for (int i = 0; i < de; ++i) {
+    se[i] = s_e ? s_e[so + i] : 1.0;
+    damp[i] = mul(mul(lambda, scaling_e[so + i]), mul(se[i], se[i]));
+  }
+  for (int j = 0; j < de; ++j)
+    for (int i = 0; i < de; ++i) {
+      double h = (double)E[eo + i + de * j];
+      H[i + de * j] = s_e ? mul(h, mul(se[i], se[j])) : h;
+    }
+  if (!inv_sym_closed(de, H, damp, inv)) {
+    atomicMin(&st->failed, (long long)e);
+    return;
+  }
+  for (int i = 0; i < de * de; ++i) {
+    Einv64[eo + i] = inv[i];
+    if (Einv32) Einv32[eo + i] = (float)inv[i];
+  }
+  for (int i = 0; i < de; ++i) {
+    double acc = inv[i] * (b_e[so] * se[0]);
+    for (int j = 1; j < de; ++j) acc = acc + inv[i + de * j] * (b_e[so + j] * se[j]);
+    z[so + i] = acc;
+  }
+}
+
+// --- phase 2: one thread per work item of one S block ---
+template <class T> struct EinvOf { using type = double; };
+template <> struct EinvOf<float> { using type = float; };
+
+template <class T>
+__device__ __forceinline__ void red_add(T* p, T v) { atomicAdd(p, v); }
+
+// MDE/MDR: compile-time bounds of d_e and d_r; the runtime sizes are checked against them by the host.
+template <class T, int MDE, int MDR>
+__global__ void __launch_bounds__(128) k_pairs(
+    int64_t nitems, const int32_t* __restrict__ item_block, const int32_t* __restrict__ item_start, const int32_t* __restrict__ item_info,
+    const int32_t* __restrict__ pair_c1, const int32_t* __restrict__ pair_c2, const int32_t* __restrict__ block_r1,
+    const int32_t* __restrict__ block_r2, const int64_t* __restrict__ block_base, const int32_t* __restrict__ block_stride, int64_t dense_nr,
+    const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boffsets_r, const int32_t* __restrict__ entry_eliminated,
+    const int32_t* __restrict__ e_dims, const int32_t* __restrict__ boffsets_e, const int32_t* __restrict__ eoffsets,
+    const int32_t* __restrict__ coffsets, const T* __restrict__ C, const typename EinvOf<T>::type* __restrict__ Einv,
+    const double* __restrict__ s_r, const double* __restrict__ s_e, T* __restrict__ S, const Status* __restrict__ st) {
+  using TE = typename EinvOf<T>::type;
+  const int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (it >= nitems) return;
+  if (!live(st)) return;
+  const int k = item_block[it], p_begin = item_start[it], info = item_info[it];
+  const int cnt = info & 0xffff;
+  const bool solo = (info >> 16) != 0;
+  const int r1 = block_r1[k], r2 = block_r2[k];
+  const bool diag = r1 == r2;
+  const int d1 = r_dims[r1], d2 = r_dims[r2], ro1 = boffsets_r[r1], ro2 = boffsets_r[r2];
+  T acc[MDR][MDR];
+#pragma unroll
+  for (int a = 0; a < MDR; ++a)
+#pragma unroll
+    for (int b = 0; b < MDR; ++b) acc[a][b] = T(0);
+  for (int p = p_begin; p < p_begin + cnt; ++p) {
+    const int c1 = pair_c1[p], c2 = pair_c2[p];
+    const int e = entry_eliminated[c2];
+    const int de = e_dims[e], so = boffsets_e[e], eo = eoffsets[e];
+    const int co1 = coffsets[c1], co2 = coffsets[c2];
+    double se[MDE];
+#pragma unroll
+    for (int s = 0; s < MDE; ++s) se[s] = (s < de && s_e) ? s_e[so + s] : 1.0;
+    TE Ei[MDE][MDE];
+#pragma unroll
+    for (int a = 0; a < MDE; ++a)
+#pragma unroll
+      for (int b = 0; b < MDE; ++b) Ei[a][b] = (a < de && b < de) ? Einv[eo + a + de * b] : TE(0);
+    // U = E^-1 * scaled(C_c2)  (d_e x d2)
+    T U[MDE][MDR];
+#pragma unroll
+    for (int w = 0; w < MDR; ++w) {
+      T cw[MDE];
+      const double fw = (w < d2 && s_r) ? s_r[ro2 + w] : 1.0;
+#pragma unroll
+      for (int s = 0; s < MDE; ++s) {
+        T c = (w < d2 && s < de) ? C[co2 + w * de + s] : T(0);
+        cw[s] = (s_r || s_e) ? T((double)c * (se[s] * fw)) : c;
+      }
+#pragma unroll
+      for (int t = 0; t < MDE; ++t) {
+        TE u = TE(0);
+#pragma unroll
+        for (int s = 0; s < MDE; ++s) u = u + Ei[t][s] * (TE)cw[s];
+        U[t][w] = (T)u;
+      }
+    }
+    // acc += scaled(C_c1)' * U
+#pragma unroll
+    for (int rho = 0; rho < MDR; ++rho) {
+      T cr[MDE];
+      const double fr = (rho < d1 && s_r) ? s_r[ro1 + rho] : 1.0;
+#pragma unroll
+      for (int s = 0; s < MDE; ++s) {
+        T c = (rho < d1 && s < de) ? C[co1 + rho * de + s] : T(0);
+        cr[s] = (s_r || s_e) ? T((double)c * (se[s] * fr)) : c;
+      }
+#pragma unroll
+      for (int w = 0; w < MDR; ++w) {
+        T a = acc[rho][w];
+#pragma unroll
+        for (int s = 0; s < MDE; ++s) a = a + cr[s] * U[s][w];
+        acc[rho][w] = a;
+      }
+    }
+  }
+  const int64_t base = block_base[k];
+  const int64_t stride = block_stride ? (int64_t)block_stride[k] : dense_nr;
+#pragma unroll
+  for (int w = 0; w < MDR; ++w) {
+    if (w >= d2) continue;
+#pragma unroll
+    for (int rho = 0; rho < MDR; ++rho) {
+      if (rho >= d1 || (diag && rho > w)) continue;
+      T* p = S + base + w * stride + rho;
+      if (solo) *p = *p - acc[rho][w];
+      else red_add(p, -acc[rho][w]);
+    }
+  }
+}
+
+// g_S = s_r .* b_r - sum over the couplings c2 of r2 of scaled(C_c2)' z_e (src/schur_reduction.jl:326-328, 473/500)
+template <class T>
+__global__ void __launch_bounds__(256) k_gradient(int64_t nrb, const int32_t* __restrict__ retained_ptr, const int32_t* __restrict__ retained_entry,
+                                                  const int32_t* __restrict__ entry_eliminated, const int32_t* __restrict__ r_dims,
+                                                  const int32_t* __restrict__ boffsets_r, const int32_t* __restrict__ e_dims,
+                                                  const int32_t* __restrict__ boffsets_e, const int32_t* __restrict__ coffsets,
+                                                  const T* __restrict__ C, const double* __restrict__ z, const double* __restrict__ b_r,
+                                                  const double* __restrict__ s_r, const double* __restrict__ s_e, double* __restrict__ g,
+                                                  const Status* __restrict__ st) {
+  const int64_t r2 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r2 >= nrb) return;
+  if (!live(st)) return;
+  const int d2 = r_dims[r2], ro2 = boffsets_r[r2];
+  double acc[16];
+  for (int w = 0; w < 16; ++w) acc[w] = 0.0;
+  for (int q = retained_ptr[r2] + lane; q < retained_ptr[r2 + 1]; q += 32) {
+    const int c2 = retained_entry[q], e = entry_eliminated[c2];
+    const int de = e_dims[e], so = boffsets_e[e], co = coffsets[c2];
+    for (int w = 0; w < d2 && w < 16; ++w) {
+      const double f = s_r ? s_r[ro2 + w] : 1.0;
+      double d = 0.0;
+      for (int s = 0; s < de; ++s) {
+        T c = C[co + w * de + s];
+        double cs = (s_r || s_e) ? (double)T((double)c * ((s_e ? s_e[so + s] : 1.0) * f)) : (double)c;
+        d = d + cs * z[so + s];
+      }
+      acc[w] += d;
+    }
+  }
+  for (int w = 0; w < 16; ++w)
+    for (int off = 16; off > 0; off >>= 1) acc[w] += __shfl_xor_sync(0xffffffffu, acc[w], off);
+  if (lane < d2 && lane < 16) {
+    double bv = b_r[ro2 + lane];
+    if (s_r) bv = bv * s_r[ro2 + lane];
+    double a = 0.0;
+    for (int w = 0; w < 16; ++w) if (w == lane) a = acc[w];
+    g[ro2 + lane] = bv - a;
+  }
+}
+
+// backsubstitute_group! (src/schur_reduction.jl:541-576): x_e = z - E^-1 t, t = sum scaled(C) x_r, all in FP64
+template <class T>
+__global__ void __launch_bounds__(256) k_backsub(int64_t neb, const int32_t* __restrict__ e_dims, const int32_t* __restrict__ eoffsets,
+                                                 const int32_t* __restrict__ boffsets_e, const int32_t* __restrict__ eliminated_ptr,
+                                                 const int32_t* __restrict__ entry_retained, const int32_t* __restrict__ coffsets,
+                                                 const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boffsets_r,
+                                                 const T* __restrict__ C, const double* __restrict__ Einv, const double* __restrict__ z,
+                                                 const double* __restrict__ x_r, const double* __restrict__ s_r, const double* __restrict__ s_e,
+                                                 double* __restrict__ x_e) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= neb) return;
+  const int de = e_dims[e], eo = eoffsets[e], so = boffsets_e[e];
+  double t[3] = {0.0, 0.0, 0.0};
+  for (int c = eliminated_ptr[e]; c < eliminated_ptr[e + 1]; ++c) {
+    const int r = entry_retained[c], dr = r_dims[r], ro = boffsets_r[r], co = coffsets[c];
+    for (int ir = 0; ir < dr; ++ir) {
+      const double xc = x_r[ro + ir], f = s_r ? s_r[ro + ir] : 1.0;
+      for (int i = 0; i < de; ++i) {
+        T cv = C[co + ir * de + i];
+        double cs = (s_r || s_e) ? (double)T((double)cv * ((s_e ? s_e[so + i] : 1.0) * f)) : (double)cv;
+        t[i] = t[i] + cs * xc;
+      }
+    }
+  }
+  for (int i = 0; i < de; ++i) {
+    double acc = Einv[eo + i] * t[0];
+    for (int j = 1; j < de; ++j) acc = acc + Einv[eo + i + de * j] * t[j];
+    x_e[so + i] = z[so + i] - acc;
+  }
+}
+
+template <class T>
+__global__ void k_gather(T* __restrict__ dest, const T* __restrict__ src, const int64_t* __restrict__ map, int64_t n) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (; i < n; i += (int64_t)gridDim.x * blockDim.x) dest[i] = src[map[i]];
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Plan construction (host, once per structure)
+// ------------------------------------------------------------------------------------------------------------------
+static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
+  if (!d || d->nrblocks < 1 || d->neblocks < 1) throw Error(BLS_EINVAL, "a plan needs at least one retained and one eliminated block");
+  std::unique_ptr<SchurPlan> P(new SchurPlan());
+  P->ctx = ctx;
+  cudaStream_t s = ctx->stream;
+  const int64_t nrb = d->nrblocks, neb = d->neblocks;
+  P->nrblocks = nrb;
+  P->neblocks = neb;
+  const int64_t nc = d->eliminated_ptr[neb];
+  P->ncoup = nc;
+  std::vector<int64_t> boff_r(nrb), boff_e(neb);
+  int64_t nr = 0, ne = 0;
+  P->uniform36 = true;
+  for (int64_t r = 0; r < nrb; ++r) {
+    if (d->r_dims[r] < 1 || d->r_dims[r] > 16) throw Error(BLS_EUNSUPPORTED, "retained block sizes above 16 are not supported on the device");
+    boff_r[r] = nr; nr += d->r_dims[r];
+    P->max_dr = std::max<int>(P->max_dr, (int)d->r_dims[r]);
+    if (d->r_dims[r] != 6) P->uniform36 = false;
+  }
+  for (int64_t e = 0; e < neb; ++e) {
+    if (d->e_dims[e] < 1 || d->e_dims[e] > 3) throw Error(BLS_EUNSUPPORTED, "eliminated block sizes above 3 are not supported on the device");
+    boff_e[e] = ne; ne += d->e_dims[e];
+    P->max_de = std::max<int>(P->max_de, (int)d->e_dims[e]);
+    if (d->e_dims[e] != 3) P->uniform36 = false;
+    if (d->eoffsets[e] < 0 || d->eliminated_ptr[e + 1] < d->eliminated_ptr[e]) throw Error(BLS_EINVAL, "malformed structure arrays");
+  }
+  P->nr = nr;
+  P->ne = ne;
+  P->E_length = neb ? d->eoffsets[neb - 1] + d->e_dims[neb - 1] * d->e_dims[neb - 1] : 0;
+  int64_t clen = 0;
+  for (int64_t e = 0; e < neb; ++e)
+    for (int64_t c = d->eliminated_ptr[e]; c < d->eliminated_ptr[e + 1]; ++c) {
+      const int64_t r = d->entry_retained[c];
+      if (r < 0 || r >= nrb) throw Error(BLS_EINVAL, "entry_retained out of range");
+      if (c > d->eliminated_ptr[e] && d->entry_retained[c - 1] >= r) throw Error(BLS_EINVAL, "entry_retained must ascend within each eliminated block");
+      clen = std::max(clen, d->coffsets[c] + d->r_dims[r] * d->e_dims[e]);
+    }
+  P->C_length = clen;
+  if (clen >= INT32_MAX || P->E_length >= INT32_MAX || nc >= INT32_MAX) throw Error(BLS_EUNSUPPORTED, "block storage beyond 2^31 entries is not supported");
+  // workspace index (src/schur_reduction.jl:71-85)
+  std::vector<int32_t> entry_elim(nc), rptr(nrb + 1, 0), rentry(nc);
+  for (int64_t e = 0; e < neb; ++e)
+    for (int64_t c = d->eliminated_ptr[e]; c < d->eliminated_ptr[e + 1]; ++c) { entry_elim[c] = (int32_t)e; rptr[d->entry_retained[c] + 1] += 1; }
+  for (int64_t r = 0; r < nrb; ++r) rptr[r + 1] += rptr[r];
+  {
+    std::vector<int32_t> fill(rptr.begin(), rptr.end() - 1);
+    for (int64_t c = 0; c < nc; ++c) rentry[fill[d->entry_retained[c]]++] = (int32_t)c;
+  }
+  // the S blocks: the given pattern, or the couplings' own block pattern for a dense-only plan
+  std::vector<int64_t> bcolptr, browval, brow_off, col_h, Scolptr;
+  P->has_sparse = d->block_colptr != nullptr;
+  if (P->has_sparse) {
+    const int64_t nb = d->block_colptr[nrb];
+    bcolptr.assign(d->block_colptr, d->block_colptr + nrb + 1);
+    browval.assign(d->block_rowval, d->block_rowval + nb);
+    brow_off.assign(d->block_row_offsets, d->block_row_offsets + nb);
+    col_h.assign(d->col_heights, d->col_heights + nrb);
+    Scolptr.assign(d->S_colptr, d->S_colptr + nr + 1);
+    P->nnzS = Scolptr[nr];
+  } else {
+    Structure st;
+    st.nrblocks = nrb; st.neblocks = neb;
+    st.r_dims.assign(d->r_dims, d->r_dims + nrb);
+    st.e_dims.assign(d->e_dims, d->e_dims + neb);
+    std::vector<std::vector<int64_t>> coup(neb);
+    for (int64_t e = 0; e < neb; ++e) coup[e].assign(d->entry_retained + d->eliminated_ptr[e], d->entry_retained + d->eliminated_ptr[e + 1]);
+    finish_structure(st, coup);
+    Pattern pat = build_pattern(st, {});
+    bcolptr = pat.block_colptr; browval = pat.block_rowval; brow_off = pat.block_row_offsets; col_h = pat.col_heights; Scolptr = pat.S_colptr;
+  }
+  const int64_t nb = bcolptr[nrb];
+  P->nblocks = nb;
+  // Every device write must stay inside S: check the pattern the caller handed in before any kernel uses it.
+  if (P->has_sparse) {
+    for (int64_t r2 = 0; r2 < nrb; ++r2) {
+      if (bcolptr[r2 + 1] < bcolptr[r2]) throw Error(BLS_EINVAL, "block_colptr must be non-decreasing");
+      for (int64_t w = 0; w < d->r_dims[r2]; ++w) {
+        const int64_t j = boff_r[r2] + w;
+        if (Scolptr[j] < 0 || Scolptr[j + 1] - Scolptr[j] != col_h[r2]) throw Error(BLS_EINVAL, "S_colptr does not match col_heights");
+      }
+      for (int64_t k = bcolptr[r2]; k < bcolptr[r2 + 1]; ++k) {
+        const int64_t r1 = browval[k];
+        if (r1 < 0 || r1 > r2 || (k > bcolptr[r2] && browval[k - 1] >= r1)) throw Error(BLS_EINVAL, "block_rowval must ascend within each column, upper triangle");
+        if (brow_off[k] < 0 || brow_off[k] + d->r_dims[r1] > col_h[r2]) throw Error(BLS_EINVAL, "block_row_offsets exceed the column height");
+      }
+    }
+    const int64_t nnz = Scolptr[nr];
+    if (d->diag_inds)
+      for (int64_t i = 0; i < nr; ++i)
+        if (d->diag_inds[i] < 0 || d->diag_inds[i] >= nnz) throw Error(BLS_EINVAL, "diag_inds out of range");
+    if (d->r_to_s_map)
+      for (int64_t i = 0; i < d->R_length; ++i)
+        if (d->r_to_s_map[i] < -1 || d->r_to_s_map[i] >= nnz) throw Error(BLS_EINVAL, "r_to_s_map out of range");
+    if (d->S_rowval)
+      for (int64_t q = 0; q < nnz; ++q)
+        if (d->S_rowval[q] < 0 || d->S_rowval[q] >= nr) throw Error(BLS_EINVAL, "S_rowval out of range");
+  }
+  for (int64_t e = 0; e < neb; ++e)
+    for (int64_t c = d->eliminated_ptr[e]; c < d->eliminated_ptr[e + 1]; ++c)
+      if (d->coffsets[c] < 0) throw Error(BLS_EINVAL, "coffsets out of range");
+  std::vector<int32_t> b_r1(nb), b_r2(nb), b_stride(nb);
+  std::vector<int64_t> b_base(nb), b_base_dense(nb);
+  for (int64_t r2 = 0; r2 < nrb; ++r2)
+    for (int64_t k = bcolptr[r2]; k < bcolptr[r2 + 1]; ++k) {
+      b_r1[k] = (int32_t)browval[k];
+      b_r2[k] = (int32_t)r2;
+      b_stride[k] = (int32_t)col_h[r2];
+      b_base[k] = Scolptr[boff_r[r2]] + brow_off[k];
+      b_base_dense[k] = boff_r[browval[k]] + boff_r[r2] * nr;
+    }
+  // pair lists per block, cut into items (columns in parallel; each column's pairs keep ascending c2 per block)
+  std::vector<int64_t> col_npairs(nrb, 0);
+  std::vector<std::vector<int32_t>> col_c1(nrb), col_c2(nrb), col_cnt(nrb);
+  int64_t missing = -1;
+#pragma omp parallel for schedule(dynamic, 8)
+  for (int64_t r2 = 0; r2 < nrb; ++r2) {
+    const int64_t kb = bcolptr[r2], ke = bcolptr[r2 + 1], nbc = ke - kb;
+    std::vector<int32_t> cnt(nbc + 1, 0);
+    std::vector<int32_t> slot_of;   // slot of each pair in visit order
+    std::vector<int32_t> pc1, pc2;
+    for (int32_t q = rptr[r2]; q < rptr[r2 + 1]; ++q) {
+      const int32_t c2 = rentry[q];
+      const int64_t e = entry_elim[c2];
+      for (int64_t c1 = d->eliminated_ptr[e]; c1 <= c2; ++c1) {
+        const int64_t r1 = d->entry_retained[c1];
+        const int64_t* lo = browval.data() + kb;
+        const int64_t* hi = browval.data() + ke;
+        const int64_t* f = std::lower_bound(lo, hi, r1);
+        if (f == hi || *f != r1) {
+#pragma omp critical
+          missing = r1 * nrb + r2;
+          continue;
+        }
+        const int32_t sl = (int32_t)(f - lo);
+        slot_of.push_back(sl);
+        pc1.push_back((int32_t)c1);
+        pc2.push_back(c2);
+        cnt[sl + 1] += 1;
+      }
+    }
+    for (int64_t i = 0; i < nbc; ++i) cnt[i + 1] += cnt[i];
+    std::vector<int32_t> o1(pc1.size()), o2(pc2.size());
+    std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
+    for (size_t i = 0; i < pc1.size(); ++i) {
+      const int32_t sl = slot_of[i];
+      o1[pos[sl]] = pc1[i];
+      o2[pos[sl]++] = pc2[i];
+    }
+    col_c1[r2].swap(o1);
+    col_c2[r2].swap(o2);
+    col_cnt[r2].swap(cnt);
+    col_npairs[r2] = (int64_t)pc1.size();
+  }
+  if (missing >= 0)
+    throw Error(BLS_EPATTERN, "The sparse pattern has no block (" + std::to_string(missing / nrb + 1) + ", " + std::to_string(missing % nrb + 1) + ")");
+  int64_t npairs = 0;
+  for (int64_t r2 = 0; r2 < nrb; ++r2) npairs += col_npairs[r2];
+  if (npairs >= INT32_MAX) throw Error(BLS_EUNSUPPORTED, "more than 2^31 coupling pairs are not supported");
+  P->npairs = npairs;
+  std::vector<int32_t> pair_c1(npairs), pair_c2(npairs), it_block, it_start, it_info;
+  int64_t off = 0;
+  for (int64_t r2 = 0; r2 < nrb; ++r2) {
+    std::copy(col_c1[r2].begin(), col_c1[r2].end(), pair_c1.begin() + off);
+    std::copy(col_c2[r2].begin(), col_c2[r2].end(), pair_c2.begin() + off);
+    const auto& cnt = col_cnt[r2];
+    for (int64_t sl = 0; sl + 1 < (int64_t)cnt.size(); ++sl) {
+      const int32_t a = cnt[sl], b = cnt[sl + 1];
+      if (b == a) continue;
+      const int nchunk = (b - a + PAIR_CHUNK - 1) / PAIR_CHUNK;
+      for (int32_t x = a; x < b; x += PAIR_CHUNK) {
+        it_block.push_back((int32_t)(bcolptr[r2] + sl));
+        it_start.push_back((int32_t)(off + x));
+        it_info.push_back(std::min(PAIR_CHUNK, b - x) | ((nchunk == 1 ? 1 : 0) << 16));
+      }
+    }
+    off += col_npairs[r2];
+    std::vector<int32_t>().swap(col_c1[r2]);
+    std::vector<int32_t>().swap(col_c2[r2]);
+  }
+  P->nitems = (int64_t)it_block.size();
+  // uploads
+  upload(P->r_dims, to32(d->r_dims, nrb, "r_dims"), s);
+  upload(P->boffsets_r, to32(boff_r.data(), nrb, "boffsets_r"), s);
+  upload(P->e_dims, to32(d->e_dims, neb, "e_dims"), s);
+  upload(P->boffsets_e, to32(boff_e.data(), neb, "boffsets_e"), s);
+  upload(P->eoffsets, to32(d->eoffsets, neb, "eoffsets"), s);
+  upload(P->eliminated_ptr, to32(d->eliminated_ptr, neb + 1, "eliminated_ptr"), s);
+  upload(P->entry_retained, to32(d->entry_retained, nc, "entry_retained"), s);
+  upload(P->coffsets, to32(d->coffsets, nc, "coffsets"), s);
+  upload(P->entry_eliminated, entry_elim, s);
+  upload(P->retained_ptr, rptr, s);
+  upload(P->retained_entry, rentry, s);
+  upload(P->block_r1, b_r1, s);
+  upload(P->block_r2, b_r2, s);
+  upload(P->block_stride_sparse, b_stride, s);
+  upload(P->block_base_sparse, b_base, s);
+  upload(P->block_base_dense, b_base_dense, s);
+  upload(P->pair_c1, pair_c1, s);
+  upload(P->pair_c2, pair_c2, s);
+  upload(P->item_block, it_block, s);
+  upload(P->item_start, it_start, s);
+  upload(P->item_info, it_info, s);
+  if (P->has_sparse) {
+    if (d->diag_inds) {
+      P->diag_inds_host.assign(d->diag_inds, d->diag_inds + nr);
+      upload(P->diag_inds, P->diag_inds_host, s);
+    }
+    if (d->r_to_s_map && d->R_length > 0) {
+      P->R_length = d->R_length;
+      std::vector<int64_t> m(d->r_to_s_map, d->r_to_s_map + d->R_length);
+      upload(P->r_to_s, m, s);
+    }
+    if (d->S_rowval) {
+      std::vector<int32_t> rv = to32(d->S_rowval, P->nnzS, "S_rowval");
+      std::vector<int32_t> cl(P->nnzS);
+      for (int64_t j = 0; j < nr; ++j)
+        for (int64_t q = Scolptr[j]; q < Scolptr[j + 1]; ++q) cl[q] = (int32_t)j;
+      upload(P->S_rowval, rv, s);
+      upload(P->S_col, cl, s);
+    }
+  }
+  P->Einv64.alloc(sizeof(double) * std::max<int64_t>(P->E_length, 1));
+  P->Einv32.alloc(sizeof(float) * std::max<int64_t>(P->E_length, 1));
+  P->z.alloc(sizeof(double) * std::max<int64_t>(ne, 1));
+  P->status.alloc(sizeof(Status));
+  Status init{NONE, NONE, NONE, 0};
+  BLS_CUDA(cudaMemcpyAsync(P->status.p, &init, sizeof(Status), cudaMemcpyHostToDevice, s));
+  BLS_CUDA(cudaMallocHost(&P->host_status, sizeof(Status)));
+  BLS_CUDA(cudaStreamSynchronize(s));
+  return P.release();
+}
+
+static int64_t plan_bytes(const SchurPlan* P) {
+  const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
+                          &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
+                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2,
+                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col,
+                          &P->Einv64, &P->Einv32, &P->z, &P->status};
+  int64_t b = 0;
+  for (auto* x : bufs) b += (int64_t)x->bytes;
+  return b;
+}
+
+// Read the status word (synchronises) and turn it into the reference's verdict.
+static int read_status(SchurPlan* P, int64_t* failed_block) {
+  cudaStream_t s = P->ctx->stream;
+  BLS_CUDA(cudaMemcpyAsync(P->host_status, P->status.p, sizeof(Status), cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaStreamSynchronize(s));
+  const Status st = *P->host_status;
+  if (st.einval_r != NONE || st.einval_e != NONE) {
+    const bool r = st.einval_r != NONE;
+    set_error(std::string(r ? "scaling_r" : "scaling_e") + " must be finite and non-negative, but entry " +
+              std::to_string((r ? st.einval_r : st.einval_e) + 1) + " is not");
+    if (failed_block) *failed_block = 0;
+    return BLS_EINVAL;
+  }
+  if (st.failed != NONE) {
+    if (failed_block) *failed_block = st.failed + 1;
+    return BLS_NOT_PD;
+  }
+  if (failed_block) *failed_block = 0;
+  return BLS_OK;
+}
+
+static void check_lambda(double lambda) {
+  if (!(std::isfinite(lambda) && lambda >= 0)) throw Error(BLS_EINVAL, "lambda must be finite and non-negative, got " + std::to_string(lambda));
+}
+
+static void begin_checked(SchurPlan* P, const double* scaling, int64_t n, int which) {
+  cudaStream_t s = P->ctx->stream;
+  k_status_begin<<<1, 1, 0, s>>>(P->status.as<Status>(), which);
+  if (n > 0) k_check_scaling<<<grid_for(n, 256), 256, 0, s>>>(scaling, n, P->status.as<Status>(), which);
+  BLS_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static void reset_sparse(SchurPlan* P, T* S, const T* R, const double* sc, double lambda, const double* s_r) {
+  if (!P->has_sparse || !P->diag_inds.p) throw Error(BLS_EINVAL, "the plan was created without a sparse pattern");
+  if (P->R_length > 0 && !P->r_to_s.p) throw Error(BLS_EINVAL, "the plan has no r -> s map");
+  if (s_r && !P->S_rowval.p) throw Error(BLS_EINVAL, "a conditioning scale needs S_rowval in the plan");
+  cudaStream_t s = P->ctx->stream;
+  Status* st = P->status.as<Status>();
+  begin_checked(P, sc, P->nr, 0);
+  k_fill<T><<<std::min<int64_t>(grid_for(P->nnzS, 256), 148 * 16), 256, 0, s>>>(S, P->nnzS, st);
+  if (P->R_length > 0)
+    k_scatter_r<T><<<std::min<int64_t>(grid_for(P->R_length, 256), 148 * 16), 256, 0, s>>>(S, R, P->r_to_s.as<int64_t>(), P->R_length, st);
+  if (s_r)
+    k_scale_sparse<T><<<std::min<int64_t>(grid_for(P->nnzS, 256), 148 * 16), 256, 0, s>>>(S, P->S_rowval.as<int32_t>(), P->S_col.as<int32_t>(), s_r, P->nnzS, st);
+  k_damp_diag<T><<<grid_for(P->nr, 256), 256, 0, s>>>(S, P->diag_inds.as<int64_t>(), 0, sc, lambda, s_r, P->nr, st);
+  k_reset_done<<<1, 1, 0, s>>>(st);
+  BLS_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static void reset_dense(SchurPlan* P, T* S, const T* R, const double* sc, double lambda, const double* s_r) {
+  cudaStream_t s = P->ctx->stream;
+  Status* st = P->status.as<Status>();
+  begin_checked(P, sc, P->nr, 0);
+  k_copy_scaled_dense<T><<<std::min<int64_t>(grid_for(P->nr * P->nr, 256), 148 * 16), 256, 0, s>>>(S, R, s_r, P->nr, st);
+  k_damp_diag<T><<<grid_for(P->nr, 256), 256, 0, s>>>(S, nullptr, P->nr, sc, lambda, s_r, P->nr, st);
+  k_reset_done<<<1, 1, 0, s>>>(st);
+  BLS_CUDA(cudaGetLastError());
+}
+
+template <class T, int MDE, int MDR>
+static void launch_pairs(SchurPlan* P, T* S, bool dense, const T* C, const double* s_r, const double* s_e) {
+  using TE = typename EinvOf<T>::type;
+  const TE* Einv = std::is_same<T, float>::value ? (const TE*)P->Einv32.p : (const TE*)P->Einv64.p;
+  if (P->nitems == 0) return;
+  k_pairs<T, MDE, MDR><<<grid_for(P->nitems, 128), 128, 0, P->ctx->stream>>>(
+      P->nitems, P->item_block.as<int32_t>(), P->item_start.as<int32_t>(), P->item_info.as<int32_t>(), P->pair_c1.as<int32_t>(),
+      P->pair_c2.as<int32_t>(), P->block_r1.as<int32_t>(), P->block_r2.as<int32_t>(),
+      dense ? P->block_base_dense.as<int64_t>() : P->block_base_sparse.as<int64_t>(), dense ? nullptr : P->block_stride_sparse.as<int32_t>(),
+      P->nr, P->r_dims.as<int32_t>(), P->boffsets_r.as<int32_t>(), P->entry_eliminated.as<int32_t>(), P->e_dims.as<int32_t>(),
+      P->boffsets_e.as<int32_t>(), P->eoffsets.as<int32_t>(), P->coffsets.as<int32_t>(), C, Einv, s_r, s_e, S, P->status.as<Status>());
+}
+
+template <class T>
+static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, const double* b_e, const double* sc_e, double lambda,
+                  const T* E, const T* C, const double* s_r, const double* s_e, int64_t* failed_block) {
+  if (!dense && !P->has_sparse) throw Error(BLS_EINVAL, "the plan was created without a sparse pattern");
+  check_lambda(lambda);
+  cudaStream_t s = P->ctx->stream;
+  Status* st = P->status.as<Status>();
+  begin_checked(P, sc_e, P->ne, 1);
+  k_arm<<<1, 1, 0, s>>>(st);
+  k_factor<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(P->neblocks, P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
+                                                         P->boffsets_e.as<int32_t>(), E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
+                                                         std::is_same<T, float>::value ? P->Einv32.as<float>() : nullptr, P->z.as<double>(), st);
+  if (P->uniform36) launch_pairs<T, 3, 6>(P, S, dense, C, s_r, s_e);
+  else launch_pairs<T, 3, 16>(P, S, dense, C, s_r, s_e);
+  k_gradient<T><<<grid_for(P->nrblocks * 32, 256), 256, 0, s>>>(
+      P->nrblocks, P->retained_ptr.as<int32_t>(), P->retained_entry.as<int32_t>(), P->entry_eliminated.as<int32_t>(), P->r_dims.as<int32_t>(),
+      P->boffsets_r.as<int32_t>(), P->e_dims.as<int32_t>(), P->boffsets_e.as<int32_t>(), P->coffsets.as<int32_t>(), C, P->z.as<double>(), b_r,
+      s_r, s_e, g, st);
+  BLS_CUDA(cudaGetLastError());
+  P->last_dtype = std::is_same<T, float>::value ? BLS_F32 : BLS_F64;
+  if (!failed_block) return BLS_OK;
+  return read_status(P, failed_block);
+}
+
+template <class T>
+static void backsub(SchurPlan* P, double* x_e, const double* x_r, const T* C, const double* s_r, const double* s_e) {
+  k_backsub<T><<<grid_for(P->neblocks, 256), 256, 0, P->ctx->stream>>>(
+      P->neblocks, P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(), P->boffsets_e.as<int32_t>(), P->eliminated_ptr.as<int32_t>(),
+      P->entry_retained.as<int32_t>(), P->coffsets.as<int32_t>(), P->r_dims.as<int32_t>(), P->boffsets_r.as<int32_t>(), C,
+      P->Einv64.as<double>(), P->z.as<double>(), x_r, s_r, s_e, x_e);
+  BLS_CUDA(cudaGetLastError());
+}
+
+}  // namespace bls
+
+// ======================================================================================================================
+// C ABI
+// ======================================================================================================================
+struct bls_schur_plan : bls::SchurPlan {};
+
+using namespace bls;
+
+#define BLS_GUARD(...)                                                        \
+  try {                                                                       \
+    __VA_ARGS__                                                               \
+  } catch (const bls::Error& e) {                                             \
+    bls::set_error(e.what());                                                 \
+    return e.code;                                                            \
+  } catch (const std::bad_alloc&) {                                           \
+    bls::set_error("out of host memory");                                     \
+    return BLS_ENOMEM;                                                        \
+  } catch (const std::exception& e) {                                         \
+    bls::set_error(e.what());                                                 \
+    return BLS_EINVAL;                                                        \
+  }
+
+extern "C" {
+
+int bls_schur_plan_create(bls_ctx* ctx, const bls_schur_plan_desc* desc, bls_schur_plan** out) {
+  BLS_GUARD({
+    if (!ctx || !out) throw Error(BLS_EINVAL, "null argument");
+    BLS_CUDA(cudaSetDevice(ctx->device));
+    *out = static_cast<bls_schur_plan*>(plan_create(ctx, desc));
+    return BLS_OK;
+  })
+}
+
+int bls_schur_plan_destroy(bls_schur_plan* plan) {
+  if (plan) {
+    cudaStreamSynchronize(plan->ctx->stream);
+    delete static_cast<SchurPlan*>(plan);
+  }
+  return BLS_OK;
+}
+
+int64_t bls_schur_plan_device_bytes(const bls_schur_plan* plan) { return plan ? plan_bytes(plan) : 0; }
+
+int bls_reset_schur_sparse(bls_schur_plan* P, int dtype, void* S, const void* R, const double* sc, double lambda, const double* s_r) {
+  BLS_GUARD({
+    check_lambda(lambda);
+    if (dtype == BLS_F64) reset_sparse<double>(P, (double*)S, (const double*)R, sc, lambda, s_r);
+    else if (dtype == BLS_F32) reset_sparse<float>(P, (float*)S, (const float*)R, sc, lambda, s_r);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_reset_schur_dense(bls_schur_plan* P, int dtype, void* S, const void* R, const double* sc, double lambda, const double* s_r) {
+  BLS_GUARD({
+    check_lambda(lambda);
+    if (dtype == BLS_F64) reset_dense<double>(P, (double*)S, (const double*)R, sc, lambda, s_r);
+    else if (dtype == BLS_F32) reset_dense<float>(P, (float*)S, (const float*)R, sc, lambda, s_r);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_reduce_schur_sparse(bls_schur_plan* P, int dtype, void* S, double* g, const double* b_r, const double* b_e, const double* sc_e,
+                            double lambda, const void* E, const void* C, const double* s_r, const double* s_e, int64_t* failed_block) {
+  BLS_GUARD({
+    if (dtype == BLS_F64) return reduce<double>(P, (double*)S, false, g, b_r, b_e, sc_e, lambda, (const double*)E, (const double*)C, s_r, s_e, failed_block);
+    if (dtype == BLS_F32) return reduce<float>(P, (float*)S, false, g, b_r, b_e, sc_e, lambda, (const float*)E, (const float*)C, s_r, s_e, failed_block);
+    throw Error(BLS_EINVAL, "unknown dtype");
+  })
+}
+
+int bls_reduce_schur_dense(bls_schur_plan* P, int dtype, void* S, double* g, const double* b_r, const double* b_e, const double* sc_e,
+                           double lambda, const void* E, const void* C, const double* s_r, const double* s_e, int64_t* failed_block) {
+  BLS_GUARD({
+    if (dtype == BLS_F64) return reduce<double>(P, (double*)S, true, g, b_r, b_e, sc_e, lambda, (const double*)E, (const double*)C, s_r, s_e, failed_block);
+    if (dtype == BLS_F32) return reduce<float>(P, (float*)S, true, g, b_r, b_e, sc_e, lambda, (const float*)E, (const float*)C, s_r, s_e, failed_block);
+    throw Error(BLS_EINVAL, "unknown dtype");
+  })
+}
+
+int bls_schur_query_status(bls_schur_plan* P, int64_t* failed_block) {
+  BLS_GUARD({ return read_status(P, failed_block); })
+}
+
+int bls_backsubstitute(bls_schur_plan* P, int dtype, double* x_e, const double* x_r, const void* C, const double* s_r, const double* s_e) {
+  BLS_GUARD({
+    if (dtype == BLS_F64) backsub<double>(P, x_e, x_r, (const double*)C, s_r, s_e);
+    else if (dtype == BLS_F32) backsub<float>(P, x_e, x_r, (const float*)C, s_r, s_e);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_scatter_copy(bls_ctx* ctx, int dtype, void* dest, const void* src, const int64_t* map, int64_t n) {
+  BLS_GUARD({
+    if (n <= 0) return BLS_OK;
+    const int grid = (int)std::min<int64_t>(grid_for(n, 256), 148 * 16);
+    if (dtype == BLS_F64) k_gather<double><<<grid, 256, 0, ctx->stream>>>((double*)dest, (const double*)src, map, n);
+    else if (dtype == BLS_F32) k_gather<float><<<grid, 256, 0, ctx->stream>>>((float*)dest, (const float*)src, map, n);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    BLS_CUDA(cudaGetLastError());
+    return BLS_OK;
+  })
+}
+
+}  // extern "C"

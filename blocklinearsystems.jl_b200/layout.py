@@ -1,0 +1,190 @@
+"""Host-side layout of an elimination, mirroring BlockLinearSystems.jl's structure API (0-based).
+
+SchurStructure            src/schur_structure.jl:50-166, src/schur_description.jl:16-101
+build_schur_pattern       src/schur_structure.jl:241-323
+build_r_to_s_map          src/schur_structure.jl:406-431 (block-level form)
+sparse_with_map           src/SparseBlockLinearSystem.jl:233-282, 343-354 (makesparseindices + the scatter map)
+
+All integer results are computed by the native library (libblsgpu.so); this module only marshals arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ptr64
+
+DEFAULT_MIN_WORK = 4096   # src/threading.jl:24
+
+
+def _csr(lists) -> tuple[np.ndarray, np.ndarray]:
+    """A list of index lists, or a (ptr, idx) pair, as int64 CSR arrays."""
+    if isinstance(lists, tuple) and len(lists) == 2 and isinstance(lists[0], np.ndarray):
+        return np.ascontiguousarray(lists[0], np.int64), np.ascontiguousarray(lists[1], np.int64)
+    ptr = np.zeros(len(lists) + 1, np.int64)
+    ptr[1:] = np.cumsum([len(x) for x in lists])
+    idx = np.fromiter((int(v) for x in lists for v in x), np.int64, count=int(ptr[-1]))
+    return ptr, idx
+
+
+class SchurStructure:
+    """The layout of an elimination on the Hessian path (src/schur_structure.jl:1-49).
+
+    SchurStructure(blocksizes, rowblocks, eliminated=..., nchunks=1, min_work=4096) lays out a description in the
+    caller's numbering (0-based column blocks; `rowblocks` a list of index lists or a (ptr, idx) CSR pair).
+    SchurStructure.positional(r_dims, e_dims, couplings) is the positional constructor. Array attributes are 0-based
+    int64 numpy arrays; `chunks` / `col_chunks` are flattened half-open ranges.
+    """
+
+    _FIELDS = ("r_dims", "e_dims", "boffsets_r", "boffsets_e", "eoffsets", "eliminated_ptr", "entry_retained", "coffsets",
+               "order", "chunks", "retained_ptr", "retained_entry", "entry_eliminated", "col_chunks", "retained_pairs")
+    _SCALARS = ("nr", "ne", "nrblocks", "neblocks", "max_coupled_dim", "E_length", "C_length", "nchunks", "min_work")
+
+    def __init__(self, blocksizes=None, rowblocks=None, *, eliminated=None, nchunks: int = 1, min_work: int = DEFAULT_MIN_WORK,
+                 _handle=None):
+        L = _lib.gpu()
+        if _handle is None:
+            if eliminated is None:
+                raise TypeError("eliminated is required")
+            bs = np.ascontiguousarray(blocksizes, np.int64)
+            el = np.ascontiguousarray(np.asarray(eliminated, bool), np.uint8)
+            if len(el) != len(bs):
+                raise _lib.DimensionMismatch(f"eliminated has length {len(el)}, but there are {len(bs)} column blocks")
+            ptr, idx = _csr(rowblocks)
+            h = C.c_void_p()
+            check(L.bls_structure_from_description(len(bs), ptr64(bs), len(ptr) - 1, ptr64(ptr), ptr64(idx),
+                                                   el.ctypes.data_as(C.POINTER(C.c_uint8)), int(nchunks), int(min_work),
+                                                   C.byref(h)))
+            _handle = h
+        self._h = _handle
+        for f in self._SCALARS:
+            setattr(self, f, int(self._field(f)[0]))
+        for f in self._FIELDS:
+            setattr(self, f, self._field(f))
+        self.retained_pairs = self.retained_pairs.reshape(-1, 2)
+
+    @classmethod
+    def positional(cls, r_dims, e_dims, couplings, *, nchunks: int = 1, min_work: int = DEFAULT_MIN_WORK) -> "SchurStructure":
+        rd = np.ascontiguousarray(r_dims, np.int64)
+        ed = np.ascontiguousarray(e_dims, np.int64)
+        ptr, idx = _csr(couplings)
+        h = C.c_void_p()
+        check(_lib.gpu().bls_structure_positional(len(rd), ptr64(rd), len(ed), ptr64(ed), ptr64(ptr), ptr64(idx), int(nchunks),
+                                                  int(min_work), C.byref(h)))
+        return cls(_handle=h)
+
+    def _field(self, name: str) -> np.ndarray:
+        L = _lib.gpu()
+        n = L.bls_structure_field(self._h, name.encode(), None)
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, np.int64)
+        if n:
+            L.bls_structure_field(self._h, name.encode(), ptr64(out))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib._gpu is not None:
+            _lib.gpu().bls_structure_destroy(h)
+            self._h = None
+
+    # accessors (src/schur_description.jl:199-214)
+    def blockorder(self) -> np.ndarray:
+        return self.order.copy()
+
+    def nretained(self) -> int:
+        return self.nrblocks
+
+    def nblocks(self) -> int:
+        return self.nrblocks + self.neblocks
+
+    def blocksizes(self) -> np.ndarray:
+        return np.concatenate([self.r_dims, self.e_dims])
+
+    def position(self) -> np.ndarray:
+        """Layout position of each caller block (invperm of blockorder)."""
+        p = np.empty_like(self.order)
+        p[self.order] = np.arange(len(self.order))
+        return p
+
+    @property
+    def handle(self):
+        return self._h
+
+
+@dataclass
+class SchurPattern:
+    """build_schur_pattern's result (src/schur_structure.jl:314-322), 0-based, plus the sparse retained storage laid
+    out on it (src/schur_hessian.jl:286): R_block_start per block (the block (r2, r1) of R for the k-th pattern block
+    (r1, r2)) and R_length."""
+    block_colptr: np.ndarray
+    block_rowval: np.ndarray
+    block_row_offsets: np.ndarray
+    col_heights: np.ndarray
+    S_colptr: np.ndarray
+    S_rowval: np.ndarray
+    diag_inds: np.ndarray
+    R_block_start: np.ndarray
+    R_length: int
+    _h: object = None
+
+    @property
+    def nnz(self) -> int:
+        return int(self.S_colptr[-1])
+
+    def R_diag_start(self, nrblocks: int) -> np.ndarray:
+        """Start of each retained block's diagonal block in the retained storage."""
+        out = np.empty(nrblocks, np.int64)
+        for r in range(nrblocks):
+            lo, hi = self.block_colptr[r], self.block_colptr[r + 1]
+            k = lo + np.searchsorted(self.block_rowval[lo:hi], r)
+            out[r] = self.R_block_start[k]
+        return out
+
+    def __del__(self):
+        if self._h is not None and _lib._gpu is not None:
+            _lib.gpu().bls_pattern_destroy(self._h)
+            self._h = None
+
+
+def build_schur_pattern(structure: SchurStructure, extra_blocks=()) -> SchurPattern:
+    """build_schur_pattern(structure; extra_blocks) (src/schur_structure.jl:241-323)."""
+    L = _lib.gpu()
+    ex = np.ascontiguousarray(np.asarray(list(extra_blocks), np.int64).reshape(-1, 2))
+    h = C.c_void_p()
+    check(L.bls_schur_pattern_build(structure.handle, len(ex), ptr64(ex) if len(ex) else None, C.byref(h)))
+
+    def f(name):
+        n = L.bls_pattern_field(h, name.encode(), None)
+        out = np.empty(n, np.int64)
+        if n:
+            L.bls_pattern_field(h, name.encode(), ptr64(out))
+        return out
+
+    return SchurPattern(f("block_colptr"), f("block_rowval"), f("block_row_offsets"), f("col_heights"), f("S_colptr"),
+                        f("S_rowval"), f("diag_inds"), f("R_block_start"), int(f("R_length")[0]), h)
+
+
+def build_r_to_s_map(structure: SchurStructure, pattern: SchurPattern) -> np.ndarray:
+    """build_r_to_s_map(R, pattern, boffsets_r) (src/schur_structure.jl:406-431) for the retained storage on the
+    pattern; -1 marks an unmapped entry (the reference's 0)."""
+    out = np.empty(pattern.R_length, np.int64)
+    check(_lib.gpu().bls_build_r_to_s_map(structure.handle, pattern._h, ptr64(out)))
+    return out
+
+
+def sparse_with_map(structure: SchurStructure, pattern: SchurPattern, symmetric: bool = False):
+    """makesparseindices + sparse_with_map (src/SparseBlockLinearSystem.jl:233-282, 343-354) for the retained storage:
+    returns (colptr, rowval, scatter_map), 0-based; the CSC values are storage[scatter_map]."""
+    L = _lib.gpu()
+    n = L.bls_sparse_indices(structure.handle, pattern._h, int(symmetric), None, None, None)
+    check(int(n) if n < 0 else 0)
+    colptr = np.empty(structure.nr + 1, np.int64)
+    rowval = np.empty(n, np.int64)
+    smap = np.empty(n, np.int64)
+    L.bls_sparse_indices(structure.handle, pattern._h, int(symmetric), ptr64(colptr), ptr64(rowval), ptr64(smap))
+    return colptr, rowval, smap

@@ -1,0 +1,166 @@
+/*
+ * blsgpu.h — C ABI of libblsgpu.so, the B200 (sm_100a) implementation of BlockLinearSystems.jl's elimination path.
+ *
+ * Conventions
+ *   - Plain C types only. Integers are int64_t; every index and offset is 0-based (the Julia caller subtracts 1).
+ *   - Arrays named *_dev are device pointers on the context's device; everything else is host memory.
+ *   - `dtype` selects the element type T of the block storage (R, E, C, S, factored tables): BLS_F64 or BLS_F32.
+ *     Gradients, right-hand sides, solutions, lambda, damping scalings and conditioning scales are always double,
+ *     as in the reference (src/schur_linear_systems.jl:11-13, src/schur_reduction.jl:21, src/qr_reduction.jl:8-10).
+ *     With BLS_F32 the kernels run the mixed form: FP32 storage and FP32 pair products and accumulation, with the
+ *     damped point-block inverse, z = E^-1 b_e, the gradient and the QR column norms / reflector scaling in FP64.
+ *   - Work runs on the context's stream. A call that takes a host `int64_t* failed_block` synchronises and returns the
+ *     reduction's verdict; passing NULL makes the call asynchronous (read it later with the *_query_status call).
+ *   - Nothing here allocates device memory except the create calls (contexts, plans); kernels only use the caller's
+ *     buffers and the plan's own scratch.
+ *
+ * Status codes: BLS_OK, BLS_NOT_PD (the reference's `false`: a singular / non-finite eliminated block; the lowest
+ * such block, 1-based as the reference's failed_block[], is reported), and negative errors. Argument errors are
+ * reported before any output is written, as the reference throws before any work (src/utils.jl:100-107).
+ */
+#ifndef BLSGPU_H
+#define BLSGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BLS_OK 0
+#define BLS_NOT_PD 1          /* reduce_schur_*! / reduce_qr! returned false (src/schur_reduction.jl:233-257) */
+#define BLS_EINVAL (-1)       /* ArgumentError (bad lambda / scaling / structure) */
+#define BLS_EDIM (-2)         /* DimensionMismatch */
+#define BLS_EPATTERN (-3)     /* a block missing from the sparse pattern (throw_missing_block, src/utils.jl:109) */
+#define BLS_ECUDA (-4)        /* a CUDA runtime error */
+#define BLS_EUNSUPPORTED (-5) /* a size this build does not handle (see the call's comment) */
+#define BLS_ENOMEM (-6)
+
+#define BLS_F64 0
+#define BLS_F32 1
+
+typedef struct bls_ctx bls_ctx;
+typedef struct bls_structure bls_structure;
+typedef struct bls_pattern bls_pattern;
+typedef struct bls_schur_plan bls_schur_plan;
+typedef struct bls_qr_structure bls_qr_structure;
+typedef struct bls_qr_plan bls_qr_plan;
+
+int bls_version(void);
+/* Message of the last error on the calling thread. */
+const char* bls_last_error(void);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Context: one device, one stream.
+ * ------------------------------------------------------------------------------------------------------------- */
+int bls_ctx_create(int device, bls_ctx** out);
+int bls_ctx_destroy(bls_ctx* ctx);
+/* Run the context's work on `cuda_stream` (a cudaStream_t; NULL = the legacy default stream). */
+int bls_ctx_set_stream(bls_ctx* ctx, void* cuda_stream);
+int bls_ctx_synchronize(bls_ctx* ctx);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Host-side layout (integer, bit-exact with the reference). A Julia caller already has these from its own
+ * SchurStructure and may skip straight to bls_schur_plan_create; the Python mirror builds them here.
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* SchurStructure(blocksizes, rowblocks; eliminated, nchunks, min_work) (src/schur_description.jl:97-101,
+ * describe_elimination :16-89, sort_schur_blocks src/schur_structure.jl:204-228, constructor :70-166).
+ * rowblocks in CSR form: row block k touches column blocks rowblock_idx[rowblock_ptr[k] .. rowblock_ptr[k+1]). */
+int bls_structure_from_description(int64_t nblocks, const int64_t* blocksizes, int64_t nrowblocks,
+                                   const int64_t* rowblock_ptr, const int64_t* rowblock_idx, const uint8_t* eliminated,
+                                   int64_t nchunks, int64_t min_work, bls_structure** out);
+/* The positional constructor SchurStructure(r_dims, e_dims, couplings) (src/schur_structure.jl:70-166).
+ * couplings in CSR form over the eliminated blocks, retained indices 0-based. */
+int bls_structure_positional(int64_t nrblocks, const int64_t* r_dims, int64_t neblocks, const int64_t* e_dims,
+                             const int64_t* coupling_ptr, const int64_t* coupling_idx, int64_t nchunks,
+                             int64_t min_work, bls_structure** out);
+/* Field getter: returns the field's length and copies it into `out` when `out` is not NULL; -1 for an unknown name.
+ * Fields: nr nrblocks neblocks r_dims e_dims boffsets_r boffsets_e eoffsets eliminated_ptr entry_retained coffsets
+ * max_coupled_dim order retained_pairs chunks retained_ptr retained_entry entry_eliminated col_chunks. */
+int64_t bls_structure_field(const bls_structure* st, const char* name, int64_t* out);
+int bls_structure_destroy(bls_structure* st);
+
+/* build_schur_pattern(structure; extra_blocks) (src/schur_structure.jl:241-323). extra_pairs: nextra (i, j) pairs.
+ * Fields: block_colptr block_rowval block_row_offsets col_heights S_colptr S_rowval diag_inds, and for the sparse
+ * retained storage on that pattern (src/schur_hessian.jl:286): R_block_start R_length. */
+int bls_schur_pattern_build(const bls_structure* st, int64_t nextra, const int64_t* extra_pairs, bls_pattern** out);
+int64_t bls_pattern_field(const bls_pattern* p, const char* name, int64_t* out);
+int bls_pattern_destroy(bls_pattern* p);
+/* build_r_to_s_map(R, pattern, boffsets_r), block-level form (src/schur_structure.jl:406-431), for the retained
+ * storage laid out on the pattern. out[R_length]; -1 marks an unmapped entry (the reference's 0). */
+int bls_build_r_to_s_map(const bls_structure* st, const bls_pattern* p, int64_t* out);
+/* makesparseindices / sparse_with_map (src/SparseBlockLinearSystem.jl:233-282, 343-354) for that retained storage:
+ * the CSC pattern (colptr[nr+1], rowval[nnz]) and the integer scatter map[nnz] (0-based positions in the storage).
+ * Returns nnz (pass NULL outputs to query it), or a negative status. */
+int64_t bls_sparse_indices(const bls_structure* st, const bls_pattern* p, int symmetric, int64_t* colptr,
+                           int64_t* rowval, int64_t* map);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Device plan of a Schur elimination: the structure and pattern uploaded once, plus the plan's scratch (the
+ * E_inv / z caches of SchurReductionWorkspace, src/schur_reduction.jl:16-27, and a status word).
+ * ------------------------------------------------------------------------------------------------------------- */
+typedef struct bls_schur_plan_desc {
+  int64_t nrblocks, neblocks;
+  const int64_t* r_dims;          /* [nrblocks] */
+  const int64_t* e_dims;          /* [neblocks]; 1..3 supported on the device */
+  const int64_t* eliminated_ptr;  /* [neblocks+1] point-major CSR of the couplings */
+  const int64_t* entry_retained;  /* [ncouplings] ascending within each eliminated block */
+  const int64_t* coffsets;        /* [ncouplings] start of each d_e x d_r coupling block in C_data */
+  const int64_t* eoffsets;        /* [neblocks]  start of each d_e x d_e block in E_data */
+  /* sparse pattern (may be NULL for a dense-only plan) */
+  const int64_t* block_colptr;      /* [nrblocks+1] */
+  const int64_t* block_rowval;      /* [nblocks_S] */
+  const int64_t* block_row_offsets; /* [nblocks_S] */
+  const int64_t* col_heights;       /* [nrblocks] */
+  const int64_t* S_colptr;          /* [nr+1] */
+  const int64_t* S_rowval;          /* [nnz_S] (needed only for conditioning scales) */
+  const int64_t* diag_inds;         /* [nr] */
+  const int64_t* r_to_s_map;        /* [R_length], -1 = unmapped */
+  int64_t R_length;
+} bls_schur_plan_desc;
+
+int bls_schur_plan_create(bls_ctx* ctx, const bls_schur_plan_desc* desc, bls_schur_plan** out);
+int bls_schur_plan_destroy(bls_schur_plan* plan);
+/* Device bytes the plan holds (index arrays + scratch). */
+int64_t bls_schur_plan_device_bytes(const bls_schur_plan* plan);
+
+/* reset_schur_sparse!(nzval, R_nzval, r_to_s_map, diag_inds, scaling_r, lambda, ws, s_r)
+ * (src/schur_reduction.jl:416-436): S = R + lambda*diag(scaling_r) (scaled by s_r when given), failure word reset.
+ * scaling_r_dev[nr]; s_r_dev may be NULL (UnitScale). */
+int bls_reset_schur_sparse(bls_schur_plan* plan, int dtype, void* S_nzval_dev, const void* R_data_dev,
+                           const double* scaling_r_dev, double lambda, const double* s_r_dev);
+/* reset_schur_dense!(S, R, scaling_r, lambda, ws, s_r) (src/schur_reduction.jl:389-407); S and R column-major nr x nr. */
+int bls_reset_schur_dense(bls_schur_plan* plan, int dtype, void* S_dev, const void* R_dev,
+                          const double* scaling_r_dev, double lambda, const double* s_r_dev);
+
+/* reduce_schur_sparse!(S, g_S, b_r, b_e, scaling_e, lambda, structure, E_data, C_data, block_colptr, block_rowval,
+ * block_row_offsets, col_heights, ws, s_r, s_e) (src/schur_reduction.jl:489-507): S.nzval -= C' E^-1 C over every
+ * eliminated block, g_S = s_r.*b_r - C' E^-1 b_e. S_nzval must hold the reset system. Returns BLS_OK, BLS_NOT_PD
+ * (failed_block = lowest failing eliminated block, 1-based; S and g_S then untouched) or an error.
+ * failed_block NULL: asynchronous, query with bls_schur_query_status. */
+int bls_reduce_schur_sparse(bls_schur_plan* plan, int dtype, void* S_nzval_dev, double* g_S_dev, const double* b_r_dev,
+                            const double* b_e_dev, const double* scaling_e_dev, double lambda, const void* E_data_dev,
+                            const void* C_data_dev, const double* s_r_dev, const double* s_e_dev,
+                            int64_t* failed_block);
+/* reduce_schur_dense!(S, g_S, b_r, b_e, scaling_e, lambda, structure, E_data, C_data, ws, s_r, s_e)
+ * (src/schur_reduction.jl:465-479): the same into the upper triangle of a column-major nr x nr S. */
+int bls_reduce_schur_dense(bls_schur_plan* plan, int dtype, void* S_dev, double* g_S_dev, const double* b_r_dev,
+                           const double* b_e_dev, const double* scaling_e_dev, double lambda, const void* E_data_dev,
+                           const void* C_data_dev, const double* s_r_dev, const double* s_e_dev,
+                           int64_t* failed_block);
+/* Status of the last reduction on this plan (synchronises): BLS_OK / BLS_NOT_PD / BLS_EINVAL. */
+int bls_schur_query_status(bls_schur_plan* plan, int64_t* failed_block);
+
+/* backsubstitute!(x_e, x_r, structure, C_data, ws, s_r, s_e) (src/schur_reduction.jl:519-576):
+ * x_e = z - E^-1 sum_r C_er x_r per eliminated block, from the caches of the last successful reduction. */
+int bls_backsubstitute(bls_schur_plan* plan, int dtype, double* x_e_dev, const double* x_r_dev,
+                       const void* C_data_dev, const double* s_r_dev, const double* s_e_dev);
+
+/* copyto!(csc, bsm, scatter_map) (src/SparseBlockLinearSystem.jl:356-362): dest[i] = src[map[i]], i < n. */
+int bls_scatter_copy(bls_ctx* ctx, int dtype, void* dest_dev, const void* src_dev, const int64_t* map_dev, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BLSGPU_H */

@@ -1,0 +1,259 @@
+"""ctypes wrapper of the oracle (liboracle.so): a CPU restatement of BlockLinearSystems.jl's elimination path.
+
+Test and baseline infrastructure only: tests/, __graft_entry__.smoke() and bench.py's CPU baseline use it as the checker
+or the timed CPU reference. The product never imports it. Integers are 0-based at this boundary.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_L = None
+i64, p64, vp, pd = C.c_int64, C.POINTER(C.c_int64), C.c_void_p, C.POINTER(C.c_double)
+pf = C.POINTER(C.c_float)
+pu8 = C.POINTER(C.c_uint8)
+
+
+class OracleError(Exception):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return HERE / "liboracle.so"
+
+
+def lib() -> C.CDLL:
+    global _L
+    if _L is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            build()
+        L = C.CDLL(str(path))
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_structure_field.restype = i64
+        L.orc_pattern_field.restype = i64
+        L.orc_work_field.restype = i64
+        L.orc_qr_field.restype = i64
+        L.orc_sparse_indices.restype = i64
+        _L = L
+    return _L
+
+
+def _p(a):
+    if a is None:
+        return None
+    if a.dtype == np.int64:
+        return a.ctypes.data_as(p64)
+    if a.dtype == np.float64:
+        return a.ctypes.data_as(pd)
+    if a.dtype == np.float32:
+        return a.ctypes.data_as(pf)
+    if a.dtype == np.uint8:
+        return a.ctypes.data_as(pu8)
+    raise TypeError(a.dtype)
+
+
+def _chk(rc):
+    if rc < 0:
+        raise OracleError(rc, lib().orc_last_error().decode())
+    return rc
+
+
+def _csr(lists):
+    if isinstance(lists, tuple):
+        return np.ascontiguousarray(lists[0], np.int64), np.ascontiguousarray(lists[1], np.int64)
+    ptr = np.zeros(len(lists) + 1, np.int64)
+    ptr[1:] = np.cumsum([len(x) for x in lists])
+    idx = np.array([v for x in lists for v in x], np.int64)
+    return ptr, idx
+
+
+class Structure:
+    SCALARS = ("nr", "nrblocks", "neblocks", "max_coupled_dim")
+    FIELDS = ("r_dims", "e_dims", "boffsets_r", "boffsets_e", "eoffsets", "eliminated_ptr", "entry_retained", "coffsets",
+              "order", "retained_pairs", "chunks")
+
+    def __init__(self, h):
+        self.h = h
+        for f in self.SCALARS:
+            setattr(self, f, int(self.field(f)[0]))
+        for f in self.FIELDS:
+            setattr(self, f, self.field(f))
+        self.ne = int(self.e_dims.sum())
+        self.E_length = int((self.e_dims ** 2).sum())
+        self.C_length = int(sum(self.r_dims[r] * self.e_dims[e] for e in range(self.neblocks)
+                                for r in self.entry_retained[self.eliminated_ptr[e]:self.eliminated_ptr[e + 1]]))
+
+    @classmethod
+    def from_description(cls, blocksizes, rowblocks, eliminated, nchunks=1, min_work=4096):
+        bs = np.ascontiguousarray(blocksizes, np.int64)
+        el = np.ascontiguousarray(np.asarray(eliminated, bool), np.uint8)
+        ptr, idx = _csr(rowblocks)
+        h = vp()
+        _chk(lib().orc_structure_from_description(i64(len(bs)), _p(bs), i64(len(ptr) - 1), _p(ptr), _p(idx), _p(el), i64(nchunks),
+                                                  i64(min_work), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def positional(cls, r_dims, e_dims, couplings, nchunks=1, min_work=4096):
+        rd = np.ascontiguousarray(r_dims, np.int64)
+        ed = np.ascontiguousarray(e_dims, np.int64)
+        ptr, idx = _csr(couplings)
+        h = vp()
+        _chk(lib().orc_structure_positional(i64(len(rd)), _p(rd), i64(len(ed)), _p(ed), _p(ptr), _p(idx), i64(nchunks), i64(min_work),
+                                            C.byref(h)))
+        return cls(h)
+
+    def field(self, name):
+        n = lib().orc_structure_field(self.h, name.encode(), None)
+        out = np.empty(n, np.int64)
+        if n:
+            lib().orc_structure_field(self.h, name.encode(), _p(out))
+        return out
+
+    def __del__(self):
+        if self.h and _L is not None:
+            _L.orc_structure_free(self.h)
+            self.h = None
+
+
+class Pattern:
+    FIELDS = ("block_colptr", "block_rowval", "block_row_offsets", "col_heights", "S_colptr", "S_rowval", "diag_inds", "R_block_start")
+
+    def __init__(self, st: Structure, extra=()):
+        ex = np.ascontiguousarray(np.asarray(list(extra), np.int64).reshape(-1, 2))
+        h = vp()
+        _chk(lib().orc_schur_pattern(st.h, i64(len(ex)), _p(ex) if len(ex) else None, C.byref(h)))
+        self.h = h
+        self.st = st
+        for f in self.FIELDS:
+            n = lib().orc_pattern_field(h, f.encode(), None)
+            a = np.empty(n, np.int64)
+            if n:
+                lib().orc_pattern_field(h, f.encode(), _p(a))
+            setattr(self, f, a)
+        a = np.empty(1, np.int64)
+        lib().orc_pattern_field(h, b"R_length", _p(a))
+        self.R_length = int(a[0])
+        self.nnz = int(self.S_colptr[-1])
+
+    def r_to_s_map(self):
+        out = np.empty(self.R_length, np.int64)
+        _chk(lib().orc_r_to_s_map(self.st.h, self.h, _p(out)))
+        return out
+
+    def sparse_indices(self, symmetric=False):
+        n = lib().orc_sparse_indices(self.st.h, self.h, int(symmetric), None, None, None)
+        colptr = np.empty(self.st.nr + 1, np.int64)
+        rowval = np.empty(n, np.int64)
+        m = np.empty(n, np.int64)
+        lib().orc_sparse_indices(self.st.h, self.h, int(symmetric), _p(colptr), _p(rowval), _p(m))
+        return colptr, rowval, m
+
+    def __del__(self):
+        if getattr(self, "h", None) and _L is not None:
+            _L.orc_pattern_free(self.h)
+            self.h = None
+
+
+class Work:
+    def __init__(self, st: Structure, nchunks=1, f32=False):
+        h = vp()
+        _chk(lib().orc_work_new(st.h, i64(nchunks), int(f32), C.byref(h)))
+        self.h, self.st, self.f32 = h, st, f32
+
+    def field(self, name):
+        n = lib().orc_work_field(self.h, name.encode(), None)
+        out = np.empty(n, np.int64)
+        if n:
+            lib().orc_work_field(self.h, name.encode(), _p(out))
+        return out
+
+    def caches(self):
+        Einv = np.empty(self.st.E_length, np.float32 if self.f32 else np.float64)
+        z = np.empty(self.st.ne)
+        lib().orc_work_caches(self.h, Einv.ctypes.data_as(vp), _p(z))
+        return Einv, z
+
+    def __del__(self):
+        if self.h and _L is not None:
+            _L.orc_work_free(self.h)
+            self.h = None
+
+
+def _sfx(a):
+    return "f32" if a.dtype == np.float32 else "f64"
+
+
+def reset_schur_sparse(st, pat, nzval, R, scaling_r, lam, s_r=None):
+    f = getattr(lib(), "orc_reset_schur_sparse_" + _sfx(nzval))
+    return _chk(f(st.h, pat.h, _p(nzval), _p(R), _p(scaling_r), C.c_double(lam), _p(s_r)))
+
+
+def reset_schur_dense(st, S, R, scaling_r, lam, s_r=None):
+    f = getattr(lib(), "orc_reset_schur_dense_" + _sfx(S))
+    return _chk(f(st.h, _p(S), _p(R), _p(scaling_r), C.c_double(lam), _p(s_r)))
+
+
+def reduce_schur_sparse(st, pat, work, nzval, g, b_r, b_e, scaling_e, lam, E, Cd, s_r=None, s_e=None, nthreads=1):
+    fb = C.c_int64(0)
+    f = getattr(lib(), "orc_reduce_schur_sparse_" + _sfx(nzval))
+    rc = _chk(f(st.h, pat.h, work.h, _p(nzval), _p(g), _p(b_r), _p(b_e), _p(scaling_e), C.c_double(lam), _p(E), _p(Cd), _p(s_r), _p(s_e),
+                C.c_int(nthreads), C.byref(fb)))
+    return rc == 0, int(fb.value)
+
+
+def reduce_schur_dense(st, work, S, g, b_r, b_e, scaling_e, lam, E, Cd, s_r=None, s_e=None, nthreads=1):
+    fb = C.c_int64(0)
+    f = getattr(lib(), "orc_reduce_schur_dense_" + _sfx(S))
+    rc = _chk(f(st.h, work.h, _p(S), _p(g), _p(b_r), _p(b_e), _p(scaling_e), C.c_double(lam), _p(E), _p(Cd), _p(s_r), _p(s_e),
+                C.c_int(nthreads), C.byref(fb)))
+    return rc == 0, int(fb.value)
+
+
+def backsubstitute(st, work, x_e, x_r, Cd, s_r=None, s_e=None, nthreads=1):
+    f = getattr(lib(), "orc_backsubstitute_" + _sfx(Cd))
+    return _chk(f(st.h, work.h, _p(x_e), _p(x_r), _p(Cd), _p(s_r), _p(s_e), C.c_int(nthreads)))
+
+
+def sort_schur_blocks(is_elim, sizes, couplings):
+    el = np.ascontiguousarray(np.asarray(is_elim, bool), np.uint8)
+    sz = np.ascontiguousarray(sizes, np.int64)
+    ptr, idx = _csr(couplings)
+    out = np.empty(len(sz), np.int64)
+    _chk(lib().orc_sort_schur_blocks(i64(len(sz)), _p(el), _p(sz), _p(ptr), _p(idx), _p(out)))
+    return out
+
+
+def expand_block_perm(perm, sizes):
+    pm = np.ascontiguousarray(perm, np.int64)
+    sz = np.ascontiguousarray(sizes, np.int64)
+    out = np.empty(int(sz.sum()), np.int64)
+    _chk(lib().orc_expand_block_perm(i64(len(sz)), _p(pm), _p(sz), _p(out)))
+    return out
+
+
+def inv_sym_block(H, damp, generic=False):
+    H = np.asfortranarray(H)
+    d = H.shape[0]
+    inv = np.zeros((d, d), H.dtype, order="F")
+    hp = np.ascontiguousarray(H.ravel(order="F"))
+    dm = np.ascontiguousarray(damp, H.dtype)
+    out = np.zeros(d * d, H.dtype)
+    if generic:
+        ok = lib().orc_inv_sym_block_generic_f64(C.c_int(d), _p(hp), _p(dm), _p(out))
+    else:
+        f = lib().orc_inv_sym_block_f32 if H.dtype == np.float32 else lib().orc_inv_sym_block_f64
+        ok = f(C.c_int(d), _p(hp), _p(dm), _p(out))
+    return bool(ok), out.reshape(d, d, order="F")
+
+
+def max_threads():
+    return lib().orc_max_threads()

@@ -1,0 +1,212 @@
+"""Device Schur reduction through the C ABI against the oracle (the reference's algorithm restated on the CPU).
+
+FP64: S, g_S and the back-substituted x_e within 1e-12 relative of the oracle (test/schur.jl:223-237 bounds the
+reference's own solutions at 1e-12; the device sums in another order, as the reference's threaded path does, which
+test/schur.jl:399-400 bounds at 1e-13). Mixed form (FP32 storage and accumulation, FP64 inverse): against the FP64
+oracle on the same FP32 inputs, within 1e-4 relative in S (FP32 accumulation of ~k^2 terms of size |C|^2/|E|).
+Failure reporting (lowest failing block, outputs untouched), argument checks, dense and sparse, conditioning scales.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle as orc
+from fixtures import COUPLED_GROUPS, GAUGE, SCHUR_JL, STANDARD, make_problem, split_hessian
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+def cu(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.to(DEV)
+
+
+def relerr(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def run_both(bls, st, ost, pat, opat, E, Cd, R, b_r, b_e, sc_r, sc_e, lam, dense, dtype, s_r=None, s_e=None):
+    """One reset + reduce + back-substitution on the device and in the oracle (FP64, on the same stored values)."""
+    npdt = np.float32 if dtype == torch.float32 else np.float64
+    E32, C32, R32 = E.astype(npdt), Cd.astype(npdt), R.astype(npdt)
+    nr = st.nr
+    ws = bls.SchurReductionWorkspace(st, pat)
+    g = torch.zeros(nr, dtype=torch.float64, device=DEV)
+    args = dict(s_r=None if s_r is None else cu(s_r), s_e=None if s_e is None else cu(s_e))
+    if dense:
+        S = torch.zeros(nr * nr, dtype=dtype, device=DEV)
+        bls.reset_schur_dense(S, cu(R32), cu(sc_r), lam, ws, s_r=args["s_r"])
+        ok = bls.reduce_schur_dense(S, g, cu(b_r), cu(b_e), cu(sc_e), lam, st, cu(E32), cu(C32), ws, **args)
+    else:
+        S = torch.zeros(pat.nnz, dtype=dtype, device=DEV)
+        bls.reset_schur_sparse(S, cu(R32), None, None, cu(sc_r), lam, ws, s_r=args["s_r"])
+        ok = bls.reduce_schur_sparse(S, g, cu(b_r), cu(b_e), cu(sc_e), lam, st, cu(E32), cu(C32), None, None, None, None, ws, **args)
+    # oracle in FP64 on the stored (possibly FP32-rounded) values
+    work = orc.Work(ost, 1)
+    og = np.zeros(nr)
+    if dense:
+        oS = np.zeros(nr * nr)
+        orc.reset_schur_dense(ost, oS, R32.astype(np.float64), sc_r, lam, s_r)
+        ook, ofb = orc.reduce_schur_dense(ost, work, oS, og, b_r, b_e, sc_e, lam, E32.astype(np.float64), C32.astype(np.float64), s_r, s_e)
+    else:
+        oS = np.zeros(opat.nnz)
+        orc.reset_schur_sparse(ost, opat, oS, R32.astype(np.float64), sc_r, lam, s_r)
+        ook, ofb = orc.reduce_schur_sparse(ost, opat, work, oS, og, b_r, b_e, sc_e, lam, E32.astype(np.float64), C32.astype(np.float64), s_r, s_e)
+    out = dict(ok=ok, fb=ws.failed_block, ook=ook, ofb=ofb, S=S.double().cpu().numpy(), oS=oS, g=g.cpu().numpy(), og=og, ws=ws, work=work)
+    if ok and ook:
+        x_r = np.random.default_rng(0).standard_normal(nr)
+        x_e = torch.zeros(st.ne, dtype=torch.float64, device=DEV)
+        bls.backsubstitute(x_e, cu(x_r), st, cu(C32), ws, s_r=args["s_r"], s_e=args["s_e"])
+        ox_e = np.zeros(st.ne)
+        orc.backsubstitute(ost, work, ox_e, x_r, C32.astype(np.float64), s_r, s_e)
+        out.update(x_e=x_e.cpu().numpy(), ox_e=ox_e)
+    return out
+
+
+def fixture_system(bls, fx, seed=7, lam=0.5):
+    rng = np.random.default_rng(seed)
+    rr = fx.get("rr_pairs", [])
+    H, b = make_problem(rng, fx["r_dims"], fx["e_dims"], fx["couplings"], rr)
+    st = bls.SchurStructure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    ost = orc.Structure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    return H, b, st, ost, rr, 1.0 + rng.random(len(b))
+
+
+@pytest.mark.parametrize("name", ["schur_jl", "standard", "coupled_groups", "gauge"])
+@pytest.mark.parametrize("dense", [False, True])
+def test_fixture_fp64(bls, name, dense):
+    fx = {"schur_jl": SCHUR_JL, "standard": STANDARD, "coupled_groups": COUPLED_GROUPS, "gauge": GAUGE}[name]
+    H, b, st, ost, rr, sc = fixture_system(bls, fx)
+    pat = None if dense else bls.build_schur_pattern(st, rr)
+    opat = None if dense else orc.Pattern(ost, rr)
+    E, Cd, R = split_hessian(H, st, pat)
+    nr = st.nr
+    o = run_both(bls, st, ost, pat, opat, E, Cd, R, b[:nr], b[nr:], sc[:nr], sc[nr:], 0.5, dense, torch.float64)
+    assert o["ok"] and o["ook"]
+    assert relerr(o["S"], o["oS"]) < 1e-12
+    assert relerr(o["g"], o["og"]) < 1e-12
+    assert relerr(o["x_e"], o["ox_e"]) < 1e-12
+
+
+@pytest.mark.parametrize("dense", [False, True])
+def test_fixture_conditioned_scales(bls, dense):
+    """Power-of-two conditioning scales applied at read (src/conditioning.jl:99-150)."""
+    H, b, st, ost, rr, sc = fixture_system(bls, STANDARD, seed=11)
+    pat = None if dense else bls.build_schur_pattern(st, rr)
+    opat = None if dense else orc.Pattern(ost, rr)
+    E, Cd, R = split_hessian(H, st, pat)
+    rng = np.random.default_rng(2)
+    s = np.ldexp(1.0, rng.integers(-6, 7, len(b)))
+    nr = st.nr
+    o = run_both(bls, st, ost, pat, opat, E, Cd, R, b[:nr], b[nr:], sc[:nr], sc[nr:], 0.3, dense, torch.float64, s_r=s[:nr], s_e=s[nr:])
+    assert o["ok"] and o["ook"]
+    assert relerr(o["S"], o["oS"]) < 1e-12 and relerr(o["g"], o["og"]) < 1e-12 and relerr(o["x_e"], o["ox_e"]) < 1e-12
+
+
+@pytest.mark.parametrize("dense", [False, True])
+def test_rank_one_block_reports_lowest(bls, dense):
+    H, b, st, ost, rr, sc = fixture_system(bls, SCHUR_JL, seed=5)
+    nr = st.nr
+    v = np.random.default_rng(9).standard_normal(3)
+    H[nr:nr + 3, nr:nr + 3] = np.outer(v, v)
+    H[nr + 12:nr + 15, nr + 12:nr + 15] = np.outer(v, v)   # a second, higher failing block
+    pat = None if dense else bls.build_schur_pattern(st)
+    opat = None if dense else orc.Pattern(ost)
+    E, Cd, R = split_hessian(H, st, pat)
+    o = run_both(bls, st, ost, pat, opat, E, Cd, R, b[:nr], b[nr:], sc[:nr], np.ones(st.ne), 0.0, dense, torch.float64)
+    assert not o["ok"] and not o["ook"]
+    assert o["fb"] == o["ofb"] == 1
+    # S is left as the reset wrote it, g_S untouched (the reference returns before phase 2)
+    assert relerr(o["S"], o["oS"]) < 1e-15
+    assert np.all(o["g"] == 0.0)
+
+
+def test_bad_damping_is_rejected_without_writes(bls):
+    H, b, st, ost, rr, sc = fixture_system(bls, STANDARD)
+    pat = bls.build_schur_pattern(st)
+    E, Cd, R = split_hessian(H, st, pat)
+    nr = st.nr
+    ws = bls.SchurReductionWorkspace(st, pat)
+    S = torch.full((pat.nnz,), 7.0, dtype=torch.float64, device=DEV)
+    g = torch.full((nr,), 5.0, dtype=torch.float64, device=DEV)
+    with pytest.raises(bls.ArgumentError):
+        bls.reset_schur_sparse(S, cu(R), None, None, cu(sc[:nr]), -1.0, ws)
+    bad = sc[:nr].copy()
+    bad[3] = np.nan
+    bls.reset_schur_sparse(S, cu(R), None, None, cu(bad), 0.1, ws)   # recorded, reported by the next reduction
+    assert torch.all(S == 7.0)
+    with pytest.raises(bls.ArgumentError, match="scaling_r must be finite and non-negative, but entry 4"):
+        bls.reduce_schur_sparse(S, g, cu(b[:nr]), cu(b[nr:]), cu(sc[nr:]), 0.1, st, cu(E), cu(Cd), None, None, None, None, ws)
+    assert torch.all(S == 7.0) and torch.all(g == 5.0)
+    bls.reset_schur_sparse(S, cu(R), None, None, cu(sc[:nr]), 0.1, ws)
+    bad_e = sc[nr:].copy()
+    bad_e[0] = -1.0
+    S2 = S.clone()
+    with pytest.raises(bls.ArgumentError, match="scaling_e"):
+        bls.reduce_schur_sparse(S, g, cu(b[:nr]), cu(b[nr:]), cu(bad_e), 0.1, st, cu(E), cu(Cd), None, None, None, None, ws)
+    assert torch.equal(S, S2) and torch.all(g == 5.0)
+    with pytest.raises(bls.ArgumentError):
+        bls.reduce_schur_sparse(S, g, cu(b[:nr]), cu(b[nr:]), cu(sc[nr:]), float("inf"), st, cu(E), cu(Cd), None, None, None, None, ws)
+
+
+def scene_system(bls, name, ncams, npoints, dense=False, seed=None):
+    spec = bls.scenes.scaled_down(bls.scenes.workload(name), ncams, npoints, seed)
+    p = bls.scenes.hessian_problem(spec, dense=dense)
+    st = p.structure
+    bs, el, ptr, idx = bls.scenes.Scene(spec).description()
+    ost = orc.Structure.from_description(bs, (ptr, idx), el)
+    opat = None if dense else orc.Pattern(ost)
+    return p, st, ost, opat
+
+
+@pytest.mark.parametrize("name,ncams,npoints,dense", [
+    ("dense_50x2000", 50, 2000, True),            # the dense workload at full size
+    ("sparse_1000x200k", 120, 8000, False),
+    ("batched_256", 60, 3000, False),
+    ("pcg_10000x1M", 150, 6000, False),
+])
+def test_scene_fp64_matches_oracle(bls, name, ncams, npoints, dense):
+    p, st, ost, opat = scene_system(bls, name, ncams, npoints, dense)
+    o = run_both(bls, st, ost, p.pattern, opat, p.E, p.C, p.R, p.b_r, p.b_e, p.scaling_r, p.scaling_e, p.lam, dense, torch.float64)
+    assert o["ok"] and o["ook"]
+    assert relerr(o["S"], o["oS"]) < 1e-12
+    assert relerr(o["g"], o["og"]) < 1e-12
+    assert relerr(o["x_e"], o["ox_e"]) < 1e-10
+
+
+@pytest.mark.parametrize("name,ncams,npoints", [("sparse_1000x200k", 120, 8000), ("pcg_10000x1M", 150, 6000)])
+def test_scene_mixed_matches_fp64_oracle(bls, name, ncams, npoints):
+    p, st, ost, opat = scene_system(bls, name, ncams, npoints)
+    o = run_both(bls, st, ost, p.pattern, opat, p.E, p.C, p.R, p.b_r, p.b_e, p.scaling_r, p.scaling_e, p.lam, False, torch.float32)
+    assert o["ok"] and o["ook"]
+    assert relerr(o["S"], o["oS"]) < 1e-4
+    assert relerr(o["g"], o["og"]) < 1e-6   # z and the gradient are FP64 from FP32 data
+    assert relerr(o["x_e"], o["ox_e"]) < 1e-6
+
+
+def test_scatter_copy_matches_map(bls):
+    p, st, ost, opat = scene_system(bls, "sparse_1000x200k", 60, 2000)
+    colptr, rowval, smap = bls.sparse_with_map(st, p.pattern, True)
+    dest = torch.empty(len(smap), dtype=torch.float64, device=DEV)
+    bls.scatter_copy(dest, cu(p.R), cu(smap))
+    assert np.array_equal(dest.cpu().numpy(), p.R[smap])
+
+
+def test_repeated_reductions_are_stable(bls):
+    """Re-running reset + reduce on the same plan gives the same S (to atomic-order rounding) every time."""
+    p, st, ost, opat = scene_system(bls, "sparse_1000x200k", 120, 8000)
+    ws = bls.SchurReductionWorkspace(st, p.pattern)
+    outs = []
+    for _ in range(3):
+        S = torch.zeros(p.pattern.nnz, dtype=torch.float64, device=DEV)
+        g = torch.zeros(st.nr, dtype=torch.float64, device=DEV)
+        bls.reset_schur_sparse(S, cu(p.R), None, None, cu(p.scaling_r), p.lam, ws)
+        assert bls.reduce_schur_sparse(S, g, cu(p.b_r), cu(p.b_e), cu(p.scaling_e), p.lam, st, cu(p.E), cu(p.C), None, None, None, None, ws)
+        outs.append(S.cpu().numpy())
+    for o in outs[1:]:
+        assert relerr(o, outs[0]) < 1e-14
