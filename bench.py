@@ -1,0 +1,318 @@
+"""Benchmark: observations/s through the Schur reduction of the sparse_1000x200k scene (1,000 cameras, 200,000 points,
+~1.2M observations), on N GPUs as N independent replicas (the reduction has no cross-GPU exchange).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+A step is one reset_schur_sparse + reduce_schur_sparse of the whole scene. `value` is the mixed form (FP32 storage
+and accumulation, FP64 point-block inverse, z and gradient) with inputs resident in device memory, L2 flushed
+between steps; `fp64` reports the plain FP64 form the same way. `e2e` runs the same step through the public API from
+pinned host buffers (inputs copied in, S and g_S copied out, every step). The roofline is the pair kernel's: the
+algorithmic bytes of the reduction (per point 84 + 76 k bytes in the mixed form, plus one read and one write of S),
+over its event-timed duration, against the measured HBM copy bandwidth.
+
+--impl reference times the reference algorithm (the oracle: a C++ restatement of BlockLinearSystems.jl's
+reset_schur_sparse! + reduce_schur_sparse!, threaded over its chunks as the reference threads over Polyester chunks)
+on every host core, in FP64: the reference's Float32 path rejects this scene's point blocks as singular.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+METRIC = "observations/s through Schur reduction, mixed vs FP64 plain; PCG s to 1e-8"
+
+
+def load_package():
+    import importlib.util
+    name = "blsgpu"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = ROOT / "blocklinearsystems.jl_b200"
+    spec = importlib.util.spec_from_file_location(name, pkg / "__init__.py", submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def algorithmic_bytes(p, dtype_bytes: int) -> float:
+    """Bytes the reduction must move: per point 9 E + 18k C entries in the storage type, b_e and scaling_e (FP64), a
+    4-byte camera index per observation; plus S read and written once (SURVEY's per-point model)."""
+    st = p.structure
+    per_point = dtype_bytes * (9 * st.neblocks + 18 * p.nobs) + 8 * (3 + 3) * st.neblocks + 4 * p.nobs
+    return float(per_point + 2 * dtype_bytes * p.pattern.nnz)
+
+
+def algorithmic_flops(p) -> float:
+    """F(k) = 58 + 270 k + 108 k (k - 1) per point (FMA = 2)."""
+    st = p.structure
+    k = np.diff(st.eliminated_ptr).astype(np.float64)
+    return float((58 + 270 * k + 108 * k * (k - 1)).sum())
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            out, _ = self.proc.communicate(timeout=10)
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args, rank: int, world: int) -> dict | None:
+    import torch
+    bls = load_package()
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    spec = bls.scenes.workload(args.workload)
+    if world > 1:
+        from dataclasses import replace
+        spec = replace(spec, seed=spec.seed + 100 * rank)   # each replica its own scene of the same distribution
+    p = bls.scenes.hessian_problem(spec)
+    st, pat = p.structure, p.pattern
+    ws = bls.SchurReductionWorkspace(st, pat, device=dev.index)
+    flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=dev)   # larger than the 126 MB L2
+
+    def device_inputs(dt):
+        f = lambda a, t=dt: torch.from_numpy(a).to(device=dev, dtype=t)
+        return dict(E=f(p.E), C=f(p.C), R=f(p.R), b_r=f(p.b_r, torch.float64), b_e=f(p.b_e, torch.float64),
+                    sr=f(p.scaling_r, torch.float64), se=f(p.scaling_e, torch.float64),
+                    S=torch.zeros(pat.nnz, dtype=dt, device=dev), g=torch.zeros(st.nr, dtype=torch.float64, device=dev))
+
+    def step(d):
+        bls.reset_schur_sparse(d["S"], d["R"], None, None, d["sr"], p.lam, ws)
+        bls.reduce_schur_sparse(d["S"], d["g"], d["b_r"], d["b_e"], d["se"], p.lam, st, d["E"], d["C"], None, None, None, None, ws,
+                                sync=False)
+
+    def timed(d, steps, warmup, instrument=False):
+        for _ in range(warmup):
+            step(d)
+        assert ws.query_status(), f"reduction failed at block {ws.failed_block}"
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        ws.instrument(instrument)
+        ws.counters()
+        total = 0.0
+        evs = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            step(d)
+            b.record()
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        total = sum(a.elapsed_time(b) for a, b in evs)
+        cnt = ws.counters()
+        ws.instrument(False)
+        ok = ws.query_status()
+        assert ok, f"reduction failed at block {ws.failed_block}"
+        if world > 1:
+            t = torch.tensor([total], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            total = float(t.item())
+        return total, cnt
+
+    d32 = device_inputs(torch.float32)
+    with ClockSampler(dev.index) as clk:
+        ms32, cnt32 = timed(d32, args.steps, args.warmup, instrument=True)
+    d64 = device_inputs(torch.float64)
+    ms64, cnt64 = timed(d64, args.steps, args.warmup, instrument=True)
+    del d64
+
+    # end to end through the public API from pinned host buffers (mixed form)
+    host = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
+            dict(E=p.E.astype(np.float32), C=p.C.astype(np.float32), R=p.R.astype(np.float32), b_r=p.b_r, b_e=p.b_e,
+                 sr=p.scaling_r, se=p.scaling_e).items()}
+    S_host = torch.empty(pat.nnz, dtype=torch.float32).pin_memory()
+    g_host = torch.empty(st.nr, dtype=torch.float64).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in host.values())
+    d2h = S_host.numel() * 4 + g_host.numel() * 8
+
+    def e2e_step():
+        for k, v in host.items():
+            d32[k].copy_(v, non_blocking=True)
+        step(d32)
+        S_host.copy_(d32["S"], non_blocking=True)
+        g_host.copy_(d32["g"], non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        e2e_step()
+    b.record()
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert ws.query_status()
+
+    if rank != 0:
+        return None
+    nobs = p.nobs
+    value = world * nobs * args.steps / (ms32 / 1e3)
+    v64 = world * nobs * args.steps / (ms64 / 1e3)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    pair_ms = cnt32["pair_kernel_ms"] / max(cnt32["pair_kernel_launches"], 1)
+    bytes32 = algorithmic_bytes(p, 4)
+    achieved = bytes32 / (pair_ms / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "pairs_sparse_1000x200k.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch_f32")
+    out = {
+        "metric": METRIC, "value": value, "unit": "obs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 storage/accumulation + f64 point inverse, z, gradient", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": args.workload, "cameras": st.nrblocks, "points": st.neblocks, "observations": nobs,
+                   "nnz_S": pat.nnz, "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MB write)",
+                   "step": "reset_schur_sparse + reduce_schur_sparse"},
+        "fp64": {"value": v64, "unit": "obs/s", "ms_per_step": ms64 / args.steps,
+                 "pair_kernel_ms": cnt64["pair_kernel_ms"] / max(cnt64["pair_kernel_launches"], 1)},
+        "mixed_over_fp64": value / v64,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "kernel": "k_pairs36<float>", "kernel_ms": pair_ms, "algorithmic_bytes": bytes32,
+                     "peak_source": "measured" if peaks else "fallback",
+                     "flops": algorithmic_flops(p), "achieved_tflops": algorithmic_flops(p) / (pair_ms / 1e3) / 1e12},
+        "e2e": {"value": world * nobs * args.steps / (e2e_ms / 1e3), "unit": "obs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": cnt32["launches"],
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(p, spec, seconds=args.cpu_seconds)
+    return out
+
+
+def oracle_problem(spec):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    bls = load_package()
+    p = bls.scenes.hessian_problem(spec)
+    sc = bls.scenes.Scene(spec)
+    bs, el, ptr, idx = sc.description()
+    cores = os.cpu_count() or 1
+    ost = orc.Structure.from_description(bs, (ptr, idx), el, nchunks=cores, min_work=4096)
+    opat = orc.Pattern(ost)
+    return orc, p, ost, opat, cores
+
+
+def cpu_baseline(p, spec, seconds: float = 10.0, steps: int | None = None, warmup: int = 1) -> dict:
+    """The reference algorithm (oracle) on every host core, FP64, reset + reduce of the same scene."""
+    orc, p, ost, opat, cores = oracle_problem(spec)
+    w = orc.Work(ost, cores, False)
+    S = np.zeros(opat.nnz)
+    g = np.zeros(ost.nr)
+
+    def one():
+        orc.reset_schur_sparse(ost, opat, S, p.R, p.scaling_r, p.lam)
+        ok, _ = orc.reduce_schur_sparse(ost, opat, w, S, g, p.b_r, p.b_e, p.scaling_e, p.lam, p.E, p.C, nthreads=cores)
+        assert ok
+
+    for _ in range(warmup):
+        one()
+    n, t0 = 0, time.perf_counter()
+    while (steps is None and (time.perf_counter() - t0 < seconds or n < 3)) or (steps is not None and n < steps):
+        one()
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": p.nobs * n / dt, "unit": "obs/s", "cores": cores, "kind": "port",
+            "sample": f"{n} x full reset_schur_sparse + reduce_schur_sparse of {spec.npoints} points / {p.nobs} observations, FP64, "
+                      f"{cores} OpenMP threads over the reference's chunks ({dt:.1f} s)"}
+
+
+def run_reference(args, rank: int, world: int) -> dict | None:
+    if rank != 0:
+        return None
+    bls = load_package()
+    spec = bls.scenes.workload(args.workload)
+    base = cpu_baseline(None, spec, steps=args.steps, warmup=args.warmup)
+    return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "obs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded scene generator)",
+            "config": {"workload": args.workload, "step": "reset_schur_sparse + reduce_schur_sparse",
+                       "note": "reference algorithm restated in C++ (Julia is unavailable); FP64 because its Float32 path rejects this scene"},
+            "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "obs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sparse_1000x200k")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        out = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch
+            torch.distributed.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

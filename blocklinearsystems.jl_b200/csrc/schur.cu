@@ -47,6 +47,7 @@ struct SchurPlan {
   bool has_sparse = false;
   int max_de = 0, max_dr = 0;
   bool uniform36 = false;   // every r_dim is 6 and every e_dim is 3
+  bool fast36 = false;      // uniform36 with the canonical offsets (coffsets = 18c, eoffsets = 9e) and packable pairs
   std::vector<int64_t> diag_inds_host;
   // structure
   DevBuf r_dims, boffsets_r, e_dims, boffsets_e, eoffsets, eliminated_ptr, entry_retained, coffsets, entry_eliminated;
@@ -54,13 +55,22 @@ struct SchurPlan {
   // blocks and pairs
   DevBuf block_r1, block_r2, block_base_sparse, block_stride_sparse, block_base_dense;
   DevBuf pair_c1, pair_c2, item_block, item_start, item_info;
+  DevBuf pair_packed;   // fast36: {c1, e | (c2 - c1) << 24} per pair
   // reset
   DevBuf r_to_s, diag_inds, S_rowval, S_col;
   // scratch: E^-1 (FP64, and FP32 for the mixed form), z, status
   DevBuf Einv64, Einv32, z, status;
+  DevBuf Einv12;   // fast36: E^-1 per point in the element type of the pair products, padded to 12 entries (16-byte rows)
   Status* host_status = nullptr;   // pinned
   int last_dtype = -1;
-  ~SchurPlan() { if (host_status) cudaFreeHost(host_status); }
+  // instrumentation: launches issued on the plan, and CUDA events around the pair kernel when timing is on
+  int64_t launches = 0;
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pair_events;
+  ~SchurPlan() {
+    if (host_status) cudaFreeHost(host_status);
+    for (auto& e : pair_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  }
 };
 
 static std::vector<int32_t> to32(const int64_t* a, int64_t n, const char* what) {
@@ -190,7 +200,7 @@ __global__ void __launch_bounds__(256) k_factor(int64_t neb, const int32_t* __re
                                                 const int32_t* __restrict__ boffsets_e, const T* __restrict__ E,
                                                 const double* __restrict__ b_e, const double* __restrict__ scaling_e, double lambda,
                                                 const double* __restrict__ s_e, double* __restrict__ Einv64, float* __restrict__ Einv32,
-                                                double* __restrict__ z, Status* st) {
+                                                double* __restrict__ z, void* __restrict__ Einv12, Status* st) {
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= neb) return;
   if (!args_ok(st)) return;
@@ -212,6 +222,15 @@ __global__ void __launch_bounds__(256) k_factor(int64_t neb, const int32_t* __re
   for (int i = 0; i < de * de; ++i) {
     Einv64[eo + i] = inv[i];
     if (Einv32) Einv32[eo + i] = (float)inv[i];
+  }
+  if (Einv12) {   // fast path: d_e = 3, rows of 12 entries in the pair products' type
+    if (Einv32) {
+      float* q = static_cast<float*>(Einv12) + 12 * e;
+      for (int i = 0; i < 9; ++i) q[i] = (float)inv[i];
+    } else {
+      double* q = static_cast<double*>(Einv12) + 12 * e;
+      for (int i = 0; i < 9; ++i) q[i] = inv[i];
+    }
   }
   for (int i = 0; i < de; ++i) {
     double acc = inv[i] * (b_e[so] * se[0]);
@@ -356,6 +375,109 @@ __global__ void __launch_bounds__(256) k_gradient(int64_t nrb, const int32_t* __
     double a = 0.0;
     for (int w = 0; w < 16; ++w) if (w == lane) a = acc[w];
     g[ro2 + lane] = bv - a;
+  }
+}
+
+// g_S = s_r .* b_r (scaled_copy!, src/conditioning.jl:237-244), before the pair kernel subtracts C' z
+__global__ void k_g_init(double* __restrict__ g, const double* __restrict__ b_r, const double* __restrict__ s_r, int64_t nr,
+                         const Status* __restrict__ st) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nr || !live(st)) return;
+  g[i] = s_r ? b_r[i] * s_r[i] : b_r[i];
+}
+
+// Phase 2 for d_r = 6, d_e = 3 in the canonical layout (coffsets = 18 c, eoffsets = 9 e): six threads per work item,
+// thread w accumulating column w of the 6 x 6 block, so the block's state is 6 values per thread rather than 36. Per
+// pair a thread loads the point's E^-1 (padded row of 12), all of C_c1 and column w of C_c2, forms u = E^-1 C_c2[:, w]
+// and adds C_c1' u to its column. A pair record {c1, e | (c2 - c1) << 24} holds every index the pair needs, so the
+// next record is fetched while the current pair is computed and no load waits on another index load. The diagonal
+// block's items also subtract C_c2' z from g_S (each coupling of r2 is exactly one diagonal pair).
+template <class T>
+__global__ void __launch_bounds__(128) k_pairs36(
+    int64_t nitems, const int32_t* __restrict__ item_block, const int32_t* __restrict__ item_start, const int32_t* __restrict__ item_info,
+    const int2* __restrict__ pairs, const int32_t* __restrict__ block_r1, const int32_t* __restrict__ block_r2,
+    const int64_t* __restrict__ block_base, const int32_t* __restrict__ block_stride, int64_t dense_nr, const T* __restrict__ C,
+    const typename EinvOf<T>::type* __restrict__ Einv12, const double* __restrict__ z, const double* __restrict__ s_r,
+    const double* __restrict__ s_e, T* __restrict__ S, double* __restrict__ g, const Status* __restrict__ st) {
+  using TE = typename EinvOf<T>::type;
+  const int lane = threadIdx.x & 31;
+  if (lane >= 30) return;
+  const int64_t it = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 5 + lane / 6;
+  const int w = lane % 6;
+  if (it >= nitems) return;
+  if (!live(st)) return;
+  const int k = __ldg(item_block + it), pb = __ldg(item_start + it), info = __ldg(item_info + it);
+  const int pe = pb + (info & 0xffff);
+  const bool solo = (info >> 16) != 0;
+  const int r1 = __ldg(block_r1 + k), r2 = __ldg(block_r2 + k);
+  const bool diag = r1 == r2;
+  const bool scaled = s_r != nullptr || s_e != nullptr;
+  const double fw = s_r ? s_r[6 * r2 + w] : 1.0;
+  T acc[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) acc[i] = T(0);
+  double gacc = 0.0;
+  int2 rec = __ldg(pairs + pb);
+  for (int p = pb; p < pe; ++p) {
+    const int2 cur = rec;
+    if (p + 1 < pe) rec = __ldg(pairs + p + 1);
+    const int c1 = cur.x, e = cur.y & 0xffffff, c2 = c1 + (cur.y >> 24);
+    TE ei[12];
+    if constexpr (std::is_same<TE, double>::value) {
+      const double2* q = reinterpret_cast<const double2*>(Einv12 + 12 * (int64_t)e);
+#pragma unroll
+      for (int i = 0; i < 5; ++i) { double2 v = __ldg(q + i); ei[2 * i] = v.x; ei[2 * i + 1] = v.y; }
+    } else {
+      const float4* q = reinterpret_cast<const float4*>(Einv12 + 12 * (int64_t)e);
+#pragma unroll
+      for (int i = 0; i < 3; ++i) { float4 v = __ldg(q + i); ei[4 * i] = v.x; ei[4 * i + 1] = v.y; ei[4 * i + 2] = v.z; ei[4 * i + 3] = v.w; }
+    }
+    T c1v[18];
+    if constexpr (std::is_same<T, double>::value) {
+      const double2* q = reinterpret_cast<const double2*>(C + 18 * (int64_t)c1);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) { double2 v = __ldg(q + i); c1v[2 * i] = v.x; c1v[2 * i + 1] = v.y; }
+    } else {
+      const float2* q = reinterpret_cast<const float2*>(C + 18 * (int64_t)c1);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) { float2 v = __ldg(q + i); c1v[2 * i] = v.x; c1v[2 * i + 1] = v.y; }
+    }
+    const T* c2p = C + 18 * (int64_t)c2 + 3 * w;
+    T c2w[3] = {__ldg(c2p), __ldg(c2p + 1), __ldg(c2p + 2)};
+    if (scaled) {
+      double se[3];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) se[s] = s_e ? s_e[3 * e + s] : 1.0;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) c2w[s] = T((double)c2w[s] * (se[s] * fw));
+#pragma unroll
+      for (int rho = 0; rho < 6; ++rho) {
+        const double fr = s_r ? s_r[6 * r1 + rho] : 1.0;
+#pragma unroll
+        for (int s = 0; s < 3; ++s) c1v[3 * rho + s] = T((double)c1v[3 * rho + s] * (se[s] * fr));
+      }
+    }
+    T u[3];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) u[t] = (T)(ei[t] * (TE)c2w[0] + ei[t + 3] * (TE)c2w[1] + ei[t + 6] * (TE)c2w[2]);
+#pragma unroll
+    for (int rho = 0; rho < 6; ++rho) acc[rho] = acc[rho] + c1v[3 * rho] * u[0] + c1v[3 * rho + 1] * u[1] + c1v[3 * rho + 2] * u[2];
+    if (diag) {
+      const double* zp = z + 3 * (int64_t)e;
+      gacc += (double)c2w[0] * zp[0] + (double)c2w[1] * zp[1] + (double)c2w[2] * zp[2];
+    }
+  }
+  const int64_t stride = block_stride ? (int64_t)__ldg(block_stride + k) : dense_nr;
+  T* col = S + __ldg(block_base + k) + w * stride;
+#pragma unroll
+  for (int rho = 0; rho < 6; ++rho) {
+    if (diag && rho > w) continue;
+    if (solo) col[rho] = col[rho] - acc[rho];
+    else atomicAdd(col + rho, -acc[rho]);
+  }
+  if (diag) {
+    if (solo) g[6 * r2 + w] -= gacc;
+    else atomicAdd(g + 6 * r2 + w, -gacc);
   }
 }
 
@@ -579,6 +701,23 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
     std::vector<int32_t>().swap(col_c2[r2]);
   }
   P->nitems = (int64_t)it_block.size();
+  // fast path: uniform 6/3 blocks in the canonical layout, and pairs that pack into {c1, e | (c2 - c1) << 24}
+  std::vector<int2> packed;
+  if (P->uniform36 && neb < (1 << 24)) {
+    bool canon = true;
+    for (int64_t e = 0; e < neb && canon; ++e) canon = d->eoffsets[e] == 9 * e;
+    for (int64_t c = 0; c < nc && canon; ++c) canon = d->coffsets[c] == 18 * c;
+    if (canon) {
+      packed.resize(npairs);
+      for (int64_t q = 0; q < npairs && canon; ++q) {
+        const int32_t c1 = pair_c1[q], c2 = pair_c2[q];
+        const int32_t dc = c2 - c1;
+        if (dc < 0 || dc > 127) canon = false;
+        packed[q] = make_int2(c1, entry_elim[c2] | (dc << 24));
+      }
+    }
+    P->fast36 = canon;
+  }
   // uploads
   upload(P->r_dims, to32(d->r_dims, nrb, "r_dims"), s);
   upload(P->boffsets_r, to32(boff_r.data(), nrb, "boffsets_r"), s);
@@ -596,8 +735,12 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
   upload(P->block_stride_sparse, b_stride, s);
   upload(P->block_base_sparse, b_base, s);
   upload(P->block_base_dense, b_base_dense, s);
-  upload(P->pair_c1, pair_c1, s);
-  upload(P->pair_c2, pair_c2, s);
+  if (P->fast36) {
+    upload(P->pair_packed, packed, s);
+  } else {
+    upload(P->pair_c1, pair_c1, s);
+    upload(P->pair_c2, pair_c2, s);
+  }
   upload(P->item_block, it_block, s);
   upload(P->item_start, it_start, s);
   upload(P->item_info, it_info, s);
@@ -623,6 +766,7 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
   P->Einv64.alloc(sizeof(double) * std::max<int64_t>(P->E_length, 1));
   P->Einv32.alloc(sizeof(float) * std::max<int64_t>(P->E_length, 1));
   P->z.alloc(sizeof(double) * std::max<int64_t>(ne, 1));
+  if (P->fast36) P->Einv12.alloc(sizeof(double) * 12 * neb);   // sized for FP64; the FP32 form uses half
   P->status.alloc(sizeof(Status));
   Status init{NONE, NONE, NONE, 0};
   BLS_CUDA(cudaMemcpyAsync(P->status.p, &init, sizeof(Status), cudaMemcpyHostToDevice, s));
@@ -634,7 +778,7 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
 static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
-                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2,
+                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->Einv12,
                           &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
@@ -670,7 +814,8 @@ static void check_lambda(double lambda) {
 static void begin_checked(SchurPlan* P, const double* scaling, int64_t n, int which) {
   cudaStream_t s = P->ctx->stream;
   k_status_begin<<<1, 1, 0, s>>>(P->status.as<Status>(), which);
-  if (n > 0) k_check_scaling<<<grid_for(n, 256), 256, 0, s>>>(scaling, n, P->status.as<Status>(), which);
+  P->launches += 1;
+  if (n > 0) { k_check_scaling<<<grid_for(n, 256), 256, 0, s>>>(scaling, n, P->status.as<Status>(), which); P->launches += 1; }
   BLS_CUDA(cudaGetLastError());
 }
 
@@ -689,6 +834,7 @@ static void reset_sparse(SchurPlan* P, T* S, const T* R, const double* sc, doubl
     k_scale_sparse<T><<<std::min<int64_t>(grid_for(P->nnzS, 256), 148 * 16), 256, 0, s>>>(S, P->S_rowval.as<int32_t>(), P->S_col.as<int32_t>(), s_r, P->nnzS, st);
   k_damp_diag<T><<<grid_for(P->nr, 256), 256, 0, s>>>(S, P->diag_inds.as<int64_t>(), 0, sc, lambda, s_r, P->nr, st);
   k_reset_done<<<1, 1, 0, s>>>(st);
+  P->launches += 3 + (P->R_length > 0 ? 1 : 0) + (s_r ? 1 : 0);
   BLS_CUDA(cudaGetLastError());
 }
 
@@ -700,6 +846,7 @@ static void reset_dense(SchurPlan* P, T* S, const T* R, const double* sc, double
   k_copy_scaled_dense<T><<<std::min<int64_t>(grid_for(P->nr * P->nr, 256), 148 * 16), 256, 0, s>>>(S, R, s_r, P->nr, st);
   k_damp_diag<T><<<grid_for(P->nr, 256), 256, 0, s>>>(S, nullptr, P->nr, sc, lambda, s_r, P->nr, st);
   k_reset_done<<<1, 1, 0, s>>>(st);
+  P->launches += 3;
   BLS_CUDA(cudaGetLastError());
 }
 
@@ -721,20 +868,50 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
                   const T* E, const T* C, const double* s_r, const double* s_e, int64_t* failed_block) {
   if (!dense && !P->has_sparse) throw Error(BLS_EINVAL, "the plan was created without a sparse pattern");
   check_lambda(lambda);
+  if (P->fast36 && reinterpret_cast<uintptr_t>(C) % (2 * sizeof(T)) != 0)
+    throw Error(BLS_EINVAL, "C_data must be aligned to two elements (the device reads coupling blocks in pairs of entries)");
   cudaStream_t s = P->ctx->stream;
   Status* st = P->status.as<Status>();
   begin_checked(P, sc_e, P->ne, 1);
   k_arm<<<1, 1, 0, s>>>(st);
   k_factor<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(P->neblocks, P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
                                                          P->boffsets_e.as<int32_t>(), E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
-                                                         std::is_same<T, float>::value ? P->Einv32.as<float>() : nullptr, P->z.as<double>(), st);
-  if (P->uniform36) launch_pairs<T, 3, 6>(P, S, dense, C, s_r, s_e);
-  else launch_pairs<T, 3, 16>(P, S, dense, C, s_r, s_e);
-  k_gradient<T><<<grid_for(P->nrblocks * 32, 256), 256, 0, s>>>(
-      P->nrblocks, P->retained_ptr.as<int32_t>(), P->retained_entry.as<int32_t>(), P->entry_eliminated.as<int32_t>(), P->r_dims.as<int32_t>(),
-      P->boffsets_r.as<int32_t>(), P->e_dims.as<int32_t>(), P->boffsets_e.as<int32_t>(), P->coffsets.as<int32_t>(), C, P->z.as<double>(), b_r,
-      s_r, s_e, g, st);
+                                                         std::is_same<T, float>::value ? P->Einv32.as<float>() : nullptr, P->z.as<double>(),
+                                                         P->fast36 ? P->Einv12.p : nullptr, st);
+  P->launches += 2;   // k_arm, k_factor
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (P->timing) {
+    BLS_CUDA(cudaEventCreate(&ev0));
+    BLS_CUDA(cudaEventCreate(&ev1));
+  }
+  if (P->fast36) {
+    using TE = typename EinvOf<T>::type;
+    k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st);
+    P->launches += 1;
+    if (P->nitems > 0) {
+      const int64_t warps = (P->nitems + 4) / 5;
+      if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
+      P->launches += 1;
+      k_pairs36<T><<<grid_for(warps * 32, 128), 128, 0, s>>>(
+          P->nitems, P->item_block.as<int32_t>(), P->item_start.as<int32_t>(), P->item_info.as<int32_t>(), P->pair_packed.as<int2>(),
+          P->block_r1.as<int32_t>(), P->block_r2.as<int32_t>(), dense ? P->block_base_dense.as<int64_t>() : P->block_base_sparse.as<int64_t>(),
+          dense ? nullptr : P->block_stride_sparse.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), s_r, s_e, S, g, st);
+      if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
+    }
+  } else {
+    if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
+    if (P->uniform36) launch_pairs<T, 3, 6>(P, S, dense, C, s_r, s_e);
+    else launch_pairs<T, 3, 16>(P, S, dense, C, s_r, s_e);
+    if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
+    P->launches += 2;
+    k_gradient<T><<<grid_for(P->nrblocks * 32, 256), 256, 0, s>>>(
+        P->nrblocks, P->retained_ptr.as<int32_t>(), P->retained_entry.as<int32_t>(), P->entry_eliminated.as<int32_t>(), P->r_dims.as<int32_t>(),
+        P->boffsets_r.as<int32_t>(), P->e_dims.as<int32_t>(), P->boffsets_e.as<int32_t>(), P->coffsets.as<int32_t>(), C, P->z.as<double>(), b_r,
+        s_r, s_e, g, st);
+  }
   BLS_CUDA(cudaGetLastError());
+  if (ev0 && ev1) P->pair_events.push_back({ev0, ev1});
+  else { if (ev0) cudaEventDestroy(ev0); if (ev1) cudaEventDestroy(ev1); }
   P->last_dtype = std::is_same<T, float>::value ? BLS_F32 : BLS_F64;
   if (!failed_block) return BLS_OK;
   return read_status(P, failed_block);
@@ -742,6 +919,7 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
 
 template <class T>
 static void backsub(SchurPlan* P, double* x_e, const double* x_r, const T* C, const double* s_r, const double* s_e) {
+  P->launches += 1;
   k_backsub<T><<<grid_for(P->neblocks, 256), 256, 0, P->ctx->stream>>>(
       P->neblocks, P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(), P->boffsets_e.as<int32_t>(), P->eliminated_ptr.as<int32_t>(),
       P->entry_retained.as<int32_t>(), P->coffsets.as<int32_t>(), P->r_dims.as<int32_t>(), P->boffsets_r.as<int32_t>(), C,
@@ -828,6 +1006,32 @@ int bls_reduce_schur_dense(bls_schur_plan* P, int dtype, void* S, double* g, con
     if (dtype == BLS_F64) return reduce<double>(P, (double*)S, true, g, b_r, b_e, sc_e, lambda, (const double*)E, (const double*)C, s_r, s_e, failed_block);
     if (dtype == BLS_F32) return reduce<float>(P, (float*)S, true, g, b_r, b_e, sc_e, lambda, (const float*)E, (const float*)C, s_r, s_e, failed_block);
     throw Error(BLS_EINVAL, "unknown dtype");
+  })
+}
+
+int bls_schur_plan_instrument(bls_schur_plan* P, int timing) {
+  if (!P) return BLS_EINVAL;
+  P->timing = timing != 0;
+  return BLS_OK;
+}
+
+int bls_schur_plan_counters(bls_schur_plan* P, int64_t* launches, double* pair_kernel_ms, int64_t* pair_kernel_launches) {
+  BLS_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "null plan");
+    double ms = 0.0;
+    if (!P->pair_events.empty()) BLS_CUDA(cudaEventSynchronize(P->pair_events.back().second));
+    for (auto& e : P->pair_events) {
+      float t = 0.f;
+      BLS_CUDA(cudaEventElapsedTime(&t, e.first, e.second));
+      ms += t;
+    }
+    if (launches) *launches = P->launches;
+    if (pair_kernel_ms) *pair_kernel_ms = ms;
+    if (pair_kernel_launches) *pair_kernel_launches = (int64_t)P->pair_events.size();
+    for (auto& e : P->pair_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    P->pair_events.clear();
+    P->launches = 0;
+    return BLS_OK;
   })
 }
 

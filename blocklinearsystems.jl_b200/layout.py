@@ -88,7 +88,7 @@ class SchurStructure:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and _lib._gpu is not None:
+        if h is not None and _lib is not None and _lib._gpu is not None:
             _lib.gpu().bls_structure_destroy(h)
             self._h = None
 
@@ -146,7 +146,7 @@ class SchurPattern:
         return out
 
     def __del__(self):
-        if self._h is not None and _lib._gpu is not None:
+        if self._h is not None and _lib is not None and _lib._gpu is not None:
             _lib.gpu().bls_pattern_destroy(self._h)
             self._h = None
 

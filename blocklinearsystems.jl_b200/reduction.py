@@ -100,7 +100,7 @@ class SchurReductionWorkspace:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and _lib._gpu is not None:
+        if h is not None and _lib is not None and _lib._gpu is not None:
             _lib.gpu().bls_schur_plan_destroy(h)
             self._h = None
 
@@ -111,6 +111,16 @@ class SchurReductionWorkspace:
 
     def device_bytes(self) -> int:
         return int(_lib.gpu().bls_schur_plan_device_bytes(self._h))
+
+    def instrument(self, timing: bool = True) -> None:
+        """Bracket the pair kernel of each reduction with CUDA events (read them with counters())."""
+        check(_lib.gpu().bls_schur_plan_instrument(self._h, int(timing)))
+
+    def counters(self) -> dict:
+        """Device launches since the last read, and the summed pair-kernel time (ms) over its timed launches."""
+        n, ms, k = C.c_int64(0), C.c_double(0.0), C.c_int64(0)
+        check(_lib.gpu().bls_schur_plan_counters(self._h, C.byref(n), C.byref(ms), C.byref(k)))
+        return {"launches": int(n.value), "pair_kernel_ms": float(ms.value), "pair_kernel_launches": int(k.value)}
 
     def query_status(self) -> bool:
         fb = C.c_int64(0)

@@ -88,7 +88,7 @@ class Scene:
         self.nobs = int(L.bls_scene_size(h, 2))
 
     def __del__(self):
-        if getattr(self, "_h", None) is not None and _lib._scene is not None:
+        if getattr(self, "_h", None) is not None and _lib is not None and _lib._scene is not None:
             _lib.scene_lib().bls_scene_destroy(self._h)
             self._h = None
 

@@ -149,6 +149,12 @@ int bls_reduce_schur_dense(bls_schur_plan* plan, int dtype, void* S_dev, double*
                            const double* b_e_dev, const double* scaling_e_dev, double lambda, const void* E_data_dev,
                            const void* C_data_dev, const double* s_r_dev, const double* s_e_dev,
                            int64_t* failed_block);
+/* Instrumentation (no counterpart in the reference): with timing on, CUDA events bracket the pair kernel of every
+ * reduction on the plan's stream. bls_schur_plan_counters synchronises on the last event, reports the device kernel
+ * launches issued since the previous read, the summed pair-kernel time and its number of launches, and resets them. */
+int bls_schur_plan_instrument(bls_schur_plan* plan, int timing);
+int bls_schur_plan_counters(bls_schur_plan* plan, int64_t* launches, double* pair_kernel_ms, int64_t* pair_kernel_launches);
+
 /* Status of the last reduction on this plan (synchronises): BLS_OK / BLS_NOT_PD / BLS_EINVAL. */
 int bls_schur_query_status(bls_schur_plan* plan, int64_t* failed_block);
 
