@@ -80,6 +80,7 @@ def gpu() -> C.CDLL:
             "bls_reduce_schur_dense": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, vp, vp, vp, p64]),
             "bls_schur_query_status": (C.c_int, [vp, p64]),
             "bls_schur_plan_instrument": (C.c_int, [vp, C.c_int]),
+            "bls_schur_plan_set_kernel": (C.c_int, [vp, C.c_int]),
             "bls_schur_plan_counters": (C.c_int, [vp, p64, pdbl, p64]),
             "bls_backsubstitute": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
             "bls_scatter_copy": (C.c_int, [vp, C.c_int, vp, vp, vp, i64]),

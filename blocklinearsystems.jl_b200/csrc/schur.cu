@@ -56,6 +56,11 @@ struct SchurPlan {
   DevBuf block_r1, block_r2, block_base_sparse, block_stride_sparse, block_base_dense;
   DevBuf pair_c1, pair_c2, item_block, item_start, item_info;
   DevBuf pair_packed;   // fast36: {c1, e | (c2 - c1) << 24} per pair
+  // fast36, column kernel: per visit {p0, e | j << 24} and the start of its row offsets; per (visit, camera) the
+  // camera's row offset in the column's tile; per column the S index of its first entry
+  DevBuf vis_rec, vis_base, vis_off, col_base, col_h;
+  int64_t max_col_h = 0;
+  int kernel = 0;   // 0: column-owned (k_columns36), 1: block-owned pairs (k_pairs36)
   // reset
   DevBuf r_to_s, diag_inds, S_rowval, S_col;
   // scratch: E^-1 (FP64, and FP32 for the mixed form), z, status
@@ -481,6 +486,113 @@ __global__ void __launch_bounds__(128) k_pairs36(
   }
 }
 
+// Phase 2 for d_r = 6, d_e = 3 in the canonical layout, owned by block column: one CTA per retained block r2 holds
+// the column's S blocks (H x 6, H = col_heights[r2], or the upper part of a dense column) in shared memory and runs the
+// column's couplings ("visits": point e seen from r2, the reference's retained_entry order) with a warp per visit. A
+// warp stages the point's E^-1 and C_c2 (two contiguous rows of global memory), forms U = E^-1 C_c2 (3 x 6) and the
+// gradient term C_c2' z, then lanes (i, rho) take row rho of camera i <= j of the point: the point's coupling blocks
+// C_{p0..c2} are contiguous, so a warp's loads cover one contiguous span. Each lane adds its row of C_ci' U to the
+// tile with shared-memory atomic adds (visits of different warps may share a block); the tile is written back to S
+// once, with no global atomics, and g_S once per column. This is the reference's column-chunk ownership
+// (src/schur_reduction.jl:30-49, :362-387) with a warp per coupling entry instead of a thread per column range.
+template <class T, bool DENSE>
+__global__ void __launch_bounds__(256) k_columns36(
+    const int32_t* __restrict__ retained_ptr, const int2* __restrict__ vis_rec, const int32_t* __restrict__ vis_base,
+    const uint16_t* __restrict__ vis_off, const int32_t* __restrict__ entry_retained, const int64_t* __restrict__ col_base,
+    const int32_t* __restrict__ col_h, int64_t dense_nr, const T* __restrict__ C, const typename EinvOf<T>::type* __restrict__ Einv12,
+    const double* __restrict__ z, const double* __restrict__ b_r, const double* __restrict__ s_r, const double* __restrict__ s_e,
+    T* __restrict__ S, double* __restrict__ g, const Status* __restrict__ st) {
+  using TE = typename EinvOf<T>::type;
+  constexpr int NW = 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int r2 = blockIdx.x;
+  if (!live(st)) return;
+  const int H = DENSE ? 6 * r2 + 6 : __ldg(col_h + r2);
+  const int64_t cstride = DENSE ? dense_nr : H;
+  const int64_t cb = DENSE ? (int64_t)6 * r2 * dense_nr : __ldg(col_base + r2);
+  // shared layout: per-warp staging [NW] { Ei[12] TE | Cj[18] T | U[18] T | zz[4] double }, then the tile [6][H] T
+  struct Stage { TE Ei[12]; T Cj[18]; T U[18]; double zz[4]; };
+  Stage* stage = reinterpret_cast<Stage*>(smem_raw);
+  T* tile = reinterpret_cast<T*>(smem_raw + sizeof(Stage) * NW);
+  for (int i = threadIdx.x; i < 6 * H; i += blockDim.x) tile[i] = T(0);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  Stage& sg = stage[warp];
+  const int q0 = __ldg(retained_ptr + r2), q1 = __ldg(retained_ptr + r2 + 1);
+  const int per = (q1 - q0 + NW - 1) / NW;
+  const int my0 = min(q1, q0 + warp * per), my1 = min(q1, my0 + per);
+  const bool scaled = s_r != nullptr || s_e != nullptr;
+  double gacc = 0.0;
+  for (int qb = my0; qb < my1; qb += 32) {
+    const int q = qb + lane;
+    int2 rec = make_int2(0, 0);
+    int vbase = 0;
+    if (q < my1) { rec = __ldg(vis_rec + q); vbase = __ldg(vis_base + q); }
+    const int nv = min(32, my1 - qb);
+    for (int v = 0; v < nv; ++v) {
+      const int p0 = __shfl_sync(0xffffffffu, rec.x, v);
+      const int ey = __shfl_sync(0xffffffffu, rec.y, v);
+      const int vb = __shfl_sync(0xffffffffu, vbase, v);
+      const int e = ey & 0xffffff, j = ey >> 24, c2 = p0 + j;
+      // stage E^-1 (12 lanes), C_c2 (18 lanes) and z (3 lanes): three contiguous rows
+      if (lane < 12) sg.Ei[lane] = __ldg(Einv12 + 12 * (int64_t)e + lane);
+      else if (lane < 30) {
+        const int x = lane - 12;   // x = 3 w + s
+        T c = __ldg(C + 18 * (int64_t)c2 + x);
+        if (scaled) c = T((double)c * ((s_e ? s_e[3 * e + x % 3] : 1.0) * (s_r ? s_r[6 * r2 + x / 3] : 1.0)));
+        sg.Cj[x] = c;
+      }
+      if (lane < 3) sg.zz[lane] = __ldg(z + 3 * (int64_t)e + lane);
+      __syncwarp();
+      if (lane < 18) {
+        const int t = lane / 6, w = lane % 6;
+        sg.U[6 * t + w] = (T)(sg.Ei[t] * (TE)sg.Cj[3 * w] + sg.Ei[t + 3] * (TE)sg.Cj[3 * w + 1] + sg.Ei[t + 6] * (TE)sg.Cj[3 * w + 2]);
+      }
+      if (lane < 6)
+        gacc += (double)sg.Cj[3 * lane] * sg.zz[0] + (double)sg.Cj[3 * lane + 1] * sg.zz[1] + (double)sg.Cj[3 * lane + 2] * sg.zz[2];
+      __syncwarp();
+      for (int i0 = 0; i0 <= j; i0 += 5) {
+        const int i = i0 + lane / 6, rho = lane % 6;
+        if (lane < 30 && i <= j) {
+          const T* cp = C + 18 * (int64_t)(p0 + i) + 3 * rho;
+          T c0 = __ldg(cp), c1 = __ldg(cp + 1), c2v = __ldg(cp + 2);
+          const int cam = (DENSE || scaled) ? __ldg(entry_retained + p0 + i) : 0;
+          if (scaled) {
+            const double fr = s_r ? s_r[6 * cam + rho] : 1.0;
+            c0 = T((double)c0 * ((s_e ? s_e[3 * e] : 1.0) * fr));
+            c1 = T((double)c1 * ((s_e ? s_e[3 * e + 1] : 1.0) * fr));
+            c2v = T((double)c2v * ((s_e ? s_e[3 * e + 2] : 1.0) * fr));
+          }
+          const int off = DENSE ? 6 * cam : (int)__ldg(vis_off + vb + i);
+          T* trow = tile + off + rho;
+          const bool diag = i == j;
+#pragma unroll
+          for (int w = 0; w < 6; ++w) {
+            if (diag && rho > w) continue;
+            atomicAdd(trow + w * H, c0 * sg.U[w] + c1 * sg.U[6 + w] + c2v * sg.U[12 + w]);
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __shared__ double gpart[NW][6];
+  if (lane < 6) gpart[warp][lane] = gacc;
+  __syncthreads();
+  for (int i = threadIdx.x; i < 6 * H; i += blockDim.x) {
+    const int w = i / H, row = i - w * H;
+    T* p = S + cb + w * cstride + row;
+    *p = *p - tile[i];
+  }
+  if (threadIdx.x < 6) {
+    double a = 0.0;
+    for (int w = 0; w < NW; ++w) a += gpart[w][threadIdx.x];
+    const int gi = 6 * r2 + threadIdx.x;
+    const double bv = s_r ? b_r[gi] * s_r[gi] : b_r[gi];
+    g[gi] = bv - a;
+  }
+}
+
 // backsubstitute_group! (src/schur_reduction.jl:541-576): x_e = z - E^-1 t, t = sum scaled(C) x_r, all in FP64
 template <class T>
 __global__ void __launch_bounds__(256) k_backsub(int64_t neb, const int32_t* __restrict__ e_dims, const int32_t* __restrict__ eoffsets,
@@ -718,6 +830,38 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
     }
     P->fast36 = canon;
   }
+  // column-kernel arrays: visits in the reference's retained_entry order (column by column, ascending coupling)
+  std::vector<int2> vrec;
+  std::vector<int32_t> vbase;
+  std::vector<uint16_t> voff;
+  std::vector<int64_t> cbase;
+  std::vector<int32_t> ch;
+  if (P->fast36) {
+    vrec.resize(nc);
+    vbase.resize(nc);
+    voff.reserve(npairs);
+    cbase.resize(nrb);
+    ch.resize(nrb);
+    for (int64_t r2 = 0; r2 < nrb; ++r2) {
+      cbase[r2] = P->has_sparse ? Scolptr[boff_r[r2]] : 0;
+      ch[r2] = (int32_t)col_h[r2];
+      P->max_col_h = std::max<int64_t>(P->max_col_h, col_h[r2]);
+      if (col_h[r2] > 65535) P->fast36 = false;
+      for (int32_t q = rptr[r2]; q < rptr[r2 + 1]; ++q) {
+        const int32_t c2 = rentry[q];
+        const int64_t e = entry_elim[c2], p0 = d->eliminated_ptr[e], j = c2 - p0;
+        vrec[q] = make_int2((int32_t)p0, (int32_t)(e | (j << 24)));
+        vbase[q] = (int32_t)voff.size();
+        for (int64_t i = 0; i <= j; ++i) {
+          const int64_t r1 = d->entry_retained[p0 + i];
+          const int64_t* lo = browval.data() + bcolptr[r2];
+          const int64_t* hi = browval.data() + bcolptr[r2 + 1];
+          const int64_t k = std::lower_bound(lo, hi, r1) - browval.data();
+          voff.push_back((uint16_t)brow_off[k]);
+        }
+      }
+    }
+  }
   // uploads
   upload(P->r_dims, to32(d->r_dims, nrb, "r_dims"), s);
   upload(P->boffsets_r, to32(boff_r.data(), nrb, "boffsets_r"), s);
@@ -736,6 +880,11 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
   upload(P->block_base_sparse, b_base, s);
   upload(P->block_base_dense, b_base_dense, s);
   if (P->fast36) {
+    upload(P->vis_rec, vrec, s);
+    upload(P->vis_base, vbase, s);
+    upload(P->vis_off, voff, s);
+    upload(P->col_base, cbase, s);
+    upload(P->col_h, ch, s);
     upload(P->pair_packed, packed, s);
   } else {
     upload(P->pair_c1, pair_c1, s);
@@ -778,7 +927,7 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
 static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
-                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->Einv12,
+                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h,
                           &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
@@ -884,7 +1033,21 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
     BLS_CUDA(cudaEventCreate(&ev0));
     BLS_CUDA(cudaEventCreate(&ev1));
   }
-  if (P->fast36) {
+  if (P->fast36 && P->kernel == 0) {
+    using TE = typename EinvOf<T>::type;
+    struct StageSz { TE a[12]; T b[18]; T c[18]; double d[4]; };
+    const int64_t hmax = dense ? P->nr : P->max_col_h;
+    const size_t smem = sizeof(StageSz) * 8 + sizeof(T) * 6 * hmax;
+    if (smem > 200 * 1024) throw Error(BLS_EUNSUPPORTED, "a block column of S exceeds the shared-memory tile of this build");
+    auto kern = dense ? k_columns36<T, true> : k_columns36<T, false>;
+    BLS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
+    P->launches += 1;
+    kern<<<(int)P->nrblocks, 256, smem, s>>>(P->retained_ptr.as<int32_t>(), P->vis_rec.as<int2>(), P->vis_base.as<int32_t>(),
+                                              P->vis_off.as<uint16_t>(), P->entry_retained.as<int32_t>(), P->col_base.as<int64_t>(),
+                                              P->col_h.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), b_r, s_r, s_e, S, g, st);
+    if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
+  } else if (P->fast36) {
     using TE = typename EinvOf<T>::type;
     k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st);
     P->launches += 1;
@@ -1007,6 +1170,12 @@ int bls_reduce_schur_dense(bls_schur_plan* P, int dtype, void* S, double* g, con
     if (dtype == BLS_F32) return reduce<float>(P, (float*)S, true, g, b_r, b_e, sc_e, lambda, (const float*)E, (const float*)C, s_r, s_e, failed_block);
     throw Error(BLS_EINVAL, "unknown dtype");
   })
+}
+
+int bls_schur_plan_set_kernel(bls_schur_plan* P, int which) {
+  if (!P || which < 0 || which > 1) return BLS_EINVAL;
+  P->kernel = which;
+  return BLS_OK;
 }
 
 int bls_schur_plan_instrument(bls_schur_plan* P, int timing) {

@@ -112,6 +112,10 @@ class SchurReductionWorkspace:
     def device_bytes(self) -> int:
         return int(_lib.gpu().bls_schur_plan_device_bytes(self._h))
 
+    def set_kernel(self, which: str) -> None:
+        """Phase-2 kernel of the 6/3 fast path: "columns" (block-column owned, default) or "pairs" (block owned)."""
+        check(_lib.gpu().bls_schur_plan_set_kernel(self._h, {"columns": 0, "pairs": 1}[which]))
+
     def instrument(self, timing: bool = True) -> None:
         """Bracket the pair kernel of each reduction with CUDA events (read them with counters())."""
         check(_lib.gpu().bls_schur_plan_instrument(self._h, int(timing)))

@@ -153,6 +153,9 @@ int bls_reduce_schur_dense(bls_schur_plan* plan, int dtype, void* S_dev, double*
  * reduction on the plan's stream. bls_schur_plan_counters synchronises on the last event, reports the device kernel
  * launches issued since the previous read, the summed pair-kernel time and its number of launches, and resets them. */
 int bls_schur_plan_instrument(bls_schur_plan* plan, int timing);
+/* Phase-2 kernel of the d_r = 6 / d_e = 3 fast path (no counterpart in the reference): 0 = block-column owned
+ * (default), 1 = block owned (pair lists). Both compute the same reduction; the choice is kept for comparisons. */
+int bls_schur_plan_set_kernel(bls_schur_plan* plan, int which);
 int bls_schur_plan_counters(bls_schur_plan* plan, int64_t* launches, double* pair_kernel_ms, int64_t* pair_kernel_launches);
 
 /* Status of the last reduction on this plan (synchronises): BLS_OK / BLS_NOT_PD / BLS_EINVAL. */

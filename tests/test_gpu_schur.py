@@ -30,12 +30,13 @@ def relerr(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-def run_both(bls, st, ost, pat, opat, E, Cd, R, b_r, b_e, sc_r, sc_e, lam, dense, dtype, s_r=None, s_e=None):
+def run_both(bls, st, ost, pat, opat, E, Cd, R, b_r, b_e, sc_r, sc_e, lam, dense, dtype, s_r=None, s_e=None, kernel="columns"):
     """One reset + reduce + back-substitution on the device and in the oracle (FP64, on the same stored values)."""
     npdt = np.float32 if dtype == torch.float32 else np.float64
     E32, C32, R32 = E.astype(npdt), Cd.astype(npdt), R.astype(npdt)
     nr = st.nr
     ws = bls.SchurReductionWorkspace(st, pat)
+    ws.set_kernel(kernel)
     g = torch.zeros(nr, dtype=torch.float64, device=DEV)
     args = dict(s_r=None if s_r is None else cu(s_r), s_e=None if s_e is None else cu(s_e))
     if dense:
@@ -164,25 +165,29 @@ def scene_system(bls, name, ncams, npoints, dense=False, seed=None):
     return p, st, ost, opat
 
 
+@pytest.mark.parametrize("kernel", ["columns", "pairs"])
 @pytest.mark.parametrize("name,ncams,npoints,dense", [
     ("dense_50x2000", 50, 2000, True),            # the dense workload at full size
     ("sparse_1000x200k", 120, 8000, False),
     ("batched_256", 60, 3000, False),
     ("pcg_10000x1M", 150, 6000, False),
 ])
-def test_scene_fp64_matches_oracle(bls, name, ncams, npoints, dense):
+def test_scene_fp64_matches_oracle(bls, name, ncams, npoints, dense, kernel):
     p, st, ost, opat = scene_system(bls, name, ncams, npoints, dense)
-    o = run_both(bls, st, ost, p.pattern, opat, p.E, p.C, p.R, p.b_r, p.b_e, p.scaling_r, p.scaling_e, p.lam, dense, torch.float64)
+    o = run_both(bls, st, ost, p.pattern, opat, p.E, p.C, p.R, p.b_r, p.b_e, p.scaling_r, p.scaling_e, p.lam, dense, torch.float64,
+                 kernel=kernel)
     assert o["ok"] and o["ook"]
     assert relerr(o["S"], o["oS"]) < 1e-12
     assert relerr(o["g"], o["og"]) < 1e-12
     assert relerr(o["x_e"], o["ox_e"]) < 1e-10
 
 
+@pytest.mark.parametrize("kernel", ["columns", "pairs"])
 @pytest.mark.parametrize("name,ncams,npoints", [("sparse_1000x200k", 120, 8000), ("pcg_10000x1M", 150, 6000)])
-def test_scene_mixed_matches_fp64_oracle(bls, name, ncams, npoints):
+def test_scene_mixed_matches_fp64_oracle(bls, name, ncams, npoints, kernel):
     p, st, ost, opat = scene_system(bls, name, ncams, npoints)
-    o = run_both(bls, st, ost, p.pattern, opat, p.E, p.C, p.R, p.b_r, p.b_e, p.scaling_r, p.scaling_e, p.lam, False, torch.float32)
+    o = run_both(bls, st, ost, p.pattern, opat, p.E, p.C, p.R, p.b_r, p.b_e, p.scaling_r, p.scaling_e, p.lam, False, torch.float32,
+                 kernel=kernel)
     assert o["ok"] and o["ook"]
     assert relerr(o["S"], o["oS"]) < 1e-4
     assert relerr(o["g"], o["og"]) < 1e-6   # z and the gradient are FP64 from FP32 data
