@@ -166,6 +166,24 @@ int bls_schur_query_status(bls_schur_plan* plan, int64_t* failed_block);
 int bls_backsubstitute(bls_schur_plan* plan, int dtype, double* x_e_dev, const double* x_r_dev,
                        const void* C_data_dev, const double* s_r_dev, const double* s_e_dev);
 
+/* No counterpart in the reference: reduce_schur_dense! for callers that cannot allocate device memory (a caller whose
+ * device memory belongs to an allocator it does not own, such as CUDA.jl's pool or PyTorch's caching allocator, or
+ * one held to a fixed memory budget). Every other reduction needs a plan, which allocates; this call takes the
+ * structure's eliminated_ptr[neblocks+1] and entry_retained[ncouplings] (0-based) already in device memory and keeps
+ * its scratch (each point's damped inverse and z, and a status word) in a static device array of the library, so it
+ * allocates nothing. Scope: retained blocks of 6 and eliminated blocks of 3 in the canonical layout (coupling c at
+ * C_data[18c], point e at E_data[9e]), dense column-major S (nr = 6 nrblocks) already holding the reset system, at most
+ * BLS_NOALLOC_MAX_POINTS eliminated blocks (larger sizes: BLS_EUNSUPPORTED, nothing launched). Results and failure
+ * reporting are those of bls_reduce_schur_dense. The array is shared by all calls on a device and keeps the last
+ * call's contents; calls whose work overlaps on the GPU race on it. The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and caches it: make that first call before any stream capture. */
+#define BLS_NOALLOC_MAX_POINTS 65536
+int bls_reduce_schur_dense_noalloc(void* cuda_stream, int dtype, int64_t nrblocks, int64_t neblocks, int64_t ncouplings,
+                                   const int64_t* eliminated_ptr_dev, const int64_t* entry_retained_dev, void* S_dev,
+                                   double* g_S_dev, const double* b_r_dev, const double* b_e_dev,
+                                   const double* scaling_e_dev, double lambda, const void* E_dev, const void* C_dev,
+                                   int64_t* failed_block);
+
 /* copyto!(csc, bsm, scatter_map) (src/SparseBlockLinearSystem.jl:356-362): dest[i] = src[map[i]], i < n. */
 int bls_scatter_copy(bls_ctx* ctx, int dtype, void* dest_dev, const void* src_dev, const int64_t* map_dev, int64_t n);
 
