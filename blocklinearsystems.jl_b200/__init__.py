@@ -6,16 +6,22 @@ The package directory is named `blocklinearsystems.jl_b200`; load it under the m
 Layout (host, integer):  SchurStructure, build_schur_pattern, build_r_to_s_map, sparse_with_map
 Device reduction:        SchurReductionWorkspace, reset_schur_sparse / reset_schur_dense,
                          reduce_schur_sparse / reduce_schur_dense, backsubstitute, scatter_copy
-Workloads:               scenes.workload, scenes.hessian_problem
+QR elimination:          SchurJacobianStructure, SchurBlockJacobian, QRReductionWorkspace, reduce_qr, qr_backsubstitute,
+                         reduced_normal_sparse / reduced_normal_dense, reduced_diagonal_blocks, free_block_pairs
+Workloads:               scenes.workload, scenes.hessian_problem, scenes.jacobian_problem
 """
 from ._lib import ArgumentError, BlsError, DimensionMismatch
 from .layout import DEFAULT_MIN_WORK, SchurPattern, SchurStructure, build_r_to_s_map, build_schur_pattern, sparse_with_map
 from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce_schur_dense, reduce_schur_sparse,
                         reset_schur_dense, reset_schur_sparse, scatter_copy)
+from .qr import (QRReductionWorkspace, SchurBlockJacobian, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
+                 reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse)
 from . import scenes
 
 __all__ = [
     "ArgumentError", "BlsError", "DimensionMismatch", "DEFAULT_MIN_WORK", "SchurPattern", "SchurStructure", "build_r_to_s_map",
     "build_schur_pattern", "sparse_with_map", "SchurReductionWorkspace", "backsubstitute", "context", "reduce_schur_dense",
-    "reduce_schur_sparse", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes",
+    "reduce_schur_sparse", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
+    "SchurBlockJacobian", "SchurJacobianStructure", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
+    "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse",
 ]

@@ -40,6 +40,15 @@ class bls_schur_plan_desc(C.Structure):
     ]
 
 
+class bls_qr_plan_desc(C.Structure):
+    _fields_ = [
+        ("nrblocks", i64), ("neblocks", i64), ("ntables", i64),
+        ("r_dims", p64), ("e_dims", p64), ("table_nrows", p64), ("table_ncols", p64), ("table_top", p64), ("table_ptr", p64),
+        ("entry_retained", p64), ("entry_col", p64), ("raw_offsets", p64), ("residual_offsets", p64),
+        ("block_colptr", p64), ("block_rowval", p64), ("block_row_offsets", p64), ("col_heights", p64), ("S_colptr", p64),
+    ]
+
+
 _gpu = None
 _scene = None
 
@@ -85,6 +94,18 @@ def gpu() -> C.CDLL:
             "bls_backsubstitute": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
             "bls_scatter_copy": (C.c_int, [vp, C.c_int, vp, vp, vp, i64]),
             "bls_reduce_schur_dense_noalloc": (C.c_int, [vp, C.c_int, i64, i64, i64, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp, vp, p64]),
+            "bls_qr_structure_from_description": (C.c_int, [i64, p64, i64, p64, p64, p64, C.POINTER(C.c_uint8), i64, i64, C.POINTER(vp)]),
+            "bls_qr_structure_positional": (C.c_int, [vp, p64, i64, p64, p64, p64, i64, C.POINTER(vp)]),
+            "bls_qr_structure_field": (i64, [vp, C.c_char_p, p64]),
+            "bls_qr_structure_schur": (C.c_int, [vp, C.POINTER(vp)]),
+            "bls_qr_structure_destroy": (C.c_int, [vp]),
+            "bls_qr_plan_create": (C.c_int, [vp, C.POINTER(bls_qr_plan_desc), C.POINTER(vp)]),
+            "bls_qr_plan_destroy": (C.c_int, [vp]),
+            "bls_reduce_qr": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, p64]),
+            "bls_qr_backsubstitute": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+            "bls_reduced_normal_sparse": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+            "bls_reduced_normal_dense": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+            "bls_reduced_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, vp]),
         }
         for fn, (res, args) in sig.items():
             f = getattr(L, fn)
@@ -108,6 +129,8 @@ def scene_lib() -> C.CDLL:
         L.bls_scene_description.argtypes = [vp, p64, C.POINTER(C.c_uint8), p64, p64]
         L.bls_scene_assemble.argtypes = [vp, p64, p64, p64, p64, p64, p64, p64, i64, p64, pdbl, i64, pdbl, i64, pdbl, i64,
                                          pdbl, i64, pdbl, i64]
+        L.bls_scene_assemble_qr.restype = C.c_int
+        L.bls_scene_assemble_qr.argtypes = [vp, p64, p64, p64, p64, p64, p64, p64, p64, p64, p64, pdbl, i64, pdbl, i64]
         _scene = L
     return _scene
 

@@ -13,6 +13,7 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 
 struct bls_structure : bls::Structure {};
 struct bls_pattern : bls::Pattern {};
+struct bls_qr_structure : bls::QRStructure {};
 
 using namespace bls;
 
@@ -199,6 +200,91 @@ int64_t bls_sparse_indices(const bls_structure* st, const bls_pattern* p, int sy
     if (!st || !p) throw Error(BLS_EINVAL, "null argument");
     return sparse_indices(*st, *p, symmetric != 0, colptr, rowval, map);
   })
+}
+
+int bls_qr_structure_from_description(int64_t nblocks, const int64_t* blocksizes, int64_t nrowblocks, const int64_t* rowblock_ptr,
+                                      const int64_t* rowblock_idx, const int64_t* rowblocksizes, const uint8_t* eliminated, int64_t nchunks,
+                                      int64_t min_work, bls_qr_structure** out) {
+  BLS_GUARD({
+    if (!out || (nblocks > 0 && (!blocksizes || !eliminated)) || (nrowblocks > 0 && (!rowblock_ptr || !rowblock_idx || !rowblocksizes)))
+      throw Error(BLS_EINVAL, "null argument");
+    auto* q = new bls_qr_structure();
+    try {
+      static_cast<QRStructure&>(*q) = qr_structure_from_description(nblocks, blocksizes, nrowblocks, rowblock_ptr, rowblock_idx, rowblocksizes,
+                                                                    eliminated, nchunks, min_work);
+    } catch (...) {
+      delete q;
+      throw;
+    }
+    *out = q;
+    return BLS_OK;
+  })
+}
+
+int bls_qr_structure_positional(const bls_structure* st, const int64_t* e_rows, int64_t nfree, const int64_t* free_rows, const int64_t* free_ptr,
+                                const int64_t* free_idx, int64_t nchunks, bls_qr_structure** out) {
+  BLS_GUARD({
+    if (!st || !out || (st->neblocks > 0 && !e_rows) || (nfree > 0 && (!free_rows || !free_ptr || !free_idx))) throw Error(BLS_EINVAL, "null argument");
+    std::vector<std::vector<int64_t>> fr(nfree);
+    for (int64_t g = 0; g < nfree; ++g) fr[g].assign(free_idx + free_ptr[g], free_idx + free_ptr[g + 1]);
+    auto* q = new bls_qr_structure();
+    try {
+      static_cast<QRStructure&>(*q) = qr_structure(*st, std::vector<int64_t>(e_rows, e_rows + st->neblocks),
+                                                   std::vector<int64_t>(free_rows, free_rows + nfree), fr, nchunks);
+    } catch (...) {
+      delete q;
+      throw;
+    }
+    *out = q;
+    return BLS_OK;
+  })
+}
+
+int64_t bls_qr_structure_field(const bls_qr_structure* q, const char* name, int64_t* out) {
+  if (!q || !name) return -1;
+  const std::string f(name);
+  auto scalar = [&](int64_t v) { if (out) out[0] = v; return (int64_t)1; };
+  if (f == "ntables") return scalar(q->ntables);
+  if (f == "raw_length") return scalar(q->raw_offsets.back());
+  if (f == "residual_length") return scalar(q->residual_offsets.back());
+  if (f == "e_rows") return put(out, q->e_rows);
+  if (f == "free_rows") return put(out, q->free_rows);
+  if (f == "table_nrows") return put(out, q->table_nrows);
+  if (f == "table_ncols") return put(out, q->table_ncols);
+  if (f == "table_top") return put(out, q->table_top);
+  if (f == "table_offsets") return put(out, q->table_offsets);
+  if (f == "raw_offsets") return put(out, q->raw_offsets);
+  if (f == "residual_offsets") return put(out, q->residual_offsets);
+  if (f == "reduced_offsets") return put(out, q->reduced_offsets);
+  if (f == "table_ptr") return put(out, q->table_ptr);
+  if (f == "entry_retained") return put(out, q->entry_retained);
+  if (f == "entry_col") return put(out, q->entry_col);
+  if (f == "entry_table") return put(out, q->entry_table);
+  if (f == "retained_ptr") return put(out, q->retained_ptr);
+  if (f == "retained_entry") return put(out, q->retained_entry);
+  if (f == "doffsets") return put(out, q->doffsets);
+  if (f == "col_chunks") return put(out, q->col_chunks);
+  if (f == "row_table") return put(out, q->row_table);
+  if (f == "row_first") return put(out, q->row_first);
+  if (f == "row_nrows") return put(out, q->row_nrows);
+  if (f == "row_ptr") return put(out, q->row_ptr);
+  if (f == "row_blocks") return put(out, q->row_blocks);
+  return -1;
+}
+
+int bls_qr_structure_schur(const bls_qr_structure* q, bls_structure** out) {
+  BLS_GUARD({
+    if (!q || !out) throw Error(BLS_EINVAL, "null argument");
+    auto* s = new bls_structure();
+    static_cast<Structure&>(*s) = q->schur;
+    *out = s;
+    return BLS_OK;
+  })
+}
+
+int bls_qr_structure_destroy(bls_qr_structure* q) {
+  delete q;
+  return BLS_OK;
 }
 
 }  // extern "C"

@@ -9,6 +9,7 @@
 #include "host_layout.hpp"
 
 #include <algorithm>
+#include <map>
 #include <cstring>
 #include <limits>
 #include <numeric>
@@ -146,7 +147,8 @@ Structure structure_positional(const std::vector<int64_t>& r_dims, const std::ve
 }
 
 Structure structure_from_description(int64_t n, const int64_t* blocksizes, int64_t K, const int64_t* rb_ptr,
-                                     const int64_t* rb_idx, const uint8_t* eliminated, int64_t nchunks, int64_t min_work) {
+                                     const int64_t* rb_idx, const uint8_t* eliminated, int64_t nchunks, int64_t min_work,
+                                     const int64_t* rowblocksizes) {
   for (int64_t i = 0; i < n; ++i) check_dim(blocksizes[i], i);
   int64_t nret = 0;
   for (int64_t i = 0; i < n; ++i) nret += eliminated[i] ? 0 : 1;
@@ -155,13 +157,17 @@ Structure structure_from_description(int64_t n, const int64_t* blocksizes, int64
                                 std::to_string(nret) + " retained and " + std::to_string(n - nret) + " eliminated");
   // one pass over the row blocks (src/schur_description.jl:37-59); coupled (e, r) pairs bucketed by e afterwards
   std::vector<int64_t> seen(n, -1), cnt(n + 1, 0);
+  std::vector<char> hasrow(rowblocksizes ? n : 0, 0);
   for (int64_t k = 0; k < K; ++k) {
+    if (rowblocksizes && rowblocksizes[k] < 1)
+      throw Error(BLS_EINVAL, "Row block " + std::to_string(k + 1) + " has " + std::to_string(rowblocksizes[k]) + " rows; every row block needs at least 1 row");
     int64_t e = -1;
     for (int64_t p = rb_ptr[k]; p < rb_ptr[k + 1]; ++p) {
       const int64_t b = rb_idx[p];
       if (b < 0 || b >= n) throw Error(BLS_EINVAL, "Row block " + std::to_string(k + 1) + " touches column block " + std::to_string(b + 1) + ", but there are " + std::to_string(n) + " column blocks");
       if (seen[b] == k) throw Error(BLS_EINVAL, "Row block " + std::to_string(k + 1) + " lists column block " + std::to_string(b + 1) + " more than once");
       seen[b] = k;
+      if (rowblocksizes) hasrow[b] = 1;
       if (eliminated[b]) {
         if (e >= 0) throw Error(BLS_EINVAL, "Row block " + std::to_string(k + 1) + " touches two eliminated column blocks, " + std::to_string(e + 1) + " and " + std::to_string(b + 1) + "; a row block may touch at most one");
         e = b;
@@ -171,6 +177,9 @@ Structure structure_from_description(int64_t n, const int64_t* blocksizes, int64
       for (int64_t p = rb_ptr[k]; p < rb_ptr[k + 1]; ++p)
         if (!eliminated[rb_idx[p]]) cnt[e + 1] += 1;
   }
+  if (rowblocksizes)
+    for (int64_t b = 0; b < n; ++b)
+      if (eliminated[b] && !hasrow[b]) throw Error(BLS_EINVAL, "Eliminated column block " + std::to_string(b + 1) + " is in no row block; eliminating a block needs at least one row");
   for (int64_t b = 0; b < n; ++b) cnt[b + 1] += cnt[b];
   std::vector<int64_t> coupled(cnt[n]);
   {
@@ -402,6 +411,128 @@ int64_t sparse_indices(const Structure& st, const Pattern& P, bool symmetric, in
     }
   }
   return nnz;
+}
+
+}  // namespace bls
+
+namespace bls {
+
+// SchurJacobianStructure(structure, e_rows; free_rows, free_retained, nchunks) (src/schur_jacobian.jl:59-160)
+QRStructure qr_structure(const Structure& st, const std::vector<int64_t>& e_rows, const std::vector<int64_t>& free_rows,
+                         const std::vector<std::vector<int64_t>>& free_retained, int64_t nchunks) {
+  QRStructure q;
+  q.schur = st;
+  const int64_t ne = st.neblocks, nrb = st.nrblocks, nfree = (int64_t)free_rows.size();
+  if ((int64_t)e_rows.size() != ne) throw Error(BLS_EDIM, "Number of eliminated row counts (" + std::to_string(e_rows.size()) + ") must match the number of eliminated blocks (" + std::to_string(ne) + ")");
+  if ((int64_t)free_retained.size() != nfree) throw Error(BLS_EDIM, "Number of free groups' retained lists must match the number of free row counts");
+  if (nchunks < 1) throw Error(BLS_EINVAL, "nchunks must be at least 1, got " + std::to_string(nchunks));
+  for (int64_t e = 0; e < ne; ++e)
+    if (e_rows[e] < 1) throw Error(BLS_EINVAL, "Eliminated block " + std::to_string(e + 1) + " has " + std::to_string(e_rows[e]) + " rows; every eliminated block needs at least 1 row");
+  for (int64_t g = 0; g < nfree; ++g)
+    if (free_rows[g] < 1) throw Error(BLS_EINVAL, "Free group " + std::to_string(g + 1) + " has " + std::to_string(free_rows[g]) + " rows; every free group needs at least 1 row");
+  {
+    std::vector<int64_t> seen(nrb, -1);
+    for (int64_t g = 0; g < nfree; ++g)
+      for (int64_t r : free_retained[g]) {
+        if (r < 0 || r >= nrb) throw Error(BLS_EINVAL, "Free group " + std::to_string(g + 1) + " references retained block " + std::to_string(r + 1));
+        if (seen[r] == g) throw Error(BLS_EINVAL, "Retained block " + std::to_string(r + 1) + " is listed more than once in free group " + std::to_string(g + 1));
+        seen[r] = g;
+      }
+  }
+  const int64_t nt = ne + nfree;
+  q.ntables = nt;
+  q.e_rows = e_rows;
+  q.free_rows = free_rows;
+  q.table_nrows.resize(nt); q.table_ncols.resize(nt); q.table_top.resize(nt); q.table_ptr.assign(nt + 1, 0);
+  for (int64_t t = 0; t < nt; ++t) {
+    std::vector<int64_t> rs;
+    if (t < ne) rs.assign(st.entry_retained.begin() + st.eliminated_ptr[t], st.entry_retained.begin() + st.eliminated_ptr[t + 1]);
+    else { rs = free_retained[t - ne]; std::sort(rs.begin(), rs.end()); }
+    int64_t col = 0;
+    for (int64_t r : rs) {
+      q.entry_retained.push_back(r);
+      q.entry_col.push_back(col);
+      q.entry_table.push_back(t);
+      col += st.r_dims[r];
+    }
+    q.table_ptr[t + 1] = (int64_t)q.entry_retained.size();
+    const int64_t de = t < ne ? st.e_dims[t] : 0;
+    q.table_top[t] = de;
+    q.table_nrows[t] = t < ne ? e_rows[t] + de : free_rows[t - ne];
+    q.table_ncols[t] = col + de + 1;
+  }
+  q.table_offsets.assign(nt + 1, 0); q.raw_offsets.assign(nt + 1, 0); q.residual_offsets.assign(nt + 1, 0); q.reduced_offsets.assign(nt + 1, 0);
+  for (int64_t t = 0; t < nt; ++t) {
+    q.table_offsets[t + 1] = q.table_offsets[t] + q.table_nrows[t] * q.table_ncols[t];
+    q.raw_offsets[t + 1] = q.raw_offsets[t] + q.table_nrows[t] * (q.table_ncols[t] - 1);
+    q.residual_offsets[t + 1] = q.residual_offsets[t] + q.table_nrows[t];
+    q.reduced_offsets[t + 1] = q.reduced_offsets[t] + q.table_nrows[t] - q.table_top[t];
+  }
+  const int64_t nent = (int64_t)q.entry_retained.size();
+  q.retained_ptr.assign(nrb + 1, 0);
+  for (int64_t u = 0; u < nent; ++u) q.retained_ptr[q.entry_retained[u] + 1] += 1;
+  for (int64_t r = 0; r < nrb; ++r) q.retained_ptr[r + 1] += q.retained_ptr[r];
+  q.retained_entry.resize(nent);
+  {
+    std::vector<int64_t> pos(q.retained_ptr.begin(), q.retained_ptr.end() - 1);
+    for (int64_t u = 0; u < nent; ++u) q.retained_entry[pos[q.entry_retained[u]]++] = u;
+  }
+  q.doffsets.assign(nrb + 1, 0);
+  for (int64_t r = 0; r < nrb; ++r) q.doffsets[r + 1] = q.doffsets[r] + st.r_dims[r] * st.r_dims[r];
+  q.col_chunks = partition_columns(q.retained_ptr, nchunks);
+  return q;
+}
+
+// SchurJacobianStructure(blocksizes, rowblocks, rowblocksizes; eliminated) (src/schur_description.jl:137-189): each row
+// block's rows go to its eliminated block's table, or to the table of its free group (row blocks with the same retained
+// blocks, numbered by first appearance), in row-block order.
+QRStructure qr_structure_from_description(int64_t n, const int64_t* blocksizes, int64_t K, const int64_t* rb_ptr, const int64_t* rb_idx,
+                                          const int64_t* rowblocksizes, const uint8_t* eliminated, int64_t nchunks, int64_t min_work) {
+  Structure st = structure_from_description(n, blocksizes, K, rb_ptr, rb_idx, eliminated, nchunks, min_work, rowblocksizes);
+  const int64_t nret = st.nrblocks, ne = st.neblocks;
+  std::vector<int64_t> position(n);
+  for (int64_t p = 0; p < n; ++p) position[st.order[p]] = p;
+  std::vector<int64_t> row_table(K), row_first(K), e_rows(ne, 0), free_rows_v, row_ptr(K + 1, 0), row_blocks(rb_ptr[K]);
+  std::vector<std::vector<int64_t>> free_retained;
+  std::map<std::vector<int64_t>, int64_t> group;
+  for (int64_t k = 0; k < K; ++k) row_ptr[k + 1] = rb_ptr[k + 1] - rb_ptr[0];
+  for (int64_t k = 0; k < K; ++k) {
+    const int64_t m = rowblocksizes[k];
+    int64_t e = -1;
+    for (int64_t p = rb_ptr[k]; p < rb_ptr[k + 1]; ++p) {
+      row_blocks[p - rb_ptr[0]] = position[rb_idx[p]];
+      if (eliminated[rb_idx[p]]) e = rb_idx[p];
+    }
+    std::sort(row_blocks.begin() + row_ptr[k], row_blocks.begin() + row_ptr[k + 1]);
+    if (e >= 0) {
+      const int64_t t = position[e] - nret;
+      row_table[k] = t;
+      row_first[k] = e_rows[t];
+      e_rows[t] += m;
+    } else {
+      std::vector<int64_t> rs(row_blocks.begin() + row_ptr[k], row_blocks.begin() + row_ptr[k + 1]);
+      auto it = group.find(rs);
+      int64_t g;
+      if (it == group.end()) {
+        free_retained.push_back(rs);
+        free_rows_v.push_back(0);
+        g = (int64_t)free_rows_v.size() - 1;
+        group[rs] = g;
+      } else {
+        g = it->second;
+      }
+      row_table[k] = ne + g;
+      row_first[k] = free_rows_v[g];
+      free_rows_v[g] += m;
+    }
+  }
+  QRStructure q = qr_structure(st, e_rows, free_rows_v, free_retained, nchunks);
+  q.row_table = row_table;
+  q.row_first = row_first;
+  q.row_nrows.assign(rowblocksizes, rowblocksizes + K);
+  q.row_ptr = row_ptr;
+  q.row_blocks = row_blocks;
+  return q;
 }
 
 }  // namespace bls

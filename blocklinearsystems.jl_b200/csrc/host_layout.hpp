@@ -40,9 +40,30 @@ void finish_structure(Structure& st, const std::vector<std::vector<int64_t>>& co
 Structure structure_positional(const std::vector<int64_t>& r_dims, const std::vector<int64_t>& e_dims,
                                const std::vector<std::vector<int64_t>>& couplings, int64_t nchunks, int64_t min_work);
 Structure structure_from_description(int64_t n, const int64_t* blocksizes, int64_t K, const int64_t* rb_ptr,
-                                     const int64_t* rb_idx, const uint8_t* eliminated, int64_t nchunks, int64_t min_work);
+                                     const int64_t* rb_idx, const uint8_t* eliminated, int64_t nchunks, int64_t min_work,
+                                     const int64_t* rowblocksizes = nullptr);
 Pattern build_pattern(const Structure& st, const std::vector<std::pair<int64_t, int64_t>>& extra);
 std::vector<int64_t> build_r_to_s(const Structure& st, const Pattern& P);
 int64_t sparse_indices(const Structure& st, const Pattern& P, bool symmetric, int64_t* colptr, int64_t* rowval, int64_t* map);
+
+}  // namespace bls
+
+namespace bls {
+
+// SchurJacobianStructure (src/schur_jacobian.jl:30-57): one table per eliminated block (its rows, then d_e damping rows;
+// columns: the coupled retained blocks' columns, then the d_e eliminated columns; the residual is a separate FP64 column),
+// then one table per free group of row blocks that touch no eliminated block.
+struct QRStructure {
+  Structure schur;
+  int64_t ntables = 0;
+  std::vector<int64_t> e_rows, free_rows, table_nrows, table_ncols, table_top, table_offsets, raw_offsets, residual_offsets;
+  std::vector<int64_t> table_ptr, entry_retained, entry_col, entry_table, retained_ptr, retained_entry, reduced_offsets, doffsets;
+  std::vector<int64_t> col_chunks, row_table, row_first, row_nrows, row_ptr, row_blocks;
+};
+
+QRStructure qr_structure(const Structure& st, const std::vector<int64_t>& e_rows, const std::vector<int64_t>& free_rows,
+                         const std::vector<std::vector<int64_t>>& free_retained, int64_t nchunks);
+QRStructure qr_structure_from_description(int64_t n, const int64_t* blocksizes, int64_t K, const int64_t* rb_ptr, const int64_t* rb_idx,
+                                          const int64_t* rowblocksizes, const uint8_t* eliminated, int64_t nchunks, int64_t min_work);
 
 }  // namespace bls

@@ -255,4 +255,38 @@ void bls_scene_assemble(const bls_scene* S, const int64_t* position, const int64
     }
 }
 
+// Fill the raw Jacobian tables of a QR structure built from bls_scene_description with rowblocksizes 2 (the
+// reference's block!/residual_block! writes, src/schur_jacobian.jl:368-387): observation o is row block o, its two rows
+// at row_first[o] of table row_table[o]; its camera Jacobian goes to the columns of the camera's entry, its point
+// Jacobian to the table's last three columns, its residual to the table's residual rows. Damping rows stay zero.
+// position: layout position of each caller block; the cameras are the retained blocks.
+int bls_scene_assemble_qr(const bls_scene* S, const int64_t* position, const int64_t* row_table, const int64_t* row_first,
+                          const int64_t* table_ptr, const int64_t* entry_retained, const int64_t* entry_col, const int64_t* table_nrows,
+                          const int64_t* table_ncols, const int64_t* raw_offsets, const int64_t* residual_offsets, double* Rw, int64_t Rw_len,
+                          double* Rr, int64_t Rr_len) {
+  std::memset(Rw, 0, Rw_len * 8);
+  std::memset(Rr, 0, Rr_len * 8);
+  int bad = 0;
+#pragma omp parallel for schedule(static, 1024) reduction(| : bad)
+  for (int64_t p = 0; p < S->npoints; ++p)
+    for (int64_t o = S->obs_ptr[p]; o < S->obs_ptr[p + 1]; ++o) {
+      const int64_t t = row_table[o], M = table_nrows[t], C = table_ncols[t] - 1, r0 = row_first[o];
+      const int64_t cam = position[S->obs_cam[o]];
+      const int64_t* lo = entry_retained + table_ptr[t];
+      const int64_t* hi = entry_retained + table_ptr[t + 1];
+      const int64_t* f = std::lower_bound(lo, hi, cam);
+      if (f == hi || *f != cam || r0 + 2 > M || raw_offsets[t + 1] > Rw_len || residual_offsets[t + 1] > Rr_len) { bad = 1; continue; }
+      const int64_t col = entry_col[f - entry_retained];
+      double* T = Rw + raw_offsets[t];
+      const double* Jc = S->Jc.data() + o * 12;
+      const double* Jp = S->Jp.data() + o * 6;
+      for (int j = 0; j < 6; ++j)
+        for (int i = 0; i < 2; ++i) T[(col + j) * M + r0 + i] = Jc[2 * j + i];
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 2; ++i) T[(C - 3 + j) * M + r0 + i] = Jp[2 * j + i];
+      for (int i = 0; i < 2; ++i) Rr[residual_offsets[t] + r0 + i] = S->r[o * 2 + i];
+    }
+  return bad ? -1 : 0;
+}
+
 }  // extern "C"

@@ -61,7 +61,7 @@ struct SchurPlan {
   // camera's row offset in the column's tile; per column the S index of its first entry
   DevBuf vis_rec, vis_base, vis_off, col_base, col_h;
   int64_t max_col_h = 0;
-  int kernel = 0;   // 0: column-owned (k_columns36), 1: block-owned pairs (k_pairs36)
+  int kernel = 1;   // 0: column-owned (k_columns36), 1: block-owned pairs (k_pairs36, the default: faster on sparse scenes)
   // reset
   DevBuf r_to_s, diag_inds, S_rowval, S_col;
   // scratch: E^-1 (FP64, and FP32 for the mixed form), z, status

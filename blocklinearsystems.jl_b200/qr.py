@@ -1,0 +1,258 @@
+"""QR elimination on the device, mirroring the reference's Jacobian-path API (0-based layout, torch CUDA tensors).
+
+SchurJacobianStructure    src/schur_jacobian.jl:30-160, src/schur_description.jl:137-189 (layout built natively)
+SchurBlockJacobian        src/schur_jacobian.jl:194-208 (raw tables `data` in T, residual `r` in float64)
+QRReductionWorkspace      src/qr_reduction.jl:11-24 (here: the device plan plus the factored tables)
+reduce_qr                 src/qr_reduction.jl:162-187 -> bool
+qr_backsubstitute         src/qr_reduced.jl:97-110 (the reference's backsubstitute!(x_e, x_r, ws))
+reduced_normal_sparse     src/qr_reduced.jl:438-480
+reduced_normal_dense      src/qr_reduced.jl:407-436
+reduced_diagonal_blocks   src/qr_reduced.jl:482-512
+free_block_pairs          src/qr_reduced.jl:5-16
+reduced_nrows             src/qr_reduced.jl:1-3
+
+Element type T is the dtype of the Jacobian's tables: torch.float64, or torch.float32 (the mixed form: FP32 tables with
+FP64 column norms, reflector scalars and reflector application, rounded once per entry; the residual is FP64 in both).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import BLS_NOT_PD, ArgumentError, DimensionMismatch, check, dptr, ptr64
+from .layout import DEFAULT_MIN_WORK, SchurPattern, SchurStructure, _csr
+from .reduction import _dev, _dtype_code, context
+
+
+class SchurJacobianStructure:
+    """The layout of a QR elimination: one table per eliminated block, then one per free group (0-based fields).
+
+    SchurJacobianStructure(blocksizes, rowblocks, rowblocksizes, eliminated=...) lays out a description in the caller's
+    numbering; SchurJacobianStructure.positional(structure, e_rows, free_rows, free_retained) is the positional form.
+    """
+
+    _FIELDS = ("e_rows", "free_rows", "table_nrows", "table_ncols", "table_top", "table_offsets", "raw_offsets",
+               "residual_offsets", "reduced_offsets", "table_ptr", "entry_retained", "entry_col", "entry_table", "retained_ptr",
+               "retained_entry", "doffsets", "col_chunks", "row_table", "row_first", "row_nrows", "row_ptr", "row_blocks")
+    _SCALARS = ("ntables", "raw_length", "residual_length")
+
+    def __init__(self, blocksizes=None, rowblocks=None, rowblocksizes=None, *, eliminated=None, nchunks: int = 1,
+                 min_work: int = DEFAULT_MIN_WORK, _handle=None):
+        L = _lib.gpu()
+        if _handle is None:
+            if eliminated is None:
+                raise TypeError("eliminated is required")
+            bs = np.ascontiguousarray(blocksizes, np.int64)
+            el = np.ascontiguousarray(np.asarray(eliminated, bool), np.uint8)
+            if len(el) != len(bs):
+                raise DimensionMismatch(f"eliminated has length {len(el)}, but there are {len(bs)} column blocks")
+            ptr, idx = _csr(rowblocks)
+            rbs = np.ascontiguousarray(rowblocksizes, np.int64)
+            if len(rbs) != len(ptr) - 1:
+                raise DimensionMismatch(f"rowblocksizes has length {len(rbs)}, but there are {len(ptr) - 1} row blocks")
+            h = C.c_void_p()
+            check(L.bls_qr_structure_from_description(len(bs), ptr64(bs), len(ptr) - 1, ptr64(ptr), ptr64(idx), ptr64(rbs),
+                                                      el.ctypes.data_as(C.POINTER(C.c_uint8)), int(nchunks), int(min_work),
+                                                      C.byref(h)))
+            _handle = h
+        self._h = _handle
+        for f in self._SCALARS:
+            setattr(self, f, int(self._field(f)[0]))
+        for f in self._FIELDS:
+            setattr(self, f, self._field(f))
+        sh = C.c_void_p()
+        check(L.bls_qr_structure_schur(self._h, C.byref(sh)))
+        self.schur = SchurStructure(_handle=sh)
+
+    @classmethod
+    def positional(cls, structure: SchurStructure, e_rows, free_rows=(), free_retained=(), *, nchunks: int = 1):
+        er = np.ascontiguousarray(e_rows, np.int64)
+        fr = np.ascontiguousarray(free_rows, np.int64)
+        if len(er) != structure.neblocks:
+            raise DimensionMismatch(f"Number of eliminated row counts ({len(er)}) must match the number of eliminated blocks "
+                                    f"({structure.neblocks})")
+        if len(free_retained) != len(fr):
+            raise DimensionMismatch("Number of free groups' retained lists must match the number of free row counts")
+        ptr, idx = _csr([list(x) for x in free_retained])
+        h = C.c_void_p()
+        check(_lib.gpu().bls_qr_structure_positional(structure.handle, ptr64(er), len(fr), ptr64(fr), ptr64(ptr), ptr64(idx),
+                                                     int(nchunks), C.byref(h)))
+        return cls(_handle=h)
+
+    def _field(self, name: str) -> np.ndarray:
+        L = _lib.gpu()
+        n = L.bls_qr_structure_field(self._h, name.encode(), None)
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, np.int64)
+        if n:
+            L.bls_qr_structure_field(self._h, name.encode(), ptr64(out))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None and _lib._gpu is not None:
+            _lib.gpu().bls_qr_structure_destroy(h)
+            self._h = None
+
+    # accessors (src/schur_description.jl:199-214)
+    def blockorder(self) -> np.ndarray:
+        return self.schur.blockorder()
+
+    def nretained(self) -> int:
+        return self.schur.nrblocks
+
+    def nblocks(self) -> int:
+        return self.schur.nrblocks + self.schur.neblocks
+
+    @property
+    def handle(self):
+        return self._h
+
+
+def free_block_pairs(jst: SchurJacobianStructure) -> list[tuple[int, int]]:
+    """Pairs of retained blocks coupled through a free group (src/qr_reduced.jl:5-16), in the reference's order."""
+    pairs: list[tuple[int, int]] = []
+    seen = set()
+    for t in range(jst.schur.neblocks, jst.ntables):
+        lo, hi = int(jst.table_ptr[t]), int(jst.table_ptr[t + 1])
+        for u2 in range(lo, hi):
+            for u1 in range(lo, u2):
+                p = (int(jst.entry_retained[u1]), int(jst.entry_retained[u2]))
+                if p not in seen:
+                    seen.add(p)
+                    pairs.append(p)
+    return pairs
+
+
+def reduced_nrows(jst: SchurJacobianStructure) -> int:
+    """Rows of the reduced Jacobian J~ (src/qr_reduced.jl:1-3)."""
+    return int(jst.reduced_offsets[-1])
+
+
+class SchurBlockJacobian:
+    """The raw tables (`data`, T, length raw_length) and the residual (`r`, float64, length residual_length) on the
+    device, zero-initialised as SchurBlockJacobian(structure, T) (src/schur_jacobian.jl:194-208)."""
+
+    def __init__(self, structure: SchurJacobianStructure, dtype=torch.float64, device: int = 0, data=None, r=None):
+        self.structure = structure
+        dev = torch.device("cuda", device)
+        self.data = torch.zeros(structure.raw_length, dtype=dtype, device=dev) if data is None else data
+        self.r = torch.zeros(structure.residual_length, dtype=torch.float64, device=dev) if r is None else r
+        _dev(self.data, "J.data", structure.raw_length)
+        _dev(self.r, "J.r", structure.residual_length, torch.float64)
+
+
+class QRReductionWorkspace:
+    """The device plan of a QR elimination plus its factored tables (`factored`, T) and factored residual (`fres`,
+    float64). `pattern` (build_schur_pattern(structure.schur, extra_blocks=free_block_pairs(structure))) is needed for
+    reduced_normal_sparse. `failed_block`: the lowest failing eliminated block of the last reduce_qr, 1-based, 0 none."""
+
+    def __init__(self, structure: SchurJacobianStructure, pattern: SchurPattern | None = None, dtype=torch.float64,
+                 *, device: int = 0):
+        self.structure, self.pattern, self.device, self.dtype = structure, pattern, device, dtype
+        ctx = context(device)
+        st = structure.schur
+        keep = []
+
+        def arr(a):
+            a = np.ascontiguousarray(a, np.int64)
+            keep.append(a)
+            return ptr64(a)
+
+        d = _lib.bls_qr_plan_desc()
+        d.nrblocks, d.neblocks, d.ntables = st.nrblocks, st.neblocks, structure.ntables
+        d.r_dims, d.e_dims = arr(st.r_dims), arr(st.e_dims)
+        d.table_nrows, d.table_ncols, d.table_top = arr(structure.table_nrows), arr(structure.table_ncols), arr(structure.table_top)
+        d.table_ptr, d.entry_retained, d.entry_col = arr(structure.table_ptr), arr(structure.entry_retained), arr(structure.entry_col)
+        d.raw_offsets, d.residual_offsets = arr(structure.raw_offsets), arr(structure.residual_offsets)
+        if pattern is not None:
+            d.block_colptr, d.block_rowval = arr(pattern.block_colptr), arr(pattern.block_rowval)
+            d.block_row_offsets, d.col_heights, d.S_colptr = arr(pattern.block_row_offsets), arr(pattern.col_heights), arr(pattern.S_colptr)
+        h = C.c_void_p()
+        check(_lib.gpu().bls_qr_plan_create(ctx, C.byref(d), C.byref(h)))
+        self._h = h
+        dev = torch.device("cuda", device)
+        self.factored = torch.zeros(structure.raw_length, dtype=dtype, device=dev)
+        self.fres = torch.zeros(structure.residual_length, dtype=torch.float64, device=dev)
+        self.failed_block = 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None and _lib._gpu is not None:
+            _lib.gpu().bls_qr_plan_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        context(self.device)
+        return self._h
+
+    @property
+    def _T(self) -> int:
+        return _dtype_code(self.factored)
+
+
+def reduce_qr(ws: QRReductionWorkspace, J: SchurBlockJacobian, scaling_e: torch.Tensor, lam: float, s: torch.Tensor | None = None) -> bool:
+    """QR elimination of every eliminated block (src/qr_reduction.jl:162-187); conditioned by `s` (over all the
+    variables, [s_r; s_e]) when given. False: a non-finite table or a numerically singular U (ws.failed_block)."""
+    jst = ws.structure
+    if J.structure is not jst:
+        raise ArgumentError("The Jacobian and the workspace were built for different structures")
+    if J.data.dtype != ws.dtype:
+        raise ArgumentError(f"the Jacobian is {J.data.dtype}, the workspace {ws.dtype}")
+    st = jst.schur
+    _dev(scaling_e, "scaling_e", st.ne, torch.float64)
+    if s is not None:
+        _dev(s, "s", st.nr + st.ne, torch.float64)
+    fb = C.c_int64(0)
+    rc = check(_lib.gpu().bls_reduce_qr(ws.handle, ws._T, dptr(ws.factored), dptr(ws.fres), dptr(J.data), dptr(J.r), dptr(scaling_e),
+                                        float(lam), dptr(s), C.byref(fb)))
+    ws.failed_block = int(fb.value)
+    return rc != BLS_NOT_PD
+
+
+def qr_backsubstitute(x_e: torch.Tensor, x_r: torch.Tensor, ws: QRReductionWorkspace) -> None:
+    """x_e = U^-1 (q - B x_r) per eliminated block, in float64 (src/qr_reduced.jl:24-110)."""
+    st = ws.structure.schur
+    _dev(x_e, "x_e", st.ne, torch.float64)
+    _dev(x_r, "x_r", st.nr, torch.float64)
+    check(_lib.gpu().bls_qr_backsubstitute(ws.handle, ws._T, dptr(x_e), dptr(x_r), dptr(ws.factored), dptr(ws.fres)))
+
+
+def reduced_normal_dense(S: torch.Tensor, g_S: torch.Tensor, ws: QRReductionWorkspace) -> bool:
+    """Overwrite the upper triangle of the column-major nr x nr S with J~'J~ and g_S with J~'r~ (src/qr_reduced.jl:407-436)."""
+    nr = ws.structure.schur.nr
+    if S.dtype != ws.dtype:
+        raise ArgumentError(f"S must be {ws.dtype}")
+    _dev(S, "S", nr * nr)
+    _dev(g_S, "g_S", nr, torch.float64)
+    check(_lib.gpu().bls_reduced_normal_dense(ws.handle, ws._T, dptr(S), dptr(g_S), dptr(ws.factored), dptr(ws.fres)))
+    return True
+
+
+def reduced_normal_sparse(S_nzval: torch.Tensor, g_S: torch.Tensor, ws: QRReductionWorkspace, pattern: SchurPattern | None = None) -> bool:
+    """Sparse counterpart of reduced_normal_dense into S.nzval on the workspace's pattern (src/qr_reduced.jl:438-480)."""
+    pat = ws.pattern
+    if pat is None:
+        raise ArgumentError("the workspace was built without a sparse pattern")
+    if pattern is not None and pattern is not pat and len(pattern.S_rowval) != len(pat.S_rowval):
+        raise DimensionMismatch("the pattern does not match the workspace's")
+    if S_nzval.dtype != ws.dtype:
+        raise ArgumentError(f"S must be {ws.dtype}")
+    _dev(S_nzval, "S.nzval", pat.nnz)
+    _dev(g_S, "g_S", ws.structure.schur.nr, torch.float64)
+    check(_lib.gpu().bls_reduced_normal_sparse(ws.handle, ws._T, dptr(S_nzval), dptr(g_S), dptr(ws.factored), dptr(ws.fres)))
+    return True
+
+
+def reduced_diagonal_blocks(D: torch.Tensor, ws: QRReductionWorkspace) -> torch.Tensor:
+    """The full d_r x d_r diagonal blocks of J~'J~, at doffsets (src/qr_reduced.jl:482-512)."""
+    if D.dtype != ws.dtype:
+        raise ArgumentError(f"D must be {ws.dtype}")
+    _dev(D, "D", int(ws.structure.doffsets[-1]))
+    check(_lib.gpu().bls_reduced_diagonal_blocks(ws.handle, ws._T, dptr(D), dptr(ws.factored)))
+    return D

@@ -113,7 +113,7 @@ class SchurReductionWorkspace:
         return int(_lib.gpu().bls_schur_plan_device_bytes(self._h))
 
     def set_kernel(self, which: str) -> None:
-        """Phase-2 kernel of the 6/3 fast path: "columns" (block-column owned, default) or "pairs" (block owned)."""
+        """Phase-2 kernel of the 6/3 fast path: "pairs" (block owned, the default) or "columns" (block-column owned)."""
         check(_lib.gpu().bls_schur_plan_set_kernel(self._h, {"columns": 0, "pairs": 1}[which]))
 
     def instrument(self, timing: bool = True) -> None:

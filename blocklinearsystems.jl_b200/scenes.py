@@ -178,3 +178,38 @@ def hessian_problem(spec: SceneSpec, *, dense: bool = False, nchunks: int = 1, m
             for i in range(d):
                 scaling_r[st.boffsets_r[r] + i] = R[R_diag[r] + i * (d + 1)]
     return HessianProblem(spec, st, pat, dense, E, Cd, R, b_r, b_e, scaling_r, scaling_e, spec.lam, sc.nobs)
+
+
+@dataclass
+class JacobianProblem:
+    """A scene laid out as the reference's SchurBlockJacobian: one row block [camera, point] of 2 rows per observation,
+    the raw tables (float64) and the residual (float64) in the structure's layout, damping sqrt(lambda * scaling_e) with
+    scaling_e = 1 (the plain sqrt(lambda) I damping rows)."""
+    spec: SceneSpec
+    structure: "object"    # qr.SchurJacobianStructure
+    Rw: np.ndarray
+    Rr: np.ndarray
+    scaling_e: np.ndarray
+    lam: float
+    nobs: int
+
+
+def jacobian_problem(spec: SceneSpec, *, nchunks: int = 1, min_work: int = 4096) -> JacobianProblem:
+    """Generate a scene, lay it out with SchurJacobianStructure(blocksizes, rowblocks, rowblocksizes; eliminated) and
+    write each observation's camera and point Jacobians and residual into its table (src/schur_jacobian.jl:368-387)."""
+    from .qr import SchurJacobianStructure
+    sc = Scene(spec)
+    bs, el, ptr, idx = sc.description()
+    rbs = np.full(len(ptr) - 1, 2, np.int64)
+    jst = SchurJacobianStructure(bs, (ptr, idx), rbs, eliminated=el, nchunks=nchunks, min_work=min_work)
+    Rw = np.empty(jst.raw_length)
+    Rr = np.empty(jst.residual_length)
+    position = np.ascontiguousarray(jst.schur.position())
+    dp = C.POINTER(C.c_double)
+    rc = _lib.scene_lib().bls_scene_assemble_qr(sc._h, ptr64(position), ptr64(jst.row_table), ptr64(jst.row_first), ptr64(jst.table_ptr),
+                                                ptr64(jst.entry_retained), ptr64(jst.entry_col), ptr64(jst.table_nrows),
+                                                ptr64(jst.table_ncols), ptr64(jst.raw_offsets), ptr64(jst.residual_offsets),
+                                                Rw.ctypes.data_as(dp), len(Rw), Rr.ctypes.data_as(dp), len(Rr))
+    if rc != 0:
+        raise ValueError("the scene does not match the structure")
+    return JacobianProblem(spec, jst, Rw, Rr, np.ones(jst.schur.ne), spec.lam, sc.nobs)

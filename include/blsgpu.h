@@ -153,8 +153,8 @@ int bls_reduce_schur_dense(bls_schur_plan* plan, int dtype, void* S_dev, double*
  * reduction on the plan's stream. bls_schur_plan_counters synchronises on the last event, reports the device kernel
  * launches issued since the previous read, the summed pair-kernel time and its number of launches, and resets them. */
 int bls_schur_plan_instrument(bls_schur_plan* plan, int timing);
-/* Phase-2 kernel of the d_r = 6 / d_e = 3 fast path (no counterpart in the reference): 0 = block-column owned
- * (default), 1 = block owned (pair lists). Both compute the same reduction; the choice is kept for comparisons. */
+/* Phase-2 kernel of the d_r = 6 / d_e = 3 fast path (no counterpart in the reference): 0 = block-column owned,
+ * 1 = block owned (pair lists; the default). Both compute the same reduction; the choice is kept for comparisons. */
 int bls_schur_plan_set_kernel(bls_schur_plan* plan, int which);
 int bls_schur_plan_counters(bls_schur_plan* plan, int64_t* launches, double* pair_kernel_ms, int64_t* pair_kernel_launches);
 
@@ -183,6 +183,75 @@ int bls_reduce_schur_dense_noalloc(void* cuda_stream, int dtype, int64_t nrblock
                                    double* g_S_dev, const double* b_r_dev, const double* b_e_dev,
                                    const double* scaling_e_dev, double lambda, const void* E_dev, const void* C_dev,
                                    int64_t* failed_block);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * QR elimination (src/schur_jacobian.jl, src/qr_reduction.jl, src/qr_reduced.jl). The Jacobian is stored as one table
+ * per eliminated block (its rows, then d_e damping rows; columns: the coupled retained blocks' columns in ascending
+ * order, then the d_e eliminated columns, column-major, `raw_offsets`), then one table per free group of row blocks
+ * that touch no eliminated block; the residual is a separate double vector (`residual_offsets`).
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* SchurJacobianStructure(blocksizes, rowblocks, rowblocksizes; eliminated, nchunks, min_work)
+ * (src/schur_description.jl:137-189), rowblocks in CSR form as for bls_structure_from_description. */
+int bls_qr_structure_from_description(int64_t nblocks, const int64_t* blocksizes, int64_t nrowblocks, const int64_t* rowblock_ptr,
+                                      const int64_t* rowblock_idx, const int64_t* rowblocksizes, const uint8_t* eliminated,
+                                      int64_t nchunks, int64_t min_work, bls_qr_structure** out);
+/* SchurJacobianStructure(structure, e_rows; free_rows, free_retained, nchunks) (src/schur_jacobian.jl:59-160):
+ * e_rows[neblocks]; free group g has free_rows[g] rows and retained blocks free_idx[free_ptr[g] .. free_ptr[g+1]). */
+int bls_qr_structure_positional(const bls_structure* st, const int64_t* e_rows, int64_t nfree, const int64_t* free_rows,
+                                const int64_t* free_ptr, const int64_t* free_idx, int64_t nchunks, bls_qr_structure** out);
+/* Fields (as bls_structure_field): ntables raw_length residual_length e_rows free_rows table_nrows table_ncols table_top
+ * table_offsets raw_offsets residual_offsets reduced_offsets table_ptr entry_retained entry_col entry_table retained_ptr
+ * retained_entry doffsets col_chunks row_table row_first row_nrows row_ptr row_blocks. */
+int64_t bls_qr_structure_field(const bls_qr_structure* q, const char* name, int64_t* out);
+/* The SchurStructure the QR structure is built on (a copy; destroy it with bls_structure_destroy). */
+int bls_qr_structure_schur(const bls_qr_structure* q, bls_structure** out);
+int bls_qr_structure_destroy(bls_qr_structure* q);
+
+/* Device plan of a QR elimination (QRReductionWorkspace, src/qr_reduction.jl:11-24, plus the J~'J~ work lists).
+ * d_r <= 16; an eliminated block's table (8 bytes per entry of its M x C columns plus its residual) must fit in
+ * 224 KB of shared memory (BLS_EUNSUPPORTED otherwise). */
+typedef struct bls_qr_plan_desc {
+  int64_t nrblocks, neblocks, ntables;
+  const int64_t* r_dims;            /* [nrblocks] */
+  const int64_t* e_dims;            /* [neblocks] */
+  const int64_t* table_nrows;       /* [ntables] */
+  const int64_t* table_ncols;       /* [ntables] including the residual column */
+  const int64_t* table_top;         /* [ntables] d_e, 0 for free tables */
+  const int64_t* table_ptr;         /* [ntables+1] entries of each table */
+  const int64_t* entry_retained;    /* [nentries] */
+  const int64_t* entry_col;         /* [nentries] first column of the entry in its table */
+  const int64_t* raw_offsets;       /* [ntables+1] */
+  const int64_t* residual_offsets;  /* [ntables+1] */
+  /* sparse pattern of J~'J~ (may be NULL for a dense-only plan), as in bls_schur_plan_desc */
+  const int64_t* block_colptr;
+  const int64_t* block_rowval;
+  const int64_t* block_row_offsets;
+  const int64_t* col_heights;
+  const int64_t* S_colptr;
+} bls_qr_plan_desc;
+
+int bls_qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* desc, bls_qr_plan** out);
+int bls_qr_plan_destroy(bls_qr_plan* plan);
+
+/* reduce_qr!(ws, J, scaling_e, lambda, s) (src/qr_reduction.jl:162-187): every eliminated table copied from the raw
+ * tables Rw / residual Rr into F / Fr, damped with sqrt(lambda*scaling_e) (times s_e) and QR-factored in place; free
+ * tables copied. s_dev: conditioning scale over all the variables [s_r; s_e], or NULL. Returns BLS_OK, BLS_NOT_PD
+ * (failed_block = the lowest eliminated block with a non-finite table or a numerically singular U, 1-based) or an error;
+ * failed_block NULL = asynchronous. */
+int bls_reduce_qr(bls_qr_plan* plan, int dtype, void* F_dev, double* Fr_dev, const void* Rw_dev, const double* Rr_dev,
+                  const double* scaling_e_dev, double lambda, const double* s_dev, int64_t* failed_block);
+/* qr_backsubstitute! (src/qr_reduced.jl:24-93): x_e = U^-1 (q - B x_r) per eliminated block, in double. */
+int bls_qr_backsubstitute(bls_qr_plan* plan, int dtype, double* x_e_dev, const double* x_r_dev, const void* F_dev,
+                          const double* Fr_dev);
+/* reduced_normal_sparse! / reduced_normal_dense! (src/qr_reduced.jl:409-480): S = J~'J~ (upper blocks; the sparse form
+ * on the plan's pattern, the dense form column-major nr x nr) and g_S = J~'r~ from the factored tables. */
+int bls_reduced_normal_sparse(bls_qr_plan* plan, int dtype, void* S_nzval_dev, double* g_S_dev, const void* F_dev,
+                              const double* Fr_dev);
+int bls_reduced_normal_dense(bls_qr_plan* plan, int dtype, void* S_dev, double* g_S_dev, const void* F_dev,
+                             const double* Fr_dev);
+/* reduced_diagonal_blocks! (src/qr_reduced.jl:484-512): the full d_r x d_r diagonal blocks of J~'J~ at doffsets. */
+int bls_reduced_diagonal_blocks(bls_qr_plan* plan, int dtype, void* D_dev, const void* F_dev);
 
 /* copyto!(csc, bsm, scatter_map) (src/SparseBlockLinearSystem.jl:356-362): dest[i] = src[map[i]], i < n. */
 int bls_scatter_copy(bls_ctx* ctx, int dtype, void* dest_dev, const void* src_dev, const int64_t* map_dev, int64_t n);

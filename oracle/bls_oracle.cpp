@@ -1582,6 +1582,14 @@ i64 orc_qr_field(OrcQR* o, const char* name, i64* out) {
   if (f == "free_rows") return put(out, q.free_rows.v, 0);
   if (f == "row_table") return put(out, q.row_table.v, -1);
   if (f == "row_first") return put(out, q.row_first.v, -1);
+  if (f == "row_nrows") return put(out, q.row_nrows.v, 0);
+  if (f == "row_ptr") return put(out, q.row_ptr.v, -1);
+  if (f == "row_blocks") return put(out, q.row_blocks.v, -1);
+  if (f == "col_chunks") {
+    std::vector<i64> v;
+    for (auto& c : q.col_chunks) { v.push_back(c.first - 1); v.push_back(c.last); }
+    return put(out, v, 0);
+  }
   return -1;
 }
 

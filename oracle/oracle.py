@@ -257,3 +257,91 @@ def inv_sym_block(H, damp, generic=False):
 
 def max_threads():
     return lib().orc_max_threads()
+
+
+class QRStructure:
+    """The oracle's SchurJacobianStructure (src/schur_jacobian.jl:59-160), 0-based fields."""
+
+    SCALARS = ("ntables",)
+    FIELDS = ("table_nrows", "table_ncols", "table_top", "table_offsets", "raw_offsets", "residual_offsets", "reduced_offsets",
+              "table_ptr", "entry_retained", "entry_col", "entry_table", "retained_ptr", "retained_entry", "doffsets", "e_rows",
+              "free_rows", "col_chunks")
+
+    def __init__(self, h, st: Structure):
+        self.h, self.st = h, st
+        for f in self.SCALARS:
+            setattr(self, f, int(self.field(f)[0]))
+        for f in self.FIELDS:
+            setattr(self, f, self.field(f))
+        self.raw_length = int(self.raw_offsets[-1])
+        self.residual_length = int(self.residual_offsets[-1])
+
+    @classmethod
+    def from_description(cls, blocksizes, rowblocks, rowblocksizes, eliminated, nchunks=1, min_work=4096):
+        bs = np.ascontiguousarray(blocksizes, np.int64)
+        el = np.ascontiguousarray(np.asarray(eliminated, bool), np.uint8)
+        rbs = np.ascontiguousarray(rowblocksizes, np.int64)
+        ptr, idx = _csr(rowblocks)
+        q, s = vp(), vp()
+        _chk(lib().orc_qr_structure_from_description(i64(len(bs)), _p(bs), i64(len(rbs)), _p(ptr), _p(idx), _p(rbs), _p(el), i64(nchunks),
+                                                     i64(min_work), C.byref(q), C.byref(s)))
+        return cls(q, Structure(s))
+
+    @classmethod
+    def positional(cls, st: Structure, e_rows, free_rows=(), free_retained=(), nchunks=1):
+        er = np.ascontiguousarray(e_rows, np.int64)
+        fr = np.ascontiguousarray(free_rows, np.int64)
+        ptr, idx = _csr([list(x) for x in free_retained])
+        q = vp()
+        _chk(lib().orc_qr_structure_positional(st.h, _p(er), i64(len(fr)), _p(fr) if len(fr) else None, _p(ptr) if len(fr) else None,
+                                               _p(idx) if len(idx) else None, i64(nchunks), C.byref(q)))
+        return cls(q, st)
+
+    def field(self, name):
+        n = lib().orc_qr_field(self.h, name.encode(), None)
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, np.int64)
+        if n:
+            lib().orc_qr_field(self.h, name.encode(), _p(out))
+        return out
+
+    def __del__(self):
+        if self.h and _L is not None:
+            _L.orc_qr_free(self.h)
+            self.h = None
+
+
+def reduce_qr(q: QRStructure, F, Fr, Rw, Rr, scaling_e, lam, s=None, nthreads=1):
+    """reduce_qr! (src/qr_reduction.jl:162-187) into F / Fr; returns (ok, failed_block 1-based)."""
+    fb = C.c_int64(0)
+    f = getattr(lib(), "orc_reduce_qr_" + _sfx(F))
+    rc = _chk(f(q.h, _p(F), _p(Fr), _p(Rw), _p(Rr), _p(scaling_e), i64(len(scaling_e)), C.c_double(lam), _p(s), C.c_int(nthreads),
+                C.byref(fb)))
+    return rc == 0, int(fb.value)
+
+
+def qr_backsubstitute(q: QRStructure, x_e, x_r, F, Fr):
+    return _chk(getattr(lib(), "orc_qr_backsubstitute_" + _sfx(F))(q.h, _p(x_e), _p(x_r), _p(F), _p(Fr)))
+
+
+def reduced_normal_sparse(q: QRStructure, pat: Pattern, nzval, g, F, Fr):
+    return _chk(getattr(lib(), "orc_reduced_normal_sparse_" + _sfx(F))(q.h, pat.h, _p(nzval), _p(g), _p(F), _p(Fr)))
+
+
+def reduced_normal_dense(q: QRStructure, S, g, F, Fr):
+    return _chk(getattr(lib(), "orc_reduced_normal_dense_" + _sfx(F))(q.h, _p(S), _p(g), _p(F), _p(Fr)))
+
+
+def reduced_diagonal_blocks(q: QRStructure, D, F):
+    return _chk(getattr(lib(), "orc_reduced_diagonal_blocks_" + _sfx(F))(q.h, _p(D), _p(F)))
+
+
+def factor_diagonal_blocks(D, dims):
+    dm = np.ascontiguousarray(dims, np.int64)
+    return _chk(getattr(lib(), "orc_factor_diagonal_blocks_" + _sfx(D))(_p(D), _p(dm), i64(len(dm)))) == 0
+
+
+def solve_diagonal_blocks(y, D, dims, x):
+    dm = np.ascontiguousarray(dims, np.int64)
+    getattr(lib(), "orc_solve_diagonal_blocks_" + _sfx(D))(_p(y), _p(D), _p(dm), i64(len(dm)), _p(x))

@@ -1,0 +1,235 @@
+"""Device QR elimination through the C ABI against the oracle (the reference's qr_table!/reduce_qr! restated on the CPU).
+
+FP64: factored tables, factored residual, J~'J~ (sparse and dense), J~'r~, the diagonal blocks and the back-substituted
+x_e within 1e-12 relative of the oracle (the device sums the column norms in another order; the reference's own
+identities, test/qr_reduction.jl:20-58, hold at 1e-10 and are checked too: J~'J~ is the Schur complement of the damped
+normal equations). Mixed form (FP32 tables, FP64 norms and reflector arithmetic): against the FP64 oracle on the same
+FP32-rounded tables, within 1e-5 relative on the reference's fixtures (condition numbers near 10) and within the
+bound stated in the scene test on the ill-conditioned QR workload.
+Failure reporting (the lowest failing table, non-finite and singular), argument checks, conditioning scales.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle as orc
+from qr_fixtures import QR_FIXTURES, fill_tables
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+def cu(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.to(DEV)
+
+
+def relerr(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def fixture(bls, name, seed=3):
+    rng = np.random.default_rng(seed)
+    fx = QR_FIXTURES[name](rng)
+    st = bls.SchurStructure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    ost = orc.Structure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    j = bls.SchurJacobianStructure.positional(st, fx["e_rows"], fx.get("free_rows", ()), fx.get("free_retained", ()))
+    o = orc.QRStructure.positional(ost, fx["e_rows"], fx.get("free_rows", ()), fx.get("free_retained", ()))
+    Rw, Rr, Jf, rf = fill_tables(j, rng)
+    sc_e = 0.5 + rng.random(j.schur.ne)
+    return j, o, Rw, Rr, Jf, rf, sc_e
+
+
+def run_both(bls, j, o, Rw, Rr, sc_e, lam, dtype, s=None, sparse=True):
+    npdt = np.float32 if dtype == torch.float32 else np.float64
+    Rw_s = Rw.astype(npdt)
+    pairs = bls.free_block_pairs(j)
+    pat = bls.build_schur_pattern(j.schur, pairs) if sparse else None
+    opat = orc.Pattern(o.st, pairs) if sparse else None
+    ws = bls.QRReductionWorkspace(j, pat, dtype)
+    J = bls.SchurBlockJacobian(j, dtype, data=cu(Rw_s), r=cu(Rr))
+    ok = bls.reduce_qr(ws, J, cu(sc_e), lam, None if s is None else cu(s))
+    F, Fr = np.zeros(o.raw_length), np.zeros(o.residual_length)
+    ook, ofb = orc.reduce_qr(o, F, Fr, Rw_s.astype(np.float64), Rr, sc_e, lam, s)
+    out = dict(ok=ok, fb=ws.failed_block, ook=ook, ofb=ofb, ws=ws, F=ws.factored.double().cpu().numpy(), oF=F,
+               Fr=ws.fres.cpu().numpy(), oFr=Fr, pat=pat, opat=opat)
+    if not (ok and ook):
+        return out
+    nr, ne = j.schur.nr, j.schur.ne
+    # J~'J~ and J~'r~, dense and sparse
+    Sd = torch.zeros(nr * nr, dtype=dtype, device=DEV)
+    gd = torch.zeros(nr, dtype=torch.float64, device=DEV)
+    bls.reduced_normal_dense(Sd, gd, ws)
+    oSd, ogd = np.zeros(nr * nr), np.zeros(nr)
+    orc.reduced_normal_dense(o, oSd, ogd, F, Fr)
+    out.update(Sd=Sd.double().cpu().numpy(), oSd=oSd, gd=gd.cpu().numpy(), ogd=ogd)
+    if sparse:
+        Ss = torch.zeros(pat.nnz, dtype=dtype, device=DEV)
+        gs = torch.zeros(nr, dtype=torch.float64, device=DEV)
+        bls.reduced_normal_sparse(Ss, gs, ws, pat)
+        oSs, ogs = np.zeros(opat.nnz), np.zeros(nr)
+        orc.reduced_normal_sparse(o, opat, oSs, ogs, F, Fr)
+        out.update(Ss=Ss.double().cpu().numpy(), oSs=oSs, gs=gs.cpu().numpy(), ogs=ogs)
+    D = torch.zeros(int(j.doffsets[-1]), dtype=dtype, device=DEV)
+    bls.reduced_diagonal_blocks(D, ws)
+    oD = np.zeros(int(o.doffsets[-1]))
+    orc.reduced_diagonal_blocks(o, oD, F)
+    x_r = np.random.default_rng(11).standard_normal(nr)
+    x_e = torch.zeros(ne, dtype=torch.float64, device=DEV)
+    bls.qr_backsubstitute(x_e, cu(x_r), ws)
+    ox_e = np.zeros(ne)
+    orc.qr_backsubstitute(o, ox_e, x_r, F, Fr)
+    out.update(D=D.double().cpu().numpy(), oD=oD, x_r=x_r, x_e=x_e.cpu().numpy(), ox_e=ox_e)
+    return out
+
+
+def check_close(out, tol, sparse=True, keys=("F", "Fr", "Sd", "gd", "D", "x_e")):
+    assert out["ok"] and out["ook"] and out["fb"] == 0
+    for k in keys + (("Ss", "gs") if sparse else ()):
+        t = tol[k] if isinstance(tol, dict) else tol
+        e = relerr(out[k], out["o" + k])
+        assert e <= t, f"{k}: relative error {e:.3e} > {t:.1e}"
+
+
+@pytest.mark.parametrize("name", list(QR_FIXTURES))
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+def test_fixtures_vs_oracle(bls, name, dtype):
+    j, o, Rw, Rr, Jf, rf, sc_e = fixture(bls, name)
+    out = run_both(bls, j, o, Rw, Rr, sc_e, 0.3, dtype)
+    check_close(out, 1e-12 if dtype == torch.float64 else 1e-5)
+
+
+@pytest.mark.parametrize("name", ["bundle adjustment", "free groups", "mixed dimensions"])
+def test_schur_identity(bls, name):
+    """J~'J~ = the Schur complement of the damped normal equations, J~'r~ the reduced right-hand side
+    (test/qr_reduction.jl:20-58), and x_e solves the eliminated rows: U x_e = q - B x_r."""
+    j, o, Rw, Rr, Jf, rf, sc_e = fixture(bls, name)
+    lam = 0.3
+    out = run_both(bls, j, o, Rw, Rr, sc_e, lam, torch.float64)
+    nr = j.schur.nr
+    H = Jf.T @ Jf
+    b = Jf.T @ rf
+    H[nr:, nr:] += lam * np.diag(sc_e)
+    X = np.linalg.solve(H[nr:, nr:], np.hstack([H[nr:, :nr], b[nr:, None]]))
+    S = H[:nr, :nr] - H[:nr, nr:] @ X[:, :nr]
+    g = b[:nr] - H[:nr, nr:] @ X[:, nr]
+    Sd = out["Sd"].reshape(nr, nr, order="F")
+    Sd = np.triu(Sd) + np.triu(Sd, 1).T
+    assert relerr(Sd, S) <= 1e-10
+    assert relerr(out["gd"], g) <= 1e-10
+    # back-substitution: the eliminated variables of the full damped solve given its retained ones
+    x_full = np.linalg.solve(H, b)
+    x_e = torch.zeros(j.schur.ne, dtype=torch.float64, device=DEV)
+    bls.qr_backsubstitute(x_e, cu(x_full[:nr]), out["ws"])
+    assert relerr(x_e.cpu().numpy(), x_full[nr:]) <= 1e-10
+
+
+def test_conditioning_scales(bls):
+    j, o, Rw, Rr, Jf, rf, sc_e = fixture(bls, "free groups")
+    rng = np.random.default_rng(5)
+    s = 2.0 ** rng.integers(-3, 4, j.schur.nr + j.schur.ne).astype(np.float64)
+    for dtype, tol in ((torch.float64, 1e-12), (torch.float32, 1e-5)):
+        check_close(run_both(bls, j, o, Rw, Rr, sc_e, 0.2, dtype, s=s), tol)
+
+
+def test_dense_only_plan(bls):
+    j, o, Rw, Rr, Jf, rf, sc_e = fixture(bls, "coupled to all")
+    out = run_both(bls, j, o, Rw, Rr, sc_e, 0.1, torch.float64, sparse=False)
+    check_close(out, 1e-12, sparse=False)
+    with pytest.raises(bls.ArgumentError):
+        bls.reduced_normal_sparse(torch.zeros(4, dtype=torch.float64, device=DEV), torch.zeros(j.schur.nr, dtype=torch.float64, device=DEV),
+                                  out["ws"])
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+def test_lowest_failure(bls, dtype):
+    """A non-finite table and a singular one (zero eliminated columns, no damping): the lowest is reported
+    (test/schur_qr.jl:395-428); free tables are then not copied."""
+    j, o, Rw, Rr, Jf, rf, sc_e = fixture(bls, "bundle adjustment")
+    for spoil in ([(41, "nan"), (17, "zero"), (30, "inf")], [(5, "zero"), (9, "nan")], [(59, "nan")]):
+        W = Rw.copy()
+        for t, how in spoil:
+            M, C = int(j.table_nrows[t]), int(j.table_ncols[t]) - 1
+            T = W[j.raw_offsets[t]:j.raw_offsets[t + 1]].reshape(C, M).T.copy()
+            if how == "zero":
+                T[:, C - 3:] = 0.0
+            else:
+                T[0, 0] = np.nan if how == "nan" else np.inf
+            W[j.raw_offsets[t]:j.raw_offsets[t + 1]] = T.T.ravel()
+        out = run_both(bls, j, o, W, Rr, sc_e, 0.0, dtype)
+        low = min(t for t, _ in spoil) + 1
+        assert not out["ok"] and not out["ook"]
+        assert out["fb"] == out["ofb"] == low
+
+
+def test_argument_errors_write_nothing(bls):
+    j, o, Rw, Rr, Jf, rf, sc_e = fixture(bls, "single eliminated block")
+    ws = bls.QRReductionWorkspace(j, None, torch.float64)
+    J = bls.SchurBlockJacobian(j, torch.float64, data=cu(Rw), r=cu(Rr))
+    ws.factored.fill_(7.0)
+    for bad_sc, lam in ((-sc_e, 0.1), (sc_e, -1.0), (sc_e, float("nan")), (np.full_like(sc_e, np.inf), 0.1)):
+        with pytest.raises(bls.ArgumentError):
+            bls.reduce_qr(ws, J, cu(bad_sc), lam)
+    torch.cuda.synchronize()
+    assert bool((ws.factored == 7.0).all())
+    with pytest.raises(bls.DimensionMismatch):
+        bls.reduce_qr(ws, J, cu(sc_e[:-1]), 0.1)
+    with pytest.raises(bls.ArgumentError):
+        bls.reduce_qr(bls.QRReductionWorkspace(j, None, torch.float32), J, cu(sc_e), 0.1)
+
+
+def _qr_scene(bls):
+    spec = bls.scenes.scaled_down(bls.scenes.workload("qr_500x100k"), ncams=60, npoints=4000)
+    p = bls.scenes.jacobian_problem(spec)
+    sc = bls.scenes.Scene(spec)
+    bs, el, ptr, idx = sc.description()
+    o = orc.QRStructure.from_description(bs, (ptr, idx), np.full(len(ptr) - 1, 2), el)
+    return spec, p, o, (bs, el, ptr, idx)
+
+
+def test_qr_scene_f64(bls):
+    """The QR workload's distributions (point Jacobians with singular values log-uniform in [1e-7, 1], damping rows
+    sqrt(1e-6) I) scaled down to 60 cameras and 4,000 points, FP64: everything within 1e-11 of the oracle."""
+    spec, p, o, _ = _qr_scene(bls)
+    check_close(run_both(bls, p.structure, o, p.Rw, p.Rr, p.scaling_e, p.lam, torch.float64), 1e-11)
+
+
+def test_qr_scene_mixed(bls):
+    """The same scene in the mixed form against the FP64 oracle on the FP32-rounded tables. With singular values down
+    to 1e-7, the third pivot of a table is at FP32 rounding level (~1e-7 against the damping entry 1e-3), so the
+    Householder sign choice (beta = -sign(a) |x|) may differ from the FP64 one: the factored tables are then another
+    valid factorisation, equal in magnitude (|F| within 1e-3) but not entrywise. What is unique is checked tightly:
+    J~'J~ (both forms), J~'r~ and the diagonal blocks within 1e-6 relative, the back-substituted x_e within 1e-4
+    (U's smallest diagonal entries are ~1e-3)."""
+    spec, p, o, _ = _qr_scene(bls)
+    out = run_both(bls, p.structure, o, p.Rw, p.Rr, p.scaling_e, p.lam, torch.float32)
+    check_close(out, {"Sd": 1e-6, "gd": 1e-6, "D": 1e-6, "x_e": 1e-4, "Ss": 1e-6, "gs": 1e-6}, keys=("Sd", "gd", "D", "x_e"))
+    assert relerr(np.abs(out["F"]), np.abs(out["oF"])) <= 1e-3
+
+
+def test_qr_mixed_beats_schur_mixed(bls):
+    """On the ill-conditioned QR scene, the mixed QR path's reduced normal equations are closer to the FP64 ones than
+    the mixed Schur path's (FP32 E = J_p'J_p squares the condition number the QR path works with): at least 10x."""
+    spec, p, o, (bs, el, ptr, idx) = _qr_scene(bls)
+    qr = run_both(bls, p.structure, o, p.Rw, p.Rr, p.scaling_e, p.lam, torch.float32)
+    hp = bls.scenes.hessian_problem(spec)
+    st, pat = hp.structure, hp.pattern
+    ost = orc.Structure.from_description(bs, (ptr, idx), el)
+    opat = orc.Pattern(ost)
+    sc_r, sc_e = np.zeros(st.nr), np.ones(st.ne)     # the QR tables' damping: lambda I on the points only
+    ws = bls.SchurReductionWorkspace(st, pat)
+    S = torch.zeros(pat.nnz, dtype=torch.float32, device=DEV)
+    g = torch.zeros(st.nr, dtype=torch.float64, device=DEV)
+    bls.reset_schur_sparse(S, cu(hp.R, torch.float32), None, None, cu(sc_r), p.lam, ws)
+    assert bls.reduce_schur_sparse(S, g, cu(hp.b_r), cu(hp.b_e), cu(sc_e), p.lam, st, cu(hp.E, torch.float32), cu(hp.C, torch.float32),
+                                   None, None, None, None, ws)
+    oS, og = np.zeros(opat.nnz), np.zeros(st.nr)
+    orc.reset_schur_sparse(ost, opat, oS, hp.R, sc_r, p.lam)
+    assert orc.reduce_schur_sparse(ost, opat, orc.Work(ost, 1), oS, og, hp.b_r, hp.b_e, sc_e, p.lam, hp.E, hp.C)[0]
+    err_schur = relerr(S.double().cpu().numpy(), oS)
+    err_qr = relerr(qr["Ss"], qr["oSs"])
+    assert err_qr * 10 <= err_schur, (err_qr, err_schur)

@@ -30,7 +30,7 @@ def relerr(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-def run_both(bls, st, ost, pat, opat, E, Cd, R, b_r, b_e, sc_r, sc_e, lam, dense, dtype, s_r=None, s_e=None, kernel="columns"):
+def run_both(bls, st, ost, pat, opat, E, Cd, R, b_r, b_e, sc_r, sc_e, lam, dense, dtype, s_r=None, s_e=None, kernel="pairs"):
     """One reset + reduce + back-substitution on the device and in the oracle (FP64, on the same stored values)."""
     npdt = np.float32 if dtype == torch.float32 else np.float64
     E32, C32, R32 = E.astype(npdt), Cd.astype(npdt), R.astype(npdt)
