@@ -235,6 +235,163 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     return out
 
 
+def qr_algorithmic_bytes(jst, dtype_bytes: int) -> float:
+    """Bytes reduce_qr must move: every raw table read and its factored copy written in the storage type, every residual
+    row read and written in FP64, scaling_e read (FP64)."""
+    cells = float(np.sum(jst.table_nrows * (jst.table_ncols - 1)))
+    rows = float(np.sum(jst.table_nrows))
+    return 2 * dtype_bytes * cells + 2 * 8 * rows + 8 * jst.schur.ne
+
+
+def run_ours_qr(args, rank: int, world: int) -> dict | None:
+    """The QR workload: a step is reduce_qr of every table plus reduced_normal_sparse (J~'J~ and J~'r~ on the pattern)."""
+    import torch
+    bls = load_package()
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    spec = bls.scenes.workload(args.workload)
+    if world > 1:
+        from dataclasses import replace
+        spec = replace(spec, seed=spec.seed + 100 * rank)
+    p = bls.scenes.jacobian_problem(spec)
+    jst = p.structure
+    pat = bls.build_schur_pattern(jst.schur, bls.free_block_pairs(jst))
+    flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=dev)
+    sc_e = torch.from_numpy(p.scaling_e).to(dev)
+
+    def setup(dt):
+        ws = bls.QRReductionWorkspace(jst, pat, dt, device=dev.index)
+        J = bls.SchurBlockJacobian(jst, dt, device=dev.index, data=torch.from_numpy(p.Rw).to(device=dev, dtype=dt),
+                                   r=torch.from_numpy(p.Rr).to(dev))
+        S = torch.zeros(pat.nnz, dtype=dt, device=dev)
+        g = torch.zeros(jst.schur.nr, dtype=torch.float64, device=dev)
+        return ws, J, S, g
+
+    def timed(ws, J, S, g):
+        for _ in range(args.warmup):
+            bls.reduce_qr(ws, J, sc_e, p.lam, sync=False)
+            bls.reduced_normal_sparse(S, g, ws, pat)
+        assert ws.query_status(), f"reduce_qr failed at block {ws.failed_block}"
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        ws.launches()
+        evs = []
+        for _ in range(args.steps):
+            flush.zero_()
+            a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a.record()
+            bls.reduce_qr(ws, J, sc_e, p.lam, sync=False)
+            b.record()
+            bls.reduced_normal_sparse(S, g, ws, pat)
+            c.record()
+            evs.append((a, b, c))
+        torch.cuda.synchronize()
+        launches = ws.launches()
+        assert ws.query_status()
+        total = sum(a.elapsed_time(c) for a, b, c in evs)
+        qr_ms = sum(a.elapsed_time(b) for a, b, c in evs) / args.steps
+        if world > 1:
+            t = torch.tensor([total], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            total = float(t.item())
+        return total, qr_ms, launches
+
+    ws32, J32, S32, g32 = setup(torch.float32)
+    with ClockSampler(dev.index) as clk:
+        ms32, qr32, launches = timed(ws32, J32, S32, g32)
+    ws64, J64, S64, g64 = setup(torch.float64)
+    ms64, qr64, _ = timed(ws64, J64, S64, g64)
+    del ws64, J64, S64, g64
+
+    # end to end from pinned host buffers: raw tables (FP32) and residual in, J~'J~ and J~'r~ out
+    hRw = torch.from_numpy(p.Rw.astype(np.float32)).pin_memory()
+    hRr = torch.from_numpy(p.Rr).pin_memory()
+    hS = torch.empty(pat.nnz, dtype=torch.float32).pin_memory()
+    hg = torch.empty(jst.schur.nr, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        J32.data.copy_(hRw, non_blocking=True)
+        J32.r.copy_(hRr, non_blocking=True)
+        bls.reduce_qr(ws32, J32, sc_e, p.lam, sync=False)
+        bls.reduced_normal_sparse(S32, g32, ws32, pat)
+        hS.copy_(S32, non_blocking=True)
+        hg.copy_(g32, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        e2e_step()
+    b.record()
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b)
+    assert ws32.query_status()
+    if rank != 0:
+        return None
+    nobs = p.nobs
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    b32 = qr_algorithmic_bytes(jst, 4)
+    achieved = b32 / (qr32 / 1e3) / 1e9
+    prof = ROOT / "profiles" / "qr_tables_qr_500x100k.json"
+    traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch_f32") if prof.exists() else None
+    out = {
+        "metric": METRIC, "value": world * nobs * args.steps / (ms32 / 1e3), "unit": "obs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 tables + f64 norms, reflector arithmetic, residual", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": args.workload, "cameras": jst.schur.nrblocks, "points": jst.schur.neblocks, "observations": nobs,
+                   "table_entries": int(np.sum(jst.table_nrows * (jst.table_ncols - 1))), "nnz_S": pat.nnz,
+                   "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MB write)",
+                   "step": "reduce_qr + reduced_normal_sparse"},
+        "fp64": {"value": world * nobs * args.steps / (ms64 / 1e3), "unit": "obs/s", "ms_per_step": ms64 / args.steps, "reduce_qr_ms": qr64},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "kernel": "reduce_qr (k_qr_tables<float>)", "kernel_ms": qr32, "algorithmic_bytes": b32,
+                     "peak_source": "measured" if peaks else "fallback"},
+        "e2e": {"value": world * nobs * args.steps / (e2e_ms / 1e3), "unit": "obs/s",
+                "h2d_bytes_per_step": hRw.numel() * 4 + hRr.numel() * 8, "d2h_bytes_per_step": hS.numel() * 4 + hg.numel() * 8},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_qr(spec, seconds=args.cpu_seconds)
+    return out
+
+
+def cpu_baseline_qr(spec, seconds: float = 10.0, steps: int | None = None, warmup: int = 1) -> dict:
+    """The reference algorithm (oracle) on every host core, FP64: reduce_qr threaded over its chunks, then
+    reduced_normal_sparse threaded over retained block columns, as the reference threads them."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    bls = load_package()
+    cores = os.cpu_count() or 1
+    p = bls.scenes.jacobian_problem(spec)
+    sc = bls.scenes.Scene(spec)
+    bs, el, ptr, idx = sc.description()
+    o = orc.QRStructure.from_description(bs, (ptr, idx), np.full(len(ptr) - 1, 2), el, nchunks=cores)
+    opat = orc.Pattern(o.st)
+    F, Fr = np.zeros(o.raw_length), np.zeros(o.residual_length)
+    S, g = np.zeros(opat.nnz), np.zeros(o.st.nr)
+
+    def one():
+        ok, _ = orc.reduce_qr(o, F, Fr, p.Rw, p.Rr, p.scaling_e, p.lam, nthreads=cores)
+        assert ok
+        orc.reduced_normal_sparse(o, opat, S, g, F, Fr)
+
+    for _ in range(warmup):
+        one()
+    n, t0 = 0, time.perf_counter()
+    while (steps is None and (time.perf_counter() - t0 < seconds or n < 3)) or (steps is not None and n < steps):
+        one()
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": p.nobs * n / dt, "unit": "obs/s", "cores": cores, "kind": "port",
+            "sample": f"{n} x full reduce_qr + reduced_normal_sparse of {spec.npoints} points / {p.nobs} observations, FP64, "
+                      f"{cores} OpenMP threads ({dt:.1f} s)"}
+
+
 def oracle_problem(spec):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
@@ -277,6 +434,14 @@ def run_reference(args, rank: int, world: int) -> dict | None:
         return None
     bls = load_package()
     spec = bls.scenes.workload(args.workload)
+    if args.workload.startswith("qr_"):
+        base = cpu_baseline_qr(spec, steps=args.steps, warmup=args.warmup)
+        return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "obs/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded scene generator)",
+                "config": {"workload": args.workload, "step": "reduce_qr + reduced_normal_sparse",
+                           "note": "reference algorithm restated in C++ (Julia is unavailable)"},
+                "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "obs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     base = cpu_baseline(None, spec, steps=args.steps, warmup=args.warmup)
     return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "obs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -305,7 +470,12 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        out = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world)
+        if args.impl == "reference":
+            out = run_reference(args, rank, world)
+        elif args.workload.startswith("qr_"):
+            out = run_ours_qr(args, rank, world)
+        else:
+            out = run_ours(args, rank, world)
     finally:
         if world > 1 and args.impl == "ours":
             import torch

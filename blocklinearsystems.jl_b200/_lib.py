@@ -103,6 +103,8 @@ def gpu() -> C.CDLL:
             "bls_qr_plan_destroy": (C.c_int, [vp]),
             "bls_reduce_qr": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, p64]),
             "bls_qr_backsubstitute": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+            "bls_qr_query_status": (C.c_int, [vp, p64]),
+            "bls_qr_plan_counters": (i64, [vp]),
             "bls_reduced_normal_sparse": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_reduced_normal_dense": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_reduced_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, vp]),

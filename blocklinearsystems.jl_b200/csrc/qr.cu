@@ -12,6 +12,12 @@
 // M = m_e + d_e is odd whenever m_e is even, so the lanes' column strides hit distinct shared-memory banks). The
 // residual column goes through the same reflectors in FP64 (SP-B6 of the reference). With FP32 storage (the mixed
 // form) the table is FP32 and each reflector application is accumulated in FP64 and rounded once per entry.
+//
+// J~'J~, J~'r~ and the diagonal blocks come from one warp per table as well: the table's bottom rows (J~ of its
+// retained columns) and residual rows are staged in shared memory, every pair of the table's entries (u1 <= u2)
+// gives one d_r x d_r block, one lane per block column holding its FP64 dot products in registers, and the block is
+// added into S with one atomic add per entry (a table contributes to each S block at most once). Tables are grouped into shared-memory classes;
+// each class is one launch of up to four warps per CTA.
 #include <algorithm>
 #include <climits>
 #include <cstring>
@@ -24,26 +30,27 @@
 namespace bls {
 
 constexpr long long QNONE = LLONG_MAX;
-constexpr int QR_PAIR_CHUNK = 32;
+constexpr int QR_MAX_WARPS = 4;
+constexpr int64_t QR_SMEM_LIMIT = 220 * 1024;
 
 struct QRPlan {
   bls_ctx* ctx = nullptr;
   int64_t nrblocks = 0, neblocks = 0, ntables = 0, nentries = 0, nr = 0, ne = 0, raw_len = 0, res_len = 0;
-  int64_t max_cells = 0, max_rows = 0, nblocks = 0, nitems = 0, nnzS = 0;
+  int64_t max_rows = 0, nblocks = 0, nnzS = 0, ndiag = 0;
   bool has_sparse = false;
   int max_dr = 0;
   // device: per table, per entry, per retained / eliminated block
   DevBuf t_rows, t_cols, t_top, t_raw, t_res, t_ptr, e_dims, boff_e;
   DevBuf u_ret, u_col, r_dims, boff_r, doff;
-  // eliminated tables by shared-memory class (bytes of the staged table and residual, per element type)
+  // tables by shared-memory class (bytes of what one warp stages, per element type): the eliminated tables for the
+  // factorisation, every table for the Gram kernel
   struct TableClass {
     DevBuf tables;
     int64_t n = 0, bytes_f64 = 0, bytes_f32 = 0;
   };
-  TableClass classes[8];
-  // J~'J~ work items (pairs of entries of one table, per S block)
-  DevBuf pair_u1, pair_u2, item_block, item_start, item_info, blk_r1, blk_r2, blk_base_sparse, blk_stride, blk_base_dense;
-  DevBuf r_ptr, r_entry, u_table;
+  TableClass classes[8], gram_classes[8];
+  // per table, per pair (u1 <= u2) of its entries in the order u2 outer, u1 inner: the S block it adds to
+  DevBuf tp_ptr, tp_blk, blk_base_sparse, blk_stride, blk_base_dense;
   DevBuf status;
   long long* host_status = nullptr;
   int64_t launches = 0;
@@ -58,6 +65,25 @@ static std::vector<int32_t> q32(const int64_t* a, int64_t n, const char* what) {
   }
   return v;
 }
+
+// Warps per CTA for a per-warp shared-memory footprint: up to QR_MAX_WARPS within the shared-memory limit.
+static int warps_per_cta(int64_t warp_bytes) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>(QR_MAX_WARPS, QR_SMEM_LIMIT / std::max<int64_t>(warp_bytes, 1)));
+}
+
+static void set_smem(const void* kernel, size_t bytes) {
+  if (bytes > 48 * 1024) BLS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// Asynchronous global -> shared copies of one element (cp.async, completed by cp_async_wait_all): a lane issues all of
+// its copies back to back, so a table's loads are in flight together instead of one DRAM latency per element.
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // status: [0] lowest failing table, [1] lowest bad scaling_e entry
 __global__ void k_qr_begin(long long* st) { st[0] = QNONE; st[1] = QNONE; }
@@ -92,7 +118,8 @@ __device__ __forceinline__ double col_scale(const double* s, int j, int t, int n
 // qr_table! for the listed eliminated tables, one warp per table; `shT` holds the table (M x C, column-major) and
 // the FP64 residual (M). Tables are assigned by `tables[blockIdx.x * warps + warp]`.
 template <class T>
-__global__ void __launch_bounds__(32) k_qr_tables(int64_t ntab, const int32_t* __restrict__ tables, const int32_t* __restrict__ t_rows,
+__global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, int warp_bytes, const int32_t* __restrict__ tables,
+                                                  const int32_t* __restrict__ t_rows,
                                                   const int32_t* __restrict__ t_cols, const int64_t* __restrict__ t_raw,
                                                   const int64_t* __restrict__ t_res, const int32_t* __restrict__ t_ptr,
                                                   const int32_t* __restrict__ u_col, const int32_t* __restrict__ u_ret,
@@ -101,29 +128,32 @@ __global__ void __launch_bounds__(32) k_qr_tables(int64_t ntab, const int32_t* _
                                                   const T* __restrict__ Rw, const double* __restrict__ Rr, const double* __restrict__ sc_e,
                                                   double lambda, const double* __restrict__ s, T* __restrict__ F, double* __restrict__ Fr,
                                                   long long* st) {
-  extern __shared__ __align__(16) unsigned char qsm[];
-  const int64_t wi = blockIdx.x;
+  extern __shared__ __align__(16) unsigned char qsm_all[];
+  const int64_t wi = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
   if (wi >= ntab) return;
   if (st[1] != QNONE) return;
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  unsigned char* qsm = qsm_all + (size_t)(threadIdx.x >> 5) * warp_bytes;
   const int t = tables[wi];
   const int M = t_rows[t], C = t_cols[t] - 1, de = e_dims[t], me = M - de, ce = C - de;
   const int64_t off = t_raw[t], rq = t_res[t];
   double* res = reinterpret_cast<double*>(qsm);
   T* A = reinterpret_cast<T*>(qsm + sizeof(double) * ((M + 1) & ~1));
-  // copy in (coalesced: the table is contiguous), with the reference's non-finite test (x - x is NaN for Inf / NaN)
+  // copy in (coalesced: the table is contiguous; all of a lane's copies in flight at once), then the reference's
+  // non-finite test (x - x is NaN for Inf / NaN) and the conditioning scales, in shared memory
+  for (int i = lane; i < M * C; i += 32) cp_async_elem(A + i, Rw + off + i);
+  for (int i = lane; i < M; i += 32) cp_async_elem(res + i, Rr + rq + i);
+  cp_async_wait_all();
+  __syncwarp();
   bool bad = false;
   for (int i = lane; i < M * C; i += 32) {
-    const int j = i / M;
-    T x = Rw[off + i];
+    T x = A[i];
     bad |= isnan((double)(x - x));
-    if (s) x = T((double)x * col_scale(s, j, t, C, de, t_ptr, u_col, u_ret, boff_r, r_dims, boff_e, nr));
-    A[i] = x;
+    if (s) A[i] = T((double)x * col_scale(s, i / M, t, C, de, t_ptr, u_col, u_ret, boff_r, r_dims, boff_e, nr));
   }
   for (int i = lane; i < M; i += 32) {
-    const double x = Rr[rq + i];
+    const double x = res[i];
     bad |= isnan(x - x);
-    res[i] = x;
   }
   bad = __any_sync(0xffffffffu, bad);
   if (bad) {
@@ -172,8 +202,17 @@ __global__ void __launch_bounds__(32) k_qr_tables(int64_t ntab, const int32_t* _
     for (int j = lane; j < C; j += 32) {
       if (j >= ce && j <= ce + k) continue;
       T* y = A + j * M;
-      double sj = (double)y[k];
-      for (int i = k + 1; i < M; ++i) sj += (double)col[i] * (double)y[i];
+      // v'y in four independent partial sums (the FMA chain is the latency of this loop)
+      double p0 = (double)y[k], p1 = 0.0, p2 = 0.0, p3 = 0.0;
+      int i = k + 1;
+      for (; i + 3 < M; i += 4) {
+        p0 += (double)col[i] * (double)y[i];
+        p1 += (double)col[i + 1] * (double)y[i + 1];
+        p2 += (double)col[i + 2] * (double)y[i + 2];
+        p3 += (double)col[i + 3] * (double)y[i + 3];
+      }
+      for (; i < M; ++i) p0 += (double)col[i] * (double)y[i];
+      double sj = (p0 + p1) + (p2 + p3);
       sj *= tau;
       y[k] = T((double)y[k] - sj);
       for (int i = k + 1; i < M; ++i) y[i] = T((double)y[i] - sj * (double)col[i]);
@@ -214,93 +253,117 @@ __global__ void k_qr_free(int64_t t0, int64_t nt, const int32_t* __restrict__ t_
   for (int i = threadIdx.x; i < M; i += blockDim.x) Fr[rq + i] = Rr[rq + i];
 }
 
-// J~'J~ and J~'r~ (accumulate_qr_entry!): six threads per work item (pairs (u1, u2) of one table with u1 <= u2, all of
-// one S block), thread w owning column w of the block: sum over the pairs of the dots of the bottom n = M - top rows.
-template <class T>
-__global__ void __launch_bounds__(128) k_qr_pairs(int64_t nitems, const int32_t* __restrict__ item_block, const int32_t* __restrict__ item_start,
-                                                  const int32_t* __restrict__ item_info, const int32_t* __restrict__ pair_u1,
-                                                  const int32_t* __restrict__ pair_u2, const int32_t* __restrict__ blk_r1,
-                                                  const int32_t* __restrict__ blk_r2, const int64_t* __restrict__ blk_base,
-                                                  const int32_t* __restrict__ blk_stride, int64_t dense_nr, const int32_t* __restrict__ u_table,
-                                                  const int32_t* __restrict__ u_col, const int32_t* __restrict__ t_rows,
-                                                  const int32_t* __restrict__ t_top, const int64_t* __restrict__ t_raw,
-                                                  const int64_t* __restrict__ t_res, const int32_t* __restrict__ r_dims,
-                                                  const int32_t* __restrict__ boff_r, const T* __restrict__ F, const double* __restrict__ Fr,
-                                                  T* __restrict__ S, double* __restrict__ g) {
+// accumulate_qr_entry! (src/qr_reduced.jl:375-405) per table. MODE 0: S blocks (upper triangle of diagonal blocks) and
+// J~'r~ into g; MODE 1: the full diagonal blocks D (reduced_diagonal_blocks!, :484-512).
+template <class T, int MODE>
+__global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int warp_bytes, const int32_t* __restrict__ tables,
+                                                              const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_cols,
+                                                              const int32_t* __restrict__ t_top, const int64_t* __restrict__ t_raw,
+                                                              const int64_t* __restrict__ t_res, const int32_t* __restrict__ t_ptr,
+                                                              const int32_t* __restrict__ u_ret, const int32_t* __restrict__ u_col,
+                                                              const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                                                              const int32_t* __restrict__ tp_ptr, const int32_t* __restrict__ tp_blk,
+                                                              const int64_t* __restrict__ blk_base, const int32_t* __restrict__ blk_stride,
+                                                              int64_t dense_nr, const int64_t* __restrict__ doff, int dmax, const T* __restrict__ F,
+                                                              const double* __restrict__ Fr, T* __restrict__ S, double* __restrict__ g) {
+  extern __shared__ __align__(16) unsigned char gsm_all[];
+  const int64_t wi = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (wi >= ntab) return;
   const int lane = threadIdx.x & 31;
-  if (lane >= 30) return;
-  const int64_t it = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 5 + lane / 6;
-  if (it >= nitems) return;
-  const int k = item_block[it], pb = item_start[it], info = item_info[it];
-  const int pe = pb + (info & 0xffff);
-  const bool solo = (info >> 16) != 0;
-  const int r1 = blk_r1[k], r2 = blk_r2[k];
-  const bool diag = r1 == r2;
-  const int d1 = r_dims[r1], d2 = r_dims[r2];
-  const int64_t stride = blk_stride ? (int64_t)blk_stride[k] : dense_nr;
-  for (int w = lane % 6; w < d2; w += 6) {
-    double acc[16];
+  unsigned char* gsm = gsm_all + (size_t)(threadIdx.x >> 5) * warp_bytes;
+  const int t = tables[wi];
+  const int M = t_rows[t], top = t_top[t], n = M - top, ce = t_cols[t] - 1 - top, ns = n | 1;
+  const int u0 = t_ptr[t], kt = t_ptr[t + 1] - u0;
+  double* rr = reinterpret_cast<double*>(gsm);
+  T* B = reinterpret_cast<T*>(gsm + sizeof(double) * ((n + 1) & ~1));
+  const T* src = F + t_raw[t] + top;
+  for (int q = lane; q < ce * n; q += 32) {
+    const int j = q / n, i = q - j * n;
+    cp_async_elem(B + j * ns + i, src + (int64_t)j * M + i);
+  }
+  if (MODE == 0)
+    for (int i = lane; i < n; i += 32) cp_async_elem(rr + i, Fr + t_res[t] + top + i);
+  cp_async_wait_all();
+  __syncwarp();
+  if (MODE == 0) {
+    // J~'r~: lane per column, entry found by scanning the table's entries
+    for (int j = lane; j < ce; j += 32) {
+      int gi = 0;
+      for (int u = u0; u < u0 + kt; ++u) {
+        const int c0 = u_col[u], r = u_ret[u];
+        if (j >= c0 && j < c0 + r_dims[r]) gi = boff_r[r] + (j - c0);
+      }
+      double acc = 0.0;
+      for (int i = 0; i < n; ++i) acc += (double)B[j * ns + i] * rr[i];
+      atomicAdd(g + gi, acc);
+    }
+  }
+  // work units: (pair, a group of three columns of the pair's block); lanes take units in order, so the lanes of one
+  // pair read the same X rows (shared-memory broadcast)
+  const int npairs = kt * (kt + 1) / 2;
+  const int upp = (dmax + 2) / 3;
+  for (int q = lane; q < npairs * upp; q += 32) {
+    const int p = q / upp, w0 = 3 * (q - p * upp);
+    int u2l = (int)((sqrtf(8.0f * p + 1.0f) - 1.0f) * 0.5f);
+    while ((u2l + 1) * (u2l + 2) / 2 <= p) ++u2l;
+    while (u2l * (u2l + 1) / 2 > p) --u2l;
+    const int u1l = p - u2l * (u2l + 1) / 2;
+    const bool diag = u1l == u2l;
+    if (MODE == 1 && !diag) continue;
+    const int r1 = u_ret[u0 + u1l], r2 = u_ret[u0 + u2l];
+    const int d1 = r_dims[r1], d2 = r_dims[r2];
+    if (w0 >= d2) continue;
+    const T* X = B + u_col[u0 + u1l] * ns;
+    const T* Y = B + (u_col[u0 + u2l] + w0) * ns;
+    T* out;
+    int64_t stride;
+    if (MODE == 0) {
+      const int k = tp_blk[tp_ptr[t] + p];
+      stride = blk_stride ? (int64_t)blk_stride[k] : dense_nr;
+      out = S + blk_base[k] + w0 * stride;
+    } else {
+      stride = d2;
+      out = S + doff[r2] + w0 * d2;
+    }
+    if (d1 == 6 && d2 == 6) {
+      double acc[3][6];
 #pragma unroll
-    for (int a = 0; a < 16; ++a) acc[a] = 0.0;
-    double gacc = 0.0;
-    for (int p = pb; p < pe; ++p) {
-      const int u1 = pair_u1[p], u2 = pair_u2[p], t = u_table[u2];
-      const int M = t_rows[t], top = t_top[t], n = M - top;
-      const T* base = F + t_raw[t] + top;
-      const T* yw = base + (int64_t)(u_col[u2] + w) * M;
-      const T* x0 = base + (int64_t)u_col[u1] * M;
-      const double* rr = Fr + t_res[t] + top;
+      for (int w = 0; w < 3; ++w)
+#pragma unroll
+        for (int a = 0; a < 6; ++a) acc[w][a] = 0.0;
       for (int i = 0; i < n; ++i) {
-        const double yv = (double)yw[i];
+        double x[6], y[3];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) x[a] = (double)X[a * ns + i];
+#pragma unroll
+        for (int w = 0; w < 3; ++w) y[w] = (double)Y[w * ns + i];
+#pragma unroll
+        for (int w = 0; w < 3; ++w)
+#pragma unroll
+          for (int a = 0; a < 6; ++a) acc[w][a] += x[a] * y[w];
+      }
+#pragma unroll
+      for (int w = 0; w < 3; ++w)
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+          if (MODE == 1 || !diag || a <= w0 + w) atomicAdd(out + w * stride + a, T(acc[w][a]));
+    } else {
+      for (int w = w0; w < d2 && w < w0 + 3; ++w) {
+        double acc[16];
+#pragma unroll
+        for (int a = 0; a < 16; ++a) acc[a] = 0.0;
+        for (int i = 0; i < n; ++i) {
+          const double y = (double)Y[(w - w0) * ns + i];
+#pragma unroll
+          for (int a = 0; a < 16; ++a)
+            if (a < d1) acc[a] += (double)X[a * ns + i] * y;
+        }
 #pragma unroll
         for (int a = 0; a < 16; ++a)
-          if (a < d1) acc[a] += (double)x0[(int64_t)a * M + i] * yv;
-        if (diag) gacc += yv * rr[i];
+          if (a < d1 && (MODE == 1 || !diag || a <= w)) atomicAdd(out + (w - w0) * stride + a, T(acc[a]));
       }
     }
-    T* colp = S + blk_base[k] + w * stride;
-#pragma unroll
-    for (int a = 0; a < 16; ++a) {
-      if (a >= d1 || (diag && a > w)) continue;
-      if (solo) colp[a] = T((double)colp[a] + acc[a]);
-      else atomicAdd(colp + a, T(acc[a]));
-    }
-    if (diag) {
-      if (solo) g[boff_r[r2] + w] += gacc;
-      else atomicAdd(g + boff_r[r2] + w, gacc);
-    }
   }
-}
-
-// reduced_diagonal_blocks!: thread (r, w) sums column w of J~_u' J~_u over the entries u of retained block r
-template <class T>
-__global__ void k_qr_diag(int64_t nrb, const int32_t* __restrict__ r_ptr, const int32_t* __restrict__ r_entry, const int32_t* __restrict__ u_table,
-                          const int32_t* __restrict__ u_col, const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
-                          const int64_t* __restrict__ t_raw, const int32_t* __restrict__ r_dims, const int64_t* __restrict__ doff,
-                          const T* __restrict__ F, T* __restrict__ D) {
-  const int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t r = id >> 4;
-  const int w = (int)(id & 15);
-  if (r >= nrb) return;
-  const int dr = r_dims[r];
-  if (w >= dr) return;
-  double acc[16];
-#pragma unroll
-  for (int a = 0; a < 16; ++a) acc[a] = 0.0;
-  for (int q = r_ptr[r]; q < r_ptr[r + 1]; ++q) {
-    const int u = r_entry[q], t = u_table[u];
-    const int M = t_rows[t], top = t_top[t];
-    const T* base = F + t_raw[t] + top + (int64_t)u_col[u] * M;
-    for (int i = 0; i < M - top; ++i) {
-      const double yv = (double)base[(int64_t)w * M + i];
-#pragma unroll
-      for (int a = 0; a < 16; ++a)
-        if (a < dr) acc[a] += (double)base[(int64_t)a * M + i] * yv;
-    }
-  }
-#pragma unroll
-  for (int a = 0; a < 16; ++a)
-    if (a < dr) D[doff[r] + (int64_t)w * dr + a] = T(acc[a]);
 }
 
 // qr_backsubstitute_group! (src/qr_reduced.jl:24-93): thread per eliminated table, FP64
@@ -362,6 +425,7 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
     boff_e[e] = ne; ne += d->e_dims[e];
   }
   P->nr = nr; P->ne = ne;
+  P->ndiag = doff[nrb];
   // tables: consistency checks that keep every device access inside the caller's buffers
   for (int64_t t = 0; t < nt; ++t) {
     const int64_t M = d->table_nrows[t], C = d->table_ncols[t] - 1;
@@ -380,27 +444,32 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
   }
   P->raw_len = d->raw_offsets[nt];
   P->res_len = d->residual_offsets[nt];
-  // shared-memory classes of the eliminated tables by their FP64 footprint (residual rounded to an even row count, then
-  // the M x C table): <= 2, 4, 8, 16, 32, 64, 128, 224 KB
-  std::vector<int32_t> cls_tables[8];
-  for (int64_t t = 0; t < neb; ++t) {
-    const int64_t M = d->table_nrows[t], C = d->table_ncols[t] - 1;
-    const int64_t b64 = 8 * ((M + 1) & ~1) + 8 * M * C, b32 = 8 * ((M + 1) & ~1) + 4 * M * C;
+  // shared-memory classes by FP64 footprint (<= 2, 4, 8, 16, 32, 64, 128, 220 KB). Factorisation (eliminated tables):
+  // the residual (rounded to an even row count) and the M x C table. Gram kernel (every table): the n = M - top residual
+  // rows and the n bottom rows of the ce retained columns at an odd column stride.
+  std::vector<int32_t> cls_tables[8], gram_tables[8];
+  auto cls_of = [](int64_t b64) {
     int c = 0;
     while (c < 7 && b64 > (int64_t(2048) << c)) ++c;
-    if (b64 > 224 * 1024) throw Error(BLS_EUNSUPPORTED, "table " + std::to_string(t + 1) + " exceeds the shared-memory capacity of this build");
-    cls_tables[c].push_back((int32_t)t);
-    P->classes[c].bytes_f64 = std::max(P->classes[c].bytes_f64, b64);
-    P->classes[c].bytes_f32 = std::max(P->classes[c].bytes_f32, b32);
-  }
-  // per entry: table; per retained block: its entries (ascending)
-  std::vector<int32_t> u_table(nent), rptr(nrb + 1, 0), rentry(nent);
-  for (int64_t t = 0; t < nt; ++t)
-    for (int64_t u = d->table_ptr[t]; u < d->table_ptr[t + 1]; ++u) { u_table[u] = (int32_t)t; rptr[d->entry_retained[u] + 1] += 1; }
-  for (int64_t r = 0; r < nrb; ++r) rptr[r + 1] += rptr[r];
-  {
-    std::vector<int32_t> fill(rptr.begin(), rptr.end() - 1);
-    for (int64_t u = 0; u < nent; ++u) rentry[fill[d->entry_retained[u]]++] = (int32_t)u;
+    return c;
+  };
+  for (int64_t t = 0; t < nt; ++t) {
+    const int64_t M = d->table_nrows[t], C = d->table_ncols[t] - 1, top = d->table_top[t];
+    if (t < neb) {
+      const int64_t b64 = 8 * ((M + 1) & ~1) + 8 * M * C, b32 = 8 * ((M + 1) & ~1) + 4 * M * C;
+      if (b64 > QR_SMEM_LIMIT) throw Error(BLS_EUNSUPPORTED, "table " + std::to_string(t + 1) + " exceeds the shared-memory capacity of this build");
+      const int c = cls_of(b64);
+      cls_tables[c].push_back((int32_t)t);
+      P->classes[c].bytes_f64 = std::max(P->classes[c].bytes_f64, b64);
+      P->classes[c].bytes_f32 = std::max(P->classes[c].bytes_f32, b32);
+    }
+    const int64_t n = M - top, ce = C - top, ns = n | 1;
+    const int64_t g64 = 8 * ((n + 1) & ~1) + 8 * ce * ns, g32 = 8 * ((n + 1) & ~1) + 4 * ce * ns;
+    if (g64 > QR_SMEM_LIMIT) throw Error(BLS_EUNSUPPORTED, "table " + std::to_string(t + 1) + " exceeds the shared-memory capacity of this build");
+    const int c = cls_of(g64);
+    gram_tables[c].push_back((int32_t)t);
+    P->gram_classes[c].bytes_f64 = std::max(P->gram_classes[c].bytes_f64, g64);
+    P->gram_classes[c].bytes_f32 = std::max(P->gram_classes[c].bytes_f32, g32);
   }
   // J~'J~ blocks: the given pattern, or the tables' own block pattern
   std::vector<int64_t> bcolptr, browval, brow_off, col_h, Scolptr;
@@ -438,44 +507,32 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
   }
   const int64_t nb = bcolptr[nrb];
   P->nblocks = nb;
-  std::vector<int32_t> b_r1(nb), b_r2(nb), b_stride(nb);
+  std::vector<int32_t> b_stride(nb);
   std::vector<int64_t> b_base(nb, 0), b_base_dense(nb);
   for (int64_t r2 = 0; r2 < nrb; ++r2)
     for (int64_t k = bcolptr[r2]; k < bcolptr[r2 + 1]; ++k) {
-      b_r1[k] = (int32_t)browval[k];
-      b_r2[k] = (int32_t)r2;
       b_stride[k] = (int32_t)col_h[r2];
       if (P->has_sparse) b_base[k] = Scolptr[boff_r[r2]] + brow_off[k];
       b_base_dense[k] = boff_r[browval[k]] + boff_r[r2] * nr;
     }
-  // pairs (u1, u2), u1 <= u2 of one table, per block (r1, r2), in ascending table order
-  std::vector<int32_t> pu1, pu2, itb, its, iti;
-  for (int64_t r2 = 0; r2 < nrb; ++r2) {
-    const int64_t kb = bcolptr[r2], ke = bcolptr[r2 + 1];
-    std::vector<std::vector<std::pair<int32_t, int32_t>>> per(ke - kb);
-    for (int32_t q = rptr[r2]; q < rptr[r2 + 1]; ++q) {
-      const int32_t u2 = rentry[q];
-      const int64_t t = u_table[u2];
-      for (int64_t u1 = d->table_ptr[t]; u1 <= u2; ++u1) {
-        const int64_t r1 = d->entry_retained[u1];
+  // per table, its entry pairs (u2 outer, u1 <= u2 inner) and the S block (r1, r2) each adds to
+  std::vector<int32_t> tp_ptr(nt + 1, 0), tp_blk;
+  for (int64_t t = 0; t < nt; ++t) {
+    const int64_t u0 = d->table_ptr[t], kt = d->table_ptr[t + 1] - u0;
+    for (int64_t b = 1; b < kt; ++b)
+      if (d->entry_retained[u0 + b] <= d->entry_retained[u0 + b - 1]) throw Error(BLS_EINVAL, "table " + std::to_string(t + 1) + ": entries must be in ascending retained order");
+    for (int64_t a2 = 0; a2 < kt; ++a2) {
+      const int64_t r2 = d->entry_retained[u0 + a2], kb = bcolptr[r2], ke = bcolptr[r2 + 1];
+      for (int64_t a1 = 0; a1 <= a2; ++a1) {
+        const int64_t r1 = d->entry_retained[u0 + a1];
         const int64_t* f = std::lower_bound(browval.data() + kb, browval.data() + ke, r1);
         if (f == browval.data() + ke || *f != r1) throw Error(BLS_EPATTERN, "The sparse pattern has no block (" + std::to_string(r1 + 1) + ", " + std::to_string(r2 + 1) + ")");
-        per[f - (browval.data() + kb)].push_back({(int32_t)u1, u2});
+        tp_blk.push_back((int32_t)(f - browval.data()));
       }
     }
-    for (int64_t sl = 0; sl < ke - kb; ++sl) {
-      const auto& v = per[sl];
-      const int nch = ((int)v.size() + QR_PAIR_CHUNK - 1) / QR_PAIR_CHUNK;
-      for (size_t x = 0; x < v.size(); x += QR_PAIR_CHUNK) {
-        itb.push_back((int32_t)(kb + sl));
-        its.push_back((int32_t)pu1.size() + 0);
-        const int cnt = (int)std::min<size_t>(QR_PAIR_CHUNK, v.size() - x);
-        iti.push_back(cnt | ((nch == 1 ? 1 : 0) << 16));
-        for (int y = 0; y < cnt; ++y) { pu1.push_back(v[x + y].first); pu2.push_back(v[x + y].second); }
-      }
-    }
+    if (tp_blk.size() > (size_t)INT32_MAX) throw Error(BLS_EUNSUPPORTED, "too many entry pairs for this build");
+    tp_ptr[t + 1] = (int32_t)tp_blk.size();
   }
-  P->nitems = (int64_t)itb.size();
   std::vector<int32_t> t_rows = q32(d->table_nrows, nt, "table_nrows"), t_cols = q32(d->table_ncols, nt, "table_ncols"),
                        t_top = q32(d->table_top, nt, "table_top"), t_ptr = q32(d->table_ptr, nt + 1, "table_ptr");
   upload(P->t_rows, t_rows, s); upload(P->t_cols, t_cols, s); upload(P->t_top, t_top, s); upload(P->t_ptr, t_ptr, s);
@@ -491,14 +548,14 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
   for (int c = 0; c < 8; ++c) {
     P->classes[c].n = (int64_t)cls_tables[c].size();
     upload(P->classes[c].tables, cls_tables[c], s);
+    P->gram_classes[c].n = (int64_t)gram_tables[c].size();
+    upload(P->gram_classes[c].tables, gram_tables[c], s);
   }
-  upload(P->u_table, u_table, s);
-  upload(P->r_ptr, rptr, s);
-  upload(P->r_entry, rentry, s);
-  upload(P->pair_u1, pu1, s); upload(P->pair_u2, pu2, s);
-  upload(P->item_block, itb, s); upload(P->item_start, its, s); upload(P->item_info, iti, s);
-  upload(P->blk_r1, b_r1, s); upload(P->blk_r2, b_r2, s); upload(P->blk_stride, b_stride, s);
-  upload(P->blk_base_sparse, b_base, s); upload(P->blk_base_dense, b_base_dense, s);
+  upload(P->tp_ptr, tp_ptr, s);
+  upload(P->tp_blk, tp_blk, s);
+  upload(P->blk_stride, b_stride, s);
+  upload(P->blk_base_sparse, b_base, s);
+  upload(P->blk_base_dense, b_base_dense, s);
   P->status.alloc(4 * sizeof(long long));
   long long init[4] = {QNONE, QNONE, QNONE, QNONE};
   BLS_CUDA(cudaMemcpyAsync(P->status.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
@@ -507,38 +564,10 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
   return P.release();
 }
 
-template <class T>
-static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr, const double* sc_e, double lambda, const double* sv,
-                     int64_t* failed_block) {
-  if (!(std::isfinite(lambda) && lambda >= 0)) throw Error(BLS_EINVAL, "lambda must be finite and non-negative, got " + std::to_string(lambda));
+// The verdict of the last reduce_qr (synchronises on the plan's stream)
+static int qr_status(QRPlan* P, int64_t* failed_block) {
   cudaStream_t s = P->ctx->stream;
-  long long* st = P->status.as<long long>();
-  k_qr_begin<<<1, 1, 0, s>>>(st);
-  k_qr_check<<<grid_for(P->ne, 256), 256, 0, s>>>(sc_e, P->ne, st);
-  P->launches += 2;
-  for (int c = 0; c < 8; ++c) {
-    const auto& k = P->classes[c];
-    if (k.n == 0) continue;
-    const size_t smem = (size_t)(std::is_same<T, double>::value ? k.bytes_f64 : k.bytes_f32);
-    if (smem > 48 * 1024) BLS_CUDA(cudaFuncSetAttribute(k_qr_tables<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_qr_tables<T><<<(unsigned)k.n, 32, smem, s>>>(k.n, k.tables.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(),
-                                                   P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(),
-                                                   P->u_ret.as<int32_t>(), P->boff_r.as<int32_t>(), P->r_dims.as<int32_t>(),
-                                                   P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), (int)P->nr, Rw, Rr, sc_e, lambda, sv, F,
-                                                   Fr, st);
-    P->launches += 1;
-  }
-  if (P->ntables > P->neblocks) {
-    k_qr_free<T><<<(unsigned)(P->ntables - P->neblocks), 128, 0, s>>>(P->neblocks, P->ntables, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(),
-                                                                       P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(),
-                                                                       P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->boff_r.as<int32_t>(),
-                                                                       P->r_dims.as<int32_t>(), P->boff_e.as<int32_t>(), (int)P->nr, Rw, Rr, sv,
-                                                                       F, Fr, st);
-    P->launches += 1;
-  }
-  BLS_CUDA(cudaGetLastError());
-  if (!failed_block) return BLS_OK;
-  BLS_CUDA(cudaMemcpyAsync(P->host_status, st, 2 * sizeof(long long), cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaMemcpyAsync(P->host_status, P->status.p, 2 * sizeof(long long), cudaMemcpyDeviceToHost, s));
   BLS_CUDA(cudaStreamSynchronize(s));
   *failed_block = 0;
   if (P->host_status[1] != QNONE) {
@@ -553,21 +582,80 @@ static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr,
 }
 
 template <class T>
+static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr, const double* sc_e, double lambda, const double* sv,
+                     int64_t* failed_block) {
+  if (!(std::isfinite(lambda) && lambda >= 0)) throw Error(BLS_EINVAL, "lambda must be finite and non-negative, got " + std::to_string(lambda));
+  cudaStream_t s = P->ctx->stream;
+  long long* st = P->status.as<long long>();
+  k_qr_begin<<<1, 1, 0, s>>>(st);
+  k_qr_check<<<grid_for(P->ne, 256), 256, 0, s>>>(sc_e, P->ne, st);
+  P->launches += 2;
+  for (int c = 0; c < 8; ++c) {
+    const auto& k = P->classes[c];
+    if (k.n == 0) continue;
+    const int64_t wb = ((std::is_same<T, double>::value ? k.bytes_f64 : k.bytes_f32) + 15) & ~int64_t(15);
+    const int wpc = warps_per_cta(wb);
+    const size_t smem = (size_t)(wb * wpc);
+    set_smem(reinterpret_cast<const void*>(k_qr_tables<T>), smem);
+    k_qr_tables<T><<<(unsigned)((k.n + wpc - 1) / wpc), 32 * wpc, smem, s>>>(
+        k.n, (int)wb, k.tables.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(),
+        P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->boff_r.as<int32_t>(), P->r_dims.as<int32_t>(),
+        P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), (int)P->nr, Rw, Rr, sc_e, lambda, sv, F, Fr, st);
+    P->launches += 1;
+  }
+  if (P->ntables > P->neblocks) {
+    k_qr_free<T><<<(unsigned)(P->ntables - P->neblocks), 128, 0, s>>>(P->neblocks, P->ntables, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(),
+                                                                       P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(),
+                                                                       P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->boff_r.as<int32_t>(),
+                                                                       P->r_dims.as<int32_t>(), P->boff_e.as<int32_t>(), (int)P->nr, Rw, Rr, sv,
+                                                                       F, Fr, st);
+    P->launches += 1;
+  }
+  BLS_CUDA(cudaGetLastError());
+  if (!failed_block) return BLS_OK;
+  return qr_status(P, failed_block);
+}
+
+// One launch per Gram class: MODE 0 writes S (sparse or dense) and g, MODE 1 the diagonal blocks D.
+template <class T, int MODE>
+static void gram(QRPlan* P, T* S, bool dense, double* g, const T* F, const double* Fr) {
+  cudaStream_t s = P->ctx->stream;
+  for (int c = 0; c < 8; ++c) {
+    const auto& k = P->gram_classes[c];
+    if (k.n == 0) continue;
+    const int64_t wb = ((std::is_same<T, double>::value ? k.bytes_f64 : k.bytes_f32) + 15) & ~int64_t(15);
+    const int wpc = warps_per_cta(wb);
+    const size_t smem = (size_t)(wb * wpc);
+    set_smem(reinterpret_cast<const void*>(k_qr_gram<T, MODE>), smem);
+    k_qr_gram<T, MODE><<<(unsigned)((k.n + wpc - 1) / wpc), 32 * wpc, smem, s>>>(
+        k.n, (int)wb, k.tables.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
+        P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(),
+        P->boff_r.as<int32_t>(), P->tp_ptr.as<int32_t>(), P->tp_blk.as<int32_t>(),
+        dense ? P->blk_base_dense.as<int64_t>() : P->blk_base_sparse.as<int64_t>(), dense ? nullptr : P->blk_stride.as<int32_t>(), P->nr,
+        P->doff.as<int64_t>(), P->max_dr, F, Fr, S, g);
+    P->launches += 1;
+  }
+  BLS_CUDA(cudaGetLastError());
+}
+
+template <class T>
 static void normal(QRPlan* P, T* S, bool dense, double* g, const T* F, const double* Fr) {
   if (!dense && !P->has_sparse) throw Error(BLS_EINVAL, "the QR plan was created without a sparse pattern");
   cudaStream_t s = P->ctx->stream;
   const int64_t nS = dense ? P->nr * P->nr : P->nnzS;
-  k_fill_t<T><<<(unsigned)std::min<int64_t>(grid_for(nS, 256), 148 * 8), 256, 0, s>>>(S, nS);
-  k_fill_t<double><<<grid_for(P->nr, 256), 256, 0, s>>>(g, P->nr);
-  if (P->nitems > 0)
-    k_qr_pairs<T><<<grid_for((P->nitems + 4) / 5 * 32, 128), 128, 0, s>>>(
-        P->nitems, P->item_block.as<int32_t>(), P->item_start.as<int32_t>(), P->item_info.as<int32_t>(), P->pair_u1.as<int32_t>(),
-        P->pair_u2.as<int32_t>(), P->blk_r1.as<int32_t>(), P->blk_r2.as<int32_t>(),
-        dense ? P->blk_base_dense.as<int64_t>() : P->blk_base_sparse.as<int64_t>(), dense ? nullptr : P->blk_stride.as<int32_t>(), P->nr,
-        P->u_table.as<int32_t>(), P->u_col.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
-        P->t_res.as<int64_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), F, Fr, S, g);
-  P->launches += 3;
-  BLS_CUDA(cudaGetLastError());
+  k_fill_t<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(nS, 256), 148 * 8)), 256, 0, s>>>(S, nS);
+  k_fill_t<double><<<(unsigned)std::max(1, grid_for(P->nr, 256)), 256, 0, s>>>(g, P->nr);
+  P->launches += 2;
+  gram<T, 0>(P, S, dense, g, F, Fr);
+}
+
+template <class T>
+static void diagonal_blocks(QRPlan* P, T* D, const T* F) {
+  cudaStream_t s = P->ctx->stream;
+  const int64_t nD = P->ndiag;
+  k_fill_t<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(nD, 256), 148 * 8)), 256, 0, s>>>(D, nD);
+  P->launches += 1;
+  gram<T, 1>(P, D, false, nullptr, F, nullptr);
 }
 
 }  // namespace bls
@@ -614,6 +702,20 @@ int bls_reduce_qr(bls_qr_plan* P, int dtype, void* F, double* Fr, const void* Rw
   })
 }
 
+int bls_qr_query_status(bls_qr_plan* P, int64_t* failed_block) {
+  QR_GUARD({
+    if (!P || !failed_block) throw Error(BLS_EINVAL, "null argument");
+    return qr_status(P, failed_block);
+  })
+}
+
+int64_t bls_qr_plan_counters(bls_qr_plan* P) {
+  if (!P) return -1;
+  const int64_t n = P->launches;
+  P->launches = 0;
+  return n;
+}
+
 int bls_qr_backsubstitute(bls_qr_plan* P, int dtype, double* x_e, const double* x_r, const void* F, const double* Fr) {
   QR_GUARD({
     cudaStream_t s = P->ctx->stream;
@@ -656,19 +758,9 @@ int bls_reduced_normal_dense(bls_qr_plan* P, int dtype, void* S, double* g, cons
 
 int bls_reduced_diagonal_blocks(bls_qr_plan* P, int dtype, void* D, const void* F) {
   QR_GUARD({
-    cudaStream_t s = P->ctx->stream;
-    const unsigned grid = (unsigned)grid_for(P->nrblocks * 16, 128);
-    if (dtype == BLS_F64)
-      k_qr_diag<double><<<grid, 128, 0, s>>>(P->nrblocks, P->r_ptr.as<int32_t>(), P->r_entry.as<int32_t>(), P->u_table.as<int32_t>(),
-                                             P->u_col.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
-                                             P->r_dims.as<int32_t>(), P->doff.as<int64_t>(), (const double*)F, (double*)D);
-    else if (dtype == BLS_F32)
-      k_qr_diag<float><<<grid, 128, 0, s>>>(P->nrblocks, P->r_ptr.as<int32_t>(), P->r_entry.as<int32_t>(), P->u_table.as<int32_t>(),
-                                            P->u_col.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
-                                            P->r_dims.as<int32_t>(), P->doff.as<int64_t>(), (const float*)F, (float*)D);
+    if (dtype == BLS_F64) diagonal_blocks<double>(P, (double*)D, (const double*)F);
+    else if (dtype == BLS_F32) diagonal_blocks<float>(P, (float*)D, (const float*)F);
     else throw Error(BLS_EINVAL, "unknown dtype");
-    P->launches += 1;
-    BLS_CUDA(cudaGetLastError());
     return BLS_OK;
   })
 }

@@ -195,10 +195,23 @@ class QRReductionWorkspace:
     def _T(self) -> int:
         return _dtype_code(self.factored)
 
+    def query_status(self) -> bool:
+        """Verdict of the last reduce_qr (synchronises); sets failed_block."""
+        fb = C.c_int64(0)
+        rc = check(_lib.gpu().bls_qr_query_status(self.handle, C.byref(fb)))
+        self.failed_block = int(fb.value)
+        return rc != BLS_NOT_PD
 
-def reduce_qr(ws: QRReductionWorkspace, J: SchurBlockJacobian, scaling_e: torch.Tensor, lam: float, s: torch.Tensor | None = None) -> bool:
+    def launches(self) -> int:
+        """Device kernel launches since the last call."""
+        return int(_lib.gpu().bls_qr_plan_counters(self._h))
+
+
+def reduce_qr(ws: QRReductionWorkspace, J: SchurBlockJacobian, scaling_e: torch.Tensor, lam: float, s: torch.Tensor | None = None,
+              *, sync: bool = True) -> bool:
     """QR elimination of every eliminated block (src/qr_reduction.jl:162-187); conditioned by `s` (over all the
-    variables, [s_r; s_e]) when given. False: a non-finite table or a numerically singular U (ws.failed_block)."""
+    variables, [s_r; s_e]) when given. False: a non-finite table or a numerically singular U (ws.failed_block).
+    sync=False launches without waiting for the verdict (read it with ws.query_status())."""
     jst = ws.structure
     if J.structure is not jst:
         raise ArgumentError("The Jacobian and the workspace were built for different structures")
@@ -210,7 +223,9 @@ def reduce_qr(ws: QRReductionWorkspace, J: SchurBlockJacobian, scaling_e: torch.
         _dev(s, "s", st.nr + st.ne, torch.float64)
     fb = C.c_int64(0)
     rc = check(_lib.gpu().bls_reduce_qr(ws.handle, ws._T, dptr(ws.factored), dptr(ws.fres), dptr(J.data), dptr(J.r), dptr(scaling_e),
-                                        float(lam), dptr(s), C.byref(fb)))
+                                        float(lam), dptr(s), C.byref(fb) if sync else None))
+    if not sync:
+        return True
     ws.failed_block = int(fb.value)
     return rc != BLS_NOT_PD
 

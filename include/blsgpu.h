@@ -241,6 +241,10 @@ int bls_qr_plan_destroy(bls_qr_plan* plan);
  * failed_block NULL = asynchronous. */
 int bls_reduce_qr(bls_qr_plan* plan, int dtype, void* F_dev, double* Fr_dev, const void* Rw_dev, const double* Rr_dev,
                   const double* scaling_e_dev, double lambda, const double* s_dev, int64_t* failed_block);
+/* Verdict of the last reduce_qr on this plan (synchronises): BLS_OK / BLS_NOT_PD (failed_block 1-based) / BLS_EINVAL. */
+int bls_qr_query_status(bls_qr_plan* plan, int64_t* failed_block);
+/* Device kernel launches issued on this plan since the previous call (no counterpart in the reference). */
+int64_t bls_qr_plan_counters(bls_qr_plan* plan);
 /* qr_backsubstitute! (src/qr_reduced.jl:24-93): x_e = U^-1 (q - B x_r) per eliminated block, in double. */
 int bls_qr_backsubstitute(bls_qr_plan* plan, int dtype, double* x_e_dev, const double* x_r_dev, const void* F_dev,
                           const double* Fr_dev);

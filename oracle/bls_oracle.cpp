@@ -1075,9 +1075,12 @@ void qr_backsubstitute(double* x_e, const double* x_r, const T* F, const double*
 }
 
 // accumulate_qr_entry! (src/qr_reduced.jl:375-405) driven by reduced_normal_sparse! (:440-480)
+// Threaded over block columns r2 as foreach_retained threads over column chunks (:116-124): each writes its own columns.
 template <class T>
 void reduced_normal_sparse(T* nzval, double* g_S, const T* F, const double* Fr, const QRStructure& q, const Pattern& P) {
   const Structure& st = q.schur;
+  int missing = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(| : missing)
   for (i64 r2 = 1; r2 <= st.nrblocks; ++r2) {
     i64 ro2 = st.boffsets_r(r2), dr2 = st.r_dims(r2);
     for (i64 i = P.S_colptr(ro2); i <= P.S_colptr(ro2 + dr2) - 1; ++i) nzval[i - 1] = T(0);
@@ -1096,7 +1099,7 @@ void reduced_normal_sparse(T* nzval, double* g_S, const T* F, const double* Fr, 
         i64 r1 = q.entry_retained(u1), dr1 = st.r_dims(r1), cb1 = off + (q.entry_col(u1) - 1) * M;
         i64 idx = b_lo;
         while (idx <= b_hi && P.block_rowval(idx) < r1) ++idx;
-        if (!(idx <= b_hi && P.block_rowval(idx) == r1)) throw BlsError(ORC_EPATTERN, "The sparse pattern has no block");
+        if (!(idx <= b_hi && P.block_rowval(idx) == r1)) { missing = 1; continue; }
         i64 row_offset = P.block_row_offsets(idx);
         for (i64 col = 1; col <= dr2; ++col) {
           i64 nrow = u1 == u2 ? col : dr1;
@@ -1109,6 +1112,7 @@ void reduced_normal_sparse(T* nzval, double* g_S, const T* F, const double* Fr, 
       }
     }
   }
+  if (missing) throw BlsError(ORC_EPATTERN, "The sparse pattern has no block");
 }
 
 // reduced_normal_dense! (src/qr_reduced.jl:409-436)
