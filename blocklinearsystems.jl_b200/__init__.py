@@ -8,6 +8,7 @@ Device reduction:        SchurReductionWorkspace, reset_schur_sparse / reset_sch
                          reduce_schur_sparse / reduce_schur_dense, backsubstitute, scatter_copy
 QR elimination:          SchurJacobianStructure, SchurBlockJacobian, QRReductionWorkspace, reduce_qr, qr_backsubstitute,
                          reduced_normal_sparse / reduced_normal_dense, reduced_diagonal_blocks, free_block_pairs
+Reduced solve:           BlockJacobi, factor_diagonal_blocks, solve_diagonal_blocks, PCGWorkspace (block-Jacobi PCG)
 Workloads:               scenes.workload, scenes.hessian_problem, scenes.jacobian_problem
 """
 from ._lib import ArgumentError, BlsError, DimensionMismatch
@@ -16,6 +17,7 @@ from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce
                         reset_schur_dense, reset_schur_sparse, scatter_copy)
 from .qr import (QRReductionWorkspace, SchurBlockJacobian, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
                  reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse)
+from .pcg import BlockJacobi, PCGResult, PCGWorkspace, factor_diagonal_blocks, solve_diagonal_blocks
 from . import scenes
 
 __all__ = [
@@ -23,5 +25,6 @@ __all__ = [
     "build_schur_pattern", "sparse_with_map", "SchurReductionWorkspace", "backsubstitute", "context", "reduce_schur_dense",
     "reduce_schur_sparse", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
     "SchurBlockJacobian", "SchurJacobianStructure", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
-    "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse",
+    "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "BlockJacobi", "PCGResult", "PCGWorkspace",
+    "factor_diagonal_blocks", "solve_diagonal_blocks",
 ]

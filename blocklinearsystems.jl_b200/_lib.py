@@ -10,6 +10,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 
 BLS_OK, BLS_NOT_PD, BLS_EINVAL, BLS_EDIM, BLS_EPATTERN, BLS_ECUDA, BLS_EUNSUPPORTED, BLS_ENOMEM = 0, 1, -1, -2, -3, -4, -5, -6
+BLS_NOT_CONVERGED = 2
 BLS_F64, BLS_F32 = 0, 1
 
 i64 = C.c_int64
@@ -108,6 +109,16 @@ def gpu() -> C.CDLL:
             "bls_reduced_normal_sparse": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_reduced_normal_dense": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_reduced_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, vp]),
+            "bls_block_jacobi_create": (C.c_int, [vp, i64, p64, C.POINTER(vp)]),
+            "bls_block_jacobi_destroy": (C.c_int, [vp]),
+            "bls_factor_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, p64]),
+            "bls_solve_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+            "bls_pcg_plan_create": (C.c_int, [vp, i64, p64, p64, p64, p64, p64, p64, C.POINTER(vp)]),
+            "bls_pcg_plan_destroy": (C.c_int, [vp]),
+            "bls_spmv_sym": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+            "bls_extract_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, vp]),
+            "bls_pcg_solve": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, i64, C.c_int, p64, pdbl, p64]),
+            "bls_pcg_plan_counters": (i64, [vp]),
         }
         for fn, (res, args) in sig.items():
             f = getattr(L, fn)

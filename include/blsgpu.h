@@ -29,6 +29,7 @@ extern "C" {
 
 #define BLS_OK 0
 #define BLS_NOT_PD 1          /* reduce_schur_*! / reduce_qr! returned false (src/schur_reduction.jl:233-257) */
+#define BLS_NOT_CONVERGED 2   /* an iterative solve stopped at its iteration limit above its tolerance */
 #define BLS_EINVAL (-1)       /* ArgumentError (bad lambda / scaling / structure) */
 #define BLS_EDIM (-2)         /* DimensionMismatch */
 #define BLS_EPATTERN (-3)     /* a block missing from the sparse pattern (throw_missing_block, src/utils.jl:109) */
@@ -45,6 +46,8 @@ typedef struct bls_pattern bls_pattern;
 typedef struct bls_schur_plan bls_schur_plan;
 typedef struct bls_qr_structure bls_qr_structure;
 typedef struct bls_qr_plan bls_qr_plan;
+typedef struct bls_pcg_plan bls_pcg_plan;
+typedef struct bls_block_jacobi bls_block_jacobi;
 
 int bls_version(void);
 /* Message of the last error on the calling thread. */
@@ -256,6 +259,42 @@ int bls_reduced_normal_dense(bls_qr_plan* plan, int dtype, void* S_dev, double* 
                              const double* Fr_dev);
 /* reduced_diagonal_blocks! (src/qr_reduced.jl:484-512): the full d_r x d_r diagonal blocks of J~'J~ at doffsets. */
 int bls_reduced_diagonal_blocks(bls_qr_plan* plan, int dtype, void* D_dev, const void* F_dev);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Block-Jacobi (src/diagonal_blocks.jl:6-61) on a flat array of square diagonal blocks (block b, d_b x d_b column-major,
+ * after the blocks before it), as reduced_diagonal_blocks! writes them. d_b <= 16.
+ * ------------------------------------------------------------------------------------------------------------- */
+int bls_block_jacobi_create(bls_ctx* ctx, int64_t nblocks, const int64_t* dims, bls_block_jacobi** out);
+int bls_block_jacobi_destroy(bls_block_jacobi* bj);
+/* factor_diagonal_blocks!(D, dims) -> Bool: each block's Cholesky factor L in place in its lower triangle. BLS_OK, or
+ * BLS_NOT_PD with failed_block = the lowest block (1-based) that is not positive definite or not finite. Synchronises. */
+int bls_factor_diagonal_blocks(bls_block_jacobi* bj, int dtype, void* D_dev, int64_t* failed_block);
+/* solve_diagonal_blocks!(y, D, dims, x): y = (L L')^-1 x block by block (y may be x); x, y double. */
+int bls_solve_diagonal_blocks(bls_block_jacobi* bj, int dtype, double* y_dev, const void* D_dev, const double* x_dev);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * PCG on the reduced system S x = g (no counterpart in the reference, which solves it with CHOLMOD / LDLFactorizations,
+ * src/schur_linear_systems.jl:362-406; its iterative path is LSMR on J~ with the same block-Jacobi preconditioner,
+ * ext/KrylovExt.jl:97-132). S: the upper block triangle on build_schur_pattern's pattern, as reduce_schur_sparse!
+ * leaves it. x, g double.
+ * ------------------------------------------------------------------------------------------------------------- */
+int bls_pcg_plan_create(bls_ctx* ctx, int64_t nrblocks, const int64_t* r_dims, const int64_t* block_colptr,
+                        const int64_t* block_rowval, const int64_t* block_row_offsets, const int64_t* col_heights,
+                        const int64_t* S_colptr, bls_pcg_plan** out);
+int bls_pcg_plan_destroy(bls_pcg_plan* plan);
+/* y = S x with S symmetric (its upper blocks mirrored), FP64 products. */
+int bls_spmv_sym(bls_pcg_plan* plan, int dtype, const void* S_nzval_dev, const double* x_dev, double* y_dev);
+/* The full d_r x d_r diagonal blocks of S (upper triangles mirrored) as doubles, block after block. */
+int bls_extract_diagonal_blocks(bls_pcg_plan* plan, int dtype, const void* S_nzval_dev, double* D_dev);
+/* PCG from the initial x to ||g - S x||_2 <= tol ||g||_2, checked on an explicit FP64 residual (restarted from x while
+ * the recursive residual has drifted: iterative refinement), preconditioned by the block-Jacobi factorisation of S's
+ * diagonal blocks. use_graph: replay runs of iterations as one CUDA graph. Returns BLS_OK, BLS_NOT_CONVERGED (maxit
+ * reached; x is the last iterate) or BLS_NOT_PD (failed_block = the lowest diagonal block of S, 1-based, that is not
+ * positive definite). iterations and rel_residual report the run. */
+int bls_pcg_solve(bls_pcg_plan* plan, int dtype, const void* S_nzval_dev, const double* g_dev, double* x_dev, double tol,
+                  int64_t maxit, int use_graph, int64_t* iterations, double* rel_residual, int64_t* failed_block);
+/* Device kernel launches issued on this plan since the previous call (no counterpart in the reference). */
+int64_t bls_pcg_plan_counters(bls_pcg_plan* plan);
 
 /* copyto!(csc, bsm, scatter_map) (src/SparseBlockLinearSystem.jl:356-362): dest[i] = src[map[i]], i < n. */
 int bls_scatter_copy(bls_ctx* ctx, int dtype, void* dest_dev, const void* src_dev, const int64_t* map_dev, int64_t n);

@@ -1281,6 +1281,104 @@ SparseIdx makesparseindices(const Structure& st, const RLayout& L, bool symmetri
 
 }  // namespace
 
+// ----------------------------------------------------------------------------------------------------------------------
+// Block-Jacobi PCG on the reduced system S x = g (no counterpart in the reference: the CPU restatement of the device
+// solve, used as its checker and its timed CPU baseline). S: the upper triangle on the pattern; the symmetric matrix's
+// rows are gathered from it through an index built once per call. FP64 vectors; the block-Jacobi blocks are S's
+// diagonal blocks factored by factor_diagonal_blocks (src/diagonal_blocks.jl:6-29). Same stopping rule as the device:
+// recursive residual, then an explicit residual with restarts while it is above tol.
+// ----------------------------------------------------------------------------------------------------------------------
+template <class T>
+int pcg_solve(const Structure& st, const Pattern& P, const T* S, const double* g, double* x, double tol, i64 maxit, int nthreads,
+              i64* iters_out, double* rel_out) {
+  const i64 nr = st.nr, nrb = st.nrblocks;
+  // symmetric rows: row i takes (j, pos) for every stored upper entry (i, j) and (j, i)
+  std::vector<i64> cnt(nr + 1, 0);
+  for (i64 j = 1; j <= nr; ++j)
+    for (i64 q = P.S_colptr(j); q <= P.S_colptr(j + 1) - 1; ++q) {
+      const i64 i = P.S_rowval(q);
+      if (i > j) continue;
+      cnt[i] += 1;
+      if (i < j) cnt[j] += 1;
+    }
+  std::vector<i64> rp(nr + 1, 0);
+  for (i64 i = 0; i < nr; ++i) rp[i + 1] = rp[i] + cnt[i + 1];
+  std::vector<i64> rc(rp[nr]), rq(rp[nr]), fill(rp.begin(), rp.end() - 1);
+  for (i64 j = 1; j <= nr; ++j)
+    for (i64 q = P.S_colptr(j); q <= P.S_colptr(j + 1) - 1; ++q) {
+      const i64 i = P.S_rowval(q);
+      if (i > j) continue;
+      rc[fill[i - 1]] = j - 1; rq[fill[i - 1]] = q - 1; fill[i - 1] += 1;
+      if (i < j) { rc[fill[j - 1]] = i - 1; rq[fill[j - 1]] = q - 1; fill[j - 1] += 1; }
+    }
+  auto spmv = [&](const double* v, double* y) {
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (i64 i = 0; i < nr; ++i) {
+      double a = 0.0;
+      for (i64 e = rp[i]; e < rp[i + 1]; ++e) a += (double)S[rq[e]] * v[rc[e]];
+      y[i] = a;
+    }
+  };
+  // block-Jacobi: S's diagonal blocks, mirrored, factored
+  std::vector<double> D;
+  std::vector<i64> doff(nrb + 1, 0), dims(nrb);
+  for (i64 r = 1; r <= nrb; ++r) { dims[r - 1] = st.r_dims(r); doff[r] = doff[r - 1] + dims[r - 1] * dims[r - 1]; }
+  D.assign(doff[nrb], 0.0);
+  for (i64 r = 1; r <= nrb; ++r) {
+    const i64 d = dims[r - 1], ro = st.boffsets_r(r);
+    for (i64 w = 0; w < d; ++w)
+      for (i64 a = 0; a < d; ++a) {
+        const i64 lo = std::min(a, w), hi = std::max(a, w);
+        const i64 col = ro + hi;
+        // the entry (ro + lo, col): the diagonal block's rows are contiguous in column col, ending at (col, col)
+        D[doff[r - 1] + w * d + a] = (double)S[P.diag_inds(col) - (hi - lo) - 1];
+      }
+  }
+  if (!factor_diagonal_blocks<double>(D.data(), dims.data(), nrb)) return ORC_NOT_PD;
+  std::vector<double> r(nr), z(nr), p(nr), q(nr);
+  auto precond = [&](const double* in, double* out) { solve_diagonal_blocks<double>(out, D.data(), dims.data(), nrb, in); };
+  auto dot = [&](const double* a, const double* b) {
+    double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static) num_threads(nthreads)
+    for (i64 i = 0; i < nr; ++i) s += a[i] * b[i];
+    return s;
+  };
+  const double gg = dot(g, g);
+  if (gg == 0.0) { for (i64 i = 0; i < nr; ++i) x[i] = 0.0; *iters_out = 0; *rel_out = 0.0; return ORC_OK; }
+  const double t2 = tol * tol * gg;
+  i64 iters = 0;
+  double rel = INFINITY;
+  for (int restart = 0; restart < 4; ++restart) {
+    spmv(x, q.data());
+    for (i64 i = 0; i < nr; ++i) r[i] = g[i] - q[i];
+    precond(r.data(), z.data());
+    p = z;
+    double rz = dot(r.data(), z.data()), rr = dot(r.data(), r.data());
+    while (rr > t2 && iters < maxit) {
+      spmv(p.data(), q.data());
+      const double alpha = rz / dot(p.data(), q.data());
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+      for (i64 i = 0; i < nr; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * q[i]; }
+      precond(r.data(), z.data());
+      const double rzn = dot(r.data(), z.data());
+      rr = dot(r.data(), r.data());
+      ++iters;
+      if (!(rr > t2)) break;
+      const double beta = rzn / rz;
+      rz = rzn;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+      for (i64 i = 0; i < nr; ++i) p[i] = z[i] + beta * p[i];
+    }
+    spmv(x, q.data());
+    for (i64 i = 0; i < nr; ++i) r[i] = g[i] - q[i];
+    rel = std::sqrt(dot(r.data(), r.data()) / gg);
+    if (rel <= tol || iters >= maxit || !std::isfinite(rel)) break;
+  }
+  *iters_out = iters;
+  *rel_out = rel;
+  return rel <= tol ? ORC_OK : 2;
+}
+
 // ======================================================================================================================
 // extern "C" boundary: 0-based integers, status codes (0 ok, 1 singular/not positive definite, < 0 argument errors)
 // ======================================================================================================================
@@ -1621,6 +1719,15 @@ i64 orc_qr_field(OrcQR* o, const char* name, i64* out) {
 
 ORC_QR_TYPED(f64, double)
 ORC_QR_TYPED(f32, float)
+
+int orc_pcg_solve_f64(OrcStructure* o, OrcPattern* p, const double* S, const double* g, double* x, double tol, i64 maxit, int nthreads,
+                      i64* iters, double* rel) {
+  ORC_TRY({ return pcg_solve<double>(o->st, p->P, S, g, x, tol, maxit, nthreads, iters, rel); })
+}
+int orc_pcg_solve_f32(OrcStructure* o, OrcPattern* p, const float* S, const double* g, double* x, double tol, i64 maxit, int nthreads,
+                      i64* iters, double* rel) {
+  ORC_TRY({ return pcg_solve<float>(o->st, p->P, S, g, x, tol, maxit, nthreads, iters, rel); })
+}
 
 // The closed-form inverse alone (tests of src/kernels.jl:14-67 and the generic path): d x d column-major H, damping
 // scale (lambda = 1 folded into `damp`). Returns 1 on success.

@@ -345,3 +345,12 @@ def factor_diagonal_blocks(D, dims):
 def solve_diagonal_blocks(y, D, dims, x):
     dm = np.ascontiguousarray(dims, np.int64)
     getattr(lib(), "orc_solve_diagonal_blocks_" + _sfx(D))(_p(y), _p(D), _p(dm), i64(len(dm)), _p(x))
+
+
+def pcg_solve(st: Structure, pat: Pattern, S, g, x, tol=1e-8, maxit=100000, nthreads=None):
+    """Block-Jacobi PCG on S x = g (S's upper triangle on the pattern); x updated in place. Returns
+    (status, iterations, rel_residual): status 0 converged, 1 a diagonal block not PD, 2 not converged."""
+    it, rel = C.c_int64(0), C.c_double(0.0)
+    f = getattr(lib(), "orc_pcg_solve_" + _sfx(S))
+    rc = _chk(f(st.h, pat.h, _p(S), _p(g), _p(x), C.c_double(tol), i64(maxit), C.c_int(nthreads or max_threads()), C.byref(it), C.byref(rel)))
+    return rc, int(it.value), float(rel.value)
