@@ -159,6 +159,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     d32 = device_inputs(torch.float32)
     with ClockSampler(dev.index) as clk:
         ms32, cnt32 = timed(d32, args.steps, args.warmup, instrument=True)
+    _LAST.update(problem=p, d32=d32)
     d64 = device_inputs(torch.float64)
     ms64, cnt64 = timed(d64, args.steps, args.warmup, instrument=True)
     del d64
@@ -392,11 +393,71 @@ def cpu_baseline_qr(spec, seconds: float = 10.0, steps: int | None = None, warmu
                       f"{cores} OpenMP threads ({dt:.1f} s)"}
 
 
-def oracle_problem(spec):
+def run_ours_pcg(args, rank: int, world: int) -> dict | None:
+    """The PCG workload: the mixed reduction of the scene (timed as the Schur workload is), then PCG on the mixed S to
+    ||g - S x|| <= 1e-8 ||g|| (FP64 residual), block-Jacobi preconditioned; seconds per solve on the device."""
+    import torch
+    out = run_ours(args, rank, world)
+    bls = load_package()
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    p = _LAST["problem"]
+    st, pat, d32 = p.structure, p.pattern, _LAST["d32"]
+    pws = bls.PCGWorkspace(st, pat, device=dev.index)
+    S, g = d32["S"], d32["g"]
+    x = torch.zeros(st.nr, dtype=torch.float64, device=dev)
+    times, iters, rels = [], [], []
+    for k in range(args.warmup + args.steps):
+        x.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record()
+        _, res = pws.solve(S, g, x, tol=1e-8)
+        b.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        assert res.converged, res
+        if k >= args.warmup:
+            times.append((a.elapsed_time(b) / 1e3, wall))
+            iters.append(res.iterations)
+            rels.append(res.rel_residual)
+    pws.launches()
+    if rank != 0:
+        return None
+    dev_s = statistics.median(t[0] for t in times)
+    out["pcg"] = {"seconds_to_1e-8": dev_s, "wall_seconds": statistics.median(t[1] for t in times), "iterations": iters[-1],
+                  "rel_residual": rels[-1], "preconditioner": "block-Jacobi (6x6)", "S_storage": "f32 (mixed reduction output)",
+                  "residual": "explicit FP64 g - S x"}
+    if not args.no_cpu_baseline:
+        out["pcg"]["cpu_baseline"] = cpu_baseline_pcg(p, args.workload)
+    return out
+
+
+_LAST: dict = {}
+
+
+def cpu_baseline_pcg(p, workload: str) -> dict:
+    """The oracle's PCG (the same algorithm on every host core) on the FP64 reduced system of the same scene."""
+    orc, _, ost, opat, cores = oracle_problem(load_package().scenes.workload(workload), p)
+    w = orc.Work(ost, cores, False)
+    S, g = np.zeros(opat.nnz), np.zeros(ost.nr)
+    orc.reset_schur_sparse(ost, opat, S, p.R, p.scaling_r, p.lam)
+    ok, _ = orc.reduce_schur_sparse(ost, opat, w, S, g, p.b_r, p.b_e, p.scaling_e, p.lam, p.E, p.C, nthreads=cores)
+    assert ok
+    x = np.zeros(ost.nr)
+    t0 = time.perf_counter()
+    rc, it, rel = orc.pcg_solve(ost, opat, S, g, x, 1e-8, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"seconds_to_1e-8": dt, "iterations": it, "rel_residual": rel, "cores": cores, "kind": "port",
+            "sample": f"one block-Jacobi PCG solve to 1e-8, FP64, {cores} OpenMP threads"}
+
+
+def oracle_problem(spec, p=None):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
     bls = load_package()
-    p = bls.scenes.hessian_problem(spec)
+    if p is None:
+        p = bls.scenes.hessian_problem(spec)
     sc = bls.scenes.Scene(spec)
     bs, el, ptr, idx = sc.description()
     cores = os.cpu_count() or 1
@@ -474,6 +535,8 @@ def main():
             out = run_reference(args, rank, world)
         elif args.workload.startswith("qr_"):
             out = run_ours_qr(args, rank, world)
+        elif args.workload.startswith("pcg_"):
+            out = run_ours_pcg(args, rank, world)
         else:
             out = run_ours(args, rank, world)
     finally:

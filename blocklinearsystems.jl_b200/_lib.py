@@ -119,6 +119,16 @@ def gpu() -> C.CDLL:
             "bls_extract_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, vp]),
             "bls_pcg_solve": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, i64, C.c_int, p64, pdbl, p64]),
             "bls_pcg_plan_counters": (i64, [vp]),
+            "bls_pcg_set_preconditioner": (C.c_int, [vp, vp]),
+            "bls_gnn_param_count": (i64, []),
+            "bls_gnn_create": (C.c_int, [vp, p64, p64, p64, p64, p64, C.POINTER(vp)]),
+            "bls_gnn_destroy": (C.c_int, [vp]),
+            "bls_gnn_prepare": (C.c_int, [vp, C.c_int, vp, p64]),
+            "bls_gnn_forward": (C.c_int, [vp, vp, C.c_int, vp]),
+            "bls_gnn_outputs": (C.c_int, [vp, vp, vp, vp]),
+            "bls_gnn_edge_count": (i64, [vp]),
+            "bls_gnn_loss_grad": (C.c_int, [vp, C.c_int, vp, vp, vp, i64, pdbl, vp]),
+            "bls_adam_step": (C.c_int, [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, i64]),
         }
         for fn, (res, args) in sig.items():
             f = getattr(L, fn)

@@ -23,47 +23,9 @@
 #include <memory>
 #include <vector>
 
-#include "common.cuh"
+#include "pcg_plan.hpp"
 
 namespace bls {
-
-// Slot layout of the per-iteration scalars: rz (r'z entering the iteration), pq, rz_next, rr_next
-constexpr int PS_RZ = 0, PS_PQ = 1, PS_RZN = 2, PS_RRN = 3, PS_W = 4;
-
-struct RowEntry {
-  int64_t base;     // S offset of the block's first entry
-  int32_t stride;   // column stride of the block in S
-  int32_t xo;       // offset of the other block's variables in x
-  int16_t dother;   // dimension of the other block
-  int16_t mode;     // 0: B x (block right of the diagonal), 1: B' x (block above), 2: diagonal (symmetric)
-  int32_t pad;
-};
-
-struct PCGPlan {
-  bls_ctx* ctx = nullptr;
-  int64_t nrb = 0, nr = 0, nnz = 0, ndiag = 0;
-  int max_d = 0;
-  DevBuf row_ptr, rows, r_dims, boff, doff, diag_base, diag_stride;
-  // solver state (FP64)
-  DevBuf D;                 // factored diagonal blocks (L in the lower triangle)
-  DevBuf r, z, p, q, scal, flags;
-  int K = 16;               // iterations per replayed graph
-  cudaGraphExec_t graph = nullptr;
-  const void* graph_S = nullptr;
-  const double* graph_x = nullptr;
-  int graph_dtype = -1;
-  cudaStream_t cap_stream = nullptr;   // the plan's own stream: graphs are captured and replayed there
-  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-  double* host = nullptr;   // pinned scratch for scalars read back
-  int64_t launches = 0;
-  ~PCGPlan() {
-    if (graph) cudaGraphExecDestroy(graph);
-    if (ev_in) cudaEventDestroy(ev_in);
-    if (ev_out) cudaEventDestroy(ev_out);
-    if (cap_stream) cudaStreamDestroy(cap_stream);
-    if (host) cudaFreeHost(host);
-  }
-};
 
 // ---------------------------------------------------------------------------------------------------------------
 // Block-Jacobi: factor_diagonal_blocks! and solve_diagonal_blocks! (src/diagonal_blocks.jl:6-61)
@@ -215,15 +177,35 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 }
 
 // Start: r = g - S x (already in r), z = M^-1 r, p = z, rz and rr into slot 0
+// z = M^-1 r for one block: the block-Jacobi solve with the factored D, or the dense block Bp (d x d, column-major)
+__device__ __forceinline__ void precondition(double* z, const double* __restrict__ D, const double* __restrict__ Bp, int d, const double* r) {
+  if (Bp) {
+    double v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = 0.0;
+    for (int j = 0; j < d; ++j) {
+      const double rj = r[j];
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        if (i < d) v[i] += Bp[j * d + i] * rj;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      if (i < d) z[i] = v[i];
+  } else {
+    block_solve<double>(z, D, d, r);
+  }
+}
+
 __global__ void k_pcg_start(int64_t nrb, const int32_t* __restrict__ dims, const int32_t* __restrict__ boff, const int64_t* __restrict__ doff,
-                            const double* __restrict__ D, const double* __restrict__ r, double* __restrict__ z, double* __restrict__ p,
-                            double* __restrict__ slot0) {
+                            const double* __restrict__ D, const double* __restrict__ Bp, const double* __restrict__ r, double* __restrict__ z,
+                            double* __restrict__ p, double* __restrict__ slot0) {
   const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double rz = 0.0, rr = 0.0;
   if (b < nrb) {
     const int d = dims[b];
     const int64_t o = boff[b];
-    block_solve<double>(z + o, D + doff[b], d, r + o);
+    precondition(z + o, D + doff[b], Bp ? Bp + doff[b] : nullptr, d, r + o);
     for (int i = 0; i < d; ++i) {
       p[o + i] = z[o + i];
       rz += r[o + i] * z[o + i];
@@ -240,7 +222,8 @@ __global__ void k_pcg_start(int64_t nrb, const int32_t* __restrict__ dims, const
 
 // (2) alpha = rz / pq; x += alpha p; r -= alpha q; z = M^-1 r; rz_next, rr_next
 __global__ void k_pcg_update(int64_t nrb, const int32_t* __restrict__ dims, const int32_t* __restrict__ boff, const int64_t* __restrict__ doff,
-                             const double* __restrict__ D, double* __restrict__ x, double* __restrict__ r, double* __restrict__ z,
+                             const double* __restrict__ D, const double* __restrict__ Bp, double* __restrict__ x, double* __restrict__ r,
+                             double* __restrict__ z,
                              const double* __restrict__ p, const double* __restrict__ q, double* __restrict__ slot,
                              const int* __restrict__ done) {
   if (*done) return;
@@ -254,7 +237,7 @@ __global__ void k_pcg_update(int64_t nrb, const int32_t* __restrict__ dims, cons
       x[o + i] += alpha * p[o + i];
       r[o + i] -= alpha * q[o + i];
     }
-    block_solve<double>(z + o, D + doff[b], d, r + o);
+    precondition(z + o, D + doff[b], Bp ? Bp + doff[b] : nullptr, d, r + o);
     for (int i = 0; i < d; ++i) {
       rz += r[o + i] * z[o + i];
       rr += r[o + i] * r[o + i];
@@ -428,18 +411,7 @@ static void extract_diag(PCGPlan* P, const T* S, double* D, cudaStream_t s) {
   P->launches += 1;
 }
 
-// Factor the block-Jacobi blocks in P->D; returns the lowest failing block (0-based) or -1
-static int64_t factor_D(PCGPlan* P, cudaStream_t s) {
-  long long* failed = reinterpret_cast<long long*>(P->flags.as<int>() + 4);
-  const long long none = LLONG_MAX;
-  BLS_CUDA(cudaMemcpyAsync(failed, &none, sizeof(long long), cudaMemcpyHostToDevice, s));
-  k_factor_blocks<double><<<grid_for(P->nrb, 128), 128, 0, s>>>(P->nrb, P->r_dims.as<int32_t>(), P->doff.as<int64_t>(), P->D.as<double>(), failed);
-  P->launches += 1;
-  long long h = 0;
-  BLS_CUDA(cudaMemcpyAsync(&h, failed, sizeof(long long), cudaMemcpyDeviceToHost, s));
-  BLS_CUDA(cudaStreamSynchronize(s));
-  return h == none ? -1 : (int64_t)h;
-}
+static int64_t factor_D(PCGPlan* P, cudaStream_t s) { return pcg_factor_blocks(P, P->D.as<double>(), s); }
 
 // The kernels of one PCG iteration on slot j
 template <class T>
@@ -449,7 +421,7 @@ static void iteration(PCGPlan* P, const T* S, double* x, int j, cudaStream_t s) 
   const unsigned gsp = (unsigned)grid_for(P->nrb * 32, 256), gb = (unsigned)grid_for(P->nrb, 128), gv = (unsigned)grid_for(P->nr, 256);
   k_spmv<T, false, true><<<gsp, 256, 0, s>>>(P->nrb, P->row_ptr.as<int64_t>(), P->rows.as<RowEntry>(), P->r_dims.as<int32_t>(),
                                              P->boff.as<int32_t>(), S, P->p.as<double>(), nullptr, P->q.as<double>(), slot + PS_PQ, flags);
-  k_pcg_update<<<gb, 128, 0, s>>>(P->nrb, P->r_dims.as<int32_t>(), P->boff.as<int32_t>(), P->doff.as<int64_t>(), P->D.as<double>(), x,
+  k_pcg_update<<<gb, 128, 0, s>>>(P->nrb, P->r_dims.as<int32_t>(), P->boff.as<int32_t>(), P->doff.as<int64_t>(), P->D.as<double>(), P->precond, x,
                                   P->r.as<double>(), P->z.as<double>(), P->p.as<double>(), P->q.as<double>(), slot, flags);
   k_pcg_direction<<<gv, 256, 0, s>>>(P->nr, P->z.as<double>(), P->p.as<double>(), slot, slot + PS_W,
                                      P->scal.as<double>() + (P->K + 1) * PS_W, flags);
@@ -507,8 +479,8 @@ static int pcg_solve(PCGPlan* P, const T* S, const double* g, double* x, double 
     BLS_CUDA(cudaMemcpyAsync(tol2, &t2, sizeof(double), cudaMemcpyHostToDevice, s));
     BLS_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(int), s));
     k_pcg_start<<<grid_for(P->nrb, 128), 128, 0, s>>>(P->nrb, P->r_dims.as<int32_t>(), P->boff.as<int32_t>(), P->doff.as<int64_t>(),
-                                                      P->D.as<double>(), P->r.as<double>(), P->z.as<double>(), P->p.as<double>(),
-                                                      scal + P->K * PS_W);
+                                                      P->D.as<double>(), P->precond, P->r.as<double>(), P->z.as<double>(),
+                                                      P->p.as<double>(), scal + P->K * PS_W);
     P->launches += 2;
     BLS_CUDA(cudaMemcpyAsync(P->host, scal + P->K * PS_W + PS_RRN, sizeof(double), cudaMemcpyDeviceToHost, s));
     BLS_CUDA(cudaStreamSynchronize(s));
@@ -520,7 +492,7 @@ static int pcg_solve(PCGPlan* P, const T* S, const double* g, double* x, double 
     while (iters + done_here < maxit) {
       const int64_t left = maxit - iters - done_here;
       if (use_graph && left >= P->K) {
-        if (!P->graph || P->graph_S != (const void*)S || P->graph_dtype != (int)sizeof(T) || P->graph_x != x) {
+        if (!P->graph || P->graph_S != (const void*)S || P->graph_dtype != (int)sizeof(T) || P->graph_x != x || P->graph_precond != P->precond) {
           if (P->graph) {
             cudaGraphExecDestroy(P->graph);
             P->graph = nullptr;
@@ -533,6 +505,7 @@ static int pcg_solve(PCGPlan* P, const T* S, const double* g, double* x, double 
           cudaGraphDestroy(gr);
           P->graph_S = S;
           P->graph_x = x;
+          P->graph_precond = P->precond;
           P->graph_dtype = (int)sizeof(T);
         }
         // order the graph after the work already on the context's stream, and the stream after the graph
@@ -566,6 +539,28 @@ static int pcg_solve(PCGPlan* P, const T* S, const double* g, double* x, double 
   *iters_out = iters;
   *rel_out = rel;
   return rel <= tol ? BLS_OK : BLS_NOT_CONVERGED;
+}
+
+void pcg_spmv(PCGPlan* P, int dtype, const void* S, const double* x, const double* g, double* y, bool residual, cudaStream_t s) {
+  if (dtype == BLS_F64) spmv<double>(P, (const double*)S, x, g, y, residual, s);
+  else spmv<float>(P, (const float*)S, x, g, y, residual, s);
+}
+
+void pcg_extract_diag(PCGPlan* P, int dtype, const void* S, double* D, cudaStream_t s) {
+  if (dtype == BLS_F64) extract_diag<double>(P, (const double*)S, D, s);
+  else extract_diag<float>(P, (const float*)S, D, s);
+}
+
+int64_t pcg_factor_blocks(PCGPlan* P, double* D, cudaStream_t s) {
+  long long* failed = reinterpret_cast<long long*>(P->flags.as<int>() + 4);
+  const long long none = LLONG_MAX;
+  BLS_CUDA(cudaMemcpyAsync(failed, &none, sizeof(long long), cudaMemcpyHostToDevice, s));
+  k_factor_blocks<double><<<grid_for(P->nrb, 128), 128, 0, s>>>(P->nrb, P->r_dims.as<int32_t>(), P->doff.as<int64_t>(), D, failed);
+  P->launches += 1;
+  long long h = 0;
+  BLS_CUDA(cudaMemcpyAsync(&h, failed, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaStreamSynchronize(s));
+  return h == none ? -1 : (int64_t)h;
 }
 
 }  // namespace bls
@@ -645,6 +640,12 @@ int bls_pcg_solve(bls_pcg_plan* P, int dtype, const void* S, const double* g, do
       return pcg_solve<float>(P, (const float*)S, g, x, tol, maxit, use_graph != 0, iterations, rel_residual, failed_block);
     throw Error(BLS_EINVAL, "unknown dtype");
   })
+}
+
+int bls_pcg_set_preconditioner(bls_pcg_plan* P, const double* blocks) {
+  if (!P) return BLS_EINVAL;
+  P->precond = blocks;
+  return BLS_OK;
 }
 
 int64_t bls_pcg_plan_counters(bls_pcg_plan* P) {

@@ -125,9 +125,19 @@ class PCGWorkspace:
         return int(_lib.gpu().bls_pcg_plan_counters(self._h))
 
     def solve(self, S: torch.Tensor, g: torch.Tensor, x: torch.Tensor | None = None, *, tol: float = 1e-8, maxit: int | None = None,
-              graph: bool = True) -> tuple[torch.Tensor, PCGResult]:
-        """Block-Jacobi PCG from x (zero when None) to ||g - S x|| <= tol ||g|| on an explicit FP64 residual. x is
-        updated in place and returned with the run's PCGResult."""
+              graph: bool = True, preconditioner: torch.Tensor | None = None) -> tuple[torch.Tensor, PCGResult]:
+        """PCG from x (zero when None) to ||g - S x|| <= tol ||g|| on an explicit FP64 residual, preconditioned by
+        block-Jacobi or, when given, by the dense SPD blocks `preconditioner` (float64, d x d per block, as
+        LearnedPreconditioner.blocks returns them). x is updated in place and returned with the run's PCGResult."""
+        if preconditioner is not None:
+            _dev(preconditioner, "preconditioner", self.ndiag, torch.float64)
+        check(_lib.gpu().bls_pcg_set_preconditioner(self.handle, dptr(preconditioner)))
+        try:
+            return self._solve(S, g, x, tol=tol, maxit=maxit, graph=graph)
+        finally:
+            _lib.gpu().bls_pcg_set_preconditioner(self._h, None)
+
+    def _solve(self, S, g, x, *, tol, maxit, graph):
         T = self._S(S)
         nr = self.structure.nr
         _dev(g, "g", nr, torch.float64)

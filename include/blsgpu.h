@@ -48,6 +48,7 @@ typedef struct bls_qr_structure bls_qr_structure;
 typedef struct bls_qr_plan bls_qr_plan;
 typedef struct bls_pcg_plan bls_pcg_plan;
 typedef struct bls_block_jacobi bls_block_jacobi;
+typedef struct bls_gnn bls_gnn;
 
 int bls_version(void);
 /* Message of the last error on the calling thread. */
@@ -295,6 +296,38 @@ int bls_pcg_solve(bls_pcg_plan* plan, int dtype, const void* S_nzval_dev, const 
                   int64_t maxit, int use_graph, int64_t* iterations, double* rel_residual, int64_t* failed_block);
 /* Device kernel launches issued on this plan since the previous call (no counterpart in the reference). */
 int64_t bls_pcg_plan_counters(bls_pcg_plan* plan);
+/* Replace the block-Jacobi solve in later bls_pcg_solve calls by z_b = B_b r_b with the dense symmetric positive definite
+ * blocks B (double, d_r x d_r column-major per retained block, block after block, in device memory the caller keeps);
+ * NULL restores block-Jacobi. */
+int bls_pcg_set_preconditioner(bls_pcg_plan* plan, const double* blocks_dev);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Learned block preconditioner (no counterpart in the reference): a 3-layer, width-64 graph network over the camera
+ * covisibility graph of S that predicts a lower-triangular correction T_b per 6 x 6 block; the preconditioner block is
+ * L_b^-T (I + T_b)' (I + T_b) L_b^-1 with L_b the Cholesky factor of S_bb (T = 0 is block-Jacobi). Parameters: a float
+ * vector of bls_gnn_param_count() entries (layout in csrc/gnn.cu). Retained blocks must all be 6 x 6.
+ * ------------------------------------------------------------------------------------------------------------- */
+int64_t bls_gnn_param_count(void);
+int bls_gnn_create(bls_pcg_plan* plan, const int64_t* block_colptr, const int64_t* block_rowval, const int64_t* block_row_offsets,
+                   const int64_t* col_heights, const int64_t* S_colptr, bls_gnn** out);
+int bls_gnn_destroy(bls_gnn* g);
+/* Graph features of S (its block-Jacobi factors, normalised couplings, node features). BLS_NOT_PD: a diagonal block of S
+ * is not positive definite (failed_block, 1-based). */
+int bls_gnn_prepare(bls_gnn* g, int dtype, const void* S_nzval_dev, int64_t* failed_block);
+/* Inference (bf16 != 0: BF16 activations and weights, FP32 accumulation; else FP32): the preconditioner blocks
+ * (36 doubles per retained block) into blocks_dev. */
+int bls_gnn_forward(bls_gnn* g, const float* params_dev, int bf16, double* blocks_dev);
+/* Copies of the last forward's outputs t (21 floats per block), the node features (8 floats per block) and the edge
+ * weights (one double per stored off-diagonal block); any may be NULL. */
+int bls_gnn_outputs(bls_gnn* g, float* t_dev, float* features_dev, double* edge_norms_dev);
+int64_t bls_gnn_edge_count(bls_gnn* g);
+/* Training loss mean_p ||G S^ G' z_p - z_p||^2 / ||z_p||^2 (S^ = L^-1 S L^-T) over nprobes probe vectors (double,
+ * nr each, one after another) and its gradient (float, bls_gnn_param_count() entries, overwritten). FP32 network. */
+int bls_gnn_loss_grad(bls_gnn* g, int dtype, const void* S_nzval_dev, const float* params_dev, const double* probes_dev,
+                      int64_t nprobes, double* loss, float* grad_dev);
+/* One Adam step on n parameters (step counts from 1). */
+int bls_adam_step(bls_ctx* ctx, float* params_dev, const float* grad_dev, float* m_dev, float* v_dev, int64_t n, float lr,
+                  float beta1, float beta2, float eps, int64_t step);
 
 /* copyto!(csc, bsm, scatter_map) (src/SparseBlockLinearSystem.jl:356-362): dest[i] = src[map[i]], i < n. */
 int bls_scatter_copy(bls_ctx* ctx, int dtype, void* dest_dev, const void* src_dev, const int64_t* map_dev, int64_t n);
