@@ -436,6 +436,140 @@ def run_ours_pcg(args, rank: int, world: int) -> dict | None:
 _LAST: dict = {}
 
 
+def run_ours_batch(args, rank: int, world: int) -> dict | None:
+    """The batched workload: 256 independent problems of uneven sizes, each with its own lambda, reduced as one plan
+    over the disjoint union of their layouts; a step is one replay of the CUDA graph holding reset + reduce of the whole
+    batch (mixed form), with the phase-2 schedule picked by the autotuner."""
+    import torch
+    bls = load_package()
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    nprob = 256
+    problems = []
+    for i in range(nprob):
+        spec = bls.scenes.workload(args.workload, i + (1000 * rank if world > 1 else 0))
+        problems.append(bls.scenes.hessian_problem(spec))
+    flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=dev)
+
+    def timed(B):
+        for _ in range(args.warmup):
+            B.step()
+        assert B.ok()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        B.ws.counters()
+        evs = []
+        for _ in range(args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            B.step()
+            b.record()
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        assert B.ok()
+        total = sum(a.elapsed_time(b) for a, b in evs)
+        if world > 1:
+            t = torch.tensor([total], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            total = float(t.item())
+        return total
+
+    B64 = bls.batch.BatchedReduction(problems, torch.float64, device=dev.index)
+    tunes64 = B64.autotune()
+    B64.capture()
+    ms64 = timed(B64)
+    S64 = B64.S.cpu().numpy()
+    del B64
+    B = bls.batch.BatchedReduction(problems, torch.float32, device=dev.index)
+    tunes = B.autotune()
+    B.ws.counters()
+    B.run(sync=False)
+    per_step = B.ws.counters()["launches"]   # the kernels one step launches (the graph holds the same kernels)
+    B.capture()
+    with ClockSampler(dev.index) as clk:
+        ms32 = timed(B)
+    # per-problem error of the mixed result against the FP64 reduction of the same problem (FP64 inputs)
+    S32 = B.S.double().cpu().numpy()
+    errs = []
+    for i in range(nprob):
+        a, b = int(B.off["nnz"][i]), int(B.off["nnz"][i + 1])
+        errs.append(float(np.linalg.norm(S32[a:b] - S64[a:b]) / np.linalg.norm(S64[a:b])))
+    # end to end: every input from pinned host memory, S and g back, through one graph replay per step
+    host = {k: getattr(B, k).cpu().pin_memory() for k in ("E", "C", "R", "b_r", "b_e", "sc_r", "sc_e")}
+    hS = torch.empty_like(B.S, device="cpu").pin_memory()
+    hg = torch.empty_like(B.g, device="cpu").pin_memory()
+
+    def e2e_step():
+        for k, v in host.items():
+            getattr(B, k).copy_(v, non_blocking=True)
+        B.step()
+        hS.copy_(B.S, non_blocking=True)
+        hg.copy_(B.g, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        e2e_step()
+    b.record()
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b)
+    assert B.ok()
+    if rank != 0:
+        return None
+    nobs = B.nobs
+    out = {
+        "metric": METRIC, "value": world * nobs * args.steps / (ms32 / 1e3), "unit": "obs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 storage/accumulation + f64 point inverse, z, gradient", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": args.workload, "problems": nprob, "cameras": int(B.U.nrblocks), "points": int(B.U.neblocks),
+                   "observations": nobs, "nnz_S": int(B.U.nnz), "parallelism": f"replicas x{world}",
+                   "l2": "flushed between timed steps (256 MB write)",
+                   "step": "one CUDA graph replay: reset_schur_sparse + reduce_schur_sparse of all problems (disjoint-union plan)"},
+        "schedule": {"chosen": B.schedule, "autotune_ms": tunes, "fp64_chosen": min(tunes64, key=tunes64.get), "fp64_autotune_ms": tunes64},
+        "fp64": {"value": world * nobs * args.steps / (ms64 / 1e3), "unit": "obs/s", "ms_per_step": ms64 / args.steps},
+        "per_problem_error_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "norm": "||S_mixed - S_fp64|| / ||S_fp64|| per problem"},
+        "e2e": {"value": world * nobs * args.steps / (e2e_ms / 1e3), "unit": "obs/s",
+                "h2d_bytes_per_step": int(sum(v.numel() * v.element_size() for v in host.values())),
+                "d2h_bytes_per_step": int(hS.numel() * 4 + hg.numel() * 8)},
+        "gpu_launches": per_step * args.steps,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_batch(problems, args.workload, seconds=args.cpu_seconds)
+    return out
+
+
+def cpu_baseline_batch(problems, workload: str, seconds: float = 10.0) -> dict:
+    """The reference algorithm (oracle) on every host core, FP64: each problem reset + reduced in turn."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    bls = load_package()
+    cores = os.cpu_count() or 1
+    prepared = []
+    for p in problems:
+        sc = bls.scenes.Scene(p.spec)
+        bs, el, ptr, idx = sc.description()
+        ost = orc.Structure.from_description(bs, (ptr, idx), el, nchunks=cores, min_work=4096)
+        opat = orc.Pattern(ost)
+        prepared.append((p, ost, opat, orc.Work(ost, cores, False), np.zeros(opat.nnz), np.zeros(ost.nr)))
+    n, nobs, t0 = 0, 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds or n < 1:
+        for p, ost, opat, w, S, g in prepared:
+            orc.reset_schur_sparse(ost, opat, S, p.R, p.scaling_r, p.lam)
+            ok, _ = orc.reduce_schur_sparse(ost, opat, w, S, g, p.b_r, p.b_e, p.scaling_e, p.lam, p.E, p.C, nthreads=cores)
+            assert ok
+            nobs += p.nobs
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": nobs / dt, "unit": "obs/s", "cores": cores, "kind": "port",
+            "sample": f"{n} x all {len(problems)} problems reset + reduced in turn, FP64, {cores} OpenMP threads ({dt:.1f} s)"}
+
+
 def cpu_baseline_pcg(p, workload: str) -> dict:
     """The oracle's PCG (the same algorithm on every host core) on the FP64 reduced system of the same scene."""
     orc, _, ost, opat, cores = oracle_problem(load_package().scenes.workload(workload), p)
@@ -537,6 +671,8 @@ def main():
             out = run_ours_qr(args, rank, world)
         elif args.workload.startswith("pcg_"):
             out = run_ours_pcg(args, rank, world)
+        elif args.workload.startswith("batched_"):
+            out = run_ours_batch(args, rank, world)
         else:
             out = run_ours(args, rank, world)
     finally:

@@ -10,6 +10,7 @@ QR elimination:          SchurJacobianStructure, SchurBlockJacobian, QRReduction
                          reduced_normal_sparse / reduced_normal_dense, reduced_diagonal_blocks, free_block_pairs
 Reduced solve:           BlockJacobi, factor_diagonal_blocks, solve_diagonal_blocks, PCGWorkspace (block-Jacobi PCG)
 Learned preconditioner:  gnn.LearnedPreconditioner, gnn.train, gnn.init_params
+Batches:                 batch.BatchedReduction (uneven problems as one plan, one CUDA graph)
 Workloads:               scenes.workload, scenes.hessian_problem, scenes.jacobian_problem
 """
 from ._lib import ArgumentError, BlsError, DimensionMismatch
@@ -19,7 +20,7 @@ from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce
 from .qr import (QRReductionWorkspace, SchurBlockJacobian, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
                  reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse)
 from .pcg import BlockJacobi, PCGResult, PCGWorkspace, factor_diagonal_blocks, solve_diagonal_blocks
-from . import gnn, scenes
+from . import batch, gnn, scenes
 
 __all__ = [
     "ArgumentError", "BlsError", "DimensionMismatch", "DEFAULT_MIN_WORK", "SchurPattern", "SchurStructure", "build_r_to_s_map",
@@ -27,5 +28,5 @@ __all__ = [
     "reduce_schur_sparse", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
     "SchurBlockJacobian", "SchurJacobianStructure", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
     "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "BlockJacobi", "PCGResult", "PCGWorkspace",
-    "factor_diagonal_blocks", "solve_diagonal_blocks", "gnn",
+    "factor_diagonal_blocks", "solve_diagonal_blocks", "gnn", "batch",
 ]
