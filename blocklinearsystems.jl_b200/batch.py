@@ -6,8 +6,8 @@ indices, coupling and point-block offsets, S positions, the r -> s map), so one 
 every problem: the union's S is block diagonal by problem, and each kernel launch spans the whole batch. Each
 problem's damping lambda_p is folded into its scalings (lambda_p * scaling, formed in FP64 exactly as the kernels form
 lambda * scaling; the batch runs with lambda = 1), so every problem's result is the one its own call would give.
-autotune() times the phase-2 schedules (block-owned pair work lists, or block-column-owned tiles) on the batch and
-keeps the faster; capture() records reset + reduce of the batch as one CUDA graph that step() replays.
+autotune() times the phase-2 schedules (block-owned pair work lists with six lanes or one lane per pair, block-column
+owned tiles with a warp per visit or with visits staged in chunks) on the batch and keeps the fastest; capture() records reset + reduce of the batch as one CUDA graph that step() replays.
 """
 from __future__ import annotations
 
@@ -126,7 +126,7 @@ class BatchedReduction:
     def autotune(self, reps: int = 5) -> dict:
         """Time each phase-2 schedule on the batch (after a warm-up run) and keep the faster."""
         times = {}
-        for name in ("pairs", "columns"):
+        for name in ("pairs", "columns", "lanes", "tiles"):
             self.ws.set_kernel(name)
             self.run()
             torch.cuda.synchronize()

@@ -61,6 +61,7 @@ struct SchurPlan {
   // camera's row offset in the column's tile; per column the S index of its first entry
   DevBuf vis_rec, vis_base, vis_off, col_base, col_h;
   int64_t max_col_h = 0;
+  bool tiles_ok = false;   // every point's coupling span fits the staging buffer of k_tiles36
   int kernel = 1;   // 0: column-owned (k_columns36), 1: block-owned pairs (k_pairs36, the default: faster on sparse scenes)
   // reset
   DevBuf r_to_s, diag_inds, S_rowval, S_col;
@@ -359,7 +360,7 @@ __global__ void k_g_init(double* __restrict__ g, const double* __restrict__ b_r,
 // block's items also subtract C_c2' z from g_S (each coupling of r2 is exactly one diagonal pair).
 template <class T>
 __global__ void __launch_bounds__(128) k_pairs36(
-    int64_t nitems, const int32_t* __restrict__ item_block, const int32_t* __restrict__ item_start, const int32_t* __restrict__ item_info,
+    int64_t nitems, int64_t ncoup, const int32_t* __restrict__ item_block, const int32_t* __restrict__ item_start, const int32_t* __restrict__ item_info,
     const int2* __restrict__ pairs, const int32_t* __restrict__ block_r1, const int32_t* __restrict__ block_r2,
     const int64_t* __restrict__ block_base, const int32_t* __restrict__ block_stride, int64_t dense_nr, const T* __restrict__ C,
     const typename EinvOf<T>::type* __restrict__ Einv12, const double* __restrict__ z, const double* __restrict__ s_r,
@@ -402,6 +403,18 @@ __global__ void __launch_bounds__(128) k_pairs36(
       const double2* q = reinterpret_cast<const double2*>(C + 18 * (int64_t)c1);
 #pragma unroll
       for (int i = 0; i < 9; ++i) { double2 v = __ldg(q + i); c1v[2 * i] = v.x; c1v[2 * i + 1] = v.y; }
+    } else if ((reinterpret_cast<uintptr_t>(C + 18 * (int64_t)c1) & 8) ? c1 > 0 : c1 + 1 < ncoup) {
+      // five 16-byte loads from the 16-byte boundary at or below the block (C is 8-byte aligned, so the block starts
+      // on a boundary or 8 bytes past one), then its 18 floats at shift 0 or 2. The 20 floats read stay inside C: a
+      // shifted read starts in the block before (so not for the first coupling), an unshifted one ends in the block
+      // after (so not for the last); those two take the 8-byte path below
+      const int sh = (reinterpret_cast<uintptr_t>(C + 18 * (int64_t)c1) & 8) ? 2 : 0;
+      const float4* q = reinterpret_cast<const float4*>(C + 18 * (int64_t)c1 - sh);
+      float w[20];
+#pragma unroll
+      for (int i = 0; i < 5; ++i) { float4 v = __ldg(q + i); w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w; }
+#pragma unroll
+      for (int i = 0; i < 18; ++i) c1v[i] = sh ? w[i + 2] : w[i];
     } else {
       const float2* q = reinterpret_cast<const float2*>(C + 18 * (int64_t)c1);
 #pragma unroll
@@ -443,6 +456,162 @@ __global__ void __launch_bounds__(128) k_pairs36(
   if (diag) {
     if (solo) g[6 * r2 + w] -= gacc;
     else atomicAdd(g + 6 * r2 + w, -gacc);
+  }
+}
+
+// Phase 2 for d_r = 6, d_e = 3, pair-per-lane form with staged operands: one warp per work item (an S block and up
+// to 32 of its pairs). The warp first copies the item's operands into shared memory with cp.async, consecutive lanes
+// taking consecutive 8-byte chunks of one span (C_c1 and C_c2, 72 bytes each, and the point's padded E^-1), so a copy
+// instruction covers a few contiguous spans instead of 32 scattered ones. Then lane i takes pair i whole from shared
+// memory (a conflict-free stride of 50 words per pair): U = E^-1 C_c2 (3 x 6) and C_c1' U (the full 6 x 6 block, 108
+// FMAs) into 36 register accumulators. The warp sums the lanes' blocks by a reduce-scatter (halving the 36 values over
+// lane distances 16 and 8, then a butterfly of the remaining 9 over 4, 2, 1); the lanes with (lane & 7) == 0 write the
+// 9 entries of their quarter: plain read-modify-write when the block has a single item, an atomic add otherwise.
+// Diagonal items also sum C_c2' z for g_S.
+template <class T>
+__device__ __forceinline__ T shfl_x(T v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+
+template <class T>
+__global__ void __launch_bounds__(128) k_pairs_lane(
+    int64_t nitems, const int32_t* __restrict__ item_block, const int32_t* __restrict__ item_start, const int32_t* __restrict__ item_info,
+    const int2* __restrict__ pairs, const int32_t* __restrict__ block_r1, const int32_t* __restrict__ block_r2,
+    const int64_t* __restrict__ block_base, const int32_t* __restrict__ block_stride, int64_t dense_nr, const T* __restrict__ C,
+    const typename EinvOf<T>::type* __restrict__ Einv12, const double* __restrict__ z, T* __restrict__ S, double* __restrict__ g,
+    const Status* __restrict__ st) {
+  using TE = typename EinvOf<T>::type;
+  // per pair: C_c1 (18 T), C_c2 (18 T), E^-1 (12 TE), padding; in 8-byte words
+  constexpr int WT = (int)sizeof(T) / 4;                     // 4-byte words per T
+  constexpr int CW = 18 * WT, EW = 12 * (int)sizeof(TE) / 4;  // words of one C block, of E^-1
+  constexpr int PW = 2 * CW + EW + 2;                        // words per pair (50 in FP32, 98 in FP64)
+  constexpr int NCH = (2 * CW + EW) / 2;                     // 8-byte chunks per pair
+  constexpr int NWARP = sizeof(T) == 4 ? 4 : 3;              // warps per CTA (the FP64 staging is twice as large)
+  __shared__ __align__(16) uint32_t stg[NWARP][32 * PW];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t it = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (it >= nitems) return;
+  if (!live(st)) return;
+  const int k = __ldg(item_block + it), pb = __ldg(item_start + it), info = __ldg(item_info + it);
+  const int cnt = info & 0xffff;
+  const bool solo = (info >> 16) != 0;
+  const int r1 = __ldg(block_r1 + k), r2 = __ldg(block_r2 + k);
+  const bool diag = r1 == r2;
+  uint32_t* sw = stg[warp];
+  int2 mine = make_int2(0, 0);
+  if (lane < cnt) mine = __ldg(pairs + pb + lane);
+  // chunk q of the item's copies: pair q / NCH (its record fetched from the lane holding it), 8-byte chunk q % NCH
+  for (int q0 = 0; q0 < cnt * NCH; q0 += 32) {
+    const int q = q0 + lane;
+    const int pr = min(q / NCH, 31), sub = q - (q / NCH) * NCH;
+    const int c1 = __shfl_sync(0xffffffffu, mine.x, pr), ey = __shfl_sync(0xffffffffu, mine.y, pr);
+    if (q < cnt * NCH) {
+      const int e = ey & 0xffffff, c2 = c1 + (ey >> 24);
+      const char* src;
+      if (sub < CW / 2) src = reinterpret_cast<const char*>(C + 18 * (int64_t)c1) + 8 * sub;
+      else if (sub < CW) src = reinterpret_cast<const char*>(C + 18 * (int64_t)c2) + 8 * (sub - CW / 2);
+      else src = reinterpret_cast<const char*>(Einv12 + 12 * (int64_t)e) + 8 * (sub - CW);
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(sw + pr * PW + 2 * sub);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncwarp();
+  T acc[36];
+#pragma unroll
+  for (int i = 0; i < 36; ++i) acc[i] = T(0);
+  double gacc[6] = {0, 0, 0, 0, 0, 0};
+  if (lane < cnt) {
+    const uint32_t* pw = sw + lane * PW;
+    T a[18], b[18];
+    TE ei[12];
+    const T* pa = reinterpret_cast<const T*>(pw);
+    const T* pbv = reinterpret_cast<const T*>(pw + CW);
+    const TE* pe = reinterpret_cast<const TE*>(pw + 2 * CW);
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        const float2 va = reinterpret_cast<const float2*>(pa)[i], vb = reinterpret_cast<const float2*>(pbv)[i];
+        a[2 * i] = va.x; a[2 * i + 1] = va.y; b[2 * i] = vb.x; b[2 * i + 1] = vb.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        const float2 v = reinterpret_cast<const float2*>(pe)[i];
+        ei[2 * i] = v.x; ei[2 * i + 1] = v.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 18; ++i) { a[i] = pa[i]; b[i] = pbv[i]; }
+#pragma unroll
+      for (int i = 0; i < 12; ++i) ei[i] = pe[i];
+    }
+#pragma unroll
+    for (int w = 0; w < 6; ++w) {
+      T u[3];
+#pragma unroll
+      for (int t = 0; t < 3; ++t) u[t] = (T)(ei[t] * (TE)b[3 * w] + ei[t + 3] * (TE)b[3 * w + 1] + ei[t + 6] * (TE)b[3 * w + 2]);
+#pragma unroll
+      for (int rho = 0; rho < 6; ++rho) acc[6 * w + rho] = acc[6 * w + rho] + a[3 * rho] * u[0] + a[3 * rho + 1] * u[1] + a[3 * rho + 2] * u[2];
+    }
+    if (diag) {
+      const int e = mine.y & 0xffffff;
+      const double* zp = z + 3 * (int64_t)e;
+      const double z0 = zp[0], z1 = zp[1], z2 = zp[2];
+#pragma unroll
+      for (int w = 0; w < 6; ++w) gacc[w] = (double)b[3 * w] * z0 + (double)b[3 * w + 1] * z1 + (double)b[3 * w + 2] * z2;
+    }
+  }
+  // reduce-scatter of the 36 accumulators: lanes with bit 4 set keep entries 18..35, then bit 3 splits each half
+  T h[18];
+  const bool up16 = (lane & 16) != 0;
+#pragma unroll
+  for (int i = 0; i < 18; ++i) {
+    const T send = up16 ? acc[i] : acc[i + 18];
+    const T keep = up16 ? acc[i + 18] : acc[i];
+    h[i] = keep + shfl_x(send, 16);
+  }
+  T q9[9];
+  const bool up8 = (lane & 8) != 0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const T send = up8 ? h[i] : h[i + 9];
+    const T keep = up8 ? h[i + 9] : h[i];
+    q9[i] = keep + shfl_x(send, 8);
+  }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    T v = q9[i];
+    v += shfl_x(v, 4);
+    v += shfl_x(v, 2);
+    v += shfl_x(v, 1);
+    q9[i] = v;
+  }
+  if ((lane & 7) == 0) {
+    const int base_idx = (up16 ? 18 : 0) + (up8 ? 9 : 0);
+    const int64_t stride = block_stride ? (int64_t)__ldg(block_stride + k) : dense_nr;
+    T* blk = S + __ldg(block_base + k);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const int idx = base_idx + i, w = idx / 6, rho = idx - 6 * w;
+      if (diag && rho > w) continue;
+      T* dst = blk + w * stride + rho;
+      if (solo) *dst = *dst - q9[i];
+      else atomicAdd(dst, -q9[i]);
+    }
+  }
+  if (diag) {
+#pragma unroll
+    for (int w = 0; w < 6; ++w) {
+      double v = gacc[w];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      gacc[w] = v;
+    }
+    if (lane < 6) {
+      double v = 0.0;
+#pragma unroll
+      for (int w = 0; w < 6; ++w)
+        if (w == lane) v = gacc[w];
+      if (solo) g[6 * r2 + lane] -= v;
+      else atomicAdd(g + 6 * r2 + lane, -v);
+    }
   }
 }
 
@@ -550,6 +719,154 @@ __global__ void __launch_bounds__(256) k_columns36(
     const int gi = 6 * r2 + threadIdx.x;
     const double bv = s_r ? b_r[gi] * s_r[gi] : b_r[gi];
     g[gi] = bv - a;
+  }
+}
+
+// Phase 2 for d_r = 6, d_e = 3, sparse S, no conditioning scales: block-column owned and staged in chunks. One CTA
+// per retained block r2 holds the column's S blocks (H x 6) in shared memory. Its visits (the points seen from r2, in
+// the reference's retained_entry order) are processed in chunks of up to 32: warp 0 sizes a chunk so that the
+// visits' coupling spans C_p0 .. C_c2 (contiguous in C) fit the staging buffer, and every warp copies whole spans,
+// E^-1 and z into shared memory with cp.async (all of a chunk's loads in flight together). Then each warp takes whole
+// visits: lanes 0-17 form U = E^-1 C_c2 (3 x 6) into the warp's slot, lanes 0-5 add C_c2' z to their gradient
+// registers, and lanes (i, rho) add row rho of C_i' U to the tile (shared-memory atomic adds: other warps' visits may
+// share a block). Two barriers per chunk; S and g_S are written once.
+template <class T>
+__global__ void __launch_bounds__(256) k_tiles36(
+    const int32_t* __restrict__ retained_ptr, const int2* __restrict__ vis_rec, const int32_t* __restrict__ vis_base,
+    const uint16_t* __restrict__ vis_off, const int64_t* __restrict__ col_base, const int32_t* __restrict__ col_h, int cap,
+    const T* __restrict__ C, const typename EinvOf<T>::type* __restrict__ Einv12, const double* __restrict__ z,
+    const double* __restrict__ b_r, T* __restrict__ S, double* __restrict__ g, const Status* __restrict__ st) {
+  using TE = typename EinvOf<T>::type;
+  constexpr int NV = 32, NW = 8;
+  extern __shared__ __align__(16) unsigned char tiles_smem[];
+  const int r2 = blockIdx.x;
+  if (!live(st)) return;
+  const int H = __ldg(col_h + r2);
+  const int64_t cb = __ldg(col_base + r2);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned char* ptr = tiles_smem;
+  double* zv = reinterpret_cast<double*>(ptr); ptr += sizeof(double) * NV * 3;
+  double* gs = reinterpret_cast<double*>(ptr); ptr += sizeof(double) * NW * 6;
+  TE* ein = reinterpret_cast<TE*>(ptr); ptr += sizeof(TE) * NV * 12;
+  T* U = reinterpret_cast<T*>(ptr); ptr += sizeof(T) * NW * 20;
+  int* m_soff = reinterpret_cast<int*>(ptr); ptr += sizeof(int) * NV;
+  int* m_j = reinterpret_cast<int*>(ptr); ptr += sizeof(int) * NV;
+  int* m_vb = reinterpret_cast<int*>(ptr); ptr += sizeof(int) * NV;
+  int* m_p0 = reinterpret_cast<int*>(ptr); ptr += sizeof(int) * NV;
+  int* m_e = reinterpret_cast<int*>(ptr); ptr += sizeof(int) * NV;
+  int* m_n = reinterpret_cast<int*>(ptr); ptr += sizeof(int) * 4;
+  ptr = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(ptr) + 15) & ~uintptr_t(15));
+  T* stage = reinterpret_cast<T*>(ptr); ptr += sizeof(T) * cap;
+  T* tile = reinterpret_cast<T*>(ptr);
+  T* Uw = U + 20 * warp;
+  for (int i = tid; i < 6 * H; i += blockDim.x) tile[i] = T(0);
+  double gacc = 0.0;   // lanes 0-5: this warp's share of g_S entry 6 r2 + lane
+  const int q1 = __ldg(retained_ptr + r2 + 1);
+  int q = __ldg(retained_ptr + r2);
+  __syncthreads();
+  while (q < q1) {
+    if (warp == 0) {
+      // size the chunk: the longest prefix of the next 32 visits whose spans fit the staging buffer (at least one)
+      const int qq = q + lane;
+      int2 rec = make_int2(0, 0);
+      int vb = 0, sz = 0, j = 0;
+      if (qq < q1) {
+        rec = __ldg(vis_rec + qq);
+        vb = __ldg(vis_base + qq);
+        j = rec.y >> 24;
+        sz = 18 * (j + 1);
+      }
+      int ssum = sz;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int a = __shfl_up_sync(0xffffffffu, ssum, o);
+        if (lane >= o) ssum += a;
+      }
+      const bool fits = qq < q1 && (ssum <= cap || lane == 0);
+      const int nv = __popc(__ballot_sync(0xffffffffu, fits));
+      if (lane < nv) {
+        m_soff[lane] = ssum - sz;
+        m_j[lane] = j;
+        m_vb[lane] = vb;
+        m_p0[lane] = rec.x;
+        m_e[lane] = rec.y & 0xffffff;
+      }
+      if (lane == 0) m_n[0] = nv;
+    }
+    __syncthreads();
+    const int nv = m_n[0];
+    // stage every visit's span C_p0 .. C_c2, E^-1 and z: a warp per visit, all copies in flight together
+    for (int v = warp; v < nv; v += NW) {
+      const int n = 18 * (m_j[v] + 1);
+      const T* src = C + 18 * (int64_t)m_p0[v];
+      T* dst = stage + m_soff[v];
+      if (sizeof(T) == 4) {
+        for (int x = lane; x < n / 2; x += 32) {
+          const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + 2 * x);
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src + 2 * x) : "memory");
+        }
+      } else {
+        for (int x = lane; x < n; x += 32) {
+          const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + x);
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src + x) : "memory");
+        }
+      }
+      const int e = m_e[v];
+      if (lane < 12) {
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(ein + 12 * v + lane);
+        if (sizeof(TE) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(Einv12 + 12 * (int64_t)e + lane) : "memory");
+        else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(Einv12 + 12 * (int64_t)e + lane) : "memory");
+      } else if (lane < 15) {
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(zv + 3 * v + (lane - 12));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(z + 3 * (int64_t)e + (lane - 12)) : "memory");
+      }
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    // a warp per visit
+    for (int v = warp; v < nv; v += NW) {
+      const int j = m_j[v];
+      const T* span = stage + m_soff[v];
+      const T* c2 = span + 18 * j;
+      if (lane < 18) {
+        const int t = lane / 6, w = lane - 6 * t;
+        const TE* ei = ein + 12 * v;
+        Uw[lane] = (T)(ei[t] * (TE)c2[3 * w] + ei[t + 3] * (TE)c2[3 * w + 1] + ei[t + 6] * (TE)c2[3 * w + 2]);
+      }
+      if (lane < 6) gacc += (double)c2[3 * lane] * zv[3 * v] + (double)c2[3 * lane + 1] * zv[3 * v + 1] + (double)c2[3 * lane + 2] * zv[3 * v + 2];
+      __syncwarp();
+      T u[18];
+#pragma unroll
+      for (int x = 0; x < 18; ++x) u[x] = Uw[x];
+      const int vb = m_vb[v], nrow = 6 * (j + 1);
+      for (int r = lane; r < nrow; r += 32) {
+        const int i = r / 6, rho = r - 6 * i;
+        const T* crow = span + 18 * i + 3 * rho;
+        const T a0 = crow[0], a1 = crow[1], a2 = crow[2];
+        T* trow = tile + (int)__ldg(vis_off + vb + i) + rho;
+        const bool diag = i == j;
+#pragma unroll
+        for (int w = 0; w < 6; ++w) {
+          if (diag && rho > w) continue;
+          atomicAdd(trow + w * H, a0 * u[w] + a1 * u[6 + w] + a2 * u[12 + w]);
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    q += nv;
+  }
+  if (lane < 6) gs[6 * warp + lane] = gacc;
+  __syncthreads();
+  for (int i = tid; i < 6 * H; i += blockDim.x) {
+    const int w = i / H, row = i - w * H;
+    T* p = S + cb + (int64_t)w * H + row;
+    *p = *p - tile[i];
+  }
+  if (tid < 6) {
+    double a = 0.0;
+    for (int w = 0; w < NW; ++w) a += gs[6 * w + tid];
+    g[6 * r2 + tid] = b_r[6 * r2 + tid] - a;
   }
 }
 
@@ -840,6 +1157,11 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
   upload(P->block_base_sparse, b_base, s);
   upload(P->block_base_dense, b_base_dense, s);
   if (P->fast36) {
+    {
+      int64_t kmax = 0;
+      for (int64_t e = 0; e < neb; ++e) kmax = std::max<int64_t>(kmax, d->eliminated_ptr[e + 1] - d->eliminated_ptr[e]);
+      P->tiles_ok = P->has_sparse && 18 * kmax <= 2048;
+    }
     upload(P->vis_rec, vrec, s);
     upload(P->vis_base, vbase, s);
     upload(P->vis_off, voff, s);
@@ -1007,6 +1329,33 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
                                               P->vis_off.as<uint16_t>(), P->entry_retained.as<int32_t>(), P->col_base.as<int64_t>(),
                                               P->col_h.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), b_r, s_r, s_e, S, g, st);
     if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
+  } else if (P->fast36 && P->kernel == 3 && !dense && !s_r && !s_e && P->tiles_ok) {
+    using TE = typename EinvOf<T>::type;
+    const int cap = (int)(sizeof(T) == 4 ? 4096 : 2048);
+    const size_t fixed = sizeof(double) * 32 * 3 + sizeof(double) * 8 * 6 + sizeof(TE) * 32 * 12 + sizeof(T) * 8 * 20 + sizeof(int) * (32 * 5 + 4) + 16;
+    const size_t smem = fixed + sizeof(T) * cap + sizeof(T) * 6 * P->max_col_h;
+    if (smem > 200 * 1024) throw Error(BLS_EUNSUPPORTED, "a block column of S exceeds the shared-memory tile of this build");
+    BLS_CUDA(cudaFuncSetAttribute(k_tiles36<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
+    P->launches += 1;
+    k_tiles36<T><<<(int)P->nrblocks, 256, smem, s>>>(P->retained_ptr.as<int32_t>(), P->vis_rec.as<int2>(), P->vis_base.as<int32_t>(),
+                                                     P->vis_off.as<uint16_t>(), P->col_base.as<int64_t>(), P->col_h.as<int32_t>(), cap, C,
+                                                     P->Einv12.as<TE>(), P->z.as<double>(), b_r, S, g, st);
+    if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
+  } else if (P->fast36 && P->kernel == 2 && !s_r && !s_e) {
+    using TE = typename EinvOf<T>::type;
+    k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st);
+    P->launches += 1;
+    if (P->nitems > 0) {
+      if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
+      P->launches += 1;
+      const int lane_threads = sizeof(T) == 4 ? 128 : 96;
+      k_pairs_lane<T><<<grid_for(P->nitems * 32, lane_threads), lane_threads, 0, s>>>(
+          P->nitems, P->item_block.as<int32_t>(), P->item_start.as<int32_t>(), P->item_info.as<int32_t>(), P->pair_packed.as<int2>(),
+          P->block_r1.as<int32_t>(), P->block_r2.as<int32_t>(), dense ? P->block_base_dense.as<int64_t>() : P->block_base_sparse.as<int64_t>(),
+          dense ? nullptr : P->block_stride_sparse.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), S, g, st);
+      if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
+    }
   } else if (P->fast36) {
     using TE = typename EinvOf<T>::type;
     k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st);
@@ -1016,7 +1365,7 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
       if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
       P->launches += 1;
       k_pairs36<T><<<grid_for(warps * 32, 128), 128, 0, s>>>(
-          P->nitems, P->item_block.as<int32_t>(), P->item_start.as<int32_t>(), P->item_info.as<int32_t>(), P->pair_packed.as<int2>(),
+          P->nitems, P->ncoup, P->item_block.as<int32_t>(), P->item_start.as<int32_t>(), P->item_info.as<int32_t>(), P->pair_packed.as<int2>(),
           P->block_r1.as<int32_t>(), P->block_r2.as<int32_t>(), dense ? P->block_base_dense.as<int64_t>() : P->block_base_sparse.as<int64_t>(),
           dense ? nullptr : P->block_stride_sparse.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), s_r, s_e, S, g, st);
       if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
@@ -1133,7 +1482,7 @@ int bls_reduce_schur_dense(bls_schur_plan* P, int dtype, void* S, double* g, con
 }
 
 int bls_schur_plan_set_kernel(bls_schur_plan* P, int which) {
-  if (!P || which < 0 || which > 1) return BLS_EINVAL;
+  if (!P || which < 0 || which > 3) return BLS_EINVAL;
   P->kernel = which;
   return BLS_OK;
 }

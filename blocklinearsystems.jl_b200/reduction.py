@@ -113,8 +113,10 @@ class SchurReductionWorkspace:
         return int(_lib.gpu().bls_schur_plan_device_bytes(self._h))
 
     def set_kernel(self, which: str) -> None:
-        """Phase-2 kernel of the 6/3 fast path: "pairs" (block owned, the default) or "columns" (block-column owned)."""
-        check(_lib.gpu().bls_schur_plan_set_kernel(self._h, {"columns": 0, "pairs": 1}[which]))
+        """Phase-2 kernel of the 6/3 fast path: "pairs" (block owned, six lanes per pair list, the default), "lanes"
+        (block owned, a lane per pair, a warp per pair list), "columns" (block-column owned, a warp per visit) or
+        "tiles" (block-column owned, visits staged in chunks; sparse S without conditioning scales, else "pairs")."""
+        check(_lib.gpu().bls_schur_plan_set_kernel(self._h, {"columns": 0, "pairs": 1, "lanes": 2, "tiles": 3}[which]))
 
     def instrument(self, timing: bool = True) -> None:
         """Bracket the pair kernel of each reduction with CUDA events (read them with counters())."""
