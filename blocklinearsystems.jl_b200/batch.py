@@ -7,7 +7,8 @@ every problem: the union's S is block diagonal by problem, and each kernel launc
 problem's damping lambda_p is folded into its scalings (lambda_p * scaling, formed in FP64 exactly as the kernels form
 lambda * scaling; the batch runs with lambda = 1), so every problem's result is the one its own call would give.
 autotune() times the phase-2 schedules (block-owned pair work lists with six lanes or one lane per pair, block-column
-owned tiles with a warp per visit or with visits staged in chunks) on the batch and keeps the fastest; capture() records reset + reduce of the batch as one CUDA graph that step() replays.
+owned tiles with a warp per visit or with visits staged in chunks) on the batch and keeps the fastest; capture()
+records reset + reduce of the batch as one CUDA graph that step() replays.
 """
 from __future__ import annotations
 
