@@ -205,9 +205,69 @@ __global__ void __launch_bounds__(256) k_factor(int64_t neb, const int32_t* __re
   }
 }
 
-// --- phase 2: one thread per work item of one S block ---
+// element type of the E^-1 copy the pair products read: FP32 in the mixed form, FP64 otherwise
 template <class T> struct EinvOf { using type = double; };
 template <> struct EinvOf<float> { using type = float; };
+
+// factor_eliminated! for the fast path (d_e = 3, canonical layout: point e's E block at 9 e, its variables at 3 e):
+// the same per-point arithmetic as k_factor, with a block's 128 points staged through shared memory so that E, b_e,
+// scaling_e and s_e are read, and E^-1 (FP64), the padded E^-1 of the pair products and z are written, in contiguous
+// coalesced runs instead of one 36-72-byte run per thread. The FP32 copy of E^-1 that only the generic phase 2 reads
+// is not written.
+template <class T>
+__global__ void __launch_bounds__(128) k_factor36(int64_t neb, const T* __restrict__ E, const double* __restrict__ b_e,
+                                                  const double* __restrict__ scaling_e, double lambda, const double* __restrict__ s_e,
+                                                  double* __restrict__ Einv64, typename EinvOf<T>::type* __restrict__ Einv12,
+                                                  double* __restrict__ z, Status* st) {
+  using TE = typename EinvOf<T>::type;
+  constexpr int NB = 128;
+  __shared__ double sE[NB * 9];      // E in, then E^-1 out
+  __shared__ TE s12[NB * 12];
+  __shared__ double sb[NB * 3], ss[NB * 3], sse[NB * 3];
+  if (!args_ok(st)) return;          // the status word is the same for every thread of the block
+  const int64_t e0 = (int64_t)blockIdx.x * NB;
+  const int n = (int)(neb - e0 < NB ? neb - e0 : NB);
+  const int t = threadIdx.x;
+  for (int i = t; i < 9 * n; i += NB) sE[i] = (double)E[9 * e0 + i];
+  for (int i = t; i < 3 * n; i += NB) {
+    sb[i] = b_e[3 * e0 + i];
+    ss[i] = scaling_e[3 * e0 + i];
+    sse[i] = s_e ? s_e[3 * e0 + i] : 1.0;
+  }
+  __syncthreads();
+  if (t < n) {
+    double se[3], damp[3], H[9], inv[9];
+    for (int i = 0; i < 3; ++i) {
+      se[i] = sse[3 * t + i];
+      damp[i] = mul(mul(lambda, ss[3 * t + i]), mul(se[i], se[i]));
+    }
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i < 3; ++i) {
+        const double h = sE[9 * t + i + 3 * j];
+        H[i + 3 * j] = s_e ? mul(h, mul(se[i], se[j])) : h;
+      }
+    if (!inv_sym_closed(3, H, damp, inv)) {
+      atomicMin(&st->failed, (long long)(e0 + t));
+      for (int i = 0; i < 9; ++i) inv[i] = 0.0;
+    }
+    for (int i = 0; i < 9; ++i) {
+      sE[9 * t + i] = inv[i];
+      s12[12 * t + i] = (TE)inv[i];
+    }
+    for (int i = 9; i < 12; ++i) s12[12 * t + i] = TE(0);
+    for (int i = 0; i < 3; ++i) {
+      double acc = inv[i] * (sb[3 * t] * se[0]);
+      for (int j = 1; j < 3; ++j) acc = acc + inv[i + 3 * j] * (sb[3 * t + j] * se[j]);
+      ss[3 * t + i] = acc;     // z, in the slot of scaling_e (read above by this thread only)
+    }
+  }
+  __syncthreads();
+  for (int i = t; i < 9 * n; i += NB) Einv64[9 * e0 + i] = sE[i];
+  for (int i = t; i < 12 * n; i += NB) Einv12[12 * e0 + i] = s12[i];
+  for (int i = t; i < 3 * n; i += NB) z[3 * e0 + i] = ss[i];
+}
+
+// --- phase 2: one thread per work item of one S block ---
 
 template <class T>
 __device__ __forceinline__ void red_add(T* p, T v) { atomicAdd(p, v); }
@@ -1305,10 +1365,16 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
   Status* st = P->status.as<Status>();
   begin_checked(P, sc_e, P->ne, 1);
   k_arm<<<1, 1, 0, s>>>(st);
-  k_factor<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(P->neblocks, P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
-                                                         P->boffsets_e.as<int32_t>(), E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
-                                                         std::is_same<T, float>::value ? P->Einv32.as<float>() : nullptr, P->z.as<double>(),
-                                                         P->fast36 ? P->Einv12.p : nullptr, st);
+  if (P->fast36) {
+    using TE = typename EinvOf<T>::type;
+    k_factor36<T><<<grid_for(P->neblocks, 128), 128, 0, s>>>(P->neblocks, E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
+                                                             P->Einv12.as<TE>(), P->z.as<double>(), st);
+  } else {
+    k_factor<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(P->neblocks, P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
+                                                           P->boffsets_e.as<int32_t>(), E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
+                                                           std::is_same<T, float>::value ? P->Einv32.as<float>() : nullptr, P->z.as<double>(),
+                                                           nullptr, st);
+  }
   P->launches += 2;   // k_arm, k_factor
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (P->timing) {
