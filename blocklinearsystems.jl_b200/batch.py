@@ -127,7 +127,7 @@ class BatchedReduction:
     def autotune(self, reps: int = 5) -> dict:
         """Time each phase-2 schedule on the batch (after a warm-up run) and keep the faster."""
         times = {}
-        for name in ("pairs", "columns", "lanes", "tiles"):
+        for name in ("pairs", "columns", "lanes", "tiles", "points"):
             self.ws.set_kernel(name)
             self.run()
             torch.cuda.synchronize()

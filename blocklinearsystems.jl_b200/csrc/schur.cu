@@ -62,9 +62,15 @@ struct SchurPlan {
   DevBuf vis_rec, vis_base, vis_off, col_base, col_h;
   int64_t max_col_h = 0;
   bool tiles_ok = false;   // every point's coupling span fits the staging buffer of k_tiles36
+  DevBuf pt_rec;   // fast36, point-major pairs: {c1, k | (c2 - c1) << 25} per pair, k the S block
+  bool points_ok = false;
   int kernel = 1;   // 0: column-owned (k_columns36), 1: block-owned pairs (k_pairs36, the default: faster on sparse scenes)
   // reset
   DevBuf r_to_s, diag_inds, S_rowval, S_col;
+  // one-pass reset (k_reset_columns): per S entry the R entry it takes or -1, and S's column pointers; used when
+  // every diag_inds[i] lies in column i
+  DevBuf r_from, S_colptr;
+  bool reset_fused = false;
   // scratch: E^-1 (FP64, and FP32 for the mixed form), z, status
   DevBuf Einv64, Einv32, z, status;
   DevBuf Einv12;   // fast36: E^-1 per point in the element type of the pair products, padded to 12 entries (16-byte rows)
@@ -161,12 +167,84 @@ __global__ void k_reset_done(Status* st) {
   if (st->einval_r == NONE) st->failed = NONE;
 }
 
+// check_damping for short vectors in one block, without a separate clearing launch: the lowest index whose entry is
+// negative or not finite (NONE if none) is written to the slot (which = 0: scaling_r, 1: scaling_e).
+__global__ void __launch_bounds__(1024) k_check_scaling1(const double* __restrict__ sc, int64_t n, Status* st, int which) {
+  __shared__ long long lowest;
+  if (threadIdx.x == 0) lowest = NONE;
+  __syncthreads();
+  long long m = NONE;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const double x = sc[i];
+    if (!(isfinite(x) && x >= 0.0) && i < m) m = i;
+  }
+  if (m != NONE) atomicMin(&lowest, m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (which == 0) st->einval_r = lowest;
+    else st->einval_e = lowest;
+  }
+}
+
+// reset_schur_sparse! (src/schur_reduction.jl:416-436) in one pass: one warp per column j of S. Entry q takes
+// R[r_from[q]] (zero when no R entry maps there; r_from keeps the last entry of the map that does, as the reference's
+// loop leaves it), scaled by T(v * (s_r[row] * s_r[j])) when conditioned; then lane 0 damps the column's diagonal
+// entry diag_inds[j] (inside the column, so no other warp touches it). Warp 0 also clears the failure word, as the
+// reference's ws.failed_block[] = 0. scaling_r was checked by the kernel before.
+template <class T>
+__global__ void __launch_bounds__(256) k_reset_columns(T* __restrict__ S, const T* __restrict__ R, const int32_t* __restrict__ r_from,
+                                                     const int64_t* __restrict__ colptr, const int32_t* __restrict__ rowval,
+                                                     const int64_t* __restrict__ diag_inds, const double* __restrict__ sc, double lambda,
+                                                     const double* __restrict__ s_r, int64_t nr, Status* st) {
+  const int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (st->einval_r != NONE) return;
+  if (j == 0 && lane == 0) st->failed = NONE;
+  if (j >= nr) return;
+  const int64_t q0 = colptr[j], q1 = colptr[j + 1];
+  const double sj = s_r ? s_r[j] : 1.0;
+  for (int64_t q = q0 + lane; q < q1; q += 32) {
+    const int32_t i = r_from[q];
+    T v = i >= 0 ? R[i] : T(0);
+    if (s_r) v = T((double)v * (s_r[rowval[q]] * sj));
+    S[q] = v;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const int64_t d = diag_inds[j];
+    S[d] = T((double)S[d] + lambda * sc[j] * (sj * sj));
+  }
+}
+
+// reset_schur_dense! (src/schur_reduction.jl:389-407) in one pass: one warp per column j, S[:, j] = R[:, j] (scaled
+// by T(R * (s_r[i] * s_r[j])) when conditioned), then lane 0 damps S[j, j]; warp 0 clears the failure word.
+template <class T>
+__global__ void __launch_bounds__(256) k_reset_dense_columns(T* __restrict__ S, const T* __restrict__ R, const double* __restrict__ sc,
+                                                           double lambda, const double* __restrict__ s_r, int64_t nr, Status* st) {
+  const int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (st->einval_r != NONE) return;
+  if (j == 0 && lane == 0) st->failed = NONE;
+  if (j >= nr) return;
+  const double sj = s_r ? s_r[j] : 1.0;
+  for (int64_t i = lane; i < nr; i += 32) S[i + nr * j] = s_r ? T((double)R[i + nr * j] * (s_r[i] * sj)) : R[i + nr * j];
+  __syncwarp();
+  if (lane == 0) S[j + nr * j] = T((double)S[j + nr * j] + lambda * sc[j] * (sj * sj));
+}
+
+// The reduction's status for the 6/3 fast path: scaling_e is checked by k_factor36 itself, so its slot is cleared
+// here, and the failure word is cleared when the reset's arguments were valid.
+__global__ void k_arm36(Status* st) {
+  st->einval_e = NONE;
+  if (st->einval_r == NONE) st->failed = NONE;
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) k_factor(int64_t neb, const int32_t* __restrict__ e_dims, const int32_t* __restrict__ eoffsets,
                                                 const int32_t* __restrict__ boffsets_e, const T* __restrict__ E,
                                                 const double* __restrict__ b_e, const double* __restrict__ scaling_e, double lambda,
                                                 const double* __restrict__ s_e, double* __restrict__ Einv64, float* __restrict__ Einv32,
-                                                double* __restrict__ z, void* __restrict__ Einv12, Status* st) {
+                                                double* __restrict__ z, Status* st) {
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= neb) return;
   if (!args_ok(st)) return;
@@ -189,15 +267,6 @@ __global__ void __launch_bounds__(256) k_factor(int64_t neb, const int32_t* __re
     Einv64[eo + i] = inv[i];
     if (Einv32) Einv32[eo + i] = (float)inv[i];
   }
-  if (Einv12) {   // fast path: d_e = 3, rows of 12 entries in the pair products' type
-    if (Einv32) {
-      float* q = static_cast<float*>(Einv12) + 12 * e;
-      for (int i = 0; i < 9; ++i) q[i] = (float)inv[i];
-    } else {
-      double* q = static_cast<double*>(Einv12) + 12 * e;
-      for (int i = 0; i < 9; ++i) q[i] = inv[i];
-    }
-  }
   for (int i = 0; i < de; ++i) {
     double acc = inv[i] * (b_e[so] * se[0]);
     for (int j = 1; j < de; ++j) acc = acc + inv[i + de * j] * (b_e[so + j] * se[j]);
@@ -213,7 +282,8 @@ template <> struct EinvOf<float> { using type = float; };
 // the same per-point arithmetic as k_factor, with a block's 128 points staged through shared memory so that E, b_e,
 // scaling_e and s_e are read, and E^-1 (FP64), the padded E^-1 of the pair products and z are written, in contiguous
 // coalesced runs instead of one 36-72-byte run per thread. The FP32 copy of E^-1 that only the generic phase 2 reads
-// is not written.
+// is not written. It also applies check_damping to scaling_e (the lowest bad entry into the status word), so the
+// reduction needs no separate checking launch; the pair kernel that follows skips its work if any entry was bad.
 template <class T>
 __global__ void __launch_bounds__(128) k_factor36(int64_t neb, const T* __restrict__ E, const double* __restrict__ b_e,
                                                   const double* __restrict__ scaling_e, double lambda, const double* __restrict__ s_e,
@@ -224,14 +294,16 @@ __global__ void __launch_bounds__(128) k_factor36(int64_t neb, const T* __restri
   __shared__ double sE[NB * 9];      // E in, then E^-1 out
   __shared__ TE s12[NB * 12];
   __shared__ double sb[NB * 3], ss[NB * 3], sse[NB * 3];
-  if (!args_ok(st)) return;          // the status word is the same for every thread of the block
+  if (st->einval_r != NONE) return;   // the reset's arguments were bad; scaling_e is checked here (k_arm36 cleared its slot)
   const int64_t e0 = (int64_t)blockIdx.x * NB;
   const int n = (int)(neb - e0 < NB ? neb - e0 : NB);
   const int t = threadIdx.x;
   for (int i = t; i < 9 * n; i += NB) sE[i] = (double)E[9 * e0 + i];
   for (int i = t; i < 3 * n; i += NB) {
     sb[i] = b_e[3 * e0 + i];
-    ss[i] = scaling_e[3 * e0 + i];
+    const double x = scaling_e[3 * e0 + i];
+    if (!(isfinite(x) && x >= 0.0)) atomicMin(&st->einval_e, (long long)(3 * e0 + i));   // check_damping, src/utils.jl:100-107
+    ss[i] = x;
     sse[i] = s_e ? s_e[3 * e0 + i] : 1.0;
   }
   __syncthreads();
@@ -412,6 +484,23 @@ __global__ void k_g_init(double* __restrict__ g, const double* __restrict__ b_r,
   g[i] = s_r ? b_r[i] * s_r[i] : b_r[i];
 }
 
+// Column w of a 3 x 6 coupling block in the canonical layout: three entries starting at 18 c + 3 w, which is even
+// exactly when w is (odd = w & 1). FP64: one 16-byte load at the even offset and one single load cover them, with
+// no divergence between the parities (C is aligned to two elements); 0.557 -> 0.539 ms on the 200k-point scene.
+// FP32: three single loads (the paired form measured slower there, 0.341 -> 0.368 ms).
+__device__ __forceinline__ void load_col3(const float* p, int, float out[3]) {
+  out[0] = __ldg(p);
+  out[1] = __ldg(p + 1);
+  out[2] = __ldg(p + 2);
+}
+__device__ __forceinline__ void load_col3(const double* p, int odd, double out[3]) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p + odd));
+  const double s = __ldg(p + (odd ? 0 : 2));
+  out[0] = odd ? s : v.x;
+  out[1] = odd ? v.x : v.y;
+  out[2] = odd ? v.y : s;
+}
+
 // Phase 2 for d_r = 6, d_e = 3 in the canonical layout (coffsets = 18 c, eoffsets = 9 e): six threads per work item,
 // thread w accumulating column w of the 6 x 6 block, so the block's state is 6 values per thread rather than 36. Per
 // pair a thread loads the point's E^-1 (padded row of 12), all of C_c1 and column w of C_c2, forms u = E^-1 C_c2[:, w]
@@ -480,8 +569,8 @@ __global__ void __launch_bounds__(128) k_pairs36(
 #pragma unroll
       for (int i = 0; i < 9; ++i) { float2 v = __ldg(q + i); c1v[2 * i] = v.x; c1v[2 * i + 1] = v.y; }
     }
-    const T* c2p = C + 18 * (int64_t)c2 + 3 * w;
-    T c2w[3] = {__ldg(c2p), __ldg(c2p + 1), __ldg(c2p + 2)};
+    T c2w[3];
+    load_col3(C + 18 * (int64_t)c2 + 3 * w, w & 1, c2w);
     if (scaled) {
       double se[3];
 #pragma unroll
@@ -516,6 +605,108 @@ __global__ void __launch_bounds__(128) k_pairs36(
   if (diag) {
     if (solo) g[6 * r2 + w] -= gacc;
     else atomicAdd(g + 6 * r2 + w, -gacc);
+  }
+}
+
+// Add six consecutive entries of a column of S (vector reductions where the address allows: red.global.add.v4/.v2
+// for FP32, scalar for FP64). v[i] goes to col[i].
+__device__ __forceinline__ void red2(float* p, float a, float b) {
+  asm volatile("red.relaxed.gpu.global.add.v2.f32 [%0], {%1, %2};\n" ::"l"(p), "f"(a), "f"(b) : "memory");
+}
+__device__ __forceinline__ void red4(float* p, float a, float b, float c, float d) {
+  asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+__device__ __forceinline__ void red_column6(float* col, const float v[6]) {
+  switch ((reinterpret_cast<uintptr_t>(col) >> 2) & 3) {   // position of col[0] within its 16-byte line
+    case 0: red4(col, v[0], v[1], v[2], v[3]); red2(col + 4, v[4], v[5]); break;
+    case 1: atomicAdd(col, v[0]); red2(col + 1, v[1], v[2]); red2(col + 3, v[3], v[4]); atomicAdd(col + 5, v[5]); break;
+    case 2: red2(col, v[0], v[1]); red4(col + 2, v[2], v[3], v[4], v[5]); break;
+    default: atomicAdd(col, v[0]); red4(col + 1, v[1], v[2], v[3], v[4]); atomicAdd(col + 5, v[5]); break;
+  }
+}
+__device__ __forceinline__ void red_column6(double* col, const double v[6]) {
+#pragma unroll
+  for (int i = 0; i < 6; ++i) atomicAdd(col + i, v[i]);
+}
+
+// Phase 2 for d_r = 6, d_e = 3, point-major form: the same pair products as the reference's column-by-column
+// accumulation (accumulate_sparse_columns!, src/schur_reduction.jl:315-387), visited by point instead of by S column.
+// The pairs (c1, c2), c1 <= c2, of every point, by point, then c2, then c1; six lanes
+// per pair (lane w computes column w of C_c1' E^-1 C_c2), five pairs per warp. Consecutive pairs share their point and
+// have consecutive c1, so a warp's operands (C of the point's couplings, its padded E^-1) lie in a few contiguous
+// lines. Each lane adds its six entries into S with vector reductions (S is expected to stay resident in L2). Record
+// {c1, k | (c2 - c1) << 25}: k is the S block (r(c1), r(c2)). The lower triangle of a diagonal block receives -0.0,
+// which leaves every value unchanged. Diagonal pairs (c1 = c2, one per coupling) also subtract C_c2' z from g_S.
+template <class T>
+__global__ void __launch_bounds__(128) k_points36(
+    int64_t npairs, const int2* __restrict__ recs, const int32_t* __restrict__ entry_elim, const int32_t* __restrict__ block_r1,
+    const int32_t* __restrict__ block_r2, const int64_t* __restrict__ block_base, const int32_t* __restrict__ block_stride,
+    int64_t dense_nr, const T* __restrict__ C, const typename EinvOf<T>::type* __restrict__ Einv12, const double* __restrict__ z,
+    const double* __restrict__ s_r, const double* __restrict__ s_e, T* __restrict__ S, double* __restrict__ g,
+    const Status* __restrict__ st) {
+  using TE = typename EinvOf<T>::type;
+  const int lane = threadIdx.x & 31;
+  if (lane >= 30) return;
+  const int64_t q = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 5 + lane / 6;
+  const int w = lane % 6;
+  if (q >= npairs) return;
+  if (!live(st)) return;
+  const int2 rec = __ldg(recs + q);
+  const uint32_t y = (uint32_t)rec.y;
+  const int c1 = rec.x, k = (int)(y & 0x1ffffffu), c2 = c1 + (int)(y >> 25);
+  const int e = __ldg(entry_elim + c1);
+  const int r1 = __ldg(block_r1 + k), r2 = __ldg(block_r2 + k);
+  const bool diag = r1 == r2;
+  TE ei[12];
+  if constexpr (std::is_same<TE, double>::value) {
+    const double2* p = reinterpret_cast<const double2*>(Einv12 + 12 * (int64_t)e);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) { double2 v = __ldg(p + i); ei[2 * i] = v.x; ei[2 * i + 1] = v.y; }
+  } else {
+    const float4* p = reinterpret_cast<const float4*>(Einv12 + 12 * (int64_t)e);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { float4 v = __ldg(p + i); ei[4 * i] = v.x; ei[4 * i + 1] = v.y; ei[4 * i + 2] = v.z; ei[4 * i + 3] = v.w; }
+  }
+  T c1v[18];
+  if constexpr (std::is_same<T, double>::value) {
+    const double2* p = reinterpret_cast<const double2*>(C + 18 * (int64_t)c1);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { double2 v = __ldg(p + i); c1v[2 * i] = v.x; c1v[2 * i + 1] = v.y; }
+  } else {
+    const float2* p = reinterpret_cast<const float2*>(C + 18 * (int64_t)c1);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { float2 v = __ldg(p + i); c1v[2 * i] = v.x; c1v[2 * i + 1] = v.y; }
+  }
+  T c2w[3];
+  load_col3(C + 18 * (int64_t)c2 + 3 * w, w & 1, c2w);
+  if (s_r != nullptr || s_e != nullptr) {
+    const double fw = s_r ? s_r[6 * r2 + w] : 1.0;
+    double se[3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) se[s] = s_e ? s_e[3 * e + s] : 1.0;
+#pragma unroll
+    for (int s = 0; s < 3; ++s) c2w[s] = T((double)c2w[s] * (se[s] * fw));
+#pragma unroll
+    for (int rho = 0; rho < 6; ++rho) {
+      const double fr = s_r ? s_r[6 * r1 + rho] : 1.0;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) c1v[3 * rho + s] = T((double)c1v[3 * rho + s] * (se[s] * fr));
+    }
+  }
+  T u[3];
+#pragma unroll
+  for (int t = 0; t < 3; ++t) u[t] = (T)(ei[t] * (TE)c2w[0] + ei[t + 3] * (TE)c2w[1] + ei[t + 6] * (TE)c2w[2]);
+  T v[6];
+#pragma unroll
+  for (int rho = 0; rho < 6; ++rho) {
+    const T a = c1v[3 * rho] * u[0] + c1v[3 * rho + 1] * u[1] + c1v[3 * rho + 2] * u[2];
+    v[rho] = (diag && rho > w) ? T(-0.0) : -a;
+  }
+  const int64_t stride = block_stride ? (int64_t)__ldg(block_stride + k) : dense_nr;
+  red_column6(S + __ldg(block_base + k) + w * stride, v);
+  if (diag) {
+    const double* zp = z + 3 * (int64_t)e;
+    atomicAdd(g + 6 * r2 + w, -((double)c2w[0] * zp[0] + (double)c2w[1] * zp[1] + (double)c2w[2] * zp[2]));
   }
 }
 
@@ -1199,6 +1390,31 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
       }
     }
   }
+  // point-major pair records for k_points36: per point, its pairs by c2 then c1, as {c1, k | (c2 - c1) << 25}
+  std::vector<int2> prec;
+  std::vector<int64_t> pptr(neb + 1, 0);
+  for (int64_t e = 0; e < neb; ++e) {
+    const int64_t kk = d->eliminated_ptr[e + 1] - d->eliminated_ptr[e];
+    pptr[e + 1] = pptr[e] + kk * (kk + 1) / 2;
+  }
+  if (P->fast36 && nb < (int64_t(1) << 25) && pptr[neb] == npairs) {
+    prec.resize(npairs);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t e = 0; e < neb; ++e) {
+      int64_t q = pptr[e];
+      const int64_t p0 = d->eliminated_ptr[e], p1 = d->eliminated_ptr[e + 1];
+      for (int64_t c2 = p0; c2 < p1; ++c2) {
+        const int64_t r2 = d->entry_retained[c2];
+        const int64_t* lo = browval.data() + bcolptr[r2];
+        const int64_t* hi = browval.data() + bcolptr[r2 + 1];
+        for (int64_t c1 = p0; c1 <= c2; ++c1) {
+          const int64_t k = std::lower_bound(lo, hi, d->entry_retained[c1]) - browval.data();   // present: checked above
+          prec[q++] = make_int2((int32_t)c1, (int32_t)((uint32_t)k | ((uint32_t)(c2 - c1) << 25)));
+        }
+      }
+    }
+    P->points_ok = true;
+  }
   // uploads
   upload(P->r_dims, to32(d->r_dims, nrb, "r_dims"), s);
   upload(P->boffsets_r, to32(boff_r.data(), nrb, "boffsets_r"), s);
@@ -1228,6 +1444,7 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
     upload(P->col_base, cbase, s);
     upload(P->col_h, ch, s);
     upload(P->pair_packed, packed, s);
+    if (P->points_ok) upload(P->pt_rec, prec, s);
   } else {
     upload(P->pair_c1, pair_c1, s);
     upload(P->pair_c2, pair_c2, s);
@@ -1253,9 +1470,21 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
       upload(P->S_rowval, rv, s);
       upload(P->S_col, cl, s);
     }
+    if (d->diag_inds && P->R_length < INT32_MAX) {
+      bool inside = true;
+      for (int64_t i = 0; i < nr && inside; ++i) inside = d->diag_inds[i] >= Scolptr[i] && d->diag_inds[i] < Scolptr[i + 1];
+      if (inside) {
+        std::vector<int32_t> rf(P->nnzS, -1);
+        for (int64_t i = 0; i < P->R_length; ++i)
+          if (d->r_to_s_map[i] >= 0) rf[d->r_to_s_map[i]] = (int32_t)i;
+        upload(P->r_from, rf, s);
+        upload(P->S_colptr, Scolptr, s);
+        P->reset_fused = true;
+      }
+    }
   }
   P->Einv64.alloc(sizeof(double) * std::max<int64_t>(P->E_length, 1));
-  P->Einv32.alloc(sizeof(float) * std::max<int64_t>(P->E_length, 1));
+  if (!P->fast36) P->Einv32.alloc(sizeof(float) * std::max<int64_t>(P->E_length, 1));
   P->z.alloc(sizeof(double) * std::max<int64_t>(ne, 1));
   if (P->fast36) P->Einv12.alloc(sizeof(double) * 12 * neb);   // sized for FP64; the FP32 form uses half
   P->status.alloc(sizeof(Status));
@@ -1269,8 +1498,8 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
 static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
-                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h,
-                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col,
+                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h,
+                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
   for (auto* x : bufs) b += (int64_t)x->bytes;
@@ -1310,6 +1539,17 @@ static void begin_checked(SchurPlan* P, const double* scaling, int64_t n, int wh
   BLS_CUDA(cudaGetLastError());
 }
 
+// check_damping of scaling_r: one launch for short vectors, else the clearing launch and a grid-wide check
+static void check_scaling_r(SchurPlan* P, const double* sc) {
+  if (P->nr <= 16384) {
+    k_check_scaling1<<<1, 1024, 0, P->ctx->stream>>>(sc, P->nr, P->status.as<Status>(), 0);
+    P->launches += 1;
+    BLS_CUDA(cudaGetLastError());
+  } else {
+    begin_checked(P, sc, P->nr, 0);
+  }
+}
+
 template <class T>
 static void reset_sparse(SchurPlan* P, T* S, const T* R, const double* sc, double lambda, const double* s_r) {
   if (!P->has_sparse || !P->diag_inds.p) throw Error(BLS_EINVAL, "the plan was created without a sparse pattern");
@@ -1317,6 +1557,15 @@ static void reset_sparse(SchurPlan* P, T* S, const T* R, const double* sc, doubl
   if (s_r && !P->S_rowval.p) throw Error(BLS_EINVAL, "a conditioning scale needs S_rowval in the plan");
   cudaStream_t s = P->ctx->stream;
   Status* st = P->status.as<Status>();
+  if (P->reset_fused) {
+    check_scaling_r(P, sc);
+    k_reset_columns<T><<<std::max(1, grid_for(P->nr * 32, 256)), 256, 0, s>>>(S, R, P->r_from.as<int32_t>(), P->S_colptr.as<int64_t>(),
+                                                               s_r ? P->S_rowval.as<int32_t>() : nullptr, P->diag_inds.as<int64_t>(),
+                                                               sc, lambda, s_r, P->nr, st);
+    P->launches += 1;
+    BLS_CUDA(cudaGetLastError());
+    return;
+  }
   begin_checked(P, sc, P->nr, 0);
   k_fill<T><<<std::min<int64_t>(grid_for(P->nnzS, 256), 148 * 16), 256, 0, s>>>(S, P->nnzS, st);
   if (P->R_length > 0)
@@ -1333,6 +1582,13 @@ template <class T>
 static void reset_dense(SchurPlan* P, T* S, const T* R, const double* sc, double lambda, const double* s_r) {
   cudaStream_t s = P->ctx->stream;
   Status* st = P->status.as<Status>();
+  if (P->nr <= 8192) {
+    check_scaling_r(P, sc);
+    k_reset_dense_columns<T><<<std::max(1, grid_for(P->nr * 32, 256)), 256, 0, s>>>(S, R, sc, lambda, s_r, P->nr, st);
+    P->launches += 1;
+    BLS_CUDA(cudaGetLastError());
+    return;
+  }
   begin_checked(P, sc, P->nr, 0);
   k_copy_scaled_dense<T><<<std::min<int64_t>(grid_for(P->nr * P->nr, 256), 148 * 16), 256, 0, s>>>(S, R, s_r, P->nr, st);
   k_damp_diag<T><<<grid_for(P->nr, 256), 256, 0, s>>>(S, nullptr, P->nr, sc, lambda, s_r, P->nr, st);
@@ -1363,17 +1619,19 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
     throw Error(BLS_EINVAL, "C_data must be aligned to two elements (the device reads coupling blocks in pairs of entries)");
   cudaStream_t s = P->ctx->stream;
   Status* st = P->status.as<Status>();
-  begin_checked(P, sc_e, P->ne, 1);
-  k_arm<<<1, 1, 0, s>>>(st);
   if (P->fast36) {
     using TE = typename EinvOf<T>::type;
-    k_factor36<T><<<grid_for(P->neblocks, 128), 128, 0, s>>>(P->neblocks, E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
+    k_arm36<<<1, 1, 0, s>>>(st);
+    if (P->neblocks > 0)
+      k_factor36<T><<<grid_for(P->neblocks, 128), 128, 0, s>>>(P->neblocks, E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
                                                              P->Einv12.as<TE>(), P->z.as<double>(), st);
   } else {
-    k_factor<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(P->neblocks, P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
+    begin_checked(P, sc_e, P->ne, 1);
+    k_arm<<<1, 1, 0, s>>>(st);
+    if (P->neblocks > 0)
+      k_factor<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(P->neblocks, P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
                                                            P->boffsets_e.as<int32_t>(), E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
-                                                           std::is_same<T, float>::value ? P->Einv32.as<float>() : nullptr, P->z.as<double>(),
-                                                           nullptr, st);
+                                                           std::is_same<T, float>::value ? P->Einv32.as<float>() : nullptr, P->z.as<double>(), st);
   }
   P->launches += 2;   // k_arm, k_factor
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1420,6 +1678,20 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
           P->nitems, P->item_block.as<int32_t>(), P->item_start.as<int32_t>(), P->item_info.as<int32_t>(), P->pair_packed.as<int2>(),
           P->block_r1.as<int32_t>(), P->block_r2.as<int32_t>(), dense ? P->block_base_dense.as<int64_t>() : P->block_base_sparse.as<int64_t>(),
           dense ? nullptr : P->block_stride_sparse.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), S, g, st);
+      if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
+    }
+  } else if (P->fast36 && P->kernel == 4 && P->points_ok) {
+    using TE = typename EinvOf<T>::type;
+    k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st);
+    P->launches += 1;
+    if (P->npairs > 0) {
+      const int64_t warps = (P->npairs + 4) / 5;
+      if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
+      P->launches += 1;
+      k_points36<T><<<grid_for(warps * 32, 128), 128, 0, s>>>(
+          P->npairs, P->pt_rec.as<int2>(), P->entry_eliminated.as<int32_t>(), P->block_r1.as<int32_t>(), P->block_r2.as<int32_t>(),
+          dense ? P->block_base_dense.as<int64_t>() : P->block_base_sparse.as<int64_t>(), dense ? nullptr : P->block_stride_sparse.as<int32_t>(),
+          P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), s_r, s_e, S, g, st);
       if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
     }
   } else if (P->fast36) {
@@ -1548,7 +1820,7 @@ int bls_reduce_schur_dense(bls_schur_plan* P, int dtype, void* S, double* g, con
 }
 
 int bls_schur_plan_set_kernel(bls_schur_plan* P, int which) {
-  if (!P || which < 0 || which > 3) return BLS_EINVAL;
+  if (!P || which < 0 || which > 4) return BLS_EINVAL;
   P->kernel = which;
   return BLS_OK;
 }

@@ -115,8 +115,9 @@ class SchurReductionWorkspace:
     def set_kernel(self, which: str) -> None:
         """Phase-2 kernel of the 6/3 fast path: "pairs" (block owned, six lanes per pair list, the default), "lanes"
         (block owned, a lane per pair, a warp per pair list), "columns" (block-column owned, a warp per visit) or
-        "tiles" (block-column owned, visits staged in chunks; sparse S without conditioning scales, else "pairs")."""
-        check(_lib.gpu().bls_schur_plan_set_kernel(self._h, {"columns": 0, "pairs": 1, "lanes": 2, "tiles": 3}[which]))
+        "tiles" (block-column owned, visits staged in chunks; sparse S without conditioning scales, else "pairs") or
+        "points" (point-major, six lanes per pair, vector reductions into S)."""
+        check(_lib.gpu().bls_schur_plan_set_kernel(self._h, {"columns": 0, "pairs": 1, "lanes": 2, "tiles": 3, "points": 4}[which]))
 
     def instrument(self, timing: bool = True) -> None:
         """Bracket the pair kernel of each reduction with CUDA events (read them with counters())."""

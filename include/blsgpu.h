@@ -159,8 +159,9 @@ int bls_reduce_schur_dense(bls_schur_plan* plan, int dtype, void* S_dev, double*
 int bls_schur_plan_instrument(bls_schur_plan* plan, int timing);
 /* Phase-2 kernel of the d_r = 6 / d_e = 3 fast path (no counterpart in the reference): 0 = block-column owned,
  * 1 = block owned, six lanes per pair list (the default), 2 = block owned, a lane per pair and a warp per pair list,
- * 3 = block-column owned with visits staged in chunks (sparse S without conditioning scales; otherwise as 1).
- * All compute the same reduction; the choice is kept for comparisons and for autotuning. */
+ * 3 = block-column owned with visits staged in chunks (sparse S without conditioning scales; otherwise as 1),
+ * 4 = point-major, six lanes per pair, entries added into S with vector reductions (as 1 when S has 2^25 or more
+ * blocks). All compute the same reduction; the choice is kept for comparisons and for autotuning. */
 int bls_schur_plan_set_kernel(bls_schur_plan* plan, int which);
 int bls_schur_plan_counters(bls_schur_plan* plan, int64_t* launches, double* pair_kernel_ms, int64_t* pair_kernel_launches);
 

@@ -56,7 +56,7 @@ def test_batch_matches_each_problem(bls, problems, dtype):
 def test_graph_autotune_and_failure(bls, problems):
     B = bls.batch.BatchedReduction(problems, torch.float32)
     times = B.autotune(reps=3)
-    assert set(times) == {"pairs", "columns", "lanes", "tiles"} and B.schedule == min(times, key=times.get)
+    assert set(times) == {"pairs", "columns", "lanes", "tiles", "points"} and B.schedule == min(times, key=times.get)
     assert B.run()
     S0, g0 = B.S.clone(), B.g.clone()
     B.capture()

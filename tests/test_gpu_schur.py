@@ -165,7 +165,7 @@ def scene_system(bls, name, ncams, npoints, dense=False, seed=None):
     return p, st, ost, opat
 
 
-@pytest.mark.parametrize("kernel", ["columns", "pairs", "lanes", "tiles"])
+@pytest.mark.parametrize("kernel", ["columns", "pairs", "lanes", "tiles", "points"])
 @pytest.mark.parametrize("name,ncams,npoints,dense", [
     ("dense_50x2000", 50, 2000, True),            # the dense workload at full size
     ("sparse_1000x200k", 120, 8000, False),
@@ -182,7 +182,7 @@ def test_scene_fp64_matches_oracle(bls, name, ncams, npoints, dense, kernel):
     assert relerr(o["x_e"], o["ox_e"]) < 1e-10
 
 
-@pytest.mark.parametrize("kernel", ["columns", "pairs", "lanes", "tiles"])
+@pytest.mark.parametrize("kernel", ["columns", "pairs", "lanes", "tiles", "points"])
 @pytest.mark.parametrize("name,ncams,npoints", [("sparse_1000x200k", 120, 8000), ("pcg_10000x1M", 150, 6000)])
 def test_scene_mixed_matches_fp64_oracle(bls, name, ncams, npoints, kernel):
     p, st, ost, opat = scene_system(bls, name, ncams, npoints)
@@ -192,6 +192,23 @@ def test_scene_mixed_matches_fp64_oracle(bls, name, ncams, npoints, kernel):
     assert relerr(o["S"], o["oS"]) < 1e-4
     assert relerr(o["g"], o["og"]) < 1e-6   # z and the gradient are FP64 from FP32 data
     assert relerr(o["x_e"], o["ox_e"]) < 1e-6
+
+
+@pytest.mark.parametrize("kernel", ["pairs", "points", "lanes"])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+@pytest.mark.parametrize("dense", [False, True])
+def test_scene_conditioned_scales(bls, kernel, dtype, dense):
+    """The 6/3 fast path with power-of-two conditioning scales (src/conditioning.jl:99-150) applied at read."""
+    p, st, ost, opat = scene_system(bls, "sparse_1000x200k", 40, 1500, dense)
+    rng = np.random.default_rng(5)
+    s_r = np.ldexp(1.0, rng.integers(-4, 5, st.nr))
+    s_e = np.ldexp(1.0, rng.integers(-4, 5, st.ne))
+    o = run_both(bls, st, ost, p.pattern, opat, p.E, p.C, p.R, p.b_r, p.b_e, p.scaling_r, p.scaling_e, p.lam, dense, dtype,
+                 s_r=s_r, s_e=s_e, kernel=kernel)
+    assert o["ok"] and o["ook"]
+    tol = 1e-12 if dtype == torch.float64 else 1e-4
+    assert relerr(o["S"], o["oS"]) < tol
+    assert relerr(o["g"], o["og"]) < (1e-12 if dtype == torch.float64 else 1e-6)
 
 
 def test_scatter_copy_matches_map(bls):
