@@ -16,7 +16,7 @@ Workloads:               scenes.workload, scenes.hessian_problem, scenes.jacobia
 from ._lib import ArgumentError, BlsError, DimensionMismatch
 from .layout import DEFAULT_MIN_WORK, SchurPattern, SchurStructure, build_r_to_s_map, build_schur_pattern, sparse_with_map
 from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce_schur_dense, reduce_schur_sparse,
-                        reset_schur_dense, reset_schur_sparse, scatter_copy)
+                        reset_reduce_schur_sparse_host, reset_schur_dense, reset_schur_sparse, scatter_copy)
 from .qr import (QRReductionWorkspace, SchurBlockJacobian, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
                  reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse)
 from .pcg import BlockJacobi, PCGResult, PCGWorkspace, factor_diagonal_blocks, solve_diagonal_blocks
@@ -25,7 +25,7 @@ from . import batch, gnn, scenes
 __all__ = [
     "ArgumentError", "BlsError", "DimensionMismatch", "DEFAULT_MIN_WORK", "SchurPattern", "SchurStructure", "build_r_to_s_map",
     "build_schur_pattern", "sparse_with_map", "SchurReductionWorkspace", "backsubstitute", "context", "reduce_schur_dense",
-    "reduce_schur_sparse", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
+    "reduce_schur_sparse", "reset_reduce_schur_sparse_host", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
     "SchurBlockJacobian", "SchurJacobianStructure", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
     "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "BlockJacobi", "PCGResult", "PCGWorkspace",
     "factor_diagonal_blocks", "solve_diagonal_blocks", "gnn", "batch",

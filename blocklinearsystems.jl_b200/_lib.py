@@ -87,6 +87,7 @@ def gpu() -> C.CDLL:
             "bls_reset_schur_sparse": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, vp]),
             "bls_reset_schur_dense": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, vp]),
             "bls_reduce_schur_sparse": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, vp, vp, vp, p64]),
+            "bls_reset_reduce_schur_sparse_host": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, C.c_double, vp, vp, vp, vp, vp, p64]),
             "bls_reduce_schur_dense": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, vp, vp, vp, p64]),
             "bls_schur_query_status": (C.c_int, [vp, p64]),
             "bls_schur_plan_instrument": (C.c_int, [vp, C.c_int]),

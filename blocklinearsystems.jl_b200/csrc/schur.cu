@@ -71,6 +71,17 @@ struct SchurPlan {
   // every diag_inds[i] lies in column i
   DevBuf r_from, S_colptr;
   bool reset_fused = false;
+  // host-buffer reduction (fast36, sparse): the points cut into stages of about equal coupling count, and the pair
+  // work items re-cut so that each item's pairs lie in one stage (stage j: items [stage_item[j], stage_item[j + 1]))
+  static constexpr int kStages = 16;
+  bool staged = false;
+  int64_t stage_pt[kStages + 1] = {}, stage_cp[kStages + 1] = {}, stage_item[kStages + 1] = {};
+  DevBuf st_block, st_start, st_info;
+  // device copies of the host call's inputs and outputs (allocated at its first call), its copy stream and events
+  DevBuf h_E, h_C, h_R, h_br, h_be, h_scr, h_sce, h_S, h_g;
+  size_t h_elem = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_free = nullptr, ev_points = nullptr, ev_in[kStages + 1] = {};
   // scratch: E^-1 (FP64, and FP32 for the mixed form), z, status
   DevBuf Einv64, Einv32, z, status;
   DevBuf Einv12;   // fast36: E^-1 per point in the element type of the pair products, padded to 12 entries (16-byte rows)
@@ -82,6 +93,10 @@ struct SchurPlan {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pair_events;
   ~SchurPlan() {
     if (host_status) cudaFreeHost(host_status);
+    if (ev_free) cudaEventDestroy(ev_free);
+    if (ev_points) cudaEventDestroy(ev_points);
+    for (auto& e : ev_in) if (e) cudaEventDestroy(e);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     for (auto& e : pair_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   }
 };
@@ -285,7 +300,7 @@ template <> struct EinvOf<float> { using type = float; };
 // is not written. It also applies check_damping to scaling_e (the lowest bad entry into the status word), so the
 // reduction needs no separate checking launch; the pair kernel that follows skips its work if any entry was bad.
 template <class T>
-__global__ void __launch_bounds__(128) k_factor36(int64_t neb, const T* __restrict__ E, const double* __restrict__ b_e,
+__global__ void __launch_bounds__(128) k_factor36(int64_t e_begin, int64_t neb, const T* __restrict__ E, const double* __restrict__ b_e,
                                                   const double* __restrict__ scaling_e, double lambda, const double* __restrict__ s_e,
                                                   double* __restrict__ Einv64, typename EinvOf<T>::type* __restrict__ Einv12,
                                                   double* __restrict__ z, Status* st) {
@@ -295,7 +310,7 @@ __global__ void __launch_bounds__(128) k_factor36(int64_t neb, const T* __restri
   __shared__ TE s12[NB * 12];
   __shared__ double sb[NB * 3], ss[NB * 3], sse[NB * 3];
   if (st->einval_r != NONE) return;   // the reset's arguments were bad; scaling_e is checked here (k_arm36 cleared its slot)
-  const int64_t e0 = (int64_t)blockIdx.x * NB;
+  const int64_t e0 = e_begin + (int64_t)blockIdx.x * NB;   // points [e_begin, neb)
   const int n = (int)(neb - e0 < NB ? neb - e0 : NB);
   const int t = threadIdx.x;
   for (int i = t; i < 9 * n; i += NB) sE[i] = (double)E[9 * e0 + i];
@@ -1415,6 +1430,53 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
     }
     P->points_ok = true;
   }
+  // staged work items for the host-buffer reduction: stage j holds points [stage_pt[j], stage_pt[j + 1]); a block's
+  // pairs ascend in point within its slot, so its pairs of one stage are a contiguous run, cut into items of at most
+  // PAIR_CHUNK pairs (solo when the run makes one item)
+  std::vector<int32_t> sb_all, ss_all, si_all;
+  if (P->fast36 && P->has_sparse) {
+    constexpr int K = SchurPlan::kStages;
+    std::vector<uint8_t> stage_of(neb);
+    P->stage_pt[0] = 0;
+    for (int j = 1; j < K; ++j) {
+      const int64_t target = nc * j / K;
+      P->stage_pt[j] = std::upper_bound(d->eliminated_ptr, d->eliminated_ptr + neb + 1, target) - d->eliminated_ptr - 1;
+      P->stage_pt[j] = std::max(P->stage_pt[j], P->stage_pt[j - 1]);
+    }
+    P->stage_pt[K] = neb;
+    for (int j = 0; j <= K; ++j) P->stage_cp[j] = d->eliminated_ptr[P->stage_pt[j]];
+    for (int j = 0; j < K; ++j)
+      for (int64_t e = P->stage_pt[j]; e < P->stage_pt[j + 1]; ++e) stage_of[e] = (uint8_t)j;
+    std::vector<std::vector<int32_t>> tb(K), ts(K), ti(K);
+    const int64_t nit = (int64_t)it_block.size();
+    for (int64_t i = 0; i < nit;) {
+      const int32_t k = it_block[i];
+      int64_t i2 = i;
+      while (i2 < nit && it_block[i2] == k) ++i2;
+      const int64_t a = it_start[i], b = it_start[i2 - 1] + (it_info[i2 - 1] & 0xffff);
+      for (int64_t p = a; p < b;) {
+        const int j = stage_of[packed[p].y & 0xffffff];
+        int64_t q = p + 1;
+        while (q < b && stage_of[packed[q].y & 0xffffff] == j) ++q;
+        const bool solo = q - p <= PAIR_CHUNK;
+        for (int64_t x = p; x < q; x += PAIR_CHUNK) {
+          tb[j].push_back(k);
+          ts[j].push_back((int32_t)x);
+          ti[j].push_back((int32_t)std::min<int64_t>(PAIR_CHUNK, q - x) | ((solo ? 1 : 0) << 16));
+        }
+        p = q;
+      }
+      i = i2;
+    }
+    P->stage_item[0] = 0;
+    for (int j = 0; j < K; ++j) {
+      sb_all.insert(sb_all.end(), tb[j].begin(), tb[j].end());
+      ss_all.insert(ss_all.end(), ts[j].begin(), ts[j].end());
+      si_all.insert(si_all.end(), ti[j].begin(), ti[j].end());
+      P->stage_item[j + 1] = (int64_t)sb_all.size();
+    }
+    P->staged = true;
+  }
   // uploads
   upload(P->r_dims, to32(d->r_dims, nrb, "r_dims"), s);
   upload(P->boffsets_r, to32(boff_r.data(), nrb, "boffsets_r"), s);
@@ -1445,6 +1507,11 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
     upload(P->col_h, ch, s);
     upload(P->pair_packed, packed, s);
     if (P->points_ok) upload(P->pt_rec, prec, s);
+    if (P->staged) {
+      upload(P->st_block, sb_all, s);
+      upload(P->st_start, ss_all, s);
+      upload(P->st_info, si_all, s);
+    }
   } else {
     upload(P->pair_c1, pair_c1, s);
     upload(P->pair_c2, pair_c2, s);
@@ -1499,7 +1566,7 @@ static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
                           &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h,
-                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr,
+                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
   for (auto* x : bufs) b += (int64_t)x->bytes;
@@ -1623,7 +1690,7 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
     using TE = typename EinvOf<T>::type;
     k_arm36<<<1, 1, 0, s>>>(st);
     if (P->neblocks > 0)
-      k_factor36<T><<<grid_for(P->neblocks, 128), 128, 0, s>>>(P->neblocks, E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
+      k_factor36<T><<<grid_for(P->neblocks, 128), 128, 0, s>>>(0, P->neblocks, E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
                                                              P->Einv12.as<TE>(), P->z.as<double>(), st);
   } else {
     begin_checked(P, sc_e, P->ne, 1);
@@ -1727,6 +1794,94 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
   return read_status(P, failed_block);
 }
 
+// reset_schur_sparse! + reduce_schur_sparse! on host buffers. The copy stream brings in scaling_r, R and b_r, then
+// E, b_e and scaling_e, then C stage by stage (few large copies: each copy costs a few microseconds of DMA setup);
+// the plan's stream resets S as soon as the first copies land, factors every point block once the point data is in,
+// and runs each stage's pair items while the next stage's couplings are still being copied. S and g_S are copied
+// back only when the status word is clean.
+template <class T>
+static int reduce_host(SchurPlan* P, T* S_h, double* g_h, const T* R_h, const double* scr_h, double lambda, const double* br_h,
+                       const double* be_h, const double* sce_h, const T* E_h, const T* C_h, int64_t* failed_block) {
+  if (!P->staged || !P->reset_fused)
+    throw Error(BLS_EUNSUPPORTED, "the host-buffer reduction needs a sparse plan on the 6/3 fast path with diag_inds in their columns");
+  if (!S_h || !g_h || !scr_h || !br_h || (P->neblocks > 0 && (!be_h || !sce_h || !E_h || !C_h)) || (P->R_length > 0 && !R_h))
+    throw Error(BLS_EINVAL, "a host buffer is NULL");
+  check_lambda(lambda);
+  constexpr int K = SchurPlan::kStages;
+  cudaStream_t s = P->ctx->stream;
+  if (!P->copy_stream) {
+    BLS_CUDA(cudaStreamCreateWithFlags(&P->copy_stream, cudaStreamNonBlocking));
+    BLS_CUDA(cudaEventCreateWithFlags(&P->ev_free, cudaEventDisableTiming));
+    BLS_CUDA(cudaEventCreateWithFlags(&P->ev_points, cudaEventDisableTiming));
+    for (auto& e : P->ev_in) BLS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  if (P->h_elem != sizeof(T)) {
+    P->h_E.alloc(sizeof(T) * std::max<int64_t>(P->E_length, 1));
+    P->h_C.alloc(sizeof(T) * std::max<int64_t>(P->C_length, 2));
+    P->h_R.alloc(sizeof(T) * std::max<int64_t>(P->R_length, 1));
+    P->h_S.alloc(sizeof(T) * std::max<int64_t>(P->nnzS, 1));
+    P->h_br.alloc(sizeof(double) * std::max<int64_t>(P->nr, 1));
+    P->h_scr.alloc(sizeof(double) * std::max<int64_t>(P->nr, 1));
+    P->h_g.alloc(sizeof(double) * std::max<int64_t>(P->nr, 1));
+    P->h_be.alloc(sizeof(double) * std::max<int64_t>(P->ne, 1));
+    P->h_sce.alloc(sizeof(double) * std::max<int64_t>(P->ne, 1));
+    P->h_elem = sizeof(T);
+  }
+  cudaStream_t cs = P->copy_stream;
+  auto h2d = [&](DevBuf& d, size_t off, const void* src, size_t bytes) {
+    if (bytes) BLS_CUDA(cudaMemcpyAsync(static_cast<char*>(d.p) + off, src, bytes, cudaMemcpyHostToDevice, cs));
+  };
+  // the copies overwrite the device inputs only after all earlier work on the plan's stream
+  BLS_CUDA(cudaEventRecord(P->ev_free, s));
+  BLS_CUDA(cudaStreamWaitEvent(cs, P->ev_free, 0));
+  h2d(P->h_scr, 0, scr_h, sizeof(double) * P->nr);
+  h2d(P->h_R, 0, R_h, sizeof(T) * P->R_length);
+  h2d(P->h_br, 0, br_h, sizeof(double) * P->nr);
+  BLS_CUDA(cudaEventRecord(P->ev_in[0], cs));
+  h2d(P->h_E, 0, E_h, sizeof(T) * 9 * P->neblocks);
+  h2d(P->h_be, 0, be_h, sizeof(double) * P->ne);
+  h2d(P->h_sce, 0, sce_h, sizeof(double) * P->ne);
+  BLS_CUDA(cudaEventRecord(P->ev_points, cs));
+  for (int j = 0; j < K; ++j) {
+    const int64_t c0 = P->stage_cp[j], c1 = P->stage_cp[j + 1];
+    h2d(P->h_C, sizeof(T) * 18 * c0, C_h + 18 * c0, sizeof(T) * 18 * (c1 - c0));
+    BLS_CUDA(cudaEventRecord(P->ev_in[j + 1], cs));
+  }
+  T* S = P->h_S.as<T>();
+  double* g = P->h_g.as<double>();
+  Status* st = P->status.as<Status>();
+  BLS_CUDA(cudaStreamWaitEvent(s, P->ev_in[0], 0));
+  reset_sparse<T>(P, S, P->h_R.as<T>(), P->h_scr.as<double>(), lambda, nullptr);
+  k_arm36<<<1, 1, 0, s>>>(st);
+  k_g_init<<<std::max(1, grid_for(P->nr, 256)), 256, 0, s>>>(g, P->h_br.as<double>(), nullptr, P->nr, st);
+  P->launches += 2;
+  using TE = typename EinvOf<T>::type;
+  BLS_CUDA(cudaStreamWaitEvent(s, P->ev_points, 0));
+  if (P->neblocks > 0) {
+    k_factor36<T><<<grid_for(P->neblocks, 128), 128, 0, s>>>(0, P->neblocks, P->h_E.as<T>(), P->h_be.as<double>(), P->h_sce.as<double>(), lambda,
+                                                             nullptr, P->Einv64.as<double>(), P->Einv12.as<TE>(), P->z.as<double>(), st);
+    P->launches += 1;
+  }
+  for (int j = 0; j < K; ++j) {
+    BLS_CUDA(cudaStreamWaitEvent(s, P->ev_in[j + 1], 0));
+    const int64_t i0 = P->stage_item[j], n = P->stage_item[j + 1] - i0;
+    if (n > 0) {
+      k_pairs36<T><<<grid_for((n + 4) / 5 * 32, 128), 128, 0, s>>>(
+          n, P->ncoup, P->st_block.as<int32_t>() + i0, P->st_start.as<int32_t>() + i0, P->st_info.as<int32_t>() + i0, P->pair_packed.as<int2>(),
+          P->block_r1.as<int32_t>(), P->block_r2.as<int32_t>(), P->block_base_sparse.as<int64_t>(), P->block_stride_sparse.as<int32_t>(), P->nr,
+          P->h_C.as<T>(), P->Einv12.as<TE>(), P->z.as<double>(), nullptr, nullptr, S, g, st);
+      P->launches += 1;
+    }
+  }
+  BLS_CUDA(cudaGetLastError());
+  const int rc = read_status(P, failed_block);
+  if (rc != BLS_OK) return rc;
+  BLS_CUDA(cudaMemcpyAsync(S_h, S, sizeof(T) * P->nnzS, cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaMemcpyAsync(g_h, g, sizeof(double) * P->nr, cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaStreamSynchronize(s));
+  return BLS_OK;
+}
+
 template <class T>
 static void backsub(SchurPlan* P, double* x_e, const double* x_r, const T* C, const double* s_r, const double* s_e) {
   P->launches += 1;
@@ -1806,6 +1961,19 @@ int bls_reduce_schur_sparse(bls_schur_plan* P, int dtype, void* S, double* g, co
   BLS_GUARD({
     if (dtype == BLS_F64) return reduce<double>(P, (double*)S, false, g, b_r, b_e, sc_e, lambda, (const double*)E, (const double*)C, s_r, s_e, failed_block);
     if (dtype == BLS_F32) return reduce<float>(P, (float*)S, false, g, b_r, b_e, sc_e, lambda, (const float*)E, (const float*)C, s_r, s_e, failed_block);
+    throw Error(BLS_EINVAL, "unknown dtype");
+  })
+}
+
+int bls_reset_reduce_schur_sparse_host(bls_schur_plan* P, int dtype, void* S, double* g, const void* R, const double* sc_r, double lambda,
+                                       const double* b_r, const double* b_e, const double* sc_e, const void* E, const void* C,
+                                       int64_t* failed_block) {
+  BLS_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (dtype == BLS_F64)
+      return reduce_host<double>(P, (double*)S, g, (const double*)R, sc_r, lambda, b_r, b_e, sc_e, (const double*)E, (const double*)C, failed_block);
+    if (dtype == BLS_F32)
+      return reduce_host<float>(P, (float*)S, g, (const float*)R, sc_r, lambda, b_r, b_e, sc_e, (const float*)E, (const float*)C, failed_block);
     throw Error(BLS_EINVAL, "unknown dtype");
   })
 }

@@ -207,6 +207,50 @@ def reduce_schur_sparse(S_nzval: torch.Tensor, g_S, b_r, b_e, scaling_e, lam, st
                    s_r, s_e, sync)
 
 
+def _host(t, name: str, n: int, dtype) -> torch.Tensor:
+    if isinstance(t, np.ndarray):
+        t = torch.from_numpy(t)
+    if not isinstance(t, torch.Tensor) or t.is_cuda:
+        raise ArgumentError(f"{name} must be a host (CPU) tensor or array")
+    if not t.is_contiguous():
+        raise ArgumentError(f"{name} must be contiguous")
+    if t.dtype != dtype:
+        raise ArgumentError(f"{name} must be {dtype}, got {t.dtype}")
+    if t.numel() != n:
+        raise DimensionMismatch(f"{name} has length {t.numel()}, expected {n}")
+    return t
+
+
+def reset_reduce_schur_sparse_host(S_nzval, g_S, R_nzval, scaling_r, lam, b_r, b_e, scaling_e, structure, E_data, C_data,
+                                   ws: SchurReductionWorkspace) -> bool:
+    """reset_schur_sparse! then reduce_schur_sparse! (src/schur_reduction.jl:416-436, 489-507) on host arrays (CPU
+    tensors or numpy arrays; page-locked tensors let the library overlap the copies with the reduction). S_nzval and
+    g_S are written only when the reduction succeeds; returns False (ws.failed_block set) when a point block fails.
+    Sparse plans on the 6/3 fast path without conditioning scales."""
+    st, pat = ws.structure, ws.pattern
+    if structure is not st:
+        raise ArgumentError("the structure and the workspace were built for different structures")
+    if pat is None:
+        raise ArgumentError("the workspace was built without a sparse pattern")
+    dt = S_nzval.dtype if isinstance(S_nzval, torch.Tensor) else torch.from_numpy(S_nzval[:0]).dtype
+    S_nzval = _host(S_nzval, "S.nzval", pat.nnz, dt)
+    T = _dtype_code(S_nzval)
+    g_S = _host(g_S, "g_S", st.nr, torch.float64)
+    R_nzval = _host(R_nzval, "R_nzval", pat.R_length, dt)
+    scaling_r = _host(scaling_r, "scaling_r", st.nr, torch.float64)
+    b_r = _host(b_r, "b_r", st.nr, torch.float64)
+    b_e = _host(b_e, "b_e", st.ne, torch.float64)
+    scaling_e = _host(scaling_e, "scaling_e", st.ne, torch.float64)
+    E_data = _host(E_data, "E_data", st.E_length, dt)
+    C_data = _host(C_data, "C_data", st.C_length, dt)
+    fb = C.c_int64(0)
+    p = lambda t: C.c_void_p(t.data_ptr())
+    rc = check(_lib.gpu().bls_reset_reduce_schur_sparse_host(ws.handle, T, p(S_nzval), p(g_S), p(R_nzval), p(scaling_r), float(lam),
+                                                             p(b_r), p(b_e), p(scaling_e), p(E_data), p(C_data), C.byref(fb)))
+    ws.failed_block = int(fb.value)
+    return rc != BLS_NOT_PD
+
+
 def reduce_schur_dense(S: torch.Tensor, g_S, b_r, b_e, scaling_e, lam, structure, E_data, C_data, ws: SchurReductionWorkspace,
                        s_r=None, s_e=None, *, sync: bool = True) -> bool:
     """Two-phase Schur reduction into the upper triangle of a dense column-major S (src/schur_reduction.jl:465-479)."""

@@ -153,6 +153,19 @@ int bls_reduce_schur_dense(bls_schur_plan* plan, int dtype, void* S_dev, double*
                            const double* b_e_dev, const double* scaling_e_dev, double lambda, const void* E_data_dev,
                            const void* C_data_dev, const double* s_r_dev, const double* s_e_dev,
                            int64_t* failed_block);
+/* reset_schur_sparse!(S.nzval, R, r_to_s_map, diag_inds, scaling_r, lambda, ws) followed by reduce_schur_sparse!(S, g_S,
+ * b_r, b_e, scaling_e, lambda, ...) (src/schur_reduction.jl:416-436 and 489-507) on HOST buffers: the pair of calls a
+ * caller whose arrays live in host memory makes, with the host-to-device copies overlapped with the reduction. The
+ * points are cut into 16 stages of about equal coupling count; R, the point data (E, b_e, scaling_e) and then C are
+ * copied on a second stream, and each stage's pairs are reduced while the next stage's part of C is still being
+ * copied. Outputs S_nzval[nnz] and g_S[nr] are written only on BLS_OK; on
+ * BLS_NOT_PD (failed_block as above) or an error they are untouched. Page-locked host buffers give the overlap;
+ * pageable ones work, with copies staged by the driver. Sparse plans on the d_r = 6 / d_e = 3 fast path whose
+ * diag_inds lie in their own columns, no conditioning scales (BLS_EUNSUPPORTED otherwise). The device copies of the
+ * inputs are allocated on the plan at the first call and freed with it. Synchronous. */
+int bls_reset_reduce_schur_sparse_host(bls_schur_plan* plan, int dtype, void* S_nzval, double* g_S, const void* R_data,
+                                       const double* scaling_r, double lambda, const double* b_r, const double* b_e,
+                                       const double* scaling_e, const void* E_data, const void* C_data, int64_t* failed_block);
 /* Instrumentation (no counterpart in the reference): with timing on, CUDA events bracket the pair kernel of every
  * reduction on the plan's stream. bls_schur_plan_counters synchronises on the last event, reports the device kernel
  * launches issued since the previous read, the summed pair-kernel time and its number of launches, and resets them. */

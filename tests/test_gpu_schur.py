@@ -211,6 +211,47 @@ def test_scene_conditioned_scales(bls, kernel, dtype, dense):
     assert relerr(o["g"], o["og"]) < (1e-12 if dtype == torch.float64 else 1e-6)
 
 
+@pytest.mark.parametrize("pinned", [True, False], ids=["pinned", "pageable"])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+def test_host_buffers_match_oracle(bls, dtype, pinned):
+    """reset + reduce from host buffers, copies overlapped stage by stage, against the FP64 oracle; a singular point
+    block leaves the host outputs untouched and is reported 1-based."""
+    p, st, ost, opat = scene_system(bls, "sparse_1000x200k", 120, 8000, False)
+    npdt = np.float32 if dtype == torch.float32 else np.float64
+    E32, C32, R32 = p.E.astype(npdt), p.C.astype(npdt), p.R.astype(npdt)
+
+    def host(a):
+        t = torch.from_numpy(np.ascontiguousarray(a))
+        return t.pin_memory() if pinned else t
+
+    ws = bls.SchurReductionWorkspace(st, p.pattern)
+    S = host(np.full(p.pattern.nnz, 7.0, npdt))
+    g = host(np.full(st.nr, 7.0))
+    args = [host(R32), host(p.scaling_r), p.lam, host(p.b_r), host(p.b_e), host(p.scaling_e), st, host(E32), host(C32), ws]
+    assert bls.reset_reduce_schur_sparse_host(S, g, *args)
+    work = orc.Work(ost, 1)
+    oS, og = np.zeros(opat.nnz), np.zeros(st.nr)
+    orc.reset_schur_sparse(ost, opat, oS, R32.astype(np.float64), p.scaling_r, p.lam)
+    ook, _ = orc.reduce_schur_sparse(ost, opat, work, oS, og, p.b_r, p.b_e, p.scaling_e, p.lam, E32.astype(np.float64), C32.astype(np.float64))
+    assert ook
+    tol = 1e-12 if dtype == torch.float64 else 1e-4
+    assert relerr(S.double().numpy(), oS) < tol
+    assert relerr(g.numpy(), og) < (1e-12 if dtype == torch.float64 else 1e-6)
+    # the same call again reproduces the result (device inputs are overwritten only after the previous call's work)
+    S2, g2 = host(np.zeros(p.pattern.nnz, npdt)), host(np.zeros(st.nr))
+    assert bls.reset_reduce_schur_sparse_host(S2, g2, *args)
+    assert relerr(S2.double().numpy(), S.double().numpy()) < (1e-14 if dtype == torch.float64 else 1e-6)
+    # point 4000 singular (its E block and damping zeroed): outputs untouched
+    E_bad, sc_bad = E32.copy(), p.scaling_e.copy()
+    E_bad[9 * 3999:9 * 4000] = 0.0
+    sc_bad[3 * 3999:3 * 4000] = 0.0
+    S3, g3 = host(np.full(p.pattern.nnz, 7.0, npdt)), host(np.full(st.nr, 7.0))
+    bad = [host(R32), host(p.scaling_r), p.lam, host(p.b_r), host(p.b_e), host(sc_bad), st, host(E_bad), host(C32), ws]
+    assert not bls.reset_reduce_schur_sparse_host(S3, g3, *bad)
+    assert ws.failed_block == 4000
+    assert (S3.numpy() == 7.0).all() and (g3.numpy() == 7.0).all()
+
+
 def test_scatter_copy_matches_map(bls):
     p, st, ost, opat = scene_system(bls, "sparse_1000x200k", 60, 2000)
     colptr, rowval, smap = bls.sparse_with_map(st, p.pattern, True)
