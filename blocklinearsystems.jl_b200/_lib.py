@@ -119,6 +119,9 @@ def gpu() -> C.CDLL:
             "bls_spmv_sym": (C.c_int, [vp, C.c_int, vp, vp, vp]),
             "bls_extract_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, vp]),
             "bls_pcg_solve": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, i64, C.c_int, p64, pdbl, p64]),
+            "bls_pcg_solve_refined": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, C.c_double, vp, vp, vp, C.c_double, C.c_double, i64, i64,
+                                                p64, p64, pdbl, p64]),
+            "bls_schur_apply_elimination": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_pcg_plan_counters": (i64, [vp]),
             "bls_pcg_set_preconditioner": (C.c_int, [vp, vp]),
             "bls_gnn_param_count": (i64, []),

@@ -308,6 +308,20 @@ __global__ void k_zero_d(double* __restrict__ p, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = 0.0;
 }
 
+// Refined solve helpers: y += lambda * sc .* x (the damping of the reset system), r = g - y, x += d
+__global__ void k_add_damping(int64_t n, double* __restrict__ y, double lambda, const double* __restrict__ sc, const double* __restrict__ x) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] += lambda * sc[i] * x[i];
+}
+__global__ void k_residual(int64_t n, double* __restrict__ r, const double* __restrict__ g, const double* __restrict__ y) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) r[i] = g[i] - y[i];
+}
+__global__ void k_add(int64_t n, double* __restrict__ x, const double* __restrict__ d) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) x[i] += d[i];
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------------------------------
@@ -541,6 +555,79 @@ static int pcg_solve(PCGPlan* P, const T* S, const double* g, double* x, double 
   return rel <= tol ? BLS_OK : BLS_NOT_CONVERGED;
 }
 
+// Mixed-precision solve refined against the FP64 reduced operator. PCG on the stored S (e.g. the FP32 reduction)
+// solves for a correction d; the outer residual r = g - A x uses A x = S0 x + lambda sc_r .* x - C' E^-1 C x in FP64,
+// where S0 is R on S's pattern (the reset system without damping) and the point term is applied from the reduction's
+// own FP64 E^-1 (bls_schur_apply_elimination), so x converges to the solution of the system the FP64 reduction of the
+// same stored inputs would give, while every PCG iteration reads only the compact S.
+template <class T>
+static int solve_refined(PCGPlan* P, bls_schur_plan* SP, const T* S, const T* S0, const double* sc_r, double lambda, const T* C,
+                         const double* g, double* x, double tol, double inner_tol, int64_t max_outer, int64_t inner_maxit,
+                         int64_t* outer_out, int64_t* inner_out, double* rel_out, int64_t* failed_block) {
+  if (!(tol > 0) || !(inner_tol > 0) || max_outer < 1 || inner_maxit < 1) throw Error(BLS_EINVAL, "tolerances must be positive, iteration limits >= 1");
+  if (!SP || !S || !S0 || !sc_r || !g || !x) throw Error(BLS_EINVAL, "a pointer is NULL");
+  if (!(std::isfinite(lambda) && lambda >= 0)) throw Error(BLS_EINVAL, "lambda must be finite and non-negative");
+  cudaStream_t s = P->ctx->stream;
+  const int64_t n = P->nr;
+  if (!P->ref_r.p) {
+    P->ref_r.alloc(sizeof(double) * std::max<int64_t>(n, 1));
+    P->ref_d.alloc(sizeof(double) * std::max<int64_t>(n, 1));
+    P->ref_y.alloc(sizeof(double) * std::max<int64_t>(n, 1));
+  }
+  double* r = P->ref_r.as<double>();
+  double* d = P->ref_d.as<double>();
+  double* y = P->ref_y.as<double>();
+  double* tr = P->scal.as<double>() + (P->K + 1) * PS_W + 2;
+  const int gb = std::max(1, grid_for(n, 256));
+  auto norm2 = [&](const double* v) {
+    k_zero_d<<<1, 32, 0, s>>>(tr, 1);
+    k_dot_self<<<std::max(1, std::min(grid_for(n, 256), 296)), 256, 0, s>>>(n, v, tr);
+    P->launches += 2;
+    BLS_CUDA(cudaMemcpyAsync(P->host, tr, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BLS_CUDA(cudaStreamSynchronize(s));
+    return P->host[0];
+  };
+  const int dt = sizeof(T) == 8 ? BLS_F64 : BLS_F32;
+  k_zero_d<<<gb, 256, 0, s>>>(x, n);
+  BLS_CUDA(cudaMemcpyAsync(r, g, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  P->launches += 1;
+  const double gnorm2 = norm2(g);
+  int64_t outer = 0, inner = 0;
+  double rel = gnorm2 == 0.0 ? 0.0 : 1.0;
+  while (rel > tol && outer < max_outer) {
+    k_zero_d<<<gb, 256, 0, s>>>(d, n);
+    P->launches += 1;
+    int64_t its = 0, fb = 0;
+    double irel = 0.0;
+    const int rc = pcg_solve<T>(P, S, r, d, inner_tol, inner_maxit, true, &its, &irel, &fb);
+    inner += its;
+    if (rc == BLS_NOT_PD) {
+      if (failed_block) *failed_block = fb;
+      *outer_out = outer;
+      *inner_out = inner;
+      *rel_out = rel;
+      return BLS_NOT_PD;
+    }
+    ++outer;
+    k_add<<<gb, 256, 0, s>>>(n, x, d);
+    // y = S0 x + lambda sc_r .* x - C' E^-1 C x; r = g - y
+    spmv<T>(P, S0, x, nullptr, y, false, s);
+    k_add_damping<<<gb, 256, 0, s>>>(n, y, lambda, sc_r, x);
+    P->launches += 2;
+    const int arc = bls_schur_apply_elimination(SP, dt, d, y, x, C);   // d is free once added into x
+    if (arc != BLS_OK) throw Error(arc, bls_last_error());
+    k_residual<<<gb, 256, 0, s>>>(n, r, g, d);
+    P->launches += 1;
+    rel = std::sqrt(norm2(r) / gnorm2);
+    if (!std::isfinite(rel)) break;
+  }
+  BLS_CUDA(cudaGetLastError());
+  *outer_out = outer;
+  *inner_out = inner;
+  *rel_out = rel;
+  return rel <= tol ? BLS_OK : BLS_NOT_CONVERGED;
+}
+
 void pcg_spmv(PCGPlan* P, int dtype, const void* S, const double* x, const double* g, double* y, bool residual, cudaStream_t s) {
   if (dtype == BLS_F64) spmv<double>(P, (const double*)S, x, g, y, residual, s);
   else spmv<float>(P, (const float*)S, x, g, y, residual, s);
@@ -638,6 +725,23 @@ int bls_pcg_solve(bls_pcg_plan* P, int dtype, const void* S, const double* g, do
       return pcg_solve<double>(P, (const double*)S, g, x, tol, maxit, use_graph != 0, iterations, rel_residual, failed_block);
     if (dtype == BLS_F32)
       return pcg_solve<float>(P, (const float*)S, g, x, tol, maxit, use_graph != 0, iterations, rel_residual, failed_block);
+    throw Error(BLS_EINVAL, "unknown dtype");
+  })
+}
+
+int bls_pcg_solve_refined(bls_pcg_plan* P, bls_schur_plan* schur, int dtype, const void* S, const void* S0, const double* scaling_r,
+                          double lambda, const void* C, const double* g, double* x, double tol, double inner_tol, int64_t max_outer,
+                          int64_t inner_maxit, int64_t* outer_iterations, int64_t* inner_iterations, double* rel_residual,
+                          int64_t* failed_block) {
+  PCG_GUARD({
+    if (!P || !outer_iterations || !inner_iterations || !rel_residual) throw Error(BLS_EINVAL, "null argument");
+    if (failed_block) *failed_block = 0;
+    if (dtype == BLS_F64)
+      return solve_refined<double>(P, schur, (const double*)S, (const double*)S0, scaling_r, lambda, (const double*)C, g, x, tol, inner_tol,
+                                   max_outer, inner_maxit, outer_iterations, inner_iterations, rel_residual, failed_block);
+    if (dtype == BLS_F32)
+      return solve_refined<float>(P, schur, (const float*)S, (const float*)S0, scaling_r, lambda, (const float*)C, g, x, tol, inner_tol,
+                                  max_outer, inner_maxit, outer_iterations, inner_iterations, rel_residual, failed_block);
     throw Error(BLS_EINVAL, "unknown dtype");
   })
 }

@@ -27,6 +27,7 @@ struct PCGPlan {
   // solver state (FP64)
   DevBuf D;                 // factored diagonal blocks (L in the lower triangle)
   DevBuf r, z, p, q, scal, flags;
+  DevBuf ref_r, ref_d, ref_y;   // refined solve: outer residual, correction, operator product (FP64, allocated at its first call)
   int K = 16;               // iterations per replayed graph
   cudaGraphExec_t graph = nullptr;
   const void* graph_S = nullptr;

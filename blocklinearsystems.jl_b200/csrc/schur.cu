@@ -84,6 +84,7 @@ struct SchurPlan {
   cudaEvent_t ev_free = nullptr, ev_points = nullptr, ev_in[kStages + 1] = {};
   // scratch: E^-1 (FP64, and FP32 for the mixed form), z, status
   DevBuf Einv64, Einv32, z, status;
+  DevBuf w_apply;  // per point E^-1 C x of bls_schur_apply_elimination (ne doubles, allocated at its first call)
   DevBuf Einv12;   // fast36: E^-1 per point in the element type of the pair products, padded to 12 entries (16-byte rows)
   Status* host_status = nullptr;   // pinned
   int last_dtype = -1;
@@ -522,6 +523,37 @@ __device__ __forceinline__ void load_col3(const double* p, int odd, double out[3
 // and adds C_c1' u to its column. A pair record {c1, e | (c2 - c1) << 24} holds every index the pair needs, so the
 // next record is fetched while the current pair is computed and no load waits on another index load. The diagonal
 // block's items also subtract C_c2' z from g_S (each coupling of r2 is exactly one diagonal pair).
+// The point term of the reduced operator applied to a vector, in FP64 (no counterpart in the reference, which forms
+// S): per eliminated block e, w_e = E_e^-1 sum_c C_c x_r(c), with E^-1 the plan's FP64 inverse of the damped block
+// from its last reduction (C_c is d_e x d_r column-major). k_gradient then forms y = y0 - sum_c C_c' w_e(c).
+template <class T>
+__global__ void __launch_bounds__(256) k_point_apply(int64_t neb, const int32_t* __restrict__ eliminated_ptr,
+                                                     const int32_t* __restrict__ entry_retained, const int32_t* __restrict__ e_dims,
+                                                     const int32_t* __restrict__ eoffsets, const int32_t* __restrict__ boffsets_e,
+                                                     const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boffsets_r,
+                                                     const int32_t* __restrict__ coffsets, const T* __restrict__ C,
+                                                     const double* __restrict__ Einv64, const double* __restrict__ x,
+                                                     double* __restrict__ w, const Status* __restrict__ st) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= neb || !live(st)) return;
+  const int de = e_dims[e];
+  double t[3] = {0.0, 0.0, 0.0};
+  for (int c = eliminated_ptr[e]; c < eliminated_ptr[e + 1]; ++c) {
+    const int r = entry_retained[c], dr = r_dims[r], xo = boffsets_r[r], co = coffsets[c];
+    for (int j = 0; j < dr; ++j) {
+      const double xj = x[xo + j];
+      for (int i = 0; i < de; ++i) t[i] += (double)C[co + i + de * j] * xj;
+    }
+  }
+  const double* inv = Einv64 + eoffsets[e];
+  const int so = boffsets_e[e];
+  for (int i = 0; i < de; ++i) {
+    double a = 0.0;
+    for (int k = 0; k < de; ++k) a += inv[i + de * k] * t[k];
+    w[so + i] = a;
+  }
+}
+
 template <class T>
 __global__ void __launch_bounds__(128) k_pairs36(
     int64_t nitems, int64_t ncoup, const int32_t* __restrict__ item_block, const int32_t* __restrict__ item_start, const int32_t* __restrict__ item_info,
@@ -1566,7 +1598,7 @@ static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
                           &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h,
-                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g,
+                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g, &P->w_apply,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
   for (auto* x : bufs) b += (int64_t)x->bytes;
@@ -1882,6 +1914,29 @@ static int reduce_host(SchurPlan* P, T* S_h, double* g_h, const T* R_h, const do
   return BLS_OK;
 }
 
+// y = y0 - C' E^-1 C x over every eliminated block, in FP64, from the plan's E^-1 of its last successful reduction
+template <class T>
+static int apply_elimination(SchurPlan* P, double* y, const double* y0, const double* x, const T* C) {
+  if (P->max_de > 3) throw Error(BLS_EUNSUPPORTED, "the reduced operator is applied for eliminated blocks of size <= 3");
+  if (!y || !y0 || !x || (P->ncoup > 0 && !C)) throw Error(BLS_EINVAL, "a device pointer is NULL");
+  cudaStream_t s = P->ctx->stream;
+  if (!P->w_apply.p) P->w_apply.alloc(sizeof(double) * std::max<int64_t>(P->ne, 1));
+  Status* st = P->status.as<Status>();
+  if (P->neblocks > 0)
+    k_point_apply<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(
+        P->neblocks, P->eliminated_ptr.as<int32_t>(), P->entry_retained.as<int32_t>(), P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
+        P->boffsets_e.as<int32_t>(), P->r_dims.as<int32_t>(), P->boffsets_r.as<int32_t>(), P->coffsets.as<int32_t>(), C,
+        P->Einv64.as<double>(), x, P->w_apply.as<double>(), st);
+  if (P->nrblocks > 0)
+    k_gradient<T><<<grid_for(P->nrblocks * 32, 256), 256, 0, s>>>(
+        P->nrblocks, P->retained_ptr.as<int32_t>(), P->retained_entry.as<int32_t>(), P->entry_eliminated.as<int32_t>(), P->r_dims.as<int32_t>(),
+        P->boffsets_r.as<int32_t>(), P->e_dims.as<int32_t>(), P->boffsets_e.as<int32_t>(), P->coffsets.as<int32_t>(), C,
+        P->w_apply.as<double>(), y0, nullptr, nullptr, y, st);
+  P->launches += 2;
+  BLS_CUDA(cudaGetLastError());
+  return BLS_OK;
+}
+
 template <class T>
 static void backsub(SchurPlan* P, double* x_e, const double* x_r, const T* C, const double* s_r, const double* s_e) {
   P->launches += 1;
@@ -1961,6 +2016,15 @@ int bls_reduce_schur_sparse(bls_schur_plan* P, int dtype, void* S, double* g, co
   BLS_GUARD({
     if (dtype == BLS_F64) return reduce<double>(P, (double*)S, false, g, b_r, b_e, sc_e, lambda, (const double*)E, (const double*)C, s_r, s_e, failed_block);
     if (dtype == BLS_F32) return reduce<float>(P, (float*)S, false, g, b_r, b_e, sc_e, lambda, (const float*)E, (const float*)C, s_r, s_e, failed_block);
+    throw Error(BLS_EINVAL, "unknown dtype");
+  })
+}
+
+int bls_schur_apply_elimination(bls_schur_plan* P, int dtype, double* y, const double* y0, const double* x, const void* C) {
+  BLS_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (dtype == BLS_F64) return apply_elimination<double>(P, y, y0, x, (const double*)C);
+    if (dtype == BLS_F32) return apply_elimination<float>(P, y, y0, x, (const float*)C);
     throw Error(BLS_EINVAL, "unknown dtype");
   })
 }

@@ -75,6 +75,15 @@ class PCGResult:
     failed_block: int = 0    # with converged False and iterations 0: a diagonal block of S that is not PD (1-based)
 
 
+@dataclass
+class RefinedResult:
+    converged: bool
+    corrections: int         # outer corrections (PCG solves on the stored S)
+    iterations: int          # PCG iterations over all corrections
+    rel_residual: float      # ||g - A x|| / ||g|| with A the FP64 reduced operator
+    failed_block: int = 0
+
+
 class PCGWorkspace:
     """The device plan of PCG on the reduced system of `structure` on `pattern`: per-row block lists for y = S x, the
     block-Jacobi factorisation and the solver's vectors."""
@@ -150,3 +159,29 @@ class PCGWorkspace:
         rc = check(_lib.gpu().bls_pcg_solve(self.handle, T, dptr(S), dptr(g), dptr(x), float(tol), int(maxit), int(graph), C.byref(it),
                                             C.byref(rel), C.byref(fb)))
         return x, PCGResult(rc == 0, int(it.value), float(rel.value), int(fb.value))
+
+    def solve_refined(self, S: torch.Tensor, S0: torch.Tensor, scaling_r: torch.Tensor, lam: float, C_data: torch.Tensor,
+                      g: torch.Tensor, schur_ws, x: torch.Tensor | None = None, *, tol: float = 1e-12, inner_tol: float = 1e-6,
+                      max_outer: int = 20, inner_maxit: int | None = None) -> tuple[torch.Tensor, RefinedResult]:
+        """Solve A x = g, A = S0 + lam diag(scaling_r) - C' E^-1 C in FP64 (the reduced operator of `schur_ws`'s last
+        reduction, applied from its stored blocks), by PCG corrections on the stored S (e.g. the FP32 reduction) until
+        ||g - A x|| <= tol ||g||. S0 is R on S's pattern (a reset with lam = 0)."""
+        T = self._S(S)
+        if S0.dtype != S.dtype:
+            raise ArgumentError("S0 must have S's dtype")
+        self._S(S0)
+        st = self.structure
+        nr = st.nr
+        _dev(g, "g", nr, torch.float64)
+        _dev(scaling_r, "scaling_r", nr, torch.float64)
+        _dev(C_data, "C_data", st.C_length, S.dtype)
+        if x is None:
+            x = torch.zeros(nr, dtype=torch.float64, device=g.device)
+        _dev(x, "x", nr, torch.float64)
+        if inner_maxit is None:
+            inner_maxit = 10 * nr
+        o, i, rel, fb = C.c_int64(0), C.c_int64(0), C.c_double(0.0), C.c_int64(0)
+        rc = check(_lib.gpu().bls_pcg_solve_refined(self.handle, schur_ws.handle, T, dptr(S), dptr(S0), dptr(scaling_r), float(lam),
+                                                    dptr(C_data), dptr(g), dptr(x), float(tol), float(inner_tol), int(max_outer),
+                                                    int(inner_maxit), C.byref(o), C.byref(i), C.byref(rel), C.byref(fb)))
+        return x, RefinedResult(rc == 0, int(o.value), int(i.value), float(rel.value), int(fb.value))

@@ -129,6 +129,15 @@ class SchurReductionWorkspace:
         check(_lib.gpu().bls_schur_plan_counters(self._h, C.byref(n), C.byref(ms), C.byref(k)))
         return {"launches": int(n.value), "pair_kernel_ms": float(ms.value), "pair_kernel_launches": int(k.value)}
 
+    def apply_elimination(self, y: torch.Tensor, y0: torch.Tensor, x: torch.Tensor, C_data: torch.Tensor) -> torch.Tensor:
+        """y = y0 - C' E^-1 C x in FP64, from the E^-1 of this plan's last successful reduction (y distinct from y0)."""
+        st = self.structure
+        for name, t in (("y", y), ("y0", y0), ("x", x)):
+            _dev(t, name, st.nr, torch.float64)
+        T = _dtype_code(_dev(C_data, "C_data", st.C_length))
+        check(_lib.gpu().bls_schur_apply_elimination(self.handle, T, dptr(y), dptr(y0), dptr(x), dptr(C_data)))
+        return y
+
     def query_status(self) -> bool:
         fb = C.c_int64(0)
         rc = check(_lib.gpu().bls_schur_query_status(self.handle, C.byref(fb)))

@@ -181,6 +181,14 @@ int bls_schur_plan_counters(bls_schur_plan* plan, int64_t* launches, double* pai
 /* Status of the last reduction on this plan (synchronises): BLS_OK / BLS_NOT_PD / BLS_EINVAL. */
 int bls_schur_query_status(bls_schur_plan* plan, int64_t* failed_block);
 
+/* The point term of the reduced operator in FP64 (no counterpart in the reference, which forms S instead):
+ * y = y0 - sum over eliminated blocks of C' E^-1 C x, with E^-1 the FP64 inverse of the damped point block from the
+ * plan's last successful reduction and C its coupling blocks (dtype storage, as reduced); y and y0 distinct. With y0 =
+ * (R + lambda diag(scaling_r)) x it is the reduced matrix times x, formed exactly in FP64 from the stored blocks.
+ * Unconditioned reductions, eliminated blocks of size <= 3. */
+int bls_schur_apply_elimination(bls_schur_plan* plan, int dtype, double* y_dev, const double* y0_dev, const double* x_dev,
+                                const void* C_data_dev);
+
 /* backsubstitute!(x_e, x_r, structure, C_data, ws, s_r, s_e) (src/schur_reduction.jl:519-576):
  * x_e = z - E^-1 sum_r C_er x_r per eliminated block, from the caches of the last successful reduction. */
 int bls_backsubstitute(bls_schur_plan* plan, int dtype, double* x_e_dev, const double* x_r_dev,
@@ -310,6 +318,18 @@ int bls_extract_diagonal_blocks(bls_pcg_plan* plan, int dtype, const void* S_nzv
  * positive definite). iterations and rel_residual report the run. */
 int bls_pcg_solve(bls_pcg_plan* plan, int dtype, const void* S_nzval_dev, const double* g_dev, double* x_dev, double tol,
                   int64_t maxit, int use_graph, int64_t* iterations, double* rel_residual, int64_t* failed_block);
+/* Mixed-precision reduced solve with iterative refinement against the FP64 reduced operator (no counterpart in the
+ * reference): x solves A x = g, A = S0 + lambda diag(scaling_r) - C' E^-1 C applied in FP64 (S0 = R on S's pattern,
+ * e.g. bls_reset_schur_sparse with lambda = 0; C and E^-1 as in bls_schur_apply_elimination, from `schur`'s last
+ * reduction), while every inner PCG iteration reads only the stored reduced S (e.g. the FP32 reduction of the same
+ * system): x = 0, r = g; repeat d = PCG(S, r) to inner_tol, x += d, r = g - A x, until ||r|| <= tol ||g|| or
+ * max_outer corrections. Both plans must be on the same context. Returns BLS_OK, BLS_NOT_CONVERGED or BLS_NOT_PD
+ * (a diagonal block of S); outer_iterations / inner_iterations count the corrections and the PCG iterations,
+ * rel_residual is the last ||g - A x|| / ||g||. */
+int bls_pcg_solve_refined(bls_pcg_plan* plan, bls_schur_plan* schur, int dtype, const void* S_nzval_dev, const void* S0_nzval_dev,
+                          const double* scaling_r_dev, double lambda, const void* C_data_dev, const double* g_dev, double* x_dev,
+                          double tol, double inner_tol, int64_t max_outer, int64_t inner_maxit, int64_t* outer_iterations,
+                          int64_t* inner_iterations, double* rel_residual, int64_t* failed_block);
 /* Device kernel launches issued on this plan since the previous call (no counterpart in the reference). */
 int64_t bls_pcg_plan_counters(bls_pcg_plan* plan);
 /* Replace the block-Jacobi solve in later bls_pcg_solve calls by z_b = B_b r_b with the dense symmetric positive definite

@@ -151,3 +151,51 @@ def test_pcg_edge_cases(bls):
     assert not res.converged and res.failed_block == 4 and res.iterations == 0
     with pytest.raises(bls.ArgumentError):
         ws.solve(cu(S), cu(g), tol=0.0)
+
+
+@pytest.mark.parametrize("name,ncams,npoints", [("pcg_10000x1M", 120, 6000), ("sparse_1000x200k", 100, 6000)])
+def test_refined_mixed_solve_reaches_fp64_solution(bls, name, ncams, npoints):
+    """The mixed (FP32) reduction solved with iterative refinement against the FP64 reduced operator: the solution is
+    within 1e-10 of the exact solution of the FP64 oracle's reduced system on the same stored inputs, where PCG on the
+    FP32 S alone stops at the FP32 reduction's own error. The operator itself matches the oracle's S at 1e-12."""
+    spec = bls.scenes.scaled_down(bls.scenes.workload(name), ncams=ncams, npoints=npoints)
+    p = bls.scenes.hessian_problem(spec)
+    st, pat = p.structure, p.pattern
+    E32, C32, R32 = (a.astype(np.float32) for a in (p.E, p.C, p.R))
+    # oracle: FP64 reduction of the FP32-stored values, solved densely
+    sc = bls.scenes.Scene(spec)
+    bs, el, ptr, idx = sc.description()
+    ost = orc.Structure.from_description(bs, (ptr, idx), el)
+    opat = orc.Pattern(ost)
+    oS, og = np.zeros(opat.nnz), np.zeros(ost.nr)
+    orc.reset_schur_sparse(ost, opat, oS, R32.astype(np.float64), p.scaling_r, p.lam)
+    ook, _ = orc.reduce_schur_sparse(ost, opat, orc.Work(ost, 1), oS, og, p.b_r, p.b_e, p.scaling_e, p.lam, E32.astype(np.float64),
+                                     C32.astype(np.float64))
+    assert ook
+    Sd = csc_to_dense_upper(st.nr, pat.S_colptr, pat.S_rowval, oS)
+    x_star = np.linalg.solve(Sd, og)
+    # device: mixed reduction, R on the pattern, refined solve
+    ws = bls.SchurReductionWorkspace(st, pat)
+    S = torch.zeros(pat.nnz, dtype=torch.float32, device=DEV)
+    S0 = torch.zeros(pat.nnz, dtype=torch.float32, device=DEV)
+    g = torch.zeros(st.nr, dtype=torch.float64, device=DEV)
+    scr, C = cu(p.scaling_r), cu(C32)
+    bls.reset_schur_sparse(S0, cu(R32), None, None, scr, 0.0, ws)
+    bls.reset_schur_sparse(S, cu(R32), None, None, scr, p.lam, ws)
+    assert bls.reduce_schur_sparse(S, g, cu(p.b_r), cu(p.b_e), cu(p.scaling_e), p.lam, st, cu(E32), C, None, None, None, None, ws)
+    # the FP64 operator against the oracle's S
+    xr = np.random.default_rng(1).standard_normal(st.nr)
+    pcg = bls.PCGWorkspace(st, pat)
+    y0 = pcg.spmv(S0, cu(xr))
+    y0 += p.lam * scr * cu(xr)
+    y = ws.apply_elimination(torch.empty_like(y0), y0, cu(xr), C)
+    assert relerr(y.cpu().numpy(), Sd @ xr) < 1e-12
+    x, res = pcg.solve_refined(S, S0, scr, p.lam, C, g, ws, tol=1e-13)
+    assert res.converged and res.rel_residual <= 1e-13, res
+    err = relerr(x.cpu().numpy(), x_star)
+    xp, pres = pcg.solve(S, g, tol=1e-12)
+    err_plain = relerr(xp.cpu().numpy(), x_star)
+    print(f"{name}: refined error {err:.2e} ({res.corrections} corrections, {res.iterations} PCG iterations); "
+          f"PCG on the FP32 S alone {err_plain:.2e}")
+    assert err <= 1e-10
+    assert err_plain > 100 * err
