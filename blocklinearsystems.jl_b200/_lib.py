@@ -110,6 +110,7 @@ def gpu() -> C.CDLL:
             "bls_reduced_normal_sparse": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_reduced_normal_dense": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_reduced_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, vp]),
+            "bls_assemble_hessian": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, C.c_int, vp]),
             "bls_block_jacobi_create": (C.c_int, [vp, i64, p64, C.POINTER(vp)]),
             "bls_block_jacobi_destroy": (C.c_int, [vp]),
             "bls_factor_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, p64]),

@@ -51,6 +51,10 @@ struct QRPlan {
   TableClass classes[8], gram_classes[8];
   // per table, per pair (u1 <= u2) of its entries in the order u2 outer, u1 inner: the S block it adds to
   DevBuf tp_ptr, tp_blk, blk_base_sparse, blk_stride, blk_base_dense;
+  // the SchurBlockHessian layout of the same structure (assembly): E offset per eliminated block, C offset per entry of
+  // an eliminated table (its coupling), and the lengths
+  DevBuf t_eoff, u_coff;
+  int64_t E_len = 0, C_len = 0;
   DevBuf status;
   long long* host_status = nullptr;
   int64_t launches = 0;
@@ -254,7 +258,8 @@ __global__ void k_qr_free(int64_t t0, int64_t nt, const int32_t* __restrict__ t_
 }
 
 // accumulate_qr_entry! (src/qr_reduced.jl:375-405) per table. MODE 0: S blocks (upper triangle of diagonal blocks) and
-// J~'r~ into g; MODE 1: the full diagonal blocks D (reduced_diagonal_blocks!, :484-512).
+// J~'r~ into g; MODE 1: the full diagonal blocks D (reduced_diagonal_blocks!, :484-512). from_raw: the same products
+// over the data rows of the raw tables, J'J of the retained columns and J'r (the retained part of the assembly).
 template <class T, int MODE>
 __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int warp_bytes, const int32_t* __restrict__ tables,
                                                               const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_cols,
@@ -265,7 +270,7 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
                                                               const int32_t* __restrict__ tp_ptr, const int32_t* __restrict__ tp_blk,
                                                               const int64_t* __restrict__ blk_base, const int32_t* __restrict__ blk_stride,
                                                               int64_t dense_nr, const int64_t* __restrict__ doff, int dmax, const T* __restrict__ F,
-                                                              const double* __restrict__ Fr, T* __restrict__ S, double* __restrict__ g) {
+                                                              const double* __restrict__ Fr, T* __restrict__ S, double* __restrict__ g, int from_raw) {
   extern __shared__ __align__(16) unsigned char gsm_all[];
   const int64_t wi = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
   if (wi >= ntab) return;
@@ -276,13 +281,15 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
   const int u0 = t_ptr[t], kt = t_ptr[t + 1] - u0;
   double* rr = reinterpret_cast<double*>(gsm);
   T* B = reinterpret_cast<T*>(gsm + sizeof(double) * ((n + 1) & ~1));
-  const T* src = F + t_raw[t] + top;
+  // rows [row0, row0 + n): the bottom rows J~ of a factored table, or the data rows of a raw one (its damping rows last)
+  const int row0 = from_raw ? 0 : top;
+  const T* src = F + t_raw[t] + row0;
   for (int q = lane; q < ce * n; q += 32) {
     const int j = q / n, i = q - j * n;
     cp_async_elem(B + j * ns + i, src + (int64_t)j * M + i);
   }
   if (MODE == 0)
-    for (int i = lane; i < n; i += 32) cp_async_elem(rr + i, Fr + t_res[t] + top + i);
+    for (int i = lane; i < n; i += 32) cp_async_elem(rr + i, Fr + t_res[t] + row0 + i);
   cp_async_wait_all();
   __syncwarp();
   if (MODE == 0) {
@@ -362,6 +369,56 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
         for (int a = 0; a < 16; ++a)
           if (a < d1 && (MODE == 1 || !diag || a <= w)) atomicAdd(out + (w - w0) * stride + a, T(acc[a]));
       }
+    }
+  }
+}
+
+// The eliminated part of H = J'J, b = J'r from the raw tables (no device counterpart in the reference, whose callers
+// fill a SchurBlockHessian block by block with addblock!, src/schur_assembly.jl:140-246; the reference's own fixtures
+// form J'J in FP64 and round it once, test/fixtures/QRFixtures.jl:109-120): one warp per eliminated table, sums over
+// its data rows (the first M - d_e; the damping rows are last) accumulated in FP64 and rounded once. E_e (d_e x d_e,
+// column-major at the point's E offset), b_e, and per entry the coupling block, d_e x d_r column-major at its C offset
+// (entry (a, w) = sum_i J[i, point col a] J[i, entry col w], add_coupling!'s transposed storage). Each table owns its
+// outputs, so every entry is written once.
+template <class T>
+__global__ void __launch_bounds__(128) k_qr_point_gram(int64_t neb, const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_cols,
+                                                       const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_res,
+                                                       const int32_t* __restrict__ t_ptr, const int32_t* __restrict__ u_ret,
+                                                       const int32_t* __restrict__ u_col, const int32_t* __restrict__ r_dims,
+                                                       const int32_t* __restrict__ e_dims, const int32_t* __restrict__ boff_e,
+                                                       const int64_t* __restrict__ t_eoff, const int64_t* __restrict__ u_coff,
+                                                       const T* __restrict__ J, const double* __restrict__ res, T* __restrict__ E,
+                                                       T* __restrict__ Cd, double* __restrict__ b_e) {
+  const int64_t e = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (e >= neb) return;
+  const int M = t_rows[e], de = e_dims[e], n = M - de, ce = t_cols[e] - 1 - de;
+  const T* tab = J + t_raw[e];
+  const T* P = tab + (int64_t)ce * M;   // the point's columns
+  const double* rr = res + t_res[e];
+  for (int q = lane; q < de * de + de; q += 32) {
+    double acc = 0.0;
+    if (q < de * de) {
+      const T* x = P + (int64_t)(q % de) * M;
+      const T* y = P + (int64_t)(q / de) * M;
+      for (int i = 0; i < n; ++i) acc += (double)x[i] * (double)y[i];
+      E[t_eoff[e] + q] = T(acc);
+    } else {
+      const T* x = P + (int64_t)(q - de * de) * M;
+      for (int i = 0; i < n; ++i) acc += (double)x[i] * rr[i];
+      b_e[boff_e[e] + (q - de * de)] = acc;
+    }
+  }
+  for (int u = t_ptr[e]; u < t_ptr[e + 1]; ++u) {
+    const int dr = r_dims[u_ret[u]];
+    const T* Y = tab + (int64_t)u_col[u] * M;
+    for (int q = lane; q < de * dr; q += 32) {
+      const int a = q % de, w = q / de;
+      const T* x = P + (int64_t)a * M;
+      const T* y = Y + (int64_t)w * M;
+      double acc = 0.0;
+      for (int i = 0; i < n; ++i) acc += (double)x[i] * (double)y[i];
+      Cd[u_coff[u] + q] = T(acc);
     }
   }
 }
@@ -553,6 +610,24 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
   }
   upload(P->tp_ptr, tp_ptr, s);
   upload(P->tp_blk, tp_blk, s);
+  {
+    // SchurStructure's prefix-sum offsets (src/schur_structure.jl:70-166): eoffsets over d_e^2, coffsets over d_e d_r in
+    // coupling order, which is the entry order of the eliminated tables (each point's entries in ascending retained order)
+    std::vector<int64_t> eoff(neb), coff((size_t)d->table_ptr[neb]);
+    int64_t eo = 0, co = 0;
+    for (int64_t e = 0; e < neb; ++e) {
+      eoff[e] = eo;
+      eo += d->e_dims[e] * d->e_dims[e];
+      for (int64_t u = d->table_ptr[e]; u < d->table_ptr[e + 1]; ++u) {
+        coff[u] = co;
+        co += d->e_dims[e] * d->r_dims[d->entry_retained[u]];
+      }
+    }
+    P->E_len = eo;
+    P->C_len = co;
+    upload(P->t_eoff, eoff, s);
+    upload(P->u_coff, coff, s);
+  }
   upload(P->blk_stride, b_stride, s);
   upload(P->blk_base_sparse, b_base, s);
   upload(P->blk_base_dense, b_base_dense, s);
@@ -618,7 +693,7 @@ static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr,
 
 // One launch per Gram class: MODE 0 writes S (sparse or dense) and g, MODE 1 the diagonal blocks D.
 template <class T, int MODE>
-static void gram(QRPlan* P, T* S, bool dense, double* g, const T* F, const double* Fr) {
+static void gram(QRPlan* P, T* S, bool dense, double* g, const T* F, const double* Fr, bool from_raw = false) {
   cudaStream_t s = P->ctx->stream;
   for (int c = 0; c < 8; ++c) {
     const auto& k = P->gram_classes[c];
@@ -632,7 +707,7 @@ static void gram(QRPlan* P, T* S, bool dense, double* g, const T* F, const doubl
         P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(),
         P->boff_r.as<int32_t>(), P->tp_ptr.as<int32_t>(), P->tp_blk.as<int32_t>(),
         dense ? P->blk_base_dense.as<int64_t>() : P->blk_base_sparse.as<int64_t>(), dense ? nullptr : P->blk_stride.as<int32_t>(), P->nr,
-        P->doff.as<int64_t>(), P->max_dr, F, Fr, S, g);
+        P->doff.as<int64_t>(), P->max_dr, F, Fr, S, g, from_raw ? 1 : 0);
     P->launches += 1;
   }
   BLS_CUDA(cudaGetLastError());
@@ -647,6 +722,24 @@ static void normal(QRPlan* P, T* S, bool dense, double* g, const T* F, const dou
   k_fill_t<double><<<(unsigned)std::max(1, grid_for(P->nr, 256)), 256, 0, s>>>(g, P->nr);
   P->launches += 2;
   gram<T, 0>(P, S, dense, g, F, Fr);
+}
+
+// H = J'J and b = J'r from the raw tables into the SchurBlockHessian layout of the same structure: E_data, C_data,
+// R on the reduced pattern (upper blocks; sparse S.nzval layout or dense column-major nr x nr) and b = [b_r; b_e].
+template <class T>
+static void assemble(QRPlan* P, const T* J, const double* r, T* E, T* Cd, T* R, bool dense, double* b) {
+  if (!dense && !P->has_sparse) throw Error(BLS_EINVAL, "the QR plan was created without a sparse pattern");
+  if (!J || !r || !E || !Cd || !R || !b) throw Error(BLS_EINVAL, "a device pointer is NULL");
+  cudaStream_t s = P->ctx->stream;
+  const int64_t nS = dense ? P->nr * P->nr : P->nnzS;
+  k_fill_t<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(grid_for(nS, 256), 148 * 8)), 256, 0, s>>>(R, nS);
+  k_fill_t<double><<<(unsigned)std::max(1, grid_for(P->nr, 256)), 256, 0, s>>>(b, P->nr);
+  k_qr_point_gram<T><<<(unsigned)grid_for(P->neblocks * 32, 128), 128, 0, s>>>(
+      P->neblocks, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(),
+      P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(), P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(),
+      P->t_eoff.as<int64_t>(), P->u_coff.as<int64_t>(), J, r, E, Cd, b + P->nr);
+  P->launches += 3;
+  gram<T, 0>(P, R, dense, b, J, r, true);
 }
 
 template <class T>
@@ -751,6 +844,16 @@ int bls_reduced_normal_dense(bls_qr_plan* P, int dtype, void* S, double* g, cons
   QR_GUARD({
     if (dtype == BLS_F64) normal<double>(P, (double*)S, true, g, (const double*)F, Fr);
     else if (dtype == BLS_F32) normal<float>(P, (float*)S, true, g, (const float*)F, Fr);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_assemble_hessian(bls_qr_plan* P, int dtype, const void* J, const double* r, void* E, void* C, void* R, int dense, double* b) {
+  QR_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (dtype == BLS_F64) assemble<double>(P, (const double*)J, r, (double*)E, (double*)C, (double*)R, dense != 0, b);
+    else if (dtype == BLS_F32) assemble<float>(P, (const float*)J, r, (float*)E, (float*)C, (float*)R, dense != 0, b);
     else throw Error(BLS_EINVAL, "unknown dtype");
     return BLS_OK;
   })

@@ -271,3 +271,24 @@ def reduced_diagonal_blocks(D: torch.Tensor, ws: QRReductionWorkspace) -> torch.
     _dev(D, "D", int(ws.structure.doffsets[-1]))
     check(_lib.gpu().bls_reduced_diagonal_blocks(ws.handle, ws._T, dptr(D), dptr(ws.factored)))
     return D
+
+
+def assemble_hessian(J: SchurBlockJacobian, ws: QRReductionWorkspace, *, dense: bool = False):
+    """H = J'J and b = J'r of the raw Jacobian J in the SchurBlockHessian layout of the same structure, on the device:
+    (E_data, C_data, R, b) with R the retained blocks on the reduced pattern (dense: column-major nr x nr), upper
+    triangle, and b = [b_r; b_e] in float64. What a caller fills with addblock! from its Jacobian (the reference's
+    fixtures form it as J64'J64, test/fixtures/QRFixtures.jl:109-120). R resets a SchurReductionWorkspace built with
+    r_to_s_map = identity (sparse) like any R on the pattern."""
+    jst = J.structure
+    st = jst.schur
+    if J.data.dtype != ws.dtype:
+        raise ArgumentError(f"J must be {ws.dtype}")
+    if not dense and ws.pattern is None:
+        raise ArgumentError("the workspace was built without a sparse pattern")
+    dev = J.data.device
+    E = torch.empty(st.E_length, dtype=ws.dtype, device=dev)
+    Cd = torch.empty(st.C_length, dtype=ws.dtype, device=dev)
+    R = torch.empty(st.nr * st.nr if dense else ws.pattern.nnz, dtype=ws.dtype, device=dev)
+    b = torch.empty(st.nr + st.ne, dtype=torch.float64, device=dev)
+    check(_lib.gpu().bls_assemble_hessian(ws.handle, ws._T, dptr(J.data), dptr(J.r), dptr(E), dptr(Cd), dptr(R), int(dense), dptr(b)))
+    return E, Cd, R, b

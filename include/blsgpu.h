@@ -269,6 +269,16 @@ int bls_qr_plan_destroy(bls_qr_plan* plan);
  * failed_block NULL = asynchronous. */
 int bls_reduce_qr(bls_qr_plan* plan, int dtype, void* F_dev, double* Fr_dev, const void* Rw_dev, const double* Rr_dev,
                   const double* scaling_e_dev, double lambda, const double* s_dev, int64_t* failed_block);
+/* The normal equations of the raw Jacobian in the Hessian layout of the same structure (no device counterpart in the
+ * reference: its callers fill a SchurBlockHessian with addblock!, src/schur_assembly.jl:140-246, and its fixtures form
+ * H = J'J, b = J'r in FP64, test/fixtures/QRFixtures.jl:109-120): over the data rows of every table (not the damping
+ * rows), E_data (d_e x d_e per eliminated block, SchurStructure's eoffsets), C_data (d_e x d_r per coupling, its
+ * coffsets), R = the retained blocks of J'J on the reduced pattern (dense = 0: S.nzval layout, upper triangle of the
+ * diagonal blocks, other entries zero; dense = 1: column-major nr x nr, upper triangle) and b = J'r = [b_r; b_e]
+ * (FP64). Sums accumulate in FP64; E and C are rounded once, R once per table. R on the pattern resets a Schur plan
+ * built with the identity r -> s map. */
+int bls_assemble_hessian(bls_qr_plan* plan, int dtype, const void* Rw_dev, const double* Rr_dev, void* E_data_dev,
+                         void* C_data_dev, void* R_dev, int dense, double* b_dev);
 /* Verdict of the last reduce_qr on this plan (synchronises): BLS_OK / BLS_NOT_PD (failed_block 1-based) / BLS_EINVAL. */
 int bls_qr_query_status(bls_qr_plan* plan, int64_t* failed_block);
 /* Device kernel launches issued on this plan since the previous call (no counterpart in the reference). */

@@ -354,3 +354,55 @@ def pcg_solve(st: Structure, pat: Pattern, S, g, x, tol=1e-8, maxit=100000, nthr
     f = getattr(lib(), "orc_pcg_solve_" + _sfx(S))
     rc = _chk(f(st.h, pat.h, _p(S), _p(g), _p(x), C.c_double(tol), i64(maxit), C.c_int(nthreads or max_threads()), C.byref(it), C.byref(rel)))
     return rc, int(it.value), float(rel.value)
+
+
+def assemble_hessian(q: QRStructure, Rw, Rr, pat: Pattern | None = None):
+    """H = J'J and b = J'r of the raw tables in the SchurBlockHessian layout (the reference's fixtures form
+    H = J64'J64 and b = J64'r, test/fixtures/QRFixtures.jl:109-120, and fill E_data / C_data / R by the layout of
+    add_eliminated! / add_coupling! / add_retained_pair!, src/schur_assembly.jl:189-246): per table, over its data rows
+    (the damping rows of an eliminated table are its last d_e rows), G = J_t'J_t and v = J_t'r_t in FP64, then
+    E_e = G[point, point] (column-major), C_c = G[point, entry] (d_e x d_r column-major), b = [v over retained
+    columns summed per block; v over the point's columns], and the retained blocks of G summed into R: on `pat`'s
+    S.nzval layout (upper triangle of diagonal blocks) or, with pat None, a column-major dense nr x nr upper triangle."""
+    st = q.st
+    nr, ne = int(st.nr), int(st.ne)
+    E, Cd, b = np.zeros(st.E_length), np.zeros(st.C_length), np.zeros(nr + ne)
+    R = np.zeros(pat.nnz if pat is not None else nr * nr)
+    for t in range(q.ntables):
+        M, C1, top = int(q.table_nrows[t]), int(q.table_ncols[t]) - 1, int(q.table_top[t])
+        n = M - top
+        off, ro = int(q.raw_offsets[t]), int(q.residual_offsets[t])
+        Jt = np.asarray(Rw[off:off + M * C1], np.float64).reshape(C1, M).T[:n]
+        rt = np.asarray(Rr[ro:ro + n], np.float64)
+        G, v = Jt.T @ Jt, Jt.T @ rt
+        u0, u1e = int(q.table_ptr[t]), int(q.table_ptr[t + 1])
+        cols = [(int(q.entry_col[u]), int(st.r_dims[q.entry_retained[u]]), int(q.entry_retained[u])) for u in range(u0, u1e)]
+        if t < st.neblocks:
+            de = int(st.e_dims[t])
+            pc = slice(C1 - de, C1)
+            eo = int(st.eoffsets[t])
+            E[eo:eo + de * de] = G[pc, pc].ravel(order="F")
+            b[nr + int(st.boffsets_e[t]):nr + int(st.boffsets_e[t]) + de] = v[pc]
+            for k, (c0, dr, r) in enumerate(cols):
+                co = int(st.coffsets[int(st.eliminated_ptr[t]) + k])
+                Cd[co:co + de * dr] = G[pc, c0:c0 + dr].ravel(order="F")
+        for k2, (c2, d2, r2) in enumerate(cols):
+            o2 = int(st.boffsets_r[r2])
+            b[o2:o2 + d2] += v[c2:c2 + d2]
+            for k1 in range(k2 + 1):
+                c1, d1, r1 = cols[k1]
+                o1 = int(st.boffsets_r[r1])
+                blk = G[c1:c1 + d1, c2:c2 + d2]
+                if pat is not None:
+                    lo, hi = int(pat.block_colptr[r2]), int(pat.block_colptr[r2 + 1])
+                    kb = lo + int(np.searchsorted(pat.block_rowval[lo:hi], r1))
+                    assert pat.block_rowval[kb] == r1
+                for w in range(d2):
+                    for a in range(d1):
+                        if k1 == k2 and a > w:
+                            continue
+                        if pat is not None:
+                            R[int(pat.S_colptr[o2 + w]) + int(pat.block_row_offsets[kb]) + a] += blk[a, w]
+                        else:
+                            R[o1 + a + nr * (o2 + w)] += blk[a, w]
+    return E, Cd, R, b

@@ -233,3 +233,53 @@ def test_qr_mixed_beats_schur_mixed(bls):
     err_schur = relerr(S.double().cpu().numpy(), oS)
     err_qr = relerr(qr["Ss"], qr["oSs"])
     assert err_qr * 10 <= err_schur, (err_qr, err_schur)
+
+
+@pytest.mark.parametrize("name", list(QR_FIXTURES))
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+def test_assembly_vs_oracle(bls, name, dtype):
+    """H = J'J, b = J'r from the raw tables into the Hessian layout (E, C, R on the pattern and dense, b) against the
+    oracle's FP64 assembly of the same stored tables: 1e-13 in FP64; FP32 rounded once (E, C) or per table (R)."""
+    j, o, Rw, Rr, Jf, rf, sc_e = fixture(bls, name)
+    npdt = np.float32 if dtype == torch.float32 else np.float64
+    Rw_s = Rw.astype(npdt)
+    pairs = bls.free_block_pairs(j)
+    pat = bls.build_schur_pattern(j.schur, pairs)
+    opat = orc.Pattern(o.st, pairs)
+    ws = bls.QRReductionWorkspace(j, pat, dtype)
+    J = bls.SchurBlockJacobian(j, dtype, data=cu(Rw_s), r=cu(Rr))
+    oE, oC, oR, ob = orc.assemble_hessian(o, Rw_s.astype(np.float64), Rr, opat)
+    _, _, oRd, _ = orc.assemble_hessian(o, Rw_s.astype(np.float64), Rr, None)
+    tol = 1e-13 if dtype == torch.float64 else 2e-6
+    for dense, oRx in ((False, oR), (True, oRd)):
+        E, Cd, R, b = bls.assemble_hessian(J, ws, dense=dense)
+        assert relerr(E.double().cpu().numpy(), oE) <= tol
+        assert relerr(Cd.double().cpu().numpy(), oC) <= tol
+        assert relerr(R.double().cpu().numpy(), oRx) <= tol
+        assert relerr(b.cpu().numpy(), ob) <= 1e-13
+
+
+@pytest.mark.parametrize("name", ["bundle adjustment", "free groups", "coupled to all"])   # d_e <= 3 (the Schur path's limit)
+def test_assembled_schur_equals_qr_reduction(bls, name):
+    """The two elimination paths from one Jacobian on the device: assemble H = J'J, reduce it by the Schur complement
+    (R reset from the pattern through the identity map, the eliminated blocks damped by lambda * scaling_e), and the
+    QR path's J~'J~ and J~'r~ agree at 1e-10 (the reference's own identity, test/qr_reduction.jl:20-58)."""
+    j, o, Rw, Rr, Jf, rf, sc_e = fixture(bls, name)
+    lam = 0.3
+    pairs = bls.free_block_pairs(j)
+    pat = bls.build_schur_pattern(j.schur, pairs)
+    qws = bls.QRReductionWorkspace(j, pat, torch.float64)
+    J = bls.SchurBlockJacobian(j, torch.float64, data=cu(Rw), r=cu(Rr))
+    E, Cd, R, b = bls.assemble_hessian(J, qws)
+    st, nr = j.schur, j.schur.nr
+    sws = bls.SchurReductionWorkspace(st, pat, r_to_s_map=np.arange(pat.nnz))
+    S = torch.zeros(pat.nnz, dtype=torch.float64, device=DEV)
+    g = torch.zeros(nr, dtype=torch.float64, device=DEV)
+    bls.reset_schur_sparse(S, R, None, None, torch.zeros(nr, dtype=torch.float64, device=DEV), lam, sws)
+    assert bls.reduce_schur_sparse(S, g, b[:nr].contiguous(), b[nr:].contiguous(), cu(sc_e), lam, st, E, Cd, None, None, None, None, sws)
+    assert bls.reduce_qr(qws, J, cu(sc_e), lam)
+    Sq = torch.zeros(pat.nnz, dtype=torch.float64, device=DEV)
+    gq = torch.zeros(nr, dtype=torch.float64, device=DEV)
+    bls.reduced_normal_sparse(Sq, gq, qws, pat)
+    assert relerr(S.cpu().numpy(), Sq.cpu().numpy()) <= 1e-10
+    assert relerr(g.cpu().numpy(), gq.cpu().numpy()) <= 1e-10
