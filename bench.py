@@ -330,6 +330,40 @@ def run_ours_qr(args, rank: int, world: int) -> dict | None:
     torch.cuda.synchronize()
     e2e_ms = a.elapsed_time(b)
     assert ws32.query_status()
+
+    # the Hessian route from the same Jacobian: assemble H = J'J, b = J'r on the device (FP32 tables, FP64 sums), then
+    # the mixed Schur reduction of it (R reset from the pattern through the identity map); the assembly alone and the
+    # whole route, per step
+    sws = bls.SchurReductionWorkspace(jst.schur, pat, r_to_s_map=np.arange(pat.nnz), device=dev.index)
+    Sh = torch.zeros(pat.nnz, dtype=torch.float32, device=dev)
+    gh = torch.zeros(jst.schur.nr, dtype=torch.float64, device=dev)
+    zr = torch.zeros(jst.schur.nr, dtype=torch.float64, device=dev)
+    nr = jst.schur.nr
+
+    def hess_step(mid=None):
+        E, Cd, R, bb = bls.assemble_hessian(J32, ws32)
+        if mid is not None:
+            mid.record()
+        bls.reset_schur_sparse(Sh, R, None, None, zr, p.lam, sws)
+        bls.reduce_schur_sparse(Sh, gh, bb[:nr], bb[nr:], sc_e, p.lam, jst.schur, E, Cd, None, None, None, None, sws, sync=False)
+
+    for _ in range(args.warmup):
+        hess_step()
+    assert sws.query_status()
+    asm_ms, route_ms = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record()
+        hess_step(b)
+        c.record()
+        torch.cuda.synchronize()
+        asm_ms.append(a.elapsed_time(b))
+        route_ms.append(a.elapsed_time(c))
+    assert sws.query_status()
+    asm = statistics.median(asm_ms)
+    st_ = jst.schur
+    asm_bytes = int(jst.raw_length * 4 + jst.residual_length * 8 + (st_.E_length + st_.C_length + pat.nnz) * 4 + (st_.nr + st_.ne) * 8)
     if rank != 0:
         return None
     nobs = p.nobs
@@ -355,6 +389,10 @@ def run_ours_qr(args, rank: int, world: int) -> dict | None:
                 "h2d_bytes_per_step": hRw.numel() * 4 + hRr.numel() * 8, "d2h_bytes_per_step": hS.numel() * 4 + hg.numel() * 8},
         "gpu_launches": launches,
         "clocks": clk.summary(),
+        "hessian_route": {"assemble_ms": asm, "assemble_gbs": asm_bytes / (asm / 1e3) / 1e9, "assemble_frac": asm_bytes / (asm / 1e3) / 1e9 / hbm,
+                          "assemble_bytes": asm_bytes, "ms_per_step": statistics.median(route_ms),
+                          "obs_per_s": nobs / (statistics.median(route_ms) / 1e3),
+                          "step": "assemble_hessian (J'J, J'r from the f32 tables) + mixed reset_schur_sparse + reduce_schur_sparse"},
     }
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_qr(spec, seconds=args.cpu_seconds)

@@ -16,8 +16,8 @@ Workloads:               scenes.workload, scenes.hessian_problem, scenes.jacobia
 from ._lib import ArgumentError, BlsError, DimensionMismatch
 from .layout import DEFAULT_MIN_WORK, SchurPattern, SchurStructure, build_r_to_s_map, build_schur_pattern, sparse_with_map
 from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce_schur_dense, reduce_schur_sparse,
-                        reset_reduce_schur_sparse_host, reset_schur_dense, reset_schur_sparse, scatter_copy)
-from .qr import (QRReductionWorkspace, SchurBlockJacobian, assemble_hessian, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
+                        prepare_scale, reset_reduce_schur_sparse_host, reset_schur_dense, reset_schur_sparse, scatter_copy)
+from .qr import (QRReductionWorkspace, SchurBlockJacobian, assemble_hessian, jtj_diag, jtj_quadform, jtr, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
                  reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse)
 from .pcg import BlockJacobi, PCGResult, PCGWorkspace, RefinedResult, factor_diagonal_blocks, solve_diagonal_blocks
 from . import batch, gnn, scenes
@@ -26,7 +26,7 @@ __all__ = [
     "ArgumentError", "BlsError", "DimensionMismatch", "DEFAULT_MIN_WORK", "SchurPattern", "SchurStructure", "build_r_to_s_map",
     "build_schur_pattern", "sparse_with_map", "SchurReductionWorkspace", "backsubstitute", "context", "reduce_schur_dense",
     "reduce_schur_sparse", "reset_reduce_schur_sparse_host", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
-    "SchurBlockJacobian", "SchurJacobianStructure", "assemble_hessian", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
+    "SchurBlockJacobian", "SchurJacobianStructure", "assemble_hessian", "jtj_diag", "jtj_quadform", "jtr", "prepare_scale", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
     "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "BlockJacobi", "PCGResult", "PCGWorkspace", "RefinedResult",
     "factor_diagonal_blocks", "solve_diagonal_blocks", "gnn", "batch",
 ]

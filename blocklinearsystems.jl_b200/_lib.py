@@ -111,6 +111,10 @@ def gpu() -> C.CDLL:
             "bls_reduced_normal_dense": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_reduced_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, vp]),
             "bls_assemble_hessian": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, C.c_int, vp]),
+            "bls_jtr": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+            "bls_jtj_diag": (C.c_int, [vp, C.c_int, vp, vp]),
+            "bls_jtj_quadform": (C.c_int, [vp, C.c_int, vp, vp, pdbl]),
+            "bls_prepare_scale": (C.c_int, [vp, C.c_int, i64, vp, C.c_double, vp, vp, C.c_int, C.POINTER(C.c_int)]),
             "bls_block_jacobi_create": (C.c_int, [vp, i64, p64, C.POINTER(vp)]),
             "bls_block_jacobi_destroy": (C.c_int, [vp]),
             "bls_factor_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, p64]),

@@ -57,6 +57,7 @@ int bls_ctx_create(int device, bls_ctx** out) {
 }
 
 int bls_ctx_destroy(bls_ctx* ctx) {
+  if (ctx && ctx->flag) cudaFree(ctx->flag);
   delete ctx;
   return BLS_OK;
 }

@@ -59,4 +59,5 @@ void upload(DevBuf& buf, const std::vector<T>& v, cudaStream_t s) {
 struct bls_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  int* flag = nullptr;   // device scratch word for calls that report a device-side decision (allocated at first use)
 };

@@ -55,6 +55,9 @@ struct QRPlan {
   // an eliminated table (its coupling), and the lengths
   DevBuf t_eoff, u_coff;
   int64_t E_len = 0, C_len = 0;
+  // per retained block its entries in ascending order (the structure's retained_ptr / retained_entry), per entry its table
+  DevBuf q_rptr, q_rent, u_tab;
+  DevBuf q_total;   // one FP64 accumulator (jtj_quadform)
   DevBuf status;
   long long* host_status = nullptr;
   int64_t launches = 0;
@@ -423,6 +426,103 @@ __global__ void __launch_bounds__(128) k_qr_point_gram(int64_t neb, const int32_
   }
 }
 
+// Quantities of the full problem from the raw or the factored tables (src/qr_reduced.jl:515-640), every row of each
+// table, FP64 accumulation. MODE 0, jtr! (:575-584): g = [J'r over the retained columns, summed per block; J'r over each
+// point's columns]. MODE 1, jtj_diag! (:586-595): the squared column norms. Retained part: one warp per retained
+// block, lanes over its entries (sum_retained_columns!, :536-560), then a butterfly sum.
+__device__ __forceinline__ double warp_sum_q(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <class T, int MODE>
+__global__ void __launch_bounds__(256) k_jt_retained(int64_t nrb, const int32_t* __restrict__ rptr, const int32_t* __restrict__ rent,
+                                                     const int32_t* __restrict__ u_tab, const int32_t* __restrict__ u_col,
+                                                     const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                                                     const int32_t* __restrict__ t_rows, const int64_t* __restrict__ t_raw,
+                                                     const int64_t* __restrict__ t_res, const T* __restrict__ D,
+                                                     const double* __restrict__ Rv, double* __restrict__ out) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= nrb) return;
+  const int dr = r_dims[r];
+  double acc[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) acc[j] = 0.0;
+  for (int k = rptr[r] + lane; k < rptr[r + 1]; k += 32) {
+    const int u = rent[k], t = u_tab[u], M = t_rows[t];
+    const T* cb = D + t_raw[t] + (int64_t)u_col[u] * M;
+    const double* rb = Rv + t_res[t];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      if (j >= dr) break;
+      const T* c = cb + (int64_t)j * M;
+      double a = 0.0;
+      for (int i = 0; i < M; ++i) a += MODE == 0 ? (double)c[i] * rb[i] : (double)c[i] * (double)c[i];
+      acc[j] += a;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) acc[j] = warp_sum_q(acc[j]);
+  if (lane < dr) {
+    double v = 0.0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (j == lane) v = acc[j];
+    out[boff_r[r] + lane] = v;
+  }
+}
+// The eliminated part: thread per eliminated table, its d_e point columns (foreach_eliminated_column, :562-573)
+template <class T, int MODE>
+__global__ void k_jt_eliminated(int64_t neb, int64_t nr, const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_cols,
+                                const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_res, const int32_t* __restrict__ e_dims,
+                                const int32_t* __restrict__ boff_e, const T* __restrict__ D, const double* __restrict__ Rv,
+                                double* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= neb) return;
+  const int M = t_rows[e], C = t_cols[e], de = e_dims[e];
+  for (int k = 0; k < de; ++k) {
+    const T* c = D + t_raw[e] + (int64_t)(C - de - 1 + k) * M;
+    const double* rb = Rv + t_res[e];
+    double a = 0.0;
+    for (int i = 0; i < M; ++i) a += MODE == 0 ? (double)c[i] * rb[i] : (double)c[i] * (double)c[i];
+    out[nr + boff_e[e] + k] = a;
+  }
+}
+// jtj_quadform (:597-640): ||J v||^2 = sum over tables and rows of (row . v)^2, FP64. One warp per table, lanes over
+// rows; each table's part is added to one FP64 accumulator.
+template <class T>
+__global__ void __launch_bounds__(256) k_jtj_quadform(int64_t nt, int64_t neb, int64_t nr, const int32_t* __restrict__ t_rows,
+                                                      const int32_t* __restrict__ t_cols, const int64_t* __restrict__ t_raw,
+                                                      const int32_t* __restrict__ t_ptr, const int32_t* __restrict__ u_ret,
+                                                      const int32_t* __restrict__ u_col, const int32_t* __restrict__ r_dims,
+                                                      const int32_t* __restrict__ boff_r, const int32_t* __restrict__ e_dims,
+                                                      const int32_t* __restrict__ boff_e, const T* __restrict__ D,
+                                                      const double* __restrict__ v, double* __restrict__ total) {
+  const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= nt) return;
+  const int M = t_rows[t], C = t_cols[t];
+  const int de = t < neb ? e_dims[t] : 0;
+  const T* tab = D + t_raw[t];
+  double part = 0.0;
+  for (int i = lane; i < M; i += 32) {
+    double y = 0.0;
+    for (int u = t_ptr[t]; u < t_ptr[t + 1]; ++u) {
+      const int r = u_ret[u], ro = boff_r[r];
+      const T* cb = tab + (int64_t)u_col[u] * M + i;
+      for (int j = 0; j < r_dims[r]; ++j) y += (double)cb[(int64_t)j * M] * v[ro + j];
+    }
+    if (de) {
+      const T* cb = tab + (int64_t)(C - de - 1) * M + i;
+      const int64_t eo = nr + boff_e[t];
+      for (int k = 0; k < de; ++k) y += (double)cb[(int64_t)k * M] * v[eo + k];
+    }
+    part += y * y;
+  }
+  part = warp_sum_q(part);
+  if (lane == 0 && part != 0.0) atomicAdd(total, part);
+}
+
 // qr_backsubstitute_group! (src/qr_reduced.jl:24-93): thread per eliminated table, FP64
 template <class T>
 __global__ void k_qr_backsub(int64_t ne_tab, const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_cols,
@@ -627,6 +727,19 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
     P->C_len = co;
     upload(P->t_eoff, eoff, s);
     upload(P->u_coff, coff, s);
+    std::vector<int32_t> rptr(nrb + 1, 0), rent((size_t)nent), utab((size_t)nent);
+    for (int64_t u = 0; u < nent; ++u) rptr[d->entry_retained[u] + 1] += 1;
+    for (int64_t r = 0; r < nrb; ++r) rptr[r + 1] += rptr[r];
+    std::vector<int32_t> fill(rptr.begin(), rptr.end() - 1);
+    for (int64_t t = 0; t < nt; ++t)
+      for (int64_t u = d->table_ptr[t]; u < d->table_ptr[t + 1]; ++u) {
+        utab[u] = (int32_t)t;
+        rent[fill[d->entry_retained[u]]++] = (int32_t)u;
+      }
+    upload(P->q_rptr, rptr, s);
+    upload(P->q_rent, rent, s);
+    upload(P->u_tab, utab, s);
+    P->q_total.alloc(sizeof(double));
   }
   upload(P->blk_stride, b_stride, s);
   upload(P->blk_base_sparse, b_base, s);
@@ -742,6 +855,38 @@ static void assemble(QRPlan* P, const T* J, const double* r, T* E, T* Cd, T* R, 
   gram<T, 0>(P, R, dense, b, J, r, true);
 }
 
+// jtr! (MODE 0) / jtj_diag! (MODE 1) of the tables D with residual Rv into out[nr + ne]
+template <class T, int MODE>
+static void jt_columns(QRPlan* P, double* out, const T* D, const double* Rv) {
+  if (!out || !D || (MODE == 0 && !Rv)) throw Error(BLS_EINVAL, "a device pointer is NULL");
+  cudaStream_t s = P->ctx->stream;
+  k_jt_retained<T, MODE><<<(unsigned)grid_for(P->nrblocks * 32, 256), 256, 0, s>>>(
+      P->nrblocks, P->q_rptr.as<int32_t>(), P->q_rent.as<int32_t>(), P->u_tab.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(),
+      P->boff_r.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(), D, Rv, out);
+  k_jt_eliminated<T, MODE><<<(unsigned)grid_for(P->neblocks, 128), 128, 0, s>>>(
+      P->neblocks, P->nr, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(),
+      P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), D, Rv, out);
+  P->launches += 2;
+  BLS_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static double jtj_quadform(QRPlan* P, const T* D, const double* v) {
+  if (!D || !v) throw Error(BLS_EINVAL, "a device pointer is NULL");
+  cudaStream_t s = P->ctx->stream;
+  double* tot = P->q_total.as<double>();
+  k_fill_t<double><<<1, 32, 0, s>>>(tot, 1);
+  k_jtj_quadform<T><<<(unsigned)grid_for(P->ntables * 32, 256), 256, 0, s>>>(
+      P->ntables, P->neblocks, P->nr, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_ptr.as<int32_t>(),
+      P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), P->e_dims.as<int32_t>(),
+      P->boff_e.as<int32_t>(), D, v, tot);
+  P->launches += 2;
+  double h = 0.0;
+  BLS_CUDA(cudaMemcpyAsync(&h, tot, sizeof(double), cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
 template <class T>
 static void diagonal_blocks(QRPlan* P, T* D, const T* F) {
   cudaStream_t s = P->ctx->stream;
@@ -844,6 +989,36 @@ int bls_reduced_normal_dense(bls_qr_plan* P, int dtype, void* S, double* g, cons
   QR_GUARD({
     if (dtype == BLS_F64) normal<double>(P, (double*)S, true, g, (const double*)F, Fr);
     else if (dtype == BLS_F32) normal<float>(P, (float*)S, true, g, (const float*)F, Fr);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_jtr(bls_qr_plan* P, int dtype, double* g, const void* D, const double* Rv) {
+  QR_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (dtype == BLS_F64) jt_columns<double, 0>(P, g, (const double*)D, Rv);
+    else if (dtype == BLS_F32) jt_columns<float, 0>(P, g, (const float*)D, Rv);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_jtj_diag(bls_qr_plan* P, int dtype, double* d, const void* D) {
+  QR_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (dtype == BLS_F64) jt_columns<double, 1>(P, d, (const double*)D, nullptr);
+    else if (dtype == BLS_F32) jt_columns<float, 1>(P, d, (const float*)D, nullptr);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_jtj_quadform(bls_qr_plan* P, int dtype, const void* D, const double* v, double* result) {
+  QR_GUARD({
+    if (!P || !result) throw Error(BLS_EINVAL, "null argument");
+    if (dtype == BLS_F64) *result = jtj_quadform<double>(P, (const double*)D, v);
+    else if (dtype == BLS_F32) *result = jtj_quadform<float>(P, (const float*)D, v);
     else throw Error(BLS_EINVAL, "unknown dtype");
     return BLS_OK;
   })

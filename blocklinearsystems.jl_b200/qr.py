@@ -292,3 +292,44 @@ def assemble_hessian(J: SchurBlockJacobian, ws: QRReductionWorkspace, *, dense: 
     b = torch.empty(st.nr + st.ne, dtype=torch.float64, device=dev)
     check(_lib.gpu().bls_assemble_hessian(ws.handle, ws._T, dptr(J.data), dptr(J.r), dptr(E), dptr(Cd), dptr(R), int(dense), dptr(b)))
     return E, Cd, R, b
+
+
+def _tables(src, ws):
+    """(plan, tables, residual, dtype code) of a SchurBlockJacobian (raw tables, with the workspace `ws` that holds the
+    plan) or of a QRReductionWorkspace (its factored tables)."""
+    if isinstance(src, QRReductionWorkspace):
+        return src, src.factored, src.fres
+    if ws is None:
+        raise ArgumentError("a SchurBlockJacobian needs the QRReductionWorkspace of its structure")
+    if src.data.dtype != ws.dtype:
+        raise ArgumentError(f"J must be {ws.dtype}")
+    return ws, src.data, src.r
+
+
+def jtr(g: torch.Tensor, src, ws: QRReductionWorkspace | None = None) -> torch.Tensor:
+    """jtr!(g, src) (src/qr_reduced.jl:575-584): the gradient g = J'r = [g_r; g_e] of the full problem, from the raw
+    tables of a SchurBlockJacobian or the factored tables of a QRReductionWorkspace (every row, FP64 sums)."""
+    w, D, Rv = _tables(src, ws)
+    st = w.structure.schur
+    _dev(g, "g", st.nr + st.ne, torch.float64)
+    check(_lib.gpu().bls_jtr(w.handle, w._T, dptr(g), dptr(D), dptr(Rv)))
+    return g
+
+
+def jtj_diag(d: torch.Tensor, src, ws: QRReductionWorkspace | None = None) -> torch.Tensor:
+    """jtj_diag!(d, src) (src/qr_reduced.jl:586-595): the squared column norms of J, diag(J'J) = [d_r; d_e], FP64."""
+    w, D, _ = _tables(src, ws)
+    st = w.structure.schur
+    _dev(d, "d", st.nr + st.ne, torch.float64)
+    check(_lib.gpu().bls_jtj_diag(w.handle, w._T, dptr(d), dptr(D)))
+    return d
+
+
+def jtj_quadform(src, v: torch.Tensor, ws: QRReductionWorkspace | None = None) -> float:
+    """jtj_quadform(src, v) (src/qr_reduced.jl:597-640): ||J v||^2 = v'(J'J)v for v = [v_r; v_e], FP64."""
+    w, D, _ = _tables(src, ws)
+    st = w.structure.schur
+    _dev(v, "v", st.nr + st.ne, torch.float64)
+    out = C.c_double(0.0)
+    check(_lib.gpu().bls_jtj_quadform(w.handle, w._T, dptr(D), dptr(v), C.byref(out)))
+    return float(out.value)

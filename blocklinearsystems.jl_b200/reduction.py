@@ -279,6 +279,23 @@ def backsubstitute(x_e: torch.Tensor, x_r: torch.Tensor, structure, C_data: torc
     check(_lib.gpu().bls_backsubstitute(ws.handle, T, dptr(x_e), dptr(x_r), dptr(C_data), dptr(s_r), dptr(s_e)))
 
 
+def prepare_scale(s: torch.Tensor, d: torch.Tensor, lam: float, sc: torch.Tensor, dtype=torch.float64, *, stale: bool) -> bool:
+    """prepare_scale! (src/conditioning.jl:60-87): s = the conditioning scale of every variable from the diagonal d (as
+    filled) and the damping lam * sc, for a system stored in `dtype`; recomputed when `stale` (the first solve of a
+    fill) or when some variable has drifted out of [2^-16, 2^16] (|d + lam sc| s^2) and its scale would change. Returns
+    whether s was rewritten. Bit-identical to the reference's scales."""
+    n = s.numel()
+    for name, t in (("s", s), ("d", d), ("sc", sc)):
+        _dev(t, name, n, torch.float64)
+    T = BLS_F64 if dtype == torch.float64 else BLS_F32 if dtype == torch.float32 else None
+    if T is None:
+        raise ArgumentError(f"dtype must be float64 or float32, got {dtype}")
+    rec = C.c_int(0)
+    check(_lib.gpu().bls_prepare_scale(context(s.device.index or 0), T, n, dptr(d), float(lam), dptr(sc), dptr(s), int(stale),
+                                       C.byref(rec)))
+    return bool(rec.value)
+
+
 def scatter_copy(dest: torch.Tensor, src: torch.Tensor, scatter_map: torch.Tensor) -> torch.Tensor:
     """copyto!(csc, bsm, scatter_map): dest[i] = src[scatter_map[i]] (src/SparseBlockLinearSystem.jl:356-362)."""
     _dev(scatter_map, "scatter_map", dest.numel(), torch.int64)

@@ -279,6 +279,14 @@ int bls_reduce_qr(bls_qr_plan* plan, int dtype, void* F_dev, double* Fr_dev, con
  * built with the identity r -> s map. */
 int bls_assemble_hessian(bls_qr_plan* plan, int dtype, const void* Rw_dev, const double* Rr_dev, void* E_data_dev,
                          void* C_data_dev, void* R_dev, int dense, double* b_dev);
+/* Quantities of the full problem from tables D (the raw J.data or the factored ws.factored, dtype) and their FP64
+ * residual Rv (J.r or ws.fres), over every row of each table, FP64 sums:
+ * jtr!(g, src) (src/qr_reduced.jl:575-584): g[nr + ne] = J'r, retained columns summed per block, then each point's;
+ * jtj_diag!(d, src) (:586-595): d[nr + ne] = the squared column norms of J;
+ * jtj_quadform(src, v) (:597-640): *result = ||J v||^2 for v[nr + ne] (synchronises). */
+int bls_jtr(bls_qr_plan* plan, int dtype, double* g_dev, const void* D_dev, const double* Rv_dev);
+int bls_jtj_diag(bls_qr_plan* plan, int dtype, double* d_dev, const void* D_dev);
+int bls_jtj_quadform(bls_qr_plan* plan, int dtype, const void* D_dev, const double* v_dev, double* result);
 /* Verdict of the last reduce_qr on this plan (synchronises): BLS_OK / BLS_NOT_PD (failed_block 1-based) / BLS_EINVAL. */
 int bls_qr_query_status(bls_qr_plan* plan, int64_t* failed_block);
 /* Device kernel launches issued on this plan since the previous call (no counterpart in the reference). */
@@ -340,6 +348,15 @@ int bls_pcg_solve_refined(bls_pcg_plan* plan, bls_schur_plan* schur, int dtype, 
                           const double* scaling_r_dev, double lambda, const void* C_data_dev, const double* g_dev, double* x_dev,
                           double tol, double inner_tol, int64_t max_outer, int64_t inner_maxit, int64_t* outer_iterations,
                           int64_t* inner_iterations, double* rel_residual, int64_t* failed_block);
+/* prepare_scale! (src/conditioning.jl:60-87) of an EliminationConditioning: s[n] = the conditioning scale of each
+ * variable (conditioning_scale, :29-36: the power of two nearest on a log scale to 1/(1e-12 + sqrt|d_j + lambda sc_j|),
+ * at least floatmin of dtype, 1 for a non-finite entry), computed for every variable when stale is set, else only when
+ * some variable's |d_j + lambda sc_j| s_j^2 lies outside [2^-16, 2^16] and its scale would change; lambda below 0 counts
+ * as 0. d, sc, s device vectors. *recomputed (may be NULL; synchronises) = whether s was rewritten. Bit-identical to
+ * the reference's scales. */
+int bls_prepare_scale(bls_ctx* ctx, int dtype, int64_t n, const double* d_dev, double lambda, const double* sc_dev, double* s_dev,
+                      int stale, int* recomputed);
+
 /* Device kernel launches issued on this plan since the previous call (no counterpart in the reference). */
 int64_t bls_pcg_plan_counters(bls_pcg_plan* plan);
 /* Replace the block-Jacobi solve in later bls_pcg_solve calls by z_b = B_b r_b with the dense symmetric positive definite

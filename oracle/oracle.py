@@ -406,3 +406,89 @@ def assemble_hessian(q: QRStructure, Rw, Rr, pat: Pattern | None = None):
                         else:
                             R[o1 + a + nr * (o2 + w)] += blk[a, w]
     return E, Cd, R, b
+
+
+def _table(q: QRStructure, D, t):
+    M, C1 = int(q.table_nrows[t]), int(q.table_ncols[t]) - 1
+    off = int(q.raw_offsets[t])
+    return np.asarray(D[off:off + M * C1], np.float64).reshape(C1, M).T, M, C1
+
+
+def jtr(q: QRStructure, D, Rv, *, diag=False):
+    """jtr!(g, src) (src/qr_reduced.jl:575-584), or with diag=True jtj_diag!(d, src) (:586-595), from tables D (raw or
+    factored) and their residual Rv: per retained block the sum over its entries, in retained_entry order, of each
+    column's dot with the residual (or itself) over every row of the entry's table (sum_retained_columns!, :536-560);
+    per eliminated block its point columns' dots (foreach_eliminated_column, :562-573). FP64."""
+    st = q.st
+    nr = int(st.nr)
+    out = np.zeros(nr + int(st.ne))
+    for r in range(int(st.nrblocks)):
+        ro, dr = int(st.boffsets_r[r]), int(st.r_dims[r])
+        for k in range(int(q.retained_ptr[r]), int(q.retained_ptr[r + 1])):
+            u = int(q.retained_entry[k])
+            t = int(q.entry_table[u])
+            A, M, _ = _table(q, D, t)
+            rv = None if diag else np.asarray(Rv[int(q.residual_offsets[t]):int(q.residual_offsets[t]) + M], np.float64)
+            for j in range(dr):
+                c = A[:, int(q.entry_col[u]) + j]
+                out[ro + j] += float(np.dot(c, c if diag else rv))
+    for e in range(int(st.neblocks)):
+        A, M, C1 = _table(q, D, e)
+        de = int(st.e_dims[e])
+        rv = np.asarray(Rv[int(q.residual_offsets[e]):int(q.residual_offsets[e]) + M], np.float64) if not diag else None
+        for k in range(de):
+            c = A[:, C1 - de + k]
+            out[nr + int(st.boffsets_e[e]) + k] = float(np.dot(c, c if diag else rv))
+    return out
+
+
+def jtj_quadform(q: QRStructure, D, v):
+    """jtj_quadform(src, v) (src/qr_reduced.jl:597-640): sum over tables, in order, of sum over rows of (row . v)^2."""
+    st = q.st
+    nr = int(st.nr)
+    total = 0.0
+    for t in range(q.ntables):
+        A, M, C1 = _table(q, D, t)
+        x = np.zeros(C1)
+        for u in range(int(q.table_ptr[t]), int(q.table_ptr[t + 1])):
+            r = int(q.entry_retained[u])
+            x[int(q.entry_col[u]):int(q.entry_col[u]) + int(st.r_dims[r])] = v[int(st.boffsets_r[r]):int(st.boffsets_r[r]) + int(st.r_dims[r])]
+        if t < int(st.neblocks):
+            de = int(st.e_dims[t])
+            x[C1 - de:] = v[nr + int(st.boffsets_e[t]):nr + int(st.boffsets_e[t]) + de]
+        total += float(np.sum((A @ x) ** 2))
+    return total
+
+
+_COND_EPS, _COND_BOUND = 1e-12, 2.0 ** 16
+_FLOATMIN = {"f64": 2.2250738585072014e-308, "f32": float(np.finfo(np.float32).tiny)}
+
+
+def conditioning_scale(d: float, T: str = "f64") -> float:
+    """conditioning_scale (src/conditioning.jl:29-36): the power of two nearest, on a log scale, to
+    1 / (1e-12 + sqrt|d|), at least floatmin(T); 1.0 for a non-finite d."""
+    import math
+    dd = abs(float(d))
+    if not math.isfinite(dd):
+        return 1.0
+    f, e = math.frexp(1.0 / (_COND_EPS + math.sqrt(dd)))
+    s = math.ldexp(1.0, e) if f >= math.sqrt(0.5) else math.ldexp(1.0, e - 1)
+    return max(s, _FLOATMIN[T])
+
+
+def prepare_scale(s, d, lam, sc, T: str = "f64", *, stale: bool) -> bool:
+    """prepare_scale! (src/conditioning.jl:60-87) on the vector s in place; returns whether it was rewritten."""
+    lam = max(float(lam), 0.0)
+    dj = [float(d[j]) + lam * float(sc[j]) for j in range(len(s))]
+    if not stale:
+        drifted = False
+        for j in range(len(s)):
+            v = abs(dj[j]) * (float(s[j]) * float(s[j]))
+            if not (1.0 / _COND_BOUND <= v <= _COND_BOUND) and conditioning_scale(dj[j], T) != s[j]:
+                drifted = True
+                break
+        if not drifted:
+            return False
+    for j in range(len(s)):
+        s[j] = conditioning_scale(dj[j], T)
+    return True

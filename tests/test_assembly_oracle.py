@@ -58,3 +58,41 @@ def orc_free_pairs(q):
                 if a < b:
                     out.add((a, b))
     return sorted(out)
+
+
+@pytest.mark.parametrize("name", list(QR_FIXTURES))
+def test_jacobian_queries_are_dense(name):
+    """jtr!, jtj_diag! and jtj_quadform of the oracle against J'r, diag(J'J) and ||J v||^2 of the dense J (the fixture's
+    damping rows are zero, so every row of the tables is a row of J)."""
+    rng = np.random.default_rng(6)
+    fx = QR_FIXTURES[name](rng)
+    st = orc.Structure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    q = orc.QRStructure.positional(st, fx["e_rows"], fx.get("free_rows", ()), fx.get("free_retained", ()))
+    Rw, Rr, Jf, rf = fill_tables(q, rng)
+    assert relerr(orc.jtr(q, Rw, Rr), Jf.T @ rf) < 1e-14
+    assert relerr(orc.jtr(q, Rw, None, diag=True), np.sum(Jf * Jf, axis=0)) < 1e-14
+    v = rng.standard_normal(Jf.shape[1])
+    assert abs(orc.jtj_quadform(q, Rw, v) - np.sum((Jf @ v) ** 2)) <= 1e-13 * np.sum((Jf @ v) ** 2)
+
+
+def test_conditioning_scale_rule():
+    """conditioning_scale (src/conditioning.jl:29-36): a power of two, the nearest on a log scale to
+    1/(1e-12 + sqrt|d|), floored at floatmin(T), 1 for a non-finite d; prepare_scale! (:60-87) keeps the scale while
+    |d + lambda sc| s^2 stays in [2^-16, 2^16] and recomputes every entry once one entry leaves it."""
+    import math
+    rng = np.random.default_rng(7)
+    for d in list(10.0 ** rng.uniform(-300, 300, 500)) + [0.0, -3.0, 1e-320, 5e-324]:
+        s = orc.conditioning_scale(d)
+        m, e = math.frexp(s)
+        assert m == 0.5
+        target = 1.0 / (1e-12 + math.sqrt(abs(d)))
+        assert abs(math.log2(s) - math.log2(target)) <= 0.5 + 1e-12
+    assert orc.conditioning_scale(float("inf")) == 1.0 and orc.conditioning_scale(float("nan")) == 1.0
+    assert orc.conditioning_scale(1e300, "f32") == float(np.finfo(np.float32).tiny)
+    d = 10.0 ** rng.uniform(-4, 4, 50)
+    sc = np.ones(50)
+    s = np.zeros(50)
+    assert orc.prepare_scale(s, d, 1e-3, sc, stale=True)
+    s0 = s.copy()
+    assert not orc.prepare_scale(s, d, 2e-3, sc, stale=False) and (s == s0).all()   # a small change of damping
+    assert orc.prepare_scale(s, d, 1e6, sc, stale=False) and not (s == s0).all()    # one far enough to drift

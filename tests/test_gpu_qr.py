@@ -283,3 +283,45 @@ def test_assembled_schur_equals_qr_reduction(bls, name):
     bls.reduced_normal_sparse(Sq, gq, qws, pat)
     assert relerr(S.cpu().numpy(), Sq.cpu().numpy()) <= 1e-10
     assert relerr(g.cpu().numpy(), gq.cpu().numpy()) <= 1e-10
+
+
+@pytest.mark.parametrize("name", list(QR_FIXTURES))
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+def test_jacobian_queries_vs_oracle(bls, name, dtype):
+    """jtr!, jtj_diag! and jtj_quadform on the raw tables and on the factored ones against the oracle on the same
+    stored values (FP64 sums in both, so 1e-13 whatever the storage type)."""
+    j, o, Rw, Rr, Jf, rf, sc_e = fixture(bls, name)
+    npdt = np.float32 if dtype == torch.float32 else np.float64
+    Rw_s = Rw.astype(npdt)
+    pat = bls.build_schur_pattern(j.schur, bls.free_block_pairs(j))
+    ws = bls.QRReductionWorkspace(j, pat, dtype)
+    J = bls.SchurBlockJacobian(j, dtype, data=cu(Rw_s), r=cu(Rr))
+    assert bls.reduce_qr(ws, J, cu(sc_e), 0.3)
+    n = j.schur.nr + j.schur.ne
+    v = np.random.default_rng(9).standard_normal(n)
+    for src, D, Rv in ((J, Rw_s, Rr), (ws, ws.factored.cpu().numpy(), ws.fres.cpu().numpy())):
+        g = bls.jtr(torch.empty(n, dtype=torch.float64, device=DEV), src, ws)
+        d = bls.jtj_diag(torch.empty(n, dtype=torch.float64, device=DEV), src, ws)
+        qf = bls.jtj_quadform(src, cu(v), ws)
+        assert relerr(g.cpu().numpy(), orc.jtr(o, D, Rv)) <= 1e-13
+        assert relerr(d.cpu().numpy(), orc.jtr(o, D, None, diag=True)) <= 1e-13
+        oq = orc.jtj_quadform(o, D, v)
+        assert abs(qf - oq) <= 1e-13 * oq
+
+
+def test_prepare_scale_bit_identical(bls):
+    """prepare_scale! on the device against the oracle, bit for bit: scales from a diagonal over 600 decades with zeros,
+    negatives, subnormals and non-finite entries (FP64 and FP32 floors), then the drift rule at two later dampings."""
+    rng = np.random.default_rng(12)
+    d = np.concatenate([10.0 ** rng.uniform(-300, 300, 4000), [0.0, -2.5, 5e-324, 1e-310, np.inf, -np.inf, np.nan, 1e300]])
+    sc = rng.random(len(d))
+    for dtype, T in ((torch.float64, "f64"), (torch.float32, "f32")):
+        s = torch.zeros(len(d), dtype=torch.float64, device=DEV)
+        os_ = np.zeros(len(d))
+        assert bls.prepare_scale(s, cu(d), 1e-3, cu(sc), dtype, stale=True)
+        orc.prepare_scale(os_, d, 1e-3, sc, T, stale=True)
+        assert (s.cpu().numpy() == os_).all()
+        for lam in (2e-3, 1e8):
+            rec = bls.prepare_scale(s, cu(d), lam, cu(sc), dtype, stale=False)
+            orec = orc.prepare_scale(os_, d, lam, sc, T, stale=False)
+            assert rec == orec and (s.cpu().numpy() == os_).all()
