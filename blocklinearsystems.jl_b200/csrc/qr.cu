@@ -38,6 +38,7 @@ struct QRPlan {
   int64_t nrblocks = 0, neblocks = 0, ntables = 0, nentries = 0, nr = 0, ne = 0, raw_len = 0, res_len = 0;
   int64_t max_rows = 0, nblocks = 0, nnzS = 0, ndiag = 0;
   bool has_sparse = false;
+  bool all6 = true;   // every retained block has 6 columns (the Gram kernel's 6 x 6 form only)
   int max_dr = 0;
   // device: per table, per entry, per retained / eliminated block
   DevBuf t_rows, t_cols, t_top, t_raw, t_res, t_ptr, e_dims, boff_e;
@@ -263,7 +264,7 @@ __global__ void k_qr_free(int64_t t0, int64_t nt, const int32_t* __restrict__ t_
 // accumulate_qr_entry! (src/qr_reduced.jl:375-405) per table. MODE 0: S blocks (upper triangle of diagonal blocks) and
 // J~'r~ into g; MODE 1: the full diagonal blocks D (reduced_diagonal_blocks!, :484-512). from_raw: the same products
 // over the data rows of the raw tables, J'J of the retained columns and J'r (the retained part of the assembly).
-template <class T, int MODE>
+template <class T, int MODE, bool ALL6>
 __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int warp_bytes, const int32_t* __restrict__ tables,
                                                               const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_cols,
                                                               const int32_t* __restrict__ t_top, const int64_t* __restrict__ t_raw,
@@ -311,9 +312,10 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
   // work units: (pair, a group of three columns of the pair's block); lanes take units in order, so the lanes of one
   // pair read the same X rows (shared-memory broadcast)
   const int npairs = kt * (kt + 1) / 2;
-  const int upp = (dmax + 2) / 3;
+  constexpr int G = (ALL6 && sizeof(T) == 8) ? 2 : 3;   // columns of the pair's block per work unit (FP64 6 x 6: fewer registers)
+  const int upp = (dmax + G - 1) / G;
   for (int q = lane; q < npairs * upp; q += 32) {
-    const int p = q / upp, w0 = 3 * (q - p * upp);
+    const int p = q / upp, w0 = G * (q - p * upp);
     int u2l = (int)((sqrtf(8.0f * p + 1.0f) - 1.0f) * 0.5f);
     while ((u2l + 1) * (u2l + 2) / 2 <= p) ++u2l;
     while (u2l * (u2l + 1) / 2 > p) --u2l;
@@ -335,30 +337,31 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
       stride = d2;
       out = S + doff[r2] + w0 * d2;
     }
-    if (d1 == 6 && d2 == 6) {
-      double acc[3][6];
+    if (ALL6 || (d1 == 6 && d2 == 6)) {
+      // products accumulated in the storage type: FP32 in the mixed form (the bulk of the arithmetic), FP64 otherwise
+      T acc[G][6];
 #pragma unroll
-      for (int w = 0; w < 3; ++w)
+      for (int w = 0; w < G; ++w)
 #pragma unroll
-        for (int a = 0; a < 6; ++a) acc[w][a] = 0.0;
+        for (int a = 0; a < 6; ++a) acc[w][a] = T(0);
       for (int i = 0; i < n; ++i) {
-        double x[6], y[3];
+        T x[6], y[G];
 #pragma unroll
-        for (int a = 0; a < 6; ++a) x[a] = (double)X[a * ns + i];
+        for (int a = 0; a < 6; ++a) x[a] = X[a * ns + i];
 #pragma unroll
-        for (int w = 0; w < 3; ++w) y[w] = (double)Y[w * ns + i];
+        for (int w = 0; w < G; ++w) y[w] = Y[w * ns + i];
 #pragma unroll
-        for (int w = 0; w < 3; ++w)
+        for (int w = 0; w < G; ++w)
 #pragma unroll
           for (int a = 0; a < 6; ++a) acc[w][a] += x[a] * y[w];
       }
 #pragma unroll
-      for (int w = 0; w < 3; ++w)
+      for (int w = 0; w < G; ++w)
 #pragma unroll
         for (int a = 0; a < 6; ++a)
-          if (MODE == 1 || !diag || a <= w0 + w) atomicAdd(out + w * stride + a, T(acc[w][a]));
-    } else {
-      for (int w = w0; w < d2 && w < w0 + 3; ++w) {
+          if (MODE == 1 || !diag || a <= w0 + w) atomicAdd(out + w * stride + a, acc[w][a]);
+    } else if (!ALL6) {
+      for (int w = w0; w < d2 && w < w0 + G; ++w) {
         double acc[16];
 #pragma unroll
         for (int a = 0; a < 16; ++a) acc[a] = 0.0;
@@ -576,6 +579,7 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
     boff_r[r] = nr; nr += d->r_dims[r];
     doff[r + 1] = doff[r] + d->r_dims[r] * d->r_dims[r];
     P->max_dr = std::max<int>(P->max_dr, (int)d->r_dims[r]);
+    if (d->r_dims[r] != 6) P->all6 = false;
   }
   for (int64_t e = 0; e < neb; ++e) {
     if (d->e_dims[e] < 1) throw Error(BLS_EINVAL, "eliminated block sizes must be positive");
@@ -814,8 +818,9 @@ static void gram(QRPlan* P, T* S, bool dense, double* g, const T* F, const doubl
     const int64_t wb = ((std::is_same<T, double>::value ? k.bytes_f64 : k.bytes_f32) + 15) & ~int64_t(15);
     const int wpc = warps_per_cta(wb);
     const size_t smem = (size_t)(wb * wpc);
-    set_smem(reinterpret_cast<const void*>(k_qr_gram<T, MODE>), smem);
-    k_qr_gram<T, MODE><<<(unsigned)((k.n + wpc - 1) / wpc), 32 * wpc, smem, s>>>(
+    auto kern = P->all6 ? k_qr_gram<T, MODE, true> : k_qr_gram<T, MODE, false>;
+    set_smem(reinterpret_cast<const void*>(kern), smem);
+    kern<<<(unsigned)((k.n + wpc - 1) / wpc), 32 * wpc, smem, s>>>(
         k.n, (int)wb, k.tables.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
         P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(),
         P->boff_r.as<int32_t>(), P->tp_ptr.as<int32_t>(), P->tp_blk.as<int32_t>(),
