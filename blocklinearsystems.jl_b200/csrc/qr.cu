@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
   // work units: (pair, a group of three columns of the pair's block); lanes take units in order, so the lanes of one
   // pair read the same X rows (shared-memory broadcast)
   const int npairs = kt * (kt + 1) / 2;
-  constexpr int G = (ALL6 && sizeof(T) == 8) ? 2 : 3;   // columns of the pair's block per work unit (FP64 6 x 6: fewer registers)
+  constexpr int G = 3;   // columns of the pair's block per work unit
   const int upp = (dmax + G - 1) / G;
   for (int q = lane; q < npairs * upp; q += 32) {
     const int p = q / upp, w0 = G * (q - p * upp);
