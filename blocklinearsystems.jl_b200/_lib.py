@@ -127,6 +127,8 @@ def gpu() -> C.CDLL:
             "bls_pcg_solve_refined": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, C.c_double, vp, vp, vp, C.c_double, C.c_double, i64, i64,
                                                 p64, p64, pdbl, p64]),
             "bls_schur_apply_elimination": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+            "bls_hessian_bilinear": (C.c_int, [vp, C.c_int, vp, C.c_int, vp, vp, vp, vp, pdbl]),
+            "bls_hessian_diagonal": (C.c_int, [vp, C.c_int, vp, C.c_int, vp, vp]),
             "bls_pcg_plan_counters": (i64, [vp]),
             "bls_pcg_set_preconditioner": (C.c_int, [vp, vp]),
             "bls_gnn_param_count": (i64, []),

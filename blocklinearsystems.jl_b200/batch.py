@@ -17,7 +17,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from .reduction import SchurReductionWorkspace, reduce_schur_sparse, reset_schur_sparse
+from .reduction import SchurReductionWorkspace, reduce_schur_sparse, reset_reduce_schur_sparse_host, reset_schur_sparse
 
 
 @dataclass
@@ -162,6 +162,13 @@ class BatchedReduction:
             self.graph.replay()
         else:
             self.run(sync=False)
+
+    def run_host(self, S_h: torch.Tensor, g_h: torch.Tensor, host: dict) -> bool:
+        """reset + reduce of the whole batch from host buffers (`host`: E, C, R, b_r, b_e, sc_r, sc_e laid out as this
+        batch's device inputs, with each lambda folded into the scalings), S and g_S copied back into S_h and g_h. One
+        call: the library copies the inputs stage by stage while the earlier stages are reduced (page-locked buffers)."""
+        return reset_reduce_schur_sparse_host(S_h, g_h, host["R"], host["sc_r"], 1.0, host["b_r"], host["b_e"], host["sc_e"], self.U,
+                                              host["E"], host["C"], self.ws)
 
     def ok(self) -> bool:
         """Verdict of the last batch reduction (synchronises): False if any problem's eliminated block failed."""

@@ -84,6 +84,7 @@ struct SchurPlan {
   cudaEvent_t ev_free = nullptr, ev_points = nullptr, ev_in[kStages + 1] = {};
   // scratch: E^-1 (FP64, and FP32 for the mixed form), z, status
   DevBuf Einv64, Einv32, z, status;
+  DevBuf acc1;     // one FP64 accumulator (bls_hessian_bilinear)
   DevBuf w_apply;  // per point E^-1 C x of bls_schur_apply_elimination (ne doubles, allocated at its first call)
   DevBuf Einv12;   // fast36: E^-1 per point in the element type of the pair products, padded to 12 entries (16-byte rows)
   Status* host_status = nullptr;   // pinned
@@ -353,6 +354,68 @@ __global__ void __launch_bounds__(128) k_factor36(int64_t e_begin, int64_t neb, 
   for (int i = t; i < 9 * n; i += NB) Einv64[9 * e0 + i] = sE[i];
   for (int i = t; i < 12 * n; i += NB) Einv12[12 * e0 + i] = s12[i];
   for (int i = t; i < 3 * n; i += NB) z[3 * e0 + i] = ss[i];
+}
+
+// dot(x, H, y) / schur_bilinear (src/linalg.jl:133-262) from a SchurBlockHessian with R on S's pattern: x'Hy, FP64,
+// each stored off-diagonal entry counted in both orientations (a_x b_y + a_y b_x), as the reference's walk of one
+// stored triangle does. Retained part: one thread per stored entry (upper part; the lower entries of the diagonal
+// blocks are not part of R); point part: one thread per eliminated block (its E block and coupling blocks). Partial
+// sums per warp, one FP64 atomic per warp.
+__device__ __forceinline__ double warp_sum_h(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <class T>
+__global__ void k_bilinear_R(int64_t nnz, int64_t dense_nr, const int32_t* __restrict__ rowval, const int32_t* __restrict__ colof,
+                             const T* __restrict__ R, const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ out) {
+  double part = 0.0;
+  const int64_t n = dense_nr ? dense_nr * dense_nr : nnz;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = dense_nr ? q % dense_nr : rowval[q], j = dense_nr ? q / dense_nr : colof[q];
+    if (i > j) continue;
+    const double v = (double)R[q];
+    part += i == j ? v * x[i] * y[i] : v * (x[i] * y[j] + x[j] * y[i]);
+  }
+  part = warp_sum_h(part);
+  if ((threadIdx.x & 31) == 0 && part != 0.0) atomicAdd(out, part);
+}
+template <class T>
+__global__ void k_bilinear_points(int64_t neb, int64_t nr, const int32_t* __restrict__ eliminated_ptr, const int32_t* __restrict__ entry_retained,
+                                  const int32_t* __restrict__ e_dims, const int32_t* __restrict__ eoffsets, const int32_t* __restrict__ boffsets_e,
+                                  const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boffsets_r, const int32_t* __restrict__ coffsets,
+                                  const T* __restrict__ E, const T* __restrict__ C, const double* __restrict__ x, const double* __restrict__ y,
+                                  double* __restrict__ out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double part = 0.0;
+  if (e < neb) {
+    const int de = e_dims[e], eo = eoffsets[e];
+    const double* xe = x + nr + boffsets_e[e];
+    const double* ye = y + nr + boffsets_e[e];
+    for (int b = 0; b < de; ++b)
+      for (int a = 0; a < de; ++a) part += xe[a] * (double)E[eo + a + de * b] * ye[b];
+    for (int c = eliminated_ptr[e]; c < eliminated_ptr[e + 1]; ++c) {
+      const int r = entry_retained[c], dr = r_dims[r], ro = boffsets_r[r], co = coffsets[c];
+      for (int w = 0; w < dr; ++w)
+        for (int a = 0; a < de; ++a) {
+          const double h = (double)C[co + a + de * w];
+          part += h * (xe[a] * y[ro + w] + ye[a] * x[ro + w]);
+        }
+    }
+  }
+  part = warp_sum_h(part);
+  if ((threadIdx.x & 31) == 0 && part != 0.0) atomicAdd(out, part);
+}
+// The diagonal of H (the `diag!` a conditioned Hessian system hands prepare_scale!): d = [diag R; diag of each E block]
+template <class T>
+__global__ void k_hessian_diag(int64_t nr, int64_t neb, const int64_t* __restrict__ diag_inds, int64_t dense_nr, const int32_t* __restrict__ e_dims,
+                               const int32_t* __restrict__ eoffsets, const int32_t* __restrict__ boffsets_e, const T* __restrict__ R,
+                               const T* __restrict__ E, double* __restrict__ d) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < nr) d[i] = (double)R[dense_nr ? i + dense_nr * i : diag_inds[i]];
+  if (i < neb) {
+    const int de = e_dims[i];
+    for (int a = 0; a < de; ++a) d[nr + boffsets_e[i] + a] = (double)E[eoffsets[i] + a + de * a];
+  }
 }
 
 // --- phase 2: one thread per work item of one S block ---
@@ -1598,7 +1661,7 @@ static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
                           &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h,
-                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g, &P->w_apply,
+                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g, &P->w_apply, &P->acc1,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
   for (auto* x : bufs) b += (int64_t)x->bytes;
@@ -1914,6 +1977,40 @@ static int reduce_host(SchurPlan* P, T* S_h, double* g_h, const T* R_h, const do
   return BLS_OK;
 }
 
+template <class T>
+static double hessian_bilinear(SchurPlan* P, const T* R, bool dense, const T* E, const T* C, const double* x, const double* y) {
+  if (!dense && !(P->has_sparse && P->S_rowval.p)) throw Error(BLS_EINVAL, "a sparse R needs a plan with the pattern and S_rowval");
+  if (!R || !x || !y || (P->neblocks > 0 && (!E || !C))) throw Error(BLS_EINVAL, "a device pointer is NULL");
+  cudaStream_t s = P->ctx->stream;
+  if (!P->acc1.p) P->acc1.alloc(sizeof(double));
+  double* out = P->acc1.as<double>();
+  BLS_CUDA(cudaMemsetAsync(out, 0, sizeof(double), s));
+  const int64_t n = dense ? P->nr * P->nr : P->nnzS;
+  k_bilinear_R<T><<<std::max(1, (int)std::min<int64_t>(grid_for(n, 256), 148 * 8)), 256, 0, s>>>(
+      P->nnzS, dense ? P->nr : 0, P->S_rowval.as<int32_t>(), P->S_col.as<int32_t>(), R, x, y, out);
+  if (P->neblocks > 0)
+    k_bilinear_points<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(
+        P->neblocks, P->nr, P->eliminated_ptr.as<int32_t>(), P->entry_retained.as<int32_t>(), P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
+        P->boffsets_e.as<int32_t>(), P->r_dims.as<int32_t>(), P->boffsets_r.as<int32_t>(), P->coffsets.as<int32_t>(), E, C, x, y, out);
+  P->launches += 2;
+  double h = 0.0;
+  BLS_CUDA(cudaMemcpyAsync(&h, out, sizeof(double), cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+template <class T>
+static void hessian_diagonal(SchurPlan* P, const T* R, bool dense, const T* E, double* d) {
+  if (!dense && !(P->has_sparse && P->diag_inds.p)) throw Error(BLS_EINVAL, "a sparse R needs a plan with the pattern");
+  if (!R || !d || (P->neblocks > 0 && !E)) throw Error(BLS_EINVAL, "a device pointer is NULL");
+  const int64_t n = std::max(P->nr, P->neblocks);
+  k_hessian_diag<T><<<std::max(1, grid_for(n, 256)), 256, 0, P->ctx->stream>>>(P->nr, P->neblocks, P->diag_inds.as<int64_t>(), dense ? P->nr : 0,
+                                                                             P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
+                                                                             P->boffsets_e.as<int32_t>(), R, E, d);
+  P->launches += 1;
+  BLS_CUDA(cudaGetLastError());
+}
+
 // y = y0 - C' E^-1 C x over every eliminated block, in FP64, from the plan's E^-1 of its last successful reduction
 template <class T>
 static int apply_elimination(SchurPlan* P, double* y, const double* y0, const double* x, const T* C) {
@@ -2017,6 +2114,27 @@ int bls_reduce_schur_sparse(bls_schur_plan* P, int dtype, void* S, double* g, co
     if (dtype == BLS_F64) return reduce<double>(P, (double*)S, false, g, b_r, b_e, sc_e, lambda, (const double*)E, (const double*)C, s_r, s_e, failed_block);
     if (dtype == BLS_F32) return reduce<float>(P, (float*)S, false, g, b_r, b_e, sc_e, lambda, (const float*)E, (const float*)C, s_r, s_e, failed_block);
     throw Error(BLS_EINVAL, "unknown dtype");
+  })
+}
+
+int bls_hessian_bilinear(bls_schur_plan* P, int dtype, const void* R, int dense, const void* E, const void* C, const double* x,
+                         const double* y, double* result) {
+  BLS_GUARD({
+    if (!P || !result) throw Error(BLS_EINVAL, "null argument");
+    if (dtype == BLS_F64) *result = hessian_bilinear<double>(P, (const double*)R, dense != 0, (const double*)E, (const double*)C, x, y);
+    else if (dtype == BLS_F32) *result = hessian_bilinear<float>(P, (const float*)R, dense != 0, (const float*)E, (const float*)C, x, y);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_hessian_diagonal(bls_schur_plan* P, int dtype, const void* R, int dense, const void* E, double* d) {
+  BLS_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (dtype == BLS_F64) hessian_diagonal<double>(P, (const double*)R, dense != 0, (const double*)E, d);
+    else if (dtype == BLS_F32) hessian_diagonal<float>(P, (const float*)R, dense != 0, (const float*)E, d);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
   })
 }
 

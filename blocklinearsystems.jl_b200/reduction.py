@@ -138,6 +138,31 @@ class SchurReductionWorkspace:
         check(_lib.gpu().bls_schur_apply_elimination(self.handle, T, dptr(y), dptr(y0), dptr(x), dptr(C_data)))
         return y
 
+    def hessian_bilinear(self, R: torch.Tensor, E_data: torch.Tensor, C_data: torch.Tensor, x: torch.Tensor, y: torch.Tensor,
+                         *, dense: bool = False) -> float:
+        """dot(x, H, y) (src/linalg.jl:133-262) of the Hessian (R on this plan's pattern, or dense nr x nr column-major;
+        E_data, C_data) for x, y = [x_r; x_e], FP64."""
+        st = self.structure
+        n = st.nr + st.ne
+        T = _dtype_code(_dev(R, "R", st.nr * st.nr if dense else self.pattern.nnz))
+        _dev(E_data, "E_data", st.E_length, R.dtype)
+        _dev(C_data, "C_data", st.C_length, R.dtype)
+        _dev(x, "x", n, torch.float64)
+        _dev(y, "y", n, torch.float64)
+        out = C.c_double(0.0)
+        check(_lib.gpu().bls_hessian_bilinear(self.handle, T, dptr(R), int(dense), dptr(E_data), dptr(C_data), dptr(x), dptr(y),
+                                              C.byref(out)))
+        return float(out.value)
+
+    def hessian_diagonal(self, R: torch.Tensor, E_data: torch.Tensor, *, dense: bool = False) -> torch.Tensor:
+        """[diag R; the diagonals of the E blocks], float64 (what prepare_scale! reads on the Hessian side)."""
+        st = self.structure
+        T = _dtype_code(_dev(R, "R", st.nr * st.nr if dense else self.pattern.nnz))
+        _dev(E_data, "E_data", st.E_length, R.dtype)
+        d = torch.empty(st.nr + st.ne, dtype=torch.float64, device=R.device)
+        check(_lib.gpu().bls_hessian_diagonal(self.handle, T, dptr(R), int(dense), dptr(E_data), dptr(d)))
+        return d
+
     def query_status(self) -> bool:
         fb = C.c_int64(0)
         rc = check(_lib.gpu().bls_schur_query_status(self.handle, C.byref(fb)))

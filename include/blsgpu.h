@@ -181,6 +181,15 @@ int bls_schur_plan_counters(bls_schur_plan* plan, int64_t* launches, double* pai
 /* Status of the last reduction on this plan (synchronises): BLS_OK / BLS_NOT_PD / BLS_EINVAL. */
 int bls_schur_query_status(bls_schur_plan* plan, int64_t* failed_block);
 
+/* dot(x, H, y) (schur_bilinear, src/linalg.jl:133-262) of a SchurBlockHessian with R on S's pattern (dense = 0:
+ * S.nzval layout, its upper part; dense = 1: column-major nr x nr, upper triangle), E_data and C_data in the plan's
+ * layout: *result = x'Hy in FP64 for x, y = [x_r; x_e] (synchronises). Sparse R needs S_rowval in the plan.
+ * bls_hessian_diagonal: d[nr + ne] = [diag R; the diagonals of the E blocks] (the diagonal a conditioned Hessian system
+ * hands prepare_scale!). */
+int bls_hessian_bilinear(bls_schur_plan* plan, int dtype, const void* R_dev, int dense, const void* E_data_dev, const void* C_data_dev,
+                         const double* x_dev, const double* y_dev, double* result);
+int bls_hessian_diagonal(bls_schur_plan* plan, int dtype, const void* R_dev, int dense, const void* E_data_dev, double* d_dev);
+
 /* The point term of the reduced operator in FP64 (no counterpart in the reference, which forms S instead):
  * y = y0 - sum over eliminated blocks of C' E^-1 C x, with E^-1 the FP64 inverse of the damped point block from the
  * plan's last successful reduction and C its coupling blocks (dtype storage, as reduced); y and y0 distinct. With y0 =

@@ -492,3 +492,32 @@ def prepare_scale(s, d, lam, sc, T: str = "f64", *, stale: bool) -> bool:
     for j in range(len(s)):
         s[j] = conditioning_scale(dj[j], T)
     return True
+
+
+def hessian_dense(st: Structure, R, E, Cd, pat: Pattern | None = None):
+    """The full symmetric H of a SchurBlockHessian from R on the reduced pattern (its upper part; dense column-major
+    nr x nr when pat is None), E_data and C_data in the structure's layout (add_eliminated! / add_coupling! /
+    add_retained_pair!, src/schur_assembly.jl:189-246). dot(x, H, y) (src/linalg.jl:133-262) is x @ H @ y."""
+    nr, ne = int(st.nr), int(st.ne)
+    H = np.zeros((nr + ne, nr + ne))
+    if pat is None:
+        A = np.asarray(R, np.float64).reshape(nr, nr, order="F")
+        U = np.triu(A)
+    else:
+        U = np.zeros((nr, nr))
+        for j in range(nr):
+            for q in range(int(pat.S_colptr[j]), int(pat.S_colptr[j + 1])):
+                i = int(pat.S_rowval[q])
+                if i <= j:
+                    U[i, j] = R[q]
+    H[:nr, :nr] = U + np.triu(U, 1).T
+    for e in range(int(st.neblocks)):
+        de, eo, so = int(st.e_dims[e]), int(st.eoffsets[e]), nr + int(st.boffsets_e[e])
+        H[so:so + de, so:so + de] = np.asarray(E[eo:eo + de * de], np.float64).reshape(de, de, order="F")
+        for c in range(int(st.eliminated_ptr[e]), int(st.eliminated_ptr[e + 1])):
+            r = int(st.entry_retained[c])
+            dr, ro, co = int(st.r_dims[r]), int(st.boffsets_r[r]), int(st.coffsets[c])
+            B = np.asarray(Cd[co:co + de * dr], np.float64).reshape(de, dr, order="F")
+            H[so:so + de, ro:ro + dr] = B
+            H[ro:ro + dr, so:so + de] = B.T
+    return H

@@ -46,6 +46,9 @@ def test_assembly_is_dense_jtj(name):
             i = int(pat.S_rowval[k])
             ref[k] = H[i, j] if i <= j else 0.0
     assert relerr(R, ref) < 1e-14
+    # and the oracle's dense H of that Hessian (the layout dot(x, H, y) reads) is J'J itself
+    assert relerr(orc.hessian_dense(st, R, E, Cd, pat), H) < 1e-14
+    assert relerr(orc.hessian_dense(st, Rd, E, Cd, None), H) < 1e-14
 
 
 def orc_free_pairs(q):

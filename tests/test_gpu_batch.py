@@ -74,3 +74,15 @@ def test_graph_autotune_and_failure(bls, problems):
     B.step()
     assert not B.ok()
     assert B.ws.failed_block == e_off + 6
+
+
+def test_host_buffer_batch_matches_device_run(bls, problems):
+    """The whole batch from page-locked host buffers in one call (stage-by-stage copies) gives the device run's S and g."""
+    B = bls.batch.BatchedReduction(problems, torch.float32)
+    assert B.run()
+    host = {k: getattr(B, k).cpu().pin_memory() for k in ("E", "C", "R", "b_r", "b_e", "sc_r", "sc_e")}
+    hS = torch.empty_like(B.S, device="cpu").pin_memory()
+    hg = torch.empty_like(B.g, device="cpu").pin_memory()
+    assert B.run_host(hS, hg, host)
+    assert relerr(hS.double().numpy(), B.S.double().cpu().numpy()) <= 1e-6
+    assert relerr(hg.numpy(), B.g.cpu().numpy()) <= 1e-12

@@ -273,3 +273,29 @@ def test_repeated_reductions_are_stable(bls):
         outs.append(S.cpu().numpy())
     for o in outs[1:]:
         assert relerr(o, outs[0]) < 1e-14
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+@pytest.mark.parametrize("dense", [False, True])
+def test_hessian_bilinear_and_diagonal(bls, dtype, dense):
+    """dot(x, H, y) and diag(H) of the Hessian (R on the pattern or dense, E, C) against the dense H the oracle builds
+    from the same stored values (FP64 sums: 1e-12 relative)."""
+    p, st, ost, opat = scene_system(bls, "sparse_1000x200k", 60, 2500, dense)
+    npdt = np.float32 if dtype == torch.float32 else np.float64
+    E, Cd, R = p.E.astype(npdt), p.C.astype(npdt), p.R.astype(npdt)
+    ws = bls.SchurReductionWorkspace(st, p.pattern)
+    if dense:
+        R0 = cu(R)
+        oR = R.astype(np.float64)
+    else:
+        R0 = torch.zeros(p.pattern.nnz, dtype=dtype, device=DEV)
+        bls.reset_schur_sparse(R0, cu(R), None, None, cu(p.scaling_r), 0.0, ws)   # R on the pattern
+        oR = np.zeros(opat.nnz)
+        orc.reset_schur_sparse(ost, opat, oR, R.astype(np.float64), p.scaling_r, 0.0)
+    H = orc.hessian_dense(ost, oR, E.astype(np.float64), Cd.astype(np.float64), None if dense else opat)
+    rng = np.random.default_rng(4)
+    x, y = rng.standard_normal(H.shape[0]), rng.standard_normal(H.shape[0])
+    v = ws.hessian_bilinear(R0, cu(E), cu(Cd), cu(x), cu(y), dense=dense)
+    assert abs(v - x @ H @ y) <= 1e-12 * (np.abs(x) @ np.abs(H) @ np.abs(y))
+    d = ws.hessian_diagonal(R0, cu(E), dense=dense)
+    assert relerr(d.cpu().numpy(), np.diag(H)) <= 1e-15
