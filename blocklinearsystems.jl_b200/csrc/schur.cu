@@ -586,6 +586,77 @@ __device__ __forceinline__ void load_col3(const double* p, int odd, double out[3
 // and adds C_c1' u to its column. A pair record {c1, e | (c2 - c1) << 24} holds every index the pair needs, so the
 // next record is fetched while the current pair is computed and no load waits on another index load. The diagonal
 // block's items also subtract C_c2' z from g_S (each coupling of r2 is exactly one diagonal pair).
+// The same two passes for the 6/3 canonical layout (C_c at 18 c, E^-1 at 9 e, variables at 6 r and 3 e): no per-block
+// index loads, each coupling block read with 8- or 16-byte loads and each x_r block with 16-byte loads, two couplings
+// of a point in flight at a time. Pass 1, one thread per point: w_e = E^-1 sum_c C_c x_r(c). Pass 2, one warp per
+// camera, lanes over its couplings: y_r = y0_r - sum_c C_c' w_e(c), six sums reduced across the warp.
+template <class T>
+__device__ __forceinline__ void coupling18(const T* __restrict__ C, int64_t c, T out[18]) {
+  if constexpr (std::is_same<T, double>::value) {
+    const double2* q = reinterpret_cast<const double2*>(C + 18 * c);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { const double2 v = __ldg(q + i); out[2 * i] = v.x; out[2 * i + 1] = v.y; }
+  } else {
+    const float2* q = reinterpret_cast<const float2*>(C + 18 * c);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { const float2 v = __ldg(q + i); out[2 * i] = v.x; out[2 * i + 1] = v.y; }
+  }
+}
+template <class T>
+__global__ void __launch_bounds__(256) k_point_apply36(int64_t neb, const int32_t* __restrict__ eliminated_ptr,
+                                                       const int32_t* __restrict__ entry_retained, const T* __restrict__ C,
+                                                       const double* __restrict__ Einv64, const double* __restrict__ x,
+                                                       double* __restrict__ w, const Status* __restrict__ st) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= neb || !live(st)) return;
+  double t[3] = {0.0, 0.0, 0.0};
+  const int c0 = eliminated_ptr[e], c1 = eliminated_ptr[e + 1];
+#pragma unroll 2
+  for (int c = c0; c < c1; ++c) {
+    const int r = __ldg(entry_retained + c);
+    const double2* xp = reinterpret_cast<const double2*>(x + 6 * (int64_t)r);
+    const double2 a = __ldg(xp), b = __ldg(xp + 1), d = __ldg(xp + 2);
+    const double xr[6] = {a.x, a.y, b.x, b.y, d.x, d.y};
+    T cb[18];
+    coupling18<T>(C, c, cb);
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) t[i] += (double)cb[i + 3 * j] * xr[j];
+  }
+  const double* inv = Einv64 + 9 * e;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) w[3 * e + i] = inv[i] * t[0] + inv[i + 3] * t[1] + inv[i + 6] * t[2];
+}
+template <class T>
+__global__ void __launch_bounds__(256) k_gather_ctw36(int64_t nrb, const int32_t* __restrict__ retained_ptr, const int32_t* __restrict__ retained_entry,
+                                                      const int32_t* __restrict__ entry_eliminated, const T* __restrict__ C,
+                                                      const double* __restrict__ w, const double* __restrict__ y0, double* __restrict__ y,
+                                                      const Status* __restrict__ st) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= nrb || !live(st)) return;
+  double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int q = retained_ptr[r] + lane; q < retained_ptr[r + 1]; q += 32) {
+    const int c = __ldg(retained_entry + q), e = __ldg(entry_eliminated + c);
+    const double w0 = w[3 * e], w1 = w[3 * e + 1], w2 = w[3 * e + 2];
+    T cb[18];
+    coupling18<T>(C, c, cb);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) acc[j] += (double)cb[3 * j] * w0 + (double)cb[3 * j + 1] * w1 + (double)cb[3 * j + 2] * w2;
+  }
+#pragma unroll
+  for (int j = 0; j < 6; ++j)
+    for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+  if (lane < 6) {
+    double v = 0.0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+      if (j == lane) v = acc[j];
+    y[6 * r + lane] = y0[6 * r + lane] - v;
+  }
+}
+
 // The point term of the reduced operator applied to a vector, in FP64 (no counterpart in the reference, which forms
 // S): per eliminated block e, w_e = E_e^-1 sum_c C_c x_r(c), with E^-1 the plan's FP64 inverse of the damped block
 // from its last reduction (C_c is d_e x d_r column-major). k_gradient then forms y = y0 - sum_c C_c' w_e(c).
@@ -2019,6 +2090,20 @@ static int apply_elimination(SchurPlan* P, double* y, const double* y0, const do
   cudaStream_t s = P->ctx->stream;
   if (!P->w_apply.p) P->w_apply.alloc(sizeof(double) * std::max<int64_t>(P->ne, 1));
   Status* st = P->status.as<Status>();
+  if (P->fast36) {
+    if (reinterpret_cast<uintptr_t>(C) % (2 * sizeof(T)) != 0)
+      throw Error(BLS_EINVAL, "C_data must be aligned to two elements (the device reads coupling blocks in pairs of entries)");
+    if (reinterpret_cast<uintptr_t>(x) % 16 != 0) throw Error(BLS_EINVAL, "x must be 16-byte aligned");
+    if (P->neblocks > 0)
+      k_point_apply36<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(P->neblocks, P->eliminated_ptr.as<int32_t>(), P->entry_retained.as<int32_t>(),
+                                                                    C, P->Einv64.as<double>(), x, P->w_apply.as<double>(), st);
+    if (P->nrblocks > 0)
+      k_gather_ctw36<T><<<grid_for(P->nrblocks * 32, 256), 256, 0, s>>>(P->nrblocks, P->retained_ptr.as<int32_t>(), P->retained_entry.as<int32_t>(),
+                                                                        P->entry_eliminated.as<int32_t>(), C, P->w_apply.as<double>(), y0, y, st);
+    P->launches += 2;
+    BLS_CUDA(cudaGetLastError());
+    return BLS_OK;
+  }
   if (P->neblocks > 0)
     k_point_apply<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(
         P->neblocks, P->eliminated_ptr.as<int32_t>(), P->entry_retained.as<int32_t>(), P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(),
