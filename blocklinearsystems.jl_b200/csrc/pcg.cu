@@ -7,13 +7,15 @@
 //
 // S is the reduction's output: the upper block triangle of the symmetric reduced matrix in the CSC layout of
 // build_schur_pattern (column r2 of blocks (r1 <= r2), column stride col_heights[r2]; diagonal blocks stored full with
-// only their upper triangle meaningful). y = S x reads each stored block twice, as B for block row r1 and as B' for
-// block row r2, from a per-row list built once per pattern: one warp per block row gathers its row, so the product has
-// no atomics and is deterministic. Vectors, scalars and products are FP64 whatever S's storage type.
+// only their upper triangle meaningful). When every retained block has 6 columns, y = S x reads each stored entry once,
+// one warp per block column (k_spmv_cols): B p_r2 is scattered into the rows r1 with FP64 atomics and B' p_r1 summed
+// for the column; otherwise it reads each stored block twice, as B for block row r1 and as B' for block row r2, from a
+// per-row list built once per pattern (one warp per block row gathers its row: no atomics, deterministic). Vectors,
+// scalars and products are FP64 whatever S's storage type.
 //
-// One PCG iteration is three kernels: (1) q = S p with the partial sums of p'q; (2) alpha = (r'z)/(p'q), x += alpha p,
-// r -= alpha q, z = M^-1 r (block solves) with the partial sums of r'z and r'r; (3) beta, p = z + beta p, and the
-// convergence test. Per-iteration scalars live in device slots, so a run of iterations can be replayed as one CUDA
+// One PCG iteration is three kernels (four with the column product): (1) q = S p with the partial sums of p'q (the
+// column form takes a separate p'q pass); (2) alpha = (r'z)/(p'q), x += alpha p, r -= alpha q, z = M^-1 r (block
+// solves) with the partial sums of r'z and r'r; (3) beta, p = z + beta p, and the convergence test. Per-iteration scalars live in device slots, so a run of iterations can be replayed as one CUDA
 // graph; after convergence the remaining kernels of the run return at once. The converged x is checked by an explicit
 // FP64 residual g - S x; if the recursive residual drifted above the tolerance, PCG restarts from x (iterative
 // refinement).
@@ -199,7 +201,7 @@ __device__ __forceinline__ void precondition(double* z, const double* __restrict
 
 __global__ void k_pcg_start(int64_t nrb, const int32_t* __restrict__ dims, const int32_t* __restrict__ boff, const int64_t* __restrict__ doff,
                             const double* __restrict__ D, const double* __restrict__ Bp, const double* __restrict__ r, double* __restrict__ z,
-                            double* __restrict__ p, double* __restrict__ slot0) {
+                            double* __restrict__ p, double* __restrict__ q, double* __restrict__ slot0) {
   const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double rz = 0.0, rr = 0.0;
   if (b < nrb) {
@@ -207,6 +209,7 @@ __global__ void k_pcg_start(int64_t nrb, const int32_t* __restrict__ dims, const
     const int64_t o = boff[b];
     precondition(z + o, D + doff[b], Bp ? Bp + doff[b] : nullptr, d, r + o);
     for (int i = 0; i < d; ++i) {
+      q[o + i] = 0.0;
       p[o + i] = z[o + i];
       rz += r[o + i] * z[o + i];
       rr += r[o + i] * r[o + i];
@@ -220,12 +223,81 @@ __global__ void k_pcg_start(int64_t nrb, const int32_t* __restrict__ dims, const
   }
 }
 
+// q += S p by block columns, for patterns whose retained blocks all have 6 columns: one warp per block column r2,
+// lanes over (block, row) of five blocks at a time, each stored entry read once. A block (r1, r2) adds B p_r2 to q_r1
+// (one FP64 atomic per row) and B' p_r1 to q_r2 (summed over the column's blocks in registers, one atomic per column
+// entry at the end); the diagonal block uses its upper triangle both ways. q must be zero on entry (k_pcg_update and
+// k_pcg_start clear it); after convergence within a replayed run the kernel returns at once.
+template <class T>
+__global__ void __launch_bounds__(256) k_spmv_cols(int64_t nrb, const int64_t* __restrict__ c_ptr, const int64_t* __restrict__ c_base,
+                                                   const int32_t* __restrict__ c_xo, const int32_t* __restrict__ c_stride,
+                                                   const T* __restrict__ S, const double* __restrict__ p, double* __restrict__ q,
+                                                   const int* __restrict__ done) {
+  if (done && *done) return;
+  const int64_t r2 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r2 >= nrb) return;
+  const int64_t j0 = 6 * r2;
+  const int64_t stride = c_stride[r2];
+  double pj[6];
+#pragma unroll
+  for (int w = 0; w < 6; ++w) pj[w] = p[j0 + w];
+  double t[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const int sub = lane / 6, a = lane - 6 * sub;
+  const int64_t kb = c_ptr[r2], ke = c_ptr[r2 + 1];
+  for (int64_t k0 = kb; k0 < ke; k0 += 5) {
+    const int64_t k = k0 + sub;
+    if (lane < 30 && k < ke) {
+      const T* B = S + c_base[k] + a;
+      const int i0 = c_xo[k];
+      const bool diag = i0 == j0;
+      double sv[6];
+#pragma unroll
+      for (int w = 0; w < 6; ++w) sv[w] = (double)B[w * stride];
+      const double pi = p[i0 + a];
+      double v = 0.0;
+#pragma unroll
+      for (int w = 0; w < 6; ++w) {
+        if (!diag || w >= a) v += sv[w] * pj[w];
+        if (!diag || w > a) t[w] += sv[w] * pi;
+      }
+      atomicAdd(q + i0 + a, v);
+    }
+  }
+#pragma unroll
+  for (int w = 0; w < 6; ++w)
+    for (int o = 16; o > 0; o >>= 1) t[w] += __shfl_xor_sync(0xffffffffu, t[w], o);
+  if (lane < 6) {
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < 6; ++w)
+      if (w == lane) v = t[w];
+    atomicAdd(q + j0 + lane, v);
+  }
+}
+
+// y = g - y (the residual from a product accumulated in y)
+__global__ void k_from_g(int64_t n, const double* __restrict__ g, double* __restrict__ y) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = g[i] - y[i];
+}
+
+// p'q into the iteration's slot (after k_spmv_cols)
+__global__ void k_dot_pq(int64_t n, const double* __restrict__ p, const double* __restrict__ q, double* __restrict__ out,
+                         const int* __restrict__ done) {
+  if (*done) return;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) s += p[i] * q[i];
+  s = warp_sum_d(s);
+  if ((threadIdx.x & 31) == 0 && s != 0.0) atomicAdd(out, s);
+}
+
 // (2) alpha = rz / pq; x += alpha p; r -= alpha q; z = M^-1 r; rz_next, rr_next
 __global__ void k_pcg_update(int64_t nrb, const int32_t* __restrict__ dims, const int32_t* __restrict__ boff, const int64_t* __restrict__ doff,
                              const double* __restrict__ D, const double* __restrict__ Bp, double* __restrict__ x, double* __restrict__ r,
                              double* __restrict__ z,
-                             const double* __restrict__ p, const double* __restrict__ q, double* __restrict__ slot,
-                             const int* __restrict__ done) {
+                             const double* __restrict__ p, double* __restrict__ q, double* __restrict__ slot,
+                             const int* __restrict__ done, int clear_q) {
   if (*done) return;
   const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const double alpha = slot[PS_RZ] / slot[PS_PQ];
@@ -236,6 +308,7 @@ __global__ void k_pcg_update(int64_t nrb, const int32_t* __restrict__ dims, cons
     for (int i = 0; i < d; ++i) {
       x[o + i] += alpha * p[o + i];
       r[o + i] -= alpha * q[o + i];
+      if (clear_q) q[o + i] = 0.0;   // the next q = S p accumulates into zeros
     }
     precondition(z + o, D + doff[b], Bp ? Bp + doff[b] : nullptr, d, r + o);
     for (int i = 0; i < d; ++i) {
@@ -388,6 +461,26 @@ static PCGPlan* pcg_plan_create(bls_ctx* ctx, int64_t nrb, const int64_t* r_dims
   }
   upload(P->row_ptr, rptr, s);
   upload(P->rows, flat, s);
+  if (P->max_d == 6) {
+    bool all6 = true;
+    for (int64_t r = 0; r < nrb && all6; ++r) all6 = dims[r] == 6;
+    if (all6 && bcolptr[nrb] < INT32_MAX) {
+      std::vector<int64_t> cptr(bcolptr, bcolptr + nrb + 1), cbase(bcolptr[nrb]);
+      std::vector<int32_t> cxo(bcolptr[nrb]), cstr(nrb);
+      for (int64_t r2 = 0; r2 < nrb; ++r2) {
+        cstr[r2] = (int32_t)col_h[r2];
+        for (int64_t k = bcolptr[r2]; k < bcolptr[r2 + 1]; ++k) {
+          cbase[k] = Scolptr[boff[r2]] + brow_off[k];
+          cxo[k] = boff[browval[k]];
+        }
+      }
+      upload(P->c_ptr, cptr, s);
+      upload(P->c_base, cbase, s);
+      upload(P->c_xo, cxo, s);
+      upload(P->c_stride, cstr, s);
+      P->cols6 = true;
+    }
+  }
   upload(P->r_dims, dims, s);
   upload(P->boff, boff, s);
   upload(P->doff, doff, s);
@@ -408,6 +501,17 @@ static PCGPlan* pcg_plan_create(bls_ctx* ctx, int64_t nrb, const int64_t* r_dims
 template <class T>
 static void spmv(PCGPlan* P, const T* S, const double* x, const double* g, double* y, bool residual, cudaStream_t s) {
   const unsigned grid = (unsigned)grid_for(P->nrb * 32, 256);
+  if (P->cols6) {   // y = 0; y += S x by block columns; r = g - y
+    BLS_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * P->nr, s));
+    k_spmv_cols<T><<<grid, 256, 0, s>>>(P->nrb, P->c_ptr.as<int64_t>(), P->c_base.as<int64_t>(), P->c_xo.as<int32_t>(), P->c_stride.as<int32_t>(),
+                                        S, x, y, nullptr);
+    P->launches += 1;
+    if (residual) {
+      k_from_g<<<std::max(1, grid_for(P->nr, 256)), 256, 0, s>>>(P->nr, g, y);
+      P->launches += 1;
+    }
+    return;
+  }
   if (residual)
     k_spmv<T, true, false><<<grid, 256, 0, s>>>(P->nrb, P->row_ptr.as<int64_t>(), P->rows.as<RowEntry>(), P->r_dims.as<int32_t>(),
                                                 P->boff.as<int32_t>(), S, x, g, y, nullptr, nullptr);
@@ -433,10 +537,17 @@ static void iteration(PCGPlan* P, const T* S, double* x, int j, cudaStream_t s) 
   double* slot = P->scal.as<double>() + j * PS_W;
   int* flags = P->flags.as<int>();
   const unsigned gsp = (unsigned)grid_for(P->nrb * 32, 256), gb = (unsigned)grid_for(P->nrb, 128), gv = (unsigned)grid_for(P->nr, 256);
-  k_spmv<T, false, true><<<gsp, 256, 0, s>>>(P->nrb, P->row_ptr.as<int64_t>(), P->rows.as<RowEntry>(), P->r_dims.as<int32_t>(),
-                                             P->boff.as<int32_t>(), S, P->p.as<double>(), nullptr, P->q.as<double>(), slot + PS_PQ, flags);
+  if (P->cols6) {
+    k_spmv_cols<T><<<gsp, 256, 0, s>>>(P->nrb, P->c_ptr.as<int64_t>(), P->c_base.as<int64_t>(), P->c_xo.as<int32_t>(), P->c_stride.as<int32_t>(),
+                                       S, P->p.as<double>(), P->q.as<double>(), flags);
+    k_dot_pq<<<std::max(1, std::min(grid_for(P->nr, 256), 296)), 256, 0, s>>>(P->nr, P->p.as<double>(), P->q.as<double>(), slot + PS_PQ, flags);
+    P->launches += 1;
+  } else {
+    k_spmv<T, false, true><<<gsp, 256, 0, s>>>(P->nrb, P->row_ptr.as<int64_t>(), P->rows.as<RowEntry>(), P->r_dims.as<int32_t>(),
+                                               P->boff.as<int32_t>(), S, P->p.as<double>(), nullptr, P->q.as<double>(), slot + PS_PQ, flags);
+  }
   k_pcg_update<<<gb, 128, 0, s>>>(P->nrb, P->r_dims.as<int32_t>(), P->boff.as<int32_t>(), P->doff.as<int64_t>(), P->D.as<double>(), P->precond, x,
-                                  P->r.as<double>(), P->z.as<double>(), P->p.as<double>(), P->q.as<double>(), slot, flags);
+                                  P->r.as<double>(), P->z.as<double>(), P->p.as<double>(), P->q.as<double>(), slot, flags, P->cols6 ? 1 : 0);
   k_pcg_direction<<<gv, 256, 0, s>>>(P->nr, P->z.as<double>(), P->p.as<double>(), slot, slot + PS_W,
                                      P->scal.as<double>() + (P->K + 1) * PS_W, flags);
   P->launches += 3;
@@ -494,7 +605,7 @@ static int pcg_solve(PCGPlan* P, const T* S, const double* g, double* x, double 
     BLS_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(int), s));
     k_pcg_start<<<grid_for(P->nrb, 128), 128, 0, s>>>(P->nrb, P->r_dims.as<int32_t>(), P->boff.as<int32_t>(), P->doff.as<int64_t>(),
                                                       P->D.as<double>(), P->precond, P->r.as<double>(), P->z.as<double>(),
-                                                      P->p.as<double>(), scal + P->K * PS_W);
+                                                      P->p.as<double>(), P->q.as<double>(), scal + P->K * PS_W);
     P->launches += 2;
     BLS_CUDA(cudaMemcpyAsync(P->host, scal + P->K * PS_W + PS_RRN, sizeof(double), cudaMemcpyDeviceToHost, s));
     BLS_CUDA(cudaStreamSynchronize(s));
@@ -528,7 +639,7 @@ static int pcg_solve(PCGPlan* P, const T* S, const double* g, double* x, double 
         BLS_CUDA(cudaGraphLaunch(P->graph, P->cap_stream));
         BLS_CUDA(cudaEventRecord(P->ev_out, P->cap_stream));
         BLS_CUDA(cudaStreamWaitEvent(s, P->ev_out, 0));
-        P->launches += 1 + 3 * P->K;
+        P->launches += 1 + (P->cols6 ? 4 : 3) * P->K;
       } else {
         run_block<T>(P, S, x, (int)std::min<int64_t>(P->K, left), s);
       }

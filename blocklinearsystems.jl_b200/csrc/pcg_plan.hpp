@@ -27,6 +27,10 @@ struct PCGPlan {
   // solver state (FP64)
   DevBuf D;                 // factored diagonal blocks (L in the lower triangle)
   DevBuf r, z, p, q, scal, flags;
+  // q = S p by block columns (every r_dim 6): per block column its blocks, per block its S offset and its row
+  // variables' offset; S is read once, the products scattered into q with FP64 atomics
+  bool cols6 = false;
+  DevBuf c_ptr, c_base, c_xo, c_stride;
   DevBuf ref_r, ref_d, ref_y;   // refined solve: outer residual, correction, operator product (FP64, allocated at its first call)
   int K = 16;               // iterations per replayed graph
   cudaGraphExec_t graph = nullptr;
