@@ -46,4 +46,50 @@ __device__ __forceinline__ bool inv_sym_closed(int de, const double* H, const do
 }
 
 
+// Blocks of 4 to 16 (src/kernels.jl:69-85 up to 8, src/schur_reduction.jl:164-225 above; in FP64 the two agree):
+// upper Cholesky U of the damped block Hd = H + diag(damp), every pivot squared over its damped diagonal entry above
+// singular_tol, inverse U^-1 U^-T (restated from the mathematics: the reference calls StaticArrays and LAPACK here, so
+// this path agrees with it to rounding, not bit for bit). H column-major d x d.
+__device__ __forceinline__ bool inv_sym_chol(int d, const double* H, const double* damp, double* inv) {
+  const double tol = 4504.0 * 2.220446049250313e-16;
+  double U[256], Ui[256];
+  for (int j = 0; j < d; ++j)
+    for (int i = 0; i < d; ++i) U[i + d * j] = i <= j ? H[i + d * j] + (i == j ? damp[i] : 0.0) : 0.0;
+  double hd[16];
+  for (int i = 0; i < d; ++i) hd[i] = U[i + d * i];
+  for (int j = 0; j < d; ++j) {
+    double s = U[j + d * j];
+    for (int k = 0; k < j; ++k) s -= U[k + d * j] * U[k + d * j];
+    if (!(s > 0.0) || !isfinite(s)) return false;
+    const double ujj = sqrt(s);
+    U[j + d * j] = ujj;
+    for (int i = j + 1; i < d; ++i) {
+      double t = U[j + d * i];
+      for (int k = 0; k < j; ++k) t -= U[k + d * j] * U[k + d * i];
+      U[j + d * i] = t / ujj;
+    }
+  }
+  for (int i = 0; i < d; ++i) {
+    const double ratio = (U[i + d * i] * U[i + d * i]) / hd[i];
+    if (!(isfinite(ratio) && ratio > tol)) return false;
+  }
+  for (int j = 0; j < d; ++j)
+    for (int i = 0; i < d; ++i) Ui[i + d * j] = 0.0;
+  for (int j = 0; j < d; ++j) {
+    Ui[j + d * j] = 1.0 / U[j + d * j];
+    for (int i = j - 1; i >= 0; --i) {
+      double s = 0.0;
+      for (int k = i + 1; k <= j; ++k) s += U[i + d * k] * Ui[k + d * j];
+      Ui[i + d * j] = -s / U[i + d * i];
+    }
+  }
+  for (int j = 0; j < d; ++j)
+    for (int i = 0; i < d; ++i) {
+      double s = 0.0;
+      for (int k = i > j ? i : j; k < d; ++k) s += Ui[i + d * k] * Ui[j + d * k];
+      inv[i + d * j] = s;
+    }
+  return true;
+}
+
 }  // namespace bls

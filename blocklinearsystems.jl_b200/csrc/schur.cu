@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(256) k_factor(int64_t neb, const int32_t* __re
   if (e >= neb) return;
   if (!args_ok(st)) return;
   const int de = e_dims[e], eo = eoffsets[e], so = boffsets_e[e];
-  double se[3], damp[3], H[9], inv[9];
+  double se[16], damp[16], H[256], inv[256];
   for (int i = 0; i < de; ++i) {
     se[i] = s_e ? s_e[so + i] : 1.0;
     damp[i] = mul(mul(lambda, scaling_e[so + i]), mul(se[i], se[i]));
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(256) k_factor(int64_t neb, const int32_t* __re
       double h = (double)E[eo + i + de * j];
       H[i + de * j] = s_e ? mul(h, mul(se[i], se[j])) : h;
     }
-  if (!inv_sym_closed(de, H, damp, inv)) {
+  if (!(de <= 3 ? inv_sym_closed(de, H, damp, inv) : inv_sym_chol(de, H, damp, inv))) {
     atomicMin(&st->failed, (long long)e);
     return;
   }
@@ -1314,7 +1314,7 @@ __global__ void __launch_bounds__(256) k_backsub(int64_t neb, const int32_t* __r
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= neb) return;
   const int de = e_dims[e], eo = eoffsets[e], so = boffsets_e[e];
-  double t[3] = {0.0, 0.0, 0.0};
+  double t[16] = {};
   for (int c = eliminated_ptr[e]; c < eliminated_ptr[e + 1]; ++c) {
     const int r = entry_retained[c], dr = r_dims[r], ro = boffsets_r[r], co = coffsets[c];
     for (int ir = 0; ir < dr; ++ir) {
@@ -1362,7 +1362,7 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
     if (d->r_dims[r] != 6) P->uniform36 = false;
   }
   for (int64_t e = 0; e < neb; ++e) {
-    if (d->e_dims[e] < 1 || d->e_dims[e] > 3) throw Error(BLS_EUNSUPPORTED, "eliminated block sizes above 3 are not supported on the device");
+    if (d->e_dims[e] < 1 || d->e_dims[e] > 16) throw Error(BLS_EUNSUPPORTED, "eliminated block sizes above 16 are not supported on the device");
     boff_e[e] = ne; ne += d->e_dims[e];
     P->max_de = std::max<int>(P->max_de, (int)d->e_dims[e]);
     if (d->e_dims[e] != 3) P->uniform36 = false;
@@ -1944,7 +1944,9 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
   } else {
     if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
     if (P->uniform36) launch_pairs<T, 3, 6>(P, S, dense, C, s_r, s_e);
-    else launch_pairs<T, 3, 16>(P, S, dense, C, s_r, s_e);
+    else if (P->max_de <= 3) launch_pairs<T, 3, 16>(P, S, dense, C, s_r, s_e);
+    else if (P->max_de <= 8) launch_pairs<T, 8, 16>(P, S, dense, C, s_r, s_e);
+    else launch_pairs<T, 16, 16>(P, S, dense, C, s_r, s_e);
     if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
     P->launches += 2;
     k_gradient<T><<<grid_for(P->nrblocks * 32, 256), 256, 0, s>>>(

@@ -21,6 +21,12 @@ COUPLED_GROUPS = dict(r_dims=[6, 6, 6, 6], e_dims=[3, 3, 3, 3, 2, 2, 1, 1],
 # test/fixtures/SchurFixtures.jl:189-208 gauge_problem (couplings only)
 GAUGE = dict(r_dims=[6, 6, 6, 6], e_dims=[3] * 6, couplings=[[0, 1], [0, 1, 2], [1, 2, 3], [2, 3], [0, 3], [0, 1, 2, 3]])
 
+# test/fixtures/SchurFixtures.jl:144-151 mixed_dims_problem: point blocks of 1 to 12 variables (the Cholesky forms above
+# 3, and the reference's LAPACK form above 8), each coupled to up to three of four retained blocks (numpy's draws)
+_mrng = np.random.default_rng(11)
+MIXED_DIMS = dict(r_dims=[6, 3, 9, 6], e_dims=[12, 12, 9, 9, 8, 8, 5, 5, 4, 4, 3, 3, 2, 2, 1, 1],
+                  couplings=[sorted(set(int(x) for x in _mrng.integers(0, 4, 3))) for _ in range(16)])
+
 DEVICE_FIXTURES = {"schur_jl": SCHUR_JL, "standard": STANDARD, "coupled_groups": COUPLED_GROUPS, "gauge": GAUGE}
 
 

@@ -11,7 +11,7 @@ import pytest
 import torch
 
 import oracle as orc
-from fixtures import COUPLED_GROUPS, GAUGE, SCHUR_JL, STANDARD, make_problem, split_hessian
+from fixtures import COUPLED_GROUPS, GAUGE, MIXED_DIMS, SCHUR_JL, STANDARD, make_problem, split_hessian
 
 pytestmark = pytest.mark.gpu
 
@@ -78,10 +78,10 @@ def fixture_system(bls, fx, seed=7, lam=0.5):
     return H, b, st, ost, rr, 1.0 + rng.random(len(b))
 
 
-@pytest.mark.parametrize("name", ["schur_jl", "standard", "coupled_groups", "gauge"])
+@pytest.mark.parametrize("name", ["schur_jl", "standard", "coupled_groups", "gauge", "mixed_dims"])
 @pytest.mark.parametrize("dense", [False, True])
 def test_fixture_fp64(bls, name, dense):
-    fx = {"schur_jl": SCHUR_JL, "standard": STANDARD, "coupled_groups": COUPLED_GROUPS, "gauge": GAUGE}[name]
+    fx = {"schur_jl": SCHUR_JL, "standard": STANDARD, "coupled_groups": COUPLED_GROUPS, "gauge": GAUGE, "mixed_dims": MIXED_DIMS}[name]
     H, b, st, ost, rr, sc = fixture_system(bls, fx)
     pat = None if dense else bls.build_schur_pattern(st, rr)
     opat = None if dense else orc.Pattern(ost, rr)
@@ -299,3 +299,26 @@ def test_hessian_bilinear_and_diagonal(bls, dtype, dense):
     assert abs(v - x @ H @ y) <= 1e-12 * (np.abs(x) @ np.abs(H) @ np.abs(y))
     d = ws.hessian_diagonal(R0, cu(E), dense=dense)
     assert relerr(d.cpu().numpy(), np.diag(H)) <= 1e-15
+
+
+@pytest.mark.parametrize("dense", [False, True])
+def test_mixed_dims_mixed_form_and_failure(bls, dense):
+    """Point blocks of 1 to 12 variables (mixed_dims_problem) in the mixed form against the FP64 oracle on the same
+    FP32 values, and a singular 5 x 5 block reported as the lowest failing one."""
+    H, b, st, ost, rr, sc = fixture_system(bls, MIXED_DIMS)
+    pat = None if dense else bls.build_schur_pattern(st, rr)
+    opat = None if dense else orc.Pattern(ost, rr)
+    E, Cd, R = split_hessian(H, st, pat)
+    nr = st.nr
+    o = run_both(bls, st, ost, pat, opat, E, Cd, R, b[:nr], b[nr:], sc[:nr], sc[nr:], 0.5, dense, torch.float32)
+    assert o["ok"] and o["ook"]
+    assert relerr(o["S"], o["oS"]) < 1e-4 and relerr(o["g"], o["og"]) < 1e-6
+    # eliminated block 7 (5 variables, 0-based 6): E and its damping zeroed
+    e = 6
+    eo, de, so = int(st.eoffsets[e]), int(st.e_dims[e]), int(st.boffsets_e[e])
+    E2, sc2 = E.copy(), sc.copy()
+    E2[eo:eo + de * de] = 0.0
+    sc2[nr + so:nr + so + de] = 0.0
+    o = run_both(bls, st, ost, pat, opat, E2, Cd, R, b[:nr], b[nr:], sc2[:nr], sc2[nr:], 0.5, dense, torch.float64)
+    assert not o["ok"] and not o["ook"]
+    assert o["fb"] == e + 1 == o["ofb"]
