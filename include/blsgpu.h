@@ -124,6 +124,9 @@ typedef struct bls_schur_plan_desc {
   int64_t R_length;
 } bls_schur_plan_desc;
 
+/* The device plan of a Schur reduction (the reference's SchurReductionWorkspace plus the pattern). Retained blocks of 1
+ * to 16 variables, eliminated blocks of 1 to 16 (closed-form inverse up to 3, Cholesky above; BLS_EUNSUPPORTED
+ * beyond); uniform 6 / 3 blocks in the canonical layout take the fast kernels. */
 int bls_schur_plan_create(bls_ctx* ctx, const bls_schur_plan_desc* desc, bls_schur_plan** out);
 int bls_schur_plan_destroy(bls_schur_plan* plan);
 /* Device bytes the plan holds (index arrays + scratch). */
