@@ -1571,31 +1571,6 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
       }
     }
   }
-  // point-major pair records for k_points36: per point, its pairs by c2 then c1, as {c1, k | (c2 - c1) << 25}
-  std::vector<int2> prec;
-  std::vector<int64_t> pptr(neb + 1, 0);
-  for (int64_t e = 0; e < neb; ++e) {
-    const int64_t kk = d->eliminated_ptr[e + 1] - d->eliminated_ptr[e];
-    pptr[e + 1] = pptr[e] + kk * (kk + 1) / 2;
-  }
-  if (P->fast36 && nb < (int64_t(1) << 25) && pptr[neb] == npairs) {
-    prec.resize(npairs);
-#pragma omp parallel for schedule(dynamic, 256)
-    for (int64_t e = 0; e < neb; ++e) {
-      int64_t q = pptr[e];
-      const int64_t p0 = d->eliminated_ptr[e], p1 = d->eliminated_ptr[e + 1];
-      for (int64_t c2 = p0; c2 < p1; ++c2) {
-        const int64_t r2 = d->entry_retained[c2];
-        const int64_t* lo = browval.data() + bcolptr[r2];
-        const int64_t* hi = browval.data() + bcolptr[r2 + 1];
-        for (int64_t c1 = p0; c1 <= c2; ++c1) {
-          const int64_t k = std::lower_bound(lo, hi, d->entry_retained[c1]) - browval.data();   // present: checked above
-          prec[q++] = make_int2((int32_t)c1, (int32_t)((uint32_t)k | ((uint32_t)(c2 - c1) << 25)));
-        }
-      }
-    }
-    P->points_ok = true;
-  }
   // staged work items for the host-buffer reduction: stage j holds points [stage_pt[j], stage_pt[j + 1]); a block's
   // pairs ascend in point within its slot, so its pairs of one stage are a contiguous run, cut into items of at most
   // PAIR_CHUNK pairs (solo when the run makes one item)
@@ -1672,7 +1647,6 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
     upload(P->col_base, cbase, s);
     upload(P->col_h, ch, s);
     upload(P->pair_packed, packed, s);
-    if (P->points_ok) upload(P->pt_rec, prec, s);
     if (P->staged) {
       upload(P->st_block, sb_all, s);
       upload(P->st_start, ss_all, s);
@@ -1841,6 +1815,44 @@ static void launch_pairs(SchurPlan* P, T* S, bool dense, const T* C, const doubl
       dense ? P->block_base_dense.as<int64_t>() : P->block_base_sparse.as<int64_t>(), dense ? nullptr : P->block_stride_sparse.as<int32_t>(),
       P->nr, P->r_dims.as<int32_t>(), P->boffsets_r.as<int32_t>(), P->entry_eliminated.as<int32_t>(), P->e_dims.as<int32_t>(),
       P->boffsets_e.as<int32_t>(), P->eoffsets.as<int32_t>(), P->coffsets.as<int32_t>(), C, Einv, s_r, s_e, S, P->status.as<Status>());
+}
+
+// The point-major pair records of k_points36, built from the plan's own lists the first time that schedule is chosen
+// (a plan that never uses it keeps no copy): every pair of the block-owned items gets its block, then the pairs are
+// ordered by point, c2, c1 as {c1, k | (c2 - c1) << 25}. Synchronises.
+static void ensure_points(SchurPlan* P) {
+  if (P->points_ok || !P->fast36 || P->nblocks >= (int64_t(1) << 25) || P->npairs == 0) return;
+  cudaStream_t s = P->ctx->stream;
+  std::vector<int32_t> ib(P->nitems), is(P->nitems), ii(P->nitems);
+  std::vector<int2> pk(P->npairs);
+  BLS_CUDA(cudaMemcpyAsync(ib.data(), P->item_block.p, sizeof(int32_t) * P->nitems, cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaMemcpyAsync(is.data(), P->item_start.p, sizeof(int32_t) * P->nitems, cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaMemcpyAsync(ii.data(), P->item_info.p, sizeof(int32_t) * P->nitems, cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaMemcpyAsync(pk.data(), P->pair_packed.p, sizeof(int2) * P->npairs, cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaStreamSynchronize(s));
+  std::vector<int32_t> blk(P->npairs);
+  for (int64_t i = 0; i < P->nitems; ++i)
+    for (int32_t q = is[i]; q < is[i] + (ii[i] & 0xffff); ++q) blk[q] = ib[i];
+  const int64_t neb = P->neblocks;
+  std::vector<int64_t> ptr(neb + 1, 0);
+  for (int64_t q = 0; q < P->npairs; ++q) ptr[(pk[q].y & 0xffffff) + 1] += 1;
+  for (int64_t e = 0; e < neb; ++e) ptr[e + 1] += ptr[e];
+  std::vector<int64_t> fill(ptr.begin(), ptr.end() - 1);
+  std::vector<int2> rec(P->npairs);
+  for (int64_t q = 0; q < P->npairs; ++q) {
+    const int32_t c1 = pk[q].x;
+    const uint32_t dc = (uint32_t)pk[q].y >> 24;
+    rec[fill[pk[q].y & 0xffffff]++] = make_int2(c1, (int32_t)((uint32_t)blk[q] | (dc << 25)));
+  }
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int64_t e = 0; e < neb; ++e)
+    std::sort(rec.begin() + ptr[e], rec.begin() + ptr[e + 1], [](const int2& a, const int2& b) {
+      const int64_t a2 = a.x + (int64_t)((uint32_t)a.y >> 25), b2 = b.x + (int64_t)((uint32_t)b.y >> 25);
+      return a2 != b2 ? a2 < b2 : a.x < b.x;
+    });
+  upload(P->pt_rec, rec, s);
+  BLS_CUDA(cudaStreamSynchronize(s));
+  P->points_ok = true;
 }
 
 template <class T>
@@ -2258,8 +2270,11 @@ int bls_reduce_schur_dense(bls_schur_plan* P, int dtype, void* S, double* g, con
 
 int bls_schur_plan_set_kernel(bls_schur_plan* P, int which) {
   if (!P || which < 0 || which > 4) return BLS_EINVAL;
-  P->kernel = which;
-  return BLS_OK;
+  BLS_GUARD({
+    if (which == 4) ensure_points(P);
+    P->kernel = which;
+    return BLS_OK;
+  })
 }
 
 int bls_schur_plan_instrument(bls_schur_plan* P, int timing) {
