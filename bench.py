@@ -102,15 +102,31 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The largest of every rank's x (a job's time is its slowest replica's); x itself on one rank."""
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_spec(spec, rank: int, world: int):
+    """Each replica's own scene: the same distribution, the seed moved by 100 per rank (one rank keeps it)."""
+    if world == 1:
+        return spec
+    from dataclasses import replace
+    return replace(spec, seed=spec.seed + 100 * rank)
+
+
 def run_ours(args, rank: int, world: int) -> dict | None:
     import torch
     bls = load_package()
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     spec = bls.scenes.workload(args.workload)
-    if world > 1:
-        from dataclasses import replace
-        spec = replace(spec, seed=spec.seed + 100 * rank)   # each replica its own scene of the same distribution
+    spec = replica_spec(spec, rank, world)   # each replica its own scene of the same distribution
     p = bls.scenes.hessian_problem(spec)
     st, pat = p.structure, p.pattern
     ws = bls.SchurReductionWorkspace(st, pat, device=dev.index)
@@ -151,10 +167,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         ws.instrument(False)
         ok = ws.query_status()
         assert ok, f"reduction failed at block {ws.failed_block}"
-        if world > 1:
-            t = torch.tensor([total], device=dev, dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(total, world, dev)
         return total, cnt
 
     d32 = device_inputs(torch.float32)
@@ -192,10 +205,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     b.record()
     torch.cuda.synchronize()
     e2e_ms = a.elapsed_time(b)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, world, dev)
     assert ws.query_status()
 
     if rank != 0:
@@ -251,9 +261,7 @@ def run_ours_qr(args, rank: int, world: int) -> dict | None:
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     spec = bls.scenes.workload(args.workload)
-    if world > 1:
-        from dataclasses import replace
-        spec = replace(spec, seed=spec.seed + 100 * rank)
+    spec = replica_spec(spec, rank, world)
     p = bls.scenes.jacobian_problem(spec)
     jst = p.structure
     pat = bls.build_schur_pattern(jst.schur, bls.free_block_pairs(jst))
@@ -292,10 +300,7 @@ def run_ours_qr(args, rank: int, world: int) -> dict | None:
         assert ws.query_status()
         total = sum(a.elapsed_time(c) for a, b, c in evs)
         qr_ms = sum(a.elapsed_time(b) for a, b, c in evs) / args.steps
-        if world > 1:
-            t = torch.tensor([total], device=dev, dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(total, world, dev)
         return total, qr_ms, launches
 
     ws32, J32, S32, g32 = setup(torch.float32)
@@ -530,10 +535,7 @@ def run_ours_batch(args, rank: int, world: int) -> dict | None:
         torch.cuda.synchronize()
         assert B.ok()
         total = sum(a.elapsed_time(b) for a, b in evs)
-        if world > 1:
-            t = torch.tensor([total], device=dev, dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(total, world, dev)
         return total
 
     B64 = bls.batch.BatchedReduction(problems, torch.float64, device=dev.index)
