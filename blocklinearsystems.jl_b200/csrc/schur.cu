@@ -2135,6 +2135,7 @@ static int apply_elimination(SchurPlan* P, double* y, const double* y0, const do
 
 template <class T>
 static void backsub(SchurPlan* P, double* x_e, const double* x_r, const T* C, const double* s_r, const double* s_e) {
+  if (P->neblocks == 0) return;
   P->launches += 1;
   k_backsub<T><<<grid_for(P->neblocks, 256), 256, 0, P->ctx->stream>>>(
       P->neblocks, P->e_dims.as<int32_t>(), P->eoffsets.as<int32_t>(), P->boffsets_e.as<int32_t>(), P->eliminated_ptr.as<int32_t>(),

@@ -322,3 +322,38 @@ def test_mixed_dims_mixed_form_and_failure(bls, dense):
     o = run_both(bls, st, ost, pat, opat, E2, Cd, R, b[:nr], b[nr:], sc2[:nr], sc2[nr:], 0.5, dense, torch.float64)
     assert not o["ok"] and not o["ook"]
     assert o["fb"] == e + 1 == o["ofb"]
+
+
+EDGE = {
+    # a camera no point observes: its S column is its reset diagonal block, its gradient b_r
+    "unobserved_camera": dict(r_dims=[6, 6, 6], e_dims=[3, 3, 3, 3], couplings=[[0, 1], [0], [1], [0, 1]]),
+    # points observed by a single camera: diagonal pairs only
+    "single_observations": dict(r_dims=[6, 6], e_dims=[3, 3, 3, 3, 3], couplings=[[0], [1], [0], [1], [0]]),
+    # a lone point on every camera at once
+    "one_point": dict(r_dims=[6, 6, 6, 6], e_dims=[3], couplings=[[0, 1, 2, 3]]),
+}
+
+
+@pytest.mark.parametrize("name", list(EDGE))
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+@pytest.mark.parametrize("dense", [False, True])
+def test_edge_structures(bls, name, dtype, dense):
+    """Ragged and degenerate structures on the 6/3 fast path against the oracle."""
+    H, b, st, ost, rr, sc = fixture_system(bls, EDGE[name])
+    pat = None if dense else bls.build_schur_pattern(st, rr)
+    opat = None if dense else orc.Pattern(ost, rr)
+    E, Cd, R = split_hessian(H, st, pat)
+    nr = st.nr
+    o = run_both(bls, st, ost, pat, opat, E, Cd, R, b[:nr], b[nr:], sc[:nr], sc[nr:], 0.5, dense, dtype)
+    assert o["ok"] and o["ook"]
+    tol = 1e-12 if dtype == torch.float64 else 1e-5
+    assert relerr(o["S"], o["oS"]) < tol and relerr(o["g"], o["og"]) < 1e-12
+
+
+def test_plan_needs_an_eliminated_block(bls):
+    """A structure without eliminated blocks has nothing to reduce: the device plan rejects it (ArgumentError) instead
+    of returning the reset system as the reference's loop over no blocks does."""
+    st = bls.SchurStructure.positional([6, 6], [], [])
+    pat = bls.build_schur_pattern(st, [])
+    with pytest.raises(bls.ArgumentError, match="at least one retained and one eliminated block"):
+        bls.SchurReductionWorkspace(st, pat)
