@@ -1980,8 +1980,8 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
 // and runs each stage's pair items while the next stage's couplings are still being copied. S and g_S are copied
 // back only when the status word is clean.
 template <class T>
-static int reduce_host(SchurPlan* P, T* S_h, double* g_h, const T* R_h, const double* scr_h, double lambda, const double* br_h,
-                       const double* be_h, const double* sce_h, const T* E_h, const T* C_h, int64_t* failed_block) {
+static int reduce_host_impl(SchurPlan* P, T* S_h, double* g_h, const T* R_h, const double* scr_h, double lambda, const double* br_h,
+                            const double* be_h, const double* sce_h, const T* E_h, const T* C_h, int64_t* failed_block) {
   if (!P->staged || !P->reset_fused)
     throw Error(BLS_EUNSUPPORTED, "the host-buffer reduction needs a sparse plan on the 6/3 fast path with diag_inds in their columns");
   if (!S_h || !g_h || !scr_h || !br_h || (P->neblocks > 0 && (!be_h || !sce_h || !E_h || !C_h)) || (P->R_length > 0 && !R_h))
@@ -2061,6 +2061,21 @@ static int reduce_host(SchurPlan* P, T* S_h, double* g_h, const T* R_h, const do
   BLS_CUDA(cudaStreamSynchronize(s));
   return BLS_OK;
 }
+
+// The host call returns only when nothing it enqueued still reads or writes the caller's host buffers: on an error the
+// copy stream and the plan's stream are drained before the error is passed on.
+template <class T>
+static int reduce_host(SchurPlan* P, T* S_h, double* g_h, const T* R_h, const double* scr_h, double lambda, const double* br_h,
+                       const double* be_h, const double* sce_h, const T* E_h, const T* C_h, int64_t* failed_block) {
+  try {
+    return reduce_host_impl<T>(P, S_h, g_h, R_h, scr_h, lambda, br_h, be_h, sce_h, E_h, C_h, failed_block);
+  } catch (...) {
+    if (P->copy_stream) cudaStreamSynchronize(P->copy_stream);
+    cudaStreamSynchronize(P->ctx->stream);
+    throw;
+  }
+}
+
 
 template <class T>
 static double hessian_bilinear(SchurPlan* P, const T* R, bool dense, const T* E, const T* C, const double* x, const double* y) {
