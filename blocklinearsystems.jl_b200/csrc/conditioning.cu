@@ -51,7 +51,7 @@ extern "C" int bls_prepare_scale(bls_ctx* ctx, int dtype, int64_t n, const doubl
     if (!ctx || n < 0 || (n > 0 && (!d || !sc || !s))) throw Error(BLS_EINVAL, "null argument");
     if (dtype != BLS_F64 && dtype != BLS_F32) throw Error(BLS_EINVAL, "unknown dtype");
     const double fmin = dtype == BLS_F64 ? 2.2250738585072014e-308 : 1.1754943508222875e-38;   // floatmin(T)
-    lambda = lambda > 0.0 ? lambda : 0.0;   // max(lambda, 0.0)
+    if (!(lambda != lambda) && !(lambda > 0.0)) lambda = 0.0;   // max(lambda, 0.0), which keeps a NaN
     cudaStream_t st = ctx->stream;
     if (!ctx->flag) BLS_CUDA(cudaMalloc(&ctx->flag, sizeof(int)));
     BLS_CUDA(cudaMemsetAsync(ctx->flag, 0, sizeof(int), st));
