@@ -210,20 +210,20 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
     for (int j = lane; j < C; j += 32) {
       if (j >= ce && j <= ce + k) continue;
       T* y = A + j * M;
-      // v'y in four independent partial sums (the FMA chain is the latency of this loop)
-      double p0 = (double)y[k], p1 = 0.0, p2 = 0.0, p3 = 0.0;
+      // v'y in four independent partial sums (the FMA chain is the latency of this loop), in the storage type: the
+      // panel update is FP32 in the mixed form, the reflector's tau (its scaling) FP64
+      T p0 = y[k], p1 = T(0), p2 = T(0), p3 = T(0);
       int i = k + 1;
       for (; i + 3 < M; i += 4) {
-        p0 += (double)col[i] * (double)y[i];
-        p1 += (double)col[i + 1] * (double)y[i + 1];
-        p2 += (double)col[i + 2] * (double)y[i + 2];
-        p3 += (double)col[i + 3] * (double)y[i + 3];
+        p0 += col[i] * y[i];
+        p1 += col[i + 1] * y[i + 1];
+        p2 += col[i + 2] * y[i + 2];
+        p3 += col[i + 3] * y[i + 3];
       }
-      for (; i < M; ++i) p0 += (double)col[i] * (double)y[i];
-      double sj = (p0 + p1) + (p2 + p3);
-      sj *= tau;
-      y[k] = T((double)y[k] - sj);
-      for (int i = k + 1; i < M; ++i) y[i] = T((double)y[i] - sj * (double)col[i]);
+      for (; i < M; ++i) p0 += col[i] * y[i];
+      const T sj = T((double)((p0 + p1) + (p2 + p3)) * tau);
+      y[k] = y[k] - sj;
+      for (int i = k + 1; i < M; ++i) y[i] = y[i] - sj * col[i];
     }
     // and to the FP64 residual
     double sr = 0.0;
