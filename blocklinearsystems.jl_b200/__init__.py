@@ -20,6 +20,7 @@ from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce
 from .qr import (QRReductionWorkspace, SchurBlockJacobian, assemble_hessian, jtj_diag, jtj_quadform, jtr, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
                  reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse)
 from .pcg import BlockJacobi, PCGResult, PCGWorkspace, RefinedResult, factor_diagonal_blocks, solve_diagonal_blocks
+from .dense import DenseCholesky
 from . import batch, gnn, scenes
 
 __all__ = [
@@ -27,6 +28,6 @@ __all__ = [
     "build_schur_pattern", "sparse_with_map", "SchurReductionWorkspace", "backsubstitute", "context", "reduce_schur_dense",
     "reduce_schur_sparse", "reset_reduce_schur_sparse_host", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
     "SchurBlockJacobian", "SchurJacobianStructure", "assemble_hessian", "jtj_diag", "jtj_quadform", "jtr", "prepare_scale", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
-    "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "BlockJacobi", "PCGResult", "PCGWorkspace", "RefinedResult",
+    "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "BlockJacobi", "PCGResult", "PCGWorkspace", "RefinedResult", "DenseCholesky",
     "factor_diagonal_blocks", "solve_diagonal_blocks", "gnn", "batch",
 ]

@@ -115,6 +115,10 @@ def gpu() -> C.CDLL:
             "bls_jtj_diag": (C.c_int, [vp, C.c_int, vp, vp]),
             "bls_jtj_quadform": (C.c_int, [vp, C.c_int, vp, vp, pdbl]),
             "bls_prepare_scale": (C.c_int, [vp, C.c_int, i64, vp, C.c_double, vp, vp, C.c_int, C.POINTER(C.c_int)]),
+            "bls_dense_solver_create": (C.c_int, [vp, i64, C.POINTER(vp)]),
+            "bls_dense_solver_destroy": (C.c_int, [vp]),
+            "bls_dense_cholesky": (C.c_int, [vp, C.c_int, vp, p64]),
+            "bls_dense_cholesky_solve": (C.c_int, [vp, vp, vp]),
             "bls_block_jacobi_create": (C.c_int, [vp, i64, p64, C.POINTER(vp)]),
             "bls_block_jacobi_destroy": (C.c_int, [vp]),
             "bls_factor_diagonal_blocks": (C.c_int, [vp, C.c_int, vp, p64]),

@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xc
               "-ccbin", "g++"] + GENCODE
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wno-unknown-pragmas"]
 
-GPU_SOURCES = ["schur.cu", "noalloc.cu", "qr.cu", "pcg.cu", "gnn.cu", "conditioning.cu", "capi.cpp", "host_layout.cpp"]
+GPU_SOURCES = ["schur.cu", "noalloc.cu", "qr.cu", "pcg.cu", "gnn.cu", "conditioning.cu", "dense.cu", "capi.cpp", "host_layout.cpp"]
 SCENE_SOURCES = ["scene.cpp"]
 
 

@@ -360,6 +360,17 @@ int bls_pcg_solve_refined(bls_pcg_plan* plan, bls_schur_plan* schur, int dtype, 
                           const double* scaling_r_dev, double lambda, const void* C_data_dev, const double* g_dev, double* x_dev,
                           double tol, double inner_tol, int64_t max_outer, int64_t inner_maxit, int64_t* outer_iterations,
                           int64_t* inner_iterations, double* rel_residual, int64_t* failed_block);
+/* Dense reduced solve (the reference hands a dense S to DampedLinearSolve's Cholesky, src/schur_linear_systems.jl:
+ * 312-320): a solver for n x n systems (n <= 16384) owning an FP64 working matrix. bls_dense_cholesky reads S
+ * (dtype, column-major, its upper triangle: reduce_schur_dense!'s output) and factors it as L L' in FP64; a pivot that
+ * is not positive returns BLS_NOT_PD with failed_column = its column, 1-based. bls_dense_cholesky_solve: x = S^-1 g
+ * (FP64 device vectors) from the last successful factorisation. */
+typedef struct bls_dense_solver bls_dense_solver;
+int bls_dense_solver_create(bls_ctx* ctx, int64_t n, bls_dense_solver** out);
+int bls_dense_solver_destroy(bls_dense_solver* solver);
+int bls_dense_cholesky(bls_dense_solver* solver, int dtype, const void* S_dev, int64_t* failed_column);
+int bls_dense_cholesky_solve(bls_dense_solver* solver, const double* g_dev, double* x_dev);
+
 /* prepare_scale! (src/conditioning.jl:60-87) of an EliminationConditioning: s[n] = the conditioning scale of each
  * variable (conditioning_scale, :29-36: the power of two nearest on a log scale to 1/(1e-12 + sqrt|d_j + lambda sc_j|),
  * at least floatmin of dtype, 1 for a non-finite entry), computed for every variable when stale is set, else only when

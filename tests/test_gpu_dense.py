@@ -1,0 +1,83 @@
+"""Dense reduced solve on the device (Cholesky of the dense S that reduce_schur_dense! produces, then x = S^-1 g)
+against a dense FP64 solve on the host of the same stored S (the oracle's reduction for the scene), within 1e-10;
+random SPD systems across tile boundaries; the first non-positive pivot reported as its 1-based column."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+def relerr(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def first_bad_pivot(A):
+    """The 1-based column of the first pivot of A's unblocked Cholesky that is not positive, 0 if none."""
+    A = np.array(A, np.float64)
+    n = A.shape[0]
+    for j in range(n):
+        d = A[j, j] - A[j, :j] @ A[j, :j]
+        if not (d > 0) or not np.isfinite(d):
+            return j + 1
+        A[j, j] = np.sqrt(d)
+        A[j + 1:, j] = (A[j + 1:, j] - A[j + 1:, :j] @ A[j, :j]) / A[j, j]
+    return 0
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+def test_dense_scene_solve(bls, dtype):
+    spec = bls.scenes.workload("dense_50x2000")
+    p = bls.scenes.hessian_problem(spec, dense=True)
+    st = p.structure
+    nr = st.nr
+    cu = lambda a, t=dtype: torch.from_numpy(np.ascontiguousarray(a)).to(device=DEV, dtype=t)
+    ws = bls.SchurReductionWorkspace(st, None)
+    S = torch.zeros(nr * nr, dtype=dtype, device=DEV)
+    g = torch.zeros(nr, dtype=torch.float64, device=DEV)
+    bls.reset_schur_dense(S, cu(p.R), cu(p.scaling_r, torch.float64), p.lam, ws)
+    assert bls.reduce_schur_dense(S, g, cu(p.b_r, torch.float64), cu(p.b_e, torch.float64), cu(p.scaling_e, torch.float64), p.lam, st,
+                                  cu(p.E), cu(p.C), ws)
+    A = S.double().cpu().numpy().reshape(nr, nr, order="F")
+    A = np.triu(A) + np.triu(A, 1).T
+    x_ref = np.linalg.solve(A, g.cpu().numpy())
+    D = bls.DenseCholesky(nr)
+    assert D.factor(S) and D.failed_column == 0
+    x = D.solve(g)
+    assert relerr(x.cpu().numpy(), x_ref) <= 1e-10
+    # a second solve from the same factorisation, another right-hand side
+    g2 = torch.from_numpy(np.random.default_rng(3).standard_normal(nr)).to(DEV)
+    assert relerr(D.solve(g2).cpu().numpy(), np.linalg.solve(A, g2.cpu().numpy())) <= 1e-10
+
+
+@pytest.mark.parametrize("n", [1, 7, 32, 33, 100, 517])
+def test_random_spd_across_tiles(bls, n):
+    rng = np.random.default_rng(n)
+    B = rng.standard_normal((n, n))
+    A = B @ B.T + n * np.eye(n)
+    Su = np.triu(A) + np.tril(rng.standard_normal((n, n)), -1)   # only the upper triangle is read
+    D = bls.DenseCholesky(n)
+    assert D.factor(torch.from_numpy(Su.ravel(order="F")).to(DEV))
+    g = rng.standard_normal(n)
+    x = D.solve(torch.from_numpy(g).to(DEV))
+    assert relerr(x.cpu().numpy(), np.linalg.solve(A, g)) <= 1e-10
+
+
+def test_not_positive_definite_reports_column(bls):
+    rng = np.random.default_rng(8)
+    n = 100
+    B = rng.standard_normal((n, n))
+    A = B @ B.T + n * np.eye(n)
+    A[57, 57] = -1e3
+    col = first_bad_pivot(A)
+    assert col > 0
+    D = bls.DenseCholesky(n)
+    assert not D.factor(torch.from_numpy(A.ravel(order="F")).to(DEV))
+    assert D.failed_column == col
+    with pytest.raises(bls.ArgumentError):
+        D.solve(torch.zeros(n, dtype=torch.float64, device=DEV))
