@@ -5,7 +5,7 @@
 // right-looking blocked Cholesky with 32 x 32 tiles: per tile column, the diagonal tile in one CTA's shared memory,
 // the tiles below it by a triangular solve, then the trailing lower triangle updated tile by tile. A pivot that is not
 // positive (or not finite) stops the factorisation; its column is reported, 1-based. The solve runs the two triangular
-// substitutions column by column in one CTA.
+// substitutions by 32-column tiles in one CTA.
 #include <algorithm>
 #include <cmath>
 #include <memory>
@@ -113,27 +113,62 @@ __global__ void __launch_bounds__(DNB * DNB) k_syrk_tiles(int64_t n, double* __r
   (void)nt;
 }
 
-// x = (L L')^-1 g: forward then backward substitution, column by column, in one CTA
+// x = (L L')^-1 g in one CTA, by 32-column tiles: each diagonal tile is solved by one warp (a lane per row, the pivot
+// broadcast by shuffle), then every thread updates the rows the tile feeds (forward: the rows below, reading the
+// tile's columns of L down a column; backward: the rows above, reading each row's 32 contiguous entries of the tile's
+// rows of L). The right-hand side lives in shared memory.
 __global__ void __launch_bounds__(1024) k_chol_solve(int64_t n, const double* __restrict__ W, const double* __restrict__ g,
                                                      double* __restrict__ x) {
   extern __shared__ double y[];
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) y[i] = g[i];
+  __shared__ double t[DNB][DNB + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int64_t i = tid; i < n; i += blockDim.x) y[i] = g[i];
   __syncthreads();
-  for (int64_t j = 0; j < n; ++j) {   // L y = g
-    const double yj = y[j] / W[j + n * j];
+  // forward: L y = g
+  for (int64_t k0 = 0; k0 < n; k0 += DNB) {
+    const int nb = (int)(n - k0 < DNB ? n - k0 : DNB);
+    for (int q = tid; q < nb * nb; q += blockDim.x) t[q % nb][q / nb] = W[(k0 + q % nb) + n * (k0 + q / nb)];
     __syncthreads();
-    for (int64_t i = j + 1 + threadIdx.x; i < n; i += blockDim.x) y[i] -= W[i + n * j] * yj;
-    if (threadIdx.x == 0) y[j] = yj;
+    if (warp == 0) {
+      double yr = lane < nb ? y[k0 + lane] : 0.0;
+      for (int c = 0; c < nb; ++c) {
+        const double yc = __shfl_sync(0xffffffffu, yr, c) / t[c][c];
+        if (lane == c) yr = yc;
+        else if (lane > c && lane < nb) yr -= t[lane][c] * yc;
+      }
+      if (lane < nb) y[k0 + lane] = yr;
+    }
+    __syncthreads();
+    for (int64_t i = k0 + nb + tid; i < n; i += blockDim.x) {
+      double s = 0.0;
+      for (int c = 0; c < nb; ++c) s += W[i + n * (k0 + c)] * y[k0 + c];
+      y[i] -= s;
+    }
     __syncthreads();
   }
-  for (int64_t j = n - 1; j >= 0; --j) {   // L' x = y
-    const double xj = y[j] / W[j + n * j];
+  // backward: L' x = y
+  for (int64_t k0 = ((n - 1) / DNB) * DNB; k0 >= 0; k0 -= DNB) {
+    const int nb = (int)(n - k0 < DNB ? n - k0 : DNB);
+    for (int q = tid; q < nb * nb; q += blockDim.x) t[q % nb][q / nb] = W[(k0 + q % nb) + n * (k0 + q / nb)];
     __syncthreads();
-    for (int64_t i = threadIdx.x; i < j; i += blockDim.x) y[i] -= W[j + n * i] * xj;
-    if (threadIdx.x == 0) y[j] = xj;
+    if (warp == 0) {
+      double yr = lane < nb ? y[k0 + lane] : 0.0;
+      for (int c = nb - 1; c >= 0; --c) {
+        const double xc = __shfl_sync(0xffffffffu, yr, c) / t[c][c];
+        if (lane == c) yr = xc;
+        else if (lane < c) yr -= t[c][lane] * xc;
+      }
+      if (lane < nb) y[k0 + lane] = yr;
+    }
+    __syncthreads();
+    for (int64_t i = tid; i < k0; i += blockDim.x) {
+      double s = 0.0;
+      for (int c = 0; c < nb; ++c) s += W[(k0 + c) + n * i] * y[k0 + c];
+      y[i] -= s;
+    }
     __syncthreads();
   }
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) x[i] = y[i];
+  for (int64_t i = tid; i < n; i += blockDim.x) x[i] = y[i];
 }
 
 template <class T>
@@ -215,7 +250,9 @@ int bls_dense_cholesky_solve(bls_dense_solver* D, const double* g, double* x) {
     if (!D || !g || !x) throw Error(BLS_EINVAL, "null argument");
     if (!D->factored) throw Error(BLS_EINVAL, "the solver holds no factorisation (bls_dense_cholesky first, and it must succeed)");
     const size_t smem = sizeof(double) * (size_t)D->n;
-    if (smem > 48 * 1024) BLS_CUDA(cudaFuncSetAttribute(k_chol_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // The static tile counts against the 48 KB default too, so opt in whenever the sum passes it.
+    const size_t tile = sizeof(double) * DNB * (DNB + 1);
+    if (smem + tile > 48 * 1024) BLS_CUDA(cudaFuncSetAttribute(k_chol_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_chol_solve<<<1, 1024, smem, D->ctx->stream>>>(D->n, D->W.as<double>(), g, x);
     BLS_CUDA(cudaGetLastError());
     return BLS_OK;
