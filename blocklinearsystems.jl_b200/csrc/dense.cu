@@ -2,10 +2,11 @@
 // reduce_schur_dense! when S is small enough to hold dense (the reference hands its dense S to DampedLinearSolve's
 // Cholesky, src/schur_linear_systems.jl:312-320). S is read from its upper triangle in its storage type (FP64 or the
 // mixed form's FP32), mirrored into an FP64 working matrix owned by the solver, and factored in place as S = L L' by a
-// right-looking blocked Cholesky with 32 x 32 tiles: per tile column, the diagonal tile in one CTA's shared memory,
-// the tiles below it by a triangular solve, then the trailing lower triangle updated tile by tile. A pivot that is not
+// right-looking blocked Cholesky with 64-column panels: per panel, the diagonal tile in one CTA's registers, the rows
+// below it by a triangular solve, then the trailing lower triangle updated in 64 x 64 tiles. A pivot that is not
 // positive (or not finite) stops the factorisation; its column is reported, 1-based. The solve runs the two triangular
-// substitutions by 32-column tiles in one CTA.
+// substitutions as one launch per 64-row tile: all CTAs apply the last solved tile to the rows it feeds, and CTA 0,
+// whose rows are the next diagonal tile, then solves that tile.
 #include <algorithm>
 #include <cmath>
 #include <memory>
@@ -14,14 +15,24 @@
 
 namespace bls {
 
-constexpr int DNB = 32;   // tile size
+constexpr int NB = 64;   // panel width and tile size
 
 struct DenseSolver {
   bls_ctx* ctx = nullptr;
   int64_t n = 0;
   DevBuf W;        // n x n FP64, column-major; L in its lower triangle after a successful factorisation
+  DevBuf dinv;     // n FP64: 1 / L[j, j], written by the factorisation
   DevBuf status;   // [0]: first failing column (0-based) or -1
   bool factored = false;
+  // The next panel's diagonal tile and triangular solve run on a high-priority stream while the rest of the trailing
+  // update runs on the caller's stream (created at the first factorisation).
+  cudaStream_t panel_stream = nullptr;
+  cudaEvent_t ev_join = nullptr, ev_panel = nullptr;
+  ~DenseSolver() {
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_panel) cudaEventDestroy(ev_panel);
+    if (panel_stream) cudaStreamDestroy(panel_stream);
+  }
 };
 
 // W = S mirrored from its upper triangle, in FP64
@@ -34,141 +45,283 @@ __global__ void k_dense_load(int64_t n, const T* __restrict__ S, double* __restr
   }
 }
 
-// The diagonal tile [k0, k0 + nb) in one CTA of 32 x 32 threads: unblocked Cholesky in shared memory, lower triangle
-// written back. A non-positive or non-finite pivot records its column and leaves W as it is.
-__global__ void __launch_bounds__(DNB * DNB) k_potrf_tile(int64_t n, double* __restrict__ W, int64_t k0, int nb,
-                                                          long long* __restrict__ status) {
-  __shared__ double a[DNB][DNB + 1];
-  __shared__ int bad;
+// The diagonal tile [k0, k0 + nb) in one CTA of 256 threads, right-looking and unblocked: thread (tx, ty) keeps the
+// entries of rows tx + 16 p and columns ty + 16 q in registers; per column the owners publish it to shared memory
+// (double-buffered, one barrier per column) and every thread scales and updates its own entries. A non-positive or
+// non-finite pivot records its column and leaves W as it is. 1 / L[j, j] goes to dinv.
+__global__ void __launch_bounds__(256) k_potrf_tile(int64_t n, double* __restrict__ W, double* __restrict__ dinv, int64_t k0,
+                                                    int nb, long long* __restrict__ status) {
+  __shared__ double col[2][NB];
   if (status[0] >= 0) return;   // uniform across the CTA
-  const int tx = threadIdx.x, ty = threadIdx.y;   // a[ty][tx] = W[k0 + ty, k0 + tx]
-  if (tx < nb && ty < nb) a[ty][tx] = W[(k0 + ty) + n * (k0 + tx)];
-  if (tx == 0 && ty == 0) bad = 0;
-  __syncthreads();
-  for (int j = 0; j < nb; ++j) {
-    const double d = a[j][j];
-    if (!(d > 0.0) || !isfinite(d)) {
-      if (tx == 0 && ty == 0) {
-        bad = 1;
-        status[0] = k0 + j;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double a[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = tx + 16 * p, c = ty + 16 * q;
+      a[p][q] = (r < nb && c <= r) ? W[(k0 + r) + n * (k0 + c)] : 0.0;
+    }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    for (int jj = 0; jj < 16; ++jj) {
+      const int j = 16 * q + jj;
+      if (j >= nb) break;   // uniform
+      const int b = j & 1;
+      if (ty == jj) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) col[b][tx + 16 * p] = a[p][q];
       }
-      return;   // every thread reads the same d: the whole CTA returns here
+      __syncthreads();
+      const double d = col[b][j];
+      if (!(d > 0.0) || !isfinite(d)) {   // every thread reads the same d: the whole CTA returns here
+        if (threadIdx.x == 0) status[0] = k0 + j;
+        return;
+      }
+      const double ljj = sqrt(d), inv = rsqrt(d);   // independent, so the column's chain waits on one of them
+      if (threadIdx.x == 0) dinv[k0 + j] = inv;
+      double li[4], lc[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        li[p] = col[b][tx + 16 * p] * inv;
+        lc[p] = col[b][ty + 16 * p] * inv;
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q2 = 0; q2 < 4; ++q2) {
+          const int r = tx + 16 * p, c = ty + 16 * q2;
+          if (c == j) {
+            if (r == j) a[p][q2] = ljj;
+            else if (r > j) a[p][q2] = li[p];
+          } else if (c > j && r >= c) {
+            a[p][q2] -= li[p] * lc[q2];
+          }
+        }
     }
-    const double ljj = sqrt(d);
-    __syncthreads();
-    if (ty > j && tx == 0) a[ty][j] /= ljj;
-    if (ty == j && tx == 0) a[j][j] = ljj;
-    __syncthreads();
-    if (ty > j && tx > j && tx <= ty && ty < nb) a[ty][tx] -= a[ty][j] * a[tx][j];
-    __syncthreads();
   }
-  if (tx < nb && ty < nb && tx <= ty) W[(k0 + ty) + n * (k0 + tx)] = a[ty][tx];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = tx + 16 * p, c = ty + 16 * q;
+      if (r < nb && c <= r) W[(k0 + r) + n * (k0 + c)] = a[p][q];
+    }
 }
 
-// The tiles below the diagonal tile: rows [k0 + nb, n) of columns [k0, k0 + nb) solved against L_kk' (X L_kk' = A),
-// one warp per 32 rows, a lane per row, columns in order
-__global__ void __launch_bounds__(DNB) k_trsm_panel(int64_t n, double* __restrict__ W, int64_t k0, int nb, const long long* __restrict__ status) {
-  __shared__ double L[DNB][DNB + 1];
-  __shared__ double x[DNB][DNB + 1];
+// The panel below the diagonal tile: rows [k0 + NB, n) of columns [k0, k0 + NB) solved against L_kk' (X L_kk' = A),
+// a thread per row holding its 64 entries in registers, L_kk transposed in shared memory (read as broadcasts).
+__global__ void __launch_bounds__(NB) k_trsm_panel(int64_t n, double* __restrict__ W, const double* __restrict__ dinv_g,
+                                                  int64_t k0, const long long* __restrict__ status) {
+  __shared__ __align__(16) double LT[NB][NB];   // LT[c][r] = L[r][c]
+  __shared__ double dinv[NB];
   if (status[0] >= 0) return;
-  const int lane = threadIdx.x;
-  for (int c = 0; c < nb; ++c)
-    if (lane < nb) L[lane][c] = W[(k0 + lane) + n * (k0 + c)];
-  const int64_t r = k0 + nb + (int64_t)blockIdx.x * DNB + lane;
-  __syncwarp();
-  if (r < n) {
-    for (int c = 0; c < nb; ++c) {
-      double v = W[r + n * (k0 + c)];
-      for (int cp = 0; cp < c; ++cp) v -= x[lane][cp] * L[c][cp];
-      x[lane][c] = v / L[c][c];
-    }
-    for (int c = 0; c < nb; ++c) W[r + n * (k0 + c)] = x[lane][c];
+  const int t = threadIdx.x;
+  for (int c = 0; c < NB; ++c) LT[c][t] = W[(k0 + t) + n * (k0 + c)];
+  dinv[t] = dinv_g[k0 + t];
+  __syncthreads();
+  const int64_t r = k0 + NB + (int64_t)blockIdx.x * NB + t;
+  if (r >= n) return;
+  double x[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) x[c] = W[r + n * (k0 + c)];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) {
+    x[c] *= dinv[c];
+#pragma unroll
+    for (int c2 = c + 1; c2 < NB; ++c2) x[c2] -= x[c] * LT[c][c2];
   }
+#pragma unroll
+  for (int c = 0; c < NB; ++c) W[r + n * (k0 + c)] = x[c];
 }
 
-// The trailing lower triangle: W[i, j] -= sum_c L[i, c] L[j, c] over the panel's columns c, for i >= j >= k0 + nb.
-// One CTA of 32 x 32 threads per 32 x 32 output tile of the lower triangle (tiles listed by their index in it).
-__global__ void __launch_bounds__(DNB * DNB) k_syrk_tiles(int64_t n, double* __restrict__ W, int64_t k0, int nb, int64_t nt,
-                                                          const long long* __restrict__ status) {
-  __shared__ double Pi[DNB][DNB + 1], Pj[DNB][DNB + 1];
+// The trailing lower triangle: W[i, j] -= sum_c L[i, c] L[j, c] over the panel's 64 columns, for i >= j >= k0 + NB,
+// in two launches: `rest` == 0 the first tile column (the next panel), `rest` == 1 the tile columns after it.
+// One CTA of 256 threads per 64 x 64 output tile of the lower triangle (tiles listed by their index in it); the two
+// row panels pass through shared memory 32 columns at a time and each thread accumulates a 4 x 4 block (rows
+// 2 tx + {0, 1, 32, 33}, columns 2 ty + {0, 1, 32, 33}) from 16-byte shared loads.
+__global__ void __launch_bounds__(256) k_syrk_tiles(int64_t n, double* __restrict__ W, int64_t k0, int rest,
+                                                    const long long* __restrict__ status) {
+  constexpr int KC = 32;
+  __shared__ __align__(16) double Pi[KC][NB], Pj[KC][NB];
   if (status[0] >= 0) return;
-  // tile (ti, tj), tj <= ti, of the trailing triangle of nt tiles
   const int64_t t = blockIdx.x;
-  int64_t ti = (int64_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-  while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
-  while (ti * (ti + 1) / 2 > t) --ti;
-  const int64_t tj = t - ti * (ti + 1) / 2;
-  const int64_t base = k0 + nb;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int64_t i = base + ti * DNB + ty, j = base + tj * DNB + ty;
-  Pi[ty][tx] = (i < n && tx < nb) ? W[i + n * (k0 + tx)] : 0.0;
-  Pj[ty][tx] = (j < n && tx < nb) ? W[j + n * (k0 + tx)] : 0.0;
-  __syncthreads();
-  const int64_t oi = base + ti * DNB + ty, oj = base + tj * DNB + tx;
-  if (oi < n && oj < n && oj <= oi) {
-    double s = 0.0;
-    for (int c = 0; c < nb; ++c) s += Pi[ty][c] * Pj[tx][c];
-    W[oi + n * oj] -= s;
+  int64_t ti = t, tj = 0;
+  if (rest) {
+    ti = (int64_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+    while (ti * (ti + 1) / 2 > t) --ti;
+    tj = t - ti * (ti + 1) / 2 + 1;
+    ti += 1;
   }
-  (void)nt;
+  const int64_t bi = k0 + NB + ti * NB, bj = k0 + NB + tj * NB;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[p][q] = 0.0;
+  for (int kc = 0; kc < NB; kc += KC) {
+#pragma unroll
+    for (int e = tid; e < KC * NB; e += 256) {
+      const int c = e >> 6, r = e & 63;
+      const int64_t col = n * (k0 + kc + c);
+      Pi[c][r] = bi + r < n ? W[bi + r + col] : 0.0;
+      Pj[c][r] = bj + r < n ? W[bj + r + col] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int c = 0; c < KC; ++c) {
+      const double2 a0 = *reinterpret_cast<const double2*>(&Pi[c][2 * tx]);
+      const double2 a1 = *reinterpret_cast<const double2*>(&Pi[c][32 + 2 * tx]);
+      const double2 b0 = *reinterpret_cast<const double2*>(&Pj[c][2 * ty]);
+      const double2 b1 = *reinterpret_cast<const double2*>(&Pj[c][32 + 2 * ty]);
+      const double ra[4] = {a0.x, a0.y, a1.x, a1.y}, rb[4] = {b0.x, b0.y, b1.x, b1.y};
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = fma(ra[p], rb[q], acc[p][q]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t oi = bi + 2 * tx + (p & 1) + 32 * (p >> 1), oj = bj + 2 * ty + (q & 1) + 32 * (q >> 1);
+      if (oi < n && oj <= oi) W[oi + n * oj] -= acc[p][q];
+    }
 }
 
-// x = (L L')^-1 g in one CTA, by 32-column tiles: each diagonal tile is solved by one warp (a lane per row, the pivot
-// broadcast by shuffle), then every thread updates the rows the tile feeds (forward: the rows below, reading the
-// tile's columns of L down a column; backward: the rows above, reading each row's 32 contiguous entries of the tile's
-// rows of L). The right-hand side lives in shared memory.
-__global__ void __launch_bounds__(1024) k_chol_solve(int64_t n, const double* __restrict__ W, const double* __restrict__ g,
-                                                     double* __restrict__ x) {
-  extern __shared__ double y[];
-  __shared__ double t[DNB][DNB + 1];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int64_t i = tid; i < n; i += blockDim.x) y[i] = g[i];
+// The forward substitution of one diagonal tile [d0, d0 + dnb) held in t (lower triangle), y in place, by one warp:
+// lanes own rows lane and lane + 32; per column the owner's value times 1 / L[c, c] is broadcast by shuffle.
+__device__ __forceinline__ void tile_forward(const double (*t)[NB + 1], const double* dv, double* y, int64_t d0, int dnb,
+                                             int lane) {
+  double y0 = lane < dnb ? y[d0 + lane] : 0.0, y1 = lane + 32 < dnb ? y[d0 + 32 + lane] : 0.0;
+  for (int c = 0; c < dnb; ++c) {
+    const double v = __shfl_sync(0xffffffffu, (c < 32 ? y0 : y1) * dv[c], c & 31);
+    if (c < 32) {
+      if (lane == c) y0 = v;
+      else if (lane > c) y0 -= t[lane][c] * v;
+    } else if (lane == c - 32) {
+      y1 = v;
+    }
+    if (lane + 32 > c && lane + 32 < dnb) y1 -= t[lane + 32][c] * v;
+  }
+  if (lane < dnb) y[d0 + lane] = y0;
+  if (lane + 32 < dnb) y[d0 + 32 + lane] = y1;
+}
+
+// The backward substitution (L' x = y) of one diagonal tile [d0, d0 + dnb), as tile_forward.
+__device__ __forceinline__ void tile_backward(const double (*t)[NB + 1], const double* dv, double* y, int64_t d0, int dnb,
+                                              int lane) {
+  double y0 = lane < dnb ? y[d0 + lane] : 0.0, y1 = lane + 32 < dnb ? y[d0 + 32 + lane] : 0.0;
+  for (int c = dnb - 1; c >= 0; --c) {
+    const double v = __shfl_sync(0xffffffffu, (c < 32 ? y0 : y1) * dv[c], c & 31);
+    if (c >= 32) {
+      if (lane == c - 32) y1 = v;
+      else if (lane < c - 32) y1 -= t[c][lane + 32] * v;
+      y0 -= t[c][lane] * v;
+    } else {
+      if (lane == c) y0 = v;
+      else if (lane < c) y0 -= t[c][lane] * v;
+    }
+  }
+  if (lane < dnb) y[d0 + lane] = y0;
+  if (lane + 32 < dnb) y[d0 + 32 + lane] = y1;
+}
+
+// One forward step of L y = g, y in place: rows [d0, n) take the update from the solved tile [d0 - NB, d0) (when
+// `update`), CTA b the 64 rows from d0 + 64 b, four threads per row over 16 columns each; then CTA 0, whose rows are
+// the next diagonal tile [d0, d0 + dnb), solves it (its tile of L is loaded before the update, to overlap the two).
+__global__ void __launch_bounds__(256) k_fwd_step(int64_t n, const double* __restrict__ W, const double* __restrict__ dinv,
+                                                  double* __restrict__ y, int64_t d0, int dnb, int update) {
+  __shared__ double t[NB][NB + 1];
+  __shared__ double dv[NB];
+  __shared__ double yk[NB];
+  __shared__ double part[4][NB];
+  const int tid = threadIdx.x, r = tid & 63, q = tid >> 6;
+  if (blockIdx.x == 0) {
+    for (int e = tid; e < NB * NB; e += 256) {
+      const int rr = e & 63, cc = e >> 6;
+      if (rr < dnb && cc <= rr) t[rr][cc] = W[(d0 + rr) + n * (d0 + cc)];
+    }
+    if (tid < dnb) dv[tid] = dinv[d0 + tid];
+  }
+  if (update) {
+    const int64_t k0 = d0 - NB, i = d0 + (int64_t)blockIdx.x * NB + r;
+    if (tid < NB) yk[tid] = y[k0 + tid];
+    __syncthreads();
+    double s = 0.0;
+    if (i < n) {
+#pragma unroll
+      for (int c = 16 * q; c < 16 * q + 16; ++c) s = fma(W[i + n * (k0 + c)], yk[c], s);
+    }
+    part[q][r] = s;
+    __syncthreads();
+    if (tid < NB && i < n) y[i] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+  }
+  if (blockIdx.x != 0) return;
   __syncthreads();
-  // forward: L y = g
-  for (int64_t k0 = 0; k0 < n; k0 += DNB) {
-    const int nb = (int)(n - k0 < DNB ? n - k0 : DNB);
-    for (int q = tid; q < nb * nb; q += blockDim.x) t[q % nb][q / nb] = W[(k0 + q % nb) + n * (k0 + q / nb)];
-    __syncthreads();
-    if (warp == 0) {
-      double yr = lane < nb ? y[k0 + lane] : 0.0;
-      for (int c = 0; c < nb; ++c) {
-        const double yc = __shfl_sync(0xffffffffu, yr, c) / t[c][c];
-        if (lane == c) yr = yc;
-        else if (lane > c && lane < nb) yr -= t[lane][c] * yc;
-      }
-      if (lane < nb) y[k0 + lane] = yr;
+  if (tid < 32) tile_forward(t, dv, y, d0, dnb, tid);
+}
+
+// One backward step of L' x = y, in place: rows [0, k0) take the update from the solved tile [k0, k0 + unb), CTA b
+// the 64 rows below k0 - 64 b, a warp per row reading that row's entries of the tile's rows of L (64 contiguous
+// values of one column of W); then CTA 0, whose rows are the tile [k0 - NB, k0), solves it.
+__global__ void __launch_bounds__(256) k_bwd_step(int64_t n, const double* __restrict__ W, const double* __restrict__ dinv,
+                                                  double* __restrict__ y, int64_t k0, int unb) {
+  __shared__ double t[NB][NB + 1];
+  __shared__ double dv[NB];
+  __shared__ double xk[NB];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t row0 = k0 - NB * (int64_t)(blockIdx.x + 1);   // this CTA's rows [row0, row0 + 64)
+  if (blockIdx.x == 0) {
+    for (int e = tid; e < NB * NB; e += 256) {
+      const int rr = e & 63, cc = e >> 6;
+      if (cc <= rr) t[rr][cc] = W[(row0 + rr) + n * (row0 + cc)];
     }
-    __syncthreads();
-    for (int64_t i = k0 + nb + tid; i < n; i += blockDim.x) {
-      double s = 0.0;
-      for (int c = 0; c < nb; ++c) s += W[i + n * (k0 + c)] * y[k0 + c];
-      y[i] -= s;
-    }
-    __syncthreads();
+    if (tid < NB) dv[tid] = dinv[row0 + tid];
   }
-  // backward: L' x = y
-  for (int64_t k0 = ((n - 1) / DNB) * DNB; k0 >= 0; k0 -= DNB) {
-    const int nb = (int)(n - k0 < DNB ? n - k0 : DNB);
-    for (int q = tid; q < nb * nb; q += blockDim.x) t[q % nb][q / nb] = W[(k0 + q % nb) + n * (k0 + q / nb)];
-    __syncthreads();
-    if (warp == 0) {
-      double yr = lane < nb ? y[k0 + lane] : 0.0;
-      for (int c = nb - 1; c >= 0; --c) {
-        const double xc = __shfl_sync(0xffffffffu, yr, c) / t[c][c];
-        if (lane == c) yr = xc;
-        else if (lane < c) yr -= t[c][lane] * xc;
-      }
-      if (lane < nb) y[k0 + lane] = yr;
-    }
-    __syncthreads();
-    for (int64_t i = tid; i < k0; i += blockDim.x) {
-      double s = 0.0;
-      for (int c = 0; c < nb; ++c) s += W[(k0 + c) + n * i] * y[k0 + c];
-      y[i] -= s;
-    }
-    __syncthreads();
+  if (tid < NB) xk[tid] = tid < unb ? y[k0 + tid] : 0.0;
+  __syncthreads();
+  const double x0 = xk[lane], x1 = xk[lane + 32];
+  double s[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const double* colj = W + n * (row0 + warp * 8 + m) + k0;
+    s[m] = (lane < unb ? colj[lane] * x0 : 0.0) + (lane + 32 < unb ? colj[lane + 32] * x1 : 0.0);
   }
-  for (int64_t i = tid; i < n; i += blockDim.x) x[i] = y[i];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[m] += __shfl_xor_sync(0xffffffffu, s[m], o);
+  }
+  if (lane < 8) {
+    double v = s[0];
+#pragma unroll
+    for (int m = 1; m < 8; ++m)
+      if (lane == m) v = s[m];
+    y[row0 + warp * 8 + lane] -= v;
+  }
+  if (blockIdx.x != 0) return;
+  __syncthreads();
+  if (tid < 32) tile_backward(t, dv, y, row0, NB, tid);
+}
+
+// The last diagonal tile [d0, n) of the backward pass (the only one that may be short), solved by one warp.
+__global__ void __launch_bounds__(32) k_bwd_last(int64_t n, const double* __restrict__ W, const double* __restrict__ dinv,
+                                                 double* __restrict__ y, int64_t d0) {
+  __shared__ double t[NB][NB + 1];
+  __shared__ double dv[NB];
+  const int lane = threadIdx.x, dnb = (int)(n - d0);
+  for (int e = lane; e < NB * NB; e += 32) {
+    const int rr = e & 63, cc = e >> 6;
+    if (rr < dnb && cc <= rr) t[rr][cc] = W[(d0 + rr) + n * (d0 + cc)];
+  }
+  for (int c = lane; c < dnb; c += 32) dv[c] = dinv[d0 + c];
+  __syncwarp();
+  tile_backward(t, dv, y, d0, dnb, lane);
 }
 
 template <class T>
@@ -177,18 +330,39 @@ static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
   cudaStream_t s = D->ctx->stream;
   const int64_t n = D->n;
   double* W = D->W.as<double>();
+  double* dv = D->dinv.as<double>();
   long long* st = D->status.as<long long>();
-  k_dense_load<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n * n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, S, W, st);
-  for (int64_t k0 = 0; k0 < n; k0 += DNB) {
-    const int nb = (int)std::min<int64_t>(DNB, n - k0);
-    k_potrf_tile<<<1, dim3(DNB, DNB), 0, s>>>(n, W, k0, nb, st);
-    const int64_t rest = n - k0 - nb;
-    if (rest > 0) {
-      k_trsm_panel<<<(unsigned)((rest + DNB - 1) / DNB), DNB, 0, s>>>(n, W, k0, nb, st);
-      const int64_t nt = (rest + DNB - 1) / DNB;
-      k_syrk_tiles<<<(unsigned)(nt * (nt + 1) / 2), dim3(DNB, DNB), 0, s>>>(n, W, k0, nb, nt, st);
-    }
+  if (!D->panel_stream) {
+    int lo = 0, hi = 0;
+    BLS_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    BLS_CUDA(cudaStreamCreateWithPriority(&D->panel_stream, cudaStreamNonBlocking, hi));
+    BLS_CUDA(cudaEventCreateWithFlags(&D->ev_join, cudaEventDisableTiming));
+    BLS_CUDA(cudaEventCreateWithFlags(&D->ev_panel, cudaEventDisableTiming));
   }
+  cudaStream_t p = D->panel_stream;
+  k_dense_load<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n * n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, S, W, st);
+  BLS_CUDA(cudaEventRecord(D->ev_join, s));
+  BLS_CUDA(cudaStreamWaitEvent(p, D->ev_join, 0));
+  // panel k: its diagonal tile, then (when rows remain below it) its triangular solve, on the panel stream
+  auto panel = [&](int64_t k0) {
+    const int nb = (int)std::min<int64_t>(NB, n - k0);
+    k_potrf_tile<<<1, 256, 0, p>>>(n, W, dv, k0, nb, st);
+    if (n - k0 - nb > 0) k_trsm_panel<<<(unsigned)((n - k0 - nb + NB - 1) / NB), NB, 0, p>>>(n, W, dv, k0, st);
+    BLS_CUDA(cudaEventRecord(D->ev_panel, p));
+  };
+  panel(0);
+  // Lookahead by one panel: the trailing update of panel k updates the next panel's tile column first; the next panel
+  // is factored on the panel stream while the caller's stream updates the tile columns after it.
+  for (int64_t k0 = 0; n - k0 > NB; k0 += NB) {
+    const int64_t nt = (n - k0 - NB + NB - 1) / NB;
+    BLS_CUDA(cudaStreamWaitEvent(s, D->ev_panel, 0));
+    k_syrk_tiles<<<(unsigned)nt, 256, 0, s>>>(n, W, k0, 0, st);
+    BLS_CUDA(cudaEventRecord(D->ev_join, s));
+    BLS_CUDA(cudaStreamWaitEvent(p, D->ev_join, 0));
+    panel(k0 + NB);
+    if (nt > 1) k_syrk_tiles<<<(unsigned)((nt - 1) * nt / 2), 256, 0, s>>>(n, W, k0, 1, st);
+  }
+  BLS_CUDA(cudaStreamWaitEvent(s, D->ev_panel, 0));
   BLS_CUDA(cudaGetLastError());
   long long h = -1;
   BLS_CUDA(cudaMemcpyAsync(&h, st, sizeof(long long), cudaMemcpyDeviceToHost, s));
@@ -225,6 +399,7 @@ int bls_dense_solver_create(bls_ctx* ctx, int64_t n, bls_dense_solver** out) {
     D->ctx = ctx;
     D->n = n;
     D->W.alloc(sizeof(double) * (size_t)(n * n));
+    D->dinv.alloc(sizeof(double) * (size_t)n);
     D->status.alloc(sizeof(long long));
     *out = D.release();
     return BLS_OK;
@@ -249,11 +424,20 @@ int bls_dense_cholesky_solve(bls_dense_solver* D, const double* g, double* x) {
   DENSE_GUARD({
     if (!D || !g || !x) throw Error(BLS_EINVAL, "null argument");
     if (!D->factored) throw Error(BLS_EINVAL, "the solver holds no factorisation (bls_dense_cholesky first, and it must succeed)");
-    const size_t smem = sizeof(double) * (size_t)D->n;
-    // The static tile counts against the 48 KB default too, so opt in whenever the sum passes it.
-    const size_t tile = sizeof(double) * DNB * (DNB + 1);
-    if (smem + tile > 48 * 1024) BLS_CUDA(cudaFuncSetAttribute(k_chol_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_chol_solve<<<1, 1024, smem, D->ctx->stream>>>(D->n, D->W.as<double>(), g, x);
+    const int64_t n = D->n;
+    const double* W = D->W.as<double>();
+    const double* dv = D->dinv.as<double>();
+    cudaStream_t s = D->ctx->stream;
+    if (x != g) BLS_CUDA(cudaMemcpyAsync(x, g, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    // forward: tile [0, NB) first, then each step updates the rows below the tile it just solved and solves the next
+    k_fwd_step<<<1, 256, 0, s>>>(n, W, dv, x, 0, (int)std::min<int64_t>(NB, n), 0);
+    for (int64_t d0 = NB; d0 < n; d0 += NB)
+      k_fwd_step<<<(unsigned)((n - d0 + NB - 1) / NB), 256, 0, s>>>(n, W, dv, x, d0, (int)std::min<int64_t>(NB, n - d0), 1);
+    // backward: the last (possibly short) tile first, then upward
+    const int64_t kl = ((n - 1) / NB) * NB;
+    k_bwd_last<<<1, 32, 0, s>>>(n, W, dv, x, kl);
+    for (int64_t k0 = kl; k0 > 0; k0 -= NB)
+      k_bwd_step<<<(unsigned)(k0 / NB), 256, 0, s>>>(n, W, dv, x, k0, (int)std::min<int64_t>(NB, n - k0));
     BLS_CUDA(cudaGetLastError());
     return BLS_OK;
   })

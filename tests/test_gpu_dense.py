@@ -55,9 +55,8 @@ def test_dense_scene_solve(bls, dtype):
     assert relerr(D.solve(g2).cpu().numpy(), np.linalg.solve(A, g2.cpu().numpy())) <= 1e-10
 
 
-# 5200: the solve's right-hand side (41.6 KB) is under the 48 KB default shared-memory limit only without the static
-# tile; 6500: the right-hand side alone is over it.
-@pytest.mark.parametrize("n", [1, 7, 32, 33, 100, 517, 5200, 6500])
+# sizes on both sides of the 64-column panels and tiles, and two large systems (about 80 and 100 panels)
+@pytest.mark.parametrize("n", [1, 7, 32, 33, 63, 64, 65, 100, 127, 128, 129, 517, 5200, 6500])
 def test_random_spd_across_tiles(bls, n):
     rng = np.random.default_rng(n)
     B = rng.standard_normal((n, n))
