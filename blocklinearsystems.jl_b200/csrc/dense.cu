@@ -2,8 +2,8 @@
 // reduce_schur_dense! when S is small enough to hold dense (the reference hands its dense S to DampedLinearSolve's
 // Cholesky, src/schur_linear_systems.jl:312-320). S is read from its upper triangle in its storage type (FP64 or the
 // mixed form's FP32), mirrored into an FP64 working matrix owned by the solver, and factored in place as S = L L' by a
-// right-looking blocked Cholesky with 64-column panels: per panel, the diagonal tile in one CTA's registers, the rows
-// below it by a triangular solve, then the trailing lower triangle updated in 64 x 64 tiles. A pivot that is not
+// right-looking blocked Cholesky with 64-column panels: per panel, the diagonal tile in one CTA's shared memory, the
+// rows below it by a triangular solve, then the trailing lower triangle updated in 64 x 64 tiles. A pivot that is not
 // positive (or not finite) stops the factorisation; its column is reported, 1-based. The solve runs the two triangular
 // substitutions as one launch per 64-row tile: all CTAs apply the last solved tile to the rows it feeds, and CTA 0,
 // whose rows are the next diagonal tile, then solves that tile.
@@ -45,68 +45,102 @@ __global__ void k_dense_load(int64_t n, const T* __restrict__ S, double* __restr
   }
 }
 
-// The diagonal tile [k0, k0 + nb) in one CTA of 256 threads, right-looking and unblocked: thread (tx, ty) keeps the
-// entries of rows tx + 16 p and columns ty + 16 q in registers; per column the owners publish it to shared memory
-// (double-buffered, one barrier per column) and every thread scales and updates its own entries. A non-positive or
-// non-finite pivot records its column and leaves W as it is. 1 / L[j, j] goes to dinv.
-__global__ void __launch_bounds__(256) k_potrf_tile(int64_t n, double* __restrict__ W, double* __restrict__ dinv, int64_t k0,
-                                                    int nb, long long* __restrict__ status) {
-  __shared__ double col[2][NB];
-  if (status[0] >= 0) return;   // uniform across the CTA
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double a[4][4];
+// The lower triangle of the diagonal tile [d0, d0 + dnb) of L into t by 256 threads, all 16 loads of a thread in flight
+// (zeros elsewhere)
+__device__ __forceinline__ void load_tile(double (*t)[NB + 1], const double* __restrict__ W, int64_t n, int64_t d0, int dnb,
+                                          int tid) {
+  double v[NB * NB / 256];
 #pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int r = tx + 16 * p, c = ty + 16 * q;
-      a[p][q] = (r < nb && c <= r) ? W[(k0 + r) + n * (k0 + c)] : 0.0;
-    }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    for (int jj = 0; jj < 16; ++jj) {
-      const int j = 16 * q + jj;
-      if (j >= nb) break;   // uniform
-      const int b = j & 1;
-      if (ty == jj) {
-#pragma unroll
-        for (int p = 0; p < 4; ++p) col[b][tx + 16 * p] = a[p][q];
-      }
-      __syncthreads();
-      const double d = col[b][j];
-      if (!(d > 0.0) || !isfinite(d)) {   // every thread reads the same d: the whole CTA returns here
-        if (threadIdx.x == 0) status[0] = k0 + j;
-        return;
-      }
-      const double ljj = sqrt(d), inv = rsqrt(d);   // independent, so the column's chain waits on one of them
-      if (threadIdx.x == 0) dinv[k0 + j] = inv;
-      double li[4], lc[4];
-#pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        li[p] = col[b][tx + 16 * p] * inv;
-        lc[p] = col[b][ty + 16 * p] * inv;
-      }
-#pragma unroll
-      for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q2 = 0; q2 < 4; ++q2) {
-          const int r = tx + 16 * p, c = ty + 16 * q2;
-          if (c == j) {
-            if (r == j) a[p][q2] = ljj;
-            else if (r > j) a[p][q2] = li[p];
-          } else if (c > j && r >= c) {
-            a[p][q2] -= li[p] * lc[q2];
-          }
-        }
-    }
+  for (int k = 0; k < NB * NB / 256; ++k) {
+    const int e = tid + 256 * k, rr = e & 63, cc = e >> 6;
+    v[k] = (rr < dnb && cc <= rr) ? W[(d0 + rr) + n * (d0 + cc)] : 0.0;
   }
 #pragma unroll
-  for (int p = 0; p < 4; ++p)
+  for (int k = 0; k < NB * NB / 256; ++k) {
+    const int e = tid + 256 * k;
+    t[e & 63][e >> 6] = v[k];
+  }
+}
+
+// The diagonal tile [k0, k0 + nb) in one CTA of 256 threads, held in shared memory and factored by 16-column
+// sub-panels. Warp 0 factors a sub-panel's rows (lane i holds rows c0 + i and c0 + 32 + i of its 16 columns in
+// registers) with no barrier: per column the pivot comes from its lane by shuffle, L[j, j] = pivot * rsqrt(pivot), and
+// each later column's entry of L is shuffled from its lane to update the rows below. Then all threads subtract the
+// sub-panel's rank-16 product from the rest of the tile. A non-positive or non-finite pivot records its column and
+// stops (W is not written). 1 / L[j, j] goes to dinv.
+__global__ void __launch_bounds__(256, 1) k_potrf_tile(int64_t n, double* __restrict__ W, double* __restrict__ dinv, int64_t k0,
+                                                    int nb, long long* __restrict__ status) {
+  __shared__ double T[NB][NB + 1];
+  __shared__ int failed;
+  if (status[0] >= 0) return;   // uniform across the CTA
+  const int tid = threadIdx.x, lane = tid & 31;
+  load_tile(T, W, n, k0, nb, tid);
+  if (tid == 0) failed = -1;
+  __syncthreads();
+  for (int c0 = 0; c0 < nb; c0 += 16) {
+    const int w = nb - c0 < 16 ? nb - c0 : 16;
+    if (tid < 32) {
+      const int r0 = c0 + lane, r1 = c0 + 32 + lane;
+      double a0[16], a1[16];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int r = tx + 16 * p, c = ty + 16 * q;
-      if (r < nb && c <= r) W[(k0 + r) + n * (k0 + c)] = a[p][q];
+      for (int k = 0; k < 16; ++k) {
+        a0[k] = r0 < NB ? T[r0][c0 + k] : 0.0;
+        a1[k] = r1 < NB ? T[r1][c0 + k] : 0.0;
+      }
+      int bad = -1;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        if (j < w && bad < 0) {   // uniform (no break, so the loop unrolls and a0, a1 stay in registers)
+          const double d = __shfl_sync(0xffffffffu, a0[j], j);
+          if (!(d > 0.0) || !isfinite(d)) {   // uniform
+            bad = c0 + j;
+          } else {
+            const double inv = rsqrt(d);
+            const double l0 = (lane == j ? d : a0[j]) * inv, l1 = a1[j] * inv;
+            if (lane >= j) a0[j] = l0;
+            a1[j] = l1;
+            if (lane == j) dinv[k0 + c0 + j] = inv;
+#pragma unroll
+            for (int k = j + 1; k < 16; ++k) {
+              const double lk = __shfl_sync(0xffffffffu, l0, k);
+              if (lane >= k) a0[k] -= l0 * lk;
+              a1[k] -= l1 * lk;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (r0 < NB && k <= lane) T[r0][c0 + k] = a0[k];
+        if (r1 < NB) T[r1][c0 + k] = a1[k];
+      }
+      if (lane == 0) failed = bad;
     }
+    __syncthreads();
+    if (failed >= 0) {   // uniform
+      if (tid == 0) status[0] = k0 + failed;
+      return;
+    }
+    // the rest of the tile's lower triangle: T[i, k] -= sum over the sub-panel's columns of L[i, c] L[k, c]
+    const int base = c0 + 16, m = nb > base ? nb - base : 0;
+    for (int e = tid; e < m * m; e += 256) {
+      const int i = base + e / m, k = base + e % m;
+      if (k > i) continue;
+      double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 16; c += 2) {
+        s0 = fma(T[i][c0 + c], T[k][c0 + c], s0);
+        s1 = fma(T[i][c0 + c + 1], T[k][c0 + c + 1], s1);
+      }
+      T[i][k] -= s0 + s1;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < NB * NB / 256; ++k) {
+    const int e = tid + 256 * k, rr = e & 63, cc = e >> 6;
+    if (rr < nb && cc <= rr) W[(k0 + rr) + n * (k0 + cc)] = T[rr][cc];
+  }
 }
 
 // The panel below the diagonal tile: rows [k0 + NB, n) of columns [k0, k0 + NB) solved against L_kk' (X L_kk' = A),
@@ -117,14 +151,22 @@ __global__ void __launch_bounds__(NB) k_trsm_panel(int64_t n, double* __restrict
   __shared__ double dinv[NB];
   if (status[0] >= 0) return;
   const int t = threadIdx.x;
-  for (int c = 0; c < NB; ++c) LT[c][t] = W[(k0 + t) + n * (k0 + c)];
-  dinv[t] = dinv_g[k0 + t];
-  __syncthreads();
   const int64_t r = k0 + NB + (int64_t)blockIdx.x * NB + t;
-  if (r >= n) return;
+  // the row's 64 entries and the tile (16 columns at a time) are loaded with every load of a batch in flight
   double x[NB];
 #pragma unroll
-  for (int c = 0; c < NB; ++c) x[c] = W[r + n * (k0 + c)];
+  for (int c = 0; c < NB; ++c) x[c] = r < n ? W[r + n * (k0 + c)] : 0.0;
+#pragma unroll
+  for (int c0 = 0; c0 < NB; c0 += 16) {
+    double v[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) v[c] = W[(k0 + t) + n * (k0 + c0 + c)];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) LT[c0 + c][t] = v[c];
+  }
+  dinv[t] = dinv_g[k0 + t];
+  __syncthreads();
+  if (r >= n) return;
 #pragma unroll
   for (int c = 0; c < NB; ++c) {
     x[c] *= dinv[c];
@@ -139,7 +181,8 @@ __global__ void __launch_bounds__(NB) k_trsm_panel(int64_t n, double* __restrict
 // in two launches: `rest` == 0 the first tile column (the next panel), `rest` == 1 the tile columns after it.
 // One CTA of 256 threads per 64 x 64 output tile of the lower triangle (tiles listed by their index in it); the two
 // row panels pass through shared memory 32 columns at a time and each thread accumulates a 4 x 4 block (rows
-// 2 tx + {0, 1, 32, 33}, columns 2 ty + {0, 1, 32, 33}) from 16-byte shared loads.
+// 2 tx + {0, 1, 32, 33}, columns 2 ty + {0, 1, 32, 33}) from 16-byte shared loads with FP64 fused multiply-adds (the
+// FP64 tensor-core form, mma.sync m8n8k4 fragments per warp, measured 1.3x slower here).
 __global__ void __launch_bounds__(256) k_syrk_tiles(int64_t n, double* __restrict__ W, int64_t k0, int rest,
                                                     const long long* __restrict__ status) {
   constexpr int KC = 32;
@@ -162,12 +205,19 @@ __global__ void __launch_bounds__(256) k_syrk_tiles(int64_t n, double* __restric
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[p][q] = 0.0;
   for (int kc = 0; kc < NB; kc += KC) {
+    double vi[KC * NB / 256], vj[KC * NB / 256];
 #pragma unroll
-    for (int e = tid; e < KC * NB; e += 256) {
-      const int c = e >> 6, r = e & 63;
+    for (int k = 0; k < KC * NB / 256; ++k) {
+      const int e = tid + 256 * k, c = e >> 6, r = e & 63;
       const int64_t col = n * (k0 + kc + c);
-      Pi[c][r] = bi + r < n ? W[bi + r + col] : 0.0;
-      Pj[c][r] = bj + r < n ? W[bj + r + col] : 0.0;
+      vi[k] = bi + r < n ? W[bi + r + col] : 0.0;
+      vj[k] = bj + r < n ? W[bj + r + col] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < KC * NB / 256; ++k) {
+      const int e = tid + 256 * k;
+      Pi[e >> 6][e & 63] = vi[k];
+      Pj[e >> 6][e & 63] = vj[k];
     }
     __syncthreads();
 #pragma unroll 8
@@ -193,13 +243,15 @@ __global__ void __launch_bounds__(256) k_syrk_tiles(int64_t n, double* __restric
     }
 }
 
-// The forward substitution of one diagonal tile [d0, d0 + dnb) held in t (lower triangle), y in place, by one warp:
-// lanes own rows lane and lane + 32; per column the owner's value times 1 / L[c, c] is broadcast by shuffle.
-__device__ __forceinline__ void tile_forward(const double (*t)[NB + 1], const double* dv, double* y, int64_t d0, int dnb,
-                                             int lane) {
-  double y0 = lane < dnb ? y[d0 + lane] : 0.0, y1 = lane + 32 < dnb ? y[d0 + 32 + lane] : 0.0;
+// The forward substitution of one diagonal tile [d0, d0 + dnb) of L held in t (lower triangle) by one warp: lanes own
+// rows lane and lane + 32, start from ys (shared) and write y; per column the owner's value times 1 / L[c, c] (held in
+// registers, dlo / dhi) is broadcast by shuffle, so the column chain is a multiply, a shuffle and a fused multiply-add.
+__device__ __forceinline__ void tile_forward(const double (*t)[NB + 1], double dlo, double dhi, const double* ys,
+                                             double* __restrict__ y, int64_t d0, int dnb, int lane) {
+  double y0 = ys[lane], y1 = ys[lane + 32];
+#pragma unroll 2
   for (int c = 0; c < dnb; ++c) {
-    const double v = __shfl_sync(0xffffffffu, (c < 32 ? y0 : y1) * dv[c], c & 31);
+    const double v = __shfl_sync(0xffffffffu, c < 32 ? y0 * dlo : y1 * dhi, c & 31);
     if (c < 32) {
       if (lane == c) y0 = v;
       else if (lane > c) y0 -= t[lane][c] * v;
@@ -213,11 +265,12 @@ __device__ __forceinline__ void tile_forward(const double (*t)[NB + 1], const do
 }
 
 // The backward substitution (L' x = y) of one diagonal tile [d0, d0 + dnb), as tile_forward.
-__device__ __forceinline__ void tile_backward(const double (*t)[NB + 1], const double* dv, double* y, int64_t d0, int dnb,
-                                              int lane) {
-  double y0 = lane < dnb ? y[d0 + lane] : 0.0, y1 = lane + 32 < dnb ? y[d0 + 32 + lane] : 0.0;
+__device__ __forceinline__ void tile_backward(const double (*t)[NB + 1], double dlo, double dhi, const double* ys,
+                                              double* __restrict__ y, int64_t d0, int dnb, int lane) {
+  double y0 = ys[lane], y1 = ys[lane + 32];
+#pragma unroll 2
   for (int c = dnb - 1; c >= 0; --c) {
-    const double v = __shfl_sync(0xffffffffu, (c < 32 ? y0 : y1) * dv[c], c & 31);
+    const double v = __shfl_sync(0xffffffffu, c < 32 ? y0 * dlo : y1 * dhi, c & 31);
     if (c >= 32) {
       if (lane == c - 32) y1 = v;
       else if (lane < c - 32) y1 -= t[c][lane + 32] * v;
@@ -233,95 +286,119 @@ __device__ __forceinline__ void tile_backward(const double (*t)[NB + 1], const d
 
 // One forward step of L y = g, y in place: rows [d0, n) take the update from the solved tile [d0 - NB, d0) (when
 // `update`), CTA b the 64 rows from d0 + 64 b, four threads per row over 16 columns each; then CTA 0, whose rows are
-// the next diagonal tile [d0, d0 + dnb), solves it (its tile of L is loaded before the update, to overlap the two).
+// the next diagonal tile [d0, d0 + dnb), solves it. Every global load of the step is issued before the first barrier,
+// and CTA 0 keeps its updated rows in shared memory, so the step costs one round trip to memory plus the tile's chain.
 __global__ void __launch_bounds__(256) k_fwd_step(int64_t n, const double* __restrict__ W, const double* __restrict__ dinv,
                                                   double* __restrict__ y, int64_t d0, int dnb, int update) {
   __shared__ double t[NB][NB + 1];
-  __shared__ double dv[NB];
   __shared__ double yk[NB];
   __shared__ double part[4][NB];
+  __shared__ double ys[NB];
   const int tid = threadIdx.x, r = tid & 63, q = tid >> 6;
-  if (blockIdx.x == 0) {
-    for (int e = tid; e < NB * NB; e += 256) {
-      const int rr = e & 63, cc = e >> 6;
-      if (rr < dnb && cc <= rr) t[rr][cc] = W[(d0 + rr) + n * (d0 + cc)];
-    }
-    if (tid < dnb) dv[tid] = dinv[d0 + tid];
-  }
+  const int64_t i = d0 + (int64_t)blockIdx.x * NB + r, k0 = d0 - NB;
+  double w[16];
+  double yi = 0.0, dlo = 0.0, dhi = 0.0;
   if (update) {
-    const int64_t k0 = d0 - NB, i = d0 + (int64_t)blockIdx.x * NB + r;
+    if (i < n) {
+#pragma unroll
+      for (int c = 0; c < 16; ++c) w[c] = W[i + n * (k0 + 16 * q + c)];
+    }
     if (tid < NB) yk[tid] = y[k0 + tid];
-    __syncthreads();
+  }
+  if (q == 0 && i < n) yi = y[i];
+  if (blockIdx.x == 0) {
+    load_tile(t, W, n, d0, dnb, tid);
+    if (tid < 32) {
+      if (tid < dnb) dlo = dinv[d0 + tid];
+      if (tid + 32 < dnb) dhi = dinv[d0 + 32 + tid];
+    }
+  }
+  __syncthreads();
+  if (update) {
     double s = 0.0;
     if (i < n) {
 #pragma unroll
-      for (int c = 16 * q; c < 16 * q + 16; ++c) s = fma(W[i + n * (k0 + c)], yk[c], s);
+      for (int c = 0; c < 16; ++c) s = fma(w[c], yk[16 * q + c], s);
     }
     part[q][r] = s;
     __syncthreads();
-    if (tid < NB && i < n) y[i] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+    if (q == 0) yi -= (part[0][r] + part[1][r]) + (part[2][r] + part[3][r]);
   }
-  if (blockIdx.x != 0) return;
+  if (blockIdx.x != 0) {
+    if (update && q == 0 && i < n) y[i] = yi;
+    return;
+  }
+  if (q == 0) ys[r] = yi;
   __syncthreads();
-  if (tid < 32) tile_forward(t, dv, y, d0, dnb, tid);
+  if (tid < 32) tile_forward(t, dlo, dhi, ys, y, d0, dnb, tid);
 }
 
 // One backward step of L' x = y, in place: rows [0, k0) take the update from the solved tile [k0, k0 + unb), CTA b
 // the 64 rows below k0 - 64 b, a warp per row reading that row's entries of the tile's rows of L (64 contiguous
-// values of one column of W); then CTA 0, whose rows are the tile [k0 - NB, k0), solves it.
+// values of one column of W); then CTA 0, whose rows are the tile [k0 - NB, k0), solves it. Loads are issued before
+// the first barrier and CTA 0's rows stay in shared memory, as in the forward step.
 __global__ void __launch_bounds__(256) k_bwd_step(int64_t n, const double* __restrict__ W, const double* __restrict__ dinv,
                                                   double* __restrict__ y, int64_t k0, int unb) {
   __shared__ double t[NB][NB + 1];
-  __shared__ double dv[NB];
   __shared__ double xk[NB];
+  __shared__ double ys[NB];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t row0 = k0 - NB * (int64_t)(blockIdx.x + 1);   // this CTA's rows [row0, row0 + 64)
-  if (blockIdx.x == 0) {
-    for (int e = tid; e < NB * NB; e += 256) {
-      const int rr = e & 63, cc = e >> 6;
-      if (cc <= rr) t[rr][cc] = W[(row0 + rr) + n * (row0 + cc)];
-    }
-    if (tid < NB) dv[tid] = dinv[row0 + tid];
+  double w0[8], w1[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const double* colj = W + n * (row0 + warp * 8 + m) + k0;
+    w0[m] = lane < unb ? colj[lane] : 0.0;
+    w1[m] = lane + 32 < unb ? colj[lane + 32] : 0.0;
   }
   if (tid < NB) xk[tid] = tid < unb ? y[k0 + tid] : 0.0;
+  const double yold = lane < 8 ? y[row0 + warp * 8 + lane] : 0.0;
+  double dlo = 0.0, dhi = 0.0;
+  if (blockIdx.x == 0) {
+    load_tile(t, W, n, row0, NB, tid);
+    if (tid < 32) {
+      dlo = dinv[row0 + tid];
+      dhi = dinv[row0 + 32 + tid];
+    }
+  }
   __syncthreads();
   const double x0 = xk[lane], x1 = xk[lane + 32];
   double s[8];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const double* colj = W + n * (row0 + warp * 8 + m) + k0;
-    s[m] = (lane < unb ? colj[lane] * x0 : 0.0) + (lane + 32 < unb ? colj[lane + 32] * x1 : 0.0);
-  }
+  for (int m = 0; m < 8; ++m) s[m] = w0[m] * x0 + w1[m] * x1;
 #pragma unroll
   for (int m = 0; m < 8; ++m) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s[m] += __shfl_xor_sync(0xffffffffu, s[m], o);
   }
-  if (lane < 8) {
-    double v = s[0];
+  double v = s[0];
 #pragma unroll
-    for (int m = 1; m < 8; ++m)
-      if (lane == m) v = s[m];
-    y[row0 + warp * 8 + lane] -= v;
+  for (int m = 1; m < 8; ++m)
+    if (lane == m) v = s[m];
+  if (blockIdx.x != 0) {
+    if (lane < 8) y[row0 + warp * 8 + lane] = yold - v;
+    return;
   }
-  if (blockIdx.x != 0) return;
+  if (lane < 8) ys[warp * 8 + lane] = yold - v;
   __syncthreads();
-  if (tid < 32) tile_backward(t, dv, y, row0, NB, tid);
+  if (tid < 32) tile_backward(t, dlo, dhi, ys, y, row0, NB, tid);
 }
 
 // The last diagonal tile [d0, n) of the backward pass (the only one that may be short), solved by one warp.
 __global__ void __launch_bounds__(32) k_bwd_last(int64_t n, const double* __restrict__ W, const double* __restrict__ dinv,
                                                  double* __restrict__ y, int64_t d0) {
   __shared__ double t[NB][NB + 1];
-  __shared__ double dv[NB];
+  __shared__ double ys[NB];
   const int lane = threadIdx.x, dnb = (int)(n - d0);
   for (int e = lane; e < NB * NB; e += 32) {
     const int rr = e & 63, cc = e >> 6;
     if (rr < dnb && cc <= rr) t[rr][cc] = W[(d0 + rr) + n * (d0 + cc)];
   }
-  for (int c = lane; c < dnb; c += 32) dv[c] = dinv[d0 + c];
+  ys[lane] = lane < dnb ? y[d0 + lane] : 0.0;
+  ys[lane + 32] = lane + 32 < dnb ? y[d0 + 32 + lane] : 0.0;
+  const double dlo = lane < dnb ? dinv[d0 + lane] : 0.0, dhi = lane + 32 < dnb ? dinv[d0 + 32 + lane] : 0.0;
   __syncwarp();
-  tile_backward(t, dv, y, d0, dnb, lane);
+  tile_backward(t, dlo, dhi, ys, y, d0, dnb, lane);
 }
 
 template <class T>
