@@ -498,6 +498,162 @@ def run_ours_pcg(args, rank: int, world: int) -> dict | None:
     return out
 
 
+def dense_launches(n: int) -> tuple[int, int]:
+    """Kernels one dense factorisation and one solve launch for an n x n system (64-column panels)."""
+    panels = (n + 63) // 64
+    factor = 1 + panels + 2 * (panels - 1) + max(panels - 2, 0)   # load, diagonal tiles, solves + next-panel updates, rest
+    solve = 2 * panels   # a forward step per tile, the last tile and a backward step per other tile
+    return factor, solve
+
+
+def run_ours_dense(args, rank: int, world: int) -> dict | None:
+    """The dense reduced solve: reduce_schur_dense! of the scene into a dense FP64 S (6 variables per camera), then a
+    step is the device Cholesky of S plus one solve x = S^-1 g (the reference's cholesky(Symmetric(S)) \\ g); S, 288 MB
+    for 1,000 cameras, is larger than L2. The roofline is FP64 over the whole factorisation against cuBLAS DGEMM measured
+    in the same run (no FP64 peak is measured for the pool)."""
+    import torch
+    bls = load_package()
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    spec = replica_spec(bls.scenes.workload(args.workload), rank, world)
+    p = bls.scenes.hessian_problem(spec, dense=True)
+    st = p.structure
+    n = st.nr
+    f = lambda a, t=torch.float64: torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=t)
+    ws = bls.SchurReductionWorkspace(st, None, device=dev.index)
+    S = torch.zeros(n * n, dtype=torch.float64, device=dev)
+    g = torch.zeros(n, dtype=torch.float64, device=dev)
+    bls.reset_schur_dense(S, f(p.R), f(p.scaling_r), p.lam, ws)
+    assert bls.reduce_schur_dense(S, g, f(p.b_r), f(p.b_e), f(p.scaling_e), p.lam, st, f(p.E), f(p.C), ws)
+    del ws
+    D = bls.DenseCholesky(n, device=dev.index)
+    x = torch.empty_like(g)
+
+    def step():
+        assert D.factor(S), f"S is not positive definite (column {D.failed_column})"
+        D.solve(g, x)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    evs = []
+    with ClockSampler(dev.index) as clk:
+        for _ in range(args.steps):
+            a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a.record()
+            assert D.factor(S)
+            b.record()
+            D.solve(g, x)
+            c.record()
+            evs.append((a, b, c))
+        torch.cuda.synchronize()
+    total = max_over_ranks(sum(a.elapsed_time(c) for a, _, c in evs), world, dev)
+    factor_ms = statistics.median(a.elapsed_time(b) for a, b, _ in evs)
+    solve_ms = statistics.median(b.elapsed_time(c) for _, b, c in evs)
+    A = S.view(n, n).t()   # S is column-major: A[i, j] = S[i + n j]; its upper triangle is the reduced system
+    Afull = torch.triu(A) + torch.triu(A, 1).t()
+    rel = float((Afull @ x - g).norm() / g.norm())
+    del Afull, A
+
+    # end to end through the public API: S and g from pinned host memory, x back to the host
+    S_host = S.cpu().pin_memory()
+    g_host = g.cpu().pin_memory()
+    x_host = torch.empty(n, dtype=torch.float64).pin_memory()
+    S_dev = torch.empty_like(S)
+    g_dev = torch.empty_like(g)
+
+    def e2e_step():
+        S_dev.copy_(S_host, non_blocking=True)
+        g_dev.copy_(g_host, non_blocking=True)
+        assert D.factor(S_dev)
+        D.solve(g_dev, x)
+        x_host.copy_(x, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        e2e_step()
+    b.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(a.elapsed_time(b), world, dev)
+    assert torch.equal(x_host, x.cpu())
+
+    # the FP64 denominator: cuBLAS DGEMM (torch.matmul, float64, 8192^3), best of 3
+    M = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    M @ M
+    best = float("inf")
+    for _ in range(3):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        M @ M
+        b.record()
+        torch.cuda.synchronize()
+        best = min(best, a.elapsed_time(b))
+    dgemm_tflops = 2 * 8192**3 / (best / 1e3) / 1e12
+    del M
+    if rank != 0:
+        return None
+    fl, sl = dense_launches(n)
+    flops = n**3 / 3.0
+    achieved = flops / (factor_ms / 1e3) / 1e12
+    out = {
+        "metric": "dense reduced solves/s (Cholesky of the dense S + one solve)", "value": world * args.steps / (total / 1e3),
+        "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": args.workload, "cameras": st.nrblocks, "points": st.neblocks, "n": n,
+                   "step": "bls_dense_cholesky + bls_dense_cholesky_solve", "l2": "S (288 MB) larger than L2",
+                   "parallelism": f"replicas x{world}"},
+        "factor_ms": factor_ms, "solve_ms": solve_ms, "rel_residual": rel,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": dgemm_tflops, "unit": "TFLOP/s", "frac": achieved / dgemm_tflops,
+                     "traffic": None, "scope": "whole factorisation (n^3 / 3 multiply-adds as flops over its event time)",
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (torch.matmul, float64)"},
+        "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": n * n * 8 + n * 8,
+                "d2h_bytes_per_step": n * 8},
+        "gpu_launches": args.steps * (fl + sl),
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_dense(S_host.numpy(), g_host.numpy(), n, seconds=args.cpu_seconds)
+    return out
+
+
+def dense_reduced_host(spec, p):
+    """The dense S and g of the scene from the oracle's reset_schur_dense + reduce_schur_dense (FP64, every host core)."""
+    orc, p, ost, _, cores = oracle_problem(spec, p)
+    n = p.structure.nr
+    S, g = np.zeros(n * n), np.zeros(n)
+    orc.reset_schur_dense(ost, S, p.R, p.scaling_r, p.lam)
+    ok, _ = orc.reduce_schur_dense(ost, orc.Work(ost, cores, False), S, g, p.b_r, p.b_e, p.scaling_e, p.lam, p.E, p.C, nthreads=cores)
+    assert ok
+    return S, g
+
+
+def cpu_baseline_dense(S: np.ndarray, g: np.ndarray, n: int, seconds: float = 10.0, steps: int | None = None) -> dict:
+    """LAPACK dpotrf + dpotrs (scipy, every host core) on the same S: the routine the reference's
+    cholesky(Symmetric(S)) \\ g reaches."""
+    import scipy.linalg as sl
+    A = np.asarray(S, np.float64).reshape(n, n, order="F")
+    cores = os.cpu_count() or 1
+
+    def one():
+        c = sl.cho_factor(A, lower=False, overwrite_a=False, check_finite=False)
+        return sl.cho_solve(c, g, check_finite=False)
+
+    one()
+    k, t0 = 0, time.perf_counter()
+    while (steps is None and (time.perf_counter() - t0 < seconds or k < 3)) or (steps is not None and k < steps):
+        one()
+        k += 1
+    dt = time.perf_counter() - t0
+    return {"value": k / dt, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"{k} x LAPACK dpotrf + dpotrs of the {n} x {n} S through scipy on {cores} host threads ({dt:.1f} s)"}
+
+
 _LAST: dict = {}
 
 
@@ -688,6 +844,15 @@ def run_reference(args, rank: int, world: int) -> dict | None:
         return None
     bls = load_package()
     spec = bls.scenes.workload(args.workload)
+    if args.workload.startswith("dense_"):
+        p = bls.scenes.hessian_problem(spec, dense=True)
+        S, g = dense_reduced_host(spec, p)
+        base = cpu_baseline_dense(S, g, p.structure.nr, steps=args.steps)
+        return {"impl": "reference", "metric": "dense reduced solves/s (Cholesky of the dense S + one solve)", "value": base["value"],
+                "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene generator)",
+                "config": {"workload": args.workload, "n": p.structure.nr, "step": "cholesky(Symmetric(S)) \\ g via LAPACK"},
+                "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload.startswith("qr_"):
         base = cpu_baseline_qr(spec, steps=args.steps, warmup=args.warmup)
         return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "obs/s", "n_gpus": world, "steps": args.steps,
@@ -732,6 +897,8 @@ def main():
             out = run_ours_pcg(args, rank, world)
         elif args.workload.startswith("batched_"):
             out = run_ours_batch(args, rank, world)
+        elif args.workload.startswith("dense_"):
+            out = run_ours_dense(args, rank, world)
         else:
             out = run_ours(args, rank, world)
     finally:

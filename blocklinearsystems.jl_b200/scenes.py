@@ -12,6 +12,7 @@ xoshiro256** streams, one per point, with seed = 1000 * workload number + proble
                       capped at 20, lambda log-uniform in [1e-6, 1e-2] per problem
   pcg_10000x1M        10,000 cameras, 1,000,000 points, window +-60, k = 2 + Geom(0.15) capped at 60, camera column
                       scales log-uniform in [1e-2, 1e2], lambda 1e-5
+  dense_1000x200k     sparse_1000x200k's distributions with its own seed, reduced into a dense S (6,000 x 6,000)
 Damping is Marquardt's, lambda * diag(H), for every Hessian workload.
 """
 from __future__ import annotations
@@ -57,6 +58,8 @@ def workload(name: str, problem: int = 0) -> SceneSpec:
         npnt = int(rng.integers(1000, 50_001))
         lam = float(math.exp(rng.uniform(math.log(1e-6), math.log(1e-2))))
         return SceneSpec(nc, npnt, "window", geom_p=0.3, kcap=20, window=15, lam=lam, seed=1000 * 4 + problem)
+    if name == "dense_1000x200k":
+        return SceneSpec(1000, 200_000, "window", geom_p=0.2, kcap=40, window=30, sv=(1e-4, 1.0), lam=1e-4, seed=1000 * 6 + problem)
     if name == "pcg_10000x1M":
         return SceneSpec(10_000, 1_000_000, "window", geom_p=0.15, kcap=60, window=60, cs=(1e-2, 1e2), lam=1e-5, seed=1000 * 5 + problem)
     raise KeyError(name)
