@@ -177,16 +177,30 @@ __global__ void __launch_bounds__(NB) k_trsm_panel(int64_t n, double* __restrict
   for (int c = 0; c < NB; ++c) W[r + n * (k0 + c)] = x[c];
 }
 
+// An asynchronous 8-byte global -> shared copy (cp.async); `bytes` 0 writes a zero and reads nothing.
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, int bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+constexpr int SYRK_SMEM = 2 * NB * NB * (int)sizeof(double);   // both 64 x 64 row panels
+
 // The trailing lower triangle: W[i, j] -= sum_c L[i, c] L[j, c] over the panel's 64 columns, for i >= j >= k0 + NB,
 // in two launches: `rest` == 0 the first tile column (the next panel), `rest` == 1 the tile columns after it.
-// One CTA of 256 threads per 64 x 64 output tile of the lower triangle (tiles listed by their index in it); the two
-// row panels pass through shared memory 32 columns at a time and each thread accumulates a 4 x 4 block (rows
+// One CTA of 256 threads per 64 x 64 output tile of the lower triangle (tiles listed by their index in it). Both row
+// panels are copied to shared memory asynchronously (cp.async, rows past n zero-filled) as two 32-column groups, so the
+// first group's products run while the second is in flight; each thread accumulates a 4 x 4 block (rows
 // 2 tx + {0, 1, 32, 33}, columns 2 ty + {0, 1, 32, 33}) from 16-byte shared loads with FP64 fused multiply-adds (the
 // FP64 tensor-core form, mma.sync m8n8k4 fragments per warp, measured 1.3x slower here).
 __global__ void __launch_bounds__(256) k_syrk_tiles(int64_t n, double* __restrict__ W, int64_t k0, int rest,
                                                     const long long* __restrict__ status) {
   constexpr int KC = 32;
-  __shared__ __align__(16) double Pi[KC][NB], Pj[KC][NB];
+  extern __shared__ __align__(16) double syrk_smem[];
+  double (*Pi)[NB] = reinterpret_cast<double (*)[NB]>(syrk_smem);
+  double (*Pj)[NB] = reinterpret_cast<double (*)[NB]>(syrk_smem + NB * NB);
   if (status[0] >= 0) return;
   const int64_t t = blockIdx.x;
   int64_t ti = t, tj = 0;
@@ -199,29 +213,30 @@ __global__ void __launch_bounds__(256) k_syrk_tiles(int64_t n, double* __restric
   }
   const int64_t bi = k0 + NB + ti * NB, bj = k0 + NB + tj * NB;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+#pragma unroll
+  for (int h = 0; h < NB / KC; ++h) {
+#pragma unroll
+    for (int k = 0; k < KC * NB / 256; ++k) {
+      const int e = tid + 256 * k, c = KC * h + (e >> 6), r = e & 63;
+      const int64_t col = n * (k0 + c);
+      const bool vi = bi + r < n, vj = bj + r < n;
+      cp_async8(&Pi[c][r], vi ? W + bi + r + col : W, vi ? 8 : 0);
+      cp_async8(&Pj[c][r], vj ? W + bj + r + col : W, vj ? 8 : 0);
+    }
+    cp_async_commit();
+  }
   double acc[4][4];
 #pragma unroll
   for (int p = 0; p < 4; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[p][q] = 0.0;
-  for (int kc = 0; kc < NB; kc += KC) {
-    double vi[KC * NB / 256], vj[KC * NB / 256];
 #pragma unroll
-    for (int k = 0; k < KC * NB / 256; ++k) {
-      const int e = tid + 256 * k, c = e >> 6, r = e & 63;
-      const int64_t col = n * (k0 + kc + c);
-      vi[k] = bi + r < n ? W[bi + r + col] : 0.0;
-      vj[k] = bj + r < n ? W[bj + r + col] : 0.0;
-    }
-#pragma unroll
-    for (int k = 0; k < KC * NB / 256; ++k) {
-      const int e = tid + 256 * k;
-      Pi[e >> 6][e & 63] = vi[k];
-      Pj[e >> 6][e & 63] = vj[k];
-    }
+  for (int h = 0; h < NB / KC; ++h) {
+    if (h == 0) cp_async_wait<1>();
+    else cp_async_wait<0>();
     __syncthreads();
 #pragma unroll 8
-    for (int c = 0; c < KC; ++c) {
+    for (int c = KC * h; c < KC * h + KC; ++c) {
       const double2 a0 = *reinterpret_cast<const double2*>(&Pi[c][2 * tx]);
       const double2 a1 = *reinterpret_cast<const double2*>(&Pi[c][32 + 2 * tx]);
       const double2 b0 = *reinterpret_cast<const double2*>(&Pj[c][2 * ty]);
@@ -232,7 +247,6 @@ __global__ void __launch_bounds__(256) k_syrk_tiles(int64_t n, double* __restric
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[p][q] = fma(ra[p], rb[q], acc[p][q]);
     }
-    __syncthreads();
   }
 #pragma unroll
   for (int p = 0; p < 4; ++p)
@@ -417,6 +431,7 @@ static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
     BLS_CUDA(cudaEventCreateWithFlags(&D->ev_panel, cudaEventDisableTiming));
   }
   cudaStream_t p = D->panel_stream;
+  BLS_CUDA(cudaFuncSetAttribute(k_syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
   k_dense_load<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n * n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, S, W, st);
   BLS_CUDA(cudaEventRecord(D->ev_join, s));
   BLS_CUDA(cudaStreamWaitEvent(p, D->ev_join, 0));
@@ -433,11 +448,11 @@ static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
   for (int64_t k0 = 0; n - k0 > NB; k0 += NB) {
     const int64_t nt = (n - k0 - NB + NB - 1) / NB;
     BLS_CUDA(cudaStreamWaitEvent(s, D->ev_panel, 0));
-    k_syrk_tiles<<<(unsigned)nt, 256, 0, s>>>(n, W, k0, 0, st);
+    k_syrk_tiles<<<(unsigned)nt, 256, SYRK_SMEM, s>>>(n, W, k0, 0, st);
     BLS_CUDA(cudaEventRecord(D->ev_join, s));
     BLS_CUDA(cudaStreamWaitEvent(p, D->ev_join, 0));
     panel(k0 + NB);
-    if (nt > 1) k_syrk_tiles<<<(unsigned)((nt - 1) * nt / 2), 256, 0, s>>>(n, W, k0, 1, st);
+    if (nt > 1) k_syrk_tiles<<<(unsigned)((nt - 1) * nt / 2), 256, SYRK_SMEM, s>>>(n, W, k0, 1, st);
   }
   BLS_CUDA(cudaStreamWaitEvent(s, D->ev_panel, 0));
   BLS_CUDA(cudaGetLastError());
