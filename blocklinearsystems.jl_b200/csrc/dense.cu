@@ -2,11 +2,11 @@
 // reduce_schur_dense! when S is small enough to hold dense (the reference hands its dense S to DampedLinearSolve's
 // Cholesky, src/schur_linear_systems.jl:312-320). S is read from its upper triangle in its storage type (FP64 or the
 // mixed form's FP32), mirrored into an FP64 working matrix owned by the solver, and factored in place as S = L L' by a
-// right-looking blocked Cholesky with 64-column panels: per panel, the diagonal tile in one CTA's shared memory, the
-// rows below it by a triangular solve, then the trailing lower triangle updated in 64 x 64 tiles. A pivot that is not
-// positive (or not finite) stops the factorisation; its column is reported, 1-based. The solve runs the two triangular
-// substitutions as one launch per 64-row tile: all CTAs apply the last solved tile to the rows it feeds, and CTA 0,
-// whose rows are the next diagonal tile, then solves that tile.
+// right-looking blocked Cholesky with 64-column panels: per panel, one launch factors the diagonal tile (in every
+// CTA's shared memory) and solves the rows below it, then the trailing lower triangle is updated in 64 x 64 tiles. A
+// pivot that is not positive (or not finite) stops the factorisation; its column is reported, 1-based. The solve runs
+// the two triangular substitutions as one launch per 64-row tile: all CTAs apply the last solved tile to the rows it
+// feeds, and CTA 0, whose rows are the next diagonal tile, then solves that tile.
 #include <algorithm>
 #include <cmath>
 #include <memory>
@@ -16,6 +16,7 @@
 namespace bls {
 
 constexpr int NB = 64;   // panel width and tile size
+constexpr int kFusedPanelTiles = 32;   // panels with at most this many 64-row tiles below run as one launch
 
 struct DenseSolver {
   bls_ctx* ctx = nullptr;
@@ -62,21 +63,23 @@ __device__ __forceinline__ void load_tile(double (*t)[NB + 1], const double* __r
   }
 }
 
-// The diagonal tile [k0, k0 + nb) in one CTA of 256 threads, held in shared memory and factored by 16-column
-// sub-panels. Warp 0 factors a sub-panel's rows (lane i holds rows c0 + i and c0 + 32 + i of its 16 columns in
-// registers) with no barrier: per column the pivot comes from its lane by shuffle, L[j, j] = pivot * rsqrt(pivot), and
-// each later column's entry of L is shuffled from its lane to update the rows below. Then all threads subtract the
-// sub-panel's rank-16 product from the rest of the tile. A non-positive or non-finite pivot records its column and
-// stops (W is not written). 1 / L[j, j] goes to dinv.
-__global__ void __launch_bounds__(256, 1) k_potrf_tile(int64_t n, double* __restrict__ W, double* __restrict__ dinv, int64_t k0,
-                                                    int nb, long long* __restrict__ status) {
-  __shared__ double T[NB][NB + 1];
-  __shared__ int failed;
-  if (status[0] >= 0) return;   // uniform across the CTA
+// An asynchronous 8-byte global -> shared copy (cp.async); `bytes` 0 writes a zero and reads nothing.
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, int bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// The diagonal tile T (lower triangle of its first nb rows and columns, in shared memory) factored in place by
+// 256 threads, by 16-column sub-panels: warp 0 factors a sub-panel's rows (lane i holds rows c0 + i and c0 + 32 + i
+// of its 16 columns in registers) with no barrier: per column the pivot comes from its lane by shuffle,
+// L[j, j] = pivot * rsqrt(pivot), and each later column's entry of L is shuffled from its lane to update the rows
+// below; then all threads subtract the sub-panel's rank-16 product from the rest of the tile. 1 / L[j, j] goes to dv.
+// Returns (to every thread) the first column whose pivot is not positive or not finite, or -1.
+__device__ int factor_tile(double (*T)[NB + 1], double* dv, int nb, int* failed) {
   const int tid = threadIdx.x, lane = tid & 31;
-  load_tile(T, W, n, k0, nb, tid);
-  if (tid == 0) failed = -1;
-  __syncthreads();
   for (int c0 = 0; c0 < nb; c0 += 16) {
     const int w = nb - c0 < 16 ? nb - c0 : 16;
     if (tid < 32) {
@@ -99,7 +102,7 @@ __global__ void __launch_bounds__(256, 1) k_potrf_tile(int64_t n, double* __rest
             const double l0 = (lane == j ? d : a0[j]) * inv, l1 = a1[j] * inv;
             if (lane >= j) a0[j] = l0;
             a1[j] = l1;
-            if (lane == j) dinv[k0 + c0 + j] = inv;
+            if (lane == j) dv[c0 + j] = inv;
 #pragma unroll
             for (int k = j + 1; k < 16; ++k) {
               const double lk = __shfl_sync(0xffffffffu, l0, k);
@@ -114,13 +117,10 @@ __global__ void __launch_bounds__(256, 1) k_potrf_tile(int64_t n, double* __rest
         if (r0 < NB && k <= lane) T[r0][c0 + k] = a0[k];
         if (r1 < NB) T[r1][c0 + k] = a1[k];
       }
-      if (lane == 0) failed = bad;
+      if (lane == 0) *failed = bad;
     }
     __syncthreads();
-    if (failed >= 0) {   // uniform
-      if (tid == 0) status[0] = k0 + failed;
-      return;
-    }
+    if (*failed >= 0) return *failed;   // uniform
     // the rest of the tile's lower triangle: T[i, k] -= sum over the sub-panel's columns of L[i, c] L[k, c]
     const int base = c0 + 16, m = nb > base ? nb - base : 0;
     for (int e = tid; e < m * m; e += 256) {
@@ -136,23 +136,55 @@ __global__ void __launch_bounds__(256, 1) k_potrf_tile(int64_t n, double* __rest
     }
     __syncthreads();
   }
+  return -1;
+}
+
+// One row of the panel below the tile solved against L_kk' (x L_kk' = a): x holds the row's 64 entries; L[c2, c] is
+// read from the factored tile as a broadcast.
+__device__ __forceinline__ void solve_row(double (&x)[NB], const double (*T)[NB + 1], const double* dv) {
+#pragma unroll
+  for (int c = 0; c < NB; ++c) {
+    x[c] *= dv[c];
+#pragma unroll
+    for (int c2 = c + 1; c2 < NB; ++c2) x[c2] -= x[c] * T[c2][c];
+  }
+}
+
+// The diagonal tile [k0, k0 + nb) alone, in one CTA (followed by k_trsm_panel when many rows lie below it). A
+// non-positive or non-finite pivot records its column and W is not written. 1 / L[j, j] goes to dinv.
+__global__ void __launch_bounds__(256, 1) k_potrf_tile(int64_t n, double* __restrict__ W, double* __restrict__ dinv, int64_t k0,
+                                                       int nb, long long* __restrict__ status) {
+  __shared__ double T[NB][NB + 1];
+  __shared__ double dv[NB];
+  __shared__ int failed;
+  if (status[0] >= 0) return;   // uniform across the CTA
+  const int tid = threadIdx.x;
+  load_tile(T, W, n, k0, nb, tid);
+  if (tid == 0) failed = -1;
+  __syncthreads();
+  const int bad = factor_tile(T, dv, nb, &failed);
+  if (bad >= 0) {
+    if (tid == 0) status[0] = k0 + bad;
+    return;
+  }
 #pragma unroll
   for (int k = 0; k < NB * NB / 256; ++k) {
     const int e = tid + 256 * k, rr = e & 63, cc = e >> 6;
     if (rr < nb && cc <= rr) W[(k0 + rr) + n * (k0 + cc)] = T[rr][cc];
   }
+  if (tid < nb) dinv[k0 + tid] = dv[tid];
 }
 
-// The panel below the diagonal tile: rows [k0 + NB, n) of columns [k0, k0 + NB) solved against L_kk' (X L_kk' = A),
-// a thread per row holding its 64 entries in registers, L_kk transposed in shared memory (read as broadcasts).
+// The panel below the diagonal tile factored by k_potrf_tile: rows [k0 + NB, n) of columns [k0, k0 + NB), a thread
+// per row with its 64 entries in registers, the tile in shared memory.
 __global__ void __launch_bounds__(NB) k_trsm_panel(int64_t n, double* __restrict__ W, const double* __restrict__ dinv_g,
-                                                  int64_t k0, const long long* __restrict__ status) {
-  __shared__ __align__(16) double LT[NB][NB];   // LT[c][r] = L[r][c]
-  __shared__ double dinv[NB];
+                                                   int64_t k0, const long long* __restrict__ status) {
+  __shared__ double T[NB][NB + 1];
+  __shared__ double dv[NB];
   if (status[0] >= 0) return;
   const int t = threadIdx.x;
   const int64_t r = k0 + NB + (int64_t)blockIdx.x * NB + t;
-  // the row's 64 entries and the tile (16 columns at a time) are loaded with every load of a batch in flight
+  // the row's 64 entries and the tile (16 columns at a time), every load of a batch in flight
   double x[NB];
 #pragma unroll
   for (int c = 0; c < NB; ++c) x[c] = r < n ? W[r + n * (k0 + c)] : 0.0;
@@ -162,29 +194,69 @@ __global__ void __launch_bounds__(NB) k_trsm_panel(int64_t n, double* __restrict
 #pragma unroll
     for (int c = 0; c < 16; ++c) v[c] = W[(k0 + t) + n * (k0 + c0 + c)];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) LT[c0 + c][t] = v[c];
+    for (int c = 0; c < 16; ++c) T[t][c0 + c] = v[c];
   }
-  dinv[t] = dinv_g[k0 + t];
+  dv[t] = dinv_g[k0 + t];
   __syncthreads();
   if (r >= n) return;
-#pragma unroll
-  for (int c = 0; c < NB; ++c) {
-    x[c] *= dinv[c];
-#pragma unroll
-    for (int c2 = c + 1; c2 < NB; ++c2) x[c2] -= x[c] * LT[c][c2];
-  }
+  solve_row(x, T, dv);
 #pragma unroll
   for (int c = 0; c < NB; ++c) W[r + n * (k0 + c)] = x[c];
 }
 
-// An asynchronous 8-byte global -> shared copy (cp.async); `bytes` 0 writes a zero and reads nothing.
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, int bytes) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+// shared memory of k_panel: the diagonal tile, the CTA's 64 panel rows, 1 / L[j, j]
+constexpr int PANEL_SMEM = (2 * NB * (NB + 1) + NB) * (int)sizeof(double);
+
+// One panel [k0, k0 + nb) in one launch of max(1, ceil(rows below / 64)) CTAs of 256 threads, for panels with few
+// rows below: every CTA factors the diagonal tile in its own shared memory (the same operations on the same values,
+// so every copy is identical; CTA 0 writes it and 1 / L[j, j] back) while its 64 rows below the tile arrive by
+// cp.async, then a thread per row solves it. A non-positive or non-finite pivot is seen by every CTA: CTA 0 records
+// its column and nothing is written.
+__global__ void __launch_bounds__(256, 1) k_panel(int64_t n, double* __restrict__ W, double* __restrict__ dinv, int64_t k0,
+                                                  int nb, long long* __restrict__ status) {
+  extern __shared__ __align__(16) double panel_smem[];
+  double (*T)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(panel_smem);
+  double (*X)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(panel_smem + NB * (NB + 1));
+  double* dv = panel_smem + 2 * NB * (NB + 1);
+  __shared__ int failed;
+  if (status[0] >= 0) return;   // uniform across the grid
+  const int tid = threadIdx.x;
+  const int64_t row0 = k0 + nb + (int64_t)blockIdx.x * NB;   // this CTA's rows below the tile
+#pragma unroll
+  for (int k = 0; k < NB * NB / 256; ++k) {
+    const int e = tid + 256 * k, r = e & 63, c = e >> 6;
+    const bool v = row0 + r < n;
+    cp_async8(&X[r][c], v ? W + (row0 + r) + n * (k0 + c) : W, v ? 8 : 0);
+  }
+  cp_async_commit();
+  load_tile(T, W, n, k0, nb, tid);
+  if (tid == 0) failed = -1;
+  __syncthreads();
+  const int bad = factor_tile(T, dv, nb, &failed);
+  if (bad >= 0) {
+    cp_async_wait<0>();
+    if (blockIdx.x == 0 && tid == 0) status[0] = k0 + bad;
+    return;
+  }
+  if (blockIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NB * NB / 256; ++k) {
+      const int e = tid + 256 * k, rr = e & 63, cc = e >> 6;
+      if (rr < nb && cc <= rr) W[(k0 + rr) + n * (k0 + cc)] = T[rr][cc];
+    }
+    if (tid < nb) dinv[k0 + tid] = dv[tid];
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  const int64_t r = row0 + tid;
+  if (tid >= NB || r >= n) return;   // rows below the tile exist only when nb == NB
+  double x[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) x[c] = X[tid][c];
+  solve_row(x, T, dv);
+#pragma unroll
+  for (int c = 0; c < NB; ++c) W[r + n * (k0 + c)] = x[c];
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 constexpr int SYRK_SMEM = 2 * NB * NB * (int)sizeof(double);   // both 64 x 64 row panels
 
@@ -432,14 +504,23 @@ static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
   }
   cudaStream_t p = D->panel_stream;
   BLS_CUDA(cudaFuncSetAttribute(k_syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
+  BLS_CUDA(cudaFuncSetAttribute(k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL_SMEM));
   k_dense_load<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n * n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, S, W, st);
   BLS_CUDA(cudaEventRecord(D->ev_join, s));
   BLS_CUDA(cudaStreamWaitEvent(p, D->ev_join, 0));
   // panel k: its diagonal tile, then (when rows remain below it) its triangular solve, on the panel stream
+  // panel k: its diagonal tile and the rows below it, on the panel stream. With few rows below, one launch in which
+  // every CTA factors the tile itself (a launch less on the panel chain); with many, the tile in one CTA and then the
+  // rows (the redundant factorisations would take SMs from the trailing update running beside them).
   auto panel = [&](int64_t k0) {
     const int nb = (int)std::min<int64_t>(NB, n - k0);
-    k_potrf_tile<<<1, 256, 0, p>>>(n, W, dv, k0, nb, st);
-    if (n - k0 - nb > 0) k_trsm_panel<<<(unsigned)((n - k0 - nb + NB - 1) / NB), NB, 0, p>>>(n, W, dv, k0, st);
+    const int64_t below = (n - k0 - nb + NB - 1) / NB;
+    if (below <= kFusedPanelTiles) {
+      k_panel<<<(unsigned)std::max<int64_t>(1, below), 256, PANEL_SMEM, p>>>(n, W, dv, k0, nb, st);
+    } else {
+      k_potrf_tile<<<1, 256, 0, p>>>(n, W, dv, k0, nb, st);
+      k_trsm_panel<<<(unsigned)below, NB, 0, p>>>(n, W, dv, k0, st);
+    }
     BLS_CUDA(cudaEventRecord(D->ev_panel, p));
   };
   panel(0);
