@@ -29,7 +29,14 @@ struct DenseSolver {
   // update runs on the caller's stream (created at the first factorisation).
   cudaStream_t panel_stream = nullptr;
   cudaEvent_t ev_join = nullptr, ev_panel = nullptr;
+  // The solve's launches (two per 64-row tile) as one CUDA graph on the solver's own right-hand side y, captured at
+  // the first solve: g is copied into y, the graph replayed, y copied out to x.
+  DevBuf y;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t solve_graph = nullptr;
   ~DenseSolver() {
+    if (solve_graph) cudaGraphExecDestroy(solve_graph);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
     if (ev_join) cudaEventDestroy(ev_join);
     if (ev_panel) cudaEventDestroy(ev_panel);
     if (panel_stream) cudaStreamDestroy(panel_stream);
@@ -487,6 +494,19 @@ __global__ void __launch_bounds__(32) k_bwd_last(int64_t n, const double* __rest
   tile_backward(t, dlo, dhi, ys, y, d0, dnb, lane);
 }
 
+// x = (L L')^-1 x in place: the forward steps, then the backward steps, on stream s
+static void launch_solve(cudaStream_t s, int64_t n, const double* W, const double* dv, double* x) {
+  // forward: tile [0, NB) first, then each step updates the rows below the tile it just solved and solves the next
+  k_fwd_step<<<1, 256, 0, s>>>(n, W, dv, x, 0, (int)std::min<int64_t>(NB, n), 0);
+  for (int64_t d0 = NB; d0 < n; d0 += NB)
+    k_fwd_step<<<(unsigned)((n - d0 + NB - 1) / NB), 256, 0, s>>>(n, W, dv, x, d0, (int)std::min<int64_t>(NB, n - d0), 1);
+  // backward: the last (possibly short) tile first, then upward
+  const int64_t kl = ((n - 1) / NB) * NB;
+  k_bwd_last<<<1, 32, 0, s>>>(n, W, dv, x, kl);
+  for (int64_t k0 = kl; k0 > 0; k0 -= NB)
+    k_bwd_step<<<(unsigned)(k0 / NB), 256, 0, s>>>(n, W, dv, x, k0, (int)std::min<int64_t>(NB, n - k0));
+}
+
 template <class T>
 static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
   if (!S) throw Error(BLS_EINVAL, "S is NULL");
@@ -601,16 +621,29 @@ int bls_dense_cholesky_solve(bls_dense_solver* D, const double* g, double* x) {
     const double* W = D->W.as<double>();
     const double* dv = D->dinv.as<double>();
     cudaStream_t s = D->ctx->stream;
-    if (x != g) BLS_CUDA(cudaMemcpyAsync(x, g, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-    // forward: tile [0, NB) first, then each step updates the rows below the tile it just solved and solves the next
-    k_fwd_step<<<1, 256, 0, s>>>(n, W, dv, x, 0, (int)std::min<int64_t>(NB, n), 0);
-    for (int64_t d0 = NB; d0 < n; d0 += NB)
-      k_fwd_step<<<(unsigned)((n - d0 + NB - 1) / NB), 256, 0, s>>>(n, W, dv, x, d0, (int)std::min<int64_t>(NB, n - d0), 1);
-    // backward: the last (possibly short) tile first, then upward
-    const int64_t kl = ((n - 1) / NB) * NB;
-    k_bwd_last<<<1, 32, 0, s>>>(n, W, dv, x, kl);
-    for (int64_t k0 = kl; k0 > 0; k0 -= NB)
-      k_bwd_step<<<(unsigned)(k0 / NB), 256, 0, s>>>(n, W, dv, x, k0, (int)std::min<int64_t>(NB, n - k0));
+    if (!D->solve_graph) {
+      D->y.alloc(sizeof(double) * (size_t)n);
+      if (!D->cap_stream) BLS_CUDA(cudaStreamCreateWithFlags(&D->cap_stream, cudaStreamNonBlocking));
+      BLS_CUDA(cudaStreamBeginCapture(D->cap_stream, cudaStreamCaptureModeThreadLocal));
+      launch_solve(D->cap_stream, n, W, dv, D->y.as<double>());
+      cudaGraph_t gr = nullptr;
+      const cudaError_t e1 = cudaGetLastError();
+      const cudaError_t e2 = cudaStreamEndCapture(D->cap_stream, &gr);
+      if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        if (gr) cudaGraphDestroy(gr);
+        throw Error(BLS_ECUDA, std::string("capturing the solve: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+      }
+      const cudaError_t e3 = cudaGraphInstantiate(&D->solve_graph, gr, 0);
+      cudaGraphDestroy(gr);
+      if (e3 != cudaSuccess) {
+        D->solve_graph = nullptr;
+        throw Error(BLS_ECUDA, std::string("instantiating the solve: ") + cudaGetErrorString(e3));
+      }
+    }
+    double* y = D->y.as<double>();
+    BLS_CUDA(cudaMemcpyAsync(y, g, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    BLS_CUDA(cudaGraphLaunch(D->solve_graph, s));
+    BLS_CUDA(cudaMemcpyAsync(x, y, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s));
     BLS_CUDA(cudaGetLastError());
     return BLS_OK;
   })
