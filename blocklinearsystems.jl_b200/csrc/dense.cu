@@ -29,6 +29,10 @@ struct DenseSolver {
   // update runs on the caller's stream (created at the first factorisation).
   cudaStream_t panel_stream = nullptr;
   cudaEvent_t ev_join = nullptr, ev_panel = nullptr;
+  int panel_priority = 0;
+  // Everything after the load of S (the launches depend on n only) as one CUDA graph, captured at the first
+  // factorisation; the panel kernels carry the high priority as a launch attribute, so the graph keeps it.
+  cudaGraphExec_t factor_graph = nullptr;
   // The solve's launches (two per 64-row tile) as one CUDA graph on the solver's own right-hand side y, captured at
   // the first solve: g is copied into y, the graph replayed, y copied out to x.
   DevBuf y;
@@ -36,6 +40,7 @@ struct DenseSolver {
   cudaGraphExec_t solve_graph = nullptr;
   ~DenseSolver() {
     if (solve_graph) cudaGraphExecDestroy(solve_graph);
+    if (factor_graph) cudaGraphExecDestroy(factor_graph);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     if (ev_join) cudaEventDestroy(ev_join);
     if (ev_panel) cudaEventDestroy(ev_panel);
@@ -507,28 +512,32 @@ static void launch_solve(cudaStream_t s, int64_t n, const double* W, const doubl
     k_bwd_step<<<(unsigned)(k0 / NB), 256, 0, s>>>(n, W, dv, x, k0, (int)std::min<int64_t>(NB, n - k0));
 }
 
-template <class T>
-static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
-  if (!S) throw Error(BLS_EINVAL, "S is NULL");
-  cudaStream_t s = D->ctx->stream;
+// Launches kernel on stream st with the given priority (a launch attribute, so that a captured graph keeps it).
+template <class... Args>
+static void launch_prio(void (*kernel)(Args...), unsigned grid, unsigned block, size_t smem, cudaStream_t st, int prio,
+                        Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributePriority;
+  attr[0].val.priority = prio;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BLS_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+}
+
+// The factorisation after the load of S into W: panels on the panel stream p, trailing updates on s, joined on s.
+static void launch_factor_body(DenseSolver* D, cudaStream_t s, cudaStream_t p) {
   const int64_t n = D->n;
   double* W = D->W.as<double>();
   double* dv = D->dinv.as<double>();
   long long* st = D->status.as<long long>();
-  if (!D->panel_stream) {
-    int lo = 0, hi = 0;
-    BLS_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-    BLS_CUDA(cudaStreamCreateWithPriority(&D->panel_stream, cudaStreamNonBlocking, hi));
-    BLS_CUDA(cudaEventCreateWithFlags(&D->ev_join, cudaEventDisableTiming));
-    BLS_CUDA(cudaEventCreateWithFlags(&D->ev_panel, cudaEventDisableTiming));
-  }
-  cudaStream_t p = D->panel_stream;
-  BLS_CUDA(cudaFuncSetAttribute(k_syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
-  BLS_CUDA(cudaFuncSetAttribute(k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL_SMEM));
-  k_dense_load<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n * n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, S, W, st);
+  const int prio = D->panel_priority;
   BLS_CUDA(cudaEventRecord(D->ev_join, s));
   BLS_CUDA(cudaStreamWaitEvent(p, D->ev_join, 0));
-  // panel k: its diagonal tile, then (when rows remain below it) its triangular solve, on the panel stream
   // panel k: its diagonal tile and the rows below it, on the panel stream. With few rows below, one launch in which
   // every CTA factors the tile itself (a launch less on the panel chain); with many, the tile in one CTA and then the
   // rows (the redundant factorisations would take SMs from the trailing update running beside them).
@@ -536,10 +545,10 @@ static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
     const int nb = (int)std::min<int64_t>(NB, n - k0);
     const int64_t below = (n - k0 - nb + NB - 1) / NB;
     if (below <= kFusedPanelTiles) {
-      k_panel<<<(unsigned)std::max<int64_t>(1, below), 256, PANEL_SMEM, p>>>(n, W, dv, k0, nb, st);
+      launch_prio(k_panel, (unsigned)std::max<int64_t>(1, below), 256, PANEL_SMEM, p, prio, n, W, dv, k0, nb, st);
     } else {
-      k_potrf_tile<<<1, 256, 0, p>>>(n, W, dv, k0, nb, st);
-      k_trsm_panel<<<(unsigned)below, NB, 0, p>>>(n, W, dv, k0, st);
+      launch_prio(k_potrf_tile, 1, 256, 0, p, prio, n, W, dv, k0, nb, st);
+      launch_prio(k_trsm_panel, (unsigned)below, NB, 0, p, prio, n, W, (const double*)dv, k0, (const long long*)st);
     }
     BLS_CUDA(cudaEventRecord(D->ev_panel, p));
   };
@@ -556,6 +565,46 @@ static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
     if (nt > 1) k_syrk_tiles<<<(unsigned)((nt - 1) * nt / 2), 256, SYRK_SMEM, s>>>(n, W, k0, 1, st);
   }
   BLS_CUDA(cudaStreamWaitEvent(s, D->ev_panel, 0));
+}
+
+template <class T>
+static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
+  if (!S) throw Error(BLS_EINVAL, "S is NULL");
+  cudaStream_t s = D->ctx->stream;
+  const int64_t n = D->n;
+  double* W = D->W.as<double>();
+  long long* st = D->status.as<long long>();
+  if (!D->panel_stream) {
+    int lo = 0, hi = 0;
+    BLS_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    D->panel_priority = hi;
+    BLS_CUDA(cudaStreamCreateWithPriority(&D->panel_stream, cudaStreamNonBlocking, hi));
+    BLS_CUDA(cudaEventCreateWithFlags(&D->ev_join, cudaEventDisableTiming));
+    BLS_CUDA(cudaEventCreateWithFlags(&D->ev_panel, cudaEventDisableTiming));
+    BLS_CUDA(cudaFuncSetAttribute(k_syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
+    BLS_CUDA(cudaFuncSetAttribute(k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL_SMEM));
+  }
+  k_dense_load<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n * n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, S, W, st);
+  if (!D->factor_graph) {
+    if (!D->cap_stream) BLS_CUDA(cudaStreamCreateWithFlags(&D->cap_stream, cudaStreamNonBlocking));
+    BLS_CUDA(cudaStreamBeginCapture(D->cap_stream, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t gr = nullptr;
+    try {
+      launch_factor_body(D, D->cap_stream, D->panel_stream);
+    } catch (...) {
+      cudaStreamEndCapture(D->cap_stream, &gr);
+      if (gr) cudaGraphDestroy(gr);
+      throw;
+    }
+    BLS_CUDA(cudaStreamEndCapture(D->cap_stream, &gr));
+    const cudaError_t e = cudaGraphInstantiate(&D->factor_graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) {
+      D->factor_graph = nullptr;
+      throw Error(BLS_ECUDA, std::string("instantiating the factorisation: ") + cudaGetErrorString(e));
+    }
+  }
+  BLS_CUDA(cudaGraphLaunch(D->factor_graph, s));
   BLS_CUDA(cudaGetLastError());
   long long h = -1;
   BLS_CUDA(cudaMemcpyAsync(&h, st, sizeof(long long), cudaMemcpyDeviceToHost, s));
