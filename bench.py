@@ -499,9 +499,15 @@ def run_ours_pcg(args, rank: int, world: int) -> dict | None:
 
 
 def dense_launches(n: int) -> tuple[int, int]:
-    """Kernels one dense factorisation and one solve launch for an n x n system (64-column panels)."""
+    """Kernels one dense factorisation and one solve launch for an n x n system (64-column panels; a panel with at most
+    32 tiles below it is one launch, otherwise its diagonal tile and its rows are two)."""
     panels = (n + 63) // 64
-    factor = 1 + panels + 2 * (panels - 1) + max(panels - 2, 0)   # load, diagonal tiles, solves + next-panel updates, rest
+    panel_kernels = 0
+    for k in range(panels):
+        nb = min(64, n - 64 * k)
+        below = (n - 64 * k - nb + 63) // 64
+        panel_kernels += 1 if below <= 32 else 2
+    factor = 1 + panel_kernels + (panels - 1) + max(panels - 2, 0)   # load, panels, next-panel updates, the rest
     solve = 2 * panels   # a forward step per tile, the last tile and a backward step per other tile
     return factor, solve
 
