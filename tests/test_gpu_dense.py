@@ -82,3 +82,31 @@ def test_not_positive_definite_reports_column(bls):
     assert D.failed_column == col
     with pytest.raises(bls.ArgumentError):
         D.solve(torch.zeros(n, dtype=torch.float64, device=DEV))
+
+
+@pytest.mark.parametrize("n", [200, 3000])
+def test_one_solver_many_systems(bls, n):
+    """One solver reused (its factorisation and solve are replayed from captured graphs): a system, a system that is
+    not positive definite (reported; the solver then holds no factorisation), another system in FP32 storage, each
+    against a host solve; solves with x aliasing g."""
+    rng = np.random.default_rng(n)
+    D = bls.DenseCholesky(n)
+    for trial, dt in enumerate([torch.float64, None, torch.float32]):
+        B = rng.standard_normal((n, n))
+        A = B @ B.T + n * np.eye(n)
+        if dt is None:   # a pivot in the third panel (or the last column) that is not positive
+            j = min(150, n - 1)
+            A[j, j] = -1.0
+            assert not D.factor(torch.from_numpy(A.ravel(order="F")).to(DEV))
+            assert D.failed_column == first_bad_pivot(A)
+            with pytest.raises(bls.ArgumentError):
+                D.solve(torch.zeros(n, dtype=torch.float64, device=DEV))
+            continue
+        S = torch.from_numpy(A.ravel(order="F")).to(DEV, dt)
+        As = S.double().cpu().numpy().reshape(n, n, order="F")   # the stored values (FP32-rounded for dt=float32)
+        assert D.factor(S) and D.failed_column == 0
+        for k in range(2):
+            g = rng.standard_normal(n)
+            gd = torch.from_numpy(g).to(DEV)
+            x = D.solve(gd, gd if k == 1 else None)   # the second solve in place
+            assert relerr(x.cpu().numpy(), np.linalg.solve(As, g)) <= 1e-10, (trial, k)
