@@ -270,21 +270,23 @@ __global__ void __launch_bounds__(256, 1) k_panel(int64_t n, double* __restrict_
   for (int c = 0; c < NB; ++c) W[r + n * (k0 + c)] = x[c];
 }
 
-constexpr int SYRK_SMEM = 2 * NB * NB * (int)sizeof(double);   // both 64 x 64 row panels
+constexpr int SYRK_KC = 16, SYRK_STAGES = 3;
+constexpr int SYRK_SMEM = SYRK_STAGES * 2 * SYRK_KC * NB * (int)sizeof(double);   // a ring of 16-column chunks of both panels
 
 // The trailing lower triangle: W[i, j] -= sum_c L[i, c] L[j, c] over the panel's 64 columns, for i >= j >= k0 + NB,
 // in two launches: `rest` == 0 the first tile column (the next panel), `rest` == 1 the tile columns after it.
-// One CTA of 256 threads per 64 x 64 output tile of the lower triangle (tiles listed by their index in it). Both row
-// panels are copied to shared memory asynchronously (cp.async, rows past n zero-filled) as two 32-column groups, so the
-// first group's products run while the second is in flight; each thread accumulates a 4 x 4 block (rows
-// 2 tx + {0, 1, 32, 33}, columns 2 ty + {0, 1, 32, 33}) from 16-byte shared loads with FP64 fused multiply-adds (the
-// FP64 tensor-core form, mma.sync m8n8k4 fragments per warp, measured 1.3x slower here).
-__global__ void __launch_bounds__(256) k_syrk_tiles(int64_t n, double* __restrict__ W, int64_t k0, int rest,
-                                                    const long long* __restrict__ status) {
-  constexpr int KC = 32;
+// One CTA of 256 threads per 64 x 64 output tile of the lower triangle (tiles listed by their index in it). The two
+// row panels pass through a three-stage ring of 16-column chunks in shared memory, copied asynchronously (cp.async,
+// rows past n zero-filled) two chunks ahead of the products (48 KB and at most 64 registers a thread, so four CTAs fit
+// an SM); each thread accumulates a 4 x 4 block (rows 2 tx + {0, 1, 32, 33}, columns 2 ty + {0, 1, 32, 33}) from
+// 16-byte shared loads with FP64 fused multiply-adds (the FP64 tensor-core form, mma.sync m8n8k4 fragments per warp,
+// measured 1.3x slower here).
+__global__ void __launch_bounds__(256, 4) k_syrk_tiles(int64_t n, double* __restrict__ W, int64_t k0, int rest,
+                                                       const long long* __restrict__ status) {
+  constexpr int KC = SYRK_KC, NCH = NB / KC;
   extern __shared__ __align__(16) double syrk_smem[];
-  double (*Pi)[NB] = reinterpret_cast<double (*)[NB]>(syrk_smem);
-  double (*Pj)[NB] = reinterpret_cast<double (*)[NB]>(syrk_smem + NB * NB);
+  auto Pi = [&](int stage) { return reinterpret_cast<double (*)[NB]>(syrk_smem + stage * 2 * KC * NB); };
+  auto Pj = [&](int stage) { return reinterpret_cast<double (*)[NB]>(syrk_smem + stage * 2 * KC * NB + KC * NB); };
   if (status[0] >= 0) return;
   const int64_t t = blockIdx.x;
   int64_t ti = t, tj = 0;
@@ -297,40 +299,46 @@ __global__ void __launch_bounds__(256) k_syrk_tiles(int64_t n, double* __restric
   }
   const int64_t bi = k0 + NB + ti * NB, bj = k0 + NB + tj * NB;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-#pragma unroll
-  for (int h = 0; h < NB / KC; ++h) {
+  auto issue = [&](int ch) {
+    double (*A)[NB] = Pi(ch % SYRK_STAGES);
+    double (*B)[NB] = Pj(ch % SYRK_STAGES);
 #pragma unroll
     for (int k = 0; k < KC * NB / 256; ++k) {
-      const int e = tid + 256 * k, c = KC * h + (e >> 6), r = e & 63;
-      const int64_t col = n * (k0 + c);
+      const int e = tid + 256 * k, c = e >> 6, r = e & 63;
+      const int64_t col = n * (k0 + KC * ch + c);
       const bool vi = bi + r < n, vj = bj + r < n;
-      cp_async8(&Pi[c][r], vi ? W + bi + r + col : W, vi ? 8 : 0);
-      cp_async8(&Pj[c][r], vj ? W + bj + r + col : W, vj ? 8 : 0);
+      cp_async8(&A[c][r], vi ? W + bi + r + col : W, vi ? 8 : 0);
+      cp_async8(&B[c][r], vj ? W + bj + r + col : W, vj ? 8 : 0);
     }
     cp_async_commit();
-  }
+  };
+  issue(0);
+  issue(1);
   double acc[4][4];
 #pragma unroll
   for (int p = 0; p < 4; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[p][q] = 0.0;
-#pragma unroll
-  for (int h = 0; h < NB / KC; ++h) {
-    if (h == 0) cp_async_wait<1>();
-    else cp_async_wait<0>();
+  for (int ch = 0; ch < NCH; ++ch) {
+    if (ch + 2 < NCH) issue(ch + 2);   // into the stage chunk ch - 1 used: every thread passed the barrier after it
+    else cp_async_commit();           // an empty group keeps the count of groups in flight uniform
+    cp_async_wait<2>();
     __syncthreads();
-#pragma unroll 8
-    for (int c = KC * h; c < KC * h + KC; ++c) {
-      const double2 a0 = *reinterpret_cast<const double2*>(&Pi[c][2 * tx]);
-      const double2 a1 = *reinterpret_cast<const double2*>(&Pi[c][32 + 2 * tx]);
-      const double2 b0 = *reinterpret_cast<const double2*>(&Pj[c][2 * ty]);
-      const double2 b1 = *reinterpret_cast<const double2*>(&Pj[c][32 + 2 * ty]);
+    double (*A)[NB] = Pi(ch % SYRK_STAGES);
+    double (*B)[NB] = Pj(ch % SYRK_STAGES);
+#pragma unroll 4
+    for (int c = 0; c < KC; ++c) {
+      const double2 a0 = *reinterpret_cast<const double2*>(&A[c][2 * tx]);
+      const double2 a1 = *reinterpret_cast<const double2*>(&A[c][32 + 2 * tx]);
+      const double2 b0 = *reinterpret_cast<const double2*>(&B[c][2 * ty]);
+      const double2 b1 = *reinterpret_cast<const double2*>(&B[c][32 + 2 * ty]);
       const double ra[4] = {a0.x, a0.y, a1.x, a1.y}, rb[4] = {b0.x, b0.y, b1.x, b1.y};
 #pragma unroll
       for (int p = 0; p < 4; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[p][q] = fma(ra[p], rb[q], acc[p][q]);
     }
+    __syncthreads();
   }
 #pragma unroll
   for (int p = 0; p < 4; ++p)
