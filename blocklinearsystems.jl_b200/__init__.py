@@ -3,9 +3,10 @@
 The package directory is named `blocklinearsystems.jl_b200`; load it under the module name `blsgpu` with
 `load_package()` in __graft_entry__.py (or any importlib loader), as the directory name is not an identifier.
 
-Layout (host, integer):  SchurStructure, build_schur_pattern, build_r_to_s_map, sparse_with_map
+Layout (host, integer):  SchurStructure, build_schur_pattern, build_r_to_s_map, sparse_with_map, BlockSystem
 Device reduction:        SchurReductionWorkspace, reset_schur_sparse / reset_schur_dense,
-                         reduce_schur_sparse / reduce_schur_dense, backsubstitute, scatter_copy
+                         reduce_schur_sparse / reduce_schur_dense, backsubstitute, scatter_copy,
+                         symmetrifyfull / symmetrifyfull_
 QR elimination:          SchurJacobianStructure, SchurBlockJacobian, QRReductionWorkspace, reduce_qr, qr_backsubstitute,
                          reduced_normal_sparse / reduced_normal_dense, reduced_diagonal_blocks, free_block_pairs
 Reduced solve:           BlockJacobi, factor_diagonal_blocks, solve_diagonal_blocks, PCGWorkspace (block-Jacobi PCG)
@@ -14,9 +15,10 @@ Batches:                 batch.BatchedReduction (uneven problems as one plan, on
 Workloads:               scenes.workload, scenes.hessian_problem, scenes.jacobian_problem
 """
 from ._lib import ArgumentError, BlsError, DimensionMismatch
-from .layout import DEFAULT_MIN_WORK, SchurPattern, SchurStructure, build_r_to_s_map, build_schur_pattern, sparse_with_map
+from .layout import DEFAULT_MIN_WORK, BlockSystem, SchurPattern, SchurStructure, build_r_to_s_map, build_schur_pattern, sparse_with_map
 from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce_schur_dense, reduce_schur_sparse,
-                        prepare_scale, reset_reduce_schur_sparse_host, reset_schur_dense, reset_schur_sparse, scatter_copy)
+                        prepare_scale, reset_reduce_schur_sparse_host, reset_schur_dense, reset_schur_sparse, scatter_copy,
+                        symmetrifyfull, symmetrifyfull_)
 from .qr import (QRReductionWorkspace, SchurBlockJacobian, assemble_hessian, jtj_diag, jtj_quadform, jtr, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
                  reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse)
 from .pcg import BlockJacobi, PCGResult, PCGWorkspace, RefinedResult, factor_diagonal_blocks, solve_diagonal_blocks
@@ -24,10 +26,10 @@ from .dense import DenseCholesky
 from . import batch, gnn, scenes
 
 __all__ = [
-    "ArgumentError", "BlsError", "DimensionMismatch", "DEFAULT_MIN_WORK", "SchurPattern", "SchurStructure", "build_r_to_s_map",
+    "ArgumentError", "BlsError", "DimensionMismatch", "DEFAULT_MIN_WORK", "BlockSystem", "SchurPattern", "SchurStructure", "build_r_to_s_map",
     "build_schur_pattern", "sparse_with_map", "SchurReductionWorkspace", "backsubstitute", "context", "reduce_schur_dense",
     "reduce_schur_sparse", "reset_reduce_schur_sparse_host", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
     "SchurBlockJacobian", "SchurJacobianStructure", "assemble_hessian", "jtj_diag", "jtj_quadform", "jtr", "prepare_scale", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
     "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "BlockJacobi", "PCGResult", "PCGWorkspace", "RefinedResult", "DenseCholesky",
-    "factor_diagonal_blocks", "solve_diagonal_blocks", "gnn", "batch",
+    "factor_diagonal_blocks", "solve_diagonal_blocks", "gnn", "batch", "symmetrifyfull", "symmetrifyfull_",
 ]

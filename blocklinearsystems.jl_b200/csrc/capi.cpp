@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <map>
 #include <string>
 
 #include "common.cuh"
@@ -286,6 +287,77 @@ int bls_qr_structure_schur(const bls_qr_structure* q, bls_structure** out) {
 int bls_qr_structure_destroy(bls_qr_structure* q) {
   delete q;
   return BLS_OK;
+}
+
+
+int bls_symmetrify_full(bls_ctx* ctx, int dtype, int64_t nb, const int64_t* blocksizes, const int64_t* it_colptr,
+                        const int64_t* it_rowval, const int64_t* it_nzval, const void* data, const int64_t* blocks,
+                        int64_t nblocks, void* mat, int64_t m) {
+  BLS_GUARD({
+    if (!ctx || nb < 0 || (nb > 0 && (!blocksizes || !it_colptr))) throw Error(BLS_EINVAL, "null argument");
+    if (dtype != BLS_F64 && dtype != BLS_F32) throw Error(BLS_EINVAL, "unknown dtype");
+    // the included blocks' sizes and 0-based starts in mat (-1: left out), as symmetrifyfull! forms them
+    std::vector<int64_t> lengths((size_t)nb, 0), starts((size_t)nb, -1);
+    if (!blocks) {
+      int64_t cur = 0;
+      for (int64_t b = 0; b < nb; ++b) {
+        lengths[b] = blocksizes[b];
+        starts[b] = cur;
+        cur += blocksizes[b];
+      }
+    } else {
+      if (nblocks < 0) throw Error(BLS_EINVAL, "nblocks is negative");
+      if (nblocks == 0) {
+        if (m != 0)
+          throw Error(BLS_EDIM, "Target matrix has size (" + std::to_string(m) + ", " + std::to_string(m) + "), expected (0, 0)");
+        return BLS_OK;
+      }
+      for (int64_t i = 0; i < nblocks; ++i)
+        if (blocks[i] < 0 || blocks[i] >= nb)
+          throw Error(BLS_EINVAL, "BoundsError: block " + std::to_string(blocks[i] + 1) + " of " + std::to_string(nb));
+      for (int64_t i = 0; i < nblocks; ++i) {
+        const int64_t b = blocks[i];
+        if (lengths[b] != 0) throw Error(BLS_EINVAL, "Block " + std::to_string(b + 1) + " is listed more than once");
+        lengths[b] = blocksizes[b];
+      }
+      int64_t cur = 0;
+      for (int64_t i = 0; i < nblocks; ++i) {
+        starts[blocks[i]] = cur;
+        cur += blocksizes[blocks[i]];
+      }
+    }
+    int64_t total = 0;
+    for (int64_t b = 0; b < nb; ++b) total += lengths[b];
+    if (m != total)
+      throw Error(BLS_EDIM, "Target matrix has size (" + std::to_string(m) + ", " + std::to_string(m) + "), expected (" +
+                                std::to_string(total) + ", " + std::to_string(total) + ")");
+    // the blocks to copy, in indicestransposed's order; of (r, c) and (c, r) only the later one (it overwrites all the
+    // earlier one wrote)
+    std::vector<SymBlock> list;
+    std::vector<std::pair<int64_t, int64_t>> rc;
+    for (int64_t r = 0; r < nb; ++r)
+      for (int64_t k = it_colptr[r]; k < it_colptr[r + 1]; ++k) {
+        const int64_t c = it_rowval[k];
+        if (c < 0 || c >= nb) throw Error(BLS_EINVAL, "indicestransposed names a block column out of range");
+        if (starts[c] < 0 || starts[r] < 0) continue;
+        list.push_back(SymBlock{it_nzval[k], starts[r], starts[c], (int32_t)lengths[r], (int32_t)lengths[c], r == c ? 1 : 0, 0});
+        rc.emplace_back(r, c);
+      }
+    std::map<std::pair<int64_t, int64_t>, size_t> last;
+    for (size_t i = 0; i < rc.size(); ++i) last[rc[i]] = i;
+    std::vector<SymBlock> keep;
+    keep.reserve(list.size());
+    for (size_t i = 0; i < list.size(); ++i) {
+      if (!list[i].diag) {
+        const auto it = last.find({rc[i].second, rc[i].first});
+        if (it != last.end() && it->second > i) continue;
+      }
+      keep.push_back(list[i]);
+    }
+    if ((m > 0 && !mat) || (!keep.empty() && !data)) throw Error(BLS_EINVAL, "null argument");
+    launch_symmetrify(ctx->stream, dtype, data, keep.data(), (int64_t)keep.size(), mat, m);
+    return BLS_OK;
+  })
 }
 
 }  // extern "C"

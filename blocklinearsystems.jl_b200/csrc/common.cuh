@@ -54,6 +54,16 @@ void upload(DevBuf& buf, const std::vector<T>& v, cudaStream_t s) {
   if (!v.empty()) BLS_CUDA(cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
 }
 
+// One block of symmetrifyfull!: data[src ...] (rd x cd, column-major) to mat's rows rs.. and columns cs.., and
+// transposed to rows cs.. and columns rs.. unless diag.
+struct SymBlock {
+  int64_t src, rs, cs;
+  int32_t rd, cd, diag, pad;
+};
+// Zeroes the m x m matrix and copies the blocks (a host list, copied to the device on stream s).
+void launch_symmetrify(cudaStream_t s, int dtype, const void* data, const SymBlock* blocks_host, int64_t nblocks, void* mat,
+                       int64_t m);
+
 }  // namespace bls
 
 struct bls_ctx {

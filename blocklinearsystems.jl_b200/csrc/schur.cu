@@ -2182,6 +2182,45 @@ using namespace bls;
     return BLS_EINVAL;                                                        \
   }
 
+namespace bls {
+
+// symmetrifyfull! blocks, a warp per block: each lane copies entries of the block and, off the diagonal, their
+// transposes (no two blocks write the same entry: the host keeps one of (r, c) and (c, r))
+template <class T>
+__global__ void __launch_bounds__(256) k_symmetrify(const T* __restrict__ data, const SymBlock* __restrict__ blk, int64_t nblk,
+                                                    T* __restrict__ mat, int64_t m) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nblk; t += nwarps) {
+    const SymBlock b = blk[t];
+    const int sz = b.rd * b.cd;
+    for (int q = lane; q < sz; q += 32) {
+      const int row = q % b.rd, col = q / b.rd;
+      const T v = data[b.src + q];
+      mat[(b.rs + row) + m * (b.cs + col)] = v;
+      if (!b.diag) mat[(b.cs + col) + m * (b.rs + row)] = v;
+    }
+  }
+}
+
+void launch_symmetrify(cudaStream_t s, int dtype, const void* data, const SymBlock* blocks_host, int64_t nblocks, void* mat,
+                       int64_t m) {
+  const size_t es = dtype == BLS_F64 ? sizeof(double) : sizeof(float);
+  if (m > 0) BLS_CUDA(cudaMemsetAsync(mat, 0, es * (size_t)m * (size_t)m, s));
+  if (nblocks == 0) return;
+  SymBlock* d = nullptr;
+  BLS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(SymBlock) * (size_t)nblocks, s));
+  // from pageable host memory: the list is staged before the call returns
+  BLS_CUDA(cudaMemcpyAsync(d, blocks_host, sizeof(SymBlock) * (size_t)nblocks, cudaMemcpyHostToDevice, s));
+  const unsigned grid = (unsigned)std::min<int64_t>((nblocks * 32 + 255) / 256, 148 * 16);
+  if (dtype == BLS_F64) k_symmetrify<double><<<grid, 256, 0, s>>>((const double*)data, d, nblocks, (double*)mat, m);
+  else k_symmetrify<float><<<grid, 256, 0, s>>>((const float*)data, d, nblocks, (float*)mat, m);
+  BLS_CUDA(cudaGetLastError());
+  BLS_CUDA(cudaFreeAsync(d, s));
+}
+
+}  // namespace bls
+
 extern "C" {
 
 int bls_schur_plan_create(bls_ctx* ctx, const bls_schur_plan_desc* desc, bls_schur_plan** out) {

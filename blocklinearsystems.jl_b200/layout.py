@@ -151,6 +151,28 @@ class SchurPattern:
             self._h = None
 
 
+@dataclass
+class BlockSystem:
+    """The layout of a block-square SparseBlockLinearSystem (src/SparseBlockLinearSystem.jl:11-35), 0-based: its block
+    sizes and indicestransposed as a CSC over block rows r (colptr), whose rows are the block columns c (rowval) and
+    whose values are the blocks' starts in the data (starts; block (r, c) is blocksizes[r] x blocksizes[c],
+    column-major)."""
+    blocksizes: np.ndarray
+    colptr: np.ndarray
+    rowval: np.ndarray
+    starts: np.ndarray
+
+    @classmethod
+    def retained(cls, structure: "SchurStructure", pattern: "SchurPattern") -> "BlockSystem":
+        """The retained storage R on a Schur pattern: block (r2, r1), r1 <= r2, of R for pattern block (r1, r2)."""
+        return cls(np.ascontiguousarray(structure.r_dims, np.int64), pattern.block_colptr, pattern.block_rowval,
+                   pattern.R_block_start)
+
+    @property
+    def size(self) -> int:
+        return int(np.sum(self.blocksizes))
+
+
 def build_schur_pattern(structure: SchurStructure, extra_blocks=()) -> SchurPattern:
     """build_schur_pattern(structure; extra_blocks) (src/schur_structure.jl:241-323)."""
     L = _lib.gpu()

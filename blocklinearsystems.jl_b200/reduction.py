@@ -7,6 +7,7 @@ reduce_schur_sparse       src/schur_reduction.jl:489-507 -> bool
 reduce_schur_dense        src/schur_reduction.jl:465-479 -> bool
 backsubstitute            src/schur_reduction.jl:519-538
 scatter_copy              src/SparseBlockLinearSystem.jl:356-362 (copyto!(csc, bsm, scatter_map))
+symmetrifyfull(_)         src/SparseBlockLinearSystem.jl:288-341 (symmetrifyfull / symmetrifyfull!)
 
 Element type T of the block storage is the dtype of the tensors: torch.float64 (FP64 throughout) or torch.float32 (the
 mixed form: FP32 storage, pair products and accumulation; FP64 damped inverse, z and gradient). Gradients, right-hand
@@ -22,7 +23,7 @@ import torch
 
 from . import _lib
 from ._lib import BLS_F32, BLS_F64, BLS_NOT_PD, ArgumentError, DimensionMismatch, check, dptr, ptr64
-from .layout import SchurPattern, SchurStructure, build_r_to_s_map, build_schur_pattern
+from .layout import BlockSystem, SchurPattern, SchurStructure, build_r_to_s_map, build_schur_pattern
 
 _contexts: dict[int, C.c_void_p] = {}
 
@@ -330,3 +331,45 @@ def scatter_copy(dest: torch.Tensor, src: torch.Tensor, scatter_map: torch.Tenso
     _dev(src, "src")
     check(_lib.gpu().bls_scatter_copy(context(dest.device.index or 0), T, dptr(dest), dptr(src), dptr(scatter_map), dest.numel()))
     return dest
+
+
+def _block_list(bsys: BlockSystem, blocks):
+    if blocks is None:
+        return None, bsys.size
+    b = np.asarray(blocks)
+    if b.dtype == bool:   # a mask, as the reference's AbstractVector{Bool}
+        if len(b) != len(bsys.blocksizes):
+            raise ArgumentError("the block mask has the wrong length")
+        b = np.flatnonzero(b)
+    b = np.ascontiguousarray(b, np.int64).reshape(-1)
+    ok = (b >= 0) & (b < len(bsys.blocksizes))
+    return b, int(np.sum(bsys.blocksizes[b[ok]]))
+
+
+def symmetrifyfull_(mat: torch.Tensor, bsys: BlockSystem, data: torch.Tensor, blocks=None) -> torch.Tensor:
+    """symmetrifyfull!(mat, bsm, blocks) (src/SparseBlockLinearSystem.jl:299-341): mat (m x m, column-major, or a
+    square tensor, the matrix being symmetric) = the dense symmetric matrix of the blocks of bsys (all, or the 0-based
+    `blocks` in the order they take, or a boolean mask), zero elsewhere. Raises ArgumentError for a block out of range
+    or listed twice and DimensionMismatch for a wrong size, before any write."""
+    T = _dtype_code(_dev(data, "data"))
+    _dev(mat, "mat")
+    if mat.dtype != data.dtype:
+        raise ArgumentError("mat and data must have the same dtype")
+    b, _ = _block_list(bsys, blocks)
+    n = mat.numel()
+    m = int(round(n ** 0.5))
+    if m * m != n:
+        raise DimensionMismatch(f"target matrix has {n} entries, not a square")
+    bs, cp, rv, st = (np.ascontiguousarray(a, np.int64) for a in (bsys.blocksizes, bsys.colptr, bsys.rowval, bsys.starts))
+    check(_lib.gpu().bls_symmetrify_full(context(data.device.index or 0), T, len(bs), ptr64(bs), ptr64(cp), ptr64(rv), ptr64(st),
+                                         dptr(data), None if b is None else ptr64(b), 0 if b is None else len(b),
+                                         dptr(mat) if n else None, m))
+    return mat
+
+
+def symmetrifyfull(bsys: BlockSystem, data: torch.Tensor, blocks=None) -> torch.Tensor:
+    """symmetrifyfull(bsm) (src/SparseBlockLinearSystem.jl:288-297), optionally of a block subset: a new m x m
+    tensor."""
+    _, m = _block_list(bsys, blocks)
+    mat = torch.empty(m, m, dtype=data.dtype, device=data.device)
+    return symmetrifyfull_(mat, bsys, data, blocks)

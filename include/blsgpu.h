@@ -418,6 +418,20 @@ int bls_adam_step(bls_ctx* ctx, float* params_dev, const float* grad_dev, float*
 /* copyto!(csc, bsm, scatter_map) (src/SparseBlockLinearSystem.jl:356-362): dest[i] = src[map[i]], i < n. */
 int bls_scatter_copy(bls_ctx* ctx, int dtype, void* dest_dev, const void* src_dev, const int64_t* map_dev, int64_t n);
 
+/* symmetrifyfull!(mat, bsm, blocks) (src/SparseBlockLinearSystem.jl:299-341): the dense symmetric matrix of a
+ * block-square SparseBlockLinearSystem, each block (r, c) copied to its place and, for r != c, transposed to (c, r).
+ * The system is given on the host by its nb block sizes and its indicestransposed as a CSC over block rows: for k in
+ * [it_colptr[r], it_colptr[r + 1]), block (r, it_rowval[k]) starts at data[it_nzval[k]] (column-major, blocksizes[r]
+ * x blocksizes[c]); for the retained part R of a Schur pattern these are r_dims, block_colptr, block_rowval and
+ * R_block_start. data and mat (m x m, column-major, zero outside the blocks) are device buffers of dtype. blocks:
+ * the 0-based blocks to include, in the order they take in mat (NULL: all, in order; nblocks is then ignored).
+ * Errors, before any write: a block out of range (the reference's BoundsError) or listed twice BLS_EINVAL; m other
+ * than the total size of the included blocks (DimensionMismatch) BLS_EDIM. Where blocks (r, c) and (c, r) are both
+ * present, the one later in indicestransposed is the one written, as the reference's loop leaves it. */
+int bls_symmetrify_full(bls_ctx* ctx, int dtype, int64_t nb, const int64_t* blocksizes, const int64_t* it_colptr,
+                        const int64_t* it_rowval, const int64_t* it_nzval, const void* data_dev, const int64_t* blocks,
+                        int64_t nblocks, void* mat_dev, int64_t m);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1524,6 +1524,58 @@ int orc_r_to_s_map(OrcStructure* o, OrcPattern* p, i64* out) {
   })
 }
 
+// symmetrifyfull!(mat, bsm, blocks) (src/SparseBlockLinearSystem.jl:299-341) for a block-square system given by its
+// block sizes and indicestransposed (a CSC over block rows r: rows it_rowval = block columns c, values it_nzval = the
+// 0-based start of block (r, c) in data, column-major blocksizes[r] x blocksizes[c]). blocks: 0-based block list, in
+// the order the blocks take in mat, or NULL for all blocks in order (nblocks is then ignored). mat: m x m, column-major.
+int orc_symmetrify_full(i64 nb, const i64* blocksizes, const i64* it_colptr, const i64* it_rowval, const i64* it_nzval,
+                        const double* data, const i64* blocks, i64 nblocks, double* mat, i64 m) {
+  ORC_TRY({
+    IV lengths(nb, 0), starts(nb, 0);   // 1-based starts; 0 marks a block left out
+    if (!blocks) {
+      i64 cur = 1;
+      for (i64 b = 1; b <= nb; ++b) { lengths(b) = blocksizes[b - 1]; starts(b) = cur; cur += blocksizes[b - 1]; }
+    } else {
+      if (nblocks == 0) {
+        if (m != 0) dim_error("Target matrix has size (" + std::to_string(m) + ", " + std::to_string(m) + "), expected (0, 0)");
+        return ORC_OK;
+      }
+      for (i64 i = 0; i < nblocks; ++i)
+        if (!(blocks[i] >= 0 && blocks[i] < nb)) arg_error("BoundsError: block " + std::to_string(blocks[i] + 1) + " of " + std::to_string(nb));
+      for (i64 i = 0; i < nblocks; ++i) {
+        const i64 b = blocks[i] + 1;
+        if (lengths(b) != 0) arg_error("Block " + std::to_string(b) + " is listed more than once");
+        lengths(b) = blocksizes[b - 1];
+      }
+      i64 cur = 1;
+      for (i64 i = 0; i < nblocks; ++i) { starts(blocks[i] + 1) = cur; cur += blocksizes[blocks[i]]; }
+    }
+    i64 total = 0;
+    for (i64 b = 1; b <= nb; ++b) total += lengths(b);
+    if (total != m)
+      dim_error("Target matrix has size (" + std::to_string(m) + ", " + std::to_string(m) + "), expected (" + std::to_string(total) + ", " +
+                std::to_string(total) + ")");
+    for (i64 q = 0; q < m * m; ++q) mat[q] = 0.0;
+    // findnz(indicestransposed): block columns r of the transpose in order, then its rows c
+    for (i64 r = 1; r <= nb; ++r)
+      for (i64 k = it_colptr[r - 1]; k < it_colptr[r]; ++k) {
+        const i64 c = it_rowval[k] + 1, index = it_nzval[k];
+        const i64 cs = starts(c);
+        if (cs == 0) continue;
+        const i64 rs = starts(r);
+        if (rs == 0) continue;
+        const i64 r_ = lengths(r), c_ = lengths(c);
+        for (i64 cc = 0; cc < c_; ++cc)
+          for (i64 rr = 0; rr < r_; ++rr) {
+            const double v = data[index + rr + cc * r_];
+            mat[(rs - 1 + rr) + m * (cs - 1 + cc)] = v;
+            if (r != c) mat[(cs - 1 + cc) + m * (rs - 1 + rr)] = v;
+          }
+      }
+    return ORC_OK;
+  })
+}
+
 // makesparseindices + sparse_with_map of the retained storage: colptr (n+1), rowval, map (0-based)
 i64 orc_sparse_indices(OrcStructure* o, OrcPattern* p, int symmetric, i64* colptr, i64* rowval, i64* map) {
   SparseIdx S;

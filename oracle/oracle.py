@@ -223,6 +223,27 @@ def backsubstitute(st, work, x_e, x_r, Cd, s_r=None, s_e=None, nthreads=1):
     return _chk(f(st.h, work.h, _p(x_e), _p(x_r), _p(Cd), _p(s_r), _p(s_e), C.c_int(nthreads)))
 
 
+def symmetrify_full(blocksizes, it_colptr, it_rowval, it_nzval, data, blocks=None, m=None):
+    """symmetrifyfull!(mat, bsm, blocks) (src/SparseBlockLinearSystem.jl:299-341) of the block system given by its
+    block sizes and indicestransposed (0-based CSC over block rows; it_nzval = 0-based block starts in data). blocks:
+    0-based block list, a boolean mask, or None for all. m: the order of the target (default: the expected one).
+    Returns the m x m matrix."""
+    bsz = np.ascontiguousarray(blocksizes, np.int64)
+    cp, rv, nz = (np.ascontiguousarray(a, np.int64) for a in (it_colptr, it_rowval, it_nzval))
+    d = np.ascontiguousarray(data, np.float64)
+    if blocks is not None:
+        blocks = np.asarray(blocks)
+        if blocks.dtype == bool:
+            blocks = np.flatnonzero(blocks)
+        blocks = np.ascontiguousarray(blocks, np.int64)
+    if m is None:
+        m = int(bsz.sum()) if blocks is None else int(bsz[blocks[(blocks >= 0) & (blocks < len(bsz))]].sum())
+    mat = np.zeros(max(m, 0) * max(m, 0))
+    _chk(lib().orc_symmetrify_full(i64(len(bsz)), _p(bsz), _p(cp), _p(rv), _p(nz), _p(d), None if blocks is None else _p(blocks),
+                                   i64(0 if blocks is None else len(blocks)), _p(mat), i64(m)))
+    return mat.reshape(m, m, order="F")
+
+
 def sort_schur_blocks(is_elim, sizes, couplings):
     el = np.ascontiguousarray(np.asarray(is_elim, bool), np.uint8)
     sz = np.ascontiguousarray(sizes, np.int64)
