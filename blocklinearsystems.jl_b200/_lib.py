@@ -119,6 +119,7 @@ def gpu() -> C.CDLL:
             "bls_dense_solver_create": (C.c_int, [vp, i64, C.POINTER(vp)]),
             "bls_dense_solver_destroy": (C.c_int, [vp]),
             "bls_dense_cholesky": (C.c_int, [vp, C.c_int, vp, p64]),
+            "bls_dense_cholesky_shifted": (C.c_int, [vp, C.c_int, vp, C.c_double, vp, p64]),
             "bls_dense_cholesky_solve": (C.c_int, [vp, vp, vp]),
             "bls_block_jacobi_create": (C.c_int, [vp, i64, p64, C.POINTER(vp)]),
             "bls_block_jacobi_destroy": (C.c_int, [vp]),

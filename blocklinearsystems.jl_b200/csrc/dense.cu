@@ -48,13 +48,16 @@ struct DenseSolver {
   }
 };
 
-// W = S mirrored from its upper triangle, in FP64
+// W = S mirrored from its upper triangle, in FP64, plus lambda s_r[j] on the diagonal when s_r is given
 template <class T>
-__global__ void k_dense_load(int64_t n, const T* __restrict__ S, double* __restrict__ W, long long* __restrict__ status) {
+__global__ void k_dense_load(int64_t n, const T* __restrict__ S, double* __restrict__ W, double lambda, const double* __restrict__ s_r,
+                             long long* __restrict__ status) {
   if (blockIdx.x == 0 && threadIdx.x == 0) status[0] = -1;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * n; q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = q % n, j = q / n;
-    W[q] = (double)(i <= j ? S[i + n * j] : S[j + n * i]);
+    double v = (double)(i <= j ? S[i + n * j] : S[j + n * i]);
+    if (s_r && i == j) v += lambda * s_r[j];
+    W[q] = v;
   }
 }
 
@@ -576,7 +579,7 @@ static void launch_factor_body(DenseSolver* D, cudaStream_t s, cudaStream_t p) {
 }
 
 template <class T>
-static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
+static int factor(DenseSolver* D, const T* S, double lambda, const double* s_r, int64_t* failed_column) {
   if (!S) throw Error(BLS_EINVAL, "S is NULL");
   cudaStream_t s = D->ctx->stream;
   const int64_t n = D->n;
@@ -592,7 +595,7 @@ static int factor(DenseSolver* D, const T* S, int64_t* failed_column) {
     BLS_CUDA(cudaFuncSetAttribute(k_syrk_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
     BLS_CUDA(cudaFuncSetAttribute(k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL_SMEM));
   }
-  k_dense_load<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n * n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, S, W, st);
+  k_dense_load<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n * n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, S, W, lambda, s_r, st);
   if (!D->factor_graph) {
     if (!D->cap_stream) BLS_CUDA(cudaStreamCreateWithFlags(&D->cap_stream, cudaStreamNonBlocking));
     BLS_CUDA(cudaStreamBeginCapture(D->cap_stream, cudaStreamCaptureModeThreadLocal));
@@ -664,8 +667,19 @@ int bls_dense_solver_destroy(bls_dense_solver* D) {
 int bls_dense_cholesky(bls_dense_solver* D, int dtype, const void* S, int64_t* failed_column) {
   DENSE_GUARD({
     if (!D) throw Error(BLS_EINVAL, "solver is NULL");
-    if (dtype == BLS_F64) return factor<double>(D, (const double*)S, failed_column);
-    if (dtype == BLS_F32) return factor<float>(D, (const float*)S, failed_column);
+    if (dtype == BLS_F64) return factor<double>(D, (const double*)S, 0.0, nullptr, failed_column);
+    if (dtype == BLS_F32) return factor<float>(D, (const float*)S, 0.0, nullptr, failed_column);
+    throw Error(BLS_EINVAL, "unknown dtype");
+  })
+}
+
+int bls_dense_cholesky_shifted(bls_dense_solver* D, int dtype, const void* S, double lambda, const double* s_r, int64_t* failed_column) {
+  DENSE_GUARD({
+    if (!D || !s_r) throw Error(BLS_EINVAL, "null argument");
+    if (!(std::isfinite(lambda) && lambda >= 0))
+      throw Error(BLS_EINVAL, "lambda must be finite and non-negative, got " + std::to_string(lambda));
+    if (dtype == BLS_F64) return factor<double>(D, (const double*)S, lambda, s_r, failed_column);
+    if (dtype == BLS_F32) return factor<float>(D, (const float*)S, lambda, s_r, failed_column);
     throw Error(BLS_EINVAL, "unknown dtype");
   })
 }

@@ -34,11 +34,18 @@ class DenseCholesky:
         context(self.device)
         return self._h
 
-    def factor(self, S: torch.Tensor) -> bool:
-        """Factor S (column-major n x n, float64 or float32, its upper triangle read). False: S is not positive definite."""
+    def factor(self, S: torch.Tensor, lam: float | None = None, s_r: torch.Tensor | None = None) -> bool:
+        """Factor S (column-major n x n, float64 or float32, its upper triangle read), or S + lam diag(s_r) when s_r is
+        given (the QR route's damped reduced normal equations, src/qr_linear_systems.jl:315-322). False: not positive
+        definite."""
         T = _dtype_code(_dev(S, "S", self.n * self.n))
         fc = C.c_int64(0)
-        rc = check(_lib.gpu().bls_dense_cholesky(self.handle, T, dptr(S), C.byref(fc)))
+        if s_r is None:
+            rc = check(_lib.gpu().bls_dense_cholesky(self.handle, T, dptr(S), C.byref(fc)))
+        else:
+            _dev(s_r, "s_r", self.n, torch.float64)
+            rc = check(_lib.gpu().bls_dense_cholesky_shifted(self.handle, T, dptr(S), float(0.0 if lam is None else lam), dptr(s_r),
+                                                             C.byref(fc)))
         self.failed_column = int(fc.value)
         return rc != BLS_NOT_PD
 

@@ -371,6 +371,12 @@ int bls_dense_solver_destroy(bls_dense_solver* solver);
 int bls_dense_cholesky(bls_dense_solver* solver, int dtype, const void* S_dev, int64_t* failed_column);
 int bls_dense_cholesky_solve(bls_dense_solver* solver, const double* g_dev, double* x_dev);
 
+/* The same factorisation of S + lambda diag(s_r) (s_r a device vector of n FP64 entries, added to the diagonal in FP64
+ * as S is read): the damped reduced normal equations of the QR route, J~'J~ from bls_reduced_normal_dense plus
+ * lambda s_r (src/qr_linear_systems.jl:315-322). lambda must be finite and non-negative (BLS_EINVAL). */
+int bls_dense_cholesky_shifted(bls_dense_solver* solver, int dtype, const void* S_dev, double lambda, const double* s_r_dev,
+                               int64_t* failed_column);
+
 /* prepare_scale! (src/conditioning.jl:60-87) of an EliminationConditioning: s[n] = the conditioning scale of each
  * variable (conditioning_scale, :29-36: the power of two nearest on a log scale to 1/(1e-12 + sqrt|d_j + lambda sc_j|),
  * at least floatmin of dtype, 1 for a non-finite entry), computed for every variable when stale is set, else only when

@@ -110,3 +110,37 @@ def test_one_solver_many_systems(bls, n):
             gd = torch.from_numpy(g).to(DEV)
             x = D.solve(gd, gd if k == 1 else None)   # the second solve in place
             assert relerr(x.cpu().numpy(), np.linalg.solve(As, g)) <= 1e-10, (trial, k)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+@pytest.mark.parametrize("name", ["bundle adjustment", "mixed dimensions", "free groups"])
+def test_qr_route_damped_normal_equations(bls, name, dtype):
+    """The QR route's dense reduced solve on the device (src/qr_linear_systems.jl:315-322): reduce_qr, J~'J~ and J~'r~
+    by reduced_normal_dense, then the Cholesky of J~'J~ + lambda diag(s_r) and the solve; against a host solve of the
+    same stored J~'J~ damped on the host, within 1e-10. lambda must be finite and non-negative."""
+    from qr_fixtures import QR_FIXTURES, fill_tables
+    rng = np.random.default_rng(11)
+    fx = QR_FIXTURES[name](rng)
+    st = bls.SchurStructure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    j = bls.SchurJacobianStructure.positional(st, fx["e_rows"], fx.get("free_rows", ()), fx.get("free_retained", ()))
+    Rw, Rr, _, _ = fill_tables(j, rng)
+    npdt = np.float32 if dtype == torch.float32 else np.float64
+    ws = bls.QRReductionWorkspace(j, None, dtype)
+    J = bls.SchurBlockJacobian(j, dtype, data=torch.from_numpy(Rw.astype(npdt)).to(DEV), r=torch.from_numpy(Rr).to(DEV))
+    lam = 1e-3
+    assert bls.reduce_qr(ws, J, torch.from_numpy(0.5 + rng.random(j.schur.ne)).to(DEV), lam)
+    nr = j.schur.nr
+    S = torch.zeros(nr * nr, dtype=dtype, device=DEV)
+    g = torch.zeros(nr, dtype=torch.float64, device=DEV)
+    bls.reduced_normal_dense(S, g, ws)
+    s_r = 0.5 + rng.random(nr)
+    A = S.double().cpu().numpy().reshape(nr, nr, order="F")
+    A = np.triu(A) + np.triu(A, 1).T + np.diag(lam * s_r)
+    D = bls.DenseCholesky(nr)
+    sr = torch.from_numpy(s_r).to(DEV)
+    assert D.factor(S, lam, sr) and D.failed_column == 0
+    x = D.solve(g)
+    assert relerr(x.cpu().numpy(), np.linalg.solve(A, g.cpu().numpy())) <= 1e-10
+    for bad in (-1e-3, float("nan"), float("inf")):
+        with pytest.raises(bls.ArgumentError):
+            D.factor(S, bad, sr)
