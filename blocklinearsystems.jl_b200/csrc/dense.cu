@@ -352,45 +352,65 @@ __global__ void __launch_bounds__(256, 4) k_syrk_tiles(int64_t n, double* __rest
     }
 }
 
-// The forward substitution of one diagonal tile [d0, d0 + dnb) of L held in t (lower triangle) by one warp: lanes own
-// rows lane and lane + 32, start from ys (shared) and write y; per column the owner's value times 1 / L[c, c] (held in
-// registers, dlo / dhi) is broadcast by shuffle, so the column chain is a multiply, a shuffle and a fused multiply-add.
+// The diagonal tile [d0, d0 + dnb) of L into t for one warp's substitution, by 256 threads (all 16 loads of a thread
+// in flight), pre-scaled so that a column step is one shuffle and one fused multiply-add: forward (rows_scaled = 0),
+// t[r][c] = L[r][c] / L[c][c] for r > c; backward (rows_scaled = 1), t[r][c] = L[r][c] / L[r][r] for r > c; zero on and
+// above the diagonal and outside the tile.
+__device__ __forceinline__ void load_scaled_tile(double (*t)[NB + 1], const double* __restrict__ W, const double* __restrict__ dinv,
+                                                 int64_t n, int64_t d0, int dnb, int rows_scaled, int tid) {
+  double v[NB * NB / 256];
+#pragma unroll
+  for (int k = 0; k < NB * NB / 256; ++k) {
+    const int e = tid + 256 * k, rr = e & 63, cc = e >> 6;
+    v[k] = (rr < dnb && cc < rr) ? W[(d0 + rr) + n * (d0 + cc)] * dinv[d0 + (rows_scaled ? rr : cc)] : 0.0;
+  }
+#pragma unroll
+  for (int k = 0; k < NB * NB / 256; ++k) {
+    const int e = tid + 256 * k;
+    t[e & 63][e >> 6] = v[k];
+  }
+}
+
+// The forward substitution of one diagonal tile [d0, d0 + dnb) by one warp, t from load_scaled_tile (forward): lanes
+// own rows lane and lane + 32 and start from ys (shared); per column the finished row value is shuffled from its lane
+// and every lane subtracts its scaled entry times it, so the column chain is a shuffle and a fused multiply-add; the
+// rows are multiplied by 1 / L[r][r] (dlo, dhi) once at the end and written to y.
 __device__ __forceinline__ void tile_forward(const double (*t)[NB + 1], double dlo, double dhi, const double* ys,
                                              double* __restrict__ y, int64_t d0, int dnb, int lane) {
   double y0 = ys[lane], y1 = ys[lane + 32];
-#pragma unroll 2
-  for (int c = 0; c < dnb; ++c) {
-    const double v = __shfl_sync(0xffffffffu, c < 32 ? y0 * dlo : y1 * dhi, c & 31);
-    if (c < 32) {
-      if (lane == c) y0 = v;
-      else if (lane > c) y0 -= t[lane][c] * v;
-    } else if (lane == c - 32) {
-      y1 = v;
-    }
-    if (lane + 32 > c && lane + 32 < dnb) y1 -= t[lane + 32][c] * v;
+#pragma unroll 8
+  for (int c = 0; c < 32; ++c) {
+    const double yc = __shfl_sync(0xffffffffu, y0, c);
+    y0 = fma(-t[lane][c], yc, y0);
+    y1 = fma(-t[lane + 32][c], yc, y1);
   }
-  if (lane < dnb) y[d0 + lane] = y0;
-  if (lane + 32 < dnb) y[d0 + 32 + lane] = y1;
+#pragma unroll 8
+  for (int c = 32; c < NB; ++c) {
+    const double yc = __shfl_sync(0xffffffffu, y1, c - 32);
+    y1 = fma(-t[lane + 32][c], yc, y1);
+  }
+  if (lane < dnb) y[d0 + lane] = y0 * dlo;
+  if (lane + 32 < dnb) y[d0 + 32 + lane] = y1 * dhi;
 }
 
-// The backward substitution (L' x = y) of one diagonal tile [d0, d0 + dnb), as tile_forward.
+// The backward substitution (L' x = y) of one diagonal tile [d0, d0 + dnb), t from load_scaled_tile (backward), as
+// tile_forward from the last column to the first.
 __device__ __forceinline__ void tile_backward(const double (*t)[NB + 1], double dlo, double dhi, const double* ys,
                                               double* __restrict__ y, int64_t d0, int dnb, int lane) {
   double y0 = ys[lane], y1 = ys[lane + 32];
-#pragma unroll 2
-  for (int c = dnb - 1; c >= 0; --c) {
-    const double v = __shfl_sync(0xffffffffu, c < 32 ? y0 * dlo : y1 * dhi, c & 31);
-    if (c >= 32) {
-      if (lane == c - 32) y1 = v;
-      else if (lane < c - 32) y1 -= t[c][lane + 32] * v;
-      y0 -= t[c][lane] * v;
-    } else {
-      if (lane == c) y0 = v;
-      else if (lane < c) y0 -= t[c][lane] * v;
-    }
+#pragma unroll 8
+  for (int c = NB - 1; c >= 32; --c) {
+    const double yc = __shfl_sync(0xffffffffu, y1, c - 32);
+    y1 = fma(-t[c][lane + 32], yc, y1);
+    y0 = fma(-t[c][lane], yc, y0);
   }
-  if (lane < dnb) y[d0 + lane] = y0;
-  if (lane + 32 < dnb) y[d0 + 32 + lane] = y1;
+#pragma unroll 8
+  for (int c = 31; c >= 0; --c) {
+    const double yc = __shfl_sync(0xffffffffu, y0, c);
+    y0 = fma(-t[c][lane], yc, y0);
+  }
+  if (lane < dnb) y[d0 + lane] = y0 * dlo;
+  if (lane + 32 < dnb) y[d0 + 32 + lane] = y1 * dhi;
 }
 
 // One forward step of L y = g, y in place: rows [d0, n) take the update from the solved tile [d0 - NB, d0) (when
@@ -416,7 +436,7 @@ __global__ void __launch_bounds__(256) k_fwd_step(int64_t n, const double* __res
   }
   if (q == 0 && i < n) yi = y[i];
   if (blockIdx.x == 0) {
-    load_tile(t, W, n, d0, dnb, tid);
+    load_scaled_tile(t, W, dinv, n, d0, dnb, 0, tid);
     if (tid < 32) {
       if (tid < dnb) dlo = dinv[d0 + tid];
       if (tid + 32 < dnb) dhi = dinv[d0 + 32 + tid];
@@ -464,7 +484,7 @@ __global__ void __launch_bounds__(256) k_bwd_step(int64_t n, const double* __res
   const double yold = lane < 8 ? y[row0 + warp * 8 + lane] : 0.0;
   double dlo = 0.0, dhi = 0.0;
   if (blockIdx.x == 0) {
-    load_tile(t, W, n, row0, NB, tid);
+    load_scaled_tile(t, W, dinv, n, row0, NB, 1, tid);
     if (tid < 32) {
       dlo = dinv[row0 + tid];
       dhi = dinv[row0 + 32 + tid];
@@ -501,7 +521,7 @@ __global__ void __launch_bounds__(32) k_bwd_last(int64_t n, const double* __rest
   const int lane = threadIdx.x, dnb = (int)(n - d0);
   for (int e = lane; e < NB * NB; e += 32) {
     const int rr = e & 63, cc = e >> 6;
-    if (rr < dnb && cc <= rr) t[rr][cc] = W[(d0 + rr) + n * (d0 + cc)];
+    t[rr][cc] = (rr < dnb && cc < rr) ? W[(d0 + rr) + n * (d0 + cc)] * dinv[d0 + rr] : 0.0;
   }
   ys[lane] = lane < dnb ? y[d0 + lane] : 0.0;
   ys[lane + 32] = lane + 32 < dnb ? y[d0 + 32 + lane] : 0.0;
