@@ -32,7 +32,7 @@ struct PCGPlan {
   bool cols6 = false;
   DevBuf c_ptr, c_base, c_xo, c_stride;
   DevBuf ref_r, ref_d, ref_y;   // refined solve: outer residual, correction, operator product (FP64, allocated at its first call)
-  int K = 16;               // iterations per replayed graph
+  int K = 8;                // iterations per replayed graph
   cudaGraphExec_t graph = nullptr;
   const void* graph_S = nullptr;
   const double* graph_x = nullptr;
