@@ -281,9 +281,9 @@ constexpr int SYRK_SMEM = SYRK_STAGES * 2 * SYRK_KC * NB * (int)sizeof(double); 
 // One CTA of 256 threads per 64 x 64 output tile of the lower triangle (tiles listed by their index in it). The two
 // row panels pass through a three-stage ring of 16-column chunks in shared memory, copied asynchronously (cp.async,
 // rows past n zero-filled) two chunks ahead of the products (48 KB and at most 64 registers a thread, so four CTAs fit
-// an SM); each thread accumulates a 4 x 4 block (rows 2 tx + {0, 1, 32, 33}, columns 2 ty + {0, 1, 32, 33}) from
-// 16-byte shared loads with FP64 fused multiply-adds (the FP64 tensor-core form, mma.sync m8n8k4 fragments per warp,
-// measured 1.3x slower here).
+// an SM), and the output tile is fetched the same way into the two free stages during the last chunk. Each thread
+// accumulates a 4 x 4 block (rows 2 tx + {0, 1, 32, 33}, columns 2 ty + {0, 1, 32, 33}) from 16-byte shared loads with
+// FP64 fused multiply-adds (the FP64 tensor-core form, mma.sync m8n8k4 fragments per warp, measured 1.3x slower here).
 __global__ void __launch_bounds__(256, 4) k_syrk_tiles(int64_t n, double* __restrict__ W, int64_t k0, int rest,
                                                        const long long* __restrict__ status) {
   constexpr int KC = SYRK_KC, NCH = NB / KC;
@@ -322,11 +322,24 @@ __global__ void __launch_bounds__(256, 4) k_syrk_tiles(int64_t n, double* __rest
   for (int p = 0; p < 4; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[p][q] = 0.0;
+  static_assert(NCH == 4 && SYRK_STAGES == 3, "the output tile is prefetched into stages 1 and 2 during the last chunk");
+  double (*O)[NB] = reinterpret_cast<double (*)[NB]>(syrk_smem + 2 * KC * NB);   // stages 1 and 2: 64 x 64, O[col][row]
   for (int ch = 0; ch < NCH; ++ch) {
     if (ch + 2 < NCH) issue(ch + 2);   // into the stage chunk ch - 1 used: every thread passed the barrier after it
     else cp_async_commit();           // an empty group keeps the count of groups in flight uniform
     cp_async_wait<2>();
     __syncthreads();
+    if (ch == NCH - 1) {
+      // stages 1 and 2 are free (chunks 1 and 2 are done): fetch the output tile for the read-modify-write while the
+      // last chunk's products run
+#pragma unroll
+      for (int k = 0; k < NB * NB / 256; ++k) {
+        const int e = tid + 256 * k, col = e >> 6, row = e & 63;
+        const bool v = bi + row < n && bj + col < n;
+        cp_async8(&O[col][row], v ? W + (bi + row) + n * (bj + col) : W, v ? 8 : 0);
+      }
+      cp_async_commit();
+    }
     double (*A)[NB] = Pi(ch % SYRK_STAGES);
     double (*B)[NB] = Pj(ch % SYRK_STAGES);
 #pragma unroll 4
@@ -343,12 +356,15 @@ __global__ void __launch_bounds__(256, 4) k_syrk_tiles(int64_t n, double* __rest
     }
     __syncthreads();
   }
+  cp_async_wait<0>();
+  __syncthreads();
 #pragma unroll
   for (int p = 0; p < 4; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int64_t oi = bi + 2 * tx + (p & 1) + 32 * (p >> 1), oj = bj + 2 * ty + (q & 1) + 32 * (q >> 1);
-      if (oi < n && oj <= oi) W[oi + n * oj] -= acc[p][q];
+      const int ri = 2 * tx + (p & 1) + 32 * (p >> 1), cj = 2 * ty + (q & 1) + 32 * (q >> 1);
+      const int64_t oi = bi + ri, oj = bj + cj;
+      if (oi < n && oj <= oi) W[oi + n * oj] = O[cj][ri] - acc[p][q];
     }
 }
 
