@@ -86,6 +86,7 @@ struct SchurPlan {
   DevBuf Einv64, Einv32, z, status;
   DevBuf acc1;     // one FP64 accumulator (bls_hessian_bilinear)
   DevBuf w_apply;  // per point E^-1 C x of bls_schur_apply_elimination (ne doubles, allocated at its first call)
+  DevBuf t_apply;  // per point C x of bls_schur_apply_elimination on the 3-variable fast path (3 neblocks doubles)
   DevBuf Einv12;   // fast36: E^-1 per point in the element type of the pair products, padded to 12 entries (16-byte rows)
   Status* host_status = nullptr;   // pinned
   int last_dtype = -1;
@@ -602,32 +603,83 @@ __device__ __forceinline__ void coupling18(const T* __restrict__ C, int64_t c, T
     for (int i = 0; i < 9; ++i) { const float2 v = __ldg(q + i); out[2 * i] = v.x; out[2 * i + 1] = v.y; }
   }
 }
+// t_e = C_e x for every point, a thread per coupling (couplings of a point are consecutive): each warp stages its 32
+// consecutive coupling blocks through shared memory with coalesced 8-byte loads, forms C_c x_r for its coupling, and
+// sums the couplings of each point by a segmented scan across the warp; a point that lies inside one warp is stored,
+// one split across warps is added atomically into t (zeroed before).
 template <class T>
-__global__ void __launch_bounds__(256) k_point_apply36(int64_t neb, const int32_t* __restrict__ eliminated_ptr,
-                                                       const int32_t* __restrict__ entry_retained, const T* __restrict__ C,
-                                                       const double* __restrict__ Einv64, const double* __restrict__ x,
-                                                       double* __restrict__ w, const Status* __restrict__ st) {
-  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (e >= neb || !live(st)) return;
-  double t[3] = {0.0, 0.0, 0.0};
-  const int c0 = eliminated_ptr[e], c1 = eliminated_ptr[e + 1];
-#pragma unroll 2
-  for (int c = c0; c < c1; ++c) {
+__global__ void __launch_bounds__(256) k_point_ct36(int64_t ncoup, const int32_t* __restrict__ eliminated_ptr,
+                                                    const int32_t* __restrict__ entry_eliminated, const int32_t* __restrict__ entry_retained,
+                                                    const T* __restrict__ C, const double* __restrict__ x, double* __restrict__ t,
+                                                    const Status* __restrict__ st) {
+  __shared__ T cs[8][32 * 18];
+  if (!live(st)) return;   // uniform
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t cw0 = (blockIdx.x * (int64_t)blockDim.x) + 32 * wid;   // the warp's first coupling
+  if (cw0 >= ncoup) return;   // uniform per warp
+  const int nw = (int)(ncoup - cw0 < 32 ? ncoup - cw0 : 32);
+  // the warp's blocks, in pairs of entries (C is aligned to two entries)
+  {
+    using V2 = typename std::conditional<std::is_same<T, double>::value, double2, float2>::type;
+    const V2* src = reinterpret_cast<const V2*>(C + 18 * cw0);
+    V2* dst = reinterpret_cast<V2*>(cs[wid]);
+    for (int i = lane; i < 9 * nw; i += 32) dst[i] = __ldg(src + i);
+  }
+  __syncwarp();
+  const int64_t c = cw0 + lane;
+  const bool valid = lane < nw;
+  int e = valid ? __ldg(entry_eliminated + c) : -1 - lane;   // lanes past the end: segments of their own
+  double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+  if (valid) {
     const int r = __ldg(entry_retained + c);
     const double2* xp = reinterpret_cast<const double2*>(x + 6 * (int64_t)r);
     const double2 a = __ldg(xp), b = __ldg(xp + 1), d = __ldg(xp + 2);
     const double xr[6] = {a.x, a.y, b.x, b.y, d.x, d.y};
-    T cb[18];
-    coupling18<T>(C, c, cb);
+    const T* cb = cs[wid] + 18 * lane;
 #pragma unroll
-    for (int j = 0; j < 6; ++j)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) t[i] += (double)cb[i + 3 * j] * xr[j];
+    for (int j = 0; j < 6; ++j) {
+      t0 += (double)cb[3 * j] * xr[j];
+      t1 += (double)cb[3 * j + 1] * xr[j];
+      t2 += (double)cb[3 * j + 2] * xr[j];
+    }
   }
-  const double* inv = Einv64 + 9 * e;
 #pragma unroll
-  for (int i = 0; i < 3; ++i) w[3 * e + i] = inv[i] * t[0] + inv[i + 3] * t[1] + inv[i + 6] * t[2];
+  for (int off = 1; off < 32; off <<= 1) {
+    const double u0 = __shfl_up_sync(0xffffffffu, t0, off), u1 = __shfl_up_sync(0xffffffffu, t1, off),
+                 u2 = __shfl_up_sync(0xffffffffu, t2, off);
+    const int eu = __shfl_up_sync(0xffffffffu, e, off);
+    if (lane >= off && eu == e) {
+      t0 += u0;
+      t1 += u1;
+      t2 += u2;
+    }
+  }
+  const int en = __shfl_down_sync(0xffffffffu, e, 1);
+  if (valid && (lane == 31 || en != e)) {   // the last coupling of its point within the warp
+    double* te = t + 3 * (int64_t)e;
+    if (__ldg(eliminated_ptr + e) >= cw0 && __ldg(eliminated_ptr + e + 1) <= cw0 + nw) {
+      te[0] = t0;
+      te[1] = t1;
+      te[2] = t2;
+    } else {
+      atomicAdd(te, t0);
+      atomicAdd(te + 1, t1);
+      atomicAdd(te + 2, t2);
+    }
+  }
 }
+
+// w_e = E^-1 t_e (FP64), a thread per point
+__global__ void __launch_bounds__(256) k_point_einv36(int64_t neb, const double* __restrict__ Einv64, const double* __restrict__ t,
+                                                      double* __restrict__ w, const Status* __restrict__ st) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= neb || !live(st)) return;
+  const double* inv = Einv64 + 9 * e;
+  const double t0 = t[3 * e], t1 = t[3 * e + 1], t2 = t[3 * e + 2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) w[3 * e + i] = inv[i] * t0 + inv[i + 3] * t1 + inv[i + 6] * t2;
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) k_gather_ctw36(int64_t nrb, const int32_t* __restrict__ retained_ptr, const int32_t* __restrict__ retained_entry,
                                                       const int32_t* __restrict__ entry_eliminated, const T* __restrict__ C,
@@ -1706,7 +1758,7 @@ static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
                           &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h,
-                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g, &P->w_apply, &P->acc1,
+                          &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g, &P->w_apply, &P->t_apply, &P->acc1,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
   for (auto* x : bufs) b += (int64_t)x->bytes;
@@ -2123,9 +2175,15 @@ static int apply_elimination(SchurPlan* P, double* y, const double* y0, const do
     if (reinterpret_cast<uintptr_t>(C) % (2 * sizeof(T)) != 0)
       throw Error(BLS_EINVAL, "C_data must be aligned to two elements (the device reads coupling blocks in pairs of entries)");
     if (reinterpret_cast<uintptr_t>(x) % 16 != 0) throw Error(BLS_EINVAL, "x must be 16-byte aligned");
-    if (P->neblocks > 0)
-      k_point_apply36<T><<<grid_for(P->neblocks, 256), 256, 0, s>>>(P->neblocks, P->eliminated_ptr.as<int32_t>(), P->entry_retained.as<int32_t>(),
-                                                                    C, P->Einv64.as<double>(), x, P->w_apply.as<double>(), st);
+    if (P->neblocks > 0) {
+      if (!P->t_apply.p) P->t_apply.alloc(sizeof(double) * 3 * (size_t)P->neblocks);
+      BLS_CUDA(cudaMemsetAsync(P->t_apply.p, 0, sizeof(double) * 3 * (size_t)P->neblocks, s));
+      k_point_ct36<T><<<grid_for(P->ncoup, 256), 256, 0, s>>>(P->ncoup, P->eliminated_ptr.as<int32_t>(), P->entry_eliminated.as<int32_t>(),
+                                                              P->entry_retained.as<int32_t>(), C, x, P->t_apply.as<double>(), st);
+      k_point_einv36<<<grid_for(P->neblocks, 256), 256, 0, s>>>(P->neblocks, P->Einv64.as<double>(), P->t_apply.as<double>(),
+                                                                 P->w_apply.as<double>(), st);
+      P->launches += 1;
+    }
     if (P->nrblocks > 0)
       k_gather_ctw36<T><<<grid_for(P->nrblocks * 32, 256), 256, 0, s>>>(P->nrblocks, P->retained_ptr.as<int32_t>(), P->retained_entry.as<int32_t>(),
                                                                         P->entry_eliminated.as<int32_t>(), C, P->w_apply.as<double>(), y0, y, st);
