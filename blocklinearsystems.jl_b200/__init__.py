@@ -8,7 +8,8 @@ Device reduction:        SchurReductionWorkspace, reset_schur_sparse / reset_sch
                          reduce_schur_sparse / reduce_schur_dense, backsubstitute, scatter_copy,
                          symmetrifyfull / symmetrifyfull_
 QR elimination:          SchurJacobianStructure, SchurBlockJacobian, QRReductionWorkspace, reduce_qr, qr_backsubstitute,
-                         reduced_normal_sparse / reduced_normal_dense, reduced_diagonal_blocks, free_block_pairs
+                         reduced_normal_sparse / reduced_normal_dense, reduced_diagonal_blocks, free_block_pairs,
+                         reduced_residual, reduced_jacobian / reduced_jacobian_sparse, build_reduced_jacobian_pattern
 Reduced solve:           BlockJacobi, factor_diagonal_blocks, solve_diagonal_blocks, PCGWorkspace (block-Jacobi PCG)
 Learned preconditioner:  gnn.LearnedPreconditioner, gnn.train, gnn.init_params
 Batches:                 batch.BatchedReduction (uneven problems as one plan, one CUDA graph)
@@ -20,7 +21,8 @@ from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce
                         prepare_scale, reset_reduce_schur_sparse_host, reset_schur_dense, reset_schur_sparse, scatter_copy,
                         symmetrifyfull, symmetrifyfull_)
 from .qr import (QRReductionWorkspace, SchurBlockJacobian, assemble_hessian, jtj_diag, jtj_quadform, jtr, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
-                 reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse)
+                 reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse, reduced_residual,
+                 reduced_jacobian, reduced_jacobian_sparse, build_reduced_jacobian_pattern)
 from .pcg import BlockJacobi, PCGResult, PCGWorkspace, RefinedResult, factor_diagonal_blocks, solve_diagonal_blocks
 from .dense import DenseCholesky
 from . import batch, gnn, scenes
@@ -30,6 +32,7 @@ __all__ = [
     "build_schur_pattern", "sparse_with_map", "SchurReductionWorkspace", "backsubstitute", "context", "reduce_schur_dense",
     "reduce_schur_sparse", "reset_reduce_schur_sparse_host", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
     "SchurBlockJacobian", "SchurJacobianStructure", "assemble_hessian", "jtj_diag", "jtj_quadform", "jtr", "prepare_scale", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
-    "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "BlockJacobi", "PCGResult", "PCGWorkspace", "RefinedResult", "DenseCholesky",
+    "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "reduced_residual", "reduced_jacobian",
+    "reduced_jacobian_sparse", "build_reduced_jacobian_pattern", "BlockJacobi", "PCGResult", "PCGWorkspace", "RefinedResult", "DenseCholesky",
     "factor_diagonal_blocks", "solve_diagonal_blocks", "gnn", "batch", "symmetrifyfull", "symmetrifyfull_",
 ]

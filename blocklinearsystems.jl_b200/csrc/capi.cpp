@@ -242,6 +242,39 @@ int bls_qr_structure_positional(const bls_structure* st, const int64_t* e_rows, 
   })
 }
 
+int64_t bls_reduced_jacobian_pattern(const bls_qr_structure* q, int64_t* colptr, int64_t* rowval) {
+  if (!q) {
+    bls::set_error("structure is NULL");
+    return BLS_EINVAL;
+  }
+  const Structure& st = q->schur;
+  std::vector<int64_t> cp((size_t)st.nr + 1, 0);
+  auto height = [&](int64_t r) {
+    int64_t h = 0;
+    for (int64_t k = q->retained_ptr[r]; k < q->retained_ptr[r + 1]; ++k) {
+      const int64_t t = q->entry_table[q->retained_entry[k]];
+      h += q->table_nrows[t] - q->table_top[t];
+    }
+    return h;
+  };
+  for (int64_t r = 0; r < st.nrblocks; ++r) {
+    const int64_t h = height(r), ro = st.boffsets_r[r];
+    for (int64_t j = 0; j < st.r_dims[r]; ++j) cp[ro + j + 1] = cp[ro + j] + h;
+  }
+  const int64_t nnz = cp[st.nr];
+  if (colptr) std::memcpy(colptr, cp.data(), sizeof(int64_t) * cp.size());
+  if (rowval)
+    for (int64_t r = 0; r < st.nrblocks; ++r)
+      for (int64_t j = 0; j < st.r_dims[r]; ++j) {
+        int64_t p = cp[st.boffsets_r[r] + j];
+        for (int64_t k = q->retained_ptr[r]; k < q->retained_ptr[r + 1]; ++k) {
+          const int64_t t = q->entry_table[q->retained_entry[k]];
+          for (int64_t i = 0; i < q->table_nrows[t] - q->table_top[t]; ++i) rowval[p++] = q->reduced_offsets[t] + i;
+        }
+      }
+  return nnz;
+}
+
 int64_t bls_qr_structure_field(const bls_qr_structure* q, const char* name, int64_t* out) {
   if (!q || !name) return -1;
   const std::string f(name);

@@ -59,6 +59,14 @@ struct QRPlan {
   // per retained block its entries in ascending order (the structure's retained_ptr / retained_entry), per entry its table
   DevBuf q_rptr, q_rent, u_tab;
   DevBuf q_total;   // one FP64 accumulator (jtj_quadform)
+  // the reduced problem (reduced_residual!, reduced_jacobian!): per table its first reduced row (t_red, nt + 1), the
+  // CSC column pointers of J~ (build_reduced_jacobian_pattern, nr + 1, also kept on the host to check a caller's
+  // pattern) and per entry the position of its run within each column of its retained block
+  DevBuf t_red, jt_colptr, u_runpos;
+  int64_t red_nrows = 0;
+  std::vector<int64_t> h_red, h_jt_colptr;
+  std::vector<int32_t> h_rptr, h_rent_tab;   // per retained block, the tables of its entries in ascending entry order
+  std::vector<int64_t> h_boff_r, h_rdims;
   DevBuf status;
   long long* host_status = nullptr;
   int64_t launches = 0;
@@ -563,6 +571,117 @@ __global__ void k_fill_t(T* __restrict__ p, int64_t n) {
 // ------------------------------------------------------------------------------------------------------------------
 // Plan
 // ------------------------------------------------------------------------------------------------------------------
+// reduced_residual! (src/qr_reduced.jl:227-243): r~, a warp per table copying its bottom residual rows
+__global__ void __launch_bounds__(256) k_reduced_residual(int64_t nt, const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
+                                                          const int64_t* __restrict__ t_res, const int64_t* __restrict__ t_red,
+                                                          const double* __restrict__ Fr, double* __restrict__ rt) {
+  const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= nt) return;
+  const int n = t_rows[t] - t_top[t];
+  const double* src = Fr + t_res[t] + t_top[t];
+  double* dst = rt + t_red[t];
+  for (int i = lane; i < n; i += 32) dst[i] = src[i];
+}
+
+// reduced_jacobian!(Jt::Matrix, ...) (src/qr_reduced.jl:245-272): a warp per table writes the bottom rows of each
+// entry's columns of the factored table into J~ (column-major, leading dimension ld = reduced_nrows; zeroed before)
+template <class T>
+__global__ void __launch_bounds__(256) k_reduced_jacobian_dense(int64_t nt, const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
+                                                                const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_red,
+                                                                const int32_t* __restrict__ t_ptr, const int32_t* __restrict__ u_ret,
+                                                                const int32_t* __restrict__ u_col, const int32_t* __restrict__ r_dims,
+                                                                const int32_t* __restrict__ boff_r, const T* __restrict__ F, T* __restrict__ Jt,
+                                                                int64_t ld) {
+  const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= nt) return;
+  const int M = t_rows[t], top = t_top[t], n = M - top;
+  const int64_t raw = t_raw[t], red = t_red[t];
+  for (int u = t_ptr[t]; u < t_ptr[t + 1]; ++u) {
+    const int r = u_ret[u], dr = r_dims[r], c0 = u_col[u];
+    const int64_t ro = boff_r[r];
+    for (int q = lane; q < dr * n; q += 32) {
+      const int j = q / n, i = q - j * n;
+      Jt[(red + i) + ld * (ro + j)] = F[raw + (int64_t)(c0 + j) * M + top + i];
+    }
+  }
+}
+
+// reduced_jacobian!(Jt::SparseMatrixCSC, ...) (src/qr_reduced.jl:336-370): a warp per entry writes its run of
+// bottom rows into every column of its retained block, at the run's position in the column
+template <class T>
+__global__ void __launch_bounds__(256) k_reduced_jacobian_sparse(int64_t nent, const int32_t* __restrict__ u_tab, const int32_t* __restrict__ t_rows,
+                                                                 const int32_t* __restrict__ t_top, const int64_t* __restrict__ t_raw,
+                                                                 const int32_t* __restrict__ u_ret, const int32_t* __restrict__ u_col,
+                                                                 const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                                                                 const int64_t* __restrict__ jt_colptr, const int64_t* __restrict__ u_runpos,
+                                                                 const T* __restrict__ F, T* __restrict__ nzval) {
+  const int64_t u = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (u >= nent) return;
+  const int t = u_tab[u], M = t_rows[t], top = t_top[t], n = M - top, r = u_ret[u], dr = r_dims[r];
+  const int64_t ro = boff_r[r], cb = t_raw[t] + (int64_t)u_col[u] * M + top, p = u_runpos[u];
+  for (int q = lane; q < dr * n; q += 32) {
+    const int j = q / n, i = q - j * n;
+    nzval[jt_colptr[ro + j] + p + i] = F[cb + (int64_t)j * M + i];
+  }
+}
+
+template <class T>
+static void reduced_jacobian_dense(QRPlan* P, T* Jt, const T* F, const double* Fr, double* rt) {
+  cudaStream_t s = P->ctx->stream;
+  const int64_t m = P->red_nrows;
+  if (m > 0) BLS_CUDA(cudaMemsetAsync(Jt, 0, sizeof(T) * (size_t)m * (size_t)P->nr, s));
+  const unsigned g = (unsigned)std::max(1, grid_for(P->ntables * 32, 256));
+  k_reduced_residual<<<g, 256, 0, s>>>(P->ntables, P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_res.as<int64_t>(), P->t_red.as<int64_t>(), Fr, rt);
+  k_reduced_jacobian_dense<T><<<g, 256, 0, s>>>(P->ntables, P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
+                                                P->t_red.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(),
+                                                P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), F, Jt, m);
+  P->launches += 2;
+  BLS_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static void reduced_jacobian_sparse(QRPlan* P, T* nzval, const T* F, const double* Fr, double* rt) {
+  cudaStream_t s = P->ctx->stream;
+  k_reduced_residual<<<(unsigned)std::max(1, grid_for(P->ntables * 32, 256)), 256, 0, s>>>(
+      P->ntables, P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_res.as<int64_t>(), P->t_red.as<int64_t>(), Fr, rt);
+  if (P->nentries > 0)
+    k_reduced_jacobian_sparse<T><<<(unsigned)grid_for(P->nentries * 32, 256), 256, 0, s>>>(
+        P->nentries, P->u_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(), P->u_ret.as<int32_t>(),
+        P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), P->jt_colptr.as<int64_t>(), P->u_runpos.as<int64_t>(), F, nzval);
+  P->launches += 2;
+  BLS_CUDA(cudaGetLastError());
+}
+
+// check_reduced_jacobian_pattern (src/qr_reduced.jl:312-334) of a caller's 0-based CSC, before any work: its size,
+// then per column of each retained block its height and the first row of every run; messages 1-based, as the
+// reference's
+static void check_jt_pattern(const QRPlan* P, int64_t nrows, int64_t ncols, const int64_t* colptr, const int64_t* rowval) {
+  if (nrows != P->red_nrows || ncols != P->nr)
+    throw Error(BLS_EDIM, "Jt has size (" + std::to_string(nrows) + ", " + std::to_string(ncols) + "), expected (" + std::to_string(P->red_nrows) +
+                              ", " + std::to_string(P->nr) + ")");
+  if (!colptr) throw Error(BLS_EINVAL, "the pattern of Jt is NULL");
+  for (int64_t r = 0; r < P->nrblocks; ++r)
+    for (int64_t c = P->h_boff_r[r]; c < P->h_boff_r[r] + P->h_rdims[r]; ++c) {
+      const int64_t h = P->h_jt_colptr[c + 1] - P->h_jt_colptr[c];
+      if (colptr[c + 1] - colptr[c] != h)
+        throw Error(BLS_EINVAL, "Jt does not have the pattern of build_reduced_jacobian_pattern: column " + std::to_string(c + 1) + " stores " +
+                                    std::to_string(colptr[c + 1] - colptr[c]) + " entries, expected " + std::to_string(h));
+      int64_t p = colptr[c];
+      for (int32_t k = P->h_rptr[r]; k < P->h_rptr[r + 1]; ++k) {
+        const int32_t t = P->h_rent_tab[k];
+        const int64_t n = P->h_red[t + 1] - P->h_red[t];
+        if (n != 0 && (!rowval || rowval[p] != P->h_red[t]))
+          throw Error(BLS_EINVAL, "Jt does not have the pattern of build_reduced_jacobian_pattern: column " + std::to_string(c + 1) +
+                                      " stores row " + (rowval ? std::to_string(rowval[p] + 1) : std::string("?")) + ", expected " +
+                                      std::to_string(P->h_red[t] + 1));
+        p += n;
+      }
+    }
+}
+
 static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
   if (!d || d->nrblocks < 1 || d->neblocks < 1 || d->ntables < d->neblocks) throw Error(BLS_EINVAL, "a QR plan needs retained blocks, eliminated blocks and their tables");
   std::unique_ptr<QRPlan> P(new QRPlan());
@@ -743,6 +862,30 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
     upload(P->q_rptr, rptr, s);
     upload(P->q_rent, rent, s);
     upload(P->u_tab, utab, s);
+    // the reduced problem: build_reduced_jacobian_pattern's column heights (the reduced rows of every table coupled to
+    // the column's retained block, tables in ascending order) and each entry's run position in those columns
+    P->h_red.assign((size_t)nt + 1, 0);
+    for (int64_t t = 0; t < nt; ++t) P->h_red[t + 1] = P->h_red[t] + d->table_nrows[t] - d->table_top[t];
+    P->red_nrows = P->h_red[nt];
+    P->h_jt_colptr.assign((size_t)nr + 1, 0);
+    P->h_boff_r = boff_r;
+    P->h_rdims.assign(d->r_dims, d->r_dims + nrb);
+    P->h_rptr = rptr;
+    P->h_rent_tab.resize((size_t)nent);
+    std::vector<int64_t> runpos((size_t)nent, 0);
+    for (int64_t r = 0; r < nrb; ++r) {
+      int64_t h = 0;
+      for (int32_t k = rptr[r]; k < rptr[r + 1]; ++k) {
+        const int32_t u = rent[k], t = utab[u];
+        P->h_rent_tab[k] = t;
+        runpos[u] = h;
+        h += d->table_nrows[t] - d->table_top[t];
+      }
+      for (int64_t j = 0; j < d->r_dims[r]; ++j) P->h_jt_colptr[boff_r[r] + j + 1] = P->h_jt_colptr[boff_r[r] + j] + h;
+    }
+    upload(P->t_red, P->h_red, s);
+    upload(P->jt_colptr, P->h_jt_colptr, s);
+    upload(P->u_runpos, runpos, s);
     P->q_total.alloc(sizeof(double));
   }
   upload(P->blk_stride, b_stride, s);
@@ -1043,6 +1186,53 @@ int bls_reduced_diagonal_blocks(bls_qr_plan* P, int dtype, void* D, const void* 
   QR_GUARD({
     if (dtype == BLS_F64) diagonal_blocks<double>(P, (double*)D, (const double*)F);
     else if (dtype == BLS_F32) diagonal_blocks<float>(P, (float*)D, (const float*)F);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+
+int bls_reduced_residual(bls_qr_plan* P, const double* Fr, double* rt, int64_t n_rt) {
+  QR_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (n_rt != P->red_nrows)
+      throw Error(BLS_EDIM, "rt has length " + std::to_string(n_rt) + ", expected " + std::to_string(P->red_nrows));
+    if (n_rt > 0 && (!Fr || !rt)) throw Error(BLS_EINVAL, "a device pointer is NULL");
+    k_reduced_residual<<<(unsigned)std::max(1, grid_for(P->ntables * 32, 256)), 256, 0, P->ctx->stream>>>(
+        P->ntables, P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_res.as<int64_t>(), P->t_red.as<int64_t>(), Fr, rt);
+    P->launches += 1;
+    BLS_CUDA(cudaGetLastError());
+    return BLS_OK;
+  })
+}
+
+int bls_reduced_jacobian_dense(bls_qr_plan* P, int dtype, const void* F, const double* Fr, void* Jt, int64_t nrows, int64_t ncols,
+                               double* rt, int64_t n_rt) {
+  QR_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (nrows != P->red_nrows || ncols != P->nr)
+      throw Error(BLS_EDIM, "Jt has size (" + std::to_string(nrows) + ", " + std::to_string(ncols) + "), expected (" +
+                                std::to_string(P->red_nrows) + ", " + std::to_string(P->nr) + ")");
+    if (n_rt != P->red_nrows)
+      throw Error(BLS_EDIM, "rt has length " + std::to_string(n_rt) + ", expected " + std::to_string(P->red_nrows));
+    if (P->red_nrows > 0 && (!F || !Fr || !Jt || !rt)) throw Error(BLS_EINVAL, "a device pointer is NULL");
+    if (dtype == BLS_F64) reduced_jacobian_dense<double>(P, (double*)Jt, (const double*)F, Fr, rt);
+    else if (dtype == BLS_F32) reduced_jacobian_dense<float>(P, (float*)Jt, (const float*)F, Fr, rt);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_reduced_jacobian_sparse(bls_qr_plan* P, int dtype, const void* F, const double* Fr, int64_t nrows, int64_t ncols,
+                                const int64_t* colptr, const int64_t* rowval, void* nzval, double* rt, int64_t n_rt) {
+  QR_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    check_jt_pattern(P, nrows, ncols, colptr, rowval);
+    if (n_rt != P->red_nrows)
+      throw Error(BLS_EDIM, "rt has length " + std::to_string(n_rt) + ", expected " + std::to_string(P->red_nrows));
+    if (P->red_nrows > 0 && (!F || !Fr || !rt || (P->h_jt_colptr[P->nr] > 0 && !nzval))) throw Error(BLS_EINVAL, "a device pointer is NULL");
+    if (dtype == BLS_F64) reduced_jacobian_sparse<double>(P, (double*)nzval, (const double*)F, Fr, rt);
+    else if (dtype == BLS_F32) reduced_jacobian_sparse<float>(P, (float*)nzval, (const float*)F, Fr, rt);
     else throw Error(BLS_EINVAL, "unknown dtype");
     return BLS_OK;
   })

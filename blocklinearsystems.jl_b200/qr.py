@@ -10,6 +10,9 @@ reduced_normal_dense      src/qr_reduced.jl:407-436
 reduced_diagonal_blocks   src/qr_reduced.jl:482-512
 free_block_pairs          src/qr_reduced.jl:5-16
 reduced_nrows             src/qr_reduced.jl:1-3
+reduced_residual          src/qr_reduced.jl:227-243
+reduced_jacobian          src/qr_reduced.jl:245-272 (dense) and 336-370 (sparse: reduced_jacobian_sparse)
+build_reduced_jacobian_pattern  src/qr_reduced.jl:284-310
 
 Element type T is the dtype of the Jacobian's tables: torch.float64, or torch.float32 (the mixed form: FP32 tables with
 FP64 column norms, reflector scalars and reflector application, rounded once per entry; the residual is FP64 in both).
@@ -333,3 +336,59 @@ def jtj_quadform(src, v: torch.Tensor, ws: QRReductionWorkspace | None = None) -
     out = C.c_double(0.0)
     check(_lib.gpu().bls_jtj_quadform(w.handle, w._T, dptr(D), dptr(v), C.byref(out)))
     return float(out.value)
+
+
+def build_reduced_jacobian_pattern(jst: SchurJacobianStructure):
+    """build_reduced_jacobian_pattern(jst) (src/qr_reduced.jl:284-310): the CSC pattern of J~ (reduced_nrows x nr),
+    0-based (colptr, rowval) on the host."""
+    L = _lib.gpu()
+    n = L.bls_reduced_jacobian_pattern(jst.handle, None, None)
+    check(int(n) if n < 0 else 0)
+    colptr = np.empty(jst.schur.nr + 1, np.int64)
+    rowval = np.empty(n, np.int64)
+    L.bls_reduced_jacobian_pattern(jst.handle, ptr64(colptr), ptr64(rowval))
+    return colptr, rowval
+
+
+def reduced_residual(rt: torch.Tensor, ws: QRReductionWorkspace) -> torch.Tensor:
+    """reduced_residual!(rt, ws) (src/qr_reduced.jl:227-243): rt = r~ (float64, reduced_nrows entries)."""
+    _dev(rt, "rt", None, torch.float64)
+    check(_lib.gpu().bls_reduced_residual(ws.handle, dptr(ws.fres), dptr(rt) if rt.numel() else None, rt.numel()))
+    return rt
+
+
+def reduced_jacobian(Jt: torch.Tensor, rt: torch.Tensor, ws: QRReductionWorkspace) -> torch.Tensor:
+    """reduced_jacobian!(Jt::Matrix, rt, ws) (src/qr_reduced.jl:245-272): Jt = J~ column-major (reduced_nrows x nr, a
+    flat tensor of the workspace's dtype, or the transposed view of an (nr, reduced_nrows) tensor) and rt = r~."""
+    if Jt.dtype != ws.dtype:
+        raise ArgumentError(f"Jt must be {ws.dtype}")
+    _dev(rt, "rt", None, torch.float64)
+    m, nr = reduced_nrows(ws.structure), ws.structure.schur.nr
+    if Jt.dim() == 2:
+        rows, cols = Jt.shape
+        if not Jt.t().is_contiguous():
+            raise ArgumentError("a 2-d Jt must be column-major (the transpose of a contiguous tensor)")
+    else:
+        _dev(Jt, "Jt")
+        rows, cols = (m, nr) if Jt.numel() == m * nr else (Jt.numel(), 1)
+    check(_lib.gpu().bls_reduced_jacobian_dense(ws.handle, ws._T, dptr(ws.factored), dptr(ws.fres), dptr(Jt) if Jt.numel() else None,
+                                                rows, cols, dptr(rt) if rt.numel() else None, rt.numel()))
+    return Jt
+
+
+def reduced_jacobian_sparse(nzval: torch.Tensor, colptr, rowval, rt: torch.Tensor, ws: QRReductionWorkspace,
+                            nrows: int | None = None, ncols: int | None = None) -> torch.Tensor:
+    """reduced_jacobian!(Jt::SparseMatrixCSC, rt, ws) (src/qr_reduced.jl:336-370): nzval (device, the workspace's
+    dtype) of J~ on the CSC pattern (colptr, rowval: 0-based host arrays, build_reduced_jacobian_pattern's), and
+    rt = r~. The pattern and the sizes are checked before any work (DimensionMismatch, ArgumentError)."""
+    if nzval.dtype != ws.dtype:
+        raise ArgumentError(f"nzval must be {ws.dtype}")
+    _dev(rt, "rt", None, torch.float64)
+    cp = np.ascontiguousarray(colptr, np.int64)
+    rv = np.ascontiguousarray(rowval, np.int64)
+    m = reduced_nrows(ws.structure) if nrows is None else nrows
+    n = len(cp) - 1 if ncols is None else ncols
+    check(_lib.gpu().bls_reduced_jacobian_sparse(ws.handle, ws._T, dptr(ws.factored), dptr(ws.fres), m, n, ptr64(cp),
+                                                 ptr64(rv) if len(rv) else None, dptr(nzval) if nzval.numel() else None,
+                                                 dptr(rt) if rt.numel() else None, rt.numel()))
+    return nzval

@@ -244,6 +244,10 @@ int bls_qr_structure_positional(const bls_structure* st, const int64_t* e_rows, 
  * table_offsets raw_offsets residual_offsets reduced_offsets table_ptr entry_retained entry_col entry_table retained_ptr
  * retained_entry doffsets col_chunks row_table row_first row_nrows row_ptr row_blocks. */
 int64_t bls_qr_structure_field(const bls_qr_structure* q, const char* name, int64_t* out);
+/* build_reduced_jacobian_pattern (src/qr_reduced.jl:284-310): the CSC pattern of J~ (reduced_nrows x nr), 0-based:
+ * column c of retained block r stores the reduced rows of every table coupled to r, tables in ascending order. Returns
+ * nnz; fills colptr[nr + 1] and rowval[nnz] when they are not NULL. */
+int64_t bls_reduced_jacobian_pattern(const bls_qr_structure* q, int64_t* colptr, int64_t* rowval);
 /* The SchurStructure the QR structure is built on (a copy; destroy it with bls_structure_destroy). */
 int bls_qr_structure_schur(const bls_qr_structure* q, bls_structure** out);
 int bls_qr_structure_destroy(bls_qr_structure* q);
@@ -314,6 +318,18 @@ int bls_reduced_normal_dense(bls_qr_plan* plan, int dtype, void* S_dev, double* 
                              const double* Fr_dev);
 /* reduced_diagonal_blocks! (src/qr_reduced.jl:484-512): the full d_r x d_r diagonal blocks of J~'J~ at doffsets. */
 int bls_reduced_diagonal_blocks(bls_qr_plan* plan, int dtype, void* D_dev, const void* F_dev);
+/* The reduced problem written out (src/qr_reduced.jl:227-370), from the factored tables F / Fr. reduced_residual!:
+ * rt = r~ (reduced_nrows FP64 entries, tables in order, each its bottom residual rows). reduced_jacobian! dense: Jt =
+ * J~, column-major nrows x ncols = reduced_nrows x nr, zero outside the tables' runs, and rt = r~. Sparse: nzval (on
+ * the device) of the CSC pattern of build_reduced_jacobian_pattern, which the caller passes (colptr[ncols + 1] and
+ * rowval, 0-based, on the host) and which is checked before any work as the reference checks it: a wrong size or rt
+ * length is BLS_EDIM (DimensionMismatch), a column of the wrong height or a run that starts at the wrong row BLS_EINVAL
+ * (ArgumentError, messages 1-based). */
+int bls_reduced_residual(bls_qr_plan* plan, const double* Fr_dev, double* rt_dev, int64_t n_rt);
+int bls_reduced_jacobian_dense(bls_qr_plan* plan, int dtype, const void* F_dev, const double* Fr_dev, void* Jt_dev, int64_t nrows,
+                               int64_t ncols, double* rt_dev, int64_t n_rt);
+int bls_reduced_jacobian_sparse(bls_qr_plan* plan, int dtype, const void* F_dev, const double* Fr_dev, int64_t nrows, int64_t ncols,
+                                const int64_t* colptr, const int64_t* rowval, void* nzval_dev, double* rt_dev, int64_t n_rt);
 
 /* ---------------------------------------------------------------------------------------------------------------
  * Block-Jacobi (src/diagonal_blocks.jl:6-61) on a flat array of square diagonal blocks (block b, d_b x d_b column-major,

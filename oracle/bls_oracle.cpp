@@ -1404,6 +1404,115 @@ static i64 put(i64* out, const std::vector<i64>& v, i64 shift) {
   return (i64)v.size();
 }
 
+// reduced_residual! (src/qr_reduced.jl:227-243): r~ in the row order of the reduced problem
+void reduced_residual(double* rt, i64 n_rt, const double* Fr, const QRStructure& q) {
+  const i64 nred = q.reduced_offsets(q.ntables + 1) - 1;
+  if (n_rt != nred) dim_error("rt has length " + std::to_string(n_rt) + ", expected " + std::to_string(nred));
+  for (i64 t = 1; t <= q.ntables; ++t) {
+    const i64 M = q.table_nrows(t), top = q.table_top(t), cb = q.residual_offsets(t) + top, ro = q.reduced_offsets(t);
+    for (i64 i = 0; i <= M - top - 1; ++i) rt[ro + i - 1] = Fr[cb + i - 1];
+  }
+}
+
+// reduced_jacobian!(Jt::AbstractMatrix, rt, ws) (src/qr_reduced.jl:245-272): J~ densely, column-major nrows x ncols
+template <class T>
+void reduced_jacobian_dense(T* Jt, i64 nrows, i64 ncols, double* rt, i64 n_rt, const T* F, const double* Fr, const QRStructure& q) {
+  const Structure& st = q.schur;
+  const i64 nred = q.reduced_offsets(q.ntables + 1) - 1;
+  if (nrows != nred || ncols != st.nr)
+    dim_error("Jt has size (" + std::to_string(nrows) + ", " + std::to_string(ncols) + "), expected (" + std::to_string(nred) + ", " +
+              std::to_string(st.nr) + ")");
+  if (n_rt != nred) dim_error("rt has length " + std::to_string(n_rt) + ", expected " + std::to_string(nred));
+  for (i64 k = 0; k < nrows * ncols; ++k) Jt[k] = T(0);
+  reduced_residual(rt, n_rt, Fr, q);
+  for (i64 t = 1; t <= q.ntables; ++t) {
+    const i64 M = q.table_nrows(t), top = q.table_top(t), off = q.raw_offsets(t), yo = q.reduced_offsets(t);
+    for (i64 u = q.table_ptr(t); u <= q.table_ptr(t + 1) - 1; ++u) {
+      const i64 r = q.entry_retained(u), ro = st.boffsets_r(r), cb = off + (q.entry_col(u) - 1) * M + top;
+      for (i64 j = 1; j <= st.r_dims(r); ++j)
+        for (i64 i = 0; i <= M - top - 1; ++i) Jt[(yo + i - 1) + nrows * (ro + j - 2)] = F[cb + (j - 1) * M + i - 1];
+    }
+  }
+}
+
+// reduced_column_height (src/qr_reduced.jl:274-282)
+i64 reduced_column_height(const QRStructure& q, i64 r) {
+  i64 h = 0;
+  for (i64 k = q.retained_ptr(r); k <= q.retained_ptr(r + 1) - 1; ++k) {
+    const i64 t = q.entry_table(q.retained_entry(k));
+    h += q.table_nrows(t) - q.table_top(t);
+  }
+  return h;
+}
+
+// build_reduced_jacobian_pattern (src/qr_reduced.jl:284-310), 1-based colptr (nr + 1) and rowval
+void reduced_jacobian_pattern(const QRStructure& q, IV& colptr, IV& rowval) {
+  const Structure& st = q.schur;
+  colptr = IV(st.nr + 1);
+  colptr(1) = 1;
+  for (i64 r = 1; r <= st.nrblocks; ++r) {
+    const i64 h = reduced_column_height(q, r), ro = st.boffsets_r(r);
+    for (i64 j = 0; j <= st.r_dims(r) - 1; ++j) colptr(ro + j + 1) = colptr(ro + j) + h;
+  }
+  rowval = IV(colptr(st.nr + 1) - 1);
+  for (i64 r = 1; r <= st.nrblocks; ++r)
+    for (i64 j = 0; j <= st.r_dims(r) - 1; ++j) {
+      i64 p = colptr(st.boffsets_r(r) + j);
+      for (i64 k = q.retained_ptr(r); k <= q.retained_ptr(r + 1) - 1; ++k) {
+        const i64 t = q.entry_table(q.retained_entry(k));
+        for (i64 i = 0; i <= q.table_nrows(t) - q.table_top(t) - 1; ++i) { rowval(p) = q.reduced_offsets(t) + i; p += 1; }
+      }
+    }
+}
+
+// check_reduced_jacobian_pattern (src/qr_reduced.jl:312-334) on a 1-based CSC
+void check_reduced_jacobian_pattern(i64 nrows, i64 ncols, const IV& colptr, const IV& rowval, const QRStructure& q) {
+  const Structure& st = q.schur;
+  const i64 nred = q.reduced_offsets(q.ntables + 1) - 1;
+  if (nrows != nred || ncols != st.nr)
+    dim_error("Jt has size (" + std::to_string(nrows) + ", " + std::to_string(ncols) + "), expected (" + std::to_string(nred) + ", " +
+              std::to_string(st.nr) + ")");
+  for (i64 r = 1; r <= st.nrblocks; ++r) {
+    const i64 h = reduced_column_height(q, r);
+    for (i64 c = st.boffsets_r(r); c <= st.boffsets_r(r) + st.r_dims(r) - 1; ++c) {
+      if (colptr(c + 1) - colptr(c) != h)
+        arg_error("Jt does not have the pattern of build_reduced_jacobian_pattern: column " + std::to_string(c) + " stores " +
+                  std::to_string(colptr(c + 1) - colptr(c)) + " entries, expected " + std::to_string(h));
+      i64 p = colptr(c);
+      for (i64 k = q.retained_ptr(r); k <= q.retained_ptr(r + 1) - 1; ++k) {
+        const i64 t = q.entry_table(q.retained_entry(k));
+        const i64 n = q.table_nrows(t) - q.table_top(t);
+        if (!(n == 0 || rowval(p) == q.reduced_offsets(t)))
+          arg_error("Jt does not have the pattern of build_reduced_jacobian_pattern: column " + std::to_string(c) + " stores row " +
+                    std::to_string(rowval(p)) + ", expected " + std::to_string(q.reduced_offsets(t)));
+        p += n;
+      }
+    }
+  }
+}
+
+// reduced_jacobian!(Jt::SparseMatrixCSC, rt, ws) (src/qr_reduced.jl:336-370): J~ into nzval of the pattern
+template <class T>
+void reduced_jacobian_sparse(i64 nrows, i64 ncols, const IV& colptr, const IV& rowval, T* nzval, double* rt, i64 n_rt, const T* F,
+                             const double* Fr, const QRStructure& q) {
+  const Structure& st = q.schur;
+  check_reduced_jacobian_pattern(nrows, ncols, colptr, rowval, q);
+  reduced_residual(rt, n_rt, Fr, q);
+  for (i64 r = 1; r <= st.nrblocks; ++r) {
+    const i64 ro = st.boffsets_r(r), dr = st.r_dims(r);
+    i64 p = 0;
+    for (i64 k = q.retained_ptr(r); k <= q.retained_ptr(r + 1) - 1; ++k) {
+      const i64 u = q.retained_entry(k), t = q.entry_table(u), M = q.table_nrows(t), top = q.table_top(t), n = M - top;
+      const i64 cb = q.raw_offsets(t) + (q.entry_col(u) - 1) * M + top;
+      for (i64 j = 0; j <= dr - 1; ++j) {
+        const i64 qq = colptr(ro + j) + p, c0 = cb + j * M;
+        for (i64 i = 0; i <= n - 1; ++i) nzval[qq + i - 1] = F[c0 + i - 1];
+      }
+      p += n;
+    }
+  }
+}
+
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
@@ -1761,6 +1870,19 @@ i64 orc_qr_field(OrcQR* o, const char* name, i64* out) {
   int orc_reduced_normal_dense_##SUFFIX(OrcQR* o, T* S, double* g_S, const T* F, const double* Fr) {                             \
     ORC_TRY({ reduced_normal_dense<T>(S, g_S, F, Fr, o->q); return ORC_OK; })                                                    \
   }                                                                                                                               \
+  int orc_reduced_jacobian_dense_##SUFFIX(OrcQR* o, T* Jt, i64 nrows, i64 ncols, double* rt, i64 n_rt, const T* F, const double* Fr) { \
+    ORC_TRY({ reduced_jacobian_dense<T>(Jt, nrows, ncols, rt, n_rt, F, Fr, o->q); return ORC_OK; })                              \
+  }                                                                                                                               \
+  int orc_reduced_jacobian_sparse_##SUFFIX(OrcQR* o, i64 nrows, i64 ncols, const i64* colptr0, const i64* rowval0, T* nzval,    \
+                                           double* rt, i64 n_rt, const T* F, const double* Fr) {                                 \
+    ORC_TRY({                                                                                                                     \
+      IV cp(ncols + 1), rv(colptr0[ncols]);                                                                                       \
+      for (i64 c = 0; c <= ncols; ++c) cp(c + 1) = colptr0[c] + 1;                                                                \
+      for (i64 k = 0; k < colptr0[ncols]; ++k) rv(k + 1) = rowval0[k] + 1;                                                       \
+      reduced_jacobian_sparse<T>(nrows, ncols, cp, rv, nzval, rt, n_rt, F, Fr, o->q);                                            \
+      return ORC_OK;                                                                                                              \
+    })                                                                                                                            \
+  }                                                                                                                               \
   int orc_reduced_diagonal_blocks_##SUFFIX(OrcQR* o, T* D, const T* F) {                                                          \
     ORC_TRY({ reduced_diagonal_blocks<T>(D, F, o->q); return ORC_OK; })                                                          \
   }                                                                                                                               \
@@ -1771,6 +1893,18 @@ i64 orc_qr_field(OrcQR* o, const char* name, i64* out) {
 
 ORC_QR_TYPED(f64, double)
 ORC_QR_TYPED(f32, float)
+
+int orc_reduced_residual(OrcQR* o, double* rt, i64 n_rt, const double* Fr) {
+  ORC_TRY({ reduced_residual(rt, n_rt, Fr, o->q); return ORC_OK; })
+}
+// build_reduced_jacobian_pattern, 0-based: returns nnz; colptr (nr + 1) and rowval filled when not NULL
+i64 orc_reduced_jacobian_pattern(OrcQR* o, i64* colptr, i64* rowval) {
+  IV cp, rv;
+  try { reduced_jacobian_pattern(o->q, cp, rv); } catch (const BlsError& e) { g_err = e.what(); return -1; }
+  put(colptr, cp.v, -1);
+  put(rowval, rv.v, -1);
+  return rv.len();
+}
 
 int orc_pcg_solve_f64(OrcStructure* o, OrcPattern* p, const double* S, const double* g, double* x, double tol, i64 maxit, int nthreads,
                       i64* iters, double* rel) {

@@ -42,6 +42,7 @@ def lib() -> C.CDLL:
         L.orc_work_field.restype = i64
         L.orc_qr_field.restype = i64
         L.orc_sparse_indices.restype = i64
+        L.orc_reduced_jacobian_pattern.restype = i64
         _L = L
     return _L
 
@@ -352,6 +353,40 @@ def reduced_normal_sparse(q: QRStructure, pat: Pattern, nzval, g, F, Fr):
 
 def reduced_normal_dense(q: QRStructure, S, g, F, Fr):
     return _chk(getattr(lib(), "orc_reduced_normal_dense_" + _sfx(F))(q.h, _p(S), _p(g), _p(F), _p(Fr)))
+
+
+def reduced_nrows(q: QRStructure) -> int:
+    """reduced_nrows (src/qr_reduced.jl:1-3): rows of the reduced problem."""
+    return int(q.reduced_offsets[-1])
+
+
+def reduced_residual(q: QRStructure, rt, Fr):
+    """reduced_residual!(rt, ws) (src/qr_reduced.jl:227-243)."""
+    return _chk(lib().orc_reduced_residual(q.h, _p(rt), i64(len(rt)), _p(Fr)))
+
+
+def reduced_jacobian_pattern(q: QRStructure):
+    """build_reduced_jacobian_pattern(jst) (src/qr_reduced.jl:284-310): the CSC pattern of J~, 0-based (colptr, rowval)."""
+    n = lib().orc_reduced_jacobian_pattern(q.h, None, None)
+    _chk(int(n) if n < 0 else 0)
+    colptr = np.empty(q.st.nr + 1, np.int64)
+    rowval = np.empty(n, np.int64)
+    lib().orc_reduced_jacobian_pattern(q.h, _p(colptr), _p(rowval))
+    return colptr, rowval
+
+
+def reduced_jacobian_dense(q: QRStructure, Jt, nrows, ncols, rt, F, Fr):
+    """reduced_jacobian!(Jt::Matrix, rt, ws) (src/qr_reduced.jl:245-272): Jt column-major nrows x ncols, flat."""
+    return _chk(getattr(lib(), "orc_reduced_jacobian_dense_" + _sfx(F))(q.h, _p(Jt), i64(nrows), i64(ncols), _p(rt), i64(len(rt)), _p(F),
+                                                                          _p(Fr)))
+
+
+def reduced_jacobian_sparse(q: QRStructure, nrows, ncols, colptr, rowval, nzval, rt, F, Fr):
+    """reduced_jacobian!(Jt::SparseMatrixCSC, rt, ws) (src/qr_reduced.jl:336-370) on a 0-based CSC pattern."""
+    cp = np.ascontiguousarray(colptr, np.int64)
+    rv = np.ascontiguousarray(rowval, np.int64)
+    return _chk(getattr(lib(), "orc_reduced_jacobian_sparse_" + _sfx(F))(q.h, i64(nrows), i64(ncols), _p(cp), _p(rv), _p(nzval), _p(rt),
+                                                                           i64(len(rt)), _p(F), _p(Fr)))
 
 
 def reduced_diagonal_blocks(q: QRStructure, D, F):

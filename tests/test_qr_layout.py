@@ -132,3 +132,36 @@ def test_rejected(bls):
         bls.SchurJacobianStructure.positional(st, [2], [3], [[0, 0]])
     with pytest.raises(bls.DimensionMismatch):
         bls.SchurJacobianStructure.positional(st, [2, 2])
+
+
+def _reduced_pattern_checks(bls, j, o):
+    colptr, rowval = bls.build_reduced_jacobian_pattern(j)
+    ocp, orv = orc.reduced_jacobian_pattern(o)
+    np.testing.assert_array_equal(colptr, ocp)
+    np.testing.assert_array_equal(rowval, orv)
+    # nnz(J~) = sum over entries of d_r of its retained block times the reduced rows of its table (test/schur_qr.jl:243-245)
+    nnz = sum(int(j.schur.r_dims[j.entry_retained[u]]) * int(j.table_nrows[j.entry_table[u]] - j.table_top[j.entry_table[u]])
+              for u in range(len(j.entry_retained)))
+    assert len(rowval) == nnz == colptr[-1]
+    assert colptr.shape == (j.schur.nr + 1,) and np.all(np.diff(colptr) >= 0)
+    assert np.all((rowval >= 0) & (rowval < bls.reduced_nrows(j)))
+
+
+@pytest.mark.parametrize("name", list(QR_FIXTURES))
+def test_reduced_jacobian_pattern_fixtures(bls, name):
+    """build_reduced_jacobian_pattern (src/qr_reduced.jl:284-310): the native host pattern equals the oracle's."""
+    fx = QR_FIXTURES[name](np.random.default_rng(3))
+    st = bls.SchurStructure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    ost = orc.Structure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    j = bls.SchurJacobianStructure.positional(st, fx["e_rows"], fx.get("free_rows", ()), fx.get("free_retained", ()))
+    o = orc.QRStructure.positional(ost, fx["e_rows"], fx.get("free_rows", ()), fx.get("free_retained", ()))
+    _reduced_pattern_checks(bls, j, o)
+
+
+def test_reduced_jacobian_pattern_scene(bls):
+    spec = bls.scenes.scaled_down(bls.scenes.workload("qr_500x100k"), ncams=40, npoints=800)
+    p = bls.scenes.jacobian_problem(spec)
+    sc = bls.scenes.Scene(spec)
+    bs, el, ptr, idx = sc.description()
+    o = orc.QRStructure.from_description(bs, (ptr, idx), np.full(len(ptr) - 1, 2), el)
+    _reduced_pattern_checks(bls, p.structure, o)
