@@ -81,6 +81,8 @@ def gpu() -> C.CDLL:
             "bls_pattern_destroy": (C.c_int, [vp]),
             "bls_build_r_to_s_map": (C.c_int, [vp, vp, p64]),
             "bls_sparse_indices": (i64, [vp, vp, C.c_int, p64, p64, p64]),
+            "bls_r_to_s_map_csc": (C.c_int, [i64, p64, p64, p64, p64, p64]),
+            "bls_r_to_s_map_blocks_csc": (C.c_int, [i64, p64, p64, p64, p64, i64, p64, p64, p64, p64]),
             "bls_schur_plan_create": (C.c_int, [vp, C.POINTER(bls_schur_plan_desc), C.POINTER(vp)]),
             "bls_schur_plan_destroy": (C.c_int, [vp]),
             "bls_schur_plan_device_bytes": (i64, [vp]),

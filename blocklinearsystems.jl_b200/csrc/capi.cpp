@@ -1,6 +1,7 @@
 // C ABI of libblsgpu: contexts, errors and the host-side layout (structure, pattern, maps).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <string>
@@ -193,6 +194,73 @@ int bls_build_r_to_s_map(const bls_structure* st, const bls_pattern* p, int64_t*
     if (!st || !p || !out) throw Error(BLS_EINVAL, "null argument");
     std::vector<int64_t> m = build_r_to_s(*st, *p);
     put(out, m);
+    return BLS_OK;
+  })
+}
+
+// find_in_column (src/schur_structure.jl:355-361): the position of `row` in column j of S (rows sorted), or -1
+static int64_t find_in_column(const int64_t* S_colptr, const int64_t* S_rowval, int64_t row, int64_t j) {
+  const int64_t* lo = S_rowval + S_colptr[j];
+  const int64_t* hi = S_rowval + S_colptr[j + 1];
+  const int64_t* f = std::lower_bound(lo, hi, row);
+  return (f != hi && *f == row) ? (int64_t)(f - S_rowval) : -1;
+}
+
+int bls_r_to_s_map_csc(int64_t ncols, const int64_t* R_colptr, const int64_t* R_rowval, const int64_t* S_colptr, const int64_t* S_rowval,
+                       int64_t* out) {
+  BLS_GUARD({
+    if (ncols < 0 || (ncols > 0 && (!R_colptr || !S_colptr)) || (ncols > 0 && R_colptr[ncols] > 0 && (!R_rowval || !out)))
+      throw Error(BLS_EINVAL, "null argument");
+    const int64_t nnz = ncols > 0 ? R_colptr[ncols] : 0;
+    std::vector<int64_t> m((size_t)nnz);
+    for (int64_t j = 0; j < ncols; ++j)
+      for (int64_t k = R_colptr[j]; k < R_colptr[j + 1]; ++k) {
+        const int64_t i = R_rowval[k], s_k = find_in_column(S_colptr, S_rowval, i, j);
+        if (s_k < 0)
+          throw Error(BLS_EINVAL, "R entry (" + std::to_string(i + 1) + ", " + std::to_string(j + 1) + ") is not present in the sparsity pattern of S");
+        m[k] = s_k;
+      }
+    if (nnz > 0) std::memcpy(out, m.data(), sizeof(int64_t) * (size_t)nnz);
+    return BLS_OK;
+  })
+}
+
+int bls_r_to_s_map_blocks_csc(int64_t nb, const int64_t* blocksizes, const int64_t* it_colptr, const int64_t* it_rowval, const int64_t* it_nzval,
+                              int64_t data_len, const int64_t* S_colptr, const int64_t* S_rowval, const int64_t* boffsets_r, int64_t* out) {
+  BLS_GUARD({
+    if (nb < 0 || data_len < 0 || (nb > 0 && (!blocksizes || !it_colptr || !S_colptr || !boffsets_r)) || (data_len > 0 && !out))
+      throw Error(BLS_EINVAL, "null argument");
+    std::vector<int64_t> m((size_t)data_len, -1);
+    // findnz(indicestransposed): block rows brow in order, then their block columns
+    for (int64_t brow = 0; brow < nb; ++brow)
+      for (int64_t k = it_colptr[brow]; k < it_colptr[brow + 1]; ++k) {
+        const int64_t bcol = it_rowval[k], start = it_nzval[k], drow = blocksizes[brow], dcol = blocksizes[bcol];
+        if (bcol < 0 || bcol >= nb || start < 0 || start + drow * dcol > data_len) throw Error(BLS_EINVAL, "indicestransposed is malformed");
+        if (brow == bcol) {
+          for (int64_t col = 0; col < dcol; ++col) {
+            const int64_t scol = boffsets_r[brow] + col;
+            for (int64_t row = 0; row <= col; ++row) {
+              const int64_t srow = boffsets_r[brow] + row, s_k = find_in_column(S_colptr, S_rowval, srow, scol);
+              if (s_k < 0)
+                throw Error(BLS_EINVAL, "Entry (" + std::to_string(srow + 1) + ", " + std::to_string(scol + 1) +
+                                            ") of a diagonal block of R is not present in the sparsity pattern of S");
+              m[start + col * drow + row] = s_k;
+            }
+          }
+        } else if (brow > bcol) {
+          for (int64_t col = 0; col < dcol; ++col) {
+            const int64_t srow = boffsets_r[bcol] + col;
+            for (int64_t row = 0; row < drow; ++row) {
+              const int64_t scol = boffsets_r[brow] + row, s_k = find_in_column(S_colptr, S_rowval, srow, scol);
+              if (s_k < 0)
+                throw Error(BLS_EINVAL, "Entry (" + std::to_string(srow + 1) + ", " + std::to_string(scol + 1) +
+                                            ") of R is not present in the sparsity pattern of S");
+              m[start + col * drow + row] = s_k;
+            }
+          }
+        }
+      }
+    if (data_len > 0) std::memcpy(out, m.data(), sizeof(int64_t) * (size_t)data_len);
     return BLS_OK;
   })
 }

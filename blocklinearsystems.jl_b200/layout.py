@@ -173,6 +173,42 @@ class BlockSystem:
         return int(np.sum(self.blocksizes))
 
 
+def retained_block_pairs(bsys: "BlockSystem") -> list:
+    """retained_block_pairs(R) (src/schur_structure.jl:325-334): the off-diagonal stored blocks of R as 0-based
+    (row_block, col_block) pairs in indicestransposed's order, to pass as extra_blocks to build_schur_pattern."""
+    out = []
+    for r in range(len(bsys.blocksizes)):
+        for k in range(int(bsys.colptr[r]), int(bsys.colptr[r + 1])):
+            c = int(bsys.rowval[k])
+            if r != c:
+                out.append((r, c))
+    return out
+
+
+def build_r_to_s_map_scalar(R_colptr, R_rowval, S_colptr, S_rowval) -> np.ndarray:
+    """build_r_to_s_map(R_sparse, S_sparse) (src/schur_structure.jl:336-353): for each stored entry of the CSC R (0-based
+    colptr / rowval) its position in S.nzval (the scalar CSC S_colptr / S_rowval, rows sorted). ArgumentError if an
+    entry of R is not in S."""
+    rc, rr, sc, sr = (np.ascontiguousarray(a, np.int64) for a in (R_colptr, R_rowval, S_colptr, S_rowval))
+    out = np.empty(len(rr), np.int64)
+    check(_lib.gpu().bls_r_to_s_map_csc(len(rc) - 1, ptr64(rc), ptr64(rr) if len(rr) else None, ptr64(sc), ptr64(sr) if len(sr) else None,
+                                        ptr64(out) if len(out) else None))
+    return out
+
+
+def build_r_to_s_map_blocks(bsys: "BlockSystem", S_colptr, S_rowval, boffsets_r, data_len: int) -> np.ndarray:
+    """build_r_to_s_map(R_sys, S_sparse, boffsets_r) (src/schur_structure.jl:363-397): for each entry of R's block storage
+    (data_len entries) its position in the scalar S.nzval: a diagonal block's upper triangle and every entry of a block
+    below the diagonal (in S's upper triangle); -1 elsewhere (the reference's 0). ArgumentError if S lacks one."""
+    bs, cp, rv, st = (np.ascontiguousarray(a, np.int64) for a in (bsys.blocksizes, bsys.colptr, bsys.rowval, bsys.starts))
+    sc, sr, bo = (np.ascontiguousarray(a, np.int64) for a in (S_colptr, S_rowval, boffsets_r))
+    out = np.empty(int(data_len), np.int64)
+    check(_lib.gpu().bls_r_to_s_map_blocks_csc(len(bs), ptr64(bs), ptr64(cp), ptr64(rv) if len(rv) else None, ptr64(st) if len(st) else None,
+                                               int(data_len), ptr64(sc), ptr64(sr) if len(sr) else None, ptr64(bo),
+                                               ptr64(out) if len(out) else None))
+    return out
+
+
 def build_schur_pattern(structure: SchurStructure, extra_blocks=()) -> SchurPattern:
     """build_schur_pattern(structure; extra_blocks) (src/schur_structure.jl:241-323)."""
     L = _lib.gpu()

@@ -94,6 +94,21 @@ int bls_pattern_destroy(bls_pattern* p);
 /* build_r_to_s_map(R, pattern, boffsets_r), block-level form (src/schur_structure.jl:406-431), for the retained
  * storage laid out on the pattern. out[R_length]; -1 marks an unmapped entry (the reference's 0). */
 int bls_build_r_to_s_map(const bls_structure* st, const bls_pattern* p, int64_t* out);
+/* The scalar-level forms of build_r_to_s_map, against a scalar CSC pattern of S (S_colptr / S_rowval, 0-based, rows
+ * sorted within each column; e.g. the pattern's S_colptr / S_rowval). Positions are found by binary search in S's
+ * column; an entry absent from S is BLS_EINVAL with the reference's message (1-based indices).
+ * bls_r_to_s_map_csc: build_r_to_s_map(R_sparse, S_sparse) (src/schur_structure.jl:336-353), R a CSC of ncols
+ *   columns: out[nnz(R)] = the position in S.nzval of each stored entry of R.
+ * bls_r_to_s_map_blocks_csc: build_r_to_s_map(R_sys, S_sparse, boffsets_r) (src/schur_structure.jl:363-397), R_sys a
+ *   block-square SparseBlockLinearSystem given by its nb block sizes and indicestransposed (a CSC over block rows r:
+ *   block (r, it_rowval[k]) starts at data[it_nzval[k]], column-major), boffsets_r[nb] the blocks' first scalar
+ *   rows: out[data_len], a diagonal block's upper triangle and every entry of a block below the diagonal (placed in
+ *   S's upper triangle), -1 elsewhere (the reference's 0). */
+int bls_r_to_s_map_csc(int64_t ncols, const int64_t* R_colptr, const int64_t* R_rowval, const int64_t* S_colptr,
+                       const int64_t* S_rowval, int64_t* out);
+int bls_r_to_s_map_blocks_csc(int64_t nb, const int64_t* blocksizes, const int64_t* it_colptr, const int64_t* it_rowval,
+                              const int64_t* it_nzval, int64_t data_len, const int64_t* S_colptr, const int64_t* S_rowval,
+                              const int64_t* boffsets_r, int64_t* out);
 /* makesparseindices / sparse_with_map (src/SparseBlockLinearSystem.jl:233-282, 343-354) for that retained storage:
  * the CSC pattern (colptr[nr+1], rowval[nnz]) and the integer scatter map[nnz] (0-based positions in the storage).
  * Returns nnz (pass NULL outputs to query it), or a negative status. */

@@ -1513,6 +1513,63 @@ void reduced_jacobian_sparse(i64 nrows, i64 ncols, const IV& colptr, const IV& r
   }
 }
 
+// find_in_column (src/schur_structure.jl:355-361) on a 1-based CSC: the index of `row` in column j, 0 if absent
+static i64 find_in_column_1(const IV& S_colptr, const IV& S_rowval, i64 row, i64 j) {
+  i64 lo = S_colptr(j), hi = S_colptr(j + 1) - 1;
+  // searchsortedfirst over rowval[lo:hi]
+  i64 a = lo, b = hi + 1;
+  while (a < b) {
+    const i64 mid = (a + b) / 2;
+    if (S_rowval(mid) < row) a = mid + 1;
+    else b = mid;
+  }
+  return (a <= hi && S_rowval(a) == row) ? a : 0;
+}
+
+// build_r_to_s_map(R_sparse, S_sparse) (src/schur_structure.jl:336-353), 1-based
+IV r_to_s_map_csc(i64 ncols, const IV& R_colptr, const IV& R_rowval, const IV& S_colptr, const IV& S_rowval) {
+  IV r_to_s(R_colptr(ncols + 1) - 1, 0);
+  i64 pos = 1;
+  for (i64 j = 1; j <= ncols; ++j)
+    for (i64 k = R_colptr(j); k <= R_colptr(j + 1) - 1; ++k) {
+      const i64 i = R_rowval(k), s_k = find_in_column_1(S_colptr, S_rowval, i, j);
+      if (s_k == 0) arg_error("R entry (" + std::to_string(i) + ", " + std::to_string(j) + ") is not present in the sparsity pattern of S");
+      r_to_s(pos++) = s_k;
+    }
+  return r_to_s;
+}
+
+// build_r_to_s_map(R_sys, S_sparse, boffsets_r) (src/schur_structure.jl:363-397), 1-based
+IV r_to_s_map_blocks_csc(i64 nb, const IV& sizes, const IV& it_colptr, const IV& it_rowval, const IV& it_nzval, i64 data_len,
+                         const IV& S_colptr, const IV& S_rowval, const IV& boffsets_r) {
+  IV r_to_s(data_len, 0);
+  for (i64 brow = 1; brow <= nb; ++brow)
+    for (i64 k = it_colptr(brow); k <= it_colptr(brow + 1) - 1; ++k) {
+      const i64 bcol = it_rowval(k), data_start = it_nzval(k), drow = sizes(brow), dcol = sizes(bcol);
+      if (brow == bcol) {
+        for (i64 col = 1; col <= dcol; ++col) {
+          const i64 scol = boffsets_r(brow) + col - 1;
+          for (i64 row = 1; row <= col; ++row) {
+            const i64 srow = boffsets_r(brow) + row - 1, s_k = find_in_column_1(S_colptr, S_rowval, srow, scol);
+            if (s_k == 0)
+              arg_error("Entry (" + std::to_string(srow) + ", " + std::to_string(scol) + ") of a diagonal block of R is not present in the sparsity pattern of S");
+            r_to_s(data_start + (col - 1) * drow + row - 1) = s_k;
+          }
+        }
+      } else if (brow > bcol) {
+        for (i64 col = 1; col <= dcol; ++col) {
+          const i64 srow = boffsets_r(bcol) + col - 1;
+          for (i64 row = 1; row <= drow; ++row) {
+            const i64 scol = boffsets_r(brow) + row - 1, s_k = find_in_column_1(S_colptr, S_rowval, srow, scol);
+            if (s_k == 0) arg_error("Entry (" + std::to_string(srow) + ", " + std::to_string(scol) + ") of R is not present in the sparsity pattern of S");
+            r_to_s(data_start + (col - 1) * drow + row - 1) = s_k;
+          }
+        }
+      }
+    }
+  return r_to_s;
+}
+
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
@@ -1893,6 +1950,34 @@ i64 orc_qr_field(OrcQR* o, const char* name, i64* out) {
 
 ORC_QR_TYPED(f64, double)
 ORC_QR_TYPED(f32, float)
+
+// the scalar-level build_r_to_s_map forms, 0-based in and out (0 -> -1 for an unmapped entry)
+int orc_r_to_s_map_csc(i64 ncols, const i64* R_colptr, const i64* R_rowval, const i64* S_colptr, const i64* S_rowval, i64 S_ncols, i64* out) {
+  ORC_TRY({
+    IV rc(ncols + 1), rr(R_colptr[ncols]), sc(S_ncols + 1), sr(S_colptr[S_ncols]);
+    for (i64 c = 0; c <= ncols; ++c) rc(c + 1) = R_colptr[c] + 1;
+    for (i64 k = 0; k < R_colptr[ncols]; ++k) rr(k + 1) = R_rowval[k] + 1;
+    for (i64 c = 0; c <= S_ncols; ++c) sc(c + 1) = S_colptr[c] + 1;
+    for (i64 k = 0; k < S_colptr[S_ncols]; ++k) sr(k + 1) = S_rowval[k] + 1;
+    IV m = r_to_s_map_csc(ncols, rc, rr, sc, sr);
+    put(out, m.v, -1);
+    return ORC_OK;
+  })
+}
+int orc_r_to_s_map_blocks_csc(i64 nb, const i64* sizes, const i64* it_colptr, const i64* it_rowval, const i64* it_nzval, i64 data_len,
+                              const i64* S_colptr, const i64* S_rowval, i64 S_ncols, const i64* boffsets_r, i64* out) {
+  ORC_TRY({
+    IV sz(nb), icp(nb + 1), irv(it_colptr[nb]), inz(it_colptr[nb]), sc(S_ncols + 1), sr(S_colptr[S_ncols]), bo(nb);
+    for (i64 b = 0; b < nb; ++b) { sz(b + 1) = sizes[b]; bo(b + 1) = boffsets_r[b] + 1; }
+    for (i64 b = 0; b <= nb; ++b) icp(b + 1) = it_colptr[b] + 1;
+    for (i64 k = 0; k < it_colptr[nb]; ++k) { irv(k + 1) = it_rowval[k] + 1; inz(k + 1) = it_nzval[k] + 1; }
+    for (i64 c = 0; c <= S_ncols; ++c) sc(c + 1) = S_colptr[c] + 1;
+    for (i64 k = 0; k < S_colptr[S_ncols]; ++k) sr(k + 1) = S_rowval[k] + 1;
+    IV m = r_to_s_map_blocks_csc(nb, sz, icp, irv, inz, data_len, sc, sr, bo);
+    put(out, m.v, -1);
+    return ORC_OK;
+  })
+}
 
 int orc_reduced_residual(OrcQR* o, double* rt, i64 n_rt, const double* Fr) {
   ORC_TRY({ reduced_residual(rt, n_rt, Fr, o->q); return ORC_OK; })

@@ -245,6 +245,29 @@ def symmetrify_full(blocksizes, it_colptr, it_rowval, it_nzval, data, blocks=Non
     return mat.reshape(m, m, order="F")
 
 
+def retained_block_pairs(it_colptr, it_rowval):
+    """retained_block_pairs(R) (src/schur_structure.jl:325-334): off-diagonal stored blocks, 0-based (row, col)."""
+    return [(r, int(it_rowval[k])) for r in range(len(it_colptr) - 1) for k in range(int(it_colptr[r]), int(it_colptr[r + 1]))
+            if int(it_rowval[k]) != r]
+
+
+def r_to_s_map_csc(R_colptr, R_rowval, S_colptr, S_rowval):
+    """build_r_to_s_map(R_sparse, S_sparse) (src/schur_structure.jl:336-353), 0-based."""
+    rc, rr, sc, sr = (np.ascontiguousarray(a, np.int64) for a in (R_colptr, R_rowval, S_colptr, S_rowval))
+    out = np.empty(len(rr), np.int64)
+    _chk(lib().orc_r_to_s_map_csc(i64(len(rc) - 1), _p(rc), _p(rr), _p(sc), _p(sr), i64(len(sc) - 1), _p(out)))
+    return out
+
+
+def r_to_s_map_blocks_csc(sizes, it_colptr, it_rowval, it_nzval, data_len, S_colptr, S_rowval, boffsets_r):
+    """build_r_to_s_map(R_sys, S_sparse, boffsets_r) (src/schur_structure.jl:363-397), 0-based, -1 unmapped."""
+    a = [np.ascontiguousarray(x, np.int64) for x in (sizes, it_colptr, it_rowval, it_nzval, S_colptr, S_rowval, boffsets_r)]
+    out = np.empty(int(data_len), np.int64)
+    _chk(lib().orc_r_to_s_map_blocks_csc(i64(len(a[0])), _p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]), i64(data_len), _p(a[4]), _p(a[5]),
+                                         i64(len(a[4]) - 1), _p(a[6]), _p(out)))
+    return out
+
+
 def sort_schur_blocks(is_elim, sizes, couplings):
     el = np.ascontiguousarray(np.asarray(is_elim, bool), np.uint8)
     sz = np.ascontiguousarray(sizes, np.int64)

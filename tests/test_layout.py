@@ -132,3 +132,90 @@ def test_rejected_descriptions(bls):
     st = bls.SchurStructure.positional([6, 6, 6, 6], [3] * 4, [[0, 1], [0, 1], [2, 3], [2, 3]])
     with pytest.raises(bls.ArgumentError):
         bls.build_schur_pattern(st, [(0, 4)])
+
+
+@pytest.mark.parametrize("fx", [STANDARD, COUPLED_GROUPS], ids=["standard", "coupled_groups"])
+def test_scalar_and_block_r_to_s_maps_agree(bls, fx):
+    """build_r_to_s_map: the scalar-level form (R's block storage against the scalar CSC of S) equals the block-level
+    one (test/schur_problems.jl:241-262); mapped slots are unique and in S's upper triangle; the count is every
+    upper-triangle entry of the diagonal blocks plus every entry of the off-diagonal blocks
+    (test/dampedlinearsolve_schurhessian.jl:108-114); the oracle's restatement agrees; and R's couplings without a slot
+    in S are rejected."""
+    st = bls.SchurStructure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    ost = orc.Structure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    extra = fx.get("rr_pairs", ())
+    pat = bls.build_schur_pattern(st, extra)
+    R = bls.BlockSystem.retained(st, pat)
+    pairs = bls.retained_block_pairs(R)
+    assert {(max(a, b), min(a, b)) for a, b in extra} <= set(pairs)   # R's couplings are among its off-diagonal blocks
+    # the retained pairs build the same pattern (they are the pattern's off-diagonal blocks)
+    pat2 = bls.build_schur_pattern(st, pairs)
+    np.testing.assert_array_equal(pat2.S_colptr, pat.S_colptr)
+    np.testing.assert_array_equal(pat2.S_rowval, pat.S_rowval)
+    m_block = bls.build_r_to_s_map(st, pat)
+    m_scalar = bls.build_r_to_s_map_blocks(R, pat.S_colptr, pat.S_rowval, st.boffsets_r, pat.R_length)
+    np.testing.assert_array_equal(m_block, m_scalar)
+    o = orc.r_to_s_map_blocks_csc(st.r_dims, pat.block_colptr, pat.block_rowval, pat.R_block_start, pat.R_length, pat.S_colptr,
+                                  pat.S_rowval, st.boffsets_r)
+    np.testing.assert_array_equal(o, m_scalar)
+    mapped = m_block[m_block >= 0]
+    assert len(np.unique(mapped)) == len(mapped)
+    cols = np.repeat(np.arange(st.nr), np.diff(pat.S_colptr))
+    assert np.all(pat.S_rowval[mapped] <= cols[mapped])
+    d = np.asarray(st.r_dims)
+    expect = int(np.sum(d * (d + 1) // 2)) + sum(int(d[a] * d[b]) for a, b in pairs)
+    assert len(mapped) == expect
+    if extra:
+        plain = bls.build_schur_pattern(st)
+        with pytest.raises(bls.ArgumentError, match="is not present in the sparsity pattern of S"):
+            bls.build_r_to_s_map_blocks(R, plain.S_colptr, plain.S_rowval, st.boffsets_r, pat.R_length)
+        with pytest.raises(orc.OracleError, match="is not present in the sparsity pattern of S"):
+            orc.r_to_s_map_blocks_csc(st.r_dims, pat.block_colptr, pat.block_rowval, pat.R_block_start, pat.R_length, plain.S_colptr,
+                                      plain.S_rowval, st.boffsets_r)
+
+
+def test_retained_block_pairs_known_answer(bls):
+    """retained_block_pairs(H.R) contains the coupled-groups problem's retained-retained couplings
+    (test/dampedlinearsolve_schurhessian.jl:108: (3, 1) and (4, 2), 1-based)."""
+    fx = COUPLED_GROUPS
+    st = bls.SchurStructure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    pat = bls.build_schur_pattern(st, fx.get("rr_pairs", ()))
+    pairs = set(bls.retained_block_pairs(bls.BlockSystem.retained(st, pat)))
+    assert {(2, 0), (3, 1)} <= pairs
+    assert pairs == set(orc.retained_block_pairs(pat.block_colptr, pat.block_rowval))
+
+
+def test_scalar_csc_r_to_s_map(bls):
+    """build_r_to_s_map(R_sparse, S_sparse): positions found by binary search equal a linear search of S's column (the
+    reference's own check, test/schur.jl:320-333, 488-489); an entry absent from S is rejected with its position."""
+    fx = STANDARD
+    st = bls.SchurStructure.positional(fx["r_dims"], fx["e_dims"], fx["couplings"])
+    pat = bls.build_schur_pattern(st)
+    rng = np.random.default_rng(4)
+    n = st.nr
+    # R: a random subset of S's stored entries, rows ascending in each column
+    rc, rr = [0], []
+    for j in range(n):
+        rows = pat.S_rowval[pat.S_colptr[j]:pat.S_colptr[j + 1]]
+        keep = rows[rng.random(len(rows)) < 0.6]
+        rr.extend(keep.tolist())
+        rc.append(len(rr))
+    rc, rr = np.array(rc), np.array(rr, np.int64)
+    expect = []
+    for j in range(n):
+        for k in range(rc[j], rc[j + 1]):
+            lo, hi = pat.S_colptr[j], pat.S_colptr[j + 1]
+            expect.append(lo + int(np.flatnonzero(pat.S_rowval[lo:hi] == rr[k])[0]))
+    got = bls.build_r_to_s_map_scalar(rc, rr, pat.S_colptr, pat.S_rowval)
+    np.testing.assert_array_equal(got, expect)
+    np.testing.assert_array_equal(orc.r_to_s_map_csc(rc, rr, pat.S_colptr, pat.S_rowval), expect)
+    # an entry of R outside S's pattern: S stores the upper block triangle, so column 0 holds no row of a later block
+    j = 0
+    missing = next(i for i in range(n) if i not in set(pat.S_rowval[pat.S_colptr[j]:pat.S_colptr[j + 1]].tolist()))
+    rr2 = np.concatenate([np.sort(np.append(rr[:rc[1]], missing)), rr[rc[1]:]])
+    rc2 = rc.copy()
+    rc2[1:] += 1
+    with pytest.raises(bls.ArgumentError, match=f"R entry \\({missing + 1}, {j + 1}\\) is not present"):
+        bls.build_r_to_s_map_scalar(rc2, rr2, pat.S_colptr, pat.S_rowval)
+    with pytest.raises(orc.OracleError, match=f"R entry \\({missing + 1}, {j + 1}\\) is not present"):
+        orc.r_to_s_map_csc(rc2, rr2, pat.S_colptr, pat.S_rowval)
