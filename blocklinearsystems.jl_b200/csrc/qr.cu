@@ -655,6 +655,77 @@ static void reduced_jacobian_sparse(QRPlan* P, T* nzval, const T* F, const doubl
   BLS_CUDA(cudaGetLastError());
 }
 
+// reduced_mul! (src/qr_reduced.jl:159-192): y = J~ v, a warp per table, a lane per reduced row accumulating over the
+// table's entries and their columns in order (FP64)
+template <class T>
+__global__ void __launch_bounds__(256) k_reduced_mul(int64_t nt, const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
+                                                     const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_red,
+                                                     const int32_t* __restrict__ t_ptr, const int32_t* __restrict__ u_ret,
+                                                     const int32_t* __restrict__ u_col, const int32_t* __restrict__ r_dims,
+                                                     const int32_t* __restrict__ boff_r, const T* __restrict__ F, const double* __restrict__ v,
+                                                     double* __restrict__ y) {
+  const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= nt) return;
+  const int M = t_rows[t], top = t_top[t], n = M - top;
+  const int64_t raw = t_raw[t] + top, red = t_red[t];
+  const int u0 = t_ptr[t], u1 = t_ptr[t + 1];
+  for (int i = lane; i < n; i += 32) {
+    double acc = 0.0;
+    for (int u = u0; u < u1; ++u) {
+      const int r = u_ret[u], dr = r_dims[r], c0 = u_col[u], ro = boff_r[r];
+      for (int j = 0; j < dr; ++j) acc += (double)F[raw + (int64_t)(c0 + j) * M + i] * v[ro + j];
+    }
+    y[red + i] = acc;
+  }
+}
+
+// reduced_tmul! (src/qr_reduced.jl:194-223): g = J~' w, a warp per retained block: per column, the dot product of each
+// of its entries' runs with w (a warp reduction in FP64), added in the order of the block's entries
+template <class T>
+__global__ void __launch_bounds__(256) k_reduced_tmul(int64_t nrb, const int32_t* __restrict__ rptr, const int32_t* __restrict__ rent,
+                                                      const int32_t* __restrict__ u_tab, const int32_t* __restrict__ t_rows,
+                                                      const int32_t* __restrict__ t_top, const int64_t* __restrict__ t_raw,
+                                                      const int64_t* __restrict__ t_red, const int32_t* __restrict__ u_col,
+                                                      const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                                                      const T* __restrict__ F, const double* __restrict__ w, double* __restrict__ g) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= nrb) return;
+  const int dr = r_dims[r], ro = boff_r[r];
+  for (int j = 0; j < dr; ++j) {
+    double sum = 0.0;
+    for (int k = rptr[r]; k < rptr[r + 1]; ++k) {
+      const int u = rent[k], t = u_tab[u], M = t_rows[t], top = t_top[t], n = M - top;
+      const T* col = F + t_raw[t] + (int64_t)(u_col[u] + j) * M + top;
+      const double* wr = w + t_red[t];
+      double acc = 0.0;
+      for (int i = lane; i < n; i += 32) acc += (double)col[i] * wr[i];
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      sum += acc;
+    }
+    if (lane == 0) g[ro + j] = sum;
+  }
+}
+
+template <class T>
+static void launch_reduced_mul(QRPlan* P, const T* F, const double* v, double* y) {
+  k_reduced_mul<T><<<(unsigned)std::max(1, grid_for(P->ntables * 32, 256)), 256, 0, P->ctx->stream>>>(
+      P->ntables, P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_red.as<int64_t>(), P->t_ptr.as<int32_t>(),
+      P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), F, v, y);
+  P->launches += 1;
+  BLS_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static void launch_reduced_tmul(QRPlan* P, const T* F, const double* w, double* g) {
+  k_reduced_tmul<T><<<(unsigned)std::max(1, grid_for(P->nrblocks * 32, 256)), 256, 0, P->ctx->stream>>>(
+      P->nrblocks, P->q_rptr.as<int32_t>(), P->q_rent.as<int32_t>(), P->u_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(),
+      P->t_raw.as<int64_t>(), P->t_red.as<int64_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), F, w, g);
+  P->launches += 1;
+  BLS_CUDA(cudaGetLastError());
+}
+
 // check_reduced_jacobian_pattern (src/qr_reduced.jl:312-334) of a caller's 0-based CSC, before any work: its size,
 // then per column of each retained block its height and the first row of every run; messages 1-based, as the
 // reference's
@@ -1233,6 +1304,33 @@ int bls_reduced_jacobian_sparse(bls_qr_plan* P, int dtype, const void* F, const 
     if (P->red_nrows > 0 && (!F || !Fr || !rt || (P->h_jt_colptr[P->nr] > 0 && !nzval))) throw Error(BLS_EINVAL, "a device pointer is NULL");
     if (dtype == BLS_F64) reduced_jacobian_sparse<double>(P, (double*)nzval, (const double*)F, Fr, rt);
     else if (dtype == BLS_F32) reduced_jacobian_sparse<float>(P, (float*)nzval, (const float*)F, Fr, rt);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+
+int bls_reduced_mul(bls_qr_plan* P, int dtype, const void* F, const double* v, int64_t nv, double* y, int64_t ny) {
+  QR_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (ny != P->red_nrows) throw Error(BLS_EDIM, "y has length " + std::to_string(ny) + ", expected " + std::to_string(P->red_nrows));
+    if (nv != P->nr) throw Error(BLS_EDIM, "v has length " + std::to_string(nv) + ", expected " + std::to_string(P->nr));
+    if (ny > 0 && (!F || !v || !y)) throw Error(BLS_EINVAL, "a device pointer is NULL");
+    if (dtype == BLS_F64) launch_reduced_mul<double>(P, (const double*)F, v, y);
+    else if (dtype == BLS_F32) launch_reduced_mul<float>(P, (const float*)F, v, y);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    return BLS_OK;
+  })
+}
+
+int bls_reduced_tmul(bls_qr_plan* P, int dtype, const void* F, const double* w, int64_t nw, double* g, int64_t ng) {
+  QR_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (ng != P->nr) throw Error(BLS_EDIM, "g has length " + std::to_string(ng) + ", expected " + std::to_string(P->nr));
+    if (nw != P->red_nrows) throw Error(BLS_EDIM, "w has length " + std::to_string(nw) + ", expected " + std::to_string(P->red_nrows));
+    if (ng > 0 && (!F || !w || !g)) throw Error(BLS_EINVAL, "a device pointer is NULL");
+    if (dtype == BLS_F64) launch_reduced_tmul<double>(P, (const double*)F, w, g);
+    else if (dtype == BLS_F32) launch_reduced_tmul<float>(P, (const float*)F, w, g);
     else throw Error(BLS_EINVAL, "unknown dtype");
     return BLS_OK;
   })

@@ -11,6 +11,7 @@ reduced_diagonal_blocks   src/qr_reduced.jl:482-512
 free_block_pairs          src/qr_reduced.jl:5-16
 reduced_nrows             src/qr_reduced.jl:1-3
 reduced_residual          src/qr_reduced.jl:227-243
+reduced_mul / reduced_tmul  src/qr_reduced.jl:159-223 (J~ v and J~' w from the factored tables)
 reduced_jacobian          src/qr_reduced.jl:245-272 (dense) and 336-370 (sparse: reduced_jacobian_sparse)
 build_reduced_jacobian_pattern  src/qr_reduced.jl:284-310
 
@@ -392,3 +393,21 @@ def reduced_jacobian_sparse(nzval: torch.Tensor, colptr, rowval, rt: torch.Tenso
                                                  ptr64(rv) if len(rv) else None, dptr(nzval) if nzval.numel() else None,
                                                  dptr(rt) if rt.numel() else None, rt.numel()))
     return nzval
+
+
+def reduced_mul(y: torch.Tensor, ws: QRReductionWorkspace, v: torch.Tensor) -> torch.Tensor:
+    """reduced_mul!(y, ws, v) (src/qr_reduced.jl:159-192): y = J~ v (float64), without forming J~."""
+    _dev(y, "y", None, torch.float64)
+    _dev(v, "v", None, torch.float64)
+    check(_lib.gpu().bls_reduced_mul(ws.handle, ws._T, dptr(ws.factored), dptr(v) if v.numel() else None, v.numel(),
+                                     dptr(y) if y.numel() else None, y.numel()))
+    return y
+
+
+def reduced_tmul(g: torch.Tensor, ws: QRReductionWorkspace, w: torch.Tensor) -> torch.Tensor:
+    """reduced_tmul!(g, ws, w) (src/qr_reduced.jl:194-223): g = J~' w (float64), without forming J~."""
+    _dev(g, "g", None, torch.float64)
+    _dev(w, "w", None, torch.float64)
+    check(_lib.gpu().bls_reduced_tmul(ws.handle, ws._T, dptr(ws.factored), dptr(w) if w.numel() else None, w.numel(),
+                                      dptr(g) if g.numel() else None, g.numel()))
+    return g

@@ -340,6 +340,12 @@ int bls_reduced_diagonal_blocks(bls_qr_plan* plan, int dtype, void* D_dev, const
  * rowval, 0-based, on the host) and which is checked before any work as the reference checks it: a wrong size or rt
  * length is BLS_EDIM (DimensionMismatch), a column of the wrong height or a run that starts at the wrong row BLS_EINVAL
  * (ArgumentError, messages 1-based). */
+/* reduced_mul! (src/qr_reduced.jl:159-192): y = J~ v (ny = reduced_nrows, nv = nr); reduced_tmul!
+ * (src/qr_reduced.jl:194-223): g = J~' w (ng = nr, nw = reduced_nrows); FP64 vectors, products accumulated in FP64,
+ * applied from the factored tables without forming J~ (the per-iteration work of an LSMR solve of the reduced
+ * problem). A wrong length is BLS_EDIM. */
+int bls_reduced_mul(bls_qr_plan* plan, int dtype, const void* F_dev, const double* v_dev, int64_t nv, double* y_dev, int64_t ny);
+int bls_reduced_tmul(bls_qr_plan* plan, int dtype, const void* F_dev, const double* w_dev, int64_t nw, double* g_dev, int64_t ng);
 int bls_reduced_residual(bls_qr_plan* plan, const double* Fr_dev, double* rt_dev, int64_t n_rt);
 int bls_reduced_jacobian_dense(bls_qr_plan* plan, int dtype, const void* F_dev, const double* Fr_dev, void* Jt_dev, int64_t nrows,
                                int64_t ncols, double* rt_dev, int64_t n_rt);

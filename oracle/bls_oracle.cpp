@@ -1404,6 +1404,49 @@ static i64 put(i64* out, const std::vector<i64>& v, i64 shift) {
   return (i64)v.size();
 }
 
+// reduced_mul! (src/qr_reduced.jl:159-192): y = J~ v, accumulated per row in the order of the table's entries and columns
+template <class T>
+void reduced_mul(double* y, i64 ny, const double* v, i64 nv, const T* F, const QRStructure& q) {
+  const Structure& st = q.schur;
+  const i64 nred = q.reduced_offsets(q.ntables + 1) - 1;
+  if (ny != nred) dim_error("y has length " + std::to_string(ny) + ", expected " + std::to_string(nred));
+  if (nv != st.nr) dim_error("v has length " + std::to_string(nv) + ", expected " + std::to_string(st.nr));
+  for (i64 t = 1; t <= q.ntables; ++t) {
+    const i64 M = q.table_nrows(t), top = q.table_top(t), off = q.raw_offsets(t), yo = q.reduced_offsets(t), n = M - top;
+    for (i64 i = 0; i <= n - 1; ++i) y[yo + i - 1] = 0.0;
+    for (i64 u = q.table_ptr(t); u <= q.table_ptr(t + 1) - 1; ++u) {
+      const i64 r = q.entry_retained(u), ro = st.boffsets_r(r), cb = off + (q.entry_col(u) - 1) * M + top;
+      for (i64 j = 1; j <= st.r_dims(r); ++j) {
+        const double vj = v[ro + j - 2];
+        const i64 c0 = cb + (j - 1) * M;
+        for (i64 i = 0; i <= n - 1; ++i) y[yo + i - 1] += (double)F[c0 + i - 1] * vj;
+      }
+    }
+  }
+}
+
+// reduced_tmul! (src/qr_reduced.jl:194-223): g = J~' w, per retained column the runs' dot products (dot_run, FP64)
+template <class T>
+void reduced_tmul(double* g, i64 ng, const double* w, i64 nw, const T* F, const QRStructure& q) {
+  const Structure& st = q.schur;
+  const i64 nred = q.reduced_offsets(q.ntables + 1) - 1;
+  if (ng != st.nr) dim_error("g has length " + std::to_string(ng) + ", expected " + std::to_string(st.nr));
+  if (nw != nred) dim_error("w has length " + std::to_string(nw) + ", expected " + std::to_string(nred));
+  for (i64 r = 1; r <= st.nrblocks; ++r) {
+    const i64 ro = st.boffsets_r(r), dr = st.r_dims(r);
+    for (i64 j = 0; j <= dr - 1; ++j) g[ro + j - 1] = 0.0;
+    for (i64 k = q.retained_ptr(r); k <= q.retained_ptr(r + 1) - 1; ++k) {
+      const i64 u = q.retained_entry(k), t = q.entry_table(u), M = q.table_nrows(t), top = q.table_top(t);
+      const i64 cb = q.raw_offsets(t) + (q.entry_col(u) - 1) * M + top, wo = q.reduced_offsets(t);
+      for (i64 j = 1; j <= dr; ++j) {
+        double acc = 0.0;
+        for (i64 i = 0; i <= M - top - 1; ++i) acc += (double)F[cb + (j - 1) * M + i - 1] * w[wo + i - 1];
+        g[ro + j - 2] += acc;
+      }
+    }
+  }
+}
+
 // reduced_residual! (src/qr_reduced.jl:227-243): r~ in the row order of the reduced problem
 void reduced_residual(double* rt, i64 n_rt, const double* Fr, const QRStructure& q) {
   const i64 nred = q.reduced_offsets(q.ntables + 1) - 1;
@@ -1926,6 +1969,12 @@ i64 orc_qr_field(OrcQR* o, const char* name, i64* out) {
   }                                                                                                                               \
   int orc_reduced_normal_dense_##SUFFIX(OrcQR* o, T* S, double* g_S, const T* F, const double* Fr) {                             \
     ORC_TRY({ reduced_normal_dense<T>(S, g_S, F, Fr, o->q); return ORC_OK; })                                                    \
+  }                                                                                                                               \
+  int orc_reduced_mul_##SUFFIX(OrcQR* o, double* y, i64 ny, const double* v, i64 nv, const T* F) {                              \
+    ORC_TRY({ reduced_mul<T>(y, ny, v, nv, F, o->q); return ORC_OK; })                                                          \
+  }                                                                                                                               \
+  int orc_reduced_tmul_##SUFFIX(OrcQR* o, double* g, i64 ng, const double* w, i64 nw, const T* F) {                             \
+    ORC_TRY({ reduced_tmul<T>(g, ng, w, nw, F, o->q); return ORC_OK; })                                                         \
   }                                                                                                                               \
   int orc_reduced_jacobian_dense_##SUFFIX(OrcQR* o, T* Jt, i64 nrows, i64 ncols, double* rt, i64 n_rt, const T* F, const double* Fr) { \
     ORC_TRY({ reduced_jacobian_dense<T>(Jt, nrows, ncols, rt, n_rt, F, Fr, o->q); return ORC_OK; })                              \

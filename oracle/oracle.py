@@ -398,6 +398,16 @@ def reduced_jacobian_pattern(q: QRStructure):
     return colptr, rowval
 
 
+def reduced_mul(q: QRStructure, y, v, F):
+    """reduced_mul!(y, ws, v) (src/qr_reduced.jl:159-192): y = J~ v."""
+    return _chk(getattr(lib(), "orc_reduced_mul_" + _sfx(F))(q.h, _p(y), i64(len(y)), _p(v), i64(len(v)), _p(F)))
+
+
+def reduced_tmul(q: QRStructure, g, w, F):
+    """reduced_tmul!(g, ws, w) (src/qr_reduced.jl:194-223): g = J~' w."""
+    return _chk(getattr(lib(), "orc_reduced_tmul_" + _sfx(F))(q.h, _p(g), i64(len(g)), _p(w), i64(len(w)), _p(F)))
+
+
 def reduced_jacobian_dense(q: QRStructure, Jt, nrows, ncols, rt, F, Fr):
     """reduced_jacobian!(Jt::Matrix, rt, ws) (src/qr_reduced.jl:245-272): Jt column-major nrows x ncols, flat."""
     return _chk(getattr(lib(), "orc_reduced_jacobian_dense_" + _sfx(F))(q.h, _p(Jt), i64(nrows), i64(ncols), _p(rt), i64(len(rt)), _p(F),

@@ -121,3 +121,38 @@ def test_rejections_before_any_write(bls):
     with pytest.raises(bls.ArgumentError, match="stores row"):
         bls.reduced_jacobian_sparse(nz, colptr, bad, rt, ws)
     assert bool((nz == 7.0).all()) and bool((rt == 7.0).all())
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+@pytest.mark.parametrize("name", list(QR_FIXTURES))
+def test_reduced_mul_tmul(bls, name, dtype):
+    """reduced_mul! / reduced_tmul! (src/qr_reduced.jl:159-223): J~ v and J~' w from the factored tables, against the
+    oracle on the device's own tables (FP64 accumulation; J~ v in the reference's order per row, the runs' dot products
+    of J~' w as warp sums: within 1e-14 relative), and J~'(J~ v) against S v with S = J~'J~ from reduced_normal_dense."""
+    j, o, Rw, Rr, sc_e = _fixture(bls, name)
+    npdt = np.float32 if dtype == torch.float32 else np.float64
+    ws = bls.QRReductionWorkspace(j, None, dtype)
+    J = bls.SchurBlockJacobian(j, dtype, data=cu(Rw.astype(npdt)), r=cu(Rr))
+    assert bls.reduce_qr(ws, J, cu(sc_e), 0.3)
+    F = ws.factored.cpu().numpy()
+    m, nr = bls.reduced_nrows(j), j.schur.nr
+    rng = np.random.default_rng(9)
+    v, w = rng.standard_normal(nr), rng.standard_normal(m)
+    y = bls.reduced_mul(torch.full((m,), float("nan"), dtype=torch.float64, device=DEV), ws, cu(v)).cpu().numpy()
+    g = bls.reduced_tmul(torch.full((nr,), float("nan"), dtype=torch.float64, device=DEV), ws, cu(w)).cpu().numpy()
+    oy, og = np.zeros(m), np.zeros(nr)
+    orc.reduced_mul(o, oy, v, F)
+    orc.reduced_tmul(o, og, w, F)
+    assert np.abs(y - oy).max() <= 1e-14 * max(np.abs(oy).max(), 1e-300)
+    assert np.abs(g - og).max() <= 1e-14 * max(np.abs(og).max(), 1e-300)
+    if dtype == torch.float64:
+        S = torch.zeros(nr * nr, dtype=dtype, device=DEV)
+        bls.reduced_normal_dense(S, torch.zeros(nr, dtype=torch.float64, device=DEV), ws)
+        Su = S.cpu().numpy().reshape(nr, nr, order="F")
+        Sf = np.triu(Su) + np.triu(Su, 1).T
+        tt = bls.reduced_tmul(torch.zeros(nr, dtype=torch.float64, device=DEV), ws, cu(y)).cpu().numpy()
+        assert np.abs(tt - Sf @ v).max() <= 1e-12 * max(np.abs(Sf @ v).max(), 1e-300)
+    with pytest.raises(bls.DimensionMismatch):
+        bls.reduced_mul(torch.zeros(m + 1, dtype=torch.float64, device=DEV), ws, cu(v))
+    with pytest.raises(bls.DimensionMismatch):
+        bls.reduced_tmul(torch.zeros(nr, dtype=torch.float64, device=DEV), ws, cu(np.zeros(m + 1)))
