@@ -115,6 +115,8 @@ def gpu() -> C.CDLL:
             "bls_reduced_residual": (C.c_int, [vp, vp, vp, i64]),
             "bls_reduced_mul": (C.c_int, [vp, C.c_int, vp, vp, i64, vp, i64]),
             "bls_reduced_tmul": (C.c_int, [vp, C.c_int, vp, vp, i64, vp, i64]),
+            "bls_lsmr_reduced": (C.c_int, [vp, C.c_int, vp, vp, C.c_double, vp, vp, i64, C.c_double, C.c_double, C.c_double, i64,
+                                           p64, C.POINTER(C.c_int), pdbl]),
             "bls_reduced_jacobian_dense": (C.c_int, [vp, C.c_int, vp, vp, vp, i64, i64, vp, i64]),
             "bls_reduced_jacobian_sparse": (C.c_int, [vp, C.c_int, vp, vp, i64, i64, p64, p64, vp, vp, i64]),
             "bls_reduced_jacobian_pattern": (i64, [vp, p64, p64]),

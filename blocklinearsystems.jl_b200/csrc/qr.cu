@@ -67,10 +67,18 @@ struct QRPlan {
   std::vector<int64_t> h_red, h_jt_colptr;
   std::vector<int32_t> h_rptr, h_rent_tab;   // per retained block, the tables of its entries in ascending entry order
   std::vector<int64_t> h_boff_r, h_rdims;
+  // LSMR on the reduced problem (allocated at its first call): the augmented vector u (reduced_nrows + nr) and a
+  // scratch of reduced_nrows, v, h, hbar and two scratch vectors (nr), sqrt(lambda s_r), the diagonal blocks (storage
+  // type) and their FP64 Cholesky factors, the norm accumulators and the factorisation's flag
+  DevBuf ls_u, ls_sc, ls_v, ls_h, ls_hbar, ls_t, ls_w, ls_sqd, ls_D, ls_L, ls_acc, ls_flag;
+  double* ls_host = nullptr;
   DevBuf status;
   long long* host_status = nullptr;
   int64_t launches = 0;
-  ~QRPlan() { if (host_status) cudaFreeHost(host_status); }
+  ~QRPlan() {
+    if (host_status) cudaFreeHost(host_status);
+    if (ls_host) cudaFreeHost(ls_host);
+  }
 };
 
 static std::vector<int32_t> q32(const int64_t* a, int64_t n, const char* what) {
@@ -1115,6 +1123,320 @@ static void diagonal_blocks(QRPlan* P, T* D, const T* F) {
   gram<T, 1>(P, D, false, nullptr, F, nullptr);
 }
 
+// ---- LSMR on the reduced problem (ext/KrylovExt.jl:25-132): min || A x - [r~; 0] ||, A = [J~; diag(sqrt(lambda s_r))]
+// (reduced_nrows + nr rows), with the block-Jacobi N = D^-1, D the diagonal blocks of A'A = J~'J~ + lambda diag(s_r).
+// Krylov's N-preconditioned LSMR is ordinary LSMR on B = A C with C C' = N; with D = L L' that is C = L^-T, so the
+// Golub-Kahan vectors u, v are B's, while h, hbar and x are kept in the original variables (t = L^-T v is what both B v
+// and the h update need). The vectors are FP64 on the device; the scalar recurrences of Fong & Saunders (SIAM J. Sci.
+// Comput. 33 (2011), LSMR with its estimates of ||r||, ||A'r||, ||A|| and cond(A)) run on the host.
+
+// D_b + sqd^2 on its diagonal, then its Cholesky factor L (lower, FP64, column-major) in place; a thread per block. A
+// block that is not positive definite (or not finite) records the lowest such block in *bad.
+template <class T>
+__global__ void k_lsmr_factor(int64_t nrb, const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                              const int64_t* __restrict__ doff, const T* __restrict__ Dt, const double* __restrict__ sqd,
+                              double* __restrict__ L, int* __restrict__ bad) {
+  const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (b >= nrb) return;
+  const int d = r_dims[b], ro = boff_r[b];
+  double* a = L + doff[b];
+  const T* src = Dt + doff[b];
+  for (int q = 0; q < d * d; ++q) a[q] = (double)src[q];
+  for (int i = 0; i < d; ++i) a[i + d * i] += sqd[ro + i] * sqd[ro + i];
+  for (int j = 0; j < d; ++j) {
+    double p = a[j + d * j];
+    for (int k = 0; k < j; ++k) p -= a[j + d * k] * a[j + d * k];
+    if (!(p > 0.0) || !isfinite(p)) {
+      atomicMin(bad, (int)b);
+      return;
+    }
+    const double ljj = sqrt(p);
+    a[j + d * j] = ljj;
+    for (int i = j + 1; i < d; ++i) {
+      double q = a[i + d * j];
+      for (int k = 0; k < j; ++k) q -= a[i + d * k] * a[j + d * k];
+      a[i + d * j] = q / ljj;
+    }
+  }
+}
+
+__device__ __forceinline__ void warp_sum_add(double v, double* out) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(out, v);
+}
+
+// v = L^-1 (sc (w + sqd .* ub)) + gamma v, block by block (w is overwritten), and acc += |v|^2; a thread per block.
+// This is B' u - beta v with u = sc ub_raw: w = J~' u_top(raw), ub = the raw bottom of u.
+__global__ void k_lsmr_fwd(int64_t nrb, const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                           const int64_t* __restrict__ doff, const double* __restrict__ L, double* __restrict__ w,
+                           const double* __restrict__ sqd, const double* __restrict__ ub, double sc, double gamma,
+                           double* __restrict__ v, double* __restrict__ acc) {
+  const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double nn = 0.0;
+  if (b < nrb) {
+    const int d = r_dims[b], ro = boff_r[b];
+    const double* a = L + doff[b];
+    for (int i = 0; i < d; ++i) {
+      double q = sc * (w[ro + i] + sqd[ro + i] * ub[ro + i]);
+      for (int k = 0; k < i; ++k) q -= a[i + d * k] * w[ro + k];
+      w[ro + i] = q / a[i + d * i];
+    }
+    for (int i = 0; i < d; ++i) {
+      const double z = w[ro + i] + gamma * v[ro + i];
+      v[ro + i] = z;
+      nn += z * z;
+    }
+  }
+  warp_sum_add(nn, acc);
+}
+
+// v *= sc, then t = L^-T v, block by block; a thread per block
+__global__ void k_lsmr_bwd(int64_t nrb, const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                           const int64_t* __restrict__ doff, const double* __restrict__ L, double sc, double* __restrict__ v,
+                           double* __restrict__ t) {
+  const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (b >= nrb) return;
+  const int d = r_dims[b], ro = boff_r[b];
+  const double* a = L + doff[b];
+  for (int i = 0; i < d; ++i) v[ro + i] *= sc;
+  for (int i = d - 1; i >= 0; --i) {
+    double q = v[ro + i];
+    for (int k = i + 1; k < d; ++k) q -= a[k + d * i] * t[ro + k];
+    t[ro + i] = q / a[i + d * i];
+  }
+}
+
+// u = [Jt; sqd .* t] - a u (B v - alpha u, with Jt = J~ t), acc += |u|^2
+__global__ void k_lsmr_bv(int64_t mt, int64_t nr, const double* __restrict__ Jt, const double* __restrict__ sqd,
+                          const double* __restrict__ t, double a, double* __restrict__ u, double* __restrict__ acc) {
+  double nn = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < mt + nr; i += (int64_t)gridDim.x * blockDim.x) {
+    const double z = (i < mt ? Jt[i] : sqd[i - mt] * t[i - mt]) - a * u[i];
+    u[i] = z;
+    nn += z * z;
+  }
+  warp_sum_add(nn, acc);
+}
+
+// hbar = h - c1 hbar; x += c2 hbar; h = t - c3 h; acc += |x|^2
+__global__ void k_lsmr_update(int64_t n, const double* __restrict__ t, double* __restrict__ h, double* __restrict__ hbar,
+                              double* __restrict__ x, double c1, double c2, double c3, double* __restrict__ acc) {
+  double nn = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double hb = h[i] - c1 * hbar[i];
+    hbar[i] = hb;
+    const double xi = x[i] + c2 * hb;
+    x[i] = xi;
+    h[i] = t[i] - c3 * h[i];
+    nn += xi * xi;
+  }
+  warp_sum_add(nn, acc);
+}
+
+// sqd = sqrt(lambda s_r) (s_r NULL: sqrt(lambda)); u's bottom rows zero; acc[0] += |r~|^2 (u's top, already written)
+__global__ void k_lsmr_init(int64_t mt, int64_t nr, double lambda, const double* __restrict__ s_r, double* __restrict__ sqd,
+                            double* __restrict__ u, double* __restrict__ acc) {
+  double nn = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < mt + nr; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < mt) {
+      nn += u[i] * u[i];
+    } else {
+      sqd[i - mt] = sqrt(lambda * (s_r ? s_r[i - mt] : 1.0));
+      u[i] = 0.0;
+    }
+  }
+  warp_sum_add(nn, acc);
+}
+
+struct LsmrOut {
+  int64_t iterations = 0;
+  int istop = 0;
+  double normr = 0, normar = 0, normA = 0, condA = 0, normx = 0;
+};
+
+// The stopping tests' order and meaning (Fong & Saunders): 1 ||r|| small (a compatible system), 2 ||A'r|| small (a
+// least-squares solution), 3 cond(A) above conlim, 4-6 the same at machine precision, 7 itmax iterations.
+template <class T>
+static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, const double* s_r, double* x, double atol,
+                        double btol, double conlim, int64_t itmax, LsmrOut* out) {
+  cudaStream_t s = P->ctx->stream;
+  const int64_t mt = P->red_nrows, nr = P->nr, nrb = P->nrblocks, m = mt + nr;
+  if (!P->ls_u.p) {
+    P->ls_u.alloc(sizeof(double) * (size_t)std::max<int64_t>(m, 1));
+    P->ls_sc.alloc(sizeof(double) * (size_t)std::max<int64_t>(mt, 1));
+    for (DevBuf* b : {&P->ls_v, &P->ls_h, &P->ls_hbar, &P->ls_t, &P->ls_w, &P->ls_sqd})
+      b->alloc(sizeof(double) * (size_t)std::max<int64_t>(nr, 1));
+    P->ls_D.alloc(sizeof(double) * (size_t)std::max<int64_t>(P->ndiag, 1));
+    P->ls_L.alloc(sizeof(double) * (size_t)std::max<int64_t>(P->ndiag, 1));
+    P->ls_acc.alloc(sizeof(double) * 4);
+    P->ls_flag.alloc(sizeof(int));
+    BLS_CUDA(cudaMallocHost(reinterpret_cast<void**>(&P->ls_host), sizeof(double) * 4));
+  }
+  double *u = P->ls_u.as<double>(), *Jt = P->ls_sc.as<double>(), *v = P->ls_v.as<double>(), *h = P->ls_h.as<double>();
+  double *hbar = P->ls_hbar.as<double>(), *t = P->ls_t.as<double>(), *w = P->ls_w.as<double>(), *sqd = P->ls_sqd.as<double>();
+  double *L = P->ls_L.as<double>(), *acc = P->ls_acc.as<double>(), *hv = P->ls_host;
+  int* flag = P->ls_flag.as<int>();
+  const int32_t *rd = P->r_dims.as<int32_t>(), *bo = P->boff_r.as<int32_t>();
+  const int64_t* doff = P->doff.as<int64_t>();
+  const unsigned gm = (unsigned)std::max(1, std::min(grid_for(m, 256), 148 * 8));
+  const unsigned gn = (unsigned)std::max(1, std::min(grid_for(nr, 256), 148 * 8));
+  const unsigned gb = (unsigned)std::max(1, grid_for(nrb, 128));
+  auto read = [&](int k) {   // the first k norm accumulators to the host
+    BLS_CUDA(cudaMemcpyAsync(hv, acc, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+    BLS_CUDA(cudaStreamSynchronize(s));
+  };
+  *out = LsmrOut();
+  // u = [r~; 0], sqd = sqrt(lambda s_r), |r~|^2; D + lambda s_r factored; x = 0
+  BLS_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 4, s));
+  BLS_CUDA(cudaMemsetAsync(flag, 0x7f, sizeof(int), s));
+  BLS_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)nr, s));
+  if (mt > 0)
+    k_reduced_residual<<<(unsigned)std::max(1, grid_for(P->ntables * 32, 256)), 256, 0, s>>>(
+        P->ntables, P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_res.as<int64_t>(), P->t_red.as<int64_t>(), Fr, u);
+  k_lsmr_init<<<gm, 256, 0, s>>>(mt, nr, lambda, s_r, sqd, u, acc);
+  diagonal_blocks<T>(P, reinterpret_cast<T*>(P->ls_D.p), F);
+  k_lsmr_factor<T><<<gb, 128, 0, s>>>(nrb, rd, bo, doff, reinterpret_cast<const T*>(P->ls_D.p), sqd, L, flag);
+  P->launches += 3 + (mt > 0);
+  BLS_CUDA(cudaGetLastError());
+  BLS_CUDA(cudaMemcpyAsync(hv, acc, sizeof(double), cudaMemcpyDeviceToHost, s));
+  int bad = 0;
+  BLS_CUDA(cudaMemcpyAsync(&bad, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaStreamSynchronize(s));
+  const double bb = hv[0];
+  if (!std::isfinite(bb)) return BLS_NOT_PD;          // a non-finite reduced residual
+  if (lambda == 0 && mt < nr) return BLS_NOT_PD;      // undamped with fewer reduced rows than variables: rank deficient
+  if (bad != 0x7f7f7f7f) return BLS_NOT_PD;           // a diagonal block of A'A is not positive definite
+  double beta = std::sqrt(bb);
+  out->normr = beta;
+  if (nr == 0 || beta == 0) return BLS_OK;            // x = 0 solves it
+  // alpha v = B' u with u = u_raw / beta; t = L^-T v; h = t
+  BLS_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 4, s));
+  BLS_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * (size_t)nr, s));
+  BLS_CUDA(cudaMemsetAsync(hbar, 0, sizeof(double) * (size_t)nr, s));
+  launch_reduced_tmul<T>(P, F, u, w);
+  k_lsmr_fwd<<<gb, 128, 0, s>>>(nrb, rd, bo, doff, L, w, sqd, u + mt, 1.0 / beta, 0.0, v, acc + 1);
+  P->launches += 1;
+  read(2);
+  double alpha = std::sqrt(hv[1]);
+  k_lsmr_bwd<<<gb, 128, 0, s>>>(nrb, rd, bo, doff, L, alpha > 0 ? 1.0 / alpha : 1.0, v, t);
+  P->launches += 1;
+  BLS_CUDA(cudaMemcpyAsync(h, t, sizeof(double) * (size_t)nr, cudaMemcpyDeviceToDevice, s));
+  double uscale = 1.0 / beta;   // u = uscale * u_raw
+
+  double zetabar = alpha * beta, alphabar = alpha, rho = 1, rhobar = 1, cbar = 1, sbar = 0;
+  double betadd = beta, betad = 0, rhodold = 1, tautildeold = 0, thetatilde = 0, zeta = 0, dsum = 0;
+  double normA2 = alpha * alpha, maxrbar = 0, minrbar = 1e100, normA = std::sqrt(normA2), condA = 1;
+  const double normb = beta, ctol = conlim > 0 ? 1.0 / conlim : 0.0;
+  double normr = beta, normar = alpha * beta, normx = 0;
+  int64_t itn = 0;
+  int istop = 0;
+  if (normar == 0) {
+    out->normr = normr;
+    return BLS_OK;
+  }
+  // The tests of an iteration need ||x||, which the update kernel accumulates; they are evaluated at the next
+  // iteration's first read-back, after B v of the next step has been launched (at itmax, without it)
+  auto tests = [&]() -> int {
+    const double test1 = normr / normb;
+    const double t2d = normA * normr;
+    const double test2 = t2d != 0 ? normar / t2d : INFINITY;
+    const double test3 = 1.0 / condA;
+    const double t1 = test1 / (1.0 + normA * normx / normb);
+    const double rtol = btol + atol * normA * normx / normb;
+    int k = 0;
+    if (itn >= itmax) k = 7;
+    if (1.0 + test3 <= 1.0) k = 6;
+    if (1.0 + test2 <= 1.0) k = 5;
+    if (1.0 + t1 <= 1.0) k = 4;
+    if (test3 <= ctol) k = 3;
+    if (test2 <= atol) k = 2;
+    if (test1 <= rtol) k = 1;
+    return k;
+  };
+  bool pending = false;
+  for (;;) {
+    // u_raw = B v - alpha u
+    if (itn < itmax) {
+      BLS_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2, s));
+      if (mt > 0) launch_reduced_mul<T>(P, F, t, Jt);
+      k_lsmr_bv<<<gm, 256, 0, s>>>(mt, nr, Jt, sqd, t, alpha * uscale, u, acc);
+      P->launches += 1;
+    }
+    read(3);
+    if (pending) {
+      normx = std::sqrt(hv[2]);
+      istop = tests();
+      if (istop) break;
+    }
+    ++itn;
+    beta = std::sqrt(hv[0]);
+    if (!std::isfinite(beta)) return BLS_NOT_PD;
+    if (beta > 0) {
+      uscale = 1.0 / beta;
+      // v_raw = B' u - beta v, alpha = |v_raw|, v = v_raw / alpha, t = L^-T v
+      launch_reduced_tmul<T>(P, F, u, w);
+      k_lsmr_fwd<<<gb, 128, 0, s>>>(nrb, rd, bo, doff, L, w, sqd, u + mt, uscale, -beta, v, acc + 1);
+      P->launches += 1;
+      read(2);
+      alpha = std::sqrt(hv[1]);
+      if (!std::isfinite(alpha)) return BLS_NOT_PD;
+      k_lsmr_bwd<<<gb, 128, 0, s>>>(nrb, rd, bo, doff, L, alpha > 0 ? 1.0 / alpha : 1.0, v, t);
+      P->launches += 1;
+    } else {
+      uscale = 0.0;
+    }
+    // the plane rotations (no regularisation in LSMR itself: the damping rows are part of A)
+    const double alphahat = alphabar;
+    const double rhoold = rho;
+    rho = std::hypot(alphahat, beta);
+    const double c = alphahat / rho, sn = beta / rho;
+    const double thetanew = sn * alpha;
+    alphabar = c * alpha;
+    const double rhobarold = rhobar, zetaold = zeta, thetabar = sbar * rho, rhotemp = cbar * rho;
+    rhobar = std::hypot(cbar * rho, thetanew);
+    cbar = cbar * rho / rhobar;
+    sbar = thetanew / rhobar;
+    zeta = cbar * zetabar;
+    zetabar = -sbar * zetabar;
+    // hbar = h - (thetabar rho / (rhoold rhobarold)) hbar; x += (zeta / (rho rhobar)) hbar; h = t - (thetanew / rho) h
+    BLS_CUDA(cudaMemsetAsync(acc + 2, 0, sizeof(double), s));
+    k_lsmr_update<<<gn, 256, 0, s>>>(nr, t, h, hbar, x, thetabar * rho / (rhoold * rhobarold), zeta / (rho * rhobar),
+                                     thetanew / rho, acc + 2);
+    P->launches += 1;
+    // ||r||: the rotations applied to (betadd, betad) and the running tau
+    const double betaacute = betadd, betahat = c * betaacute;
+    betadd = -sn * betaacute;
+    const double thetatildeold = thetatilde, rhotildeold = std::hypot(rhodold, thetabar);
+    const double ctildeold = rhodold / rhotildeold, stildeold = thetabar / rhotildeold;
+    thetatilde = stildeold * rhobar;
+    rhodold = ctildeold * rhobar;
+    betad = -stildeold * betad + ctildeold * betahat;
+    tautildeold = (zetaold - thetatildeold * tautildeold) / rhotildeold;
+    const double taud = (zeta - thetatilde * tautildeold) / rhodold;
+    normr = std::sqrt(dsum + (betad - taud) * (betad - taud) + betadd * betadd);
+    // ||A|| (of B) and cond(A)
+    normA2 += beta * beta;
+    normA = std::sqrt(normA2);
+    normA2 += alpha * alpha;
+    maxrbar = std::max(maxrbar, rhobarold);
+    if (itn > 1) minrbar = std::min(minrbar, rhobarold);
+    condA = std::max(maxrbar, rhotemp) / std::min(minrbar, rhotemp);
+    normar = std::fabs(zetabar);
+    pending = true;
+  }
+  out->iterations = itn;
+  out->istop = istop;
+  out->normr = normr;
+  out->normar = normar;
+  out->normA = normA;
+  out->condA = condA;
+  out->normx = normx;
+  if (!std::isfinite(normx)) return BLS_NOT_PD;
+  if (istop == 7) return BLS_NOT_CONVERGED;
+  if (istop == 3 || istop == 6) return BLS_NOT_PD;   // cond(A) above conlim: not solved
+  return BLS_OK;
+}
+
 }  // namespace bls
 
 struct bls_qr_plan : bls::QRPlan {};
@@ -1333,6 +1655,34 @@ int bls_reduced_tmul(bls_qr_plan* P, int dtype, const void* F, const double* w, 
     else if (dtype == BLS_F32) launch_reduced_tmul<float>(P, (const float*)F, w, g);
     else throw Error(BLS_EINVAL, "unknown dtype");
     return BLS_OK;
+  })
+}
+
+int bls_lsmr_reduced(bls_qr_plan* P, int dtype, const void* F, const double* Fr, double lambda, const double* s_r, double* x,
+                     int64_t nx, double atol, double btol, double conlim, int64_t itmax, int64_t* iterations, int* istop,
+                     double* stats) {
+  QR_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "plan is NULL");
+    if (nx != P->nr) throw Error(BLS_EDIM, "x has length " + std::to_string(nx) + ", expected " + std::to_string(P->nr));
+    if (P->nr > 0 && (!F || !x || (P->red_nrows > 0 && !Fr))) throw Error(BLS_EINVAL, "a device pointer is NULL");
+    if (!(lambda >= 0) || !(atol >= 0) || !(btol >= 0) || !(conlim >= 0))
+      throw Error(BLS_EINVAL, "lambda, atol, btol and conlim must be non-negative");
+    if (itmax < 0) itmax = P->red_nrows + P->nr;
+    LsmrOut o;
+    int rc;
+    if (dtype == BLS_F64) rc = lsmr_reduced<double>(P, (const double*)F, Fr, lambda, s_r, x, atol, btol, conlim, itmax, &o);
+    else if (dtype == BLS_F32) rc = lsmr_reduced<float>(P, (const float*)F, Fr, lambda, s_r, x, atol, btol, conlim, itmax, &o);
+    else throw Error(BLS_EINVAL, "unknown dtype");
+    if (iterations) *iterations = o.iterations;
+    if (istop) *istop = o.istop;
+    if (stats) {
+      stats[0] = o.normr;
+      stats[1] = o.normar;
+      stats[2] = o.normA;
+      stats[3] = o.condA;
+      stats[4] = o.normx;
+    }
+    return rc;
   })
 }
 

@@ -21,12 +21,13 @@ FP64 column norms, reflector scalars and reflector application, rounded once per
 from __future__ import annotations
 
 import ctypes as C
+from dataclasses import dataclass
 
 import numpy as np
 import torch
 
 from . import _lib
-from ._lib import BLS_NOT_PD, ArgumentError, DimensionMismatch, check, dptr, ptr64
+from ._lib import BLS_NOT_CONVERGED, BLS_NOT_PD, ArgumentError, DimensionMismatch, check, dptr, ptr64
 from .layout import DEFAULT_MIN_WORK, SchurPattern, SchurStructure, _csr
 from .reduction import _dev, _dtype_code, context
 
@@ -411,3 +412,43 @@ def reduced_tmul(g: torch.Tensor, ws: QRReductionWorkspace, w: torch.Tensor) -> 
     check(_lib.gpu().bls_reduced_tmul(ws.handle, ws._T, dptr(ws.factored), dptr(w) if w.numel() else None, w.numel(),
                                       dptr(g) if g.numel() else None, g.numel()))
     return g
+
+
+@dataclass
+class LsmrResult:
+    """The outcome of lsmr_reduced: `solved` (the reference's Success), the iterations, Fong & Saunders' istop (1, 2, 4,
+    5 solved; 3, 6 cond(A) above conlim; 7 itmax) and their estimates for the preconditioned operator."""
+    solved: bool
+    iterations: int
+    istop: int
+    normr: float
+    normar: float
+    normA: float
+    condA: float
+    normx: float
+
+
+def lsmr_reduced(x_r: torch.Tensor, ws: QRReductionWorkspace, lam: float, s_r: torch.Tensor | None = None, *,
+                 atol: float | None = None, btol: float | None = None, conlim: float | None = None,
+                 itmax: int | None = None) -> LsmrResult:
+    """The reduced system's LSMR solve (ext/KrylovExt.jl:97-132) on the device: x_r = argmin ||[J~; sqrt(lam s_r)] x -
+    [r~; 0]|| from the workspace's factored tables (reduce_qr first), block-Jacobi preconditioned by the diagonal blocks
+    of J~'J~ + lam diag(s_r). Tolerances default to the reference's: sqrt(eps(T)) and conlim 1/sqrt(eps(T)) for the
+    workspace's storage type T; itmax to reduced_nrows + nr. `solved` is False where the reference returns
+    NotPositiveDefinite (a non-finite r~, lam == 0 with fewer reduced rows than retained variables, a diagonal block
+    that is not positive definite, cond(A) above conlim, itmax reached)."""
+    nr = ws.structure.schur.nr
+    _dev(x_r, "x_r", nr, torch.float64)
+    if s_r is not None:
+        _dev(s_r, "s_r", nr, torch.float64)
+    eps = float(np.finfo(np.float32 if ws.dtype == torch.float32 else np.float64).eps)
+    tol = np.sqrt(eps)
+    it, ist, stats = C.c_int64(0), C.c_int(0), (C.c_double * 5)()
+    rc = _lib.gpu().bls_lsmr_reduced(ws.handle, ws._T, dptr(ws.factored), dptr(ws.fres) if ws.fres.numel() else None, float(lam),
+                                     dptr(s_r) if s_r is not None and s_r.numel() else None,
+                                     dptr(x_r) if x_r.numel() else None, x_r.numel(), tol if atol is None else atol,
+                                     tol if btol is None else btol, 1.0 / tol if conlim is None else conlim,
+                                     -1 if itmax is None else itmax, C.byref(it), C.byref(ist), stats)
+    if rc not in (BLS_NOT_PD, BLS_NOT_CONVERGED):
+        check(rc)
+    return LsmrResult(rc == 0, int(it.value), int(ist.value), *[float(v) for v in stats])

@@ -352,6 +352,21 @@ int bls_reduced_jacobian_dense(bls_qr_plan* plan, int dtype, const void* F_dev, 
 int bls_reduced_jacobian_sparse(bls_qr_plan* plan, int dtype, const void* F_dev, const double* Fr_dev, int64_t nrows, int64_t ncols,
                                 const int64_t* colptr, const int64_t* rowval, void* nzval_dev, double* rt_dev, int64_t n_rt);
 
+/* LSMR on the reduced problem (replaces KrylovExt's solve!, ext/KrylovExt.jl:97-132, with reduced_mul! / reduced_tmul! /
+ * reduced_diagonal_blocks! of src/qr_reduced.jl as its operator): x_dev (nr doubles) = argmin || A x - [r~; 0] ||,
+ * A = [J~; diag(sqrt(lambda s_r))], J~ and r~ read from the factored tables F_dev / Fr_dev of the last reduce_qr, block-
+ * Jacobi preconditioned by the diagonal blocks of A'A (Krylov's N = D^-1). s_r_dev NULL: all ones. Stopping by the
+ * tolerances atol, btol and conlim of Fong & Saunders' LSMR (the reference passes sqrt(eps(T)) for the three and
+ * 1/sqrt(eps(T)) for conlim); itmax < 0: reduced_nrows + nr. The vectors and the block factors are FP64 for both dtypes.
+ * Returns BLS_OK (solved: istop 1, 2, 4 or 5), BLS_NOT_PD where the reference's solve! returns NotPositiveDefinite (a
+ * non-finite r~, lambda == 0 with fewer reduced rows than nr, a diagonal block that is not positive definite, cond(A)
+ * above conlim: istop 3 or 6, a non-finite x), BLS_NOT_CONVERGED at itmax (istop 7; also NotPositiveDefinite there).
+ * iterations, istop, stats (5 doubles: the estimates of ||r||, ||A'r||, ||A||, cond(A) of the preconditioned operator,
+ * and ||x||) may be NULL. */
+int bls_lsmr_reduced(bls_qr_plan* plan, int dtype, const void* F_dev, const double* Fr_dev, double lambda, const double* s_r_dev,
+                     double* x_dev, int64_t nx, double atol, double btol, double conlim, int64_t itmax, int64_t* iterations,
+                     int* istop, double* stats);
+
 /* ---------------------------------------------------------------------------------------------------------------
  * Block-Jacobi (src/diagonal_blocks.jl:6-61) on a flat array of square diagonal blocks (block b, d_b x d_b column-major,
  * after the blocks before it), as reduced_diagonal_blocks! writes them. d_b <= 16.
