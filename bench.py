@@ -367,6 +367,23 @@ def run_ours_qr(args, rank: int, world: int) -> dict | None:
         route_ms.append(a.elapsed_time(c))
     assert sws.query_status()
     asm = statistics.median(asm_ms)
+    # the matrix-free LSMR solve of the reduced problem (block-Jacobi preconditioned; the reference's Krylov extension)
+    # on the mixed tables: at the reference's tolerances for Float32 storage, and at 1e-10; wall time of the
+    # synchronous call, median of three
+    assert bls.reduce_qr(ws32, J32, sc_e, p.lam)
+    xr = torch.zeros(nr, dtype=torch.float64, device=dev)
+    lsmr = {}
+    for name, kw in (("tol_sqrt_eps_f32", {}), ("tol_1e-10", dict(atol=1e-10, btol=1e-10, conlim=1e14))):
+        res = bls.lsmr_reduced(xr, ws32, p.lam, **kw)
+        walls = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = bls.lsmr_reduced(xr, ws32, p.lam, **kw)
+            walls.append((time.perf_counter() - t0) * 1e3)
+        ms = statistics.median(walls)
+        lsmr[name] = {"ms": ms, "iterations": res.iterations, "istop": res.istop, "solved": res.solved,
+                      "ms_per_iteration": ms / max(res.iterations, 1)}
     st_ = jst.schur
     asm_bytes = int(jst.raw_length * 4 + jst.residual_length * 8 + (st_.E_length + st_.C_length + pat.nnz) * 4 + (st_.nr + st_.ne) * 8)
     if rank != 0:
@@ -398,6 +415,7 @@ def run_ours_qr(args, rank: int, world: int) -> dict | None:
                           "assemble_bytes": asm_bytes, "ms_per_step": statistics.median(route_ms),
                           "obs_per_s": nobs / (statistics.median(route_ms) / 1e3),
                           "step": "assemble_hessian (J'J, J'r from the f32 tables) + mixed reset_schur_sparse + reduce_schur_sparse"},
+        "lsmr": dict(lsmr, step="lsmr_reduced on the mixed factored tables, lambda of the workload, s_r = 1"),
     }
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_qr(spec, seconds=args.cpu_seconds)

@@ -70,6 +70,9 @@ struct QRPlan {
   // LSMR on the reduced problem (allocated at its first call): the augmented vector u (reduced_nrows + nr) and a
   // scratch of reduced_nrows, v, h, hbar and two scratch vectors (nr), sqrt(lambda s_r), the diagonal blocks (storage
   // type) and their FP64 Cholesky factors, the norm accumulators and the factorisation's flag
+  // reduced_tmul!'s per-(entry, column) dot products (allocated at its first call), rdmax = the largest retained block
+  DevBuf tm_part;
+  int rdmax = 0;
   DevBuf ls_u, ls_sc, ls_v, ls_h, ls_hbar, ls_t, ls_w, ls_sqd, ls_D, ls_L, ls_acc, ls_flag;
   double* ls_host = nullptr;
   DevBuf status;
@@ -688,32 +691,44 @@ __global__ void __launch_bounds__(256) k_reduced_mul(int64_t nt, const int32_t* 
   }
 }
 
-// reduced_tmul! (src/qr_reduced.jl:194-223): g = J~' w, a warp per retained block: per column, the dot product of each
-// of its entries' runs with w (a warp reduction in FP64), added in the order of the block's entries
+// reduced_tmul! (src/qr_reduced.jl:194-223): g = J~' w in two passes, so that the work spreads over every entry rather
+// than one warp per retained block (a few hundred warps on a bundle-adjustment scene, each walking thousands of runs
+// in sequence). Pass 1, a thread per (entry, column): the dot product of the entry's run in that column with w, FP64,
+// into part[u * dmax + j]. Pass 2, a warp per (retained block, column): the sum over the block's entries in their order
+// (lanes strided, then a butterfly), written to g. Deterministic: no atomics.
 template <class T>
-__global__ void __launch_bounds__(256) k_reduced_tmul(int64_t nrb, const int32_t* __restrict__ rptr, const int32_t* __restrict__ rent,
-                                                      const int32_t* __restrict__ u_tab, const int32_t* __restrict__ t_rows,
-                                                      const int32_t* __restrict__ t_top, const int64_t* __restrict__ t_raw,
-                                                      const int64_t* __restrict__ t_red, const int32_t* __restrict__ u_col,
-                                                      const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
-                                                      const T* __restrict__ F, const double* __restrict__ w, double* __restrict__ g) {
-  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+__global__ void __launch_bounds__(256) k_tmul_entries(int64_t nent, int dmax, const int32_t* __restrict__ u_tab,
+                                                      const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
+                                                      const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_red,
+                                                      const int32_t* __restrict__ u_col, const int32_t* __restrict__ u_ret,
+                                                      const int32_t* __restrict__ r_dims, const T* __restrict__ F,
+                                                      const double* __restrict__ w, double* __restrict__ part) {
+  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (gid >= nent * dmax) return;
+  const int64_t u = gid / dmax;
+  const int j = (int)(gid - u * dmax);
+  if (j >= r_dims[u_ret[u]]) return;
+  const int t = u_tab[u], M = t_rows[t], top = t_top[t], n = M - top;
+  const T* col = F + t_raw[t] + (int64_t)(u_col[u] + j) * M + top;
+  const double* wr = w + t_red[t];
+  double acc = 0.0;
+  for (int i = 0; i < n; ++i) acc += (double)col[i] * wr[i];
+  part[gid] = acc;
+}
+
+__global__ void __launch_bounds__(256) k_tmul_reduce(int64_t nrb, int dmax, const int32_t* __restrict__ rptr,
+                                                     const int32_t* __restrict__ rent, const int32_t* __restrict__ r_dims,
+                                                     const int32_t* __restrict__ boff_r, const double* __restrict__ part,
+                                                     double* __restrict__ g) {
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (r >= nrb) return;
-  const int dr = r_dims[r], ro = boff_r[r];
-  for (int j = 0; j < dr; ++j) {
-    double sum = 0.0;
-    for (int k = rptr[r]; k < rptr[r + 1]; ++k) {
-      const int u = rent[k], t = u_tab[u], M = t_rows[t], top = t_top[t], n = M - top;
-      const T* col = F + t_raw[t] + (int64_t)(u_col[u] + j) * M + top;
-      const double* wr = w + t_red[t];
-      double acc = 0.0;
-      for (int i = lane; i < n; i += 32) acc += (double)col[i] * wr[i];
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      sum += acc;
-    }
-    if (lane == 0) g[ro + j] = sum;
-  }
+  const int64_t r = gw / dmax;
+  const int j = (int)(gw - r * dmax);
+  if (r >= nrb || j >= r_dims[r]) return;   // uniform across the warp
+  double acc = 0.0;
+  for (int k = rptr[r] + lane; k < rptr[r + 1]; k += 32) acc += part[(int64_t)rent[k] * dmax + j];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) g[boff_r[r] + j] = acc;
 }
 
 template <class T>
@@ -727,10 +742,20 @@ static void launch_reduced_mul(QRPlan* P, const T* F, const double* v, double* y
 
 template <class T>
 static void launch_reduced_tmul(QRPlan* P, const T* F, const double* w, double* g) {
-  k_reduced_tmul<T><<<(unsigned)std::max(1, grid_for(P->nrblocks * 32, 256)), 256, 0, P->ctx->stream>>>(
-      P->nrblocks, P->q_rptr.as<int32_t>(), P->q_rent.as<int32_t>(), P->u_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(),
-      P->t_raw.as<int64_t>(), P->t_red.as<int64_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), F, w, g);
-  P->launches += 1;
+  cudaStream_t s = P->ctx->stream;
+  if (P->rdmax == 0)
+    for (int64_t d : P->h_rdims) P->rdmax = std::max<int>(P->rdmax, (int)d);
+  const int dm = std::max(P->rdmax, 1);
+  const size_t need = sizeof(double) * (size_t)std::max<int64_t>(P->nentries * dm, 1);
+  if (P->tm_part.bytes < need) P->tm_part.alloc(need);
+  double* part = P->tm_part.as<double>();
+  if (P->nentries > 0)
+    k_tmul_entries<T><<<(unsigned)grid_for(P->nentries * dm, 256), 256, 0, s>>>(
+        P->nentries, dm, P->u_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
+        P->t_red.as<int64_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->r_dims.as<int32_t>(), F, w, part);
+  k_tmul_reduce<<<(unsigned)std::max(1, grid_for(P->nrblocks * dm * 32, 256)), 256, 0, s>>>(
+      P->nrblocks, dm, P->q_rptr.as<int32_t>(), P->q_rent.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), part, g);
+  P->launches += 1 + (P->nentries > 0);
   BLS_CUDA(cudaGetLastError());
 }
 
