@@ -71,7 +71,7 @@ struct QRPlan {
   // scratch of reduced_nrows, v, h, hbar and two scratch vectors (nr), sqrt(lambda s_r), the diagonal blocks (storage
   // type) and their FP64 Cholesky factors, the norm accumulators and the factorisation's flag
   // reduced_tmul!'s per-(entry, column) dot products (allocated at its first call), rdmax = the largest retained block
-  DevBuf tm_part;
+  DevBuf tm_part, red_tab;
   int rdmax = 0;
   DevBuf ls_u, ls_sc, ls_v, ls_h, ls_hbar, ls_t, ls_w, ls_sqd, ls_D, ls_L, ls_acc, ls_flag;
   double* ls_host = nullptr;
@@ -666,29 +666,28 @@ static void reduced_jacobian_sparse(QRPlan* P, T* nzval, const T* F, const doubl
   BLS_CUDA(cudaGetLastError());
 }
 
-// reduced_mul! (src/qr_reduced.jl:159-192): y = J~ v, a warp per table, a lane per reduced row accumulating over the
-// table's entries and their columns in order (FP64)
+// reduced_mul! (src/qr_reduced.jl:159-192): y = J~ v, a thread per reduced row (its table from red_tab, so that warps
+// run across table boundaries rather than idling lanes past a table's few rows), accumulating over the table's entries
+// and their columns in order (FP64)
 template <class T>
-__global__ void __launch_bounds__(256) k_reduced_mul(int64_t nt, const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
-                                                     const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_red,
-                                                     const int32_t* __restrict__ t_ptr, const int32_t* __restrict__ u_ret,
-                                                     const int32_t* __restrict__ u_col, const int32_t* __restrict__ r_dims,
-                                                     const int32_t* __restrict__ boff_r, const T* __restrict__ F, const double* __restrict__ v,
-                                                     double* __restrict__ y) {
-  const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (t >= nt) return;
-  const int M = t_rows[t], top = t_top[t], n = M - top;
-  const int64_t raw = t_raw[t] + top, red = t_red[t];
+__global__ void __launch_bounds__(256) k_reduced_mul(int64_t nrows, const int32_t* __restrict__ red_tab, const int32_t* __restrict__ t_rows,
+                                                     const int32_t* __restrict__ t_top, const int64_t* __restrict__ t_raw,
+                                                     const int64_t* __restrict__ t_red, const int32_t* __restrict__ t_ptr,
+                                                     const int32_t* __restrict__ u_ret, const int32_t* __restrict__ u_col,
+                                                     const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                                                     const T* __restrict__ F, const double* __restrict__ v, double* __restrict__ y) {
+  const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (row >= nrows) return;
+  const int t = red_tab[row];
+  const int M = t_rows[t], top = t_top[t];
+  const int64_t raw = t_raw[t] + top + (row - t_red[t]);
   const int u0 = t_ptr[t], u1 = t_ptr[t + 1];
-  for (int i = lane; i < n; i += 32) {
-    double acc = 0.0;
-    for (int u = u0; u < u1; ++u) {
-      const int r = u_ret[u], dr = r_dims[r], c0 = u_col[u], ro = boff_r[r];
-      for (int j = 0; j < dr; ++j) acc += (double)F[raw + (int64_t)(c0 + j) * M + i] * v[ro + j];
-    }
-    y[red + i] = acc;
+  double acc = 0.0;
+  for (int u = u0; u < u1; ++u) {
+    const int r = u_ret[u], dr = r_dims[r], c0 = u_col[u], ro = boff_r[r];
+    for (int j = 0; j < dr; ++j) acc += (double)F[raw + (int64_t)(c0 + j) * M] * v[ro + j];
   }
+  y[row] = acc;
 }
 
 // reduced_tmul! (src/qr_reduced.jl:194-223): g = J~' w in two passes, so that the work spreads over every entry rather
@@ -733,9 +732,10 @@ __global__ void __launch_bounds__(256) k_tmul_reduce(int64_t nrb, int dmax, cons
 
 template <class T>
 static void launch_reduced_mul(QRPlan* P, const T* F, const double* v, double* y) {
-  k_reduced_mul<T><<<(unsigned)std::max(1, grid_for(P->ntables * 32, 256)), 256, 0, P->ctx->stream>>>(
-      P->ntables, P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_red.as<int64_t>(), P->t_ptr.as<int32_t>(),
-      P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), F, v, y);
+  if (P->red_nrows == 0) return;
+  k_reduced_mul<T><<<(unsigned)grid_for(P->red_nrows, 256), 256, 0, P->ctx->stream>>>(
+      P->red_nrows, P->red_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_red.as<int64_t>(),
+      P->t_ptr.as<int32_t>(), P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), F, v, y);
   P->launches += 1;
   BLS_CUDA(cudaGetLastError());
 }
@@ -971,6 +971,12 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
     P->h_red.assign((size_t)nt + 1, 0);
     for (int64_t t = 0; t < nt; ++t) P->h_red[t + 1] = P->h_red[t] + d->table_nrows[t] - d->table_top[t];
     P->red_nrows = P->h_red[nt];
+    {   // the table of every reduced row (reduced_mul!'s thread per row)
+      std::vector<int32_t> rtab((size_t)P->red_nrows);
+      for (int64_t t = 0; t < nt; ++t)
+        for (int64_t i = P->h_red[t]; i < P->h_red[t + 1]; ++i) rtab[(size_t)i] = (int32_t)t;
+      upload(P->red_tab, rtab, s);
+    }
     P->h_jt_colptr.assign((size_t)nr + 1, 0);
     P->h_boff_r = boff_r;
     P->h_rdims.assign(d->r_dims, d->r_dims + nrb);
