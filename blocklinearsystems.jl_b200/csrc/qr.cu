@@ -68,12 +68,12 @@ struct QRPlan {
   std::vector<int32_t> h_rptr, h_rent_tab;   // per retained block, the tables of its entries in ascending entry order
   std::vector<int64_t> h_boff_r, h_rdims;
   // LSMR on the reduced problem (allocated at its first call): the augmented vector u (reduced_nrows + nr) and a
-  // scratch of reduced_nrows, v, h, hbar and two scratch vectors (nr), sqrt(lambda s_r), the diagonal blocks (storage
-  // type) and their FP64 Cholesky factors, the norm accumulators and the factorisation's flag
+  // scratch of reduced_nrows, v, h, hbar and two scratch vectors (nr), sqrt(lambda s_r), the per-(entry, column pair)
+  // products of the diagonal blocks, their FP64 Cholesky factors, the norm accumulators and the factorisation's flag
   // reduced_tmul!'s per-(entry, column) dot products (allocated at its first call), rdmax = the largest retained block
   DevBuf tm_part, red_tab;
   int rdmax = 0;
-  DevBuf ls_u, ls_sc, ls_v, ls_h, ls_hbar, ls_t, ls_w, ls_sqd, ls_D, ls_L, ls_acc, ls_flag;
+  DevBuf ls_u, ls_sc, ls_v, ls_h, ls_hbar, ls_t, ls_w, ls_sqd, ls_part, ls_L, ls_acc, ls_flag;
   double* ls_host = nullptr;
   DevBuf status;
   long long* host_status = nullptr;
@@ -1161,18 +1161,64 @@ static void diagonal_blocks(QRPlan* P, T* D, const T* F) {
 // and the h update need). The vectors are FP64 on the device; the scalar recurrences of Fong & Saunders (SIAM J. Sci.
 // Comput. 33 (2011), LSMR with its estimates of ||r||, ||A'r||, ||A|| and cond(A)) run on the host.
 
-// D_b + sqd^2 on its diagonal, then its Cholesky factor L (lower, FP64, column-major) in place; a thread per block. A
-// block that is not positive definite (or not finite) records the lowest such block in *bad.
+// The diagonal blocks of J~'J~ in FP64, straight from the factored tables, in two passes as reduced_tmul!: a thread
+// per (entry, column pair a <= b) forms the pair's dot product over the entry's reduced rows into
+// part[u * npair + b (b + 1) / 2 + a]; a warp per (retained block, pair) sums its entries in order into both triangles
+// of L's block (column-major, at doff).
 template <class T>
+__global__ void __launch_bounds__(256) k_lsmr_diag_entries(int64_t nent, int npair, const int32_t* __restrict__ u_tab,
+                                                           const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
+                                                           const int64_t* __restrict__ t_raw, const int32_t* __restrict__ u_col,
+                                                           const int32_t* __restrict__ u_ret, const int32_t* __restrict__ r_dims,
+                                                           const T* __restrict__ F, double* __restrict__ part) {
+  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (gid >= nent * npair) return;
+  const int64_t u = gid / npair;
+  const int p = (int)(gid - u * npair);
+  int b = (int)((sqrtf(8.0f * p + 1.0f) - 1.0f) * 0.5f);
+  while ((b + 1) * (b + 2) / 2 <= p) ++b;
+  while (b * (b + 1) / 2 > p) --b;
+  const int a = p - b * (b + 1) / 2;
+  if (b >= r_dims[u_ret[u]]) return;
+  const int t = u_tab[u], M = t_rows[t], top = t_top[t], n = M - top;
+  const T* ca = F + t_raw[t] + (int64_t)(u_col[u] + a) * M + top;
+  const T* cb = F + t_raw[t] + (int64_t)(u_col[u] + b) * M + top;
+  double acc = 0.0;
+  for (int i = 0; i < n; ++i) acc += (double)ca[i] * (double)cb[i];
+  part[gid] = acc;
+}
+
+__global__ void __launch_bounds__(256) k_lsmr_diag_reduce(int64_t nrb, int npair, const int32_t* __restrict__ rptr,
+                                                          const int32_t* __restrict__ rent, const int32_t* __restrict__ r_dims,
+                                                          const int64_t* __restrict__ doff, const double* __restrict__ part,
+                                                          double* __restrict__ L) {
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t r = gw / npair;
+  const int p = (int)(gw - r * npair);
+  if (r >= nrb) return;
+  int b = 0;
+  while ((b + 1) * (b + 2) / 2 <= p) ++b;
+  const int a = p - b * (b + 1) / 2, d = r_dims[r];
+  if (b >= d) return;   // uniform across the warp
+  double acc = 0.0;
+  for (int k = rptr[r] + lane; k < rptr[r + 1]; k += 32) acc += part[(int64_t)rent[k] * npair + p];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) {
+    L[doff[r] + a + (int64_t)d * b] = acc;
+    L[doff[r] + b + (int64_t)d * a] = acc;
+  }
+}
+
+// D_b + sqd^2 on its diagonal, then its Cholesky factor (lower, column-major) in place in L; a thread per block. A
+// block that is not positive definite (or not finite) records the lowest such block in *bad.
 __global__ void k_lsmr_factor(int64_t nrb, const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
-                              const int64_t* __restrict__ doff, const T* __restrict__ Dt, const double* __restrict__ sqd,
-                              double* __restrict__ L, int* __restrict__ bad) {
+                              const int64_t* __restrict__ doff, const double* __restrict__ sqd, double* __restrict__ L,
+                              int* __restrict__ bad) {
   const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (b >= nrb) return;
   const int d = r_dims[b], ro = boff_r[b];
   double* a = L + doff[b];
-  const T* src = Dt + doff[b];
-  for (int q = 0; q < d * d; ++q) a[q] = (double)src[q];
   for (int i = 0; i < d; ++i) a[i + d * i] += sqd[ro + i] * sqd[ro + i];
   for (int j = 0; j < d; ++j) {
     double p = a[j + d * j];
@@ -1297,7 +1343,6 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
     P->ls_sc.alloc(sizeof(double) * (size_t)std::max<int64_t>(mt, 1));
     for (DevBuf* b : {&P->ls_v, &P->ls_h, &P->ls_hbar, &P->ls_t, &P->ls_w, &P->ls_sqd})
       b->alloc(sizeof(double) * (size_t)std::max<int64_t>(nr, 1));
-    P->ls_D.alloc(sizeof(double) * (size_t)std::max<int64_t>(P->ndiag, 1));
     P->ls_L.alloc(sizeof(double) * (size_t)std::max<int64_t>(P->ndiag, 1));
     P->ls_acc.alloc(sizeof(double) * 4);
     P->ls_flag.alloc(sizeof(int));
@@ -1325,9 +1370,22 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
     k_reduced_residual<<<(unsigned)std::max(1, grid_for(P->ntables * 32, 256)), 256, 0, s>>>(
         P->ntables, P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_res.as<int64_t>(), P->t_red.as<int64_t>(), Fr, u);
   k_lsmr_init<<<gm, 256, 0, s>>>(mt, nr, lambda, s_r, sqd, u, acc);
-  diagonal_blocks<T>(P, reinterpret_cast<T*>(P->ls_D.p), F);
-  k_lsmr_factor<T><<<gb, 128, 0, s>>>(nrb, rd, bo, doff, reinterpret_cast<const T*>(P->ls_D.p), sqd, L, flag);
-  P->launches += 3 + (mt > 0);
+  {
+    if (P->rdmax == 0)
+      for (int64_t d : P->h_rdims) P->rdmax = std::max<int>(P->rdmax, (int)d);
+    const int np = std::max(P->rdmax, 1) * (std::max(P->rdmax, 1) + 1) / 2;
+    const size_t need = sizeof(double) * (size_t)std::max<int64_t>(P->nentries * np, 1);
+    if (P->ls_part.bytes < need) P->ls_part.alloc(need);
+    BLS_CUDA(cudaMemsetAsync(L, 0, sizeof(double) * (size_t)P->ndiag, s));   // blocks without entries stay zero
+    if (P->nentries > 0)
+      k_lsmr_diag_entries<T><<<(unsigned)grid_for(P->nentries * np, 256), 256, 0, s>>>(
+          P->nentries, np, P->u_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
+          P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), rd, F, P->ls_part.as<double>());
+    k_lsmr_diag_reduce<<<(unsigned)std::max(1, grid_for(nrb * np * 32, 256)), 256, 0, s>>>(
+        nrb, np, P->q_rptr.as<int32_t>(), P->q_rent.as<int32_t>(), rd, doff, P->ls_part.as<double>(), L);
+  }
+  k_lsmr_factor<<<gb, 128, 0, s>>>(nrb, rd, bo, doff, sqd, L, flag);
+  P->launches += 4 + (mt > 0);
   BLS_CUDA(cudaGetLastError());
   BLS_CUDA(cudaMemcpyAsync(hv, acc, sizeof(double), cudaMemcpyDeviceToHost, s));
   int bad = 0;
