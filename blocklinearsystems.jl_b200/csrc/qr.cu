@@ -67,13 +67,12 @@ struct QRPlan {
   std::vector<int64_t> h_red, h_jt_colptr;
   std::vector<int32_t> h_rptr, h_rent_tab;   // per retained block, the tables of its entries in ascending entry order
   std::vector<int64_t> h_boff_r, h_rdims;
-  // LSMR on the reduced problem (allocated at its first call): the augmented vector u (reduced_nrows + nr) and a
-  // scratch of reduced_nrows, v, h, hbar and two scratch vectors (nr), sqrt(lambda s_r), the per-(entry, column pair)
+  // LSMR on the reduced problem (allocated at its first call): the augmented vector u (reduced_nrows + nr), v, h, hbar and two scratch vectors (nr), sqrt(lambda s_r), the per-(entry, column pair)
   // products of the diagonal blocks, their FP64 Cholesky factors, the norm accumulators and the factorisation's flag
   // reduced_tmul!'s per-(entry, column) dot products (allocated at its first call), rdmax = the largest retained block
   DevBuf tm_part, red_tab;
   int rdmax = 0;
-  DevBuf ls_u, ls_sc, ls_v, ls_h, ls_hbar, ls_t, ls_w, ls_sqd, ls_part, ls_L, ls_acc, ls_flag;
+  DevBuf ls_u, ls_v, ls_h, ls_hbar, ls_t, ls_w, ls_sqd, ls_part, ls_L, ls_acc, ls_flag;
   double* ls_host = nullptr;
   DevBuf status;
   long long* host_status = nullptr;
@@ -1283,14 +1282,35 @@ __global__ void k_lsmr_bwd(int64_t nrb, const int32_t* __restrict__ r_dims, cons
   }
 }
 
-// u = [Jt; sqd .* t] - a u (B v - alpha u, with Jt = J~ t), acc += |u|^2
-__global__ void k_lsmr_bv(int64_t mt, int64_t nr, const double* __restrict__ Jt, const double* __restrict__ sqd,
-                          const double* __restrict__ t, double a, double* __restrict__ u, double* __restrict__ acc) {
+// u = B t - a u with B t = [J~ t; sqd .* t] (a thread per row of u: a reduced row's product as reduced_mul! forms it,
+// then the damping rows), acc += |u|^2
+template <class T>
+__global__ void __launch_bounds__(256) k_lsmr_bv(int64_t mt, int64_t nr, const int32_t* __restrict__ red_tab,
+                                                 const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
+                                                 const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_red,
+                                                 const int32_t* __restrict__ t_ptr, const int32_t* __restrict__ u_ret,
+                                                 const int32_t* __restrict__ u_col, const int32_t* __restrict__ r_dims,
+                                                 const int32_t* __restrict__ boff_r, const T* __restrict__ F,
+                                                 const double* __restrict__ sqd, const double* __restrict__ t, double a,
+                                                 double* __restrict__ u, double* __restrict__ acc) {
+  const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double nn = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < mt + nr; i += (int64_t)gridDim.x * blockDim.x) {
-    const double z = (i < mt ? Jt[i] : sqd[i - mt] * t[i - mt]) - a * u[i];
-    u[i] = z;
-    nn += z * z;
+  if (row < mt) {
+    const int tb = red_tab[row];
+    const int M = t_rows[tb], top = t_top[tb];
+    const int64_t raw = t_raw[tb] + top + (row - t_red[tb]);
+    double y = 0.0;
+    for (int e = t_ptr[tb]; e < t_ptr[tb + 1]; ++e) {
+      const int r = u_ret[e], dr = r_dims[r], c0 = u_col[e], ro = boff_r[r];
+      for (int j = 0; j < dr; ++j) y += (double)F[raw + (int64_t)(c0 + j) * M] * t[ro + j];
+    }
+    const double z = y - a * u[row];
+    u[row] = z;
+    nn = z * z;
+  } else if (row < mt + nr) {
+    const double z = sqd[row - mt] * t[row - mt] - a * u[row];
+    u[row] = z;
+    nn = z * z;
   }
   warp_sum_add(nn, acc);
 }
@@ -1340,7 +1360,6 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
   const int64_t mt = P->red_nrows, nr = P->nr, nrb = P->nrblocks, m = mt + nr;
   if (!P->ls_u.p) {
     P->ls_u.alloc(sizeof(double) * (size_t)std::max<int64_t>(m, 1));
-    P->ls_sc.alloc(sizeof(double) * (size_t)std::max<int64_t>(mt, 1));
     for (DevBuf* b : {&P->ls_v, &P->ls_h, &P->ls_hbar, &P->ls_t, &P->ls_w, &P->ls_sqd})
       b->alloc(sizeof(double) * (size_t)std::max<int64_t>(nr, 1));
     P->ls_L.alloc(sizeof(double) * (size_t)std::max<int64_t>(P->ndiag, 1));
@@ -1348,7 +1367,7 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
     P->ls_flag.alloc(sizeof(int));
     BLS_CUDA(cudaMallocHost(reinterpret_cast<void**>(&P->ls_host), sizeof(double) * 4));
   }
-  double *u = P->ls_u.as<double>(), *Jt = P->ls_sc.as<double>(), *v = P->ls_v.as<double>(), *h = P->ls_h.as<double>();
+  double *u = P->ls_u.as<double>(), *v = P->ls_v.as<double>(), *h = P->ls_h.as<double>();
   double *hbar = P->ls_hbar.as<double>(), *t = P->ls_t.as<double>(), *w = P->ls_w.as<double>(), *sqd = P->ls_sqd.as<double>();
   double *L = P->ls_L.as<double>(), *acc = P->ls_acc.as<double>(), *hv = P->ls_host;
   int* flag = P->ls_flag.as<int>();
@@ -1447,8 +1466,10 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
     // u_raw = B v - alpha u
     if (itn < itmax) {
       BLS_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2, s));
-      if (mt > 0) launch_reduced_mul<T>(P, F, t, Jt);
-      k_lsmr_bv<<<gm, 256, 0, s>>>(mt, nr, Jt, sqd, t, alpha * uscale, u, acc);
+      k_lsmr_bv<T><<<(unsigned)grid_for(m, 256), 256, 0, s>>>(
+          mt, nr, P->red_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
+          P->t_red.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), rd, bo, F, sqd, t,
+          alpha * uscale, u, acc);
       P->launches += 1;
     }
     read(3);
