@@ -70,7 +70,7 @@ struct QRPlan {
   // LSMR on the reduced problem (allocated at its first call): the augmented vector u (reduced_nrows + nr), v, h, hbar and two scratch vectors (nr), sqrt(lambda s_r), the per-(entry, column pair)
   // products of the diagonal blocks, their FP64 Cholesky factors, the norm accumulators and the factorisation's flag
   // reduced_tmul!'s per-(entry, column) dot products (allocated at its first call), rdmax = the largest retained block
-  DevBuf tm_part, red_tab;
+  DevBuf tm_part, red_tab, u_meta;
   int rdmax = 0;
   DevBuf ls_u, ls_v, ls_h, ls_hbar, ls_t, ls_w, ls_sqd, ls_part, ls_L, ls_acc, ls_flag;
   double* ls_host = nullptr;
@@ -695,19 +695,19 @@ __global__ void __launch_bounds__(256) k_reduced_mul(int64_t nrows, const int32_
 // into part[u * dmax + j]. Pass 2, a warp per (retained block, column): the sum over the block's entries in their order
 // (lanes strided, then a butterfly), written to g. Deterministic: no atomics.
 template <class T>
-__global__ void __launch_bounds__(256) k_tmul_entries(int64_t nent, int dmax, const int32_t* __restrict__ u_tab,
+__global__ void __launch_bounds__(256) k_tmul_entries(int64_t nent, int dmax, const int4* __restrict__ meta,
                                                       const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
                                                       const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_red,
-                                                      const int32_t* __restrict__ u_col, const int32_t* __restrict__ u_ret,
-                                                      const int32_t* __restrict__ r_dims, const T* __restrict__ F,
-                                                      const double* __restrict__ w, double* __restrict__ part) {
+                                                      const T* __restrict__ F, const double* __restrict__ w,
+                                                      double* __restrict__ part) {
   const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (gid >= nent * dmax) return;
   const int64_t u = gid / dmax;
   const int j = (int)(gid - u * dmax);
-  if (j >= r_dims[u_ret[u]]) return;
-  const int t = u_tab[u], M = t_rows[t], top = t_top[t], n = M - top;
-  const T* col = F + t_raw[t] + (int64_t)(u_col[u] + j) * M + top;
+  const int4 q = meta[u];   // column, retained offset, retained size, table
+  if (j >= q.z) return;
+  const int t = q.w, M = t_rows[t], top = t_top[t], n = M - top;
+  const T* col = F + t_raw[t] + (int64_t)(q.x + j) * M + top;
   const double* wr = w + t_red[t];
   double acc = 0.0;
   for (int i = 0; i < n; ++i) acc += (double)col[i] * wr[i];
@@ -750,8 +750,8 @@ static void launch_reduced_tmul(QRPlan* P, const T* F, const double* w, double* 
   double* part = P->tm_part.as<double>();
   if (P->nentries > 0)
     k_tmul_entries<T><<<(unsigned)grid_for(P->nentries * dm, 256), 256, 0, s>>>(
-        P->nentries, dm, P->u_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
-        P->t_red.as<int64_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->r_dims.as<int32_t>(), F, w, part);
+        P->nentries, dm, P->u_meta.as<int4>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
+        P->t_red.as<int64_t>(), F, w, part);
   k_tmul_reduce<<<(unsigned)std::max(1, grid_for(P->nrblocks * dm * 32, 256)), 256, 0, s>>>(
       P->nrblocks, dm, P->q_rptr.as<int32_t>(), P->q_rent.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), part, g);
   P->launches += 1 + (P->nentries > 0);
@@ -965,6 +965,15 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
     upload(P->q_rptr, rptr, s);
     upload(P->q_rent, rent, s);
     upload(P->u_tab, utab, s);
+    {   // each entry's column, retained offset, retained size and table in one 16-byte load (the products of the
+        // reduced problem read them per entry)
+      std::vector<int4> meta((size_t)nent);
+      for (int64_t u = 0; u < nent; ++u) {
+        const int64_t r = d->entry_retained[u];
+        meta[(size_t)u] = make_int4((int)d->entry_col[u], (int)boff_r[r], (int)d->r_dims[r], utab[(size_t)u]);
+      }
+      upload(P->u_meta, meta, s);
+    }
     // the reduced problem: build_reduced_jacobian_pattern's column heights (the reduced rows of every table coupled to
     // the column's retained block, tables in ascending order) and each entry's run position in those columns
     P->h_red.assign((size_t)nt + 1, 0);
@@ -1165,11 +1174,10 @@ static void diagonal_blocks(QRPlan* P, T* D, const T* F) {
 // part[u * npair + b (b + 1) / 2 + a]; a warp per (retained block, pair) sums its entries in order into both triangles
 // of L's block (column-major, at doff).
 template <class T>
-__global__ void __launch_bounds__(256) k_lsmr_diag_entries(int64_t nent, int npair, const int32_t* __restrict__ u_tab,
+__global__ void __launch_bounds__(256) k_lsmr_diag_entries(int64_t nent, int npair, const int4* __restrict__ meta,
                                                            const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
-                                                           const int64_t* __restrict__ t_raw, const int32_t* __restrict__ u_col,
-                                                           const int32_t* __restrict__ u_ret, const int32_t* __restrict__ r_dims,
-                                                           const T* __restrict__ F, double* __restrict__ part) {
+                                                           const int64_t* __restrict__ t_raw, const T* __restrict__ F,
+                                                           double* __restrict__ part) {
   const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (gid >= nent * npair) return;
   const int64_t u = gid / npair;
@@ -1178,10 +1186,11 @@ __global__ void __launch_bounds__(256) k_lsmr_diag_entries(int64_t nent, int npa
   while ((b + 1) * (b + 2) / 2 <= p) ++b;
   while (b * (b + 1) / 2 > p) --b;
   const int a = p - b * (b + 1) / 2;
-  if (b >= r_dims[u_ret[u]]) return;
-  const int t = u_tab[u], M = t_rows[t], top = t_top[t], n = M - top;
-  const T* ca = F + t_raw[t] + (int64_t)(u_col[u] + a) * M + top;
-  const T* cb = F + t_raw[t] + (int64_t)(u_col[u] + b) * M + top;
+  const int4 q = meta[u];   // column, retained offset, retained size, table
+  if (b >= q.z) return;
+  const int t = q.w, M = t_rows[t], top = t_top[t], n = M - top;
+  const T* ca = F + t_raw[t] + (int64_t)(q.x + a) * M + top;
+  const T* cb = F + t_raw[t] + (int64_t)(q.x + b) * M + top;
   double acc = 0.0;
   for (int i = 0; i < n; ++i) acc += (double)ca[i] * (double)cb[i];
   part[gid] = acc;
@@ -1288,10 +1297,9 @@ template <class T>
 __global__ void __launch_bounds__(256) k_lsmr_bv(int64_t mt, int64_t nr, const int32_t* __restrict__ red_tab,
                                                  const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_top,
                                                  const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_red,
-                                                 const int32_t* __restrict__ t_ptr, const int32_t* __restrict__ u_ret,
-                                                 const int32_t* __restrict__ u_col, const int32_t* __restrict__ r_dims,
-                                                 const int32_t* __restrict__ boff_r, const T* __restrict__ F,
-                                                 const double* __restrict__ sqd, const double* __restrict__ t, double a,
+                                                 const int32_t* __restrict__ t_ptr, const int4* __restrict__ meta,
+                                                 const T* __restrict__ F, const double* __restrict__ sqd,
+                                                 const double* __restrict__ t, double a,
                                                  double* __restrict__ u, double* __restrict__ acc) {
   const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double nn = 0.0;
@@ -1301,8 +1309,8 @@ __global__ void __launch_bounds__(256) k_lsmr_bv(int64_t mt, int64_t nr, const i
     const int64_t raw = t_raw[tb] + top + (row - t_red[tb]);
     double y = 0.0;
     for (int e = t_ptr[tb]; e < t_ptr[tb + 1]; ++e) {
-      const int r = u_ret[e], dr = r_dims[r], c0 = u_col[e], ro = boff_r[r];
-      for (int j = 0; j < dr; ++j) y += (double)F[raw + (int64_t)(c0 + j) * M] * t[ro + j];
+      const int4 q = meta[e];   // column, retained offset, retained size
+      for (int j = 0; j < q.z; ++j) y += (double)F[raw + (int64_t)(q.x + j) * M] * t[q.y + j];
     }
     const double z = y - a * u[row];
     u[row] = z;
@@ -1398,8 +1406,8 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
     BLS_CUDA(cudaMemsetAsync(L, 0, sizeof(double) * (size_t)P->ndiag, s));   // blocks without entries stay zero
     if (P->nentries > 0)
       k_lsmr_diag_entries<T><<<(unsigned)grid_for(P->nentries * np, 256), 256, 0, s>>>(
-          P->nentries, np, P->u_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
-          P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), rd, F, P->ls_part.as<double>());
+          P->nentries, np, P->u_meta.as<int4>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(), F,
+          P->ls_part.as<double>());
     k_lsmr_diag_reduce<<<(unsigned)std::max(1, grid_for(nrb * np * 32, 256)), 256, 0, s>>>(
         nrb, np, P->q_rptr.as<int32_t>(), P->q_rent.as<int32_t>(), rd, doff, P->ls_part.as<double>(), L);
   }
@@ -1468,8 +1476,7 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
       BLS_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 2, s));
       k_lsmr_bv<T><<<(unsigned)grid_for(m, 256), 256, 0, s>>>(
           mt, nr, P->red_tab.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
-          P->t_red.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), rd, bo, F, sqd, t,
-          alpha * uscale, u, acc);
+          P->t_red.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_meta.as<int4>(), F, sqd, t, alpha * uscale, u, acc);
       P->launches += 1;
     }
     read(3);
