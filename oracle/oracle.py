@@ -610,3 +610,112 @@ def hessian_dense(st: Structure, R, E, Cd, pat: Pattern | None = None):
             H[so:so + de, ro:ro + dr] = B
             H[ro:ro + dr, so:so + de] = B.T
     return H
+
+
+def lsmr_reduced(Jt, rt, r_dims, lam, s_r=None, atol=1e-8, btol=1e-8, conlim=1e8, itmax=None):
+    """The LSMR solve of the reduced problem (ext/KrylovExt.jl:97-132) restated with numpy on the written-out J~ (dense,
+    m x nr) and r~: min ||[J~; sqrt(lam s_r)] x - [r~; 0]|| with the block-Jacobi N = D^-1 (D the diagonal blocks of
+    A'A, blocks of sizes r_dims) as the change of variables x = L^-T y, D = L L'. The recurrences are Fong & Saunders'
+    LSMR (SIAM J. Sci. Comput. 33, 2011: two plane rotations per step, the estimates of ||r||, ||A'r||, ||A||,
+    cond(A), stopping tests 1-7) without internal damping, ||x|| taken in the original variables. Returns
+    (x, status, iterations, istop) with status "ok", "not_pd" (the reference's NotPositiveDefinite: non-finite r~, lam
+    == 0 with fewer rows than columns, a block of D not positive definite, istop 3 or 6) or "itmax"."""
+    Jt = np.asarray(Jt, np.float64)
+    m, nr = Jt.shape
+    itmax = m + nr if itmax is None else itmax
+    sqd = np.sqrt(lam * (np.ones(nr) if s_r is None else np.asarray(s_r, np.float64)))
+    A = np.vstack([Jt, np.diag(sqd)])
+    b = np.concatenate([np.asarray(rt, np.float64), np.zeros(nr)])
+    if not np.all(np.isfinite(rt)):
+        return np.zeros(nr), "not_pd", 0, 0
+    if lam == 0 and m < nr:
+        return np.zeros(nr), "not_pd", 0, 0
+    Linv = np.zeros((nr, nr))   # block diagonal L^-1
+    o = 0
+    for d in r_dims:
+        d = int(d)
+        Db = A[:, o:o + d].T @ A[:, o:o + d]
+        try:
+            Lb = np.linalg.cholesky(Db)
+        except np.linalg.LinAlgError:
+            return np.zeros(nr), "not_pd", 0, 0
+        Linv[o:o + d, o:o + d] = np.linalg.inv(Lb)
+        o += d
+    C = Linv.T                  # x = C y
+    B = A @ C
+    x = np.zeros(nr)
+    beta = np.linalg.norm(b)
+    if beta == 0:
+        return x, "ok", 0, 0
+    u = b / beta
+    v = B.T @ u
+    alpha = np.linalg.norm(v)
+    if alpha > 0:
+        v = v / alpha
+    h, hbar = C @ v, np.zeros(nr)
+    zetabar, alphabar, rho, rhobar, cbar, sbar = alpha * beta, alpha, 1.0, 1.0, 1.0, 0.0
+    betadd, betad, rhodold, tautildeold, thetatilde, zeta = beta, 0.0, 1.0, 0.0, 0.0, 0.0
+    normA2, maxrbar, minrbar = alpha * alpha, 0.0, 1e100
+    normb, ctol = beta, (1.0 / conlim if conlim > 0 else 0.0)
+    if alpha * beta == 0:
+        return x, "ok", 0, 0
+    itn, istop = 0, 0
+    while istop == 0:
+        itn += 1
+        u = B @ v - alpha * u
+        beta = np.linalg.norm(u)
+        if beta > 0:
+            u = u / beta
+            v = B.T @ u - beta * v
+            alpha = np.linalg.norm(v)
+            if alpha > 0:
+                v = v / alpha
+        rhoold = rho
+        rho = np.hypot(alphabar, beta)
+        c, s = alphabar / rho, beta / rho
+        thetanew = s * alpha
+        alphabar = c * alpha
+        rhobarold, zetaold, thetabar, rhotemp = rhobar, zeta, sbar * rho, cbar * rho
+        rhobar = np.hypot(cbar * rho, thetanew)
+        cbar, sbar = cbar * rho / rhobar, thetanew / rhobar
+        zeta, zetabar = cbar * zetabar, -sbar * zetabar
+        hbar = h - (thetabar * rho / (rhoold * rhobarold)) * hbar
+        x = x + (zeta / (rho * rhobar)) * hbar
+        h = C @ v - (thetanew / rho) * h
+        betahat, betadd = c * betadd, -s * betadd
+        thetatildeold, rhotildeold = thetatilde, np.hypot(rhodold, thetabar)
+        ctildeold, stildeold = rhodold / rhotildeold, thetabar / rhotildeold
+        thetatilde, rhodold = stildeold * rhobar, ctildeold * rhobar
+        betad = -stildeold * betad + ctildeold * betahat
+        tautildeold = (zetaold - thetatildeold * tautildeold) / rhotildeold
+        taud = (zeta - thetatilde * tautildeold) / rhodold
+        normr = np.sqrt((betad - taud) ** 2 + betadd ** 2)
+        normA2 += beta * beta
+        normA = np.sqrt(normA2)
+        normA2 += alpha * alpha
+        maxrbar = max(maxrbar, rhobarold)
+        if itn > 1:
+            minrbar = min(minrbar, rhobarold)
+        condA = max(maxrbar, rhotemp) / min(minrbar, rhotemp)
+        normar, normx = abs(zetabar), np.linalg.norm(x)
+        test1 = normr / normb
+        test2 = normar / (normA * normr) if normA * normr != 0 else np.inf
+        test3 = 1.0 / condA
+        t1 = test1 / (1.0 + normA * normx / normb)
+        rtol = btol + atol * normA * normx / normb
+        if itn >= itmax:
+            istop = 7
+        if 1.0 + test3 <= 1.0:
+            istop = 6
+        if 1.0 + test2 <= 1.0:
+            istop = 5
+        if 1.0 + t1 <= 1.0:
+            istop = 4
+        if test3 <= ctol:
+            istop = 3
+        if test2 <= atol:
+            istop = 2
+        if test1 <= rtol:
+            istop = 1
+    status = "itmax" if istop == 7 else ("not_pd" if istop in (3, 6) else "ok")
+    return x, status, itn, istop

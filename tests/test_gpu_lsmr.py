@@ -3,7 +3,8 @@
 against the direct solution of the same damped least-squares problem, here numpy's lstsq of the written-out
 [J~; sqrt(lambda s_r)] and [r~; 0] (reduced_jacobian! of the same factored tables), at rtol 1e-6 in the norm, for
 lambda in {0, 1e-8, 1e-4}, with and without a scaling s_r, on the QR fixtures with retained columns scaled over six
-orders of magnitude, in FP64 and the mixed form; then the reference's NotPositiveDefinite cases and an itmax stop."""
+orders of magnitude, in FP64 and the mixed form; then the reference's NotPositiveDefinite cases and an itmax stop;
+and against the oracle's restatement of the same LSMR on the same written-out problem (stops, iterations, iterates)."""
 import numpy as np
 import pytest
 import torch
@@ -134,3 +135,36 @@ def test_not_positive_definite_and_itmax(bls):
     assert not res.solved and res.istop == 7 and res.iterations == 2
     with pytest.raises(bls.DimensionMismatch):
         bls.lsmr_reduced(torch.zeros(nr + 1, dtype=torch.float64, device=DEV), ws, 1e-4)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+@pytest.mark.parametrize("name", list(QR_FIXTURES))
+def test_lsmr_against_the_oracle(bls, name, dtype):
+    """The device's LSMR against the oracle's restatement on the same written-out J~ and r~ (the device's own factored
+    tables), at the reference's tolerances for the storage type: the same stop (istop), iteration counts within one,
+    solutions within 1e-6 (at equal iteration counts)."""
+    import oracle as orc
+    j, Rw, Rr, sc_e, s_r = problem(bls, name)
+    npdt = np.float32 if dtype == torch.float32 else np.float64
+    ws = bls.QRReductionWorkspace(j, None, dtype)
+    J = bls.SchurBlockJacobian(j, dtype, data=cu(Rw.astype(npdt)), r=cu(Rr))
+    m, nr = bls.reduced_nrows(j), j.schur.nr
+    tol = float(np.sqrt(np.finfo(npdt).eps))
+    for lam, scaled in CASES:
+        if lam == 0 and m < nr:
+            continue
+        assert bls.reduce_qr(ws, J, cu(sc_e), lam)
+        s = s_r if scaled else None
+        Jt = torch.zeros(m * nr, dtype=dtype, device=DEV)
+        rt = torch.zeros(m, dtype=torch.float64, device=DEV)
+        bls.reduced_jacobian(Jt, rt, ws)
+        A = Jt.cpu().double().numpy().reshape(m, nr, order="F")
+        xo, status, it, istop = orc.lsmr_reduced(A, rt.cpu().numpy(), j.schur.r_dims, lam, s, atol=tol, btol=tol, conlim=1 / tol)
+        x = torch.zeros(nr, dtype=torch.float64, device=DEV)
+        res = bls.lsmr_reduced(x, ws, lam, None if s is None else cu(s))
+        assert res.solved == (status == "ok"), (lam, scaled, res, status)
+        assert abs(res.iterations - it) <= 1, (lam, scaled, res.iterations, it)
+        if res.iterations == it:
+            assert res.istop == istop
+        if res.solved:   # the same iterate to rounding; one iteration apart, within the stopping tolerance's reach
+            assert close(x.cpu().numpy(), xo, 1e-6 if res.iterations == it else 100 * tol), (lam, scaled, res)
