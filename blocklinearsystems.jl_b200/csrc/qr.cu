@@ -1450,6 +1450,13 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
     out->normr = normr;
     return BLS_OK;
   }
+  if (itmax == 0) {   // no iteration allowed: x = 0, stopped on itmax
+    out->istop = 7;
+    out->normr = normr;
+    out->normar = normar;
+    BLS_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)nr, s));
+    return BLS_NOT_CONVERGED;
+  }
   // The tests of an iteration need ||x||, which the update kernel accumulates; they are evaluated at the next
   // iteration's first read-back, after B v of the next step has been launched (at itmax, without it)
   auto tests = [&]() -> int {

@@ -659,6 +659,8 @@ def lsmr_reduced(Jt, rt, r_dims, lam, s_r=None, atol=1e-8, btol=1e-8, conlim=1e8
     normb, ctol = beta, (1.0 / conlim if conlim > 0 else 0.0)
     if alpha * beta == 0:
         return x, "ok", 0, 0
+    if itmax == 0:
+        return x, "itmax", 0, 7
     itn, istop = 0, 0
     while istop == 0:
         itn += 1

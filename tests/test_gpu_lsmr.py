@@ -133,6 +133,9 @@ def test_not_positive_definite_and_itmax(bls):
     assert bls.reduce_qr(ws, J, cu(sc_e), 1e-4)
     res = bls.lsmr_reduced(x, ws, 1e-4, atol=0.0, btol=0.0, conlim=0.0, itmax=2)
     assert not res.solved and res.istop == 7 and res.iterations == 2
+    x.fill_(1.0)
+    res = bls.lsmr_reduced(x, ws, 1e-4, itmax=0)
+    assert not res.solved and res.istop == 7 and res.iterations == 0 and not bool(x.any())
     with pytest.raises(bls.DimensionMismatch):
         bls.lsmr_reduced(torch.zeros(nr + 1, dtype=torch.float64, device=DEV), ws, 1e-4)
 

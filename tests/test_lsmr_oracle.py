@@ -53,3 +53,5 @@ def test_not_positive_definite_and_itmax():
     assert orc.lsmr_reduced(J, rn, rd, 1e-4)[1] == "not_pd"
     x, status, it, istop = orc.lsmr_reduced(J, r, rd, 1e-4, atol=0.0, btol=0.0, conlim=0.0, itmax=2)
     assert status == "itmax" and istop == 7 and it == 2
+    x, status, it, istop = orc.lsmr_reduced(J, r, rd, 1e-4, itmax=0)
+    assert status == "itmax" and istop == 7 and it == 0 and not x.any()
