@@ -327,6 +327,30 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
       atomicAdd(g + gi, acc);
     }
   }
+  // From the raw tables (the assembly), an entry's columns are zero outside its own observations' rows in a
+  // bundle-adjustment table: each entry's nonzero row span [lo, hi) bounds its products, and a pair whose spans do not
+  // meet adds nothing (the output was zeroed). The spans go to rr once J'r is done; a table with more entries than rr
+  // has slots keeps the full range.
+  const int2* span = nullptr;
+  if (from_raw && kt <= ((n + 1) & ~1)) {
+    __syncwarp();
+    int2* sp = reinterpret_cast<int2*>(rr);
+    for (int ul = lane; ul < kt; ul += 32) {
+      const int c0 = u_col[u0 + ul], d = r_dims[u_ret[u0 + ul]];
+      int lo = n, hi = 0;
+      for (int i = 0; i < n; ++i) {
+        bool nz = false;
+        for (int a = 0; a < d; ++a) nz |= B[(c0 + a) * ns + i] != T(0);
+        if (nz) {
+          lo = min(lo, i);
+          hi = i + 1;
+        }
+      }
+      sp[ul] = make_int2(lo, hi);
+    }
+    __syncwarp();
+    span = sp;
+  }
   // work units: (pair, a group of three columns of the pair's block); lanes take units in order, so the lanes of one
   // pair read the same X rows (shared-memory broadcast)
   const int npairs = kt * (kt + 1) / 2;
@@ -343,6 +367,8 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
     const int r1 = u_ret[u0 + u1l], r2 = u_ret[u0 + u2l];
     const int d1 = r_dims[r1], d2 = r_dims[r2];
     if (w0 >= d2) continue;
+    const int ilo = span ? max(span[u1l].x, span[u2l].x) : 0, ihi = span ? min(span[u1l].y, span[u2l].y) : n;
+    if (ilo >= ihi) continue;
     const T* X = B + u_col[u0 + u1l] * ns;
     const T* Y = B + (u_col[u0 + u2l] + w0) * ns;
     T* out;
@@ -362,7 +388,7 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
       for (int w = 0; w < G; ++w)
 #pragma unroll
         for (int a = 0; a < 6; ++a) acc[w][a] = T(0);
-      for (int i = 0; i < n; ++i) {
+      for (int i = ilo; i < ihi; ++i) {
         T x[6], y[G];
 #pragma unroll
         for (int a = 0; a < 6; ++a) x[a] = X[a * ns + i];
@@ -383,7 +409,7 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
         double acc[16];
 #pragma unroll
         for (int a = 0; a < 16; ++a) acc[a] = 0.0;
-        for (int i = 0; i < n; ++i) {
+        for (int i = ilo; i < ihi; ++i) {
           const double y = (double)Y[(w - w0) * ns + i];
 #pragma unroll
           for (int a = 0; a < 16; ++a)
