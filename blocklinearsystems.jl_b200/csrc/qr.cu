@@ -736,6 +736,7 @@ __global__ void __launch_bounds__(256) k_tmul_entries(int64_t nent, int dmax, co
   const T* col = F + t_raw[t] + (int64_t)(q.x + j) * M + top;
   const double* wr = w + t_red[t];
   double acc = 0.0;
+#pragma unroll 4
   for (int i = 0; i < n; ++i) acc += (double)col[i] * wr[i];
   part[gid] = acc;
 }
@@ -1336,7 +1337,16 @@ __global__ void __launch_bounds__(256) k_lsmr_bv(int64_t mt, int64_t nr, const i
     double y = 0.0;
     for (int e = t_ptr[tb]; e < t_ptr[tb + 1]; ++e) {
       const int4 q = meta[e];   // column, retained offset, retained size
-      for (int j = 0; j < q.z; ++j) y += (double)F[raw + (int64_t)(q.x + j) * M] * t[q.y + j];
+      const T* col = F + raw + (int64_t)q.x * M;
+      if (q.z == 6) {           // the common camera block: six independent loads in flight
+        T f[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) f[j] = col[(int64_t)j * M];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) y += (double)f[j] * t[q.y + j];
+      } else {
+        for (int j = 0; j < q.z; ++j) y += (double)col[(int64_t)j * M] * t[q.y + j];
+      }
     }
     const double z = y - a * u[row];
     u[row] = z;
