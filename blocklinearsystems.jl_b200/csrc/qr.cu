@@ -710,7 +710,16 @@ __global__ void __launch_bounds__(256) k_reduced_mul(int64_t nrows, const int32_
   double acc = 0.0;
   for (int u = u0; u < u1; ++u) {
     const int r = u_ret[u], dr = r_dims[r], c0 = u_col[u], ro = boff_r[r];
-    for (int j = 0; j < dr; ++j) acc += (double)F[raw + (int64_t)(c0 + j) * M] * v[ro + j];
+    const T* col = F + raw + (int64_t)c0 * M;
+    if (dr == 6) {   // the common camera block: six independent loads in flight
+      T f[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) f[j] = col[(int64_t)j * M];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) acc += (double)f[j] * v[ro + j];
+    } else {
+      for (int j = 0; j < dr; ++j) acc += (double)col[(int64_t)j * M] * v[ro + j];
+    }
   }
   y[row] = acc;
 }
@@ -1219,6 +1228,7 @@ __global__ void __launch_bounds__(256) k_lsmr_diag_entries(int64_t nent, int npa
   const T* ca = F + t_raw[t] + (int64_t)(q.x + a) * M + top;
   const T* cb = F + t_raw[t] + (int64_t)(q.x + b) * M + top;
   double acc = 0.0;
+#pragma unroll 4
   for (int i = 0; i < n; ++i) acc += (double)ca[i] * (double)cb[i];
   part[gid] = acc;
 }
