@@ -343,7 +343,8 @@ int bls_reduced_diagonal_blocks(bls_qr_plan* plan, int dtype, void* D_dev, const
 /* reduced_mul! (src/qr_reduced.jl:159-192): y = J~ v (ny = reduced_nrows, nv = nr); reduced_tmul!
  * (src/qr_reduced.jl:194-223): g = J~' w (ng = nr, nw = reduced_nrows); FP64 vectors, products accumulated in FP64,
  * applied from the factored tables without forming J~ (the per-iteration work of an LSMR solve of the reduced
- * problem). A wrong length is BLS_EDIM. */
+ * problem). A wrong length is BLS_EDIM. reduced_tmul! keeps a scratch of n_entries x (largest retained block) doubles
+ * in the plan, allocated at its first call; its sums are deterministic (no atomics). */
 int bls_reduced_mul(bls_qr_plan* plan, int dtype, const void* F_dev, const double* v_dev, int64_t nv, double* y_dev, int64_t ny);
 int bls_reduced_tmul(bls_qr_plan* plan, int dtype, const void* F_dev, const double* w_dev, int64_t nw, double* g_dev, int64_t ng);
 int bls_reduced_residual(bls_qr_plan* plan, const double* Fr_dev, double* rt_dev, int64_t n_rt);
@@ -362,7 +363,8 @@ int bls_reduced_jacobian_sparse(bls_qr_plan* plan, int dtype, const void* F_dev,
  * non-finite r~, lambda == 0 with fewer reduced rows than nr, a diagonal block that is not positive definite, cond(A)
  * above conlim: istop 3 or 6, a non-finite x), BLS_NOT_CONVERGED at itmax (istop 7; also NotPositiveDefinite there).
  * iterations, istop, stats (5 doubles: the estimates of ||r||, ||A'r||, ||A||, cond(A) of the preconditioned operator,
- * and ||x||) may be NULL. */
+ * and ||x||) may be NULL. The plan keeps the solve's vectors and scratch (allocated at its first call); the call
+ * synchronises the context's stream twice per iteration to read the norms. */
 int bls_lsmr_reduced(bls_qr_plan* plan, int dtype, const void* F_dev, const double* Fr_dev, double lambda, const double* s_r_dev,
                      double* x_dev, int64_t nx, double atol, double btol, double conlim, int64_t itmax, int64_t* iterations,
                      int* istop, double* stats);
