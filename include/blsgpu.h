@@ -11,8 +11,10 @@
  *     damped point-block inverse, z = E^-1 b_e, the gradient and the QR column norms / reflector scaling in FP64.
  *   - Work runs on the context's stream. A call that takes a host `int64_t* failed_block` synchronises and returns the
  *     reduction's verdict; passing NULL makes the call asynchronous (read it later with the *_query_status call).
- *   - Nothing here allocates device memory except the create calls (contexts, plans); kernels only use the caller's
- *     buffers and the plan's own scratch.
+ *   - Device memory is allocated by the create calls (contexts, plans, solvers) and, once per plan, by the first call
+ *     of bls_reduced_tmul and bls_lsmr_reduced (their scratch, kept in the plan); bls_symmetrify_full stages its block
+ *     list in stream-ordered memory (cudaMallocAsync) for the call. Kernels otherwise use only the caller's buffers
+ *     and the plan's own scratch; bls_reduce_schur_dense_noalloc allocates nothing.
  *
  * Status codes: BLS_OK, BLS_NOT_PD (the reference's `false`: a singular / non-finite eliminated block; the lowest
  * such block, 1-based as the reference's failed_block[], is reported), and negative errors. Argument errors are
