@@ -384,6 +384,15 @@ def run_ours_qr(args, rank: int, world: int) -> dict | None:
         ms = statistics.median(walls)
         lsmr[name] = {"ms": ms, "iterations": res.iterations, "istop": res.istop, "solved": res.solved,
                       "ms_per_iteration": ms / max(res.iterations, 1)}
+    # the bound of an iteration: J~ read twice (J~ t and J~' u; the retained columns of every table's reduced rows)
+    n_red = (np.asarray(jst.table_nrows) - np.asarray(jst.table_top)).astype(np.int64)
+    ent_tab = np.repeat(np.arange(jst.ntables), np.diff(np.asarray(jst.table_ptr)))
+    jt_bytes = int(np.sum(n_red[ent_tab] * np.asarray(jst.schur.r_dims)[np.asarray(jst.entry_retained)])) * 4
+    a_, b_ = lsmr["tol_sqrt_eps_f32"], lsmr["tol_1e-10"]
+    if b_["iterations"] > a_["iterations"]:
+        per_it = (b_["ms"] - a_["ms"]) / (b_["iterations"] - a_["iterations"])
+        lsmr["per_iteration"] = {"ms": per_it, "jt_bytes_f32": jt_bytes, "achieved_gbs": 2 * jt_bytes / (per_it / 1e3) / 1e9,
+                                 "note": "wall ms per extra iteration (two host read-backs included) over two passes of J~"}
     st_ = jst.schur
     asm_bytes = int(jst.raw_length * 4 + jst.residual_length * 8 + (st_.E_length + st_.C_length + pat.nnz) * 4 + (st_.nr + st_.ne) * 8)
     if rank != 0:
