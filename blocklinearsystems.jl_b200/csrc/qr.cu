@@ -1369,17 +1369,31 @@ __global__ void __launch_bounds__(256) k_lsmr_bv(int64_t mt, int64_t nr, const i
   warp_sum_add(nn, acc);
 }
 
-// hbar = h - c1 hbar; x += c2 hbar; h = t - c3 h; acc += |x|^2
-__global__ void k_lsmr_update(int64_t n, const double* __restrict__ t, double* __restrict__ h, double* __restrict__ hbar,
-                              double* __restrict__ x, double c1, double c2, double c3, double* __restrict__ acc) {
+// One iteration's end, a thread per block: v *= sc, t = L^-T v, then for the block's entries hbar = h - c1 hbar,
+// x += c2 hbar, h = t - c3 h; acc += |x|^2
+__global__ void k_lsmr_bwd_update(int64_t nrb, const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                                  const int64_t* __restrict__ doff, const double* __restrict__ L, double sc, double* __restrict__ v,
+                                  double* __restrict__ t, double* __restrict__ h, double* __restrict__ hbar, double* __restrict__ x,
+                                  double c1, double c2, double c3, double* __restrict__ acc) {
+  const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double nn = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double hb = h[i] - c1 * hbar[i];
-    hbar[i] = hb;
-    const double xi = x[i] + c2 * hb;
-    x[i] = xi;
-    h[i] = t[i] - c3 * h[i];
-    nn += xi * xi;
+  if (b < nrb) {
+    const int d = r_dims[b], ro = boff_r[b];
+    const double* a = L + doff[b];
+    for (int i = 0; i < d; ++i) v[ro + i] *= sc;
+    for (int i = d - 1; i >= 0; --i) {
+      double q = v[ro + i];
+      for (int k = i + 1; k < d; ++k) q -= a[k + d * i] * t[ro + k];
+      t[ro + i] = q / a[i + d * i];
+    }
+    for (int i = ro; i < ro + d; ++i) {
+      const double hb = h[i] - c1 * hbar[i];
+      hbar[i] = hb;
+      const double xi = x[i] + c2 * hb;
+      x[i] = xi;
+      h[i] = t[i] - c3 * h[i];
+      nn += xi * xi;
+    }
   }
   warp_sum_add(nn, acc);
 }
@@ -1428,7 +1442,6 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
   const int32_t *rd = P->r_dims.as<int32_t>(), *bo = P->boff_r.as<int32_t>();
   const int64_t* doff = P->doff.as<int64_t>();
   const unsigned gm = (unsigned)std::max(1, std::min(grid_for(m, 256), 148 * 8));
-  const unsigned gn = (unsigned)std::max(1, std::min(grid_for(nr, 256), 148 * 8));
   const unsigned gb = (unsigned)std::max(1, grid_for(nrb, 128));
   auto read = [&](int k) {   // the first k norm accumulators to the host
     BLS_CUDA(cudaMemcpyAsync(hv, acc, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
@@ -1550,11 +1563,10 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
       read(2);
       alpha = std::sqrt(hv[1]);
       if (!std::isfinite(alpha)) return BLS_NOT_PD;
-      k_lsmr_bwd<<<gb, 128, 0, s>>>(nrb, rd, bo, doff, L, alpha > 0 ? 1.0 / alpha : 1.0, v, t);
-      P->launches += 1;
     } else {
       uscale = 0.0;
     }
+    const double vscale = beta > 0 && alpha > 0 ? 1.0 / alpha : 1.0;   // v unchanged when beta = 0: t is recomputed as is
     // the plane rotations (no regularisation in LSMR itself: the damping rows are part of A)
     const double alphahat = alphabar;
     const double rhoold = rho;
@@ -1570,8 +1582,8 @@ static int lsmr_reduced(QRPlan* P, const T* F, const double* Fr, double lambda, 
     zetabar = -sbar * zetabar;
     // hbar = h - (thetabar rho / (rhoold rhobarold)) hbar; x += (zeta / (rho rhobar)) hbar; h = t - (thetanew / rho) h
     BLS_CUDA(cudaMemsetAsync(acc + 2, 0, sizeof(double), s));
-    k_lsmr_update<<<gn, 256, 0, s>>>(nr, t, h, hbar, x, thetabar * rho / (rhoold * rhobarold), zeta / (rho * rhobar),
-                                     thetanew / rho, acc + 2);
+    k_lsmr_bwd_update<<<gb, 128, 0, s>>>(nrb, rd, bo, doff, L, vscale, v, t, h, hbar, x, thetabar * rho / (rhoold * rhobarold),
+                                         zeta / (rho * rhobar), thetanew / rho, acc + 2);
     P->launches += 1;
     // ||r||: the rotations applied to (betadd, betad) and the running tau
     const double betaacute = betadd, betahat = c * betaacute;
