@@ -1,5 +1,6 @@
-"""Benchmark: observations/s through the Schur reduction of the sparse_1000x200k scene (1,000 cameras, 200,000 points,
-~1.2M observations), on N GPUs as N independent replicas (the reduction has no cross-GPU exchange).
+"""Benchmark: observations/s through the Schur reduction of the pcg_10000x1M scene (10,000 cameras, 1,000,000 points,
+~7.7M observations), then block-Jacobi PCG on the reduced system to 1e-8, on N GPUs as N independent replicas (the
+reduction has no cross-GPU exchange).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
@@ -7,13 +8,17 @@ A step is one reset_schur_sparse + reduce_schur_sparse of the whole scene. `valu
 and accumulation, FP64 point-block inverse, z and gradient) with inputs resident in device memory, L2 flushed
 between steps; `fp64` reports the plain FP64 form the same way. `e2e` runs the same step through the public API from
 pinned host buffers: one reset_reduce_schur_sparse_host call per step, which copies the inputs in stage by stage while
-the earlier stages are reduced and copies S and g_S out. The roofline is the pair kernel's: the
-algorithmic bytes of the reduction (per point 84 + 76 k bytes in the mixed form, plus one read and one write of S),
-over its event-timed duration, against the measured HBM copy bandwidth.
+the earlier stages are reduced and copies S and g_S out. The roofline is the phase-2 kernel's: the algorithmic bytes
+of the reduction (per point 84 + 76 k bytes in the mixed form, plus one read and one write of S), over its
+event-timed duration, against the measured HBM copy bandwidth. `pcg` adds seconds to ||g - S x|| <= 1e-8 ||g||
+(FP64 residual) on the mixed S, and the refined solve against the FP64 reduced operator to 1e-10. The CPU-baseline
+leg runs the oracle's FP64 reduction of the same scene and reports the device results' distance from it (`parity`).
 
 --impl reference times the reference algorithm (the oracle: a C++ restatement of BlockLinearSystems.jl's
 reset_schur_sparse! + reduce_schur_sparse!, threaded over its chunks as the reference threads over Polyester chunks)
-on every host core, in FP64: the reference's Float32 path rejects this scene's point blocks as singular.
+on every host core, in FP64: the reference's Float32 path rejects this scene's point blocks as singular. Its inputs
+are generated by a separate, untimed child process and read back from .npy files, so the timed process loads no
+library of this repository.
 """
 from __future__ import annotations
 
@@ -25,6 +30,7 @@ import subprocess
 import sys
 import time
 from pathlib import Path
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -120,6 +126,60 @@ def replica_spec(spec, rank: int, world: int):
     return replace(spec, seed=spec.seed + 100 * rank)
 
 
+L2_NOTE = "flushed between timed steps (256 MB write)"
+SCHUR_STEP = "reset_schur_sparse + reduce_schur_sparse"
+QR_STEP = "reduce_qr + reduced_normal_sparse"
+
+
+def hessian_config(workload: str, world: int, cameras: int, points: int, observations: int, nnz_S: int) -> dict:
+    """The `config` both arms print for a Hessian workload (the reference arm reads the numbers from its fixture)."""
+    return {"workload": workload, "cameras": int(cameras), "points": int(points), "observations": int(observations),
+            "nnz_S": int(nnz_S), "parallelism": f"replicas x{world}", "l2": L2_NOTE, "step": SCHUR_STEP}
+
+
+def qr_config(workload: str, world: int, cameras: int, points: int, observations: int, table_entries: int, nnz_S: int) -> dict:
+    return {"workload": workload, "cameras": int(cameras), "points": int(points), "observations": int(observations),
+            "table_entries": int(table_entries), "nnz_S": int(nnz_S), "parallelism": f"replicas x{world}", "l2": L2_NOTE,
+            "step": QR_STEP}
+
+
+def dense_config(workload: str, world: int, cameras: int, points: int, n: int) -> dict:
+    return {"workload": workload, "cameras": int(cameras), "points": int(points), "n": int(n),
+            "step": "bls_dense_cholesky + bls_dense_cholesky_solve", "l2": "S (288 MB) larger than L2",
+            "parallelism": f"replicas x{world}"}
+
+
+def batch_config(workload: str, world: int, problems: int, cameras: int, points: int, observations: int, nnz_S: int) -> dict:
+    return {"workload": workload, "problems": int(problems), "cameras": int(cameras), "points": int(points),
+            "observations": int(observations), "nnz_S": int(nnz_S), "parallelism": f"replicas x{world}", "l2": L2_NOTE,
+            "step": "one CUDA graph replay: reset_schur_sparse + reduce_schur_sparse of all problems (disjoint-union plan)"}
+
+
+def measured_traffic(workload: str, kernel: str) -> float | None:
+    """DRAM read + write bytes per launch of `kernel` on `workload`, from one ncu capture summarised under profiles/
+    (traffic_<workload>.json, keyed by kernel name); None when no capture of that kernel on that workload exists."""
+    f = ROOT / "profiles" / f"traffic_{workload}.json"
+    if not f.exists():
+        return None
+    rec = json.loads(f.read_text()).get(kernel)
+    return None if rec is None else rec.get("dram_bytes_per_launch")
+
+
+def schur_parity(S_orc: np.ndarray, g_orc: np.ndarray, results: dict) -> dict:
+    """Distance of the device results from the oracle's FP64 reduction of the same scene: ||S - S_oracle|| /
+    ||S_oracle|| and the same for g_S, per form, against the tolerances the tests use (1e-12 FP64, 1e-4 mixed)."""
+    out = {"reference": "oracle FP64 reset_schur_sparse + reduce_schur_sparse of the same inputs (the CPU-baseline run)"}
+    ok = True
+    ns, ng = float(np.linalg.norm(S_orc)), float(np.linalg.norm(g_orc))
+    for name, (S, g, tol) in results.items():
+        es = float(np.linalg.norm(S.astype(np.float64) - S_orc)) / ns
+        eg = float(np.linalg.norm(g - g_orc)) / ng
+        out[name] = {"S_rel": es, "g_rel": eg, "tol": tol}
+        ok = ok and es <= tol and eg <= tol
+    out["ok"] = ok
+    return out
+
+
 def run_ours(args, rank: int, world: int) -> dict | None:
     import torch
     bls = load_package()
@@ -174,8 +234,10 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     with ClockSampler(dev.index) as clk:
         ms32, cnt32 = timed(d32, args.steps, args.warmup, instrument=True)
     _LAST.update(problem=p, d32=d32, ws=ws, step=step)
+    S32h, g32h = d32["S"].cpu().numpy(), d32["g"].cpu().numpy()   # the last timed step's results (parity below)
     d64 = device_inputs(torch.float64)
     ms64, cnt64 = timed(d64, args.steps, args.warmup, instrument=True)
+    S64h, g64h = d64["S"].cpu().numpy(), d64["g"].cpu().numpy()
     del d64
 
     # end to end through the public API from pinned host buffers (mixed form)
@@ -218,23 +280,19 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     pair_ms = cnt32["pair_kernel_ms"] / max(cnt32["pair_kernel_launches"], 1)
     bytes32 = algorithmic_bytes(p, 4)
     achieved = bytes32 / (pair_ms / 1e3) / 1e9
-    traffic = None
-    prof = ROOT / "profiles" / "pairs_sparse_1000x200k.json"
-    if prof.exists():
-        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch_f32")
+    kernel = ws.phase2_kernel_name(torch.float32)
     out = {
         "metric": METRIC, "value": value, "unit": "obs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 storage/accumulation + f64 point inverse, z, gradient", "data": "synthetic (seeded scene generator)",
-        "config": {"workload": args.workload, "cameras": st.nrblocks, "points": st.neblocks, "observations": nobs,
-                   "nnz_S": pat.nnz, "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MB write)",
-                   "step": "reset_schur_sparse + reduce_schur_sparse"},
+        "config": hessian_config(args.workload, world, st.nrblocks, st.neblocks, nobs, pat.nnz),
         "fp64": {"value": v64, "unit": "obs/s", "ms_per_step": ms64 / args.steps,
-                 "pair_kernel_ms": cnt64["pair_kernel_ms"] / max(cnt64["pair_kernel_launches"], 1)},
+                 "phase2_kernel_ms": cnt64["pair_kernel_ms"] / max(cnt64["pair_kernel_launches"], 1),
+                 "phase2_kernel": ws.phase2_kernel_name(torch.float64)},
         "mixed_over_fp64": value / v64,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                     "kernel": "k_pairs36<float>", "kernel_ms": pair_ms, "algorithmic_bytes": bytes32,
-                     "peak_source": "measured" if peaks else "fallback",
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": measured_traffic(args.workload, kernel), "kernel": kernel, "kernel_ms": pair_ms,
+                     "algorithmic_bytes": bytes32, "peak_source": "measured" if peaks else "fallback",
                      "flops": algorithmic_flops(p), "achieved_tflops": algorithmic_flops(p) / (pair_ms / 1e3) / 1e12},
         "e2e": {"value": world * nobs * args.steps / (e2e_ms / 1e3), "unit": "obs/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
@@ -242,7 +300,11 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(p, spec, seconds=args.cpu_seconds)
+        view = hessian_view(bls, spec, p)
+        base, S_orc, g_orc = cpu_baseline(view, seconds=args.cpu_seconds)
+        _LAST.update(view=view, oracle_S=S_orc, oracle_g=g_orc)
+        out["cpu_baseline"] = base
+        out["parity"] = schur_parity(S_orc, g_orc, {"fp64": (S64h, g64h, 1e-12), "mixed": (S32h, g32h, 1e-4)})
     return out
 
 
@@ -427,27 +489,22 @@ def run_ours_qr(args, rank: int, world: int) -> dict | None:
         "lsmr": dict(lsmr, step="lsmr_reduced on the mixed factored tables, lambda of the workload, s_r = 1"),
     }
     if not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline_qr(spec, seconds=args.cpu_seconds)
+        out["cpu_baseline"] = cpu_baseline_qr(jacobian_view(bls, spec, p), seconds=args.cpu_seconds)
     return out
 
 
-def cpu_baseline_qr(spec, seconds: float = 10.0, steps: int | None = None, warmup: int = 1) -> dict:
+def cpu_baseline_qr(v, seconds: float = 10.0, steps: int | None = None, warmup: int = 1) -> dict:
     """The reference algorithm (oracle) on every host core, FP64: reduce_qr threaded over its chunks, then
     reduced_normal_sparse threaded over retained block columns, as the reference threads them."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as orc
-    bls = load_package()
+    orc = oracle_module()
     cores = os.cpu_count() or 1
-    p = bls.scenes.jacobian_problem(spec)
-    sc = bls.scenes.Scene(spec)
-    bs, el, ptr, idx = sc.description()
-    o = orc.QRStructure.from_description(bs, (ptr, idx), np.full(len(ptr) - 1, 2), el, nchunks=cores)
+    o = orc.QRStructure.from_description(v.bs, (v.ptr, v.idx), np.full(len(v.ptr) - 1, 2), v.el, nchunks=cores)
     opat = orc.Pattern(o.st)
     F, Fr = np.zeros(o.raw_length), np.zeros(o.residual_length)
     S, g = np.zeros(opat.nnz), np.zeros(o.st.nr)
 
     def one():
-        ok, _ = orc.reduce_qr(o, F, Fr, p.Rw, p.Rr, p.scaling_e, p.lam, nthreads=cores)
+        ok, _ = orc.reduce_qr(o, F, Fr, v.Rw, v.Rr, v.scaling_e, v.lam, nthreads=cores)
         assert ok
         orc.reduced_normal_sparse(o, opat, S, g, F, Fr)
 
@@ -458,8 +515,8 @@ def cpu_baseline_qr(spec, seconds: float = 10.0, steps: int | None = None, warmu
         one()
         n += 1
     dt = time.perf_counter() - t0
-    return {"value": p.nobs * n / dt, "unit": "obs/s", "cores": cores, "kind": "port",
-            "sample": f"{n} x full reduce_qr + reduced_normal_sparse of {spec.npoints} points / {p.nobs} observations, FP64, "
+    return {"value": v.nobs * n / dt, "unit": "obs/s", "cores": cores, "kind": "port",
+            "sample": f"{n} x full reduce_qr + reduced_normal_sparse of {int(v.el.sum())} points / {v.nobs} observations, FP64, "
                       f"{cores} OpenMP threads ({dt:.1f} s)"}
 
 
@@ -521,7 +578,7 @@ def run_ours_pcg(args, rank: int, world: int) -> dict | None:
                              "residual": "FP64 g - A x, A = R + lambda D - C' E^-1 C from the stored blocks",
                              "inner": "PCG on the f32 S to 1e-6 per correction"}
     if not args.no_cpu_baseline:
-        out["pcg"]["cpu_baseline"] = cpu_baseline_pcg(p, args.workload)
+        out["pcg"]["cpu_baseline"] = cpu_baseline_pcg(_LAST["view"], _LAST["oracle_S"], _LAST["oracle_g"])
     return out
 
 
@@ -655,13 +712,14 @@ def run_ours_dense(args, rank: int, world: int) -> dict | None:
     return out
 
 
-def dense_reduced_host(spec, p):
+def dense_reduced_host(v):
     """The dense S and g of the scene from the oracle's reset_schur_dense + reduce_schur_dense (FP64, every host core)."""
-    orc, p, ost, _, cores = oracle_problem(spec, p)
-    n = p.structure.nr
+    cores = os.cpu_count() or 1
+    orc, ost, _ = oracle_structure(v, cores)
+    n = ost.nr
     S, g = np.zeros(n * n), np.zeros(n)
-    orc.reset_schur_dense(ost, S, p.R, p.scaling_r, p.lam)
-    ok, _ = orc.reduce_schur_dense(ost, orc.Work(ost, cores, False), S, g, p.b_r, p.b_e, p.scaling_e, p.lam, p.E, p.C, nthreads=cores)
+    orc.reset_schur_dense(ost, S, v.R, v.scaling_r, v.lam)
+    ok, _ = orc.reduce_schur_dense(ost, orc.Work(ost, cores, False), S, g, v.b_r, v.b_e, v.scaling_e, v.lam, v.E, v.C, nthreads=cores)
     assert ok
     return S, g
 
@@ -788,44 +846,36 @@ def run_ours_batch(args, rank: int, world: int) -> dict | None:
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline_batch(problems, args.workload, seconds=args.cpu_seconds)
+        out["cpu_baseline"] = cpu_baseline_batch([hessian_view(bls, p.spec, p) for p in problems], seconds=args.cpu_seconds)
     return out
 
 
-def cpu_baseline_batch(problems, workload: str, seconds: float = 10.0) -> dict:
+def cpu_baseline_batch(views, seconds: float = 10.0) -> dict:
     """The reference algorithm (oracle) on every host core, FP64: each problem reset + reduced in turn."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as orc
-    bls = load_package()
+    orc = oracle_module()
     cores = os.cpu_count() or 1
     prepared = []
-    for p in problems:
-        sc = bls.scenes.Scene(p.spec)
-        bs, el, ptr, idx = sc.description()
-        ost = orc.Structure.from_description(bs, (ptr, idx), el, nchunks=cores, min_work=4096)
-        opat = orc.Pattern(ost)
-        prepared.append((p, ost, opat, orc.Work(ost, cores, False), np.zeros(opat.nnz), np.zeros(ost.nr)))
+    for v in views:
+        _, ost, opat = oracle_structure(v, cores)
+        prepared.append((v, ost, opat, orc.Work(ost, cores, False), np.zeros(opat.nnz), np.zeros(ost.nr)))
     n, nobs, t0 = 0, 0, time.perf_counter()
     while time.perf_counter() - t0 < seconds or n < 1:
-        for p, ost, opat, w, S, g in prepared:
-            orc.reset_schur_sparse(ost, opat, S, p.R, p.scaling_r, p.lam)
-            ok, _ = orc.reduce_schur_sparse(ost, opat, w, S, g, p.b_r, p.b_e, p.scaling_e, p.lam, p.E, p.C, nthreads=cores)
+        for v, ost, opat, w, S, g in prepared:
+            orc.reset_schur_sparse(ost, opat, S, v.R, v.scaling_r, v.lam)
+            ok, _ = orc.reduce_schur_sparse(ost, opat, w, S, g, v.b_r, v.b_e, v.scaling_e, v.lam, v.E, v.C, nthreads=cores)
             assert ok
-            nobs += p.nobs
+            nobs += v.nobs
         n += 1
     dt = time.perf_counter() - t0
     return {"value": nobs / dt, "unit": "obs/s", "cores": cores, "kind": "port",
-            "sample": f"{n} x all {len(problems)} problems reset + reduced in turn, FP64, {cores} OpenMP threads ({dt:.1f} s)"}
+            "sample": f"{n} x all {len(views)} problems reset + reduced in turn, FP64, {cores} OpenMP threads ({dt:.1f} s)"}
 
 
-def cpu_baseline_pcg(p, workload: str) -> dict:
-    """The oracle's PCG (the same algorithm on every host core) on the FP64 reduced system of the same scene."""
-    orc, _, ost, opat, cores = oracle_problem(load_package().scenes.workload(workload), p)
-    w = orc.Work(ost, cores, False)
-    S, g = np.zeros(opat.nnz), np.zeros(ost.nr)
-    orc.reset_schur_sparse(ost, opat, S, p.R, p.scaling_r, p.lam)
-    ok, _ = orc.reduce_schur_sparse(ost, opat, w, S, g, p.b_r, p.b_e, p.scaling_e, p.lam, p.E, p.C, nthreads=cores)
-    assert ok
+def cpu_baseline_pcg(v, S: np.ndarray, g: np.ndarray) -> dict:
+    """The oracle's PCG (the same algorithm on every host core) on the oracle's FP64 reduced system of the same scene."""
+    orc = oracle_module()
+    _, ost, opat = oracle_structure(v, os.cpu_count() or 1)
+    cores = os.cpu_count() or 1
     x = np.zeros(ost.nr)
     t0 = time.perf_counter()
     rc, it, rel = orc.pcg_solve(ost, opat, S, g, x, 1e-8, nthreads=cores)
@@ -834,30 +884,102 @@ def cpu_baseline_pcg(p, workload: str) -> dict:
             "sample": f"one block-Jacobi PCG solve to 1e-8, FP64, {cores} OpenMP threads"}
 
 
-def oracle_problem(spec, p=None):
+# --- the inputs of a workload as plain numpy arrays ------------------------------------------------------------------
+# Both arms hand the oracle a "view": the scene's description (blocksizes, eliminated flags, row-block pointers and
+# indices) and its assembled arrays. The repository arm builds it from its own problem; the reference arm reads it from
+# .npy files that a separate, untimed child process wrote, so that the timed reference process maps no library of
+# this repository (only numpy and the oracle).
+HESSIAN_ARRAYS = ("bs", "el", "ptr", "idx", "E", "C", "R", "b_r", "b_e", "scaling_r", "scaling_e")
+JACOBIAN_ARRAYS = ("bs", "el", "ptr", "idx", "Rw", "Rr", "scaling_e")
+
+
+def hessian_view(bls, spec, p) -> SimpleNamespace:
+    bs, el, ptr, idx = bls.scenes.Scene(spec).description()
+    return SimpleNamespace(bs=bs, el=el, ptr=ptr, idx=idx, E=p.E, C=p.C, R=p.R, b_r=p.b_r, b_e=p.b_e, scaling_r=p.scaling_r,
+                           scaling_e=p.scaling_e, lam=float(p.lam), nobs=int(p.nobs))
+
+
+def jacobian_view(bls, spec, p) -> SimpleNamespace:
+    bs, el, ptr, idx = bls.scenes.Scene(spec).description()
+    return SimpleNamespace(bs=bs, el=el, ptr=ptr, idx=idx, Rw=p.Rw, Rr=p.Rr, scaling_e=p.scaling_e, lam=float(p.lam),
+                           nobs=int(p.nobs))
+
+
+def _save_view(d: Path, v: SimpleNamespace, names) -> None:
+    d.mkdir(parents=True, exist_ok=True)
+    for k in names:
+        a = getattr(v, k)
+        np.save(d / f"{k}.npy", np.ascontiguousarray(a.astype(np.uint8) if k == "el" else a))
+    (d / "scalars.json").write_text(json.dumps({"lam": v.lam, "nobs": v.nobs}))
+
+
+def _load_view(d: Path, names) -> SimpleNamespace:
+    v = SimpleNamespace(**{k: np.load(d / f"{k}.npy") for k in names})
+    v.el = v.el.astype(bool)
+    sc = json.loads((d / "scalars.json").read_text())
+    v.lam, v.nobs = float(sc["lam"]), int(sc["nobs"])
+    return v
+
+
+def write_fixture(workload: str, out: Path) -> None:
+    """Generate the workload with this repository's scene generator and write the reference arm's inputs and the
+    numbers of its `config` (run in a child process by --impl reference)."""
+    bls = load_package()
+    out.mkdir(parents=True, exist_ok=True)
+    if workload.startswith("batched_"):
+        nprob, sums = 256, dict(cameras=0, points=0, observations=0, nnz_S=0)
+        for i in range(nprob):
+            spec = bls.scenes.workload(workload, i)
+            p = bls.scenes.hessian_problem(spec)
+            _save_view(out / f"p{i:03d}", hessian_view(bls, spec, p), HESSIAN_ARRAYS)
+            sums["cameras"] += p.structure.nrblocks
+            sums["points"] += p.structure.neblocks
+            sums["observations"] += p.nobs
+            sums["nnz_S"] += p.pattern.nnz
+        meta = dict(kind="batch", problems=nprob, **sums)
+    elif workload.startswith("qr_"):
+        spec = bls.scenes.workload(workload)
+        p = bls.scenes.jacobian_problem(spec)
+        jst = p.structure
+        pat = bls.build_schur_pattern(jst.schur, bls.free_block_pairs(jst))
+        _save_view(out, jacobian_view(bls, spec, p), JACOBIAN_ARRAYS)
+        meta = dict(kind="qr", cameras=jst.schur.nrblocks, points=jst.schur.neblocks, observations=p.nobs,
+                    table_entries=int(np.sum(jst.table_nrows * (jst.table_ncols - 1))), nnz_S=pat.nnz)
+    else:
+        spec = bls.scenes.workload(workload)
+        dense = workload.startswith("dense_")
+        p = bls.scenes.hessian_problem(spec, dense=dense)
+        _save_view(out, hessian_view(bls, spec, p), HESSIAN_ARRAYS)
+        st = p.structure
+        meta = dict(kind="dense" if dense else "hessian", cameras=st.nrblocks, points=st.neblocks, observations=p.nobs,
+                    n=st.nr, nnz_S=0 if dense else p.pattern.nnz)
+    (out / "meta.json").write_text(json.dumps(meta))
+
+
+def oracle_module():
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
-    bls = load_package()
-    if p is None:
-        p = bls.scenes.hessian_problem(spec)
-    sc = bls.scenes.Scene(spec)
-    bs, el, ptr, idx = sc.description()
+    return orc
+
+
+def oracle_structure(v, cores: int):
+    orc = oracle_module()
+    ost = orc.Structure.from_description(v.bs, (v.ptr, v.idx), v.el, nchunks=cores, min_work=4096)
+    return orc, ost, orc.Pattern(ost)
+
+
+def cpu_baseline(v, seconds: float = 10.0, steps: int | None = None, warmup: int = 1):
+    """The reference algorithm (oracle) on every host core, FP64, reset + reduce of the scene in `v`; returns the
+    baseline record and the oracle's S and g_S of its last run."""
     cores = os.cpu_count() or 1
-    ost = orc.Structure.from_description(bs, (ptr, idx), el, nchunks=cores, min_work=4096)
-    opat = orc.Pattern(ost)
-    return orc, p, ost, opat, cores
-
-
-def cpu_baseline(p, spec, seconds: float = 10.0, steps: int | None = None, warmup: int = 1) -> dict:
-    """The reference algorithm (oracle) on every host core, FP64, reset + reduce of the same scene."""
-    orc, p, ost, opat, cores = oracle_problem(spec)
+    orc, ost, opat = oracle_structure(v, cores)
     w = orc.Work(ost, cores, False)
     S = np.zeros(opat.nnz)
     g = np.zeros(ost.nr)
 
     def one():
-        orc.reset_schur_sparse(ost, opat, S, p.R, p.scaling_r, p.lam)
-        ok, _ = orc.reduce_schur_sparse(ost, opat, w, S, g, p.b_r, p.b_e, p.scaling_e, p.lam, p.E, p.C, nthreads=cores)
+        orc.reset_schur_sparse(ost, opat, S, v.R, v.scaling_r, v.lam)
+        ok, _ = orc.reduce_schur_sparse(ost, opat, w, S, g, v.b_r, v.b_e, v.scaling_e, v.lam, v.E, v.C, nthreads=cores)
         assert ok
 
     for _ in range(warmup):
@@ -867,40 +989,62 @@ def cpu_baseline(p, spec, seconds: float = 10.0, steps: int | None = None, warmu
         one()
         n += 1
     dt = time.perf_counter() - t0
-    return {"value": p.nobs * n / dt, "unit": "obs/s", "cores": cores, "kind": "port",
-            "sample": f"{n} x full reset_schur_sparse + reduce_schur_sparse of {spec.npoints} points / {p.nobs} observations, FP64, "
-                      f"{cores} OpenMP threads over the reference's chunks ({dt:.1f} s)"}
+    base = {"value": v.nobs * n / dt, "unit": "obs/s", "cores": cores, "kind": "port",
+            "sample": f"{n} x full reset_schur_sparse + reduce_schur_sparse of {int(v.el.sum())} points / {v.nobs} "
+                      f"observations, FP64, {cores} OpenMP threads over the reference's chunks ({dt:.1f} s)"}
+    return base, S, g
+
+
+def reference_line(args, world: int, base: dict, config: dict, metric: str = METRIC, unit: str = "obs/s",
+                   dtype: str = "f64") -> dict:
+    return {"impl": "reference", "metric": metric, "value": base["value"], "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic (seeded scene generator)", "config": config,
+            "note": "reference algorithm restated in C++ (the oracle; Julia is unavailable); inputs read from .npy files "
+                    "written by an untimed child process",
+            "cpu_baseline": base, "e2e": {"value": base["value"], "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def run_reference(args, rank: int, world: int) -> dict | None:
     if rank != 0:
         return None
-    bls = load_package()
-    spec = bls.scenes.workload(args.workload)
-    if args.workload.startswith("dense_"):
-        p = bls.scenes.hessian_problem(spec, dense=True)
-        S, g = dense_reduced_host(spec, p)
-        base = cpu_baseline_dense(S, g, p.structure.nr, steps=args.steps)
-        return {"impl": "reference", "metric": "dense reduced solves/s (Cholesky of the dense S + one solve)", "value": base["value"],
-                "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene generator)",
-                "config": {"workload": args.workload, "n": p.structure.nr, "step": "cholesky(Symmetric(S)) \\ g via LAPACK"},
-                "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if args.workload.startswith("qr_"):
-        base = cpu_baseline_qr(spec, steps=args.steps, warmup=args.warmup)
-        return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "obs/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded scene generator)",
-                "config": {"workload": args.workload, "step": "reduce_qr + reduced_normal_sparse",
-                           "note": "reference algorithm restated in C++ (Julia is unavailable)"},
-                "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "obs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    base = cpu_baseline(None, spec, steps=args.steps, warmup=args.warmup)
-    return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "obs/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded scene generator)",
-            "config": {"workload": args.workload, "step": "reset_schur_sparse + reduce_schur_sparse",
-                       "note": "reference algorithm restated in C++ (Julia is unavailable); FP64 because its Float32 path rejects this scene"},
-            "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "obs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    import shutil
+    import tempfile
+    tmp = Path(tempfile.mkdtemp(prefix="bls_ref_"))
+    try:
+        subprocess.run([sys.executable, str(Path(__file__).resolve()), "--write-fixture", str(tmp), "--workload", args.workload],
+                       check=True)
+        meta = json.loads((tmp / "meta.json").read_text())
+        if meta["kind"] == "batch":
+            views = [_load_view(tmp / f"p{i:03d}", HESSIAN_ARRAYS) for i in range(meta["problems"])]
+            shutil.rmtree(tmp, ignore_errors=True)
+            base = cpu_baseline_batch(views, seconds=args.cpu_seconds)
+            cfg = batch_config(args.workload, world, meta["problems"], meta["cameras"], meta["points"], meta["observations"],
+                               meta["nnz_S"])
+            return reference_line(args, world, base, cfg)
+        if meta["kind"] == "qr":
+            v = _load_view(tmp, JACOBIAN_ARRAYS)
+            shutil.rmtree(tmp, ignore_errors=True)
+            base = cpu_baseline_qr(v, steps=args.steps, warmup=args.warmup)
+            cfg = qr_config(args.workload, world, meta["cameras"], meta["points"], meta["observations"], meta["table_entries"],
+                            meta["nnz_S"])
+            return reference_line(args, world, base, cfg)
+        v = _load_view(tmp, HESSIAN_ARRAYS)
+        shutil.rmtree(tmp, ignore_errors=True)
+        if meta["kind"] == "dense":
+            S, g = dense_reduced_host(v)
+            base = cpu_baseline_dense(S, g, meta["n"], steps=args.steps)
+            cfg = dense_config(args.workload, world, meta["cameras"], meta["points"], meta["n"])
+            return reference_line(args, world, base, cfg, metric="dense reduced solves/s (Cholesky of the dense S + one solve)",
+                                  unit="solves/s")
+        base, S, g = cpu_baseline(v, steps=args.steps, warmup=args.warmup)
+        cfg = hessian_config(args.workload, world, meta["cameras"], meta["points"], meta["observations"], meta["nnz_S"])
+        out = reference_line(args, world, base, cfg)
+        if args.workload.startswith("pcg_"):
+            out["pcg"] = cpu_baseline_pcg(v, S, g)
+        return out
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
 
 
 def main():
@@ -909,10 +1053,14 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sparse_1000x200k")
+    ap.add_argument("--workload", default="pcg_10000x1M")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--write-fixture", default=None, help=argparse.SUPPRESS)   # the reference arm's untimed child
     args = ap.parse_args()
+    if args.write_fixture:
+        write_fixture(args.workload, Path(args.write_fixture))
+        return
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -99,6 +99,7 @@ def gpu() -> C.CDLL:
             "bls_scatter_copy": (C.c_int, [vp, C.c_int, vp, vp, vp, i64]),
             "bls_symmetrify_full": (C.c_int, [vp, C.c_int, i64, p64, p64, p64, p64, vp, p64, i64, vp, i64]),
             "bls_reduce_schur_dense_noalloc": (C.c_int, [vp, C.c_int, i64, i64, i64, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp, vp, p64]),
+            "bls_reduce_schur_dense_noalloc_status": (C.c_int, [vp, p64]),
             "bls_qr_structure_from_description": (C.c_int, [i64, p64, i64, p64, p64, p64, C.POINTER(C.c_uint8), i64, i64, C.POINTER(vp)]),
             "bls_qr_structure_positional": (C.c_int, [vp, p64, i64, p64, p64, p64, i64, C.POINTER(vp)]),
             "bls_qr_structure_field": (i64, [vp, C.c_char_p, p64]),

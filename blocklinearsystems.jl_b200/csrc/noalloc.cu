@@ -107,7 +107,8 @@ __global__ void k_na_ginit(double* __restrict__ g, const double* __restrict__ b_
 }
 
 // One warp per point: its k(k+1)/2 pair blocks C_ci' (E^-1 C_cj), i <= j (upper triangle of the diagonal blocks), and
-// the gradient terms C_cj' z, added to S and g_S with atomics.
+// the gradient terms C_cj' z, added to S and g_S with atomics. Work indices are 64-bit (a point may couple to many
+// retained blocks), and the pair (i, j) of a work index is found in closed form from the triangular numbers.
 template <class T>
 __global__ void k_na_accumulate(int64_t neb, int64_t nr, const int64_t* __restrict__ eptr, const int64_t* __restrict__ eret,
                                 const T* __restrict__ C, T* __restrict__ S, double* __restrict__ g, double* scratch) {
@@ -115,17 +116,20 @@ __global__ void k_na_accumulate(int64_t neb, int64_t nr, const int64_t* __restri
   const int lane = threadIdx.x & 31;
   if (e >= neb || !na_live(scratch)) return;
   const int64_t p0 = eptr[e];
-  const int k = (int)(eptr[e + 1] - p0);
+  const int64_t k = eptr[e + 1] - p0;
   const double* q = scratch + 12 * e;
   double Ei[9], z[3];
   for (int i = 0; i < 9; ++i) Ei[i] = q[i];
   for (int i = 0; i < 3; ++i) z[i] = q[9 + i];
-  const int npairs = k * (k + 1) / 2;
-  for (int t = lane; t < npairs * 36; t += 32) {
-    const int pi = t / 36, ent = t - 36 * pi, rho = ent / 6, w = ent - 6 * rho;
-    int j = 0;
-    while ((j + 1) * (j + 2) / 2 <= pi) ++j;   // pair pi = (i, j) with i <= j, ordered by j then i
-    const int i = pi - j * (j + 1) / 2;
+  const int64_t npairs = k * (k + 1) / 2;
+  for (int64_t t = lane; t < npairs * 36; t += 32) {
+    const int64_t pi = t / 36;
+    const int ent = (int)(t - 36 * pi), rho = ent / 6, w = ent - 6 * rho;
+    // pair pi = (i, j) with i <= j, ordered by j then i: j is the largest with j (j + 1) / 2 <= pi
+    int64_t j = (int64_t)((sqrt(8.0 * (double)pi + 1.0) - 1.0) * 0.5);
+    while ((j + 1) * (j + 2) / 2 <= pi) ++j;
+    while (j * (j + 1) / 2 > pi) --j;
+    const int64_t i = pi - j * (j + 1) / 2;
     if (i == j && rho > w) continue;
     const T* ci = C + 18 * (p0 + i) + 3 * rho;
     const T* cj = C + 18 * (p0 + j) + 3 * w;
@@ -135,8 +139,9 @@ __global__ void k_na_accumulate(int64_t neb, int64_t nr, const int64_t* __restri
     const int64_t ri = eret[p0 + i], rj = eret[p0 + j];
     atomicAdd(S + (6 * ri + rho) + (6 * rj + w) * nr, T(-v));
   }
-  for (int t = lane; t < 6 * k; t += 32) {
-    const int j = t / 6, w = t - 6 * j;
+  for (int64_t t = lane; t < 6 * k; t += 32) {
+    const int64_t j = t / 6;
+    const int w = (int)(t - 6 * j);
     const T* cj = C + 18 * (p0 + j) + 3 * w;
     atomicAdd(g + 6 * eret[p0 + j] + w, -((double)cj[0] * z[0] + (double)cj[1] * z[1] + (double)cj[2] * z[2]));
   }
@@ -153,6 +158,22 @@ static void na_launch(cudaStream_t s, double* sc, int64_t nrb, int64_t neb, int6
   k_na_ginit<<<grid_for(nr, 256), 256, 0, s>>>(g, b_r, nr, sc);
   k_na_accumulate<T><<<grid_for(neb * 32, 256), 256, 0, s>>>(neb, nr, eptr, eret, C, S, g, sc);
   BLS_CUDA(cudaGetLastError());
+}
+
+// The verdict of the last call on this device, from the status words of the static array (copied on `s`, which
+// waits for that call's kernels when it is the call's stream). Allocates nothing.
+static int na_verdict(cudaStream_t s, double* sc, int64_t* failed_block) {
+  long long st[3];
+  BLS_CUDA(cudaMemcpyAsync(st, sc + 12 * BLS_NOALLOC_MAX_POINTS, sizeof(st), cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaStreamSynchronize(s));
+  if (failed_block) *failed_block = 0;
+  if (st[2] != NA_NONE) throw Error(BLS_EINVAL, "malformed structure: eliminated block " + std::to_string(st[2] + 1) + " has out-of-range couplings");
+  if (st[1] != NA_NONE) throw Error(BLS_EINVAL, "scaling_e must be finite and non-negative, but entry " + std::to_string(st[1] + 1) + " is not");
+  if (st[0] != NA_NONE) {
+    if (failed_block) *failed_block = st[0] + 1;
+    return BLS_NOT_PD;
+  }
+  return BLS_OK;
 }
 
 }  // namespace bls
@@ -182,17 +203,18 @@ extern "C" int bls_reduce_schur_dense_noalloc(void* cuda_stream, int dtype, int6
       na_launch<float>(s, sc, nrblocks, neblocks, ncouplings, eliminated_ptr_dev, entry_retained_dev, (float*)S_dev, g_S_dev, b_r_dev,
                        b_e_dev, scaling_e_dev, lambda, (const float*)E_dev, (const float*)C_dev);
     if (!failed_block) return BLS_OK;
-    long long st[3];
-    BLS_CUDA(cudaMemcpyAsync(st, sc + 12 * BLS_NOALLOC_MAX_POINTS, sizeof(st), cudaMemcpyDeviceToHost, s));
-    BLS_CUDA(cudaStreamSynchronize(s));
-    *failed_block = 0;
-    if (st[2] != NA_NONE) throw Error(BLS_EINVAL, "malformed structure: eliminated block " + std::to_string(st[2] + 1) + " has out-of-range couplings");
-    if (st[1] != NA_NONE) throw Error(BLS_EINVAL, "scaling_e must be finite and non-negative, but entry " + std::to_string(st[1] + 1) + " is not");
-    if (st[0] != NA_NONE) {
-      *failed_block = st[0] + 1;
-      return BLS_NOT_PD;
-    }
-    return BLS_OK;
+    return na_verdict(s, sc, failed_block);
+  } catch (const Error& e) {
+    set_error(e.what());
+    return e.code;
+  }
+}
+
+extern "C" int bls_reduce_schur_dense_noalloc_status(void* cuda_stream, int64_t* failed_block) {
+  try {
+    int dev = 0;
+    BLS_CUDA(cudaGetDevice(&dev));
+    return na_verdict(static_cast<cudaStream_t>(cuda_stream), noalloc_scratch(dev), failed_block);
   } catch (const Error& e) {
     set_error(e.what());
     return e.code;

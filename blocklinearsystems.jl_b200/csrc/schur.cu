@@ -2268,13 +2268,19 @@ void launch_symmetrify(cudaStream_t s, int dtype, const void* data, const SymBlo
   if (nblocks == 0) return;
   SymBlock* d = nullptr;
   BLS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(SymBlock) * (size_t)nblocks, s));
+  // the stream-ordered block list is released on every path, an error included (freed in stream order after the
+  // work queued before it)
+  struct FreeAsync {
+    SymBlock* p;
+    cudaStream_t s;
+    ~FreeAsync() { if (p) cudaFreeAsync(p, s); }
+  } guard{d, s};
   // from pageable host memory: the list is staged before the call returns
   BLS_CUDA(cudaMemcpyAsync(d, blocks_host, sizeof(SymBlock) * (size_t)nblocks, cudaMemcpyHostToDevice, s));
   const unsigned grid = (unsigned)std::min<int64_t>((nblocks * 32 + 255) / 256, 148 * 16);
   if (dtype == BLS_F64) k_symmetrify<double><<<grid, 256, 0, s>>>((const double*)data, d, nblocks, (double*)mat, m);
   else k_symmetrify<float><<<grid, 256, 0, s>>>((const float*)data, d, nblocks, (float*)mat, m);
   BLS_CUDA(cudaGetLastError());
-  BLS_CUDA(cudaFreeAsync(d, s));
 }
 
 }  // namespace bls

@@ -230,16 +230,25 @@ int bls_backsubstitute(bls_schur_plan* plan, int dtype, double* x_e_dev, const d
  * its scratch (each point's damped inverse and z, and a status word) in a static device array of the library, so it
  * allocates nothing. Scope: retained blocks of 6 and eliminated blocks of 3 in the canonical layout (coupling c at
  * C_data[18c], point e at E_data[9e]), dense column-major S (nr = 6 nrblocks) already holding the reset system, at most
- * BLS_NOALLOC_MAX_POINTS eliminated blocks (larger sizes: BLS_EUNSUPPORTED, nothing launched). Results and failure
- * reporting are those of bls_reduce_schur_dense. The array is shared by all calls on a device and keeps the last
- * call's contents; calls whose work overlaps on the GPU race on it. The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) and caches it: make that first call before any stream capture. */
+ * BLS_NOALLOC_MAX_POINTS eliminated blocks (larger sizes: BLS_EUNSUPPORTED, nothing launched). Results are those of
+ * bls_reduce_schur_dense. With a host `failed_block` the call synchronises on `cuda_stream` and returns the verdict:
+ * BLS_NOT_PD with the lowest failing block (1-based), or BLS_EINVAL for a bad scaling_e entry or a malformed
+ * structure (an eliminated_ptr or entry_retained index out of range, or entry_retained not ascending within a point),
+ * in which case S and g_S are left untouched. With failed_block NULL the call only queues its kernels; the verdict
+ * stays in the array's status words until the next call on the device and is read with
+ * bls_reduce_schur_dense_noalloc_status. The array is shared by all calls on a device and keeps the last call's
+ * contents; calls whose work overlaps on the GPU race on it. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and caches it: make that first call before any stream capture. */
 #define BLS_NOALLOC_MAX_POINTS 65536
 int bls_reduce_schur_dense_noalloc(void* cuda_stream, int dtype, int64_t nrblocks, int64_t neblocks, int64_t ncouplings,
                                    const int64_t* eliminated_ptr_dev, const int64_t* entry_retained_dev, void* S_dev,
                                    double* g_S_dev, const double* b_r_dev, const double* b_e_dev,
                                    const double* scaling_e_dev, double lambda, const void* E_dev, const void* C_dev,
                                    int64_t* failed_block);
+/* No counterpart in the reference: the verdict of the last bls_reduce_schur_dense_noalloc call on the current device
+ * (the same codes and failed_block as its synchronous form), read from the static array's status words after the work
+ * queued on `cuda_stream`. Synchronises on `cuda_stream`; allocates nothing. */
+int bls_reduce_schur_dense_noalloc_status(void* cuda_stream, int64_t* failed_block);
 
 /* ---------------------------------------------------------------------------------------------------------------
  * QR elimination (src/schur_jacobian.jl, src/qr_reduction.jl, src/qr_reduced.jl). The Jacobian is stored as one table

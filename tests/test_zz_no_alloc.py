@@ -91,3 +91,86 @@ def test_noalloc_reports_failure_and_refuses_oversize(bls, problem):
     rc = L.bls_reduce_schur_dense_noalloc(stream, bls._lib.BLS_F64, st.nrblocks, 65537, len(st.entry_retained), *ptrs(*args, S, g, b_r, b_e, se),
                                           0.0, *ptrs(Et, Ct), C.byref(fb))
     assert rc == bls._lib.BLS_EUNSUPPORTED and b"65536" in L.bls_last_error()
+
+
+def _noalloc_args(bls, p, E=None, scaling_e=None, eret=None):
+    st = p.structure
+    nr = st.nr
+    t = lambda a, d=torch.float64: torch.from_numpy(np.ascontiguousarray(a)).to(device=DEV, dtype=d)
+    bufs = dict(eptr=t(st.eliminated_ptr, torch.int64), eret=t(st.entry_retained if eret is None else eret, torch.int64),
+                S=torch.full((nr * nr,), 3.0, dtype=torch.float64, device=DEV), g=torch.full((nr,), 5.0, dtype=torch.float64, device=DEV),
+                b_r=t(p.b_r), b_e=t(p.b_e), se=t(p.scaling_e if scaling_e is None else scaling_e), E=t(p.E if E is None else E),
+                C=t(p.C))
+    return bufs
+
+
+def _call(bls, p, b, failed_block):
+    st = p.structure
+    L = bls._lib.gpu()
+    v = lambda x: C.c_void_p(x.data_ptr())
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return L.bls_reduce_schur_dense_noalloc(stream, bls._lib.BLS_F64, st.nrblocks, st.neblocks, len(st.entry_retained), v(b["eptr"]),
+                                           v(b["eret"]), v(b["S"]), v(b["g"]), v(b["b_r"]), v(b["b_e"]), v(b["se"]), p.lam, v(b["E"]),
+                                           v(b["C"]), failed_block)
+
+
+def test_noalloc_async_verdict_is_queried(bls, problem):
+    """With failed_block NULL the call queues its work and keeps its verdict in the static array's status words;
+    bls_reduce_schur_dense_noalloc_status reads it (the lowest failing block, 1-based), and a clean call reads OK."""
+    p = problem
+    L = bls._lib.gpu()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    E = p.E.copy()
+    v = np.array([1.0, 2.0, 3.0])
+    for e in (7, 11):
+        E[9 * e:9 * e + 9] = np.outer(v, v).ravel(order="F")
+    b = _noalloc_args(bls, p, E=E, scaling_e=np.zeros_like(p.scaling_e))
+    assert _call(bls, p, b, None) == 0
+    fb = C.c_int64(-1)
+    assert L.bls_reduce_schur_dense_noalloc_status(stream, C.byref(fb)) == bls._lib.BLS_NOT_PD and fb.value == 8
+    assert torch.all(b["S"] == 3.0) and torch.all(b["g"] == 5.0)
+    b = _noalloc_args(bls, p)
+    assert _call(bls, p, b, None) == 0
+    fb = C.c_int64(-1)
+    assert L.bls_reduce_schur_dense_noalloc_status(stream, C.byref(fb)) == 0 and fb.value == 0
+    assert not torch.all(b["S"] == 3.0)
+
+
+@pytest.mark.parametrize("case", ["descending", "out_of_range", "negative_scaling", "nan_scaling"])
+def test_noalloc_rejects_bad_arguments_untouched(bls, problem, case):
+    """A malformed structure (entry_retained not ascending within a point, or beyond nrblocks) and a negative or NaN
+    scaling_e entry are BLS_EINVAL, found by the call's own checks before its atomics touch S or g_S: both stay as
+    they were, synchronously and through the status query."""
+    p = problem
+    st = p.structure
+    L = bls._lib.gpu()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    eret, se = None, None
+    e = 3
+    a, z = int(st.eliminated_ptr[e]), int(st.eliminated_ptr[e + 1])
+    assert z - a >= 2
+    if case == "descending":
+        eret = st.entry_retained.copy()
+        eret[a], eret[a + 1] = eret[a + 1], eret[a]
+    elif case == "out_of_range":
+        eret = st.entry_retained.copy()
+        eret[z - 1] = st.nrblocks
+    elif case == "negative_scaling":
+        se = p.scaling_e.copy()
+        se[10] = -1.0
+    else:
+        se = p.scaling_e.copy()
+        se[10] = np.nan
+    for sync in (True, False):
+        b = _noalloc_args(bls, p, scaling_e=se, eret=eret)
+        fb = C.c_int64(-1)
+        if sync:
+            rc = _call(bls, p, b, C.byref(fb))
+        else:
+            assert _call(bls, p, b, None) == 0
+            rc = L.bls_reduce_schur_dense_noalloc_status(stream, C.byref(fb))
+        assert rc == bls._lib.BLS_EINVAL, (case, sync, rc)
+        msg = L.bls_last_error()
+        assert (b"scaling_e" in msg) if "scaling" in case else (b"malformed structure" in msg and b"block 4 " in msg), msg
+        torch.cuda.synchronize()
+        assert torch.all(b["S"] == 3.0) and torch.all(b["g"] == 5.0), (case, sync)
