@@ -94,6 +94,9 @@ def gpu() -> C.CDLL:
             "bls_schur_query_status": (C.c_int, [vp, p64]),
             "bls_schur_plan_instrument": (C.c_int, [vp, C.c_int]),
             "bls_schur_plan_set_kernel": (C.c_int, [vp, C.c_int]),
+            "bls_schur_plan_phase2_kernel": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_char_p, i64]),
+            "bls_schur_plan_set_problems": (C.c_int, [vp, i64, p64, p64, p64, p64]),
+            "bls_schur_plan_problem_status": (C.c_int, [vp, p64]),
             "bls_schur_plan_counters": (C.c_int, [vp, p64, pdbl, p64]),
             "bls_backsubstitute": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
             "bls_scatter_copy": (C.c_int, [vp, C.c_int, vp, vp, vp, i64]),
@@ -107,6 +110,7 @@ def gpu() -> C.CDLL:
             "bls_qr_structure_destroy": (C.c_int, [vp]),
             "bls_qr_plan_create": (C.c_int, [vp, C.POINTER(bls_qr_plan_desc), C.POINTER(vp)]),
             "bls_qr_plan_destroy": (C.c_int, [vp]),
+            "bls_qr_plan_set_staging": (C.c_int, [vp, C.c_int]),
             "bls_reduce_qr": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, p64]),
             "bls_qr_backsubstitute": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_qr_query_status": (C.c_int, [vp, p64]),

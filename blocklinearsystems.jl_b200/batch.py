@@ -6,9 +6,10 @@ indices, coupling and point-block offsets, S positions, the r -> s map), so one 
 every problem: the union's S is block diagonal by problem, and each kernel launch spans the whole batch. Each
 problem's damping lambda_p is folded into its scalings (lambda_p * scaling, formed in FP64 exactly as the kernels form
 lambda * scaling; the batch runs with lambda = 1), so every problem's result is the one its own call would give.
-autotune() times the phase-2 schedules (block-owned pair work lists with six lanes or one lane per pair, block-column
-owned tiles with a warp per visit or with visits staged in chunks) on the batch and keeps the fastest; capture()
-records reset + reduce of the batch as one CUDA graph that step() replays.
+Each problem fails on its own (problem_status): a singular point in problem p leaves p's S reset and its g_S as it was,
+and the other problems are reduced, as separate reference calls would. autotune() times the phase-2 schedules that
+keep that (the block-column owned schedule with staged point operands, the block-owned pair lists) and keeps the
+faster; capture() records reset + reduce of the batch as one CUDA graph that step() replays.
 """
 from __future__ import annotations
 
@@ -103,6 +104,11 @@ class BatchedReduction:
         self.U, self.off = union_layout(problems)
         U = self.U
         self.ws = SchurReductionWorkspace(U, U, U.r_to_s_map, device=device)
+        # each problem fails on its own, as its own reduce_schur_sparse! call would
+        from . import _lib
+        from ._lib import check, ptr64
+        offs = [np.ascontiguousarray(self.off[k], np.int64) for k in ("eb", "rb", "nr", "nnz")]
+        check(_lib.gpu().bls_schur_plan_set_problems(self.ws._h, len(problems), *[ptr64(a) for a in offs]))
         dev = torch.device("cuda", device)
         f = lambda xs, t=dtype: torch.from_numpy(np.ascontiguousarray(np.concatenate(xs))).to(device=dev, dtype=t)
         self.E = f([p.E for p in problems])
@@ -125,9 +131,10 @@ class BatchedReduction:
                                    self.ws, sync=sync)
 
     def autotune(self, reps: int = 5) -> dict:
-        """Time each phase-2 schedule on the batch (after a warm-up run) and keep the faster."""
+        """Time the phase-2 schedules that keep per-problem failure (block-column owned with staged point operands,
+        block-owned pair lists) on the batch, after a warm-up run, and keep the faster."""
         times = {}
-        for name in ("pairs", "columns", "lanes", "tiles", "points"):
+        for name in ("stage", "pairs"):
             self.ws.set_kernel(name)
             self.run()
             torch.cuda.synchronize()
@@ -170,9 +177,22 @@ class BatchedReduction:
         return reset_reduce_schur_sparse_host(S_h, g_h, host["R"], host["sc_r"], 1.0, host["b_r"], host["b_e"], host["sc_e"], self.U,
                                               host["E"], host["C"], self.ws)
 
+    def problem_status(self) -> np.ndarray:
+        """Per problem of the last batch reduction (synchronises): 0, or the problem's lowest failing eliminated block
+        (1-based, local to the problem), as that problem's own reduce_schur_sparse! call reports it. A failing problem
+        keeps its reset S and its g_S; the other problems are reduced."""
+        from . import _lib
+        from ._lib import ptr64
+        out = np.zeros(len(self.problems), np.int64)
+        rc = _lib.gpu().bls_schur_plan_problem_status(self.ws._h, ptr64(out))
+        if rc < 0:
+            _lib.check(rc)
+        return out
+
     def ok(self) -> bool:
-        """Verdict of the last batch reduction (synchronises): False if any problem's eliminated block failed."""
-        return self.ws.query_status()
+        """Verdict of the last batch reduction (synchronises): True when the arguments were valid and no problem's
+        eliminated block failed (see problem_status for the problems that did)."""
+        return self.ws.query_status() and not self.problem_status().any()
 
     def problem_S(self, i: int) -> torch.Tensor:
         return self.S[int(self.off["nnz"][i]):int(self.off["nnz"][i + 1])]

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <type_traits>
 
+#include "bulk.cuh"
 #include "common.cuh"
 
 namespace bls {
@@ -39,6 +40,7 @@ struct QRPlan {
   int64_t max_rows = 0, nblocks = 0, nnzS = 0, ndiag = 0;
   bool has_sparse = false;
   bool all6 = true;   // every retained block has 6 columns (the Gram kernel's 6 x 6 form only)
+  bool bulk = true;   // stage tables with bulk copies (false: element copies; bls_qr_plan_set_staging)
   int max_dr = 0;
   // device: per table, per entry, per retained / eliminated block
   DevBuf t_rows, t_cols, t_top, t_raw, t_res, t_ptr, e_dims, boff_e;
@@ -112,7 +114,7 @@ __device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // status: [0] lowest failing table, [1] lowest bad scaling_e entry
-__global__ void k_qr_begin(long long* st) { st[0] = QNONE; st[1] = QNONE; }
+__global__ void k_qr_begin(long long* st) { st[0] = QNONE; st[1] = QNONE; st[2] = QNONE; }
 __global__ void k_qr_check(const double* __restrict__ sc, int64_t n, long long* st) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -153,6 +155,7 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
                                                   const int32_t* __restrict__ e_dims, const int32_t* __restrict__ boff_e, int nr,
                                                   const T* __restrict__ Rw, const double* __restrict__ Rr, const double* __restrict__ sc_e,
                                                   double lambda, const double* __restrict__ s, T* __restrict__ F, double* __restrict__ Fr,
+                                                  const T* __restrict__ Rw_end, const double* __restrict__ Rr_end, int bulk,
                                                   long long* st) {
   extern __shared__ __align__(16) unsigned char qsm_all[];
   const int64_t wi = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -163,14 +166,42 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
   const int t = tables[wi];
   const int M = t_rows[t], C = t_cols[t] - 1, de = e_dims[t], me = M - de, ce = C - de;
   const int64_t off = t_raw[t], rq = t_res[t];
-  double* res = reinterpret_cast<double*>(qsm);
-  T* A = reinterpret_cast<T*>(qsm + sizeof(double) * ((M + 1) & ~1));
-  // copy in (coalesced: the table is contiguous; all of a lane's copies in flight at once), then the reference's
-  // non-finite test (x - x is NaN for Inf / NaN) and the conditioning scales, in shared memory
-  for (int i = lane; i < M * C; i += 32) cp_async_elem(A + i, Rw + off + i);
-  for (int i = lane; i < M; i += 32) cp_async_elem(res + i, Rr + rq + i);
-  cp_async_wait_all();
-  __syncwarp();
+  // the warp's region: its mbarrier, then the FP64 residual and the M x C table, each with 32 bytes of room for the
+  // 16-byte alignment of a bulk copy
+  uint64_t* bar = reinterpret_cast<uint64_t*>(qsm);
+  unsigned char* rbase = qsm + 16;
+  unsigned char* abase = rbase + ((8 * M + 32 + 15) & ~15);
+  double* res;
+  T* A;
+  if (bulk) {
+    // the table and its residual are contiguous: one bulk copy each (TMA), completed on the warp's mbarrier
+    const Span sa = span_of(Rw + off, (int64_t)M * C, Rw_end), sr = span_of(Rr + rq, (int64_t)M, Rr_end);
+    if (lane == 0) {
+      mbar_init(bar, 1);
+      mbar_fence_init();
+      mbar_arrive_expect_tx(bar, span_bytes(sa) + span_bytes(sr));
+      span_issue(reinterpret_cast<T*>(abase), sa, bar);
+      span_issue(reinterpret_cast<double*>(rbase), sr, bar);
+    }
+    A = span_first(reinterpret_cast<T*>(abase), sa);
+    res = span_first(reinterpret_cast<double*>(rbase), sr);
+    __syncwarp();
+    if (!mbar_wait(bar, 0)) {
+      if (lane == 0) atomicExch(reinterpret_cast<unsigned long long*>(st + 2), 1ull);   // a copy that did not land: fault
+      mbar_wait(bar, 0);                                                               // drain (bounded), then leave
+      return;
+    }
+    __syncwarp();
+  } else {
+    res = reinterpret_cast<double*>(rbase);
+    A = reinterpret_cast<T*>(abase);
+    // element copies (coalesced: the table is contiguous; all of a lane's copies in flight at once)
+    for (int i = lane; i < M * C; i += 32) cp_async_elem(A + i, Rw + off + i);
+    for (int i = lane; i < M; i += 32) cp_async_elem(res + i, Rr + rq + i);
+    cp_async_wait_all();
+    __syncwarp();
+  }
+  // the reference's non-finite test (x - x is NaN for Inf / NaN) and the conditioning scales, in shared memory
   bool bad = false;
   for (int i = lane; i < M * C; i += 32) {
     T x = A[i];
@@ -292,28 +323,62 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_gram(int64_t ntab, int
                                                               const int32_t* __restrict__ tp_ptr, const int32_t* __restrict__ tp_blk,
                                                               const int64_t* __restrict__ blk_base, const int32_t* __restrict__ blk_stride,
                                                               int64_t dense_nr, const int64_t* __restrict__ doff, int dmax, const T* __restrict__ F,
-                                                              const double* __restrict__ Fr, T* __restrict__ S, double* __restrict__ g, int from_raw) {
+                                                              const double* __restrict__ Fr, T* __restrict__ S, double* __restrict__ g, int from_raw,
+                                                              const T* __restrict__ F_end, const double* __restrict__ Fr_end, int bulk,
+                                                              long long* st) {
   extern __shared__ __align__(16) unsigned char gsm_all[];
   const int64_t wi = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
   if (wi >= ntab) return;
   const int lane = threadIdx.x & 31;
   unsigned char* gsm = gsm_all + (size_t)(threadIdx.x >> 5) * warp_bytes;
   const int t = tables[wi];
-  const int M = t_rows[t], top = t_top[t], n = M - top, ce = t_cols[t] - 1 - top, ns = n | 1;
+  const int M = t_rows[t], top = t_top[t], n = M - top, ce = t_cols[t] - 1 - top;
   const int u0 = t_ptr[t], kt = t_ptr[t + 1] - u0;
-  double* rr = reinterpret_cast<double*>(gsm);
-  T* B = reinterpret_cast<T*>(gsm + sizeof(double) * ((n + 1) & ~1));
+  // the warp's region: its mbarrier, the residual rows (FP64), then the retained columns
+  uint64_t* bar = reinterpret_cast<uint64_t*>(gsm);
+  unsigned char* rbase = gsm + 16;
+  unsigned char* bbase = rbase + ((8 * n + 32 + 15) & ~15);
+  double* rr;
+  T* B;
+  int ns;   // column stride of B in shared memory
   // rows [row0, row0 + n): the bottom rows J~ of a factored table, or the data rows of a raw one (its damping rows last)
   const int row0 = from_raw ? 0 : top;
   const T* src = F + t_raw[t] + row0;
-  for (int q = lane; q < ce * n; q += 32) {
-    const int j = q / n, i = q - j * n;
-    cp_async_elem(B + j * ns + i, src + (int64_t)j * M + i);
+  if (bulk && ce > 0) {
+    // rows row0.. of columns 0..ce-1 lie in one contiguous span of (ce - 1) M + n entries: one bulk copy (TMA), the
+    // columns then at stride M (the rows above row0 of columns 1.. come along and are not read)
+    ns = M;
+    const Span sb = span_of(src, (int64_t)(ce - 1) * M + n, F_end);
+    const Span sr = span_of(Fr + t_res[t] + row0, (int64_t)n, Fr_end);
+    if (lane == 0) {
+      mbar_init(bar, 1);
+      mbar_fence_init();
+      mbar_arrive_expect_tx(bar, span_bytes(sb) + (MODE == 0 ? span_bytes(sr) : 0u));
+      span_issue(reinterpret_cast<T*>(bbase), sb, bar);
+      if (MODE == 0) span_issue(reinterpret_cast<double*>(rbase), sr, bar);
+    }
+    B = span_first(reinterpret_cast<T*>(bbase), sb);
+    rr = span_first(reinterpret_cast<double*>(rbase), sr);
+    __syncwarp();
+    if (!mbar_wait(bar, 0)) {
+      if (lane == 0) atomicExch(reinterpret_cast<unsigned long long*>(st + 2), 1ull);   // a copy that did not land: fault
+      mbar_wait(bar, 0);
+      return;
+    }
+    __syncwarp();
+  } else {
+    ns = n | 1;
+    rr = reinterpret_cast<double*>(rbase);
+    B = reinterpret_cast<T*>(bbase);
+    for (int q = lane; q < ce * n; q += 32) {
+      const int j = q / n, i = q - j * n;
+      cp_async_elem(B + j * ns + i, src + (int64_t)j * M + i);
+    }
+    if (MODE == 0)
+      for (int i = lane; i < n; i += 32) cp_async_elem(rr + i, Fr + t_res[t] + row0 + i);
+    cp_async_wait_all();
+    __syncwarp();
   }
-  if (MODE == 0)
-    for (int i = lane; i < n; i += 32) cp_async_elem(rr + i, Fr + t_res[t] + row0 + i);
-  cp_async_wait_all();
-  __syncwarp();
   if (MODE == 0) {
     // J~'r~: lane per column, entry found by scanning the table's entries
     for (int j = lane; j < ce; j += 32) {
@@ -875,15 +940,21 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
   for (int64_t t = 0; t < nt; ++t) {
     const int64_t M = d->table_nrows[t], C = d->table_ncols[t] - 1, top = d->table_top[t];
     if (t < neb) {
-      const int64_t b64 = 8 * ((M + 1) & ~1) + 8 * M * C, b32 = 8 * ((M + 1) & ~1) + 4 * M * C;
+      // the warp's mbarrier, the residual and the table, each with room for a bulk copy's 16-byte alignment
+      const int64_t rb = (8 * M + 32 + 15) & ~int64_t(15);
+      const int64_t b64 = 16 + rb + 8 * M * C + 32, b32 = 16 + rb + 4 * M * C + 32;
       if (b64 > QR_SMEM_LIMIT) throw Error(BLS_EUNSUPPORTED, "table " + std::to_string(t + 1) + " exceeds the shared-memory capacity of this build");
       const int c = cls_of(b64);
       cls_tables[c].push_back((int32_t)t);
       P->classes[c].bytes_f64 = std::max(P->classes[c].bytes_f64, b64);
       P->classes[c].bytes_f32 = std::max(P->classes[c].bytes_f32, b32);
     }
+    // the warp's mbarrier, the residual rows and the retained columns: at stride M from one bulk copy (plus 32 bytes
+    // of alignment room), or at the odd stride n | 1 from element copies; the larger of the two
     const int64_t n = M - top, ce = C - top, ns = n | 1;
-    const int64_t g64 = 8 * ((n + 1) & ~1) + 8 * ce * ns, g32 = 8 * ((n + 1) & ~1) + 4 * ce * ns;
+    const int64_t cells = std::max<int64_t>(ce > 0 ? (ce - 1) * M + n : 0, ce * ns) + 8;
+    const int64_t rb = (8 * n + 32 + 15) & ~int64_t(15);
+    const int64_t g64 = 16 + rb + 8 * cells, g32 = 16 + rb + 4 * cells;
     if (g64 > QR_SMEM_LIMIT) throw Error(BLS_EUNSUPPORTED, "table " + std::to_string(t + 1) + " exceeds the shared-memory capacity of this build");
     const int c = cls_of(g64);
     gram_tables[c].push_back((int32_t)t);
@@ -1056,9 +1127,10 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
 // The verdict of the last reduce_qr (synchronises on the plan's stream)
 static int qr_status(QRPlan* P, int64_t* failed_block) {
   cudaStream_t s = P->ctx->stream;
-  BLS_CUDA(cudaMemcpyAsync(P->host_status, P->status.p, 2 * sizeof(long long), cudaMemcpyDeviceToHost, s));
+  BLS_CUDA(cudaMemcpyAsync(P->host_status, P->status.p, 3 * sizeof(long long), cudaMemcpyDeviceToHost, s));
   BLS_CUDA(cudaStreamSynchronize(s));
   *failed_block = 0;
+  if (P->host_status[2] != QNONE) throw Error(BLS_ECUDA, "a bulk copy of a table did not complete within its wait limit");
   if (P->host_status[1] != QNONE) {
     set_error("scaling_e must be finite and non-negative, but entry " + std::to_string(P->host_status[1] + 1) + " is not");
     return BLS_EINVAL;
@@ -1079,6 +1151,9 @@ static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr,
   k_qr_begin<<<1, 1, 0, s>>>(st);
   k_qr_check<<<grid_for(P->ne, 256), 256, 0, s>>>(sc_e, P->ne, st);
   P->launches += 2;
+  // bulk copies need the buffers' starts on 16-byte boundaries (the device allocators give 256); otherwise the tables
+  // are staged element by element
+  const bool bulk = P->bulk && (reinterpret_cast<uintptr_t>(Rw) & 15) == 0 && (reinterpret_cast<uintptr_t>(Rr) & 15) == 0;
   for (int c = 0; c < 8; ++c) {
     const auto& k = P->classes[c];
     if (k.n == 0) continue;
@@ -1089,7 +1164,8 @@ static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr,
     k_qr_tables<T><<<(unsigned)((k.n + wpc - 1) / wpc), 32 * wpc, smem, s>>>(
         k.n, (int)wb, k.tables.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(),
         P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->boff_r.as<int32_t>(), P->r_dims.as<int32_t>(),
-        P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), (int)P->nr, Rw, Rr, sc_e, lambda, sv, F, Fr, st);
+        P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), (int)P->nr, Rw, Rr, sc_e, lambda, sv, F, Fr, Rw + P->raw_len, Rr + P->res_len,
+        bulk ? 1 : 0, st);
     P->launches += 1;
   }
   if (P->ntables > P->neblocks) {
@@ -1109,6 +1185,7 @@ static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr,
 template <class T, int MODE>
 static void gram(QRPlan* P, T* S, bool dense, double* g, const T* F, const double* Fr, bool from_raw = false) {
   cudaStream_t s = P->ctx->stream;
+  const bool bulk = P->bulk && (reinterpret_cast<uintptr_t>(F) & 15) == 0 && (reinterpret_cast<uintptr_t>(Fr) & 15) == 0;
   for (int c = 0; c < 8; ++c) {
     const auto& k = P->gram_classes[c];
     if (k.n == 0) continue;
@@ -1122,7 +1199,8 @@ static void gram(QRPlan* P, T* S, bool dense, double* g, const T* F, const doubl
         P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(),
         P->boff_r.as<int32_t>(), P->tp_ptr.as<int32_t>(), P->tp_blk.as<int32_t>(),
         dense ? P->blk_base_dense.as<int64_t>() : P->blk_base_sparse.as<int64_t>(), dense ? nullptr : P->blk_stride.as<int32_t>(), P->nr,
-        P->doff.as<int64_t>(), P->max_dr, F, Fr, S, g, from_raw ? 1 : 0);
+        P->doff.as<int64_t>(), P->max_dr, F, Fr, S, g, from_raw ? 1 : 0, F + P->raw_len, Fr + P->res_len, bulk ? 1 : 0,
+        P->status.as<long long>());
     P->launches += 1;
   }
   BLS_CUDA(cudaGetLastError());
@@ -1651,6 +1729,12 @@ int bls_qr_plan_destroy(bls_qr_plan* plan) {
     cudaStreamSynchronize(plan->ctx->stream);
     delete static_cast<QRPlan*>(plan);
   }
+  return BLS_OK;
+}
+
+int bls_qr_plan_set_staging(bls_qr_plan* plan, int bulk) {
+  if (!plan) return BLS_EINVAL;
+  static_cast<QRPlan*>(plan)->bulk = bulk != 0;
   return BLS_OK;
 }
 

@@ -22,6 +22,7 @@
 // where it is used, so nothing the size of C_data is written. W' C and C' (E^-1 C) are the same product (E^-1 is
 // symmetric); the order of the additions differs, which the tests bound by tolerance.
 #include <algorithm>
+#include <cstdio>
 #include <climits>
 #include <cstring>
 #include <memory>
@@ -64,6 +65,22 @@ struct SchurPlan {
   bool tiles_ok = false;   // every point's coupling span fits the staging buffer of k_tiles36
   DevBuf pt_rec;   // fast36, point-major pairs: {c1, k | (c2 - c1) << 25} per pair, k the S block
   bool points_ok = false;
+  // fast36, sparse: the column-owned schedule (k_stage36). Work items are runs of a block column's visits (most
+  // columns are one item); per item {r2, first visit, visit count, items of its column}. Each item's pairs are cut into
+  // units (one S block, at most stage_unit pairs, in visit order) spread over the CTA's threads; per item and thread
+  // the first of its units (stg_thr, STAGE_NT + 1 per item). Units {first pair, pair count, the block's row offset in
+  // the column, r1 | diagonal << 31}; pairs {visit within the item | c1's index within its point << 16}.
+  static constexpr int STAGE_NT = 256;
+  bool stage_ok = false;
+  int stage_unit = 8;
+  int64_t stage_items = 0, stage_max_nv = 0, stage_units = 0;
+  DevBuf stg_items, stg_thr, stg_units, stg_pairs;
+  DevBuf EZ;   // per point E' = s_e E^-1 s_e (9, column-major) and z' = s_e .* z (3), FP64, for k_stage36
+  // a batch of independent problems in one plan (bls_schur_plan_set_problems): per problem the lowest failing point
+  // (global index, NONE if none), per point and per camera its problem; a failing problem skips its own phase 2 only
+  int64_t nprob = 0;
+  std::vector<int64_t> prob_point_off, prob_row_off, prob_nnz_off;
+  DevBuf prob_fail, prob_of_point, prob_of_cam;
   int kernel = 1;   // 0: column-owned (k_columns36), 1: block-owned pairs (k_pairs36, the default: faster on sparse scenes)
   // reset
   DevBuf r_to_s, diag_inds, S_rowval, S_col;
@@ -306,12 +323,14 @@ template <class T>
 __global__ void __launch_bounds__(128) k_factor36(int64_t e_begin, int64_t neb, const T* __restrict__ E, const double* __restrict__ b_e,
                                                   const double* __restrict__ scaling_e, double lambda, const double* __restrict__ s_e,
                                                   double* __restrict__ Einv64, typename EinvOf<T>::type* __restrict__ Einv12,
-                                                  double* __restrict__ z, Status* st) {
+                                                  double* __restrict__ z, double* __restrict__ EZ, const int32_t* __restrict__ prob_of_point,
+                                                  long long* __restrict__ prob_fail, Status* st) {
   using TE = typename EinvOf<T>::type;
   constexpr int NB = 128;
   __shared__ double sE[NB * 9];      // E in, then E^-1 out
   __shared__ TE s12[NB * 12];
   __shared__ double sb[NB * 3], ss[NB * 3], sse[NB * 3];
+  __shared__ double sez[NB * 12];    // k_stage36's record: E' = s_e E^-1 s_e and z' = s_e .* z
   if (st->einval_r != NONE) return;   // the reset's arguments were bad; scaling_e is checked here (k_arm36 cleared its slot)
   const int64_t e0 = e_begin + (int64_t)blockIdx.x * NB;   // points [e_begin, neb)
   const int n = (int)(neb - e0 < NB ? neb - e0 : NB);
@@ -337,7 +356,8 @@ __global__ void __launch_bounds__(128) k_factor36(int64_t e_begin, int64_t neb, 
         H[i + 3 * j] = s_e ? mul(h, mul(se[i], se[j])) : h;
       }
     if (!inv_sym_closed(3, H, damp, inv)) {
-      atomicMin(&st->failed, (long long)(e0 + t));
+      if (prob_fail) atomicMin(prob_fail + prob_of_point[e0 + t], (long long)(e0 + t));   // this problem's lowest failing point
+      else atomicMin(&st->failed, (long long)(e0 + t));
       for (int i = 0; i < 9; ++i) inv[i] = 0.0;
     }
     for (int i = 0; i < 9; ++i) {
@@ -349,11 +369,17 @@ __global__ void __launch_bounds__(128) k_factor36(int64_t e_begin, int64_t neb, 
       double acc = inv[i] * (sb[3 * t] * se[0]);
       for (int j = 1; j < 3; ++j) acc = acc + inv[i + 3 * j] * (sb[3 * t + j] * se[j]);
       ss[3 * t + i] = acc;     // z, in the slot of scaling_e (read above by this thread only)
+      sez[12 * t + 9 + i] = se[i] * acc;
     }
+    for (int j = 0; j < 3; ++j)
+      for (int i = 0; i < 3; ++i) sez[12 * t + i + 3 * j] = se[i] * inv[i + 3 * j] * se[j];
   }
   __syncthreads();
   for (int i = t; i < 9 * n; i += NB) Einv64[9 * e0 + i] = sE[i];
-  for (int i = t; i < 12 * n; i += NB) Einv12[12 * e0 + i] = s12[i];
+  if (Einv12)
+    for (int i = t; i < 12 * n; i += NB) Einv12[12 * e0 + i] = s12[i];
+  if (EZ)
+    for (int i = t; i < 12 * n; i += NB) EZ[12 * e0 + i] = sez[i];
   for (int i = t; i < 3 * n; i += NB) z[3 * e0 + i] = ss[i];
 }
 
@@ -558,10 +584,16 @@ __global__ void __launch_bounds__(256) k_gradient(int64_t nrb, const int32_t* __
 
 // g_S = s_r .* b_r (scaled_copy!, src/conditioning.jl:237-244), before the pair kernel subtracts C' z
 __global__ void k_g_init(double* __restrict__ g, const double* __restrict__ b_r, const double* __restrict__ s_r, int64_t nr,
-                         const Status* __restrict__ st) {
+                         const Status* __restrict__ st, const int32_t* __restrict__ prob_of_cam = nullptr,
+                         const long long* __restrict__ prob_fail = nullptr) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= nr || !live(st)) return;
+  if (prob_fail && prob_fail[prob_of_cam[i / 6]] != NONE) return;   // a failing problem keeps its g_S
   g[i] = s_r ? b_r[i] * s_r[i] : b_r[i];
+}
+__global__ void k_prob_arm(long long* __restrict__ prob_fail, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) prob_fail[i] = NONE;
 }
 
 // Column w of a 3 x 6 coupling block in the canonical layout: three entries starting at 18 c + 3 w, which is even
@@ -746,7 +778,8 @@ __global__ void __launch_bounds__(128) k_pairs36(
     const int2* __restrict__ pairs, const int32_t* __restrict__ block_r1, const int32_t* __restrict__ block_r2,
     const int64_t* __restrict__ block_base, const int32_t* __restrict__ block_stride, int64_t dense_nr, const T* __restrict__ C,
     const typename EinvOf<T>::type* __restrict__ Einv12, const double* __restrict__ z, const double* __restrict__ s_r,
-    const double* __restrict__ s_e, T* __restrict__ S, double* __restrict__ g, const Status* __restrict__ st) {
+    const double* __restrict__ s_e, T* __restrict__ S, double* __restrict__ g, const Status* __restrict__ st,
+    const int32_t* __restrict__ prob_of_cam = nullptr, const long long* __restrict__ prob_fail = nullptr) {
   using TE = typename EinvOf<T>::type;
   const int lane = threadIdx.x & 31;
   if (lane >= 30) return;
@@ -758,6 +791,7 @@ __global__ void __launch_bounds__(128) k_pairs36(
   const int pe = pb + (info & 0xffff);
   const bool solo = (info >> 16) != 0;
   const int r1 = __ldg(block_r1 + k), r2 = __ldg(block_r2 + k);
+  if (prob_fail && prob_fail[prob_of_cam[r2]] != NONE) return;   // the block's problem failed: its S stays reset
   const bool diag = r1 == r2;
   const bool scaled = s_r != nullptr || s_e != nullptr;
   const double fw = s_r ? s_r[6 * r2 + w] : 1.0;
@@ -1394,6 +1428,332 @@ __global__ void k_gather(T* __restrict__ dest, const T* __restrict__ src, const 
 // ------------------------------------------------------------------------------------------------------------------
 // Plan construction (host, once per structure)
 // ------------------------------------------------------------------------------------------------------------------
+// Phase 2 for d_r = 6, d_e = 3 and a sparse S, column-owned (the "stage" schedule): one CTA per work item, a run of
+// the visits of block column r2 (the points that observe camera r2, in the reference's retained_entry order).
+// 1. Each visit's point-side operand W = E' C_c2 (3 x 6, E' = s_e E^-1 s_e from the factor kernel, formed in FP64 and
+//    rounded to the storage type) goes to shared memory, with the visit point's first coupling index; the same pass
+//    adds C_c2' z' (z' = s_e .* z, FP64) to the column's gradient sums.
+// 2. Each thread runs its units: one S block (r1, r2) and a run of its pairs (c1, c2) of this item, in visit order.
+//    The thread owns the whole 6 x 6 block: acc += C_c1' W_c2 (C_c1 from global memory, W_c2 from shared memory), 108
+//    multiply-adds per pair in registers, then the block (times the conditioning scales s_r of its rows and columns)
+//    is added into the column's tile in shared memory (upper triangle only for the diagonal block).
+// 3. The tile is subtracted from the column of S (contiguous: the column's six scalar columns of H entries each), with
+//    atomics when the column is split into several items; g_S[r2] -= s_r .* sum C_c2' z'.
+// The reference's accumulate_sparse_columns! (src/schur_reduction.jl:315-387) walks the same pairs of each column; W
+// is its W_c2 = E^-1 scaled(C_c2) with the point scales folded in, and the pair product C_c1' W_c2 its W_c1' C_c2
+// transposed (E^-1 is symmetric).
+template <class T>
+__host__ __device__ constexpr int stage_wr() { return sizeof(T) == 4 ? 20 : 18; }   // W record stride (16-byte multiple)
+template <class T>
+static size_t stage_smem(int64_t max_h, int64_t max_nv) {
+  const size_t tile = ((size_t)6 * max_h * sizeof(T) + 15) & ~size_t(15);
+  const size_t w = (size_t)max_nv * stage_wr<T>() * sizeof(T);
+  const size_t p0 = ((size_t)max_nv * 4 + 15) & ~size_t(15);
+  return tile + w + p0 + (SchurPlan::STAGE_NT / 32) * 6 * sizeof(double);
+}
+
+// 18 entries of one coupling block of C (72 bytes FP32 at an 8-byte boundary, 144 bytes FP64 at a 16-byte boundary;
+// C itself on a 16-byte boundary)
+__device__ __forceinline__ void load_block18(const float* __restrict__ C, int64_t c, int64_t ncoup, float* a) {
+  const float* src = C + 18 * c;
+  if (c & 1) {
+    // 8 bytes past a 16-byte boundary: five 16-byte loads from the boundary below, entries 2..19
+    const float4* q = reinterpret_cast<const float4*>(src - 2);
+    float w[20];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) { float4 v = __ldg(q + i); w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w; }
+#pragma unroll
+    for (int i = 0; i < 18; ++i) a[i] = w[i + 2];
+  } else if (c + 1 < ncoup) {
+    // on a 16-byte boundary: five 16-byte loads (the last reaches 8 bytes into the next block)
+    const float4* q = reinterpret_cast<const float4*>(src);
+    float w[20];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) { float4 v = __ldg(q + i); w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w; }
+#pragma unroll
+    for (int i = 0; i < 18; ++i) a[i] = w[i];
+  } else {
+    const float2* q = reinterpret_cast<const float2*>(src);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { float2 v = __ldg(q + i); a[2 * i] = v.x; a[2 * i + 1] = v.y; }
+  }
+}
+__device__ __forceinline__ void load_block18(const double* __restrict__ C, int64_t c, int64_t, double* a) {
+  const double2* q = reinterpret_cast<const double2*>(C + 18 * c);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) { double2 v = __ldg(q + i); a[2 * i] = v.x; a[2 * i + 1] = v.y; }
+}
+__device__ __forceinline__ void load_w18(const float* w, float* b) {
+  const float4* q = reinterpret_cast<const float4*>(w);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) { float4 v = q[i]; b[4 * i] = v.x; b[4 * i + 1] = v.y; b[4 * i + 2] = v.z; b[4 * i + 3] = v.w; }
+  const float2 v = reinterpret_cast<const float2*>(w)[8];
+  b[16] = v.x;
+  b[17] = v.y;
+}
+__device__ __forceinline__ void load_w18(const double* w, double* b) {
+  const double2* q = reinterpret_cast<const double2*>(w);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) { double2 v = q[i]; b[2 * i] = v.x; b[2 * i + 1] = v.y; }
+}
+
+template <class T>
+__global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k_stage36(
+    const int4* __restrict__ items, const int32_t* __restrict__ thr, const int4* __restrict__ units, const uint32_t* __restrict__ pairs,
+    const int32_t* __restrict__ rentry, const int32_t* __restrict__ entry_elim, const int32_t* __restrict__ eptr,
+    const int32_t* __restrict__ col_h, const int64_t* __restrict__ col_base, int64_t ncoup, const T* __restrict__ C,
+    const double* __restrict__ EZ, const double* __restrict__ s_r, T* __restrict__ S, double* __restrict__ g, const Status* __restrict__ st,
+    const int32_t* __restrict__ prob_of_cam, const long long* __restrict__ prob_fail) {
+  constexpr int NT = SchurPlan::STAGE_NT;
+  constexpr int WR = stage_wr<T>();
+  extern __shared__ __align__(16) unsigned char sm[];
+  if (!live(st)) return;
+  const int4 it = items[blockIdx.x];
+  const int r2 = it.x, q0 = it.y, nv = it.z, nseg = it.w;
+  if (prob_fail && prob_fail[prob_of_cam[r2]] != NONE) return;   // the column's problem failed: its S stays reset
+  const int H = __ldg(col_h + r2);
+  const int tid = threadIdx.x;
+  T* tile = reinterpret_cast<T*>(sm);
+  T* W = reinterpret_cast<T*>(sm + (((size_t)6 * H * sizeof(T) + 15) & ~size_t(15)));
+  int* p0s = reinterpret_cast<int*>(W + (size_t)nv * WR);
+  double* gp = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(p0s) + (((size_t)nv * 4 + 15) & ~size_t(15)));
+  for (int i = tid; i < 6 * H; i += NT) tile[i] = T(0);
+  // 1. W and the gradient sums, a thread per visit
+  double ga[6];
+#pragma unroll
+  for (int w = 0; w < 6; ++w) ga[w] = 0.0;
+  for (int v = tid; v < nv; v += NT) {
+    const int c2 = __ldg(rentry + q0 + v);
+    const int e = __ldg(entry_elim + c2);
+    p0s[v] = __ldg(eptr + e);
+    const double2* ez = reinterpret_cast<const double2*>(EZ + 12 * (int64_t)e);
+    double Ep[12];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) { double2 x = __ldg(ez + i); Ep[2 * i] = x.x; Ep[2 * i + 1] = x.y; }
+    T c[18];
+    load_block18(C, c2, ncoup, c);
+    T* wv = W + (size_t)v * WR;
+#pragma unroll
+    for (int w = 0; w < 6; ++w) {
+      const double c0 = (double)c[3 * w], c1 = (double)c[3 * w + 1], c2v = (double)c[3 * w + 2];
+#pragma unroll
+      for (int t = 0; t < 3; ++t) wv[3 * w + t] = T(Ep[t] * c0 + Ep[t + 3] * c1 + Ep[t + 6] * c2v);
+      ga[w] += c0 * Ep[9] + c1 * Ep[10] + c2v * Ep[11];
+    }
+  }
+  __syncthreads();
+  // 2. the thread's units
+  const int* tp = thr + (int64_t)blockIdx.x * (NT + 1);
+  const int ub = __ldg(tp + tid), ue = __ldg(tp + tid + 1);
+  double fc[6];
+#pragma unroll
+  for (int w = 0; w < 6; ++w) fc[w] = s_r ? s_r[6 * r2 + w] : 1.0;
+  for (int u = ub; u < ue; ++u) {
+    const int4 un = __ldg(units + u);
+    const int pb = un.x, pe = un.x + un.y, row = un.z;
+    const bool diag = un.w < 0;
+    const int r1 = un.w & 0x7fffffff;
+    T acc[36];
+#pragma unroll
+    for (int i = 0; i < 36; ++i) acc[i] = T(0);
+    uint32_t pr = __ldg(pairs + pb);
+    T a[18];
+    load_block18(C, p0s[pr & 0xffff] + (int)(pr >> 16), ncoup, a);
+    for (int p = pb; p < pe; ++p) {
+      const int v = pr & 0xffff;
+      T b[18];
+      load_w18(W + (size_t)v * WR, b);
+      T an[18];
+      if (p + 1 < pe) {   // the next pair's coupling block, in flight during this pair's products
+        pr = __ldg(pairs + p + 1);
+        load_block18(C, p0s[pr & 0xffff] + (int)(pr >> 16), ncoup, an);
+      }
+#pragma unroll
+      for (int rho = 0; rho < 6; ++rho)
+#pragma unroll
+        for (int w = 0; w < 6; ++w) {
+          T x = acc[6 * rho + w];
+          x = fma(a[3 * rho], b[3 * w], x);
+          x = fma(a[3 * rho + 1], b[3 * w + 1], x);
+          x = fma(a[3 * rho + 2], b[3 * w + 2], x);
+          acc[6 * rho + w] = x;
+        }
+      if (p + 1 < pe) {
+#pragma unroll
+        for (int i = 0; i < 18; ++i) a[i] = an[i];
+      }
+    }
+#pragma unroll
+    for (int rho = 0; rho < 6; ++rho) {
+      const double fr = s_r ? s_r[6 * r1 + rho] : 1.0;
+#pragma unroll
+      for (int w = 0; w < 6; ++w) {
+        if (diag && rho > w) continue;
+        T val = acc[6 * rho + w];
+        if (s_r) val = T((double)val * (fr * fc[w]));
+        atomicAdd(tile + w * H + row + rho, val);
+      }
+    }
+  }
+  __syncthreads();
+  // 3. the column of S and the gradient
+  const int64_t cb = __ldg(col_base + r2);
+  if (nseg == 1) {
+    for (int i = tid; i < 6 * H; i += NT) S[cb + i] = S[cb + i] - tile[i];
+  } else {
+    for (int i = tid; i < 6 * H; i += NT) atomicAdd(S + cb + i, -tile[i]);
+  }
+  const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int w = 0; w < 6; ++w) {
+    double x = ga[w];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) gp[6 * warp + w] = x;
+  }
+  __syncthreads();
+  if (tid < 6) {
+    double x = 0.0;
+    for (int w = 0; w < NT / 32; ++w) x += gp[6 * w + tid];
+    atomicAdd(g + 6 * r2 + tid, -(s_r ? s_r[6 * r2 + tid] : 1.0) * x);
+  }
+}
+
+// The column-owned schedule of k_stage36 (SchurPlan::stg_*), from the plan's block-owned pair lists (pairs of a
+// column grouped by block slot, each block's in visit order). An item is a run of one block column's visits: its
+// shared memory holds the column's S tile (6 H entries) and per visit W = E' C_c2 (18 entries) and the visit point's
+// first coupling; in FP64 this must fit STAGE_BUDGET bytes, so a column with more visits is cut into several items
+// (their tiles are added to S with atomics). A block's pairs of one item are cut into units of at most stage_unit
+// pairs, and the units are spread over the item's STAGE_NT threads largest first, each to the least loaded thread.
+static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int64_t nc, const std::vector<int32_t>& rptr,
+                                 const std::vector<int32_t>& rentry, const std::vector<int32_t>& entry_elim, const int64_t* eptr,
+                                 const std::vector<int64_t>& bcolptr, const std::vector<int64_t>& browval,
+                                 const std::vector<int64_t>& brow_off, const std::vector<int64_t>& col_h,
+                                 const std::vector<int32_t>& pair_c1, const std::vector<int32_t>& pair_c2,
+                                 const std::vector<int64_t>& colstart, const std::vector<std::vector<int32_t>>& col_cnt) {
+  constexpr int NT = SchurPlan::STAGE_NT;
+  constexpr int64_t STAGE_BUDGET = 200 * 1024;
+  const int U = P->stage_unit;
+  std::vector<int32_t> pos_of(nc);
+  for (int64_t q = 0; q < nc; ++q) pos_of[rentry[q]] = (int32_t)q;
+  struct ColOut {
+    std::vector<int4> items, units;
+    std::vector<int32_t> thr;
+    std::vector<uint32_t> pairs;
+  };
+  std::vector<ColOut> out(nrb);
+  // one launch serves every item, with the largest column tile and the largest visit run: the visit cap is set by the
+  // largest tile, so that any item's share fits the same shared-memory size
+  int64_t max_h = 0;
+  for (int64_t r2 = 0; r2 < nrb; ++r2) max_h = std::max<int64_t>(max_h, col_h[r2]);
+  const int64_t vcap = (STAGE_BUDGET - 48 * max_h - 2048) / 148;
+  if (vcap < 32 || max_h > 65535) return;
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 8) reduction(| : bad)
+  for (int64_t r2 = 0; r2 < nrb; ++r2) {
+    const int64_t nv = rptr[r2 + 1] - rptr[r2];
+    if (nv == 0) continue;
+    const int64_t nseg = (nv + vcap - 1) / vcap;
+    std::vector<int64_t> bnd(nseg + 1);
+    for (int64_t g = 0; g <= nseg; ++g) bnd[g] = g * nv / nseg;
+    // units per item: {block slot, first pair index in `pr`, count}
+    struct Unit { int32_t k, first, n; };
+    std::vector<std::vector<Unit>> seg_units(nseg);
+    std::vector<uint32_t> pr;
+    const auto& cnt = col_cnt[r2];
+    for (int64_t sl = 0; sl + 1 < (int64_t)cnt.size(); ++sl) {
+      const int64_t a = colstart[r2] + cnt[sl], b = colstart[r2] + cnt[sl + 1];
+      int64_t cur_seg = -1, run_first = 0, run_n = 0;
+      for (int64_t x = a; x < b; ++x) {
+        const int32_t c1 = pair_c1[x], c2 = pair_c2[x];
+        const int64_t q = pos_of[c2] - rptr[r2];
+        int64_t g = q * nseg / nv;
+        while (g + 1 <= nseg - 1 && bnd[g + 1] <= q) ++g;
+        while (g > 0 && bnd[g] > q) --g;
+        const int64_t v = q - bnd[g], i1 = c1 - eptr[entry_elim[c2]];
+        if (v > 65535 || i1 < 0 || i1 > 65535) bad = 1;
+        if (g != cur_seg || run_n == U) {
+          if (run_n) seg_units[cur_seg].push_back({(int32_t)(bcolptr[r2] + sl), (int32_t)run_first, (int32_t)run_n});
+          cur_seg = g;
+          run_first = (int64_t)pr.size();
+          run_n = 0;
+        }
+        pr.push_back((uint32_t)v | ((uint32_t)i1 << 16));
+        ++run_n;
+      }
+      if (run_n) seg_units[cur_seg].push_back({(int32_t)(bcolptr[r2] + sl), (int32_t)run_first, (int32_t)run_n});
+    }
+    ColOut& o = out[r2];
+    for (int64_t g = 0; g < nseg; ++g) {
+      auto& us = seg_units[g];
+      // largest first, each to the least loaded thread
+      std::stable_sort(us.begin(), us.end(), [](const Unit& x, const Unit& y) { return x.n > y.n; });
+      std::vector<int32_t> owner(us.size());
+      std::vector<std::pair<int64_t, int>> heap;
+      for (int t = 0; t < NT; ++t) heap.push_back({0, t});
+      auto cmp = [](const std::pair<int64_t, int>& x, const std::pair<int64_t, int>& y) { return x > y; };
+      std::make_heap(heap.begin(), heap.end(), cmp);
+      for (size_t i = 0; i < us.size(); ++i) {
+        std::pop_heap(heap.begin(), heap.end(), cmp);
+        owner[i] = heap.back().second;
+        heap.back().first += us[i].n;
+        std::push_heap(heap.begin(), heap.end(), cmp);
+      }
+      std::vector<int32_t> tcount(NT + 1, 0);
+      for (size_t i = 0; i < us.size(); ++i) tcount[owner[i] + 1] += 1;
+      for (int t = 0; t < NT; ++t) tcount[t + 1] += tcount[t];
+      const int32_t ubase = (int32_t)o.units.size();
+      o.units.resize(o.units.size() + us.size());
+      std::vector<int32_t> fill(tcount.begin(), tcount.end() - 1);
+      for (size_t i = 0; i < us.size(); ++i) {
+        const Unit& u = us[i];
+        const int32_t k = u.k;
+        const int32_t r1 = (int32_t)browval[k];
+        // pair start relative to the column's `pr` for now (made global when the columns are concatenated)
+        o.units[ubase + fill[owner[i]]++] = make_int4(u.first, u.n, (int32_t)brow_off[k], r1 | (r1 == (int32_t)r2 ? INT32_MIN : 0));
+      }
+      for (int t = 0; t <= NT; ++t) o.thr.push_back(ubase + tcount[t]);
+      o.items.push_back(make_int4((int32_t)r2, (int32_t)(rptr[r2] + bnd[g]), (int32_t)(bnd[g + 1] - bnd[g]), (int32_t)nseg));
+    }
+    o.pairs.swap(pr);
+  }
+  if (bad) return;
+  int64_t nitems = 0, nunits = 0, npairs = 0, max_nv = 0;
+  for (int64_t r2 = 0; r2 < nrb; ++r2) {
+    nitems += (int64_t)out[r2].items.size();
+    nunits += (int64_t)out[r2].units.size();
+    npairs += (int64_t)out[r2].pairs.size();
+    for (const int4& it : out[r2].items) max_nv = std::max<int64_t>(max_nv, it.z);
+  }
+  if (npairs >= INT32_MAX || nunits >= INT32_MAX || nitems >= INT32_MAX) return;
+  std::vector<int4> items, units;
+  std::vector<int32_t> thr;
+  std::vector<uint32_t> pairs;
+  items.reserve(nitems);
+  units.reserve(nunits);
+  thr.reserve(nitems * (NT + 1));
+  pairs.reserve(npairs);
+  for (int64_t r2 = 0; r2 < nrb; ++r2) {
+    ColOut& o = out[r2];
+    const int32_t pbase = (int32_t)pairs.size(), ubase = (int32_t)units.size();
+    for (int4 u : o.units) units.push_back(make_int4(u.x + pbase, u.y, u.z, u.w));
+    for (int32_t t : o.thr) thr.push_back(t + ubase);
+    items.insert(items.end(), o.items.begin(), o.items.end());
+    pairs.insert(pairs.end(), o.pairs.begin(), o.pairs.end());
+    std::vector<int4>().swap(o.items);
+    std::vector<int4>().swap(o.units);
+    std::vector<int32_t>().swap(o.thr);
+    std::vector<uint32_t>().swap(o.pairs);
+  }
+  upload(P->stg_items, items, s);
+  upload(P->stg_thr, thr, s);
+  upload(P->stg_units, units, s);
+  upload(P->stg_pairs, pairs, s);
+  P->stage_items = nitems;
+  P->stage_units = nunits;
+  P->stage_max_nv = max_nv;
+  P->stage_ok = true;
+}
+
 static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
   if (!d || d->nrblocks < 1 || d->neblocks < 1) throw Error(BLS_EINVAL, "a plan needs at least one retained and one eliminated block");
   std::unique_ptr<SchurPlan> P(new SchurPlan());
@@ -1623,6 +1983,13 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
       }
     }
   }
+  // the column-owned schedule (k_stage36), sparse S only
+  if (P->fast36 && P->has_sparse) {
+    std::vector<int64_t> colstart(nrb + 1, 0);
+    for (int64_t r2 = 0; r2 < nrb; ++r2) colstart[r2 + 1] = colstart[r2] + col_npairs[r2];
+    build_stage_schedule(P.get(), s, nrb, nc, rptr, rentry, entry_elim, d->eliminated_ptr, bcolptr, browval, brow_off, col_h,
+                         pair_c1, pair_c2, colstart, col_cnt);
+  }
   // staged work items for the host-buffer reduction: stage j holds points [stage_pt[j], stage_pt[j + 1]); a block's
   // pairs ascend in point within its slot, so its pairs of one stage are a contiguous run, cut into items of at most
   // PAIR_CHUNK pairs (solo when the run makes one item)
@@ -1746,6 +2113,10 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
   if (!P->fast36) P->Einv32.alloc(sizeof(float) * std::max<int64_t>(P->E_length, 1));
   P->z.alloc(sizeof(double) * std::max<int64_t>(ne, 1));
   if (P->fast36) P->Einv12.alloc(sizeof(double) * 12 * neb);   // sized for FP64; the FP32 form uses half
+  if (P->stage_ok) {
+    P->EZ.alloc(sizeof(double) * 12 * neb);
+    P->kernel = 5;   // the column-owned schedule is the default where it applies
+  }
   P->status.alloc(sizeof(Status));
   Status init{NONE, NONE, NONE, 0};
   BLS_CUDA(cudaMemcpyAsync(P->status.p, &init, sizeof(Status), cudaMemcpyHostToDevice, s));
@@ -1757,7 +2128,7 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
 static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
-                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h,
+                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h, &P->stg_items, &P->stg_thr, &P->stg_units, &P->stg_pairs, &P->EZ,
                           &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g, &P->w_apply, &P->t_apply, &P->acc1,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
@@ -1916,12 +2287,24 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
     throw Error(BLS_EINVAL, "C_data must be aligned to two elements (the device reads coupling blocks in pairs of entries)");
   cudaStream_t s = P->ctx->stream;
   Status* st = P->status.as<Status>();
+  // the column-owned schedule reads C with 16-byte loads (C_data on a 16-byte boundary, as the device allocators give)
+  const bool c16 = (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+  const bool batch = P->nprob > 0 && !dense;
+  const bool use_stage = P->fast36 && (P->kernel == 5 || batch) && !dense && P->stage_ok && c16;
+  const int32_t* poc = batch ? P->prob_of_cam.as<int32_t>() : nullptr;
+  long long* pf = batch ? P->prob_fail.as<long long>() : nullptr;
+  if (batch) {
+    k_prob_arm<<<grid_for(P->nprob, 256), 256, 0, s>>>(pf, P->nprob);
+    P->launches += 1;
+  }
   if (P->fast36) {
     using TE = typename EinvOf<T>::type;
     k_arm36<<<1, 1, 0, s>>>(st);
     if (P->neblocks > 0)
       k_factor36<T><<<grid_for(P->neblocks, 128), 128, 0, s>>>(0, P->neblocks, E, b_e, sc_e, lambda, s_e, P->Einv64.as<double>(),
-                                                             P->Einv12.as<TE>(), P->z.as<double>(), st);
+                                                             use_stage ? nullptr : P->Einv12.as<TE>(), P->z.as<double>(),
+                                                             use_stage ? P->EZ.as<double>() : nullptr,
+                                                             batch ? P->prob_of_point.as<int32_t>() : nullptr, pf, st);
   } else {
     begin_checked(P, sc_e, P->ne, 1);
     k_arm<<<1, 1, 0, s>>>(st);
@@ -1936,7 +2319,21 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
     BLS_CUDA(cudaEventCreate(&ev0));
     BLS_CUDA(cudaEventCreate(&ev1));
   }
-  if (P->fast36 && P->kernel == 0) {
+  if (use_stage) {
+    k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st, poc, pf);
+    P->launches += 1;
+    if (P->stage_items > 0) {
+      const size_t smem = stage_smem<T>(P->max_col_h, P->stage_max_nv);
+      BLS_CUDA(cudaFuncSetAttribute(k_stage36<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
+      P->launches += 1;
+      k_stage36<T><<<(unsigned)P->stage_items, SchurPlan::STAGE_NT, smem, s>>>(
+          P->stg_items.as<int4>(), P->stg_thr.as<int32_t>(), P->stg_units.as<int4>(), P->stg_pairs.as<uint32_t>(),
+          P->retained_entry.as<int32_t>(), P->entry_eliminated.as<int32_t>(), P->eliminated_ptr.as<int32_t>(), P->col_h.as<int32_t>(),
+          P->col_base.as<int64_t>(), P->ncoup, C, P->EZ.as<double>(), s_r, S, g, st, poc, pf);
+      if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
+    }
+  } else if (P->fast36 && !batch && P->kernel == 0) {
     using TE = typename EinvOf<T>::type;
     struct StageSz { TE a[12]; T b[18]; T c[18]; double d[4]; };
     const int64_t hmax = dense ? P->nr : P->max_col_h;
@@ -1950,7 +2347,7 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
                                               P->vis_off.as<uint16_t>(), P->entry_retained.as<int32_t>(), P->col_base.as<int64_t>(),
                                               P->col_h.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), b_r, s_r, s_e, S, g, st);
     if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
-  } else if (P->fast36 && P->kernel == 3 && !dense && !s_r && !s_e && P->tiles_ok) {
+  } else if (P->fast36 && !batch && P->kernel == 3 && !dense && !s_r && !s_e && P->tiles_ok) {
     using TE = typename EinvOf<T>::type;
     const int cap = (int)(sizeof(T) == 4 ? 4096 : 2048);
     const size_t fixed = sizeof(double) * 32 * 3 + sizeof(double) * 8 * 6 + sizeof(TE) * 32 * 12 + sizeof(T) * 8 * 20 + sizeof(int) * (32 * 5 + 4) + 16;
@@ -1963,7 +2360,7 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
                                                      P->vis_off.as<uint16_t>(), P->col_base.as<int64_t>(), P->col_h.as<int32_t>(), cap, C,
                                                      P->Einv12.as<TE>(), P->z.as<double>(), b_r, S, g, st);
     if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
-  } else if (P->fast36 && P->kernel == 2 && !s_r && !s_e) {
+  } else if (P->fast36 && !batch && P->kernel == 2 && !s_r && !s_e) {
     using TE = typename EinvOf<T>::type;
     k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st);
     P->launches += 1;
@@ -1977,7 +2374,7 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
           dense ? nullptr : P->block_stride_sparse.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), S, g, st);
       if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
     }
-  } else if (P->fast36 && P->kernel == 4 && P->points_ok) {
+  } else if (P->fast36 && !batch && P->kernel == 4 && P->points_ok) {
     using TE = typename EinvOf<T>::type;
     k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st);
     P->launches += 1;
@@ -1993,7 +2390,7 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
     }
   } else if (P->fast36) {
     using TE = typename EinvOf<T>::type;
-    k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st);
+    k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st, poc, pf);
     P->launches += 1;
     if (P->nitems > 0) {
       const int64_t warps = (P->nitems + 4) / 5;
@@ -2002,7 +2399,8 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
       k_pairs36<T><<<grid_for(warps * 32, 128), 128, 0, s>>>(
           P->nitems, P->ncoup, P->item_block.as<int32_t>(), P->item_start.as<int32_t>(), P->item_info.as<int32_t>(), P->pair_packed.as<int2>(),
           P->block_r1.as<int32_t>(), P->block_r2.as<int32_t>(), dense ? P->block_base_dense.as<int64_t>() : P->block_base_sparse.as<int64_t>(),
-          dense ? nullptr : P->block_stride_sparse.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), s_r, s_e, S, g, st);
+          dense ? nullptr : P->block_stride_sparse.as<int32_t>(), P->nr, C, P->Einv12.as<TE>(), P->z.as<double>(), s_r, s_e, S, g, st,
+          poc, pf);
       if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
     }
   } else {
@@ -2082,16 +2480,30 @@ static int reduce_host_impl(SchurPlan* P, T* S_h, double* g_h, const T* R_h, con
   T* S = P->h_S.as<T>();
   double* g = P->h_g.as<double>();
   Status* st = P->status.as<Status>();
+  const bool batch = P->nprob > 0;
+  const int32_t* poc = batch ? P->prob_of_cam.as<int32_t>() : nullptr;
+  long long* pf = batch ? P->prob_fail.as<long long>() : nullptr;
   BLS_CUDA(cudaStreamWaitEvent(s, P->ev_in[0], 0));
   reset_sparse<T>(P, S, P->h_R.as<T>(), P->h_scr.as<double>(), lambda, nullptr);
   k_arm36<<<1, 1, 0, s>>>(st);
-  k_g_init<<<std::max(1, grid_for(P->nr, 256)), 256, 0, s>>>(g, P->h_br.as<double>(), nullptr, P->nr, st);
-  P->launches += 2;
+  P->launches += 1;
+  if (batch) {
+    k_prob_arm<<<grid_for(P->nprob, 256), 256, 0, s>>>(pf, P->nprob);
+    P->launches += 1;
+  } else {
+    k_g_init<<<std::max(1, grid_for(P->nr, 256)), 256, 0, s>>>(g, P->h_br.as<double>(), nullptr, P->nr, st);
+    P->launches += 1;
+  }
   using TE = typename EinvOf<T>::type;
   BLS_CUDA(cudaStreamWaitEvent(s, P->ev_points, 0));
   if (P->neblocks > 0) {
     k_factor36<T><<<grid_for(P->neblocks, 128), 128, 0, s>>>(0, P->neblocks, P->h_E.as<T>(), P->h_be.as<double>(), P->h_sce.as<double>(), lambda,
-                                                             nullptr, P->Einv64.as<double>(), P->Einv12.as<TE>(), P->z.as<double>(), st);
+                                                             nullptr, P->Einv64.as<double>(), P->Einv12.as<TE>(), P->z.as<double>(), nullptr,
+                                                             batch ? P->prob_of_point.as<int32_t>() : nullptr, pf, st);
+    P->launches += 1;
+  }
+  if (batch) {   // after the factorisation: a failing problem keeps its g_S
+    k_g_init<<<std::max(1, grid_for(P->nr, 256)), 256, 0, s>>>(g, P->h_br.as<double>(), nullptr, P->nr, st, poc, pf);
     P->launches += 1;
   }
   for (int j = 0; j < K; ++j) {
@@ -2101,15 +2513,31 @@ static int reduce_host_impl(SchurPlan* P, T* S_h, double* g_h, const T* R_h, con
       k_pairs36<T><<<grid_for((n + 4) / 5 * 32, 128), 128, 0, s>>>(
           n, P->ncoup, P->st_block.as<int32_t>() + i0, P->st_start.as<int32_t>() + i0, P->st_info.as<int32_t>() + i0, P->pair_packed.as<int2>(),
           P->block_r1.as<int32_t>(), P->block_r2.as<int32_t>(), P->block_base_sparse.as<int64_t>(), P->block_stride_sparse.as<int32_t>(), P->nr,
-          P->h_C.as<T>(), P->Einv12.as<TE>(), P->z.as<double>(), nullptr, nullptr, S, g, st);
+          P->h_C.as<T>(), P->Einv12.as<TE>(), P->z.as<double>(), nullptr, nullptr, S, g, st, poc, pf);
       P->launches += 1;
     }
   }
   BLS_CUDA(cudaGetLastError());
   const int rc = read_status(P, failed_block);
   if (rc != BLS_OK) return rc;
-  BLS_CUDA(cudaMemcpyAsync(S_h, S, sizeof(T) * P->nnzS, cudaMemcpyDeviceToHost, s));
-  BLS_CUDA(cudaMemcpyAsync(g_h, g, sizeof(double) * P->nr, cudaMemcpyDeviceToHost, s));
+  if (batch) {
+    // only the problems that succeeded are copied back: a failing problem's S and g_S stay as the caller had them
+    std::vector<long long> f((size_t)P->nprob);
+    BLS_CUDA(cudaMemcpyAsync(f.data(), pf, sizeof(long long) * P->nprob, cudaMemcpyDeviceToHost, s));
+    BLS_CUDA(cudaStreamSynchronize(s));
+    for (int64_t a = 0; a < P->nprob;) {
+      if (f[a] != NONE) { ++a; continue; }
+      int64_t b = a;
+      while (b < P->nprob && f[b] == NONE) ++b;   // a run of problems that succeeded: one copy of S and one of g_S
+      const int64_t s0 = P->prob_nnz_off[a], s1 = P->prob_nnz_off[b], g0 = P->prob_row_off[a], g1 = P->prob_row_off[b];
+      BLS_CUDA(cudaMemcpyAsync(S_h + s0, S + s0, sizeof(T) * (s1 - s0), cudaMemcpyDeviceToHost, s));
+      BLS_CUDA(cudaMemcpyAsync(g_h + g0, g + g0, sizeof(double) * (g1 - g0), cudaMemcpyDeviceToHost, s));
+      a = b;
+    }
+  } else {
+    BLS_CUDA(cudaMemcpyAsync(S_h, S, sizeof(T) * P->nnzS, cudaMemcpyDeviceToHost, s));
+    BLS_CUDA(cudaMemcpyAsync(g_h, g, sizeof(double) * P->nr, cudaMemcpyDeviceToHost, s));
+  }
   BLS_CUDA(cudaStreamSynchronize(s));
   return BLS_OK;
 }
@@ -2388,11 +2816,78 @@ int bls_reduce_schur_dense(bls_schur_plan* P, int dtype, void* S, double* g, con
 }
 
 int bls_schur_plan_set_kernel(bls_schur_plan* P, int which) {
-  if (!P || which < 0 || which > 4) return BLS_EINVAL;
+  if (!P || which < 0 || which > 5) return BLS_EINVAL;
   BLS_GUARD({
     if (which == 4) ensure_points(P);
     P->kernel = which;
     return BLS_OK;
+  })
+}
+
+// The phase-2 kernel the next reduction of this storage type launches (the dispatch of reduce(), without the calls).
+int bls_schur_plan_phase2_kernel(bls_schur_plan* P, int dtype, int dense, int scaled, char* buf, int64_t cap) {
+  if (!P || !buf || cap < 1 || (dtype != BLS_F64 && dtype != BLS_F32)) return BLS_EINVAL;
+  const std::string t = dtype == BLS_F32 ? "<float>" : "<double>";
+  std::string name;
+  if (P->fast36 && (P->kernel == 5 || P->nprob > 0) && !dense && P->stage_ok) name = "k_stage36" + t;
+  else if (P->fast36 && P->nprob > 0 && !dense) name = "k_pairs36" + t;
+  else if (P->fast36 && P->kernel == 0) name = std::string("k_columns36") + t;
+  else if (P->fast36 && P->kernel == 3 && !dense && !scaled && P->tiles_ok) name = "k_tiles36" + t;
+  else if (P->fast36 && P->kernel == 2 && !scaled) name = "k_pairs_lane" + t;
+  else if (P->fast36 && P->kernel == 4 && P->points_ok) name = "k_points36" + t;
+  else if (P->fast36) name = "k_pairs36" + t;
+  else name = "k_pairs" + t;
+  std::snprintf(buf, (size_t)cap, "%s", name.c_str());
+  return BLS_OK;
+}
+
+int bls_schur_plan_set_problems(bls_schur_plan* P, int64_t nprob, const int64_t* point_off, const int64_t* camera_off,
+                                const int64_t* row_off, const int64_t* nnz_off) {
+  BLS_GUARD({
+    if (!P) throw Error(BLS_EINVAL, "null plan");
+    if (nprob == 0) { P->nprob = 0; return BLS_OK; }
+    if (nprob < 0 || !point_off || !camera_off || !row_off || !nnz_off) throw Error(BLS_EINVAL, "null argument");
+    if (!P->fast36 || !P->has_sparse)
+      throw Error(BLS_EUNSUPPORTED, "per-problem failure needs a sparse plan on the 6/3 fast path");
+    if (point_off[0] != 0 || point_off[nprob] != P->neblocks || camera_off[0] != 0 || camera_off[nprob] != P->nrblocks ||
+        row_off[0] != 0 || row_off[nprob] != P->nr || nnz_off[0] != 0 || nnz_off[nprob] != P->nnzS)
+      throw Error(BLS_EINVAL, "problem offsets must start at 0 and end at the plan's sizes");
+    std::vector<int32_t> pop((size_t)P->neblocks), poc((size_t)P->nrblocks);
+    for (int64_t p = 0; p < nprob; ++p) {
+      if (point_off[p + 1] < point_off[p] || camera_off[p + 1] < camera_off[p] || row_off[p + 1] < row_off[p] || nnz_off[p + 1] < nnz_off[p])
+        throw Error(BLS_EINVAL, "problem offsets must be non-decreasing");
+      for (int64_t e = point_off[p]; e < point_off[p + 1]; ++e) pop[e] = (int32_t)p;
+      for (int64_t r = camera_off[p]; r < camera_off[p + 1]; ++r) poc[r] = (int32_t)p;
+    }
+    cudaStream_t s = P->ctx->stream;
+    upload(P->prob_of_point, pop, s);
+    upload(P->prob_of_cam, poc, s);
+    P->prob_fail.alloc(sizeof(long long) * (size_t)nprob);
+    std::vector<long long> none((size_t)nprob, NONE);
+    BLS_CUDA(cudaMemcpyAsync(P->prob_fail.p, none.data(), sizeof(long long) * nprob, cudaMemcpyHostToDevice, s));
+    BLS_CUDA(cudaStreamSynchronize(s));
+    P->prob_point_off.assign(point_off, point_off + nprob + 1);
+    P->prob_row_off.assign(row_off, row_off + nprob + 1);
+    P->prob_nnz_off.assign(nnz_off, nnz_off + nprob + 1);
+    P->nprob = nprob;
+    return BLS_OK;
+  })
+}
+
+int bls_schur_plan_problem_status(bls_schur_plan* P, int64_t* failed_blocks) {
+  BLS_GUARD({
+    if (!P || !failed_blocks) throw Error(BLS_EINVAL, "null argument");
+    if (P->nprob == 0) throw Error(BLS_EINVAL, "the plan has no problem partition");
+    std::vector<long long> f((size_t)P->nprob);
+    cudaStream_t s = P->ctx->stream;
+    BLS_CUDA(cudaMemcpyAsync(f.data(), P->prob_fail.p, sizeof(long long) * P->nprob, cudaMemcpyDeviceToHost, s));
+    BLS_CUDA(cudaStreamSynchronize(s));
+    int64_t nfail = 0;
+    for (int64_t p = 0; p < P->nprob; ++p) {
+      failed_blocks[p] = f[p] == NONE ? 0 : f[p] - P->prob_point_off[p] + 1;
+      nfail += f[p] != NONE;
+    }
+    return nfail ? BLS_NOT_PD : BLS_OK;
   })
 }
 

@@ -211,6 +211,11 @@ class QRReductionWorkspace:
         """Device kernel launches since the last call."""
         return int(_lib.gpu().bls_qr_plan_counters(self._h))
 
+    def set_staging(self, bulk: bool) -> None:
+        """Stage each table into shared memory with one bulk (TMA) copy per contiguous span (True, the default) or with
+        element-wise asynchronous copies (False); the results are the same."""
+        check(_lib.gpu().bls_qr_plan_set_staging(self._h, int(bulk)))
+
 
 def reduce_qr(ws: QRReductionWorkspace, J: SchurBlockJacobian, scaling_e: torch.Tensor, lam: float, s: torch.Tensor | None = None,
               *, sync: bool = True) -> bool:

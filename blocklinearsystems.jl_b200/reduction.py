@@ -114,11 +114,21 @@ class SchurReductionWorkspace:
         return int(_lib.gpu().bls_schur_plan_device_bytes(self._h))
 
     def set_kernel(self, which: str) -> None:
-        """Phase-2 kernel of the 6/3 fast path: "pairs" (block owned, six lanes per pair list, the default), "lanes"
-        (block owned, a lane per pair, a warp per pair list), "columns" (block-column owned, a warp per visit) or
-        "tiles" (block-column owned, visits staged in chunks; sparse S without conditioning scales, else "pairs") or
-        "points" (point-major, six lanes per pair, vector reductions into S)."""
-        check(_lib.gpu().bls_schur_plan_set_kernel(self._h, {"columns": 0, "pairs": 1, "lanes": 2, "tiles": 3, "points": 4}[which]))
+        """Phase-2 kernel of the 6/3 fast path: "stage" (block-column owned: the column's point-side operands staged in
+        shared memory, a thread per 6 x 6 block accumulating in registers; the default for a sparse S), "pairs" (block
+        owned, six lanes per pair list; the default for a dense S), "lanes" (block owned, a lane per pair, a warp per
+        pair list), "columns" (block-column owned, a warp per visit), "tiles" (block-column owned, visits staged in
+        chunks; sparse S without conditioning scales, else "pairs") or "points" (point-major, six lanes per pair,
+        vector reductions into S)."""
+        check(_lib.gpu().bls_schur_plan_set_kernel(self._h, {"columns": 0, "pairs": 1, "lanes": 2, "tiles": 3, "points": 4,
+                                                             "stage": 5}[which]))
+
+    def phase2_kernel_name(self, dtype=torch.float32, *, dense: bool = False, scaled: bool = False) -> str:
+        """The phase-2 kernel the next reduction with this storage type launches (as the profiler lists it)."""
+        buf = C.create_string_buffer(64)
+        check(_lib.gpu().bls_schur_plan_phase2_kernel(self._h, _lib.BLS_F32 if dtype == torch.float32 else _lib.BLS_F64,
+                                                      int(dense), int(scaled), buf, 64))
+        return buf.value.decode()
 
     def instrument(self, timing: bool = True) -> None:
         """Bracket the pair kernel of each reduction with CUDA events (read them with counters())."""

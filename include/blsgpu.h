@@ -196,6 +196,23 @@ int bls_schur_plan_instrument(bls_schur_plan* plan, int timing);
  * 4 = point-major, six lanes per pair, entries added into S with vector reductions (as 1 when S has 2^25 or more
  * blocks). All compute the same reduction; the choice is kept for comparisons and for autotuning. */
 int bls_schur_plan_set_kernel(bls_schur_plan* plan, int which);
+/* No counterpart in the reference (a batch of the reference's calls in one plan): declare that the plan's structure is
+ * the disjoint union of `nprob` independent problems, problem p owning eliminated blocks [point_off[p],
+ * point_off[p+1]), retained blocks [camera_off[p], camera_off[p+1]), rows [row_off[p], row_off[p+1]) of g_S and
+ * entries [nnz_off[p], nnz_off[p+1]) of S.nzval (host arrays of nprob + 1, from 0 to the plan's sizes). Each problem
+ * then fails on its own, as a separate reduce_schur_sparse! call would (src/schur_reduction.jl:233-257): a problem with
+ * a failing eliminated block keeps its reset S and its g_S, the others are reduced; the reduction's own status is
+ * BLS_OK and the problems' verdicts are read with bls_schur_plan_problem_status. Sparse plans on the 6/3 fast path
+ * only; nprob = 0 removes the partition. */
+int bls_schur_plan_set_problems(bls_schur_plan* plan, int64_t nprob, const int64_t* point_off, const int64_t* camera_off,
+                                const int64_t* row_off, const int64_t* nnz_off);
+/* Per problem of the last reduction: 0, or its lowest failing eliminated block (1-based, local to the problem) in
+ * failed_blocks[nprob] (host). Returns BLS_NOT_PD if any problem failed. Synchronises. */
+int bls_schur_plan_problem_status(bls_schur_plan* plan, int64_t* failed_blocks);
+/* No counterpart in the reference (instrumentation): the name of the phase-2 kernel that the next reduction of storage
+ * type `dtype` launches on this plan, for a dense (`dense` != 0) or sparse S, with conditioning scales (`scaled` != 0)
+ * or without, written NUL-terminated into buf[cap]. */
+int bls_schur_plan_phase2_kernel(bls_schur_plan* plan, int dtype, int dense, int scaled, char* buf, int64_t cap);
 int bls_schur_plan_counters(bls_schur_plan* plan, int64_t* launches, double* pair_kernel_ms, int64_t* pair_kernel_launches);
 
 /* Status of the last reduction on this plan (synchronises): BLS_OK / BLS_NOT_PD / BLS_EINVAL. */
@@ -303,6 +320,11 @@ typedef struct bls_qr_plan_desc {
 
 int bls_qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* desc, bls_qr_plan** out);
 int bls_qr_plan_destroy(bls_qr_plan* plan);
+/* No counterpart in the reference (a staging choice of this build): how the table kernels (reduce_qr, the Gram kernels
+ * of reduced_normal_*, reduced_diagonal_blocks and bls_assemble_hessian) bring each table into shared memory. bulk != 0
+ * (the default): one bulk (TMA) copy per contiguous span, completed on an mbarrier; 0: element-wise asynchronous copies.
+ * Buffers whose starts are not 16-byte aligned are always staged element-wise. Results are identical either way. */
+int bls_qr_plan_set_staging(bls_qr_plan* plan, int bulk);
 
 /* reduce_qr!(ws, J, scaling_e, lambda, s) (src/qr_reduction.jl:162-187): every eliminated table copied from the raw
  * tables Rw / residual Rr into F / Fr, damped with sqrt(lambda*scaling_e) (times s_e) and QR-factored in place; free

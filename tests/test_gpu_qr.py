@@ -326,3 +326,33 @@ def test_prepare_scale_bit_identical(bls):
             rec = bls.prepare_scale(s, cu(d), lam, cu(sc), dtype, stale=False)
             orec = orc.prepare_scale(os_, d, lam, sc, T, stale=False)
             assert rec == orec and (s.cpu().numpy() == os_).all()
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+def test_bulk_staging_matches_element_staging(bls, dtype):
+    """The table kernels stage each table with one bulk (TMA) copy per contiguous span by default; element-wise
+    staging (the other mode) must give bit-identical factored tables, residual, J~'J~, J~'r~, diagonal blocks and
+    assembled Hessian, on the scaled QR scene and on a table buffer offset by one element from a 16-byte boundary
+    (which falls back to element staging)."""
+    spec, p, o, _ = _qr_scene(bls)
+    j = p.structure
+    pat = bls.build_schur_pattern(j.schur, bls.free_block_pairs(j))
+    nr = j.schur.nr
+    outs = []
+    for bulk, shift in ((True, 0), (False, 0), (True, 1)):
+        ws = bls.QRReductionWorkspace(j, pat, dtype)
+        ws.set_staging(bulk)
+        raw = torch.zeros(len(p.Rw) + 1, dtype=dtype, device=DEV)
+        raw[shift:shift + len(p.Rw)] = cu(p.Rw, dtype)
+        J = bls.SchurBlockJacobian(j, dtype, data=raw[shift:shift + len(p.Rw)], r=cu(p.Rr))
+        assert bls.reduce_qr(ws, J, cu(p.scaling_e), p.lam)
+        S = torch.zeros(pat.nnz, dtype=dtype, device=DEV)
+        g = torch.zeros(nr, dtype=torch.float64, device=DEV)
+        bls.reduced_normal_sparse(S, g, ws, pat)
+        D = torch.zeros(int(j.doffsets[-1]), dtype=dtype, device=DEV)
+        bls.reduced_diagonal_blocks(D, ws)
+        E, Cd, R, b = bls.assemble_hessian(J, ws)
+        outs.append([t.double().cpu().numpy().copy() for t in (ws.factored, ws.fres, S, g, D, E, Cd, R, b)])
+    for other in outs[1:]:
+        for a, b_ in zip(outs[0], other):
+            assert np.array_equal(a, b_)

@@ -165,7 +165,7 @@ def scene_system(bls, name, ncams, npoints, dense=False, seed=None):
     return p, st, ost, opat
 
 
-@pytest.mark.parametrize("kernel", ["columns", "pairs", "lanes", "tiles", "points"])
+@pytest.mark.parametrize("kernel", ["stage", "columns", "pairs", "lanes", "tiles", "points"])
 @pytest.mark.parametrize("name,ncams,npoints,dense", [
     ("dense_50x2000", 50, 2000, True),            # the dense workload at full size
     ("sparse_1000x200k", 120, 8000, False),
@@ -182,7 +182,7 @@ def test_scene_fp64_matches_oracle(bls, name, ncams, npoints, dense, kernel):
     assert relerr(o["x_e"], o["ox_e"]) < 1e-10
 
 
-@pytest.mark.parametrize("kernel", ["columns", "pairs", "lanes", "tiles", "points"])
+@pytest.mark.parametrize("kernel", ["stage", "columns", "pairs", "lanes", "tiles", "points"])
 @pytest.mark.parametrize("name,ncams,npoints", [("sparse_1000x200k", 120, 8000), ("pcg_10000x1M", 150, 6000)])
 def test_scene_mixed_matches_fp64_oracle(bls, name, ncams, npoints, kernel):
     p, st, ost, opat = scene_system(bls, name, ncams, npoints)
@@ -194,7 +194,7 @@ def test_scene_mixed_matches_fp64_oracle(bls, name, ncams, npoints, kernel):
     assert relerr(o["x_e"], o["ox_e"]) < 1e-6
 
 
-@pytest.mark.parametrize("kernel", ["pairs", "points", "lanes"])
+@pytest.mark.parametrize("kernel", ["stage", "pairs", "points", "lanes"])
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
 @pytest.mark.parametrize("dense", [False, True])
 def test_scene_conditioned_scales(bls, kernel, dtype, dense):
