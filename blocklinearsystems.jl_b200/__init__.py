@@ -11,7 +11,8 @@ Device reduction:        SchurReductionWorkspace, reset_schur_sparse / reset_sch
 QR elimination:          SchurJacobianStructure, SchurBlockJacobian, QRReductionWorkspace, reduce_qr, qr_backsubstitute,
                          reduced_normal_sparse / reduced_normal_dense, reduced_diagonal_blocks, free_block_pairs,
                          reduced_residual, reduced_jacobian / reduced_jacobian_sparse, build_reduced_jacobian_pattern,
-                         reduced_mul / reduced_tmul, lsmr_reduced (the matrix-free LSMR solve of the reduced problem)
+                         reduced_mul / reduced_tmul, lsmr_reduced (the matrix-free LSMR solve of the reduced problem),
+                         qr_refine (iterative refinement of the QR route's solve against the FP64 normal equations)
 Reduced solve:           BlockJacobi, factor_diagonal_blocks, solve_diagonal_blocks, PCGWorkspace (block-Jacobi PCG)
 Learned preconditioner:  gnn.LearnedPreconditioner, gnn.train, gnn.init_params
 Batches:                 batch.BatchedReduction (uneven problems as one plan, one CUDA graph)
@@ -26,7 +27,7 @@ from .reduction import (SchurReductionWorkspace, backsubstitute, context, reduce
 from .qr import (QRReductionWorkspace, SchurBlockJacobian, assemble_hessian, jtj_diag, jtj_quadform, jtr, SchurJacobianStructure, free_block_pairs, qr_backsubstitute, reduce_qr,
                  reduced_diagonal_blocks, reduced_nrows, reduced_normal_dense, reduced_normal_sparse, reduced_residual,
                  reduced_jacobian, reduced_jacobian_sparse, build_reduced_jacobian_pattern, reduced_mul, reduced_tmul,
-                 lsmr_reduced, LsmrResult)
+                 lsmr_reduced, LsmrResult, qr_refine, RefineResult)
 from .pcg import BlockJacobi, PCGResult, PCGWorkspace, RefinedResult, factor_diagonal_blocks, solve_diagonal_blocks
 from .dense import DenseCholesky
 from . import batch, gnn, scenes
@@ -38,6 +39,6 @@ __all__ = [
     "reduce_schur_sparse", "reset_reduce_schur_sparse_host", "reset_schur_dense", "reset_schur_sparse", "scatter_copy", "scenes", "QRReductionWorkspace",
     "SchurBlockJacobian", "SchurJacobianStructure", "assemble_hessian", "jtj_diag", "jtj_quadform", "jtr", "prepare_scale", "free_block_pairs", "qr_backsubstitute", "reduce_qr", "reduced_diagonal_blocks",
     "reduced_nrows", "reduced_normal_dense", "reduced_normal_sparse", "reduced_residual", "reduced_jacobian",
-    "reduced_jacobian_sparse", "build_reduced_jacobian_pattern", "reduced_mul", "reduced_tmul", "lsmr_reduced", "LsmrResult", "BlockJacobi", "PCGResult", "PCGWorkspace", "RefinedResult", "DenseCholesky",
+    "reduced_jacobian_sparse", "build_reduced_jacobian_pattern", "reduced_mul", "reduced_tmul", "lsmr_reduced", "LsmrResult", "qr_refine", "RefineResult", "BlockJacobi", "PCGResult", "PCGWorkspace", "RefinedResult", "DenseCholesky",
     "factor_diagonal_blocks", "solve_diagonal_blocks", "gnn", "batch", "symmetrifyfull", "symmetrifyfull_",
 ]

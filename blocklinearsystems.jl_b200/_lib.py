@@ -111,6 +111,9 @@ def gpu() -> C.CDLL:
             "bls_qr_plan_create": (C.c_int, [vp, C.POINTER(bls_qr_plan_desc), C.POINTER(vp)]),
             "bls_qr_plan_destroy": (C.c_int, [vp]),
             "bls_qr_plan_set_staging": (C.c_int, [vp, C.c_int]),
+            "bls_qr_normal_residual": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_double, vp, vp, vp]),
+            "bls_qr_reduce_rhs": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+            "bls_qr_backsubstitute_rhs": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_reduce_qr": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, p64]),
             "bls_qr_backsubstitute": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bls_qr_query_status": (C.c_int, [vp, p64]),

@@ -42,6 +42,7 @@ struct QRPlan {
   bool all6 = true;   // every retained block has 6 columns (the Gram kernel's 6 x 6 form only)
   bool bulk = true;   // stage tables with bulk copies (false: element copies; bls_qr_plan_set_staging)
   int max_dr = 0;
+  int max_de = 0;
   // device: per table, per entry, per retained / eliminated block
   DevBuf t_rows, t_cols, t_top, t_raw, t_res, t_ptr, e_dims, boff_e;
   DevBuf u_ret, u_col, r_dims, boff_r, doff;
@@ -641,14 +642,16 @@ __global__ void k_qr_backsub(int64_t ne_tab, const int32_t* __restrict__ t_rows,
                              const int64_t* __restrict__ t_raw, const int64_t* __restrict__ t_res, const int32_t* __restrict__ t_ptr,
                              const int32_t* __restrict__ u_col, const int32_t* __restrict__ u_ret, const int32_t* __restrict__ r_dims,
                              const int32_t* __restrict__ boff_r, const int32_t* __restrict__ e_dims, const int32_t* __restrict__ boff_e,
-                             const T* __restrict__ F, const double* __restrict__ Fr, const double* __restrict__ x_r, double* __restrict__ x_e) {
+                             const T* __restrict__ F, const double* __restrict__ Fr, const double* __restrict__ x_r, double* __restrict__ x_e,
+                             const double* __restrict__ w = nullptr) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= ne_tab) return;
   const int M = t_rows[e], C = t_cols[e], de = e_dims[e], ce = C - de - 1;
   const int64_t off = t_raw[e];
-  // t = q - B x_r accumulated in x_e's own entries, then U x_e = t solved in place (the same operations in the same order)
+  // t = q - B x_r accumulated in x_e's own entries, then U x_e = t solved in place (the same operations in the same order);
+  // q is the factored residual's top rows, or the given w (a refinement step's U^-T d_e)
   double* xe = x_e + boff_e[e];
-  for (int i = 0; i < de; ++i) xe[i] = Fr[t_res[e] + i];
+  for (int i = 0; i < de; ++i) xe[i] = w ? w[boff_e[e] + i] : Fr[t_res[e] + i];
   for (int u = t_ptr[e]; u < t_ptr[e + 1]; ++u) {
     const int r = u_ret[u], ro = boff_r[r];
     const T* cb = F + off + (int64_t)u_col[u] * M;
@@ -661,6 +664,81 @@ __global__ void k_qr_backsub(int64_t ne_tab, const int32_t* __restrict__ t_rows,
     double acc = xe[i];
     for (int j = i + 1; j < de; ++j) acc -= (double)F[off + (int64_t)(ce + j) * M + i] * xe[j];
     xe[i] = acc / (double)F[off + (int64_t)(ce + i) * M + i];
+  }
+}
+
+// Iterative refinement of the QR route (no reference counterpart; the reference solves the reduced system once,
+// src/qr_linear_systems.jl:250-300). A step needs the normal-equation residual of the whole damped problem in FP64 and
+// the reduction of that residual through the factored tables:
+//   y = r - J x on every row of the raw tables (the damping rows of an eliminated table are zero: its damping is
+//       lambda * scaling, added below), then d = J' y - lambda * scaling .* x (d through jtr!'s kernels);
+//   per eliminated table, with its factored top rows [U B]: w = U^-T d_e and d_r -= B' w, so that the correction of x_r
+//       solves (J~'J~ + lambda diag(scaling_r)) dx_r = d_r, and dx_e = U^-1 (w - B dx_r) (the back-substitution with w).
+// U' U and U' B are the eliminated and coupling blocks of J'J + lambda diag(scaling) (the table's QR), so the three
+// steps are the block elimination of the normal equations with the factored tables; everything is FP64 arithmetic on
+// the tables' storage type.
+template <class T>
+__global__ void __launch_bounds__(256) k_qr_rows_residual(int64_t ntab, int64_t neb, const int32_t* __restrict__ t_rows,
+                                                          const int32_t* __restrict__ t_cols, const int64_t* __restrict__ t_raw,
+                                                          const int64_t* __restrict__ t_res, const int32_t* __restrict__ t_ptr,
+                                                          const int32_t* __restrict__ u_col, const int32_t* __restrict__ u_ret,
+                                                          const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                                                          const int32_t* __restrict__ e_dims, const int32_t* __restrict__ boff_e, int64_t nr,
+                                                          const T* __restrict__ J, const double* __restrict__ r, const double* __restrict__ x,
+                                                          double* __restrict__ y) {
+  const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= ntab) return;
+  const int M = t_rows[t], C = t_cols[t] - 1;
+  const bool elim = t < neb;
+  const int de = elim ? e_dims[t] : 0, me = M - de, ce = C - de;
+  const int64_t off = t_raw[t], rq = t_res[t];
+  for (int i = lane; i < M; i += 32) {
+    if (i >= me) {   // an eliminated table's damping rows
+      y[rq + i] = 0.0;
+      continue;
+    }
+    double acc = r[rq + i];
+    for (int u = t_ptr[t]; u < t_ptr[t + 1]; ++u) {
+      const int c0 = u_col[u], ro = boff_r[u_ret[u]], d = r_dims[u_ret[u]];
+      for (int j = 0; j < d; ++j) acc -= (double)J[off + (int64_t)(c0 + j) * M + i] * x[ro + j];
+    }
+    for (int j = 0; j < de; ++j) acc -= (double)J[off + (int64_t)(ce + j) * M + i] * x[nr + boff_e[t] + j];
+    y[rq + i] = acc;
+  }
+}
+
+__global__ void k_sub_damping(int64_t n, double lambda, const double* __restrict__ sc, const double* __restrict__ x, double* __restrict__ d) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) d[i] -= lambda * sc[i] * x[i];
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_qr_reduce_rhs(int64_t neb, const int32_t* __restrict__ t_rows, const int32_t* __restrict__ t_cols,
+                                                       const int64_t* __restrict__ t_raw, const int32_t* __restrict__ t_ptr,
+                                                       const int32_t* __restrict__ u_col, const int32_t* __restrict__ u_ret,
+                                                       const int32_t* __restrict__ r_dims, const int32_t* __restrict__ boff_r,
+                                                       const int32_t* __restrict__ e_dims, const int32_t* __restrict__ boff_e, int64_t nr,
+                                                       const T* __restrict__ F, const double* __restrict__ d, double* __restrict__ w,
+                                                       double* __restrict__ d_r) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= neb) return;
+  const int M = t_rows[e], C = t_cols[e] - 1, de = e_dims[e], ce = C - de;
+  const int64_t off = t_raw[e];
+  double we[16];
+  for (int i = 0; i < de; ++i) {   // U' w = d_e, forward substitution (U upper triangular in the top rows)
+    double acc = d[nr + boff_e[e] + i];
+    for (int k = 0; k < i; ++k) acc -= (double)F[off + (int64_t)(ce + i) * M + k] * we[k];
+    we[i] = acc / (double)F[off + (int64_t)(ce + i) * M + i];
+    w[boff_e[e] + i] = we[i];
+  }
+  for (int u = t_ptr[e]; u < t_ptr[e + 1]; ++u) {   // d_r -= B' w
+    const int c0 = u_col[u], ro = boff_r[u_ret[u]], dr = r_dims[u_ret[u]];
+    for (int j = 0; j < dr; ++j) {
+      double acc = 0.0;
+      for (int i = 0; i < de; ++i) acc += (double)F[off + (int64_t)(c0 + j) * M + i] * we[i];
+      atomicAdd(d_r + ro + j, -acc);
+    }
   }
 }
 
@@ -906,6 +984,7 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
   }
   for (int64_t e = 0; e < neb; ++e) {
     if (d->e_dims[e] < 1) throw Error(BLS_EINVAL, "eliminated block sizes must be positive");
+    P->max_de = std::max<int>(P->max_de, (int)std::min<int64_t>(d->e_dims[e], 1 << 20));
     boff_e[e] = ne; ne += d->e_dims[e];
   }
   P->nr = nr; P->ne = ne;
@@ -1730,6 +1809,84 @@ int bls_qr_plan_destroy(bls_qr_plan* plan) {
     delete static_cast<QRPlan*>(plan);
   }
   return BLS_OK;
+}
+
+int bls_qr_normal_residual(bls_qr_plan* P, int dtype, const void* J, const double* r, const double* scaling, double lambda,
+                           const double* x, double* y, double* d) {
+  QR_GUARD({
+    if (!P || !J || !r || !scaling || !x || !y || !d) throw Error(BLS_EINVAL, "a device pointer is NULL");
+    if (!(std::isfinite(lambda) && lambda >= 0)) throw Error(BLS_EINVAL, "lambda must be finite and non-negative");
+    cudaStream_t s = P->ctx->stream;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, grid_for(P->ntables * 32, 256));
+    if (dtype == BLS_F64) {
+      k_qr_rows_residual<double><<<grid, 256, 0, s>>>(P->ntables, P->neblocks, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(),
+                                                     P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(),
+                                                     P->u_ret.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(),
+                                                     P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), P->nr, (const double*)J, r, x, y);
+      jt_columns<double, 0>(P, d, (const double*)J, y);
+    } else if (dtype == BLS_F32) {
+      k_qr_rows_residual<float><<<grid, 256, 0, s>>>(P->ntables, P->neblocks, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(),
+                                                    P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(),
+                                                    P->u_ret.as<int32_t>(), P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(),
+                                                    P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), P->nr, (const float*)J, r, x, y);
+      jt_columns<float, 0>(P, d, (const float*)J, y);
+    } else {
+      throw Error(BLS_EINVAL, "unknown dtype");
+    }
+    const int64_t n = P->nr + P->ne;
+    k_sub_damping<<<(unsigned)std::max<int64_t>(1, grid_for(n, 256)), 256, 0, s>>>(n, lambda, scaling, x, d);
+    P->launches += 2;
+    BLS_CUDA(cudaGetLastError());
+    return BLS_OK;
+  })
+}
+
+int bls_qr_reduce_rhs(bls_qr_plan* P, int dtype, const void* F, const double* d, double* w, double* d_r) {
+  QR_GUARD({
+    if (!P || !F || !d || !w || !d_r) throw Error(BLS_EINVAL, "a device pointer is NULL");
+    if (P->max_de > 16) throw Error(BLS_EUNSUPPORTED, "eliminated blocks above 16 variables");
+    cudaStream_t s = P->ctx->stream;
+    BLS_CUDA(cudaMemcpyAsync(d_r, d, sizeof(double) * P->nr, cudaMemcpyDeviceToDevice, s));
+    const unsigned grid = (unsigned)std::max<int64_t>(1, grid_for(P->neblocks, 128));
+    if (dtype == BLS_F64)
+      k_qr_reduce_rhs<double><<<grid, 128, 0, s>>>(P->neblocks, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(),
+                                                  P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->r_dims.as<int32_t>(),
+                                                  P->boff_r.as<int32_t>(), P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), P->nr,
+                                                  (const double*)F, d, w, d_r);
+    else if (dtype == BLS_F32)
+      k_qr_reduce_rhs<float><<<grid, 128, 0, s>>>(P->neblocks, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(),
+                                                 P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->r_dims.as<int32_t>(),
+                                                 P->boff_r.as<int32_t>(), P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), P->nr,
+                                                 (const float*)F, d, w, d_r);
+    else
+      throw Error(BLS_EINVAL, "unknown dtype");
+    P->launches += 1;
+    BLS_CUDA(cudaGetLastError());
+    return BLS_OK;
+  })
+}
+
+int bls_qr_backsubstitute_rhs(bls_qr_plan* P, int dtype, const void* F, const double* w, const double* x_r, double* x_e) {
+  QR_GUARD({
+    if (!P || !F || !w || !x_r || !x_e) throw Error(BLS_EINVAL, "a device pointer is NULL");
+    cudaStream_t s = P->ctx->stream;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, grid_for(P->neblocks, 128));
+    if (dtype == BLS_F64)
+      k_qr_backsub<double><<<grid, 128, 0, s>>>(P->neblocks, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(),
+                                               P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(),
+                                               P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(),
+                                               (const double*)F, nullptr, x_r, x_e, w);
+    else if (dtype == BLS_F32)
+      k_qr_backsub<float><<<grid, 128, 0, s>>>(P->neblocks, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(),
+                                              P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(),
+                                              P->r_dims.as<int32_t>(), P->boff_r.as<int32_t>(), P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(),
+                                              (const float*)F, nullptr, x_r, x_e, w);
+    else
+      throw Error(BLS_EINVAL, "unknown dtype");
+    P->launches += 1;
+    BLS_CUDA(cudaGetLastError());
+    return BLS_OK;
+  })
 }
 
 int bls_qr_plan_set_staging(bls_qr_plan* plan, int bulk) {

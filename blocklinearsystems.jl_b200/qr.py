@@ -457,3 +457,58 @@ def lsmr_reduced(x_r: torch.Tensor, ws: QRReductionWorkspace, lam: float, s_r: t
     if rc not in (BLS_NOT_PD, BLS_NOT_CONVERGED):
         check(rc)
     return LsmrResult(rc == 0, int(it.value), int(ist.value), *[float(v) for v in stats])
+
+
+@dataclass
+class RefineResult:
+    """Outcome of qr_refine: steps taken (the first is the plain reduced solve), ||d|| / ||J'r|| after each step (d the
+    FP64 normal-equation residual of the damped problem), and whether the last one is within the tolerance."""
+    steps: int
+    rel_residuals: list
+    converged: bool
+
+
+def qr_refine(x: torch.Tensor, ws: QRReductionWorkspace, J: SchurBlockJacobian, scaling_r: torch.Tensor, scaling_e: torch.Tensor,
+              lam: float, solve_reduced, *, tol: float = 1e-12, maxit: int = 5) -> RefineResult:
+    """Iterative refinement of the QR route (no reference counterpart: the reference solves the reduced system once,
+    src/qr_linear_systems.jl:250-300). x = [x_r; x_e] (float64, nr + ne) solves the damped least-squares problem
+    min ||J x - r||^2 + lam x' diag([scaling_r; scaling_e]) x of the raw tables J to `tol` in the normal equations:
+    each step forms d = J'(r - J x) - lam scaling .* x in FP64 from the raw tables, reduces it through the factored
+    tables of the last reduce_qr(ws, J, scaling_e, lam) (U' w = d_e, d_r -= B' w), solves the reduced system with
+    `solve_reduced(d_r) -> dx_r` (e.g. DenseCholesky.solve after factor(J~'J~, lam, scaling_r)), back-substitutes
+    dx_e = U^-1 (w - B dx_r) and adds dx. The first step from x = 0 is the plain QR-route solve; with FP32 tables the
+    following steps recover what FP32 lost, the residual being FP64. Unconditioned tables only (reduce_qr with s = None)."""
+    st = ws.structure.schur
+    nr, ne = st.nr, st.ne
+    if J.data.dtype != ws.dtype:
+        raise ArgumentError(f"J must be {ws.dtype}")
+    _dev(x, "x", nr + ne, torch.float64)
+    _dev(scaling_r, "scaling_r", nr, torch.float64)
+    _dev(scaling_e, "scaling_e", ne, torch.float64)
+    dev = x.device
+    sc = torch.cat([scaling_r, scaling_e])
+    y = torch.empty(ws.structure.residual_length, dtype=torch.float64, device=dev)
+    d = torch.empty(nr + ne, dtype=torch.float64, device=dev)
+    w = torch.empty(max(ne, 1), dtype=torch.float64, device=dev)
+    d_r = torch.empty(nr, dtype=torch.float64, device=dev)
+    dx_e = torch.empty(max(ne, 1), dtype=torch.float64, device=dev)
+    L = _lib.gpu()
+    h, T = ws.handle, ws._T
+    x.zero_()
+    rels = []
+    bnorm = None
+    for k in range(maxit + 1):
+        check(L.bls_qr_normal_residual(h, T, dptr(J.data), dptr(J.r), dptr(sc), float(lam), dptr(x), dptr(y), dptr(d)))
+        dn = float(torch.linalg.vector_norm(d))
+        if bnorm is None:
+            bnorm = max(dn, 1e-300)     # x = 0: d = J'r
+        else:
+            rels.append(dn / bnorm)
+            if rels[-1] <= tol or k == maxit:
+                break
+        check(L.bls_qr_reduce_rhs(h, T, dptr(ws.factored), dptr(d), dptr(w), dptr(d_r)))
+        dx_r = solve_reduced(d_r)
+        check(L.bls_qr_backsubstitute_rhs(h, T, dptr(ws.factored), dptr(w), dptr(dx_r), dptr(dx_e)))
+        x[:nr] += dx_r
+        x[nr:] += dx_e[:ne]
+    return RefineResult(len(rels), rels, bool(rels) and rels[-1] <= tol)

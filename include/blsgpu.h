@@ -320,6 +320,22 @@ typedef struct bls_qr_plan_desc {
 
 int bls_qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* desc, bls_qr_plan** out);
 int bls_qr_plan_destroy(bls_qr_plan* plan);
+/* No counterpart in the reference (iterative refinement of the QR route, the reduced solve being mixed precision; the
+ * reference solves once, src/qr_linear_systems.jl:250-300). The steps of one refinement step x += dx of the damped
+ * least-squares problem min ||J x - r||^2 + lambda x' diag(scaling) x, x = [x_r; x_e] (nr + ne, FP64):
+ *  - bls_qr_normal_residual: d = J' (r - J x) - lambda scaling .* x in FP64 from the RAW tables J (raw_offsets layout,
+ *    storage type `dtype`; the damping rows of the eliminated tables are ignored, their damping is the lambda term) and
+ *    the raw residual r; y (residual_length doubles) receives r - J x per row;
+ *  - bls_qr_reduce_rhs: from the FACTORED tables F of the last reduce_qr, per eliminated block w = U^-T d_e (ne
+ *    doubles) and d_r = d[0:nr] - sum B' w, so that (J~'J~ + lambda diag(scaling_r)) dx_r = d_r;
+ *  - bls_qr_backsubstitute_rhs: dx_e = U^-1 (w - B dx_r).
+ * The reduced solve between the last two is the caller's (bls_dense_cholesky_shifted + bls_dense_cholesky_solve, or a
+ * PCG on the sparse J~'J~). */
+int bls_qr_normal_residual(bls_qr_plan* plan, int dtype, const void* J_dev, const double* r_dev, const double* scaling_dev,
+                           double lambda, const double* x_dev, double* y_dev, double* d_dev);
+int bls_qr_reduce_rhs(bls_qr_plan* plan, int dtype, const void* F_dev, const double* d_dev, double* w_dev, double* d_r_dev);
+int bls_qr_backsubstitute_rhs(bls_qr_plan* plan, int dtype, const void* F_dev, const double* w_dev, const double* x_r_dev,
+                              double* x_e_dev);
 /* No counterpart in the reference (a staging choice of this build): how the table kernels (reduce_qr, the Gram kernels
  * of reduced_normal_*, reduced_diagonal_blocks and bls_assemble_hessian) bring each table into shared memory. bulk != 0
  * (the default): one bulk (TMA) copy per contiguous span, completed on an mbarrier; 0: element-wise asynchronous copies.
