@@ -74,6 +74,7 @@ struct SchurPlan {
   bool stage_ok = false;
   int stage_unit = 8;
   int64_t stage_items = 0, stage_max_nv = 0, stage_units = 0;
+  int stage_grid[2] = {0, 0};   // persistent CTAs of k_stage36 (FP32, FP64): resident blocks per SM x SMs
   DevBuf stg_items, stg_thr, stg_units, stg_pairs;
   DevBuf EZ;   // per point E' = s_e E^-1 s_e (9, column-major) and z' = s_e .* z (3), FP64, for k_stage36
   // a batch of independent problems in one plan (bls_schur_plan_set_problems): per problem the lowest failing point
@@ -272,6 +273,7 @@ __global__ void __launch_bounds__(256) k_reset_dense_columns(T* __restrict__ S, 
 __global__ void k_arm36(Status* st) {
   st->einval_e = NONE;
   if (st->einval_r == NONE) st->failed = NONE;
+  st->pad = 0;   // the work queue of k_stage36
 }
 
 template <class T>
@@ -1503,16 +1505,27 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
     const int32_t* __restrict__ rentry, const int32_t* __restrict__ entry_elim, const int32_t* __restrict__ eptr,
     const int32_t* __restrict__ col_h, const int64_t* __restrict__ col_base, int64_t ncoup, const T* __restrict__ C,
     const double* __restrict__ EZ, const double* __restrict__ s_r, T* __restrict__ S, double* __restrict__ g, const Status* __restrict__ st,
-    const int32_t* __restrict__ prob_of_cam, const long long* __restrict__ prob_fail) {
+    const int32_t* __restrict__ prob_of_cam, const long long* __restrict__ prob_fail, int64_t nitems,
+    unsigned long long* __restrict__ queue) {
   constexpr int NT = SchurPlan::STAGE_NT;
   constexpr int WR = stage_wr<T>();
   extern __shared__ __align__(16) unsigned char sm[];
+  __shared__ int s_item;
   if (!live(st)) return;
-  const int4 it = items[blockIdx.x];
-  const int r2 = it.x, q0 = it.y, nv = it.z, nseg = it.w;
-  if (prob_fail && prob_fail[prob_of_cam[r2]] != NONE) return;   // the column's problem failed: its S stays reset
-  const int H = __ldg(col_h + r2);
   const int tid = threadIdx.x;
+  // persistent: each CTA takes the next item (largest first) from the queue until none is left
+  for (;;) {
+  if (tid == 0) s_item = (int)atomicAdd(queue, 1ull);
+  __syncthreads();
+  const int item = s_item;
+  if (item >= nitems) break;
+  const int4 it = items[item];
+  const int r2 = it.x, q0 = it.y, nv = it.z, nseg = it.w;
+  if (prob_fail && prob_fail[prob_of_cam[r2]] != NONE) {   // the column's problem failed: its S stays reset
+    __syncthreads();
+    continue;
+  }
+  const int H = __ldg(col_h + r2);
   T* tile = reinterpret_cast<T*>(sm);
   T* W = reinterpret_cast<T*>(sm + (((size_t)6 * H * sizeof(T) + 15) & ~size_t(15)));
   int* p0s = reinterpret_cast<int*>(W + (size_t)nv * WR);
@@ -1543,7 +1556,7 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
   }
   __syncthreads();
   // 2. the thread's units
-  const int* tp = thr + (int64_t)blockIdx.x * (NT + 1);
+  const int* tp = thr + (int64_t)item * (NT + 1);
   const int ub = __ldg(tp + tid), ue = __ldg(tp + tid + 1);
   double fc[6];
 #pragma unroll
@@ -1615,6 +1628,8 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
     double x = 0.0;
     for (int w = 0; w < NT / 32; ++w) x += gp[6 * w + tid];
     atomicAdd(g + 6 * r2 + tid, -(s_r ? s_r[6 * r2 + tid] : 1.0) * x);
+  }
+  __syncthreads();   // the item's shared memory is free for the next one
   }
 }
 
@@ -1743,6 +1758,27 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int6
     std::vector<int4>().swap(o.units);
     std::vector<int32_t>().swap(o.thr);
     std::vector<uint32_t>().swap(o.pairs);
+  }
+  // items largest first: the kernel's CTAs take items from a queue in this order, so the long ones start early and the
+  // short ones fill the tail (work ~ pairs plus the staging of the visits)
+  {
+    std::vector<int64_t> work(nitems, 0);
+    for (int64_t i = 0; i < nitems; ++i) {
+      const int32_t u0 = thr[i * (NT + 1)], u1 = thr[i * (NT + 1) + NT];
+      for (int32_t u = u0; u < u1; ++u) work[i] += units[u].y;
+      work[i] += 2 * (int64_t)items[i].z;
+    }
+    std::vector<int64_t> order(nitems);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return work[a] > work[b]; });
+    std::vector<int4> items2(nitems);
+    std::vector<int32_t> thr2((size_t)nitems * (NT + 1));
+    for (int64_t i = 0; i < nitems; ++i) {
+      items2[i] = items[order[i]];
+      std::copy(thr.begin() + order[i] * (NT + 1), thr.begin() + (order[i] + 1) * (NT + 1), thr2.begin() + i * (NT + 1));
+    }
+    items.swap(items2);
+    thr.swap(thr2);
   }
   upload(P->stg_items, items, s);
   upload(P->stg_thr, thr, s);
@@ -2327,10 +2363,19 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
       BLS_CUDA(cudaFuncSetAttribute(k_stage36<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
       P->launches += 1;
-      k_stage36<T><<<(unsigned)P->stage_items, SchurPlan::STAGE_NT, smem, s>>>(
+      if (P->stage_grid[sizeof(T) == 4 ? 0 : 1] == 0) {
+        int per_sm = 0, nsm = 0, dev = 0;
+        BLS_CUDA(cudaGetDevice(&dev));
+        BLS_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        BLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage36<T>, SchurPlan::STAGE_NT, smem));
+        P->stage_grid[sizeof(T) == 4 ? 0 : 1] = std::max(1, per_sm) * nsm;
+      }
+      const int64_t grid = std::min<int64_t>(P->stage_items, P->stage_grid[sizeof(T) == 4 ? 0 : 1]);
+      k_stage36<T><<<(unsigned)grid, SchurPlan::STAGE_NT, smem, s>>>(
           P->stg_items.as<int4>(), P->stg_thr.as<int32_t>(), P->stg_units.as<int4>(), P->stg_pairs.as<uint32_t>(),
           P->retained_entry.as<int32_t>(), P->entry_eliminated.as<int32_t>(), P->eliminated_ptr.as<int32_t>(), P->col_h.as<int32_t>(),
-          P->col_base.as<int64_t>(), P->ncoup, C, P->EZ.as<double>(), s_r, S, g, st, poc, pf);
+          P->col_base.as<int64_t>(), P->ncoup, C, P->EZ.as<double>(), s_r, S, g, st, poc, pf, P->stage_items,
+          reinterpret_cast<unsigned long long*>(&st->pad));
       if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
     }
   } else if (P->fast36 && !batch && P->kernel == 0) {
