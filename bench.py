@@ -555,6 +555,21 @@ def run_ours_pcg(args, rank: int, world: int) -> dict | None:
     out["pcg"] = {"seconds_to_1e-8": dev_s, "wall_seconds": statistics.median(t[1] for t in times), "iterations": iters[-1],
                   "rel_residual": rels[-1], "preconditioner": "block-Jacobi (6x6)", "S_storage": "f32 (mixed reduction output)",
                   "residual": "explicit FP64 g - S x"}
+    # the learned block preconditioner (trained by blocklinearsystems.jl_b200/train_gnn.py on the 1k-5k-camera scenes of
+    # this workload's family) against block-Jacobi on this scene: iterations and device seconds to 1e-8, the learned side
+    # including its BF16 inference of the blocks
+    pfile = ROOT / "blocklinearsystems.jl_b200" / "gnn_pcg_params.npy"
+    if pfile.exists():
+        net = bls.gnn.LearnedPreconditioner(pws)
+        assert net.prepare(S)
+        params = torch.from_numpy(np.load(pfile)).to(dev)
+        for _ in range(args.warmup):
+            bls.gnn.pcg_comparison(net, S, g, params)
+        cmp_ = bls.gnn.pcg_comparison(net, S, g, params)
+        if rank == 0:
+            out["pcg"]["learned"] = dict(cmp_, target="learned time <= 0.6 x block-Jacobi",
+                                         params=f"{pfile.name}, trained by train_gnn.py (summary in {pfile.with_suffix('.json').name})")
+        del net
     # the same solve refined against the FP64 reduced operator (R + lambda D - C' E^-1 C applied from the stored blocks
     # and the reduction's FP64 E^-1) to 1e-10: PCG corrections on the FP32 S, outer residual in FP64
     ws = _LAST["ws"]

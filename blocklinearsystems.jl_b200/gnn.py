@@ -144,3 +144,62 @@ def train(systems, params: torch.Tensor | None = None, *, steps: int = 200, lr: 
         if log_every and k % log_every == 0:
             print(f"step {k}: loss {loss:.5f}")
     return params, losses
+
+
+def scene_system(ncams: int, npoints: int, seed: int, *, device: int = 0):
+    """A reduced system of the 1M-point workload's distributions (pcg_10000x1M's generator on `ncams` cameras and
+    `npoints` points: window +-60, k = 2 + Geom(0.15), camera column scales over four decades, lambda 1e-5), produced by
+    the plain mixed Schur path on the device, with its PCG workspace and network graph prepared on the FP32 S.
+    Returns (LearnedPreconditioner, S, g)."""
+    from . import scenes
+    from .reduction import SchurReductionWorkspace, reduce_schur_sparse, reset_schur_sparse
+    spec = scenes.scaled_down(scenes.workload("pcg_10000x1M"), ncams=ncams, npoints=npoints, seed=seed)
+    p = scenes.hessian_problem(spec)
+    st, pat = p.structure, p.pattern
+    dev = torch.device("cuda", device)
+    f = lambda a, t=torch.float32: torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=t)
+    ws = SchurReductionWorkspace(st, pat, device=device)
+    S = torch.zeros(pat.nnz, dtype=torch.float32, device=dev)
+    g = torch.zeros(st.nr, dtype=torch.float64, device=dev)
+    reset_schur_sparse(S, f(p.R), None, None, f(p.scaling_r, torch.float64), p.lam, ws)
+    if not reduce_schur_sparse(S, g, f(p.b_r, torch.float64), f(p.b_e, torch.float64), f(p.scaling_e, torch.float64), p.lam, st, f(p.E),
+                               f(p.C), None, None, None, None, ws):
+        raise ArgumentError(f"the scene's point block {ws.failed_block} is singular")
+    net = LearnedPreconditioner(PCGWorkspace(st, pat, device=device))
+    if not net.prepare(S):
+        raise ArgumentError("a diagonal block of the reduced system is not positive definite")
+    return net, S, g
+
+
+def pcg_comparison(net: LearnedPreconditioner, S: torch.Tensor, g: torch.Tensor, params: torch.Tensor, *, tol: float = 1e-8) -> dict:
+    """Block-Jacobi PCG against PCG with the learned blocks on one prepared system: iterations, device seconds (the
+    learned side including its BF16 inference of the blocks) and the final FP64 residuals."""
+    out = {}
+    for name in ("block_jacobi", "learned"):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        B = net.blocks(params, bf16=True) if name == "learned" else None
+        _, res = net.pcg.solve(S, g, tol=tol, preconditioner=B)
+        b.record()
+        torch.cuda.synchronize()
+        out[name] = {"iterations": res.iterations, "seconds": a.elapsed_time(b) / 1e3, "rel_residual": res.rel_residual,
+                     "converged": res.converged}
+    out["iteration_ratio"] = out["learned"]["iterations"] / max(out["block_jacobi"]["iterations"], 1)
+    out["time_ratio"] = out["learned"]["seconds"] / out["block_jacobi"]["seconds"]
+    return out
+
+
+def train_on_scenes(n_scenes: int = 48, ncams=(1000, 5000), points_per_camera: int = 100, *, steps: int = 600, lr: float = 2e-3,
+                    probes: int = 4, seed: int = 0, device: int = 0, log_every: int = 0):
+    """Train the network on `n_scenes` seeded scenes of the 1M-point workload's family with camera counts drawn
+    uniformly from `ncams` (points_per_camera points per camera, as the 1M-point scene has), their reduced systems
+    from the plain Schur path (scene_system). Returns (params, losses, systems)."""
+    rng = np.random.default_rng(seed)
+    systems = []
+    for i in range(n_scenes):
+        nc = int(rng.integers(ncams[0], ncams[1] + 1))
+        net, _, _ = scene_system(nc, points_per_camera * nc, seed=70_000 + 97 * seed + i, device=device)
+        systems.append(net)
+    params, losses = train(systems, None, steps=steps, lr=lr, probes=probes, seed=seed, log_every=log_every)
+    return params, losses, systems
