@@ -1454,36 +1454,74 @@ static size_t stage_smem(int64_t max_h, int64_t max_nv) {
   return tile + w + p0 + (SchurPlan::STAGE_NT / 32) * 6 * sizeof(double);
 }
 
-// 18 entries of one coupling block of C (72 bytes FP32 at an 8-byte boundary, 144 bytes FP64 at a 16-byte boundary;
-// C itself on a 16-byte boundary)
-__device__ __forceinline__ void load_block18(const float* __restrict__ C, int64_t c, int64_t ncoup, float* a) {
-  const float* src = C + 18 * c;
-  if (c & 1) {
-    // 8 bytes past a 16-byte boundary: five 16-byte loads from the boundary below, entries 2..19
-    const float4* q = reinterpret_cast<const float4*>(src - 2);
-    float w[20];
-#pragma unroll
-    for (int i = 0; i < 5; ++i) { float4 v = __ldg(q + i); w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w; }
-#pragma unroll
-    for (int i = 0; i < 18; ++i) a[i] = w[i + 2];
-  } else if (c + 1 < ncoup) {
-    // on a 16-byte boundary: five 16-byte loads (the last reaches 8 bytes into the next block)
-    const float4* q = reinterpret_cast<const float4*>(src);
-    float w[20];
-#pragma unroll
-    for (int i = 0; i < 5; ++i) { float4 v = __ldg(q + i); w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w; }
-#pragma unroll
-    for (int i = 0; i < 18; ++i) a[i] = w[i];
+// 18 entries of one coupling block of C, read with 32-byte loads from the 32-byte boundary at or below the block (C on
+// a 32-byte boundary): FP32 blocks (72 bytes at 18 c floats) start 0, 2, 4 or 6 floats past a boundary and lie in the
+// three 32-byte chunks from it; FP64 blocks (144 bytes) start 0 or 2 doubles past one and lie in five. The last block
+// of C takes 8-byte loads instead, so that nothing past C's end is read.
+__device__ __forceinline__ void ld256(const float* p, float* w) {
+  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(w[0]), "=f"(w[1]), "=f"(w[2]), "=f"(w[3]), "=f"(w[4]), "=f"(w[5]), "=f"(w[6]), "=f"(w[7]) : "l"(p));
+}
+__device__ __forceinline__ void ld256(const double* p, double* w) {
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(w[0]), "=d"(w[1]), "=d"(w[2]), "=d"(w[3]) : "l"(p));
+}
+// The raw chunks of block c (24 floats / 20 doubles) and its shift within them.
+struct Raw32 { float w[24]; int sh; };
+struct Raw64 { double w[20]; int sh; };
+__device__ __forceinline__ void load_raw(const float* __restrict__ C, int64_t c, int64_t ncoup, Raw32& r) {
+  const int64_t f = 18 * c;
+  r.sh = (int)(f & 7);
+  if (c + 1 < ncoup || r.sh == 6) {
+    const float* q = C + (f - r.sh);
+    ld256(q, r.w);
+    ld256(q + 8, r.w + 8);
+    ld256(q + 16, r.w + 16);
   } else {
-    const float2* q = reinterpret_cast<const float2*>(src);
+    const float2* q = reinterpret_cast<const float2*>(C + f);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) { float2 v = __ldg(q + i); a[2 * i] = v.x; a[2 * i + 1] = v.y; }
+    for (int i = 0; i < 9; ++i) { float2 v = __ldg(q + i); r.w[2 * i] = v.x; r.w[2 * i + 1] = v.y; }
+    r.sh = 0;
   }
 }
-__device__ __forceinline__ void load_block18(const double* __restrict__ C, int64_t c, int64_t, double* a) {
-  const double2* q = reinterpret_cast<const double2*>(C + 18 * c);
+__device__ __forceinline__ void load_raw(const double* __restrict__ C, int64_t c, int64_t ncoup, Raw64& r) {
+  const int64_t f = 18 * c;
+  r.sh = (int)(f & 3);   // 0 or 2
+  if (c + 1 < ncoup || r.sh == 2) {
+    const double* q = C + (f - r.sh);
 #pragma unroll
-  for (int i = 0; i < 9; ++i) { double2 v = __ldg(q + i); a[2 * i] = v.x; a[2 * i + 1] = v.y; }
+    for (int i = 0; i < 5; ++i) ld256(q + 4 * i, r.w + 4 * i);
+  } else {
+    const double2* q = reinterpret_cast<const double2*>(C + f);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { double2 v = __ldg(q + i); r.w[2 * i] = v.x; r.w[2 * i + 1] = v.y; }
+    r.sh = 0;
+  }
+}
+// the block's 18 entries from its raw chunks (two selects per entry for FP32, one for FP64)
+__device__ __forceinline__ void take18(const Raw32& r, float* a) {
+  float t[20];
+  const bool b4 = (r.sh & 4) != 0, b2 = (r.sh & 2) != 0;
+#pragma unroll
+  for (int i = 0; i < 20; ++i) t[i] = b4 ? r.w[i + 4] : r.w[i];
+#pragma unroll
+  for (int i = 0; i < 18; ++i) a[i] = b2 ? t[i + 2] : t[i];
+}
+__device__ __forceinline__ void take18(const Raw64& r, double* a) {
+  const bool b2 = r.sh != 0;
+#pragma unroll
+  for (int i = 0; i < 18; ++i) a[i] = b2 ? r.w[i + 2] : r.w[i];
+}
+template <class T> struct RawOf { using type = Raw32; };
+template <> struct RawOf<double> { using type = Raw64; };
+__device__ __forceinline__ void load_block18(const float* __restrict__ C, int64_t c, int64_t ncoup, float* a) {
+  Raw32 r;
+  load_raw(C, c, ncoup, r);
+  take18(r, a);
+}
+__device__ __forceinline__ void load_block18(const double* __restrict__ C, int64_t c, int64_t ncoup, double* a) {
+  Raw64 r;
+  load_raw(C, c, ncoup, r);
+  take18(r, a);
 }
 __device__ __forceinline__ void load_w18(const float* w, float* b) {
   const float4* q = reinterpret_cast<const float4*>(w);
@@ -1502,18 +1540,18 @@ __device__ __forceinline__ void load_w18(const double* w, double* b) {
 template <class T>
 __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k_stage36(
     const int4* __restrict__ items, const int32_t* __restrict__ thr, const int4* __restrict__ units, const uint32_t* __restrict__ pairs,
-    const int32_t* __restrict__ rentry, const int32_t* __restrict__ entry_elim, const int32_t* __restrict__ eptr,
-    const int32_t* __restrict__ col_h, const int64_t* __restrict__ col_base, int64_t ncoup, const T* __restrict__ C,
-    const double* __restrict__ EZ, const double* __restrict__ s_r, T* __restrict__ S, double* __restrict__ g, const Status* __restrict__ st,
-    const int32_t* __restrict__ prob_of_cam, const long long* __restrict__ prob_fail, int64_t nitems,
+    const int2* __restrict__ vis_rec, const int32_t* __restrict__ col_h, const int64_t* __restrict__ col_base, int64_t ncoup,
+    const T* __restrict__ C, const double* __restrict__ EZ, const double* __restrict__ s_r, T* __restrict__ S, double* __restrict__ g,
+    const Status* __restrict__ st, const int32_t* __restrict__ prob_of_cam, const long long* __restrict__ prob_fail, int64_t nitems,
     unsigned long long* __restrict__ queue) {
   constexpr int NT = SchurPlan::STAGE_NT;
   constexpr int WR = stage_wr<T>();
+  using Raw = typename RawOf<T>::type;
   extern __shared__ __align__(16) unsigned char sm[];
   __shared__ int s_item;
   if (!live(st)) return;
   const int tid = threadIdx.x;
-  // persistent: each CTA takes the next item (largest first) from the queue until none is left
+  // persistent: each CTA takes the next item (in column order) from the queue until none is left
   for (;;) {
   if (tid == 0) s_item = (int)atomicAdd(queue, 1ull);
   __syncthreads();
@@ -1531,14 +1569,14 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
   int* p0s = reinterpret_cast<int*>(W + (size_t)nv * WR);
   double* gp = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(p0s) + (((size_t)nv * 4 + 15) & ~size_t(15)));
   for (int i = tid; i < 6 * H; i += NT) tile[i] = T(0);
-  // 1. W and the gradient sums, a thread per visit
+  // 1. W and the gradient sums, a thread per visit ({first coupling, point | index of c2 << 24} per visit)
   double ga[6];
 #pragma unroll
   for (int w = 0; w < 6; ++w) ga[w] = 0.0;
   for (int v = tid; v < nv; v += NT) {
-    const int c2 = __ldg(rentry + q0 + v);
-    const int e = __ldg(entry_elim + c2);
-    p0s[v] = __ldg(eptr + e);
+    const int2 vr = __ldg(vis_rec + q0 + v);
+    const int e = vr.y & 0xffffff, c2 = vr.x + (int)((unsigned)vr.y >> 24);
+    p0s[v] = vr.x;
     const double2* ez = reinterpret_cast<const double2*>(EZ + 12 * (int64_t)e);
     double Ep[12];
 #pragma unroll
@@ -1555,31 +1593,42 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
     }
   }
   __syncthreads();
-  // 2. the thread's units
+  // 2. the thread's units: its pair stream is units[ub].x .. (contiguous, 16-byte aligned), read four pairs at a time
   const int* tp = thr + (int64_t)item * (NT + 1);
   const int ub = __ldg(tp + tid), ue = __ldg(tp + tid + 1);
   double fc[6];
 #pragma unroll
   for (int w = 0; w < 6; ++w) fc[w] = s_r ? s_r[6 * r2 + w] : 1.0;
-  for (int u = ub; u < ue; ++u) {
-    const int4 un = __ldg(units + u);
-    const int pb = un.x, pe = un.x + un.y, row = un.z;
-    const bool diag = un.w < 0;
-    const int r1 = un.w & 0x7fffffff;
+  if (ub < ue) {
+    const uint4* q4 = reinterpret_cast<const uint4*>(pairs);
+    int4 un = __ldg(units + ub);
+    int u = ub, left = un.y;
+    int p = un.x;                       // stream position (a multiple of 4 at the first unit)
+    uint4 qa = __ldg(q4 + (p >> 2)), qb = __ldg(q4 + (p >> 2) + 1);
+    auto code = [&](int pos) -> uint32_t {   // the pair code at stream position pos (within the buffered 8)
+      const int o = pos - (p & ~3);
+      const uint4& q = o < 4 ? qa : qb;
+      const int k = o & 3;
+      return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;
+    };
+    Raw raw;
+    {
+      const uint32_t pr = code(p);
+      load_raw(C, p0s[pr & 0xffff] + (int)(pr >> 16), ncoup, raw);
+    }
     T acc[36];
 #pragma unroll
     for (int i = 0; i < 36; ++i) acc[i] = T(0);
-    uint32_t pr = __ldg(pairs + pb);
-    T a[18];
-    load_block18(C, p0s[pr & 0xffff] + (int)(pr >> 16), ncoup, a);
-    for (int p = pb; p < pe; ++p) {
-      const int v = pr & 0xffff;
-      T b[18];
-      load_w18(W + (size_t)v * WR, b);
-      T an[18];
-      if (p + 1 < pe) {   // the next pair's coupling block, in flight during this pair's products
-        pr = __ldg(pairs + p + 1);
-        load_block18(C, p0s[pr & 0xffff] + (int)(pr >> 16), ncoup, an);
+    for (;;) {
+      const uint32_t pr = code(p);
+      T a[18], b[18];
+      take18(raw, a);
+      load_w18(W + (size_t)(pr & 0xffff) * WR, b);
+      // the next pair's block, in flight during this pair's products (the next unit's first pair when this one ends)
+      const bool more = left > 1 || u + 1 < ue;
+      if (more) {
+        const uint32_t pn = code(p + 1);
+        load_raw(C, p0s[pn & 0xffff] + (int)(pn >> 16), ncoup, raw);
       }
 #pragma unroll
       for (int rho = 0; rho < 6; ++rho)
@@ -1591,20 +1640,30 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
           x = fma(a[3 * rho + 2], b[3 * w + 2], x);
           acc[6 * rho + w] = x;
         }
-      if (p + 1 < pe) {
-#pragma unroll
-        for (int i = 0; i < 18; ++i) a[i] = an[i];
+      ++p;
+      if ((p & 3) == 0) {               // next quad: the buffered second quad, and read one more ahead
+        qa = qb;
+        qb = __ldg(q4 + (p >> 2) + 1);
       }
-    }
+      if (--left == 0) {
+        const bool diag = un.w < 0;
+        const int r1 = un.w & 0x7fffffff, row = un.z;
 #pragma unroll
-    for (int rho = 0; rho < 6; ++rho) {
-      const double fr = s_r ? s_r[6 * r1 + rho] : 1.0;
+        for (int rho = 0; rho < 6; ++rho) {
+          const double fr = s_r ? s_r[6 * r1 + rho] : 1.0;
 #pragma unroll
-      for (int w = 0; w < 6; ++w) {
-        if (diag && rho > w) continue;
-        T val = acc[6 * rho + w];
-        if (s_r) val = T((double)val * (fr * fc[w]));
-        atomicAdd(tile + w * H + row + rho, val);
+          for (int w = 0; w < 6; ++w) {
+            if (diag && rho > w) continue;
+            T val = acc[6 * rho + w];
+            if (s_r) val = T((double)val * (fr * fc[w]));
+            atomicAdd(tile + w * H + row + rho, val);
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 36; ++i) acc[i] = T(0);
+        if (++u == ue) break;
+        un = __ldg(units + u);
+        left = un.y;
       }
     }
   }
@@ -1637,22 +1696,26 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
 // column grouped by block slot, each block's in visit order). An item is a run of one block column's visits: its
 // shared memory holds the column's S tile (6 H entries) and per visit W = E' C_c2 (18 entries) and the visit point's
 // first coupling; in FP64 this must fit STAGE_BUDGET bytes, so a column with more visits is cut into several items
-// (their tiles are added to S with atomics). A block's pairs of one item are cut into units of at most stage_unit
-// pairs, and the units are spread over the item's STAGE_NT threads largest first, each to the least loaded thread.
+// (their tiles are added to S with atomics). Items stay in column order: neighbouring columns read the couplings of
+// overlapping sets of points, which then stay in L2 while the columns in flight move along the cameras.
+// A block's pairs of one item are cut into units of at most stage_unit pairs, spread over the item's STAGE_NT threads
+// largest first, each to the least loaded; the k-th assignment goes to warp k mod (NT / 32), so that the units of one
+// block (assigned one after the other) flush from different warps. A thread's units and their pairs are stored one
+// after the other (its pair stream, padded to a multiple of four pairs so that it is read 16 bytes at a time).
 static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int64_t nc, const std::vector<int32_t>& rptr,
                                  const std::vector<int32_t>& rentry, const std::vector<int32_t>& entry_elim, const int64_t* eptr,
                                  const std::vector<int64_t>& bcolptr, const std::vector<int64_t>& browval,
                                  const std::vector<int64_t>& brow_off, const std::vector<int64_t>& col_h,
                                  const std::vector<int32_t>& pair_c1, const std::vector<int32_t>& pair_c2,
                                  const std::vector<int64_t>& colstart, const std::vector<std::vector<int32_t>>& col_cnt) {
-  constexpr int NT = SchurPlan::STAGE_NT;
+  constexpr int NT = SchurPlan::STAGE_NT, NW = NT / 32;
   constexpr int64_t STAGE_BUDGET = 200 * 1024;
   const int U = P->stage_unit;
   std::vector<int32_t> pos_of(nc);
   for (int64_t q = 0; q < nc; ++q) pos_of[rentry[q]] = (int32_t)q;
   struct ColOut {
-    std::vector<int4> items, units;
-    std::vector<int32_t> thr;
+    std::vector<int4> items, units;   // units: pair start relative to the column's `pairs`
+    std::vector<int32_t> thr;         // per item NT + 1 unit offsets relative to the column's `units`
     std::vector<uint32_t> pairs;
   };
   std::vector<ColOut> out(nrb);
@@ -1670,14 +1733,12 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int6
     const int64_t nseg = (nv + vcap - 1) / vcap;
     std::vector<int64_t> bnd(nseg + 1);
     for (int64_t g = 0; g <= nseg; ++g) bnd[g] = g * nv / nseg;
-    // units per item: {block slot, first pair index in `pr`, count}
-    struct Unit { int32_t k, first, n; };
+    struct Unit { int32_t k; std::vector<uint32_t> pr; };
     std::vector<std::vector<Unit>> seg_units(nseg);
-    std::vector<uint32_t> pr;
     const auto& cnt = col_cnt[r2];
     for (int64_t sl = 0; sl + 1 < (int64_t)cnt.size(); ++sl) {
       const int64_t a = colstart[r2] + cnt[sl], b = colstart[r2] + cnt[sl + 1];
-      int64_t cur_seg = -1, run_first = 0, run_n = 0;
+      int64_t cur = -1;
       for (int64_t x = a; x < b; ++x) {
         const int32_t c1 = pair_c1[x], c2 = pair_c2[x];
         const int64_t q = pos_of[c2] - rptr[r2];
@@ -1686,50 +1747,45 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int6
         while (g > 0 && bnd[g] > q) --g;
         const int64_t v = q - bnd[g], i1 = c1 - eptr[entry_elim[c2]];
         if (v > 65535 || i1 < 0 || i1 > 65535) bad = 1;
-        if (g != cur_seg || run_n == U) {
-          if (run_n) seg_units[cur_seg].push_back({(int32_t)(bcolptr[r2] + sl), (int32_t)run_first, (int32_t)run_n});
-          cur_seg = g;
-          run_first = (int64_t)pr.size();
-          run_n = 0;
+        if (g != cur || (int)seg_units[g].back().pr.size() == U) {
+          seg_units[g].push_back({(int32_t)(bcolptr[r2] + sl), {}});
+          cur = g;
         }
-        pr.push_back((uint32_t)v | ((uint32_t)i1 << 16));
-        ++run_n;
+        seg_units[g].back().pr.push_back((uint32_t)v | ((uint32_t)i1 << 16));
       }
-      if (run_n) seg_units[cur_seg].push_back({(int32_t)(bcolptr[r2] + sl), (int32_t)run_first, (int32_t)run_n});
     }
     ColOut& o = out[r2];
     for (int64_t g = 0; g < nseg; ++g) {
       auto& us = seg_units[g];
-      // largest first, each to the least loaded thread
-      std::stable_sort(us.begin(), us.end(), [](const Unit& x, const Unit& y) { return x.n > y.n; });
-      std::vector<int32_t> owner(us.size());
+      std::stable_sort(us.begin(), us.end(), [](const Unit& x, const Unit& y) { return x.pr.size() > y.pr.size(); });
+      // largest first, each to the least loaded slot; slot k is thread (k mod NW) * 32 + k / NW
+      std::vector<std::vector<int32_t>> mine(NT);
       std::vector<std::pair<int64_t, int>> heap;
       for (int t = 0; t < NT; ++t) heap.push_back({0, t});
       auto cmp = [](const std::pair<int64_t, int>& x, const std::pair<int64_t, int>& y) { return x > y; };
       std::make_heap(heap.begin(), heap.end(), cmp);
       for (size_t i = 0; i < us.size(); ++i) {
         std::pop_heap(heap.begin(), heap.end(), cmp);
-        owner[i] = heap.back().second;
-        heap.back().first += us[i].n;
+        const int slot = heap.back().second;
+        mine[(slot % NW) * 32 + slot / NW].push_back((int32_t)i);
+        heap.back().first += (int64_t)us[i].pr.size();
         std::push_heap(heap.begin(), heap.end(), cmp);
       }
-      std::vector<int32_t> tcount(NT + 1, 0);
-      for (size_t i = 0; i < us.size(); ++i) tcount[owner[i] + 1] += 1;
-      for (int t = 0; t < NT; ++t) tcount[t + 1] += tcount[t];
       const int32_t ubase = (int32_t)o.units.size();
-      o.units.resize(o.units.size() + us.size());
-      std::vector<int32_t> fill(tcount.begin(), tcount.end() - 1);
-      for (size_t i = 0; i < us.size(); ++i) {
-        const Unit& u = us[i];
-        const int32_t k = u.k;
-        const int32_t r1 = (int32_t)browval[k];
-        // pair start relative to the column's `pr` for now (made global when the columns are concatenated)
-        o.units[ubase + fill[owner[i]]++] = make_int4(u.first, u.n, (int32_t)brow_off[k], r1 | (r1 == (int32_t)r2 ? INT32_MIN : 0));
+      for (int t = 0; t < NT; ++t) {
+        o.thr.push_back((int32_t)o.units.size());
+        for (int32_t i : mine[t]) {
+          const Unit& u = us[i];
+          const int32_t r1 = (int32_t)browval[u.k];
+          o.units.push_back(make_int4((int32_t)o.pairs.size(), (int32_t)u.pr.size(), (int32_t)brow_off[u.k],
+                                      r1 | (r1 == (int32_t)r2 ? INT32_MIN : 0)));
+          o.pairs.insert(o.pairs.end(), u.pr.begin(), u.pr.end());
+        }
+        while (o.pairs.size() % 4) o.pairs.push_back(0u);   // the thread's stream padded to 16 bytes
       }
-      for (int t = 0; t <= NT; ++t) o.thr.push_back(ubase + tcount[t]);
+      o.thr.push_back((int32_t)o.units.size());
       o.items.push_back(make_int4((int32_t)r2, (int32_t)(rptr[r2] + bnd[g]), (int32_t)(bnd[g + 1] - bnd[g]), (int32_t)nseg));
     }
-    o.pairs.swap(pr);
   }
   if (bad) return;
   int64_t nitems = 0, nunits = 0, npairs = 0, max_nv = 0;
@@ -1749,7 +1805,7 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int6
   pairs.reserve(npairs);
   for (int64_t r2 = 0; r2 < nrb; ++r2) {
     ColOut& o = out[r2];
-    const int32_t pbase = (int32_t)pairs.size(), ubase = (int32_t)units.size();
+    const int32_t pbase = (int32_t)pairs.size(), ubase = (int32_t)units.size();   // pbase stays a multiple of 4
     for (int4 u : o.units) units.push_back(make_int4(u.x + pbase, u.y, u.z, u.w));
     for (int32_t t : o.thr) thr.push_back(t + ubase);
     items.insert(items.end(), o.items.begin(), o.items.end());
@@ -1759,27 +1815,7 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int6
     std::vector<int32_t>().swap(o.thr);
     std::vector<uint32_t>().swap(o.pairs);
   }
-  // items largest first: the kernel's CTAs take items from a queue in this order, so the long ones start early and the
-  // short ones fill the tail (work ~ pairs plus the staging of the visits)
-  {
-    std::vector<int64_t> work(nitems, 0);
-    for (int64_t i = 0; i < nitems; ++i) {
-      const int32_t u0 = thr[i * (NT + 1)], u1 = thr[i * (NT + 1) + NT];
-      for (int32_t u = u0; u < u1; ++u) work[i] += units[u].y;
-      work[i] += 2 * (int64_t)items[i].z;
-    }
-    std::vector<int64_t> order(nitems);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return work[a] > work[b]; });
-    std::vector<int4> items2(nitems);
-    std::vector<int32_t> thr2((size_t)nitems * (NT + 1));
-    for (int64_t i = 0; i < nitems; ++i) {
-      items2[i] = items[order[i]];
-      std::copy(thr.begin() + order[i] * (NT + 1), thr.begin() + (order[i] + 1) * (NT + 1), thr2.begin() + i * (NT + 1));
-    }
-    items.swap(items2);
-    thr.swap(thr2);
-  }
+  pairs.resize(pairs.size() + 8, 0u);   // the kernel's read-ahead of a stream's next 16 bytes stays inside the array
   upload(P->stg_items, items, s);
   upload(P->stg_thr, thr, s);
   upload(P->stg_units, units, s);
@@ -2324,7 +2360,7 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
   cudaStream_t s = P->ctx->stream;
   Status* st = P->status.as<Status>();
   // the column-owned schedule reads C with 16-byte loads (C_data on a 16-byte boundary, as the device allocators give)
-  const bool c16 = (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+  const bool c16 = (reinterpret_cast<uintptr_t>(C) & 31) == 0;   // 32-byte loads of C
   const bool batch = P->nprob > 0 && !dense;
   const bool use_stage = P->fast36 && (P->kernel == 5 || batch) && !dense && P->stage_ok && c16;
   const int32_t* poc = batch ? P->prob_of_cam.as<int32_t>() : nullptr;
@@ -2373,8 +2409,8 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
       const int64_t grid = std::min<int64_t>(P->stage_items, P->stage_grid[sizeof(T) == 4 ? 0 : 1]);
       k_stage36<T><<<(unsigned)grid, SchurPlan::STAGE_NT, smem, s>>>(
           P->stg_items.as<int4>(), P->stg_thr.as<int32_t>(), P->stg_units.as<int4>(), P->stg_pairs.as<uint32_t>(),
-          P->retained_entry.as<int32_t>(), P->entry_eliminated.as<int32_t>(), P->eliminated_ptr.as<int32_t>(), P->col_h.as<int32_t>(),
-          P->col_base.as<int64_t>(), P->ncoup, C, P->EZ.as<double>(), s_r, S, g, st, poc, pf, P->stage_items,
+          P->vis_rec.as<int2>(), P->col_h.as<int32_t>(), P->col_base.as<int64_t>(), P->ncoup, C, P->EZ.as<double>(), s_r, S, g, st,
+          poc, pf, P->stage_items,
           reinterpret_cast<unsigned long long*>(&st->pad));
       if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
     }

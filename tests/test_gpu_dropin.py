@@ -8,7 +8,8 @@ methods, mirrored over ctypes in dropin_shim.py with the reference's exact posit
     backsubstitute!(x_e, x_r, structure, C_data, ws, s_r, s_e)
 
 on host arrays, as the reference's linear system holds them. The solution must equal a dense FP64 solve of the full
-damped system within 1e-9 (test/schur_problems.jl:20-22), in FP64 and with conditioning scales; a singular point
+damped system: backward error <= 1e-13 and forward error <= 1e-8 (test/schur_problems.jl:20-22 bounds the
+reference's at 1e-9 on better-conditioned fixtures), in FP64 and with conditioning scales; a singular point
 returns false with the lowest failing block (1-based) and leaves S and g_S untouched; bad damping arguments throw
 before anything is written.
 """
@@ -99,7 +100,11 @@ def test_schur_solve_through_the_shim(bls, scaled):
     else:
         y = np.linalg.solve(H, b)
     x = np.concatenate([x_r, x_e])
-    assert np.linalg.norm(x - y) / np.linalg.norm(y) < 1e-9
+    # the point blocks' singular values reach 1e-4 (cond(H) ~ 1e8 with the conditioning scales), so the dense
+    # reference itself is accurate to ~1e-8 only: the backward error is the tight check, the forward error the loose one
+    A, rhs = (s[:, None] * H * s[None, :], s * b) if scaled else (H, b)
+    assert np.linalg.norm(A @ x - rhs) / (np.linalg.norm(A, 2) * np.linalg.norm(x)) < 1e-13
+    assert np.linalg.norm(x - y) / np.linalg.norm(y) < 1e-8
 
 
 def test_shim_failure_and_argument_errors(bls):
