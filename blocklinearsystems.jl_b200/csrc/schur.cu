@@ -72,7 +72,7 @@ struct SchurPlan {
   // the column, r1 | diagonal << 31}; pairs {visit within the item | c1's index within its point << 16}.
   static constexpr int STAGE_NT = 256;
   bool stage_ok = false;
-  int stage_unit = 8;
+  int stage_unit = 16;
   int64_t stage_items = 0, stage_max_nv = 0, stage_units = 0;
   int stage_grid[2] = {0, 0};   // persistent CTAs of k_stage36 (FP32, FP64): resident blocks per SM x SMs
   DevBuf stg_items, stg_thr, stg_units, stg_pairs;
@@ -1698,10 +1698,12 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
 // first coupling; in FP64 this must fit STAGE_BUDGET bytes, so a column with more visits is cut into several items
 // (their tiles are added to S with atomics). Items stay in column order: neighbouring columns read the couplings of
 // overlapping sets of points, which then stay in L2 while the columns in flight move along the cameras.
-// A block's pairs of one item are cut into units of at most stage_unit pairs, spread over the item's STAGE_NT threads
-// largest first, each to the least loaded; the k-th assignment goes to warp k mod (NT / 32), so that the units of one
-// block (assigned one after the other) flush from different warps. A thread's units and their pairs are stored one
-// after the other (its pair stream, padded to a multiple of four pairs so that it is read 16 bytes at a time).
+// A block's pairs of one item are cut into units of at most stage_unit pairs. The item's units, largest first, are dealt
+// out in rounds of STAGE_NT, one per thread: the lanes of a warp then run units of about the same length and add them
+// to the tile at the same time (a warp-wide shared-memory atomic costs the same for one lane as for 32), and the k-th
+// unit of a round goes to warp k mod (NT / 32), so that the units of one block (dealt one after the other) land in
+// different warps. A thread's units and their pairs are stored one after the other (its pair stream, padded to a
+// multiple of four pairs so that it is read 16 bytes at a time).
 static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int64_t nc, const std::vector<int32_t>& rptr,
                                  const std::vector<int32_t>& rentry, const std::vector<int32_t>& entry_elim, const int64_t* eptr,
                                  const std::vector<int64_t>& bcolptr, const std::vector<int64_t>& browval,
@@ -1758,18 +1760,13 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int6
     for (int64_t g = 0; g < nseg; ++g) {
       auto& us = seg_units[g];
       std::stable_sort(us.begin(), us.end(), [](const Unit& x, const Unit& y) { return x.pr.size() > y.pr.size(); });
-      // largest first, each to the least loaded slot; slot k is thread (k mod NW) * 32 + k / NW
+      // in rounds, largest first: round r is units [r NT, (r + 1) NT), one per thread, so that the lanes of a warp run
+      // units of about the same length and add them to the tile together; slot k of a round is thread
+      // (k mod NW) * 32 + k / NW, so that the units of one block (consecutive slots) are in different warps
       std::vector<std::vector<int32_t>> mine(NT);
-      std::vector<std::pair<int64_t, int>> heap;
-      for (int t = 0; t < NT; ++t) heap.push_back({0, t});
-      auto cmp = [](const std::pair<int64_t, int>& x, const std::pair<int64_t, int>& y) { return x > y; };
-      std::make_heap(heap.begin(), heap.end(), cmp);
       for (size_t i = 0; i < us.size(); ++i) {
-        std::pop_heap(heap.begin(), heap.end(), cmp);
-        const int slot = heap.back().second;
+        const int slot = (int)(i % NT);
         mine[(slot % NW) * 32 + slot / NW].push_back((int32_t)i);
-        heap.back().first += (int64_t)us[i].pr.size();
-        std::push_heap(heap.begin(), heap.end(), cmp);
       }
       const int32_t ubase = (int32_t)o.units.size();
       for (int t = 0; t < NT; ++t) {
