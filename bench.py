@@ -190,6 +190,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     p = bls.scenes.hessian_problem(spec)
     st, pat = p.structure, p.pattern
     ws = bls.SchurReductionWorkspace(st, pat, device=dev.index)
+    if args.stage_unit:
+        ws.set_stage_unit(args.stage_unit)
     flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=dev)   # larger than the 126 MB L2
 
     def device_inputs(dt):
@@ -292,6 +294,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         "mixed_over_fp64": value / v64,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": measured_traffic(args.workload, kernel), "kernel": kernel, "kernel_ms": pair_ms,
+                     "stage_unit": args.stage_unit or 16,
                      "algorithmic_bytes": bytes32, "peak_source": "measured" if peaks else "fallback",
                      "flops": algorithmic_flops(p), "achieved_tflops": algorithmic_flops(p) / (pair_ms / 1e3) / 1e12},
         "e2e": {"value": world * nobs * args.steps / (e2e_ms / 1e3), "unit": "obs/s", "h2d_bytes_per_step": h2d,
@@ -851,7 +854,7 @@ def run_ours_batch(args, rank: int, world: int) -> dict | None:
                    "observations": nobs, "nnz_S": int(B.U.nnz), "parallelism": f"replicas x{world}",
                    "l2": "flushed between timed steps (256 MB write)",
                    "step": "one CUDA graph replay: reset_schur_sparse + reduce_schur_sparse of all problems (disjoint-union plan)"},
-        "schedule": {"chosen": B.schedule, "autotune_ms": tunes, "fp64_chosen": min(tunes64, key=tunes64.get), "fp64_autotune_ms": tunes64},
+        "schedule": {"chosen": B.schedule + (f"/{B.stage_unit}" if B.schedule == "stage" else ""), "autotune_ms": tunes, "fp64_chosen": min(tunes64, key=tunes64.get), "fp64_autotune_ms": tunes64},
         "fp64": {"value": world * nobs * args.steps / (ms64 / 1e3), "unit": "obs/s", "ms_per_step": ms64 / args.steps},
         "per_problem_error_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "norm": "||S_mixed - S_fp64|| / ||S_fp64|| per problem"},
         "e2e": {"value": world * nobs * args.steps / (e2e_ms / 1e3), "unit": "obs/s",
@@ -1071,6 +1074,7 @@ def main():
     ap.add_argument("--workload", default="pcg_10000x1M")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stage-unit", type=int, default=None, help="pairs per unit of the column-owned schedule (default 16)")
     ap.add_argument("--write-fixture", default=None, help=argparse.SUPPRESS)   # the reference arm's untimed child
     args = ap.parse_args()
     if args.write_fixture:

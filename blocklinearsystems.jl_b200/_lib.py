@@ -94,6 +94,7 @@ def gpu() -> C.CDLL:
             "bls_schur_query_status": (C.c_int, [vp, p64]),
             "bls_schur_plan_instrument": (C.c_int, [vp, C.c_int]),
             "bls_schur_plan_set_kernel": (C.c_int, [vp, C.c_int]),
+            "bls_schur_plan_set_stage_unit": (C.c_int, [vp, C.c_int]),
             "bls_schur_plan_phase2_kernel": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_char_p, i64]),
             "bls_schur_plan_set_problems": (C.c_int, [vp, i64, p64, p64, p64, p64]),
             "bls_schur_plan_problem_status": (C.c_int, [vp, p64]),

@@ -8,8 +8,8 @@ problem's damping lambda_p is folded into its scalings (lambda_p * scaling, form
 lambda * scaling; the batch runs with lambda = 1), so every problem's result is the one its own call would give.
 Each problem fails on its own (problem_status): a singular point in problem p leaves p's S reset and its g_S as it was,
 and the other problems are reduced, as separate reference calls would. autotune() times the phase-2 schedules that
-keep that (the block-column owned schedule with staged point operands, the block-owned pair lists) and keeps the
-faster; capture() records reset + reduce of the batch as one CUDA graph that step() replays.
+keep that (the block-column owned schedule with staged point operands at several unit sizes, the block-owned pair
+lists) and keeps the fastest; capture() records reset + reduce of the batch as one CUDA graph that step() replays.
 """
 from __future__ import annotations
 
@@ -124,18 +124,23 @@ class BatchedReduction:
         self.nobs = int(sum(p.nobs for p in problems))
         self.graph = None
         self.schedule = "pairs"
+        self.stage_unit = 16
 
     def run(self, sync: bool = True) -> bool:
         reset_schur_sparse(self.S, self.R, None, None, self.sc_r, 1.0, self.ws)
         return reduce_schur_sparse(self.S, self.g, self.b_r, self.b_e, self.sc_e, 1.0, self.U, self.E, self.C, None, None, None, None,
                                    self.ws, sync=sync)
 
+    STAGE_UNITS = (8, 16, 32)
+
     def autotune(self, reps: int = 5) -> dict:
-        """Time the phase-2 schedules that keep per-problem failure (block-column owned with staged point operands,
-        block-owned pair lists) on the batch, after a warm-up run, and keep the faster."""
+        """Time the phase-2 schedules that keep per-problem failure on the batch, after a warm-up run each, and keep
+        the fastest: the block-column owned schedule with staged point operands at each unit size of STAGE_UNITS
+        (pairs per thread between two writes to the column tile; keys "stage/8", ...) and the block-owned pair lists
+        ("pairs"). The schedule is left at the winner (stage_unit holds its unit size)."""
         times = {}
-        for name in ("stage", "pairs"):
-            self.ws.set_kernel(name)
+
+        def timed(key):
             self.run()
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -144,8 +149,19 @@ class BatchedReduction:
                 self.run(sync=False)
             b.record()
             torch.cuda.synchronize()
-            times[name] = a.elapsed_time(b) / reps
-        self.schedule = min(times, key=times.get)
+            times[key] = a.elapsed_time(b) / reps
+
+        self.ws.set_kernel("stage")
+        for u in self.STAGE_UNITS:
+            self.ws.set_stage_unit(u)
+            timed(f"stage/{u}")
+        self.ws.set_kernel("pairs")
+        timed("pairs")
+        best = min(times, key=times.get)
+        self.schedule = best.split("/")[0]
+        if self.schedule == "stage":
+            self.stage_unit = int(best.split("/")[1])
+            self.ws.set_stage_unit(self.stage_unit)
         self.ws.set_kernel(self.schedule)
         self.graph = None
         return times

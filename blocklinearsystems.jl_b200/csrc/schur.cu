@@ -66,16 +66,18 @@ struct SchurPlan {
   DevBuf pt_rec;   // fast36, point-major pairs: {c1, k | (c2 - c1) << 25} per pair, k the S block
   bool points_ok = false;
   // fast36, sparse: the column-owned schedule (k_stage36). Work items are runs of a block column's visits (most
-  // columns are one item); per item {r2, first visit, visit count, items of its column}. Each item's pairs are cut into
-  // units (one S block, at most stage_unit pairs, in visit order) spread over the CTA's threads; per item and thread
-  // the first of its units (stg_thr, STAGE_NT + 1 per item). Units {first pair, pair count, the block's row offset in
-  // the column, r1 | diagonal << 31}; pairs {visit within the item | c1's index within its point << 16}.
+  // columns are one item); per item {r2, first visit, visit count, items of its column} (stg_items) and its first
+  // batch (stg_ibat, nitems + 1). Each item's off-diagonal pairs are cut into units (one S block, at most stage_unit
+  // pairs, in visit order), and its units, longest first, into batches of 32, one unit per lane of the warp that takes
+  // the batch: per batch {first pair, iterations} (stg_bat), per batch and lane {the block's row offset in the column |
+  // unit length << 16 | (the block's only unit in the item) << 31} (stg_lane); pairs batch by batch, iteration-major
+  // (lane fastest), {visit within the item | c1's index within its point << 16}, 0 past a lane's unit (stg_pairs).
   static constexpr int STAGE_NT = 256;
   bool stage_ok = false;
   int stage_unit = 16;
-  int64_t stage_items = 0, stage_max_nv = 0, stage_units = 0;
+  int64_t stage_items = 0, stage_max_nv = 0, stage_units = 0, stage_batches = 0, stage_slots = 0;
   int stage_grid[2] = {0, 0};   // persistent CTAs of k_stage36 (FP32, FP64): resident blocks per SM x SMs
-  DevBuf stg_items, stg_thr, stg_units, stg_pairs;
+  DevBuf stg_items, stg_ibat, stg_bat, stg_lane, stg_pairs;
   DevBuf EZ;   // per point E' = s_e E^-1 s_e (9, column-major) and z' = s_e .* z (3), FP64, for k_stage36
   // a batch of independent problems in one plan (bls_schur_plan_set_problems): per problem the lowest failing point
   // (global index, NONE if none), per point and per camera its problem; a failing problem skips its own phase 2 only
@@ -1432,15 +1434,18 @@ __global__ void k_gather(T* __restrict__ dest, const T* __restrict__ src, const 
 // ------------------------------------------------------------------------------------------------------------------
 // Phase 2 for d_r = 6, d_e = 3 and a sparse S, column-owned (the "stage" schedule): one CTA per work item, a run of
 // the visits of block column r2 (the points that observe camera r2, in the reference's retained_entry order).
-// 1. Each visit's point-side operand W = E' C_c2 (3 x 6, E' = s_e E^-1 s_e from the factor kernel, formed in FP64 and
-//    rounded to the storage type) goes to shared memory, with the visit point's first coupling index; the same pass
-//    adds C_c2' z' (z' = s_e .* z, FP64) to the column's gradient sums.
-// 2. Each thread runs its units: one S block (r1, r2) and a run of its pairs (c1, c2) of this item, in visit order.
-//    The thread owns the whole 6 x 6 block: acc += C_c1' W_c2 (C_c1 from global memory, W_c2 from shared memory), 108
-//    multiply-adds per pair in registers, then the block (times the conditioning scales s_r of its rows and columns)
-//    is added into the column's tile in shared memory (upper triangle only for the diagonal block).
-// 3. The tile is subtracted from the column of S (contiguous: the column's six scalar columns of H entries each), with
-//    atomics when the column is split into several items; g_S[r2] -= s_r .* sum C_c2' z'.
+// 1. Each visit's point-side operand W = E' C_c2 diag(s_r[r2]) (3 x 6, E' = s_e E^-1 s_e from the factor kernel, formed
+//    in FP64 and rounded to the storage type) goes to shared memory, with the visit point's first coupling index; the
+//    same pass adds C_c2' z' (z' = s_e .* z, FP64) to the column's gradient sums; the diagonal block's pairs (c2, c2),
+//    C_c2' W_c2 (upper triangle), are summed over the CTA into the tile's last six rows.
+// 2. The warps take batches of 32 units, a lane per unit: one off-diagonal S block (r1, r2) and a run of its pairs
+//    (c1, c2) of this item, in visit order. The lane owns the whole 6 x 6 block: acc += C_c1' W_c2 (C_c1 from global
+//    memory, the next pair's in flight; W_c2 from shared memory), 108 multiply-adds per pair in registers, then the
+//    block goes into the column's tile in shared memory (stored when it is its block's only unit, added with atomics
+//    otherwise).
+// 3. The tile, times the conditioning scales s_r of its rows, is subtracted from the column of S (contiguous: the
+//    column's six scalar columns of H entries each), with atomics when the column is split into several items;
+//    g_S[r2] -= s_r .* sum C_c2' z'.
 // The reference's accumulate_sparse_columns! (src/schur_reduction.jl:315-387) walks the same pairs of each column; W
 // is its W_c2 = E^-1 scaled(C_c2) with the point scales folded in, and the pair product C_c1' W_c2 its W_c1' C_c2
 // transposed (E^-1 is symmetric).
@@ -1539,21 +1544,25 @@ __device__ __forceinline__ void load_w18(const double* w, double* b) {
 
 template <class T>
 __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k_stage36(
-    const int4* __restrict__ items, const int32_t* __restrict__ thr, const int4* __restrict__ units, const uint32_t* __restrict__ pairs,
+    const int4* __restrict__ items, const int32_t* __restrict__ ibat, const int2* __restrict__ bat, const uint32_t* __restrict__ lane_rec,
+    const uint32_t* __restrict__ pairs,
     const int2* __restrict__ vis_rec, const int32_t* __restrict__ col_h, const int64_t* __restrict__ col_base, int64_t ncoup,
     const T* __restrict__ C, const double* __restrict__ EZ, const double* __restrict__ s_r, T* __restrict__ S, double* __restrict__ g,
     const Status* __restrict__ st, const int32_t* __restrict__ prob_of_cam, const long long* __restrict__ prob_fail, int64_t nitems,
-    unsigned long long* __restrict__ queue) {
+    unsigned long long* __restrict__ queue, const int32_t* __restrict__ S_rowval) {
   constexpr int NT = SchurPlan::STAGE_NT;
   constexpr int WR = stage_wr<T>();
   using Raw = typename RawOf<T>::type;
   extern __shared__ __align__(16) unsigned char sm[];
-  __shared__ int s_item;
+  __shared__ int s_item, s_bat;
   if (!live(st)) return;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31;
   // persistent: each CTA takes the next item (in column order) from the queue until none is left
   for (;;) {
-  if (tid == 0) s_item = (int)atomicAdd(queue, 1ull);
+  if (tid == 0) {
+    s_item = (int)atomicAdd(queue, 1ull);
+    s_bat = 0;
+  }
   __syncthreads();
   const int item = s_item;
   if (item >= nitems) break;
@@ -1569,10 +1578,33 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
   int* p0s = reinterpret_cast<int*>(W + (size_t)nv * WR);
   double* gp = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(p0s) + (((size_t)nv * 4 + 15) & ~size_t(15)));
   for (int i = tid; i < 6 * H; i += NT) tile[i] = T(0);
+  // the column's conditioning scales s_r, folded into W (the rows' scales are applied when the tile is written to S)
+  double fc[6];
+#pragma unroll
+  for (int w = 0; w < 6; ++w) fc[w] = s_r ? s_r[6 * r2 + w] : 1.0;
   // 1. W and the gradient sums, a thread per visit ({first coupling, point | index of c2 << 24} per visit)
+  // The visits' diagonal pairs (c2, c2), rows rho <= w of C_c2' W_c2: in FP64 formed in the same pass, in FP32 in a
+  // second pass over the thread's own W records (forming them in the first pass needs more registers than FP32's
+  // two CTAs per SM leave)
+  constexpr bool fused = sizeof(T) == 8;
+  auto diag_pair = [](T* dg, const T* c, const T* wt) {
+#pragma unroll
+    for (int w = 0, k = 0; w < 6; ++w)
+#pragma unroll
+      for (int rho = 0; rho <= w; ++rho, ++k) {
+        T x = dg[k];
+        x = fma(c[3 * rho], wt[3 * w], x);
+        x = fma(c[3 * rho + 1], wt[3 * w + 1], x);
+        x = fma(c[3 * rho + 2], wt[3 * w + 2], x);
+        dg[k] = x;
+      }
+  };
   double ga[6];
+  T dg[21];
 #pragma unroll
   for (int w = 0; w < 6; ++w) ga[w] = 0.0;
+#pragma unroll
+  for (int i = 0; i < 21; ++i) dg[i] = T(0);
   for (int v = tid; v < nv; v += NT) {
     const int2 vr = __ldg(vis_rec + q0 + v);
     const int e = vr.y & 0xffffff, c2 = vr.x + (int)((unsigned)vr.y >> 24);
@@ -1581,108 +1613,115 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
     double Ep[12];
 #pragma unroll
     for (int i = 0; i < 6; ++i) { double2 x = __ldg(ez + i); Ep[2 * i] = x.x; Ep[2 * i + 1] = x.y; }
-    T c[18];
+    T c[18], wt[18];
     load_block18(C, c2, ncoup, c);
     T* wv = W + (size_t)v * WR;
 #pragma unroll
     for (int w = 0; w < 6; ++w) {
       const double c0 = (double)c[3 * w], c1 = (double)c[3 * w + 1], c2v = (double)c[3 * w + 2];
 #pragma unroll
-      for (int t = 0; t < 3; ++t) wv[3 * w + t] = T(Ep[t] * c0 + Ep[t + 3] * c1 + Ep[t + 6] * c2v);
+      for (int t = 0; t < 3; ++t) {
+        wt[3 * w + t] = T(fc[w] * (Ep[t] * c0 + Ep[t + 3] * c1 + Ep[t + 6] * c2v));
+        wv[3 * w + t] = wt[3 * w + t];
+      }
       ga[w] += c0 * Ep[9] + c1 * Ep[10] + c2v * Ep[11];
     }
+    if constexpr (fused) diag_pair(dg, c, wt);
+  }
+  if constexpr (!fused) {
+    for (int v = tid; v < nv; v += NT) {
+      const int2 vr = __ldg(vis_rec + q0 + v);
+      T c[18], wt[18];
+      load_block18(C, vr.x + (int)((unsigned)vr.y >> 24), ncoup, c);
+      load_w18(W + (size_t)v * WR, wt);
+      diag_pair(dg, c, wt);
+    }
+  }
+  // the CTA's diagonal block: a warp sum, then one lane per warp into the tile (rows H - 6 .. H - 1)
+  {
+#pragma unroll
+    for (int w = 0, k = 0; w < 6; ++w)
+#pragma unroll
+      for (int rho = 0; rho <= w; ++rho, ++k) {
+        T x = dg[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) atomicAdd(tile + w * H + (H - 6) + rho, x);
+      }
+    // the gradient sums, per warp into shared memory (added up after phase 2)
+#pragma unroll
+    for (int w = 0; w < 6; ++w) {
+      double x = ga[w];
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (lane == 0) gp[6 * (tid >> 5) + w] = x;
+    }
   }
   __syncthreads();
-  // 2. the thread's units: its pair stream is units[ub].x .. (contiguous, 16-byte aligned), read four pairs at a time
-  const int* tp = thr + (int64_t)item * (NT + 1);
-  const int ub = __ldg(tp + tid), ue = __ldg(tp + tid + 1);
-  double fc[6];
-#pragma unroll
-  for (int w = 0; w < 6; ++w) fc[w] = s_r ? s_r[6 * r2 + w] : 1.0;
-  if (ub < ue) {
-    const uint4* q4 = reinterpret_cast<const uint4*>(pairs);
-    int4 un = __ldg(units + ub);
-    int u = ub, left = un.y;
-    int p = un.x;                       // stream position (a multiple of 4 at the first unit)
-    uint4 qa = __ldg(q4 + (p >> 2)), qb = __ldg(q4 + (p >> 2) + 1);
-    auto code = [&](int pos) -> uint32_t {   // the pair code at stream position pos (within the buffered 8)
-      const int o = pos - (p & ~3);
-      const uint4& q = o < 4 ? qa : qb;
-      const int k = o & 3;
-      return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;
-    };
-    Raw raw;
-    {
-      const uint32_t pr = code(p);
-      load_raw(C, p0s[pr & 0xffff] + (int)(pr >> 16), ncoup, raw);
-    }
-    T acc[36];
-#pragma unroll
-    for (int i = 0; i < 36; ++i) acc[i] = T(0);
+  // 2. the item's batches, taken by the warps from a counter, longest first; a lane per unit of the batch
+  {
+    const int bb = __ldg(ibat + item), nb = __ldg(ibat + item + 1) - bb;
     for (;;) {
-      const uint32_t pr = code(p);
-      T a[18], b[18];
-      take18(raw, a);
-      load_w18(W + (size_t)(pr & 0xffff) * WR, b);
-      // the next pair's block, in flight during this pair's products (the next unit's first pair when this one ends)
-      const bool more = left > 1 || u + 1 < ue;
-      if (more) {
-        const uint32_t pn = code(p + 1);
-        load_raw(C, p0s[pn & 0xffff] + (int)(pn >> 16), ncoup, raw);
-      }
+      int b = 0;
+      if (lane == 0) b = atomicAdd(&s_bat, 1);
+      b = __shfl_sync(0xffffffffu, b, 0);
+      if (b >= nb) break;
+      const int2 br = __ldg(bat + bb + b);   // {first pair, iterations}
+      const uint32_t lr = __ldg(lane_rec + (int64_t)(bb + b) * 32 + lane);
+      const int len = (int)((lr >> 16) & 0x7fff), iters = br.y;
+      const uint32_t* pc = pairs + br.x + lane;
+      // the codes of the current and the next iteration; the block of the current one is in flight
+      uint32_t cur = __ldg(pc), nxt = iters > 1 ? __ldg(pc + 32) : 0u;
+      Raw raw;
+      if (len > 0) load_raw(C, p0s[cur & 0xffff] + (int)(cur >> 16), ncoup, raw);
+      T acc[36];
 #pragma unroll
-      for (int rho = 0; rho < 6; ++rho)
+      for (int i = 0; i < 36; ++i) acc[i] = T(0);
+      for (int it = 0; it < iters; ++it) {
+        if (it < len) {
+          T a[18], w[18];
+          take18(raw, a);
+          load_w18(W + (size_t)(cur & 0xffff) * WR, w);
+          // the next pair's block, in flight during this pair's products
+          if (it + 1 < len) load_raw(C, p0s[nxt & 0xffff] + (int)(nxt >> 16), ncoup, raw);
 #pragma unroll
-        for (int w = 0; w < 6; ++w) {
-          T x = acc[6 * rho + w];
-          x = fma(a[3 * rho], b[3 * w], x);
-          x = fma(a[3 * rho + 1], b[3 * w + 1], x);
-          x = fma(a[3 * rho + 2], b[3 * w + 2], x);
-          acc[6 * rho + w] = x;
+          for (int rho = 0; rho < 6; ++rho)
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+              T x = acc[6 * rho + c];
+              x = fma(a[3 * rho], w[3 * c], x);
+              x = fma(a[3 * rho + 1], w[3 * c + 1], x);
+              x = fma(a[3 * rho + 2], w[3 * c + 2], x);
+              acc[6 * rho + c] = x;
+            }
         }
-      ++p;
-      if ((p & 3) == 0) {               // next quad: the buffered second quad, and read one more ahead
-        qa = qb;
-        qb = __ldg(q4 + (p >> 2) + 1);
+        cur = nxt;
+        if (it + 2 < iters) nxt = __ldg(pc + (int64_t)(it + 2) * 32);
       }
-      if (--left == 0) {
-        const bool diag = un.w < 0;
-        const int r1 = un.w & 0x7fffffff, row = un.z;
+      // the unit's block into the tile: a plain store when it is its block's only unit in the item
+      if (len > 0) {
+        T* tb = tile + (lr & 0xffff);
+        if (lr >> 31) {
 #pragma unroll
-        for (int rho = 0; rho < 6; ++rho) {
-          const double fr = s_r ? s_r[6 * r1 + rho] : 1.0;
+          for (int c = 0; c < 6; ++c)
 #pragma unroll
-          for (int w = 0; w < 6; ++w) {
-            if (diag && rho > w) continue;
-            T val = acc[6 * rho + w];
-            if (s_r) val = T((double)val * (fr * fc[w]));
-            atomicAdd(tile + w * H + row + rho, val);
-          }
+            for (int rho = 0; rho < 6; ++rho) tb[c * H + rho] = acc[6 * rho + c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 6; ++c)
+#pragma unroll
+            for (int rho = 0; rho < 6; ++rho) atomicAdd(tb + c * H + rho, acc[6 * rho + c]);
         }
-#pragma unroll
-        for (int i = 0; i < 36; ++i) acc[i] = T(0);
-        if (++u == ue) break;
-        un = __ldg(units + u);
-        left = un.y;
       }
     }
   }
   __syncthreads();
-  // 3. the column of S and the gradient
+  // 3. the column of S (times the rows' conditioning scales) and the gradient
   const int64_t cb = __ldg(col_base + r2);
-  if (nseg == 1) {
-    for (int i = tid; i < 6 * H; i += NT) S[cb + i] = S[cb + i] - tile[i];
-  } else {
-    for (int i = tid; i < 6 * H; i += NT) atomicAdd(S + cb + i, -tile[i]);
+  for (int i = tid; i < 6 * H; i += NT) {
+    T x = tile[i];
+    if (s_r) x = T((double)x * s_r[__ldg(S_rowval + cb + i)]);
+    if (nseg == 1) S[cb + i] = S[cb + i] - x;
+    else atomicAdd(S + cb + i, -x);
   }
-  const int lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-  for (int w = 0; w < 6; ++w) {
-    double x = ga[w];
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane == 0) gp[6 * warp + w] = x;
-  }
-  __syncthreads();
   if (tid < 6) {
     double x = 0.0;
     for (int w = 0; w < NT / 32; ++w) x += gp[6 * w + tid];
@@ -1698,27 +1737,26 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
 // first coupling; in FP64 this must fit STAGE_BUDGET bytes, so a column with more visits is cut into several items
 // (their tiles are added to S with atomics). Items stay in column order: neighbouring columns read the couplings of
 // overlapping sets of points, which then stay in L2 while the columns in flight move along the cameras.
-// A block's pairs of one item are cut into units of at most stage_unit pairs. The item's units, largest first, are dealt
-// out in rounds of STAGE_NT, one per thread: the lanes of a warp then run units of about the same length and add them
-// to the tile at the same time (a warp-wide shared-memory atomic costs the same for one lane as for 32), and the k-th
-// unit of a round goes to warp k mod (NT / 32), so that the units of one block (dealt one after the other) land in
-// different warps. A thread's units and their pairs are stored one after the other (its pair stream, padded to a
-// multiple of four pairs so that it is read 16 bytes at a time).
-static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int64_t nc, const std::vector<int32_t>& rptr,
+// A block's pairs of one item (the diagonal block's excepted: the staging pass forms those) are cut into units of at
+// most stage_unit pairs. The item's units, longest first, are cut into batches of 32 consecutive ones, a lane per unit:
+// the lanes of a batch run units of about the same length and write them to the tile at the same time (a warp-wide
+// shared-memory store or atomic costs the same for one lane as for 32), and the CTA's warps take batches from a
+// counter in shared memory, longest first, so that they finish the item together. Among units of one length the first
+// units of their blocks come first, then the second ones, so that the units of one block fall on different lanes. A
+// batch's pairs are stored iteration by iteration, 32 codes (one per lane) each, so that a warp reads them as one
+// 128-byte line per iteration.
+static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, const std::vector<int32_t>& rptr,
                                  const std::vector<int32_t>& rentry, const std::vector<int32_t>& entry_elim, const int64_t* eptr,
-                                 const std::vector<int64_t>& bcolptr, const std::vector<int64_t>& browval,
-                                 const std::vector<int64_t>& brow_off, const std::vector<int64_t>& col_h,
-                                 const std::vector<int32_t>& pair_c1, const std::vector<int32_t>& pair_c2,
-                                 const std::vector<int64_t>& colstart, const std::vector<std::vector<int32_t>>& col_cnt) {
-  constexpr int NT = SchurPlan::STAGE_NT, NW = NT / 32;
+                                 const int64_t* eret, const std::vector<int64_t>& bcolptr, const std::vector<int64_t>& browval,
+                                 const std::vector<int64_t>& brow_off, const std::vector<int64_t>& col_h) {
   constexpr int64_t STAGE_BUDGET = 200 * 1024;
   const int U = P->stage_unit;
-  std::vector<int32_t> pos_of(nc);
-  for (int64_t q = 0; q < nc; ++q) pos_of[rentry[q]] = (int32_t)q;
   struct ColOut {
-    std::vector<int4> items, units;   // units: pair start relative to the column's `pairs`
-    std::vector<int32_t> thr;         // per item NT + 1 unit offsets relative to the column's `units`
-    std::vector<uint32_t> pairs;
+    std::vector<int4> items;
+    std::vector<int32_t> nbat;   // per item its number of batches
+    std::vector<int2> bat;       // batches: first pair relative to the column's `pairs`, iterations
+    std::vector<uint32_t> lane, pairs;
+    int64_t nunits = 0;
   };
   std::vector<ColOut> out(nrb);
   // one launch serves every item, with the largest column tile and the largest visit run: the visit cap is set by the
@@ -1732,93 +1770,142 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, int6
   for (int64_t r2 = 0; r2 < nrb; ++r2) {
     const int64_t nv = rptr[r2 + 1] - rptr[r2];
     if (nv == 0) continue;
+    const int64_t kb = bcolptr[r2], nbc = bcolptr[r2 + 1] - kb;
+    // the kernel adds the diagonal block at rows H - 6 .. H - 1 of the tile: the column's last block must be (r2, r2)
+    if (nbc == 0 || browval[kb + nbc - 1] != r2 || brow_off[kb + nbc - 1] != col_h[r2] - 6) {
+      bad = 1;
+      continue;
+    }
     const int64_t nseg = (nv + vcap - 1) / vcap;
     std::vector<int64_t> bnd(nseg + 1);
     for (int64_t g = 0; g <= nseg; ++g) bnd[g] = g * nv / nseg;
-    struct Unit { int32_t k; std::vector<uint32_t> pr; };
+    // the column's off-diagonal pairs (c1 < c2 of the points observing r2) in visit order, then grouped by block slot
+    // (a counting sort keeps visit order within a block): {visit within its item | c1's index within its point << 16}
+    std::vector<int32_t> p_slot, p_seg;
+    std::vector<uint32_t> p_code;
+    std::vector<int32_t> cnt(nbc + 1, 0);
+    for (int64_t g = 0; g < nseg; ++g)
+      for (int64_t va = bnd[g]; va < bnd[g + 1]; ++va) {
+        const int32_t c2 = rentry[rptr[r2] + va];
+        const int64_t e = entry_elim[c2], v = va - bnd[g];
+        for (int64_t c1 = eptr[e]; c1 < c2; ++c1) {
+          const int64_t* lo = browval.data() + kb;
+          const int64_t* f = std::lower_bound(lo, lo + nbc, eret[c1]);
+          const int64_t i1 = c1 - eptr[e];
+          if (f == lo + nbc || *f != eret[c1] || v > 65535 || i1 > 65535) {
+            bad = 1;
+            continue;
+          }
+          p_slot.push_back((int32_t)(f - lo));
+          p_seg.push_back((int32_t)g);
+          p_code.push_back((uint32_t)v | ((uint32_t)i1 << 16));
+          cnt[f - lo + 1] += 1;
+        }
+      }
+    for (int64_t i = 0; i < nbc; ++i) cnt[i + 1] += cnt[i];
+    std::vector<int32_t> order(p_slot.size());
+    {
+      std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
+      for (size_t i = 0; i < p_slot.size(); ++i) order[pos[p_slot[i]]++] = (int32_t)i;
+    }
+    struct Unit { int32_t k, j; bool sole; std::vector<uint32_t> pr; };
     std::vector<std::vector<Unit>> seg_units(nseg);
-    const auto& cnt = col_cnt[r2];
-    for (int64_t sl = 0; sl + 1 < (int64_t)cnt.size(); ++sl) {
-      const int64_t a = colstart[r2] + cnt[sl], b = colstart[r2] + cnt[sl + 1];
+    for (int64_t sl = 0; sl < nbc; ++sl) {
       int64_t cur = -1;
-      for (int64_t x = a; x < b; ++x) {
-        const int32_t c1 = pair_c1[x], c2 = pair_c2[x];
-        const int64_t q = pos_of[c2] - rptr[r2];
-        int64_t g = q * nseg / nv;
-        while (g + 1 <= nseg - 1 && bnd[g + 1] <= q) ++g;
-        while (g > 0 && bnd[g] > q) --g;
-        const int64_t v = q - bnd[g], i1 = c1 - eptr[entry_elim[c2]];
-        if (v > 65535 || i1 < 0 || i1 > 65535) bad = 1;
+      std::vector<size_t> first(nseg, SIZE_MAX);   // per segment the block's first unit
+      for (int32_t x = cnt[sl]; x < cnt[sl + 1]; ++x) {
+        const int32_t i = order[x];
+        const int32_t g = p_seg[i];
         if (g != cur || (int)seg_units[g].back().pr.size() == U) {
-          seg_units[g].push_back({(int32_t)(bcolptr[r2] + sl), {}});
+          if (first[g] == SIZE_MAX) first[g] = seg_units[g].size();
+          const int32_t j = (int32_t)(seg_units[g].size() - first[g]);
+          seg_units[g].push_back({(int32_t)(kb + sl), j, true, {}});
           cur = g;
         }
-        seg_units[g].back().pr.push_back((uint32_t)v | ((uint32_t)i1 << 16));
+        seg_units[g].back().pr.push_back(p_code[i]);
       }
+      for (int64_t g = 0; g < nseg; ++g)
+        if (first[g] != SIZE_MAX && seg_units[g].size() - first[g] > 1)
+          for (size_t i = first[g]; i < seg_units[g].size(); ++i) seg_units[g][i].sole = false;
     }
     ColOut& o = out[r2];
     for (int64_t g = 0; g < nseg; ++g) {
       auto& us = seg_units[g];
-      std::stable_sort(us.begin(), us.end(), [](const Unit& x, const Unit& y) { return x.pr.size() > y.pr.size(); });
-      // in rounds, largest first: round r is units [r NT, (r + 1) NT), one per thread, so that the lanes of a warp run
-      // units of about the same length and add them to the tile together; slot k of a round is thread
-      // (k mod NW) * 32 + k / NW, so that the units of one block (consecutive slots) are in different warps
-      std::vector<std::vector<int32_t>> mine(NT);
-      for (size_t i = 0; i < us.size(); ++i) {
-        const int slot = (int)(i % NT);
-        mine[(slot % NW) * 32 + slot / NW].push_back((int32_t)i);
-      }
-      const int32_t ubase = (int32_t)o.units.size();
-      for (int t = 0; t < NT; ++t) {
-        o.thr.push_back((int32_t)o.units.size());
-        for (int32_t i : mine[t]) {
-          const Unit& u = us[i];
-          const int32_t r1 = (int32_t)browval[u.k];
-          o.units.push_back(make_int4((int32_t)o.pairs.size(), (int32_t)u.pr.size(), (int32_t)brow_off[u.k],
-                                      r1 | (r1 == (int32_t)r2 ? INT32_MIN : 0)));
-          o.pairs.insert(o.pairs.end(), u.pr.begin(), u.pr.end());
-        }
-        while (o.pairs.size() % 4) o.pairs.push_back(0u);   // the thread's stream padded to 16 bytes
-      }
-      o.thr.push_back((int32_t)o.units.size());
+      // longest first; among units of one length the first units of their blocks, then the second ones, ..., so that
+      // the units of one block fall on different lanes (or batches)
+      std::stable_sort(us.begin(), us.end(), [](const Unit& x, const Unit& y) {
+        return x.pr.size() != y.pr.size() ? x.pr.size() > y.pr.size() : x.j < y.j;
+      });
       o.items.push_back(make_int4((int32_t)r2, (int32_t)(rptr[r2] + bnd[g]), (int32_t)(bnd[g + 1] - bnd[g]), (int32_t)nseg));
+      o.nbat.push_back((int32_t)((us.size() + 31) / 32));
+      o.nunits += (int64_t)us.size();
+      // batches of 32 consecutive units: a lane per unit, as many iterations as the batch's first (longest) unit
+      for (size_t b0 = 0; b0 < us.size(); b0 += 32) {
+        const int32_t iters = (int32_t)us[b0].pr.size();
+        o.bat.push_back(make_int2((int32_t)o.pairs.size(), iters));
+        for (int L = 0; L < 32; ++L) {
+          if (b0 + L < us.size()) {
+            const Unit& u = us[b0 + L];
+            o.lane.push_back((uint32_t)brow_off[u.k] | ((uint32_t)u.pr.size() << 16) | (u.sole ? 0x80000000u : 0u));
+          } else {
+            o.lane.push_back(0u);
+          }
+        }
+        for (int32_t it = 0; it < iters; ++it)
+          for (int L = 0; L < 32; ++L) {
+            const size_t i = b0 + L;
+            o.pairs.push_back(i < us.size() && it < (int32_t)us[i].pr.size() ? us[i].pr[it] : 0u);
+          }
+      }
     }
   }
   if (bad) return;
-  int64_t nitems = 0, nunits = 0, npairs = 0, max_nv = 0;
+  int64_t nitems = 0, nbat = 0, nslots = 0, max_nv = 0, nunits = 0;
   for (int64_t r2 = 0; r2 < nrb; ++r2) {
     nitems += (int64_t)out[r2].items.size();
-    nunits += (int64_t)out[r2].units.size();
-    npairs += (int64_t)out[r2].pairs.size();
+    nbat += (int64_t)out[r2].bat.size();
+    nslots += (int64_t)out[r2].pairs.size();
+    nunits += out[r2].nunits;
     for (const int4& it : out[r2].items) max_nv = std::max<int64_t>(max_nv, it.z);
   }
-  if (npairs >= INT32_MAX || nunits >= INT32_MAX || nitems >= INT32_MAX) return;
-  std::vector<int4> items, units;
-  std::vector<int32_t> thr;
-  std::vector<uint32_t> pairs;
+  if (nslots >= INT32_MAX || nbat >= INT32_MAX / 32 || nitems >= INT32_MAX) return;
+  std::vector<int4> items;
+  std::vector<int32_t> ibat;
+  std::vector<int2> bat;
+  std::vector<uint32_t> lane, pairs;
   items.reserve(nitems);
-  units.reserve(nunits);
-  thr.reserve(nitems * (NT + 1));
-  pairs.reserve(npairs);
+  ibat.reserve(nitems + 1);
+  bat.reserve(nbat);
+  lane.reserve(nbat * 32);
+  pairs.reserve(nslots);
   for (int64_t r2 = 0; r2 < nrb; ++r2) {
     ColOut& o = out[r2];
-    const int32_t pbase = (int32_t)pairs.size(), ubase = (int32_t)units.size();   // pbase stays a multiple of 4
-    for (int4 u : o.units) units.push_back(make_int4(u.x + pbase, u.y, u.z, u.w));
-    for (int32_t t : o.thr) thr.push_back(t + ubase);
+    const int32_t pbase = (int32_t)pairs.size();
+    int32_t first = (int32_t)bat.size();
+    for (int32_t n : o.nbat) {
+      ibat.push_back(first);
+      first += n;
+    }
     items.insert(items.end(), o.items.begin(), o.items.end());
+    for (int2 b : o.bat) bat.push_back(make_int2(b.x + pbase, b.y));
+    lane.insert(lane.end(), o.lane.begin(), o.lane.end());
     pairs.insert(pairs.end(), o.pairs.begin(), o.pairs.end());
     std::vector<int4>().swap(o.items);
-    std::vector<int4>().swap(o.units);
-    std::vector<int32_t>().swap(o.thr);
+    std::vector<int2>().swap(o.bat);
+    std::vector<uint32_t>().swap(o.lane);
     std::vector<uint32_t>().swap(o.pairs);
   }
-  pairs.resize(pairs.size() + 8, 0u);   // the kernel's read-ahead of a stream's next 16 bytes stays inside the array
+  ibat.push_back((int32_t)bat.size());
+  pairs.resize(pairs.size() + 32, 0u);   // the kernel's read-ahead of the next iteration's codes stays inside the array
   upload(P->stg_items, items, s);
-  upload(P->stg_thr, thr, s);
-  upload(P->stg_units, units, s);
+  upload(P->stg_ibat, ibat, s);
+  upload(P->stg_bat, bat, s);
+  upload(P->stg_lane, lane, s);
   upload(P->stg_pairs, pairs, s);
   P->stage_items = nitems;
   P->stage_units = nunits;
+  P->stage_batches = nbat;
+  P->stage_slots = nslots;
   P->stage_max_nv = max_nv;
   P->stage_ok = true;
 }
@@ -2053,12 +2140,9 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
     }
   }
   // the column-owned schedule (k_stage36), sparse S only
-  if (P->fast36 && P->has_sparse) {
-    std::vector<int64_t> colstart(nrb + 1, 0);
-    for (int64_t r2 = 0; r2 < nrb; ++r2) colstart[r2 + 1] = colstart[r2] + col_npairs[r2];
-    build_stage_schedule(P.get(), s, nrb, nc, rptr, rentry, entry_elim, d->eliminated_ptr, bcolptr, browval, brow_off, col_h,
-                         pair_c1, pair_c2, colstart, col_cnt);
-  }
+  if (P->fast36 && P->has_sparse)
+    build_stage_schedule(P.get(), s, nrb, rptr, rentry, entry_elim, d->eliminated_ptr, d->entry_retained, bcolptr, browval,
+                         brow_off, col_h);
   // staged work items for the host-buffer reduction: stage j holds points [stage_pt[j], stage_pt[j + 1]); a block's
   // pairs ascend in point within its slot, so its pairs of one stage are a contiguous run, cut into items of at most
   // PAIR_CHUNK pairs (solo when the run makes one item)
@@ -2197,7 +2281,7 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
 static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
-                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h, &P->stg_items, &P->stg_thr, &P->stg_units, &P->stg_pairs, &P->EZ,
+                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h, &P->stg_items, &P->stg_ibat, &P->stg_bat, &P->stg_lane, &P->stg_pairs, &P->EZ,
                           &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g, &P->w_apply, &P->t_apply, &P->acc1,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
@@ -2359,7 +2443,7 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
   // the column-owned schedule reads C with 16-byte loads (C_data on a 16-byte boundary, as the device allocators give)
   const bool c16 = (reinterpret_cast<uintptr_t>(C) & 31) == 0;   // 32-byte loads of C
   const bool batch = P->nprob > 0 && !dense;
-  const bool use_stage = P->fast36 && (P->kernel == 5 || batch) && !dense && P->stage_ok && c16;
+  const bool use_stage = P->fast36 && (P->kernel == 5 || batch) && !dense && P->stage_ok && c16 && (!s_r || P->S_rowval.p);
   const int32_t* poc = batch ? P->prob_of_cam.as<int32_t>() : nullptr;
   long long* pf = batch ? P->prob_fail.as<long long>() : nullptr;
   if (batch) {
@@ -2405,10 +2489,10 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
       }
       const int64_t grid = std::min<int64_t>(P->stage_items, P->stage_grid[sizeof(T) == 4 ? 0 : 1]);
       k_stage36<T><<<(unsigned)grid, SchurPlan::STAGE_NT, smem, s>>>(
-          P->stg_items.as<int4>(), P->stg_thr.as<int32_t>(), P->stg_units.as<int4>(), P->stg_pairs.as<uint32_t>(),
+          P->stg_items.as<int4>(), P->stg_ibat.as<int32_t>(), P->stg_bat.as<int2>(), P->stg_lane.as<uint32_t>(), P->stg_pairs.as<uint32_t>(),
           P->vis_rec.as<int2>(), P->col_h.as<int32_t>(), P->col_base.as<int64_t>(), P->ncoup, C, P->EZ.as<double>(), s_r, S, g, st,
           poc, pf, P->stage_items,
-          reinterpret_cast<unsigned long long*>(&st->pad));
+          reinterpret_cast<unsigned long long*>(&st->pad), P->S_rowval.as<int32_t>());
       if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
     }
   } else if (P->fast36 && !batch && P->kernel == 0) {
@@ -2898,6 +2982,51 @@ int bls_schur_plan_set_kernel(bls_schur_plan* P, int which) {
   BLS_GUARD({
     if (which == 4) ensure_points(P);
     P->kernel = which;
+    return BLS_OK;
+  })
+}
+
+// Rebuild the column-owned schedule with units of at most `unit` pairs, from the plan's device copies of the structure
+// (the schedule is a plan-time product; this is the autotuner's knob). On failure the previous schedule stays.
+int bls_schur_plan_set_stage_unit(bls_schur_plan* P, int unit) {
+  if (!P || unit < 1 || unit > 4096) return BLS_EINVAL;
+  BLS_GUARD({
+    if (!P->fast36 || !P->has_sparse || !P->stage_ok) throw Error(BLS_EUNSUPPORTED, "the plan has no column-owned schedule");
+    if (unit == P->stage_unit) return BLS_OK;
+    cudaStream_t s = P->ctx->stream;
+    const int64_t nrb = P->nrblocks, neb = P->neblocks, nc = P->ncoup;
+    const int64_t nb = P->nblocks;
+    auto down32 = [&](const DevBuf& b, int64_t n) {
+      std::vector<int32_t> v((size_t)n);
+      if (n) BLS_CUDA(cudaMemcpyAsync(v.data(), b.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      return v;
+    };
+    std::vector<int32_t> rptr = down32(P->retained_ptr, nrb + 1), rentry = down32(P->retained_entry, nc);
+    std::vector<int32_t> entry_elim = down32(P->entry_eliminated, nc), ep32 = down32(P->eliminated_ptr, neb + 1);
+    std::vector<int32_t> er32 = down32(P->entry_retained, nc), b_r1 = down32(P->block_r1, nb), b_r2 = down32(P->block_r2, nb);
+    std::vector<int32_t> ch = down32(P->col_h, nrb);
+    std::vector<int64_t> b_base((size_t)nb), cbase((size_t)nrb);
+    if (nb) BLS_CUDA(cudaMemcpyAsync(b_base.data(), P->block_base_sparse.p, (size_t)nb * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    BLS_CUDA(cudaMemcpyAsync(cbase.data(), P->col_base.p, (size_t)nrb * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    BLS_CUDA(cudaStreamSynchronize(s));
+    std::vector<int64_t> eptr(ep32.begin(), ep32.end()), eret(er32.begin(), er32.end());
+    std::vector<int64_t> bcolptr(nrb + 1, 0), browval(nb), brow_off(nb), col_h(ch.begin(), ch.end());
+    for (int64_t k = 0; k < nb; ++k) {
+      bcolptr[b_r2[k] + 1] += 1;
+      browval[k] = b_r1[k];
+      brow_off[k] = b_base[k] - cbase[b_r2[k]];
+    }
+    for (int64_t r = 0; r < nrb; ++r) bcolptr[r + 1] += bcolptr[r];
+    const int old = P->stage_unit;
+    P->stage_unit = unit;
+    P->stage_ok = false;
+    build_stage_schedule(P, s, nrb, rptr, rentry, entry_elim, eptr.data(), eret.data(), bcolptr, browval, brow_off, col_h);
+    if (!P->stage_ok) {
+      P->stage_unit = old;
+      P->stage_ok = true;
+      throw Error(BLS_EUNSUPPORTED, "the schedule does not fit this unit size");
+    }
+    P->stage_grid[0] = P->stage_grid[1] = 0;
     return BLS_OK;
   })
 }

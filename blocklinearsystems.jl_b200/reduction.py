@@ -123,6 +123,11 @@ class SchurReductionWorkspace:
         check(_lib.gpu().bls_schur_plan_set_kernel(self._h, {"columns": 0, "pairs": 1, "lanes": 2, "tiles": 3, "points": 4,
                                                              "stage": 5}[which]))
 
+    def set_stage_unit(self, unit: int) -> None:
+        """Rebuild the "stage" schedule with units of at most `unit` pairs (one thread's run of one S block's pairs
+        between two writes to the column tile); 16 at plan creation."""
+        check(_lib.gpu().bls_schur_plan_set_stage_unit(self._h, int(unit)))
+
     def phase2_kernel_name(self, dtype=torch.float32, *, dense: bool = False, scaled: bool = False) -> str:
         """The phase-2 kernel the next reduction with this storage type launches (as the profiler lists it)."""
         buf = C.create_string_buffer(64)

@@ -196,6 +196,11 @@ int bls_schur_plan_instrument(bls_schur_plan* plan, int timing);
  * 4 = point-major, six lanes per pair, entries added into S with vector reductions (as 1 when S has 2^25 or more
  * blocks). All compute the same reduction; the choice is kept for comparisons and for autotuning. */
 int bls_schur_plan_set_kernel(bls_schur_plan* plan, int which);
+/* No counterpart in the reference (a tuning knob of this build's schedule): rebuild the column-owned schedule (which = 5)
+ * with units of at most `unit` pairs (1..4096; 16 at plan creation), a unit being one thread's run of one S block's
+ * pairs between two writes to the column tile. Sparse plans on the 6/3 fast path only (BLS_EUNSUPPORTED otherwise);
+ * on failure the previous schedule stays. Synchronises. */
+int bls_schur_plan_set_stage_unit(bls_schur_plan* plan, int unit);
 /* No counterpart in the reference (a batch of the reference's calls in one plan): declare that the plan's structure is
  * the disjoint union of `nprob` independent problems, problem p owning eliminated blocks [point_off[p],
  * point_off[p+1]), retained blocks [camera_off[p], camera_off[p+1]), rows [row_off[p], row_off[p+1]) of g_S and

@@ -30,13 +30,16 @@ def relerr(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-def run_both(bls, st, ost, pat, opat, E, Cd, R, b_r, b_e, sc_r, sc_e, lam, dense, dtype, s_r=None, s_e=None, kernel="pairs"):
+def run_both(bls, st, ost, pat, opat, E, Cd, R, b_r, b_e, sc_r, sc_e, lam, dense, dtype, s_r=None, s_e=None, kernel="pairs",
+             stage_unit=None):
     """One reset + reduce + back-substitution on the device and in the oracle (FP64, on the same stored values)."""
     npdt = np.float32 if dtype == torch.float32 else np.float64
     E32, C32, R32 = E.astype(npdt), Cd.astype(npdt), R.astype(npdt)
     nr = st.nr
     ws = bls.SchurReductionWorkspace(st, pat)
     ws.set_kernel(kernel)
+    if stage_unit is not None:
+        ws.set_stage_unit(stage_unit)
     g = torch.zeros(nr, dtype=torch.float64, device=DEV)
     args = dict(s_r=None if s_r is None else cu(s_r), s_e=None if s_e is None else cu(s_e))
     if dense:
@@ -192,6 +195,34 @@ def test_scene_mixed_matches_fp64_oracle(bls, name, ncams, npoints, kernel):
     assert relerr(o["S"], o["oS"]) < 1e-4
     assert relerr(o["g"], o["og"]) < 1e-6   # z and the gradient are FP64 from FP32 data
     assert relerr(o["x_e"], o["ox_e"]) < 1e-6
+
+
+@pytest.mark.parametrize("unit", [1, 3, 16, 64, 4096])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
+def test_stage_unit_sizes(bls, unit, dtype):
+    """The column-owned schedule rebuilt with other unit sizes (one pair per unit up to whole blocks per unit) gives
+    the same reduction, conditioning scales included."""
+    p, st, ost, opat = scene_system(bls, "pcg_10000x1M", 150, 6000)
+    rng = np.random.default_rng(11)
+    s_r = np.ldexp(1.0, rng.integers(-4, 5, st.nr))
+    s_e = np.ldexp(1.0, rng.integers(-4, 5, st.ne))
+    o = run_both(bls, st, ost, p.pattern, opat, p.E, p.C, p.R, p.b_r, p.b_e, p.scaling_r, p.scaling_e, p.lam, False, dtype,
+                 s_r=s_r, s_e=s_e, kernel="stage", stage_unit=unit)
+    assert o["ok"] and o["ook"]
+    tol = 1e-12 if dtype == torch.float64 else 1e-4
+    assert relerr(o["S"], o["oS"]) < tol
+    assert relerr(o["g"], o["og"]) < (1e-12 if dtype == torch.float64 else 1e-6)
+
+
+def test_stage_unit_rejected(bls):
+    p, st, ost, opat = scene_system(bls, "sparse_1000x200k", 40, 1500)
+    ws = bls.SchurReductionWorkspace(st, p.pattern, None)
+    with pytest.raises(bls.ArgumentError):
+        ws.set_stage_unit(0)
+    dp, dst, _, _ = scene_system(bls, "dense_50x2000", 20, 400, dense=True)
+    wd = bls.SchurReductionWorkspace(dst, None, None)
+    with pytest.raises(Exception, match="column-owned schedule"):
+        wd.set_stage_unit(8)
 
 
 @pytest.mark.parametrize("kernel", ["stage", "pairs", "points", "lanes"])
