@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <memory>
+#include <type_traits>
 #include <vector>
 
 #include "pcg_plan.hpp"
@@ -196,6 +197,69 @@ __global__ void __launch_bounds__(256) k_lin_fwd(int64_t n, int K1, const IN1* _
   if (relu) acc = fmaxf(acc, 0.f);
   if (outA) outA[b * O + o] = from_f<A>(acc);
   if (outF) outF[b * O + o] = acc;
+}
+
+// The BF16 inference form of k_lin_fwd on the tensor cores: out[b, :] = act(bias + [in1 in2][b, :] W'), BF16 operands
+// and FP32 accumulation by mma.sync m16n8k16; a warp per 16 nodes, the layer's weights rounded to BF16 in shared memory
+// (O padded to a multiple of 8, row o = column o of the B operand). Needs K1 and K2 multiples of 16, K1 + K2 <= 128,
+// O <= 64.
+__device__ __forceinline__ void mma_bf16_16816(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+               : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+               : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+constexpr int LIN_MMA_KMAX = 128, LIN_MMA_OMAX = 64;
+__global__ void __launch_bounds__(128) k_lin_mma(int64_t n, int K1, const __nv_bfloat16* __restrict__ in1, int K2,
+                                                 const __nv_bfloat16* __restrict__ in2, const float* __restrict__ W1,
+                                                 const float* __restrict__ W2, const float* __restrict__ bias, int O, bool relu,
+                                                 __nv_bfloat16* __restrict__ outA, float* __restrict__ outF) {
+  __shared__ __align__(16) __nv_bfloat16 wsm[LIN_MMA_OMAX * LIN_MMA_KMAX];
+  __shared__ float bsm[LIN_MMA_OMAX];
+  const int K = K1 + K2, NT8 = (O + 7) / 8;
+  for (int i = threadIdx.x; i < NT8 * 8 * K; i += blockDim.x) {
+    const int o = i / K, k = i - o * K;
+    const float wv = o >= O ? 0.f : (k < K1 ? W1[o * K1 + k] : W2[o * K2 + (k - K1)]);
+    wsm[i] = __float2bfloat16(wv);
+  }
+  for (int o = threadIdx.x; o < LIN_MMA_OMAX; o += blockDim.x) bsm[o] = o < O ? bias[o] : 0.f;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int64_t r0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + warp) * 16;
+  if (r0 >= n) return;
+  const int64_t ra = r0 + g, rb = r0 + g + 8;
+  // two BF16 entries (columns k, k + 1) of row r of [in1 in2]; zero past the last node
+  auto ld2 = [&](int64_t r, int k) -> uint32_t {
+    if (r >= n) return 0u;
+    const __nv_bfloat16* src = k < K1 ? in1 + r * K1 + k : in2 + r * K2 + (k - K1);
+    return *reinterpret_cast<const uint32_t*>(src);
+  };
+  float acc[LIN_MMA_OMAX / 8][4];
+#pragma unroll
+  for (int j = 0; j < LIN_MMA_OMAX / 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  for (int kk = 0; kk < K; kk += 16) {
+    const uint32_t a0 = ld2(ra, kk + 2 * t), a1 = ld2(rb, kk + 2 * t), a2 = ld2(ra, kk + 8 + 2 * t), a3 = ld2(rb, kk + 8 + 2 * t);
+#pragma unroll
+    for (int j = 0; j < LIN_MMA_OMAX / 8; ++j)
+      if (j < NT8) {
+        const __nv_bfloat16* wb = wsm + (j * 8 + g) * K + kk + 2 * t;
+        mma_bf16_16816(acc[j], a0, a1, a2, a3, *reinterpret_cast<const uint32_t*>(wb), *reinterpret_cast<const uint32_t*>(wb + 8));
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < LIN_MMA_OMAX / 8; ++j)
+    if (j < NT8) {
+      const int c = j * 8 + 2 * t;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const int64_t r = h < 2 ? ra : rb;
+        const int o = c + (h & 1);
+        if (r >= n || o >= O) continue;
+        float v = acc[j][h] + bsm[o];
+        if (relu) v = fmaxf(v, 0.f);
+        if (outA) outA[r * O + o] = __float2bfloat16(v);
+        if (outF) outF[r * O + o] = v;
+      }
+    }
 }
 
 // m[b, :] = sum_q w[q] h[other_q, :]; one warp per node, two channels per lane
@@ -491,6 +555,13 @@ template <class A, class IN1>
 static void lin_fwd(GNNPlan* G, int K1, const IN1* in1, int K2, const A* in2, const float* W1, const float* W2, const float* b, int O, bool relu,
                     A* outA, float* outF) {
   cudaStream_t s = G->pcg->ctx->stream;
+  if constexpr (std::is_same<A, __nv_bfloat16>::value && std::is_same<IN1, __nv_bfloat16>::value) {
+    if (K1 % 16 == 0 && K2 % 16 == 0 && K1 + K2 <= LIN_MMA_KMAX && O <= LIN_MMA_OMAX) {   // the width-64 layers
+      k_lin_mma<<<grid_for(G->n, 64), 128, 0, s>>>(G->n, K1, in1, K2, in2, W1, W2, b, O, relu, outA, outF);
+      G->pcg->launches += 1;
+      return;
+    }
+  }
   const size_t smem = sizeof(float) * O * (K1 + K2);
   if (smem > 48 * 1024) BLS_CUDA(cudaFuncSetAttribute(k_lin_fwd<A, IN1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_lin_fwd<A, IN1><<<grid_for(G->n * O, 256), 256, smem, s>>>(G->n, K1, in1, K2, in2, W1, W2, b, O, relu, outA, outF);

@@ -67,11 +67,12 @@ struct SchurPlan {
   bool points_ok = false;
   // fast36, sparse: the column-owned schedule (k_stage36). Work items are runs of a block column's visits (most
   // columns are one item); per item {r2, first visit, visit count, items of its column} (stg_items) and its first
-  // batch (stg_ibat, nitems + 1). Each item's off-diagonal pairs are cut into units (one S block, at most stage_unit
-  // pairs, in visit order), and its units, longest first, into batches of 32, one unit per lane of the warp that takes
-  // the batch: per batch {first pair, iterations} (stg_bat), per batch and lane {the block's row offset in the column |
-  // unit length << 16 | (the block's only unit in the item) << 31} (stg_lane); pairs batch by batch, iteration-major
-  // (lane fastest), {visit within the item | c1's index within its point << 16}, 0 past a lane's unit (stg_pairs).
+  // batch (stg_ibat, nitems + 1). Each item's first batch holds its diagonal block's pairs, its visits cut into 32 runs;
+  // its off-diagonal pairs are cut into units (one S block, at most stage_unit pairs, in visit order), and those units,
+  // longest first, into the following batches of 32, one unit per lane of the warp that takes the batch: per batch
+  // {first pair, iterations} (stg_bat), per batch and lane {the block's row offset in the column | unit length << 16 |
+  // (the block's only unit in the item) << 31} (stg_lane); pairs batch by batch, iteration-major (lane fastest),
+  // {visit within the item | c1's index within its point << 16}, 0 past a lane's unit (stg_pairs).
   static constexpr int STAGE_NT = 256;
   bool stage_ok = false;
   int stage_unit = 16;
@@ -1436,13 +1437,13 @@ __global__ void k_gather(T* __restrict__ dest, const T* __restrict__ src, const 
 // the visits of block column r2 (the points that observe camera r2, in the reference's retained_entry order).
 // 1. Each visit's point-side operand W = E' C_c2 diag(s_r[r2]) (3 x 6, E' = s_e E^-1 s_e from the factor kernel, formed
 //    in FP64 and rounded to the storage type) goes to shared memory, with the visit point's first coupling index; the
-//    same pass adds C_c2' z' (z' = s_e .* z, FP64) to the column's gradient sums; the diagonal block's pairs (c2, c2),
-//    C_c2' W_c2 (upper triangle), are summed over the CTA into the tile's last six rows.
-// 2. The warps take batches of 32 units, a lane per unit: one off-diagonal S block (r1, r2) and a run of its pairs
-//    (c1, c2) of this item, in visit order. The lane owns the whole 6 x 6 block: acc += C_c1' W_c2 (C_c1 from global
-//    memory, the next pair's in flight; W_c2 from shared memory), 108 multiply-adds per pair in registers, then the
-//    block goes into the column's tile in shared memory (stored when it is its block's only unit, added with atomics
-//    otherwise).
+//    same pass adds C_c2' z' (z' = s_e .* z, FP64) to the column's gradient sums.
+// 2. The warps take batches of 32 units, a lane per unit: one S block (r1, r2) and a run of its pairs (c1, c2) of
+//    this item, in visit order. The lane owns the whole 6 x 6 block: acc += C_c1' W_c2 (C_c1 from global memory, the
+//    next pair's in flight; W_c2 from shared memory), 108 multiply-adds per pair in registers, then the block goes
+//    into the column's tile in shared memory (stored when it is its block's only unit, added with atomics otherwise).
+//    The item's first batch is the diagonal block's pairs (c2, c2), the visits cut into 32 runs: its lanes' blocks
+//    are summed over the warp and the upper triangle stored into the tile's last six rows.
 // 3. The tile, times the conditioning scales s_r of its rows, is subtracted from the column of S (contiguous: the
 //    column's six scalar columns of H entries each), with atomics when the column is split into several items;
 //    g_S[r2] -= s_r .* sum C_c2' z'.
@@ -1582,78 +1583,40 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
   double fc[6];
 #pragma unroll
   for (int w = 0; w < 6; ++w) fc[w] = s_r ? s_r[6 * r2 + w] : 1.0;
-  // 1. W and the gradient sums, a thread per visit ({first coupling, point | index of c2 << 24} per visit)
-  // The visits' diagonal pairs (c2, c2), rows rho <= w of C_c2' W_c2: in FP64 formed in the same pass, in FP32 in a
-  // second pass over the thread's own W records (forming them in the first pass needs more registers than FP32's
-  // two CTAs per SM leave)
-  constexpr bool fused = sizeof(T) == 8;
-  auto diag_pair = [](T* dg, const T* c, const T* wt) {
-#pragma unroll
-    for (int w = 0, k = 0; w < 6; ++w)
-#pragma unroll
-      for (int rho = 0; rho <= w; ++rho, ++k) {
-        T x = dg[k];
-        x = fma(c[3 * rho], wt[3 * w], x);
-        x = fma(c[3 * rho + 1], wt[3 * w + 1], x);
-        x = fma(c[3 * rho + 2], wt[3 * w + 2], x);
-        dg[k] = x;
-      }
-  };
+  // 1. W and the gradient sums, a thread per visit ({first coupling, point | index of c2 << 24} per visit); the next
+  //    visit's record is loaded while the current one is formed
   double ga[6];
-  T dg[21];
 #pragma unroll
   for (int w = 0; w < 6; ++w) ga[w] = 0.0;
-#pragma unroll
-  for (int i = 0; i < 21; ++i) dg[i] = T(0);
-  for (int v = tid; v < nv; v += NT) {
-    const int2 vr = __ldg(vis_rec + q0 + v);
-    const int e = vr.y & 0xffffff, c2 = vr.x + (int)((unsigned)vr.y >> 24);
-    p0s[v] = vr.x;
-    const double2* ez = reinterpret_cast<const double2*>(EZ + 12 * (int64_t)e);
-    double Ep[12];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) { double2 x = __ldg(ez + i); Ep[2 * i] = x.x; Ep[2 * i + 1] = x.y; }
-    T c[18], wt[18];
-    load_block18(C, c2, ncoup, c);
-    T* wv = W + (size_t)v * WR;
-#pragma unroll
-    for (int w = 0; w < 6; ++w) {
-      const double c0 = (double)c[3 * w], c1 = (double)c[3 * w + 1], c2v = (double)c[3 * w + 2];
-#pragma unroll
-      for (int t = 0; t < 3; ++t) {
-        wt[3 * w + t] = T(fc[w] * (Ep[t] * c0 + Ep[t + 3] * c1 + Ep[t + 6] * c2v));
-        wv[3 * w + t] = wt[3 * w + t];
-      }
-      ga[w] += c0 * Ep[9] + c1 * Ep[10] + c2v * Ep[11];
-    }
-    if constexpr (fused) diag_pair(dg, c, wt);
-  }
-  if constexpr (!fused) {
-    for (int v = tid; v < nv; v += NT) {
-      const int2 vr = __ldg(vis_rec + q0 + v);
-      T c[18], wt[18];
-      load_block18(C, vr.x + (int)((unsigned)vr.y >> 24), ncoup, c);
-      load_w18(W + (size_t)v * WR, wt);
-      diag_pair(dg, c, wt);
-    }
-  }
-  // the CTA's diagonal block: a warp sum, then one lane per warp into the tile (rows H - 6 .. H - 1)
   {
+    int2 vr = tid < nv ? __ldg(vis_rec + q0 + tid) : make_int2(0, 0);
+    for (int v = tid; v < nv; v += NT) {
+      const double2* ez = reinterpret_cast<const double2*>(EZ + 12 * (int64_t)(vr.y & 0xffffff));
+      double Ep[12];
 #pragma unroll
-    for (int w = 0, k = 0; w < 6; ++w)
+      for (int i = 0; i < 6; ++i) { double2 x = __ldg(ez + i); Ep[2 * i] = x.x; Ep[2 * i + 1] = x.y; }
+      T c[18];
+      load_block18(C, vr.x + (int)((unsigned)vr.y >> 24), ncoup, c);
+      int2 vn = make_int2(0, 0);
+      if (v + NT < nv) vn = __ldg(vis_rec + q0 + v + NT);
+      p0s[v] = vr.x;
+      T* wv = W + (size_t)v * WR;
 #pragma unroll
-      for (int rho = 0; rho <= w; ++rho, ++k) {
-        T x = dg[k];
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) atomicAdd(tile + w * H + (H - 6) + rho, x);
+      for (int w = 0; w < 6; ++w) {
+        const double c0 = (double)c[3 * w], c1 = (double)c[3 * w + 1], c2v = (double)c[3 * w + 2];
+#pragma unroll
+        for (int t = 0; t < 3; ++t) wv[3 * w + t] = T(fc[w] * (Ep[t] * c0 + Ep[t + 3] * c1 + Ep[t + 6] * c2v));
+        ga[w] += c0 * Ep[9] + c1 * Ep[10] + c2v * Ep[11];
       }
-    // the gradient sums, per warp into shared memory (added up after phase 2)
-#pragma unroll
-    for (int w = 0; w < 6; ++w) {
-      double x = ga[w];
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      if (lane == 0) gp[6 * (tid >> 5) + w] = x;
+      vr = vn;
     }
+  }
+  // the gradient sums, per warp into shared memory (added up after phase 2)
+#pragma unroll
+  for (int w = 0; w < 6; ++w) {
+    double x = ga[w];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) gp[6 * (tid >> 5) + w] = x;
   }
   __syncthreads();
   // 2. the item's batches, taken by the warps from a counter, longest first; a lane per unit of the batch
@@ -1696,8 +1659,18 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
         cur = nxt;
         if (it + 2 < iters) nxt = __ldg(pc + (int64_t)(it + 2) * 32);
       }
-      // the unit's block into the tile: a plain store when it is its block's only unit in the item
-      if (len > 0) {
+      if (b == 0) {
+        // the diagonal batch: the lanes' blocks summed over the warp, the upper triangle into the tile's last six rows
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+#pragma unroll
+          for (int rho = 0; rho <= c; ++rho) {
+            T x = acc[6 * rho + c];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) tile[c * H + (H - 6) + rho] = x;
+          }
+      } else if (len > 0) {
+        // the unit's block into the tile: a plain store when it is its block's only unit in the item
         T* tb = tile + (lr & 0xffff);
         if (lr >> 31) {
 #pragma unroll
@@ -1715,12 +1688,22 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
   }
   __syncthreads();
   // 3. the column of S (times the rows' conditioning scales) and the gradient
+  // a thread per tile row: its conditioning scale once, then the row's six entries (one per scalar column), all six
+  // loads of S in flight together
   const int64_t cb = __ldg(col_base + r2);
-  for (int i = tid; i < 6 * H; i += NT) {
-    T x = tile[i];
-    if (s_r) x = T((double)x * s_r[__ldg(S_rowval + cb + i)]);
-    if (nseg == 1) S[cb + i] = S[cb + i] - x;
-    else atomicAdd(S + cb + i, -x);
+  for (int rr = tid; rr < H; rr += NT) {
+    const double f = s_r ? s_r[__ldg(S_rowval + cb + rr)] : 1.0;
+    T* Sr = S + cb + rr;
+    if (nseg == 1) {
+      T old[6];
+#pragma unroll
+      for (int w = 0; w < 6; ++w) old[w] = Sr[(int64_t)w * H];
+#pragma unroll
+      for (int w = 0; w < 6; ++w) Sr[(int64_t)w * H] = old[w] - T((double)tile[w * H + rr] * f);
+    } else {
+#pragma unroll
+      for (int w = 0; w < 6; ++w) atomicAdd(Sr + (int64_t)w * H, -T((double)tile[w * H + rr] * f));
+    }
   }
   if (tid < 6) {
     double x = 0.0;
@@ -1737,14 +1720,14 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
 // first coupling; in FP64 this must fit STAGE_BUDGET bytes, so a column with more visits is cut into several items
 // (their tiles are added to S with atomics). Items stay in column order: neighbouring columns read the couplings of
 // overlapping sets of points, which then stay in L2 while the columns in flight move along the cameras.
-// A block's pairs of one item (the diagonal block's excepted: the staging pass forms those) are cut into units of at
-// most stage_unit pairs. The item's units, longest first, are cut into batches of 32 consecutive ones, a lane per unit:
-// the lanes of a batch run units of about the same length and write them to the tile at the same time (a warp-wide
-// shared-memory store or atomic costs the same for one lane as for 32), and the CTA's warps take batches from a
-// counter in shared memory, longest first, so that they finish the item together. Among units of one length the first
-// units of their blocks come first, then the second ones, so that the units of one block fall on different lanes. A
-// batch's pairs are stored iteration by iteration, 32 codes (one per lane) each, so that a warp reads them as one
-// 128-byte line per iteration.
+// A block's pairs of one item are cut into units of at most stage_unit pairs, except the diagonal block's, which make
+// the item's first batch (the item's visits cut into 32 runs, one per lane). The item's other units, longest first,
+// are cut into batches of 32 consecutive ones, a lane per unit: the lanes of a batch run units of about the same
+// length and write them to the tile at the same time (a warp-wide shared-memory store or atomic costs the same for
+// one lane as for 32), and the CTA's warps take batches from a counter in shared memory, longest first, so that they
+// finish the item together. Among units of one length the first units of their blocks come first, then the second
+// ones, so that the units of one block fall on different lanes. A batch's pairs are stored iteration by iteration, 32
+// codes (one per lane) each, so that a warp reads them as one 128-byte line per iteration.
 static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, const std::vector<int32_t>& rptr,
                                  const std::vector<int32_t>& rentry, const std::vector<int32_t>& entry_elim, const int64_t* eptr,
                                  const int64_t* eret, const std::vector<int64_t>& bcolptr, const std::vector<int64_t>& browval,
@@ -1831,14 +1814,34 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, cons
     ColOut& o = out[r2];
     for (int64_t g = 0; g < nseg; ++g) {
       auto& us = seg_units[g];
-      // longest first; among units of one length the first units of their blocks, then the second ones, ..., so that
-      // the units of one block fall on different lanes (or batches)
+      // the off-diagonal units longest first; among units of one length the first units of their blocks, then the
+      // second ones, ..., so that the units of one block fall on different lanes (or batches)
       std::stable_sort(us.begin(), us.end(), [](const Unit& x, const Unit& y) {
         return x.pr.size() != y.pr.size() ? x.pr.size() > y.pr.size() : x.j < y.j;
       });
       o.items.push_back(make_int4((int32_t)r2, (int32_t)(rptr[r2] + bnd[g]), (int32_t)(bnd[g + 1] - bnd[g]), (int32_t)nseg));
-      o.nbat.push_back((int32_t)((us.size() + 31) / 32));
-      o.nunits += (int64_t)us.size();
+      o.nbat.push_back((int32_t)((us.size() + 31) / 32) + 1);
+      o.nunits += (int64_t)us.size() + 32;
+      // the item's first batch: the diagonal block's pairs (c2, c2), the item's visits cut into 32 runs, one per lane
+      // (the kernel sums the lanes' blocks over the warp)
+      {
+        const int64_t n = bnd[g + 1] - bnd[g];
+        const int32_t iters = (int32_t)((n + 31) / 32);
+        o.bat.push_back(make_int2((int32_t)o.pairs.size(), iters));
+        for (int L = 0; L < 32; ++L)
+          o.lane.push_back((uint32_t)(col_h[r2] - 6) | ((uint32_t)((L + 1) * n / 32 - L * n / 32) << 16) | 0x80000000u);
+        for (int32_t it = 0; it < iters; ++it)
+          for (int L = 0; L < 32; ++L) {
+            const int64_t lo = L * n / 32, hi = (L + 1) * n / 32;
+            uint32_t code = 0u;
+            if (lo + it < hi) {
+              const int64_t v = lo + it;
+              const int32_t c2 = rentry[rptr[r2] + bnd[g] + v];
+              code = (uint32_t)v | ((uint32_t)(c2 - eptr[entry_elim[c2]]) << 16);
+            }
+            o.pairs.push_back(code);
+          }
+      }
       // batches of 32 consecutive units: a lane per unit, as many iterations as the batch's first (longest) unit
       for (size_t b0 = 0; b0 < us.size(); b0 += 32) {
         const int32_t iters = (int32_t)us[b0].pr.size();
@@ -2443,7 +2446,9 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
   // the column-owned schedule reads C with 16-byte loads (C_data on a 16-byte boundary, as the device allocators give)
   const bool c16 = (reinterpret_cast<uintptr_t>(C) & 31) == 0;   // 32-byte loads of C
   const bool batch = P->nprob > 0 && !dense;
-  const bool use_stage = P->fast36 && (P->kernel == 5 || batch) && !dense && P->stage_ok && c16 && (!s_r || P->S_rowval.p);
+  // a batch runs the column-owned schedule unless the block-owned pair lists are chosen (both keep per-problem failure)
+  const bool use_stage = P->fast36 && (P->kernel == 5 || (batch && P->kernel != 1)) && !dense && P->stage_ok && c16 &&
+                         (!s_r || P->S_rowval.p);
   const int32_t* poc = batch ? P->prob_of_cam.as<int32_t>() : nullptr;
   long long* pf = batch ? P->prob_fail.as<long long>() : nullptr;
   if (batch) {
@@ -3036,7 +3041,7 @@ int bls_schur_plan_phase2_kernel(bls_schur_plan* P, int dtype, int dense, int sc
   if (!P || !buf || cap < 1 || (dtype != BLS_F64 && dtype != BLS_F32)) return BLS_EINVAL;
   const std::string t = dtype == BLS_F32 ? "<float>" : "<double>";
   std::string name;
-  if (P->fast36 && (P->kernel == 5 || P->nprob > 0) && !dense && P->stage_ok) name = "k_stage36" + t;
+  if (P->fast36 && (P->kernel == 5 || (P->nprob > 0 && P->kernel != 1)) && !dense && P->stage_ok) name = "k_stage36" + t;
   else if (P->fast36 && P->nprob > 0 && !dense) name = "k_pairs36" + t;
   else if (P->fast36 && P->kernel == 0) name = std::string("k_columns36") + t;
   else if (P->fast36 && P->kernel == 3 && !dense && !scaled && P->tiles_ok) name = "k_tiles36" + t;
@@ -3150,3 +3155,4 @@ int bls_scatter_copy(bls_ctx* ctx, int dtype, void* dest, const void* src, const
 }
 
 }  // extern "C"
+

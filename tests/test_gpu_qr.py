@@ -331,9 +331,9 @@ def test_prepare_scale_bit_identical(bls):
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "mixed"])
 def test_bulk_staging_matches_element_staging(bls, dtype):
     """The table kernels stage each table with one bulk (TMA) copy per contiguous span by default; element-wise
-    staging (the other mode) must give bit-identical factored tables, residual, J~'J~, J~'r~, diagonal blocks and
-    assembled Hessian, on the scaled QR scene and on a table buffer offset by one element from a 16-byte boundary
-    (which falls back to element staging)."""
+    staging (the other mode) must give bit-identical factored tables and residual, and the same J~'J~, J~'r~,
+    diagonal blocks and assembled Hessian up to the order of their atomic sums, on the scaled QR scene and on a table
+    buffer offset by one element from a 16-byte boundary (which falls back to element staging)."""
     spec, p, o, _ = _qr_scene(bls)
     j = p.structure
     pat = bls.build_schur_pattern(j.schur, bls.free_block_pairs(j))
@@ -353,6 +353,14 @@ def test_bulk_staging_matches_element_staging(bls, dtype):
         bls.reduced_diagonal_blocks(D, ws)
         E, Cd, R, b = bls.assemble_hessian(J, ws)
         outs.append([t.double().cpu().numpy().copy() for t in (ws.factored, ws.fres, S, g, D, E, Cd, R, b)])
+    # the factored tables and their residual come from each table's own staged copy: bit-identical; the Gram,
+    # diagonal-block and assembly outputs add per-table contributions with atomics, whose order varies from run to run:
+    # equal to a few units in the last place
+    names = ("factored", "fres", "S", "g", "D", "E", "C", "R", "b")
+    tol = 1e-14 if dtype == torch.float64 else 1e-6
     for other in outs[1:]:
-        for a, b_ in zip(outs[0], other):
-            assert np.array_equal(a, b_)
+        for name, a, b_ in zip(names, outs[0], other):
+            if name in ("factored", "fres"):
+                assert np.array_equal(a, b_), name
+            else:
+                assert np.linalg.norm(a - b_) <= tol * np.linalg.norm(a), name
