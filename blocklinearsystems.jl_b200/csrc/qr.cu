@@ -144,37 +144,6 @@ __device__ __forceinline__ double col_scale(const double* s, int j, int t, int n
   return 1.0;
 }
 
-// I - tau_k v_k v_k' for k = 0, 1, 2 (v_k = [1; A[ce + k][k+1:]], tau in FP64) applied in turn to column y of M <= MM
-// rows, held in registers: the same operations in the same order as applying each reflector to the column in shared
-// memory (v'y in four partial sums over the rows after k, the rows left over added to the first; the update in the
-// storage type), with one read and one write of the column instead of three of each.
-template <class T, int MM>
-__device__ __forceinline__ void apply3_registers(T* yp, const T* __restrict__ V, int M, double tau0, double tau1, double tau2) {
-  T y[MM];
-#pragma unroll
-  for (int i = 0; i < MM; ++i) y[i] = i < M ? yp[i] : T(0);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const T* col = V + k * M;
-    const int lim = k + 1 + ((M - k - 1) & ~3);   // rows k + 1 .. lim - 1 go to the four partial sums
-    T p[4] = {y[k], T(0), T(0), T(0)};
-#pragma unroll
-    for (int i = k + 1; i < MM; ++i)
-      if (i < M) {
-        if (i < lim) p[(i - k - 1) & 3] += col[i] * y[i];
-        else p[0] += col[i] * y[i];
-      }
-    const T sj = T((double)((p[0] + p[1]) + (p[2] + p[3])) * (k == 0 ? tau0 : k == 1 ? tau1 : tau2));
-    y[k] = y[k] - sj;
-#pragma unroll
-    for (int i = k + 1; i < MM; ++i)
-      if (i < M) y[i] = y[i] - sj * col[i];
-  }
-#pragma unroll
-  for (int i = 0; i < MM; ++i)
-    if (i < M) yp[i] = y[i];
-}
-
 // qr_table! for the listed eliminated tables, one warp per table; `shT` holds the table (M x C, column-major) and
 // the FP64 residual (M). Tables are assigned by `tables[blockIdx.x * warps + warp]`.
 template <class T>
@@ -264,11 +233,6 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
   }
   __syncwarp();
   const double tol = (double)M * eps_of<T>();
-  // Point tables (three eliminated columns, at most 32 rows): the three reflectors are formed first (each applied at
-  // once to the later eliminated columns and the residual), then applied to each retained column together, from
-  // registers. Other tables apply each reflector to every column in turn, in shared memory. Both give the same values.
-  const bool three = de == 3 && M <= 32;
-  double tau0 = 0.0, tau1 = 0.0, tau2 = 0.0;
   for (int k = 0; k < de; ++k) {
     T* col = A + (ce + k) * M;
     double s_top = 0.0, s_sub = 0.0;
@@ -292,14 +256,8 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
     for (int i = k + 1 + lane; i < M; i += 32) col[i] = T((double)col[i] * scale);
     __syncwarp();
     if (lane == 0) col[k] = T(beta);
-    if (three) {
-      if (k == 0) tau0 = tau;
-      else if (k == 1) tau1 = tau;
-      else tau2 = tau;
-    }
-    // apply I - tau v v' (v = [1; col[k+1:]]) to every column outside the eliminated columns ce..ce+k (to the later
-    // eliminated columns only in the three-reflector form)
-    for (int j = three ? ce + k + 1 + lane : lane; j < C; j += 32) {
+    // apply I - tau v v' (v = [1; col[k+1:]]) to every column outside the eliminated columns ce..ce+k
+    for (int j = lane; j < C; j += 32) {
       if (j >= ce && j <= ce + k) continue;
       T* y = A + j * M;
       // v'y in four independent partial sums (the FMA chain is the latency of this loop), in the storage type: the
@@ -326,20 +284,7 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
     if (lane == 0) res[k] -= sr;
     for (int i = k + 1 + lane; i < M; i += 32) res[i] -= sr * (double)col[i];
     __syncwarp();
-    if (!three) {
-      for (int i = k + 1 + lane; i < M; i += 32) col[i] = T(0);
-      __syncwarp();
-    }
-  }
-  if (three) {
-    const T* V = A + ce * M;
-    for (int j = lane; j < ce; j += 32) {
-      if (M <= 16) apply3_registers<T, 16>(A + j * M, V, M, tau0, tau1, tau2);
-      else apply3_registers<T, 32>(A + j * M, V, M, tau0, tau1, tau2);
-    }
-    __syncwarp();
-    for (int k = 0; k < 3; ++k)
-      for (int i = k + 1 + lane; i < M; i += 32) A[(ce + k) * M + i] = T(0);
+    for (int i = k + 1 + lane; i < M; i += 32) col[i] = T(0);
     __syncwarp();
   }
   for (int i = lane; i < M * C; i += 32) F[off + i] = A[i];
