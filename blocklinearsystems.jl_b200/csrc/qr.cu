@@ -51,6 +51,7 @@ struct QRPlan {
   struct TableClass {
     DevBuf tables;
     int64_t n = 0, bytes_f64 = 0, bytes_f32 = 0;
+    int64_t maxc = 0;   // the widest table's column count (the factorisation's lanes per table follow it)
   };
   TableClass classes[8], gram_classes[8];
   // per table, per pair (u1 <= u2) of its entries in the order u2 outer, u1 inner: the S block it adds to
@@ -99,6 +100,12 @@ static std::vector<int32_t> q32(const int64_t* a, int64_t n, const char* what) {
 static int warps_per_cta(int64_t warp_bytes) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(QR_MAX_WARPS, QR_SMEM_LIMIT / std::max<int64_t>(warp_bytes, 1)));
 }
+// Tables per CTA of the factorisation with G lanes per table: whole warps (32 / G tables each), up to QR_MAX_WARPS
+// within the shared-memory limit; 0 when not even one warp's tables fit.
+static int tables_per_cta(int64_t table_bytes, int G) {
+  const int64_t per_warp = 32 / G, fit = QR_SMEM_LIMIT / std::max<int64_t>(table_bytes, 1);
+  return (int)(std::min<int64_t>(QR_MAX_WARPS, fit / per_warp) * per_warp);
+}
 
 static void set_smem(const void* kernel, size_t bytes) {
   if (bytes > 48 * 1024) BLS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -131,6 +138,13 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// the sum over a group of G lanes (G a power of two up to 32, the group's lanes in gmask)
+template <int G>
+__device__ __forceinline__ double group_sum(double v, unsigned gmask) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+  return v;
+}
 
 // Scale of table column j (the variable it belongs to): s over all variables [s_r; s_e]; 1 when s is null.
 __device__ __forceinline__ double col_scale(const double* s, int j, int t, int ncols_f, int de, const int32_t* t_ptr, const int32_t* u_col,
@@ -144,9 +158,11 @@ __device__ __forceinline__ double col_scale(const double* s, int j, int t, int n
   return 1.0;
 }
 
-// qr_table! for the listed eliminated tables, one warp per table; `shT` holds the table (M x C, column-major) and
-// the FP64 residual (M). Tables are assigned by `tables[blockIdx.x * warps + warp]`.
-template <class T>
+// qr_table! for the listed eliminated tables, a group of G lanes per table (G = 8 or 16 for narrow tables, so that a
+// warp factors several tables at once and its lanes are not left idle over a few columns; 32 otherwise); the group's
+// shared-memory region holds the table (M x C, column-major) and the FP64 residual (M). Tables are assigned by
+// `tables[blockIdx.x * groups + group]`.
+template <class T, int G>
 __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, int warp_bytes, const int32_t* __restrict__ tables,
                                                   const int32_t* __restrict__ t_rows,
                                                   const int32_t* __restrict__ t_cols, const int64_t* __restrict__ t_raw,
@@ -159,15 +175,18 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
                                                   const T* __restrict__ Rw_end, const double* __restrict__ Rr_end, int bulk,
                                                   long long* st) {
   extern __shared__ __align__(16) unsigned char qsm_all[];
-  const int64_t wi = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  // a group of G lanes per table (G = 8, 16 or 32, a warp holding 32 / G groups); gmask names the group's lanes
+  const int grp = threadIdx.x / G;
+  const int64_t wi = blockIdx.x * (int64_t)(blockDim.x / G) + grp;
   if (wi >= ntab) return;
   if (st[1] != QNONE) return;
-  const int lane = threadIdx.x & 31;
-  unsigned char* qsm = qsm_all + (size_t)(threadIdx.x >> 5) * warp_bytes;
+  const int lane = threadIdx.x & (G - 1);
+  const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (threadIdx.x & 31 & ~(G - 1)));
+  unsigned char* qsm = qsm_all + (size_t)grp * warp_bytes;
   const int t = tables[wi];
   const int M = t_rows[t], C = t_cols[t] - 1, de = e_dims[t], me = M - de, ce = C - de;
   const int64_t off = t_raw[t], rq = t_res[t];
-  // the warp's region: its mbarrier, then the FP64 residual and the M x C table, each with 32 bytes of room for the
+  // the group's region: its mbarrier, then the FP64 residual and the M x C table, each with 32 bytes of room for the
   // 16-byte alignment of a bulk copy
   uint64_t* bar = reinterpret_cast<uint64_t*>(qsm);
   unsigned char* rbase = qsm + 16;
@@ -175,7 +194,7 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
   double* res;
   T* A;
   if (bulk) {
-    // the table and its residual are contiguous: one bulk copy each (TMA), completed on the warp's mbarrier
+    // the table and its residual are contiguous: one bulk copy each (TMA), completed on the group's mbarrier
     const Span sa = span_of(Rw + off, (int64_t)M * C, Rw_end), sr = span_of(Rr + rq, (int64_t)M, Rr_end);
     if (lane == 0) {
       mbar_init(bar, 1);
@@ -186,63 +205,63 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
     }
     A = span_first(reinterpret_cast<T*>(abase), sa);
     res = span_first(reinterpret_cast<double*>(rbase), sr);
-    __syncwarp();
+    __syncwarp(gmask);
     if (!mbar_wait(bar, 0)) {
       if (lane == 0) atomicExch(reinterpret_cast<unsigned long long*>(st + 2), 1ull);   // a copy that did not land: fault
       mbar_wait(bar, 0);                                                               // drain (bounded), then leave
       return;
     }
-    __syncwarp();
+    __syncwarp(gmask);
   } else {
     res = reinterpret_cast<double*>(rbase);
     A = reinterpret_cast<T*>(abase);
     // element copies (coalesced: the table is contiguous; all of a lane's copies in flight at once)
-    for (int i = lane; i < M * C; i += 32) cp_async_elem(A + i, Rw + off + i);
-    for (int i = lane; i < M; i += 32) cp_async_elem(res + i, Rr + rq + i);
+    for (int i = lane; i < M * C; i += G) cp_async_elem(A + i, Rw + off + i);
+    for (int i = lane; i < M; i += G) cp_async_elem(res + i, Rr + rq + i);
     cp_async_wait_all();
-    __syncwarp();
+    __syncwarp(gmask);
   }
   // the reference's non-finite test (x - x is NaN for Inf / NaN) and the conditioning scales, in shared memory
   bool bad = false;
-  for (int i = lane; i < M * C; i += 32) {
+  for (int i = lane; i < M * C; i += G) {
     T x = A[i];
     bad |= isnan((double)(x - x));
     if (s) A[i] = T((double)x * col_scale(s, i / M, t, C, de, t_ptr, u_col, u_ret, boff_r, r_dims, boff_e, nr));
   }
-  for (int i = lane; i < M; i += 32) {
+  for (int i = lane; i < M; i += G) {
     const double x = res[i];
     bad |= isnan(x - x);
   }
-  bad = __any_sync(0xffffffffu, bad);
+  bad = __any_sync(gmask, bad);
   if (bad) {
     if (lane == 0) atomicMin(st, (long long)t);
     return;
   }
-  __syncwarp();
+  __syncwarp(gmask);
   // damping rows: zero, then sqrt(lambda * scaling_e) * s_e on their diagonal (formed in FP64)
-  for (int i = lane; i < de * C; i += 32) {
+  for (int i = lane; i < de * C; i += G) {
     const int j = i / de, r = me + (i - j * de);
     A[j * M + r] = T(0);
   }
-  for (int l = lane; l < de; l += 32) res[me + l] = 0.0;
-  __syncwarp();
-  for (int l = lane; l < de; l += 32) {
+  for (int l = lane; l < de; l += G) res[me + l] = 0.0;
+  __syncwarp(gmask);
+  for (int l = lane; l < de; l += G) {
     const int so = boff_e[t];
     const double sv = s ? s[nr + so + l] : 1.0;
     A[(ce + l) * M + me + l] = T(sqrt(lambda * sc_e[so + l]) * sv);
   }
-  __syncwarp();
+  __syncwarp(gmask);
   const double tol = (double)M * eps_of<T>();
   for (int k = 0; k < de; ++k) {
     T* col = A + (ce + k) * M;
     double s_top = 0.0, s_sub = 0.0;
-    for (int i = lane; i < M; i += 32) {
+    for (int i = lane; i < M; i += G) {
       const double v = (double)col[i];
       if (i < k) s_top += v * v;
       else s_sub += v * v;
     }
-    s_top = warp_sum(s_top);
-    s_sub = warp_sum(s_sub);
+    s_top = group_sum<G>(s_top, gmask);
+    s_sub = group_sum<G>(s_sub, gmask);
     const double nrm = sqrt(s_sub), full = sqrt(s_top + s_sub);
     const double a = (double)col[k];
     const double beta = a >= 0.0 ? -nrm : nrm;
@@ -252,12 +271,12 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
     }
     const double scale = 1.0 / (a - beta);
     const double tau = (beta - a) / beta;
-    __syncwarp();
-    for (int i = k + 1 + lane; i < M; i += 32) col[i] = T((double)col[i] * scale);
-    __syncwarp();
+    __syncwarp(gmask);
+    for (int i = k + 1 + lane; i < M; i += G) col[i] = T((double)col[i] * scale);
+    __syncwarp(gmask);
     if (lane == 0) col[k] = T(beta);
     // apply I - tau v v' (v = [1; col[k+1:]]) to every column outside the eliminated columns ce..ce+k
-    for (int j = lane; j < C; j += 32) {
+    for (int j = lane; j < C; j += G) {
       if (j >= ce && j <= ce + k) continue;
       T* y = A + j * M;
       // v'y in four independent partial sums (the FMA chain is the latency of this loop), in the storage type: the
@@ -277,18 +296,18 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
     }
     // and to the FP64 residual
     double sr = 0.0;
-    for (int i = k + 1 + lane; i < M; i += 32) sr += (double)col[i] * res[i];
-    sr = warp_sum(sr) + res[k];
+    for (int i = k + 1 + lane; i < M; i += G) sr += (double)col[i] * res[i];
+    sr = group_sum<G>(sr, gmask) + res[k];
     sr *= tau;
-    __syncwarp();
+    __syncwarp(gmask);
     if (lane == 0) res[k] -= sr;
-    for (int i = k + 1 + lane; i < M; i += 32) res[i] -= sr * (double)col[i];
-    __syncwarp();
-    for (int i = k + 1 + lane; i < M; i += 32) col[i] = T(0);
-    __syncwarp();
+    for (int i = k + 1 + lane; i < M; i += G) res[i] -= sr * (double)col[i];
+    __syncwarp(gmask);
+    for (int i = k + 1 + lane; i < M; i += G) col[i] = T(0);
+    __syncwarp(gmask);
   }
-  for (int i = lane; i < M * C; i += 32) F[off + i] = A[i];
-  for (int i = lane; i < M; i += 32) Fr[rq + i] = res[i];
+  for (int i = lane; i < M * C; i += G) F[off + i] = A[i];
+  for (int i = lane; i < M; i += G) Fr[rq + i] = res[i];
 }
 
 // Free tables are copied (scaled when conditioned): copy_table! (src/qr_reduction.jl:183-185)
@@ -1027,6 +1046,7 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
       cls_tables[c].push_back((int32_t)t);
       P->classes[c].bytes_f64 = std::max(P->classes[c].bytes_f64, b64);
       P->classes[c].bytes_f32 = std::max(P->classes[c].bytes_f32, b32);
+      P->classes[c].maxc = std::max(P->classes[c].maxc, C);
     }
     // the warp's mbarrier, the residual rows and the retained columns: at stride M from one bulk copy (plus 32 bytes
     // of alignment room), or at the odd stride n | 1 from element copies; the larger of the two
@@ -1237,14 +1257,25 @@ static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr,
     const auto& k = P->classes[c];
     if (k.n == 0) continue;
     const int64_t wb = ((std::is_same<T, double>::value ? k.bytes_f64 : k.bytes_f32) + 15) & ~int64_t(15);
-    const int wpc = warps_per_cta(wb);
-    const size_t smem = (size_t)(wb * wpc);
-    set_smem(reinterpret_cast<const void*>(k_qr_tables<T>), smem);
-    k_qr_tables<T><<<(unsigned)((k.n + wpc - 1) / wpc), 32 * wpc, smem, s>>>(
-        k.n, (int)wb, k.tables.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(),
-        P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->boff_r.as<int32_t>(), P->r_dims.as<int32_t>(),
-        P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), (int)P->nr, Rw, Rr, sc_e, lambda, sv, F, Fr, Rw + P->raw_len, Rr + P->res_len,
-        bulk ? 1 : 0, st);
+    // lanes per table from the widest table of the class: a lane per column in the reflector updates
+    int G = k.maxc <= 24 ? 8 : k.maxc <= 48 ? 16 : 32;
+    int tpc = tables_per_cta(wb, G);
+    if (tpc == 0) {
+      G = 32;
+      tpc = warps_per_cta(wb);
+    }
+    const size_t smem = (size_t)(wb * tpc);
+    auto launch = [&](auto kern) {
+      set_smem(reinterpret_cast<const void*>(kern), smem);
+      kern<<<(unsigned)((k.n + tpc - 1) / tpc), tpc * G, smem, s>>>(
+          k.n, (int)wb, k.tables.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(),
+          P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->boff_r.as<int32_t>(), P->r_dims.as<int32_t>(),
+          P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), (int)P->nr, Rw, Rr, sc_e, lambda, sv, F, Fr, Rw + P->raw_len, Rr + P->res_len,
+          bulk ? 1 : 0, st);
+    };
+    if (G == 8) launch(k_qr_tables<T, 8>);
+    else if (G == 16) launch(k_qr_tables<T, 16>);
+    else launch(k_qr_tables<T, 32>);
     P->launches += 1;
   }
   if (P->ntables > P->neblocks) {
