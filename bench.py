@@ -1015,8 +1015,11 @@ def cpu_baseline(v, seconds: float = 10.0, steps: int | None = None, warmup: int
 
 def reference_line(args, world: int, base: dict, config: dict, metric: str = METRIC, unit: str = "obs/s",
                    dtype: str = "f64") -> dict:
+    # the time of one step of the workload at the measured rate (observations per step, or one solve)
+    per_step = config.get("observations", 1) if unit == "obs/s" else 1
+    ms = 1e3 * per_step / base["value"] if base["value"] else None
     return {"impl": "reference", "metric": metric, "value": base["value"], "unit": unit, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
             "data": "synthetic (seeded scene generator)", "config": config,
             "note": "reference algorithm restated in C++ (the oracle; Julia is unavailable); inputs read from .npy files "
                     "written by an untimed child process",
