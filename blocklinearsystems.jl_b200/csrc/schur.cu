@@ -73,12 +73,16 @@ struct SchurPlan {
   // {first pair, iterations} (stg_bat), per batch and lane {the block's row offset in the column | unit length << 16 |
   // (the block's only unit in the item) << 31} (stg_lane); pairs batch by batch, iteration-major (lane fastest),
   // {visit within the item | c1's index within its point << 16}, 0 past a lane's unit (stg_pairs).
-  static constexpr int STAGE_NT = 256;
+  // One schedule per storage type (index 0 FP32, 1 FP64): FP32 items fit two 256-thread CTAs per SM, FP64 items (half
+  // the visits) two 128-thread CTAs.
   bool stage_ok = false;
   int stage_unit = 16;
-  int64_t stage_items = 0, stage_max_nv = 0, stage_units = 0, stage_batches = 0, stage_slots = 0;
+  struct StageSchedule {
+    int64_t items = 0, max_nv = 0, units = 0, batches = 0, slots = 0;
+    DevBuf stg_items, stg_ibat, stg_bat, stg_lane, stg_pairs;
+  };
+  StageSchedule stage[2];
   int stage_grid[2] = {0, 0};   // persistent CTAs of k_stage36 (FP32, FP64): resident blocks per SM x SMs
-  DevBuf stg_items, stg_ibat, stg_bat, stg_lane, stg_pairs;
   DevBuf EZ;   // per point E' = s_e E^-1 s_e (9, column-major) and z' = s_e .* z (3), FP64, for k_stage36
   // a batch of independent problems in one plan (bls_schur_plan_set_problems): per problem the lowest failing point
   // (global index, NONE if none), per point and per camera its problem; a failing problem skips its own phase 2 only
@@ -1452,12 +1456,15 @@ __global__ void k_gather(T* __restrict__ dest, const T* __restrict__ src, const 
 // transposed (E^-1 is symmetric).
 template <class T>
 __host__ __device__ constexpr int stage_wr() { return sizeof(T) == 4 ? 20 : 18; }   // W record stride (16-byte multiple)
+// threads per CTA of k_stage36: 256 in FP32 (two CTAs per SM at 128 registers), 128 in FP64 (two per SM at ~200)
+template <class T>
+__host__ __device__ constexpr int stage_nt() { return sizeof(T) == 4 ? 256 : 128; }
 template <class T>
 static size_t stage_smem(int64_t max_h, int64_t max_nv) {
   const size_t tile = ((size_t)6 * max_h * sizeof(T) + 15) & ~size_t(15);
   const size_t w = (size_t)max_nv * stage_wr<T>() * sizeof(T);
   const size_t p0 = ((size_t)max_nv * 4 + 15) & ~size_t(15);
-  return tile + w + p0 + (SchurPlan::STAGE_NT / 32) * 6 * sizeof(double);
+  return tile + w + p0 + (stage_nt<T>() / 32) * 6 * sizeof(double);
 }
 
 // 18 entries of one coupling block of C, read with 32-byte loads from the 32-byte boundary at or below the block (C on
@@ -1544,14 +1551,14 @@ __device__ __forceinline__ void load_w18(const double* w, double* b) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k_stage36(
+__global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
     const int4* __restrict__ items, const int32_t* __restrict__ ibat, const int2* __restrict__ bat, const uint32_t* __restrict__ lane_rec,
     const uint32_t* __restrict__ pairs,
     const int2* __restrict__ vis_rec, const int32_t* __restrict__ col_h, const int64_t* __restrict__ col_base, int64_t ncoup,
     const T* __restrict__ C, const double* __restrict__ EZ, const double* __restrict__ s_r, T* __restrict__ S, double* __restrict__ g,
     const Status* __restrict__ st, const int32_t* __restrict__ prob_of_cam, const long long* __restrict__ prob_fail, int64_t nitems,
     unsigned long long* __restrict__ queue, const int32_t* __restrict__ S_rowval) {
-  constexpr int NT = SchurPlan::STAGE_NT;
+  constexpr int NT = stage_nt<T>();
   constexpr int WR = stage_wr<T>();
   using Raw = typename RawOf<T>::type;
   extern __shared__ __align__(16) unsigned char sm[];
@@ -1714,11 +1721,11 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
   }
 }
 
-// The column-owned schedule of k_stage36 (SchurPlan::stg_*), from the plan's block-owned pair lists (pairs of a
-// column grouped by block slot, each block's in visit order). An item is a run of one block column's visits: its
-// shared memory holds the column's S tile (6 H entries) and per visit W = E' C_c2 (18 entries) and the visit point's
-// first coupling; in FP64 this must fit STAGE_BUDGET bytes, so a column with more visits is cut into several items
-// (their tiles are added to S with atomics). Items stay in column order: neighbouring columns read the couplings of
+// One column-owned schedule of k_stage36 (SchurPlan::stage[sd], sd 0 for FP32 and 1 for FP64), from the structure:
+// each column's pairs grouped by block slot, each block's in visit order. An item is a run of one block column's
+// visits: its shared memory holds the column's S tile (6 H entries) and per visit W = E' C_c2 (18 entries) and the
+// visit point's first coupling; sized in FP64 bytes this must fit the schedule's STAGE_BUDGET, so a column with more
+// visits is cut into several items (their tiles are added to S with atomics). Items stay in column order: neighbouring columns read the couplings of
 // overlapping sets of points, which then stay in L2 while the columns in flight move along the cameras.
 // A block's pairs of one item are cut into units of at most stage_unit pairs, except the diagonal block's, which make
 // the item's first batch (the item's visits cut into 32 runs, one per lane). The item's other units, longest first,
@@ -1728,11 +1735,14 @@ __global__ void __launch_bounds__(SchurPlan::STAGE_NT, sizeof(T) == 4 ? 2 : 1) k
 // finish the item together. Among units of one length the first units of their blocks come first, then the second
 // ones, so that the units of one block fall on different lanes. A batch's pairs are stored iteration by iteration, 32
 // codes (one per lane) each, so that a warp reads them as one 128-byte line per iteration.
-static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, const std::vector<int32_t>& rptr,
+static bool build_stage_schedule(SchurPlan* P, int sd, cudaStream_t s, int64_t nrb, const std::vector<int32_t>& rptr,
                                  const std::vector<int32_t>& rentry, const std::vector<int32_t>& entry_elim, const int64_t* eptr,
                                  const int64_t* eret, const std::vector<int64_t>& bcolptr, const std::vector<int64_t>& browval,
                                  const std::vector<int64_t>& brow_off, const std::vector<int64_t>& col_h) {
-  constexpr int64_t STAGE_BUDGET = 200 * 1024;
+  // the shared-memory budget of an item, sized in FP64 bytes (48 per tile row, 148 per visit): 200 KB for the FP32
+  // schedule (whose FP32 items then take about 110 KB, two 256-thread CTAs per SM), 96 KB for the FP64 one (two
+  // 128-thread CTAs per SM)
+  const int64_t STAGE_BUDGET = sd == 0 ? 200 * 1024 : 96 * 1024;
   const int U = P->stage_unit;
   struct ColOut {
     std::vector<int4> items;
@@ -1747,7 +1757,7 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, cons
   int64_t max_h = 0;
   for (int64_t r2 = 0; r2 < nrb; ++r2) max_h = std::max<int64_t>(max_h, col_h[r2]);
   const int64_t vcap = (STAGE_BUDGET - 48 * max_h - 2048) / 148;
-  if (vcap < 32 || max_h > 65535) return;
+  if (vcap < 32 || max_h > 65535) return false;
   int bad = 0;
 #pragma omp parallel for schedule(dynamic, 8) reduction(| : bad)
   for (int64_t r2 = 0; r2 < nrb; ++r2) {
@@ -1862,7 +1872,7 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, cons
       }
     }
   }
-  if (bad) return;
+  if (bad) return false;
   int64_t nitems = 0, nbat = 0, nslots = 0, max_nv = 0, nunits = 0;
   for (int64_t r2 = 0; r2 < nrb; ++r2) {
     nitems += (int64_t)out[r2].items.size();
@@ -1871,7 +1881,7 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, cons
     nunits += out[r2].nunits;
     for (const int4& it : out[r2].items) max_nv = std::max<int64_t>(max_nv, it.z);
   }
-  if (nslots >= INT32_MAX || nbat >= INT32_MAX / 32 || nitems >= INT32_MAX) return;
+  if (nslots >= INT32_MAX || nbat >= INT32_MAX / 32 || nitems >= INT32_MAX) return false;
   std::vector<int4> items;
   std::vector<int32_t> ibat;
   std::vector<int2> bat;
@@ -1900,17 +1910,18 @@ static void build_stage_schedule(SchurPlan* P, cudaStream_t s, int64_t nrb, cons
   }
   ibat.push_back((int32_t)bat.size());
   pairs.resize(pairs.size() + 32, 0u);   // the kernel's read-ahead of the next iteration's codes stays inside the array
-  upload(P->stg_items, items, s);
-  upload(P->stg_ibat, ibat, s);
-  upload(P->stg_bat, bat, s);
-  upload(P->stg_lane, lane, s);
-  upload(P->stg_pairs, pairs, s);
-  P->stage_items = nitems;
-  P->stage_units = nunits;
-  P->stage_batches = nbat;
-  P->stage_slots = nslots;
-  P->stage_max_nv = max_nv;
-  P->stage_ok = true;
+  SchurPlan::StageSchedule& S = P->stage[sd];
+  upload(S.stg_items, items, s);
+  upload(S.stg_ibat, ibat, s);
+  upload(S.stg_bat, bat, s);
+  upload(S.stg_lane, lane, s);
+  upload(S.stg_pairs, pairs, s);
+  S.items = nitems;
+  S.units = nunits;
+  S.batches = nbat;
+  S.slots = nslots;
+  S.max_nv = max_nv;
+  return true;
 }
 
 static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
@@ -2143,9 +2154,13 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
     }
   }
   // the column-owned schedule (k_stage36), sparse S only
-  if (P->fast36 && P->has_sparse)
-    build_stage_schedule(P.get(), s, nrb, rptr, rentry, entry_elim, d->eliminated_ptr, d->entry_retained, bcolptr, browval,
-                         brow_off, col_h);
+  if (P->fast36 && P->has_sparse) {
+    bool ok = true;
+    for (int sd = 0; sd < 2 && ok; ++sd)
+      ok = build_stage_schedule(P.get(), sd, s, nrb, rptr, rentry, entry_elim, d->eliminated_ptr, d->entry_retained, bcolptr,
+                                browval, brow_off, col_h);
+    P->stage_ok = ok;
+  }
   // staged work items for the host-buffer reduction: stage j holds points [stage_pt[j], stage_pt[j + 1]); a block's
   // pairs ascend in point within its slot, so its pairs of one stage are a contiguous run, cut into items of at most
   // PAIR_CHUNK pairs (solo when the run makes one item)
@@ -2284,7 +2299,7 @@ static SchurPlan* plan_create(bls_ctx* ctx, const bls_schur_plan_desc* d) {
 static int64_t plan_bytes(const SchurPlan* P) {
   const DevBuf* bufs[] = {&P->r_dims, &P->boffsets_r, &P->e_dims, &P->boffsets_e, &P->eoffsets, &P->eliminated_ptr, &P->entry_retained,
                           &P->coffsets, &P->entry_eliminated, &P->retained_ptr, &P->retained_entry, &P->block_r1, &P->block_r2,
-                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h, &P->stg_items, &P->stg_ibat, &P->stg_bat, &P->stg_lane, &P->stg_pairs, &P->EZ,
+                          &P->block_base_sparse, &P->block_stride_sparse, &P->block_base_dense, &P->pair_c1, &P->pair_c2, &P->pair_packed, &P->pt_rec, &P->Einv12, &P->vis_rec, &P->vis_base, &P->vis_off, &P->col_base, &P->col_h, &P->stage[0].stg_items, &P->stage[0].stg_ibat, &P->stage[0].stg_bat, &P->stage[0].stg_lane, &P->stage[0].stg_pairs, &P->stage[1].stg_items, &P->stage[1].stg_ibat, &P->stage[1].stg_bat, &P->stage[1].stg_lane, &P->stage[1].stg_pairs, &P->EZ,
                           &P->item_block, &P->item_start, &P->item_info, &P->r_to_s, &P->diag_inds, &P->S_rowval, &P->S_col, &P->r_from, &P->S_colptr, &P->st_block, &P->st_start, &P->st_info, &P->h_E, &P->h_C, &P->h_R, &P->h_br, &P->h_be, &P->h_scr, &P->h_sce, &P->h_S, &P->h_g, &P->w_apply, &P->t_apply, &P->acc1,
                           &P->Einv64, &P->Einv32, &P->z, &P->status};
   int64_t b = 0;
@@ -2480,8 +2495,9 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
   if (use_stage) {
     k_g_init<<<grid_for(P->nr, 256), 256, 0, s>>>(g, b_r, s_r, P->nr, st, poc, pf);
     P->launches += 1;
-    if (P->stage_items > 0) {
-      const size_t smem = stage_smem<T>(P->max_col_h, P->stage_max_nv);
+    const SchurPlan::StageSchedule& SS = P->stage[sizeof(T) == 4 ? 0 : 1];
+    if (SS.items > 0) {
+      const size_t smem = stage_smem<T>(P->max_col_h, SS.max_nv);
       BLS_CUDA(cudaFuncSetAttribute(k_stage36<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       if (ev0) BLS_CUDA(cudaEventRecord(ev0, s));
       P->launches += 1;
@@ -2489,14 +2505,14 @@ static int reduce(SchurPlan* P, T* S, bool dense, double* g, const double* b_r, 
         int per_sm = 0, nsm = 0, dev = 0;
         BLS_CUDA(cudaGetDevice(&dev));
         BLS_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        BLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage36<T>, SchurPlan::STAGE_NT, smem));
+        BLS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage36<T>, stage_nt<T>(), smem));
         P->stage_grid[sizeof(T) == 4 ? 0 : 1] = std::max(1, per_sm) * nsm;
       }
-      const int64_t grid = std::min<int64_t>(P->stage_items, P->stage_grid[sizeof(T) == 4 ? 0 : 1]);
-      k_stage36<T><<<(unsigned)grid, SchurPlan::STAGE_NT, smem, s>>>(
-          P->stg_items.as<int4>(), P->stg_ibat.as<int32_t>(), P->stg_bat.as<int2>(), P->stg_lane.as<uint32_t>(), P->stg_pairs.as<uint32_t>(),
+      const int64_t grid = std::min<int64_t>(SS.items, P->stage_grid[sizeof(T) == 4 ? 0 : 1]);
+      k_stage36<T><<<(unsigned)grid, stage_nt<T>(), smem, s>>>(
+          SS.stg_items.as<int4>(), SS.stg_ibat.as<int32_t>(), SS.stg_bat.as<int2>(), SS.stg_lane.as<uint32_t>(), SS.stg_pairs.as<uint32_t>(),
           P->vis_rec.as<int2>(), P->col_h.as<int32_t>(), P->col_base.as<int64_t>(), P->ncoup, C, P->EZ.as<double>(), s_r, S, g, st,
-          poc, pf, P->stage_items,
+          poc, pf, SS.items,
           reinterpret_cast<unsigned long long*>(&st->pad), P->S_rowval.as<int32_t>());
       if (ev1) BLS_CUDA(cudaEventRecord(ev1, s));
     }
@@ -3024,11 +3040,13 @@ int bls_schur_plan_set_stage_unit(bls_schur_plan* P, int unit) {
     for (int64_t r = 0; r < nrb; ++r) bcolptr[r + 1] += bcolptr[r];
     const int old = P->stage_unit;
     P->stage_unit = unit;
-    P->stage_ok = false;
-    build_stage_schedule(P, s, nrb, rptr, rentry, entry_elim, eptr.data(), eret.data(), bcolptr, browval, brow_off, col_h);
-    if (!P->stage_ok) {
+    // each schedule is replaced only when its rebuild succeeds (a schedule with the old unit size stays valid)
+    bool ok = true;
+    for (int sd = 0; sd < 2; ++sd)
+      ok = build_stage_schedule(P, sd, s, nrb, rptr, rentry, entry_elim, eptr.data(), eret.data(), bcolptr, browval, brow_off,
+                                col_h) && ok;
+    if (!ok) {
       P->stage_unit = old;
-      P->stage_ok = true;
       throw Error(BLS_EUNSUPPORTED, "the schedule does not fit this unit size");
     }
     P->stage_grid[0] = P->stage_grid[1] = 0;
