@@ -190,6 +190,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     p = bls.scenes.hessian_problem(spec)
     st, pat = p.structure, p.pattern
     ws = bls.SchurReductionWorkspace(st, pat, device=dev.index)
+    if args.schedule:
+        ws.set_kernel(args.schedule)
     if args.stage_unit:
         ws.set_stage_unit(args.stage_unit)
     flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=dev)   # larger than the 126 MB L2
@@ -1078,6 +1080,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--stage-unit", type=int, default=None, help="pairs per unit of the column-owned schedule (default 16)")
+    ap.add_argument("--schedule", default=None, help="phase-2 schedule of the Schur workloads (default: the plan's, stage)")
     ap.add_argument("--write-fixture", default=None, help=argparse.SUPPRESS)   # the reference arm's untimed child
     args = ap.parse_args()
     if args.write_fixture:
