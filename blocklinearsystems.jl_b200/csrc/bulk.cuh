@@ -84,4 +84,30 @@ __device__ __forceinline__ T* span_first(T* dst16, const Span& s) {
   return reinterpret_cast<T*>(reinterpret_cast<char*>(dst16) + (s.src - s.lo));
 }
 
+// Shared -> global bulk copy (both 16-byte aligned, bytes a multiple of 16), in this thread's bulk group.
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)), "r"(bytes) : "memory");
+}
+
+// Store n elements from shared memory at src to global memory at dst, both at the same offset within a 16-byte chunk:
+// the aligned interior by one bulk copy, the ragged head and tail (under 16 bytes each) by plain stores, so nothing
+// outside [dst, dst + n) is written. One thread calls it, after every thread that wrote src has run
+// fence_proxy_async_shared() and a barrier with it; it returns once the copy has read src (so src may be reused or the
+// CTA may exit); the global writes complete before the kernel does.
+template <class T>
+__device__ __forceinline__ void span_store(T* dst, const T* src, int64_t n) {
+  const uintptr_t d0 = reinterpret_cast<uintptr_t>(dst), d1 = d0 + (uintptr_t)n * sizeof(T);
+  const uintptr_t lo = (d0 + 15) & ~uintptr_t(15), hi = d1 & ~uintptr_t(15);
+  const char* s = reinterpret_cast<const char*>(src);
+  if (hi <= lo) {
+    for (int64_t i = 0; i < n; ++i) dst[i] = src[i];
+    return;
+  }
+  for (uintptr_t a = d0; a < lo; a += sizeof(T)) *reinterpret_cast<T*>(a) = *reinterpret_cast<const T*>(s + (a - d0));
+  for (uintptr_t a = hi; a < d1; a += sizeof(T)) *reinterpret_cast<T*>(a) = *reinterpret_cast<const T*>(s + (a - d0));
+  bulk_s2g(reinterpret_cast<void*>(lo), s + (lo - d0), (uint32_t)(hi - lo));
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
 }  // namespace bls

@@ -5,23 +5,28 @@
 // :225-255), src/qr_reduced.jl (qr_backsubstitute_group! :24-93, accumulate_qr_entry! :375-405, reduced_normal_* :409-480,
 // reduced_diagonal_blocks! :484-512), layout src/schur_jacobian.jl:30-160.
 //
-// One warp per eliminated block's table: the table (M rows, C columns, column-major, contiguous in the raw storage) is
-// copied into shared memory with coalesced loads, checked for non-finite entries, damped, and factored there: for each
-// of the d_e eliminated columns the column norms, beta, tau and the reflector scaling are FP64 (warp reductions), and
-// the reflector is applied with lanes owning columns, each lane walking its column down the rows (a table's row count
-// M = m_e + d_e is odd whenever m_e is even, so the lanes' column strides hit distinct shared-memory banks). The
-// residual column goes through the same reflectors in FP64 (SP-B6 of the reference). With FP32 storage (the mixed
-// form) the table is FP32 and each reflector application is accumulated in FP64 and rounded once per entry.
+// A group of 8, 16 or 32 lanes per eliminated block's table: the table (M rows, C columns, column-major, contiguous in
+// the raw storage) is copied into shared memory by a bulk copy, checked for non-finite entries, damped, and factored
+// there. The d_e eliminated columns come first: for each, the column norms, beta, tau and the reflector scaling are FP64
+// (group reductions), and the reflector is applied to the later eliminated columns. For d_e <= 4 the d_e reflectors then
+// reach every retained column at once in compact form (y - V s with a = V'y and a d_e x d_e triangular recurrence for
+// s), a lane per column reading its column twice; larger blocks take the reflectors one at a time, lanes owning
+// columns. The residual column goes through the same reflectors in FP64 (SP-B6 of the reference). With FP32 storage
+// (the mixed form) the table and its column updates are FP32, the norms, tau and s FP64. The factored table goes back by
+// a bulk copy of its 16-byte-aligned interior.
 //
 // J~'J~, J~'r~ and the diagonal blocks come from one warp per table as well: the table's bottom rows (J~ of its
 // retained columns) and residual rows are staged in shared memory, every pair of the table's entries (u1 <= u2)
 // gives one d_r x d_r block, one lane per block column holding its FP64 dot products in registers, and the block is
 // added into S with one atomic add per entry (a table contributes to each S block at most once). Tables are grouped into shared-memory classes;
-// each class is one launch of up to four warps per CTA.
+// each class is one launch whose CTA size packs an SM's shared memory best, and the classes of one call run
+// concurrently on the plan's side streams.
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <cmath>
 #include <type_traits>
 
@@ -81,9 +86,18 @@ struct QRPlan {
   DevBuf status;
   long long* host_status = nullptr;
   int64_t launches = 0;
+  // side streams of the per-class launches (factorisation and Gram kernels; created at the first use): the classes
+  // run concurrently, so that one class's last wave overlaps the others' and small classes fill the SMs beside large
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
   ~QRPlan() {
     if (host_status) cudaFreeHost(host_status);
     if (ls_host) cudaFreeHost(ls_host);
+    for (int i = 0; i < 3; ++i) {
+      if (side[i]) cudaStreamDestroy(side[i]);
+      if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
   }
 };
 
@@ -102,13 +116,59 @@ static int warps_per_cta(int64_t warp_bytes) {
 }
 // Tables per CTA of the factorisation with G lanes per table: whole warps (32 / G tables each), up to QR_MAX_WARPS
 // within the shared-memory limit; 0 when not even one warp's tables fit.
-static int tables_per_cta(int64_t table_bytes, int G) {
-  const int64_t per_warp = 32 / G, fit = QR_SMEM_LIMIT / std::max<int64_t>(table_bytes, 1);
-  return (int)(std::min<int64_t>(QR_MAX_WARPS, fit / per_warp) * per_warp);
+// The warps of `kernel` that an SM's 64 K registers hold (cached per kernel).
+static int warp_cap(const void* kernel) {
+  static std::mutex mu;
+  static std::map<const void*, int> cap;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cap.find(kernel);
+  if (it != cap.end()) return it->second;
+  cudaFuncAttributes a;
+  BLS_CUDA(cudaFuncGetAttributes(&a, kernel));
+  const int regs = (std::max(a.numRegs, 1) + 7) / 8 * 8;
+  return cap[kernel] = std::max(1, std::min(64, 65536 / (regs * 32)));
+}
+
+// Of the CTA sizes that fit, the one that keeps the most warps resident on an SM (228 KB of shared memory, 1 KB of it
+// reserved per CTA; at most 32 CTAs and `max_warps` warps by registers), the larger one on a tie: a large table class
+// in four-warp CTAs would leave a quarter of an SM's shared memory unused.
+static int tables_per_cta(int64_t table_bytes, int G, int max_warps) {
+  const int64_t per_warp = 32 / G, warp_bytes = per_warp * std::max<int64_t>(table_bytes, 1);
+  int64_t best_w = 0, best = 0;
+  for (int64_t w = 1; w <= QR_MAX_WARPS && w * warp_bytes <= QR_SMEM_LIMIT; ++w) {
+    const int64_t ctas = std::min<int64_t>(32, (228 * 1024) / (w * warp_bytes + 1024));
+    const int64_t warps = std::min<int64_t>(max_warps, ctas * w);
+    if (warps >= best) {
+      best = warps;
+      best_w = w;
+    }
+  }
+  return (int)(best_w * per_warp);
 }
 
 static void set_smem(const void* kernel, size_t bytes) {
   if (bytes > 48 * 1024) BLS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// Fork the plan's side streams off s (they wait for all work issued on s so far); class q of a run of per-class
+// launches goes to class_stream(P, s, q), and join_sides makes s wait for the side streams' work.
+static void fork_sides(QRPlan* P, cudaStream_t s) {
+  if (!P->ev_fork) {
+    BLS_CUDA(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
+    for (int i = 0; i < 3; ++i) {
+      BLS_CUDA(cudaStreamCreateWithFlags(&P->side[i], cudaStreamNonBlocking));
+      BLS_CUDA(cudaEventCreateWithFlags(&P->ev_join[i], cudaEventDisableTiming));
+    }
+  }
+  BLS_CUDA(cudaEventRecord(P->ev_fork, s));
+  for (int i = 0; i < 3; ++i) BLS_CUDA(cudaStreamWaitEvent(P->side[i], P->ev_fork, 0));
+}
+static cudaStream_t class_stream(QRPlan* P, cudaStream_t s, int q) { return (q & 3) == 0 ? s : P->side[(q & 3) - 1]; }
+static void join_sides(QRPlan* P, cudaStream_t s) {
+  for (int i = 0; i < 3; ++i) {
+    BLS_CUDA(cudaEventRecord(P->ev_join[i], P->side[i]));
+    BLS_CUDA(cudaStreamWaitEvent(s, P->ev_join[i], 0));
+  }
 }
 
 // Asynchronous global -> shared copies of one element (cp.async, completed by cp_async_wait_all): a lane issues all of
@@ -158,12 +218,90 @@ __device__ __forceinline__ double col_scale(const double* s, int j, int t, int n
   return 1.0;
 }
 
+// Eliminated blocks of up to QR_WY_MAX variables are factored in the compact form below; larger ones reflector by
+// reflector.
+constexpr int QR_WY_MAX = 4;
+
+// Row i of the packed reflectors (QR_WY_MAX entries per row, those past the table's de zero): one 16-byte load in FP32,
+// one or two in FP64.
+template <class T, int ND>
+__device__ __forceinline__ void load_vrow(const T* __restrict__ Vp, int i, T (&v)[QR_WY_MAX]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 x = reinterpret_cast<const float4*>(Vp)[i];
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  } else {
+    const double2* p = reinterpret_cast<const double2*>(Vp) + 2 * i;
+    const double2 x = p[0];
+    v[0] = x.x; v[1] = x.y;
+    if constexpr (ND > 2) {
+      const double2 y = p[1];
+      v[2] = y.x; v[3] = y.y;
+    } else {
+      v[2] = T(0); v[3] = T(0);
+    }
+  }
+}
+
+// The ND reflectors H_k = I - tau_k v_k v_k' of a table applied to its retained columns in compact form: for a column y,
+// H_{ND-1} ... H_0 y = y - V s with a = V' y and s_k = tau_k (a_k - sum_{l<k} s_l g_kl), g_kl = v_k' v_l, so each column
+// is read twice (a, then the update) instead of twice per reflector. A lane per column; rows from me on are the
+// damping rows, zero before the reflectors (read only for the non-finite test when `check`). V' y accumulates in the
+// storage type, s in FP64. Returns whether a column held a non-finite entry (x * 0 is NaN exactly for Inf and NaN).
+template <class T, int ND>
+__device__ __forceinline__ bool wy_columns(T* A, const T* __restrict__ Vp, int ncols, int M, int me, const double* tau,
+                                           const double* gkl, bool check, int lane, int G) {
+  T chk = T(0);
+  for (int j = lane; j < ncols; j += G) {
+    T* y = A + (size_t)j * M;
+    T a[ND];
+#pragma unroll
+    for (int k = 0; k < ND; ++k) a[k] = T(0);
+    for (int i = 0; i < me; ++i) {
+      const T x = y[i];
+      T v[QR_WY_MAX];
+      load_vrow<T, ND>(Vp, i, v);
+      if (check) chk = fma(x, T(0), chk);
+#pragma unroll
+      for (int k = 0; k < ND; ++k) a[k] = fma(v[k], x, a[k]);
+    }
+    if (check)
+      for (int i = me; i < M; ++i) chk = fma(y[i], T(0), chk);
+    double sd[ND];
+    T sv[ND];
+#pragma unroll
+    for (int k = 0; k < ND; ++k) {
+      double x = (double)a[k];
+#pragma unroll
+      for (int l = 0; l < k; ++l) x -= sd[l] * gkl[k * (k - 1) / 2 + l];
+      sd[k] = tau[k] * x;
+      sv[k] = T(-sd[k]);
+    }
+    for (int i = 0; i < me; ++i) {
+      T v[QR_WY_MAX];
+      load_vrow<T, ND>(Vp, i, v);
+      T x = y[i];
+#pragma unroll
+      for (int k = 0; k < ND; ++k) x = fma(sv[k], v[k], x);
+      y[i] = x;
+    }
+    for (int i = me; i < M; ++i) {
+      T v[QR_WY_MAX];
+      load_vrow<T, ND>(Vp, i, v);
+      T x = sv[0] * v[0];
+#pragma unroll
+      for (int k = 1; k < ND; ++k) x = fma(sv[k], v[k], x);
+      y[i] = x;
+    }
+  }
+  return check && isnan((double)chk);
+}
+
 // qr_table! for the listed eliminated tables, a group of G lanes per table (G = 8 or 16 for narrow tables, so that a
 // warp factors several tables at once and its lanes are not left idle over a few columns; 32 otherwise); the group's
 // shared-memory region holds the table (M x C, column-major) and the FP64 residual (M). Tables are assigned by
 // `tables[blockIdx.x * groups + group]`.
 template <class T, int G>
-__global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, int warp_bytes, const int32_t* __restrict__ tables,
+__global__ void __launch_bounds__(32 * QR_MAX_WARPS, 8) k_qr_tables(int64_t ntab, int warp_bytes, const int32_t* __restrict__ tables,
                                                   const int32_t* __restrict__ t_rows,
                                                   const int32_t* __restrict__ t_cols, const int64_t* __restrict__ t_raw,
                                                   const int64_t* __restrict__ t_res, const int32_t* __restrict__ t_ptr,
@@ -186,14 +324,18 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
   const int t = tables[wi];
   const int M = t_rows[t], C = t_cols[t] - 1, de = e_dims[t], me = M - de, ce = C - de;
   const int64_t off = t_raw[t], rq = t_res[t];
-  // the group's region: its mbarrier, then the FP64 residual and the M x C table, each with 32 bytes of room for the
-  // 16-byte alignment of a bulk copy
+  // the group's region: its mbarrier, the packed reflectors of the compact form (M rows of QR_WY_MAX entries, when the
+  // class left room for them), then the FP64 residual and the M x C table, each with 32 bytes of room for the 16-byte
+  // alignment of a bulk copy
   uint64_t* bar = reinterpret_cast<uint64_t*>(qsm);
-  unsigned char* rbase = qsm + 16;
-  unsigned char* abase = rbase + ((8 * M + 32 + 15) & ~15);
+  const int rb = (8 * M + 32 + 15) & ~15, vb = QR_WY_MAX * (int)sizeof(T) * M;
+  const bool wy = de <= QR_WY_MAX && 16 + vb + rb + (int64_t)sizeof(T) * M * C + 32 <= warp_bytes;
+  T* Vp = reinterpret_cast<T*>(qsm + 16);
+  unsigned char* rbase = qsm + 16 + (wy ? vb : 0);
+  unsigned char* abase = rbase + rb;
   double* res;
   T* A;
-  if (bulk) {
+  if (bulk & 1) {
     // the table and its residual are contiguous: one bulk copy each (TMA), completed on the group's mbarrier
     const Span sa = span_of(Rw + off, (int64_t)M * C, Rw_end), sr = span_of(Rr + rq, (int64_t)M, Rr_end);
     if (lane == 0) {
@@ -221,9 +363,11 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
     cp_async_wait_all();
     __syncwarp(gmask);
   }
-  // the reference's non-finite test (x - x is NaN for Inf / NaN) and the conditioning scales, in shared memory
+  // the reference's non-finite test (x - x is NaN for Inf / NaN) and the conditioning scales, in shared memory; in the
+  // compact form without scales the retained columns are tested inside their update (before anything is written out)
+  const bool fused = wy && !s;
   bool bad = false;
-  for (int i = lane; i < M * C; i += G) {
+  for (int i = (fused ? ce * M : 0) + lane; i < M * C; i += G) {
     T x = A[i];
     bad |= isnan((double)(x - x));
     if (s) A[i] = T((double)x * col_scale(s, i / M, t, C, de, t_ptr, u_col, u_ret, boff_r, r_dims, boff_e, nr));
@@ -238,10 +382,12 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
     return;
   }
   __syncwarp(gmask);
-  // damping rows: zero, then sqrt(lambda * scaling_e) * s_e on their diagonal (formed in FP64)
-  for (int i = lane; i < de * C; i += G) {
-    const int j = i / de, r = me + (i - j * de);
-    A[j * M + r] = T(0);
+  // damping rows: zero, then sqrt(lambda * scaling_e) * s_e on their diagonal (formed in FP64); the compact form writes
+  // the retained columns' damping rows whole, so only the eliminated columns' are cleared for it
+  const int z0 = wy ? ce : 0;
+  for (int i = lane; i < de * (C - z0); i += G) {
+    const int jj = i / de, r = me + (i - jj * de);
+    A[(z0 + jj) * M + r] = T(0);
   }
   for (int l = lane; l < de; l += G) res[me + l] = 0.0;
   __syncwarp(gmask);
@@ -252,61 +398,163 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS) k_qr_tables(int64_t ntab, i
   }
   __syncwarp(gmask);
   const double tol = (double)M * eps_of<T>();
-  for (int k = 0; k < de; ++k) {
-    T* col = A + (ce + k) * M;
-    double s_top = 0.0, s_sub = 0.0;
-    for (int i = lane; i < M; i += G) {
-      const double v = (double)col[i];
-      if (i < k) s_top += v * v;
-      else s_sub += v * v;
+  if (wy) {
+    // the eliminated columns first (each reflector applied to the later ones, lanes over rows, FP64 sums), keeping
+    // the reflectors' vectors below the diagonal
+    double tau[QR_WY_MAX] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < QR_WY_MAX; ++k) {
+      if (k >= de) break;   // unrolled, so that tau and gkl stay in registers
+      T* col = A + (ce + k) * M;
+      double s_top = 0.0, s_sub = 0.0;
+      for (int i = lane; i < M; i += G) {
+        const double v = (double)col[i];
+        if (i < k) s_top += v * v;
+        else s_sub += v * v;
+      }
+      s_top = group_sum<G>(s_top, gmask);
+      s_sub = group_sum<G>(s_sub, gmask);
+      const double nrm = sqrt(s_sub), full = sqrt(s_top + s_sub);
+      const double a = (double)col[k];
+      const double beta = a >= 0.0 ? -nrm : nrm;
+      if (!(isfinite(beta) && fabs(beta) > tol * full)) {
+        if (lane == 0) atomicMin(st, (long long)t);
+        return;
+      }
+      const double scale = 1.0 / (a - beta);
+      tau[k] = (beta - a) / beta;
+      __syncwarp(gmask);
+      for (int i = k + 1 + lane; i < M; i += G) col[i] = T((double)col[i] * scale);
+      __syncwarp(gmask);
+      if (lane == 0) col[k] = T(beta);
+      for (int jj = k + 1; jj < de; ++jj) {
+        T* y = A + (ce + jj) * M;
+        double p = 0.0;
+        for (int i = k + 1 + lane; i < M; i += G) p += (double)col[i] * (double)y[i];
+        p = group_sum<G>(p, gmask);
+        p = (p + (double)y[k]) * tau[k];
+        __syncwarp(gmask);
+        if (lane == 0) y[k] = T((double)y[k] - p);
+        for (int i = k + 1 + lane; i < M; i += G) y[i] = T((double)y[i] - p * (double)col[i]);
+        __syncwarp(gmask);
+      }
     }
-    s_top = group_sum<G>(s_top, gmask);
-    s_sub = group_sum<G>(s_sub, gmask);
-    const double nrm = sqrt(s_sub), full = sqrt(s_top + s_sub);
-    const double a = (double)col[k];
-    const double beta = a >= 0.0 ? -nrm : nrm;
-    if (!(isfinite(beta) && fabs(beta) > tol * full)) {
+    // the packed reflectors V (v_k: zero above row k, one at row k, the column's stored vector below) and the
+    // products g_kl = v_k' v_l, l < k, in FP64
+    for (int i = lane; i < M; i += G)
+#pragma unroll
+      for (int k = 0; k < QR_WY_MAX; ++k)
+        Vp[QR_WY_MAX * i + k] = k < de ? (i < k ? T(0) : i == k ? T(1) : A[(ce + k) * M + i]) : T(0);
+    double gkl[QR_WY_MAX * (QR_WY_MAX - 1) / 2] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 1; k < QR_WY_MAX; ++k)
+#pragma unroll
+      for (int l = 0; l < k; ++l) {
+        if (k >= de) break;
+        double p = 0.0;
+        for (int i = k + 1 + lane; i < M; i += G) p += (double)A[(ce + k) * M + i] * (double)A[(ce + l) * M + i];
+        gkl[k * (k - 1) / 2 + l] = group_sum<G>(p, gmask) + (double)A[(ce + l) * M + k];
+      }
+    __syncwarp(gmask);
+    // the factored eliminated columns are zero below their diagonal
+    for (int k = 0; k < de; ++k)
+      for (int i = k + 1 + lane; i < M; i += G) A[(ce + k) * M + i] = T(0);
+    // the retained columns
+    bool badr = false;
+    if (de == 1) badr = wy_columns<T, 1>(A, Vp, ce, M, me, tau, gkl, fused, lane, G);
+    else if (de == 2) badr = wy_columns<T, 2>(A, Vp, ce, M, me, tau, gkl, fused, lane, G);
+    else if (de == 3) badr = wy_columns<T, 3>(A, Vp, ce, M, me, tau, gkl, fused, lane, G);
+    else badr = wy_columns<T, 4>(A, Vp, ce, M, me, tau, gkl, fused, lane, G);
+    if (__any_sync(gmask, badr)) {
       if (lane == 0) atomicMin(st, (long long)t);
       return;
     }
-    const double scale = 1.0 / (a - beta);
-    const double tau = (beta - a) / beta;
-    __syncwarp(gmask);
-    for (int i = k + 1 + lane; i < M; i += G) col[i] = T((double)col[i] * scale);
-    __syncwarp(gmask);
-    if (lane == 0) col[k] = T(beta);
-    // apply I - tau v v' (v = [1; col[k+1:]]) to every column outside the eliminated columns ce..ce+k
-    for (int j = lane; j < C; j += G) {
-      if (j >= ce && j <= ce + k) continue;
-      T* y = A + j * M;
-      // v'y in four independent partial sums (the FMA chain is the latency of this loop), in the storage type: the
-      // panel update is FP32 in the mixed form, the reflector's tau (its scaling) FP64
-      T p0 = y[k], p1 = T(0), p2 = T(0), p3 = T(0);
-      int i = k + 1;
-      for (; i + 3 < M; i += 4) {
-        p0 += col[i] * y[i];
-        p1 += col[i + 1] * y[i + 1];
-        p2 += col[i + 2] * y[i + 2];
-        p3 += col[i + 3] * y[i + 3];
-      }
-      for (; i < M; ++i) p0 += col[i] * y[i];
-      const T sj = T((double)((p0 + p1) + (p2 + p3)) * tau);
-      y[k] = y[k] - sj;
-      for (int i = k + 1; i < M; ++i) y[i] = y[i] - sj * col[i];
+    // and the FP64 residual (lanes over rows; its damping rows are zero)
+    double ar[QR_WY_MAX] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = lane; i < M; i += G) {
+      const double r = res[i];
+#pragma unroll
+      for (int k = 0; k < QR_WY_MAX; ++k) ar[k] += (double)Vp[QR_WY_MAX * i + k] * r;
     }
-    // and to the FP64 residual
-    double sr = 0.0;
-    for (int i = k + 1 + lane; i < M; i += G) sr += (double)col[i] * res[i];
-    sr = group_sum<G>(sr, gmask) + res[k];
-    sr *= tau;
-    __syncwarp(gmask);
-    if (lane == 0) res[k] -= sr;
-    for (int i = k + 1 + lane; i < M; i += G) res[i] -= sr * (double)col[i];
-    __syncwarp(gmask);
-    for (int i = k + 1 + lane; i < M; i += G) col[i] = T(0);
-    __syncwarp(gmask);
+    double sd[QR_WY_MAX];
+#pragma unroll
+    for (int k = 0; k < QR_WY_MAX; ++k) {
+      double x = group_sum<G>(ar[k], gmask);
+#pragma unroll
+      for (int l = 0; l < k; ++l) x -= sd[l] * gkl[k * (k - 1) / 2 + l];
+      sd[k] = tau[k] * x;
+    }
+    for (int i = lane; i < M; i += G) {
+      double r = res[i];
+#pragma unroll
+      for (int k = 0; k < QR_WY_MAX; ++k) r -= sd[k] * (double)Vp[QR_WY_MAX * i + k];
+      res[i] = r;
+    }
+  } else {
+    for (int k = 0; k < de; ++k) {
+      T* col = A + (ce + k) * M;
+      double s_top = 0.0, s_sub = 0.0;
+      for (int i = lane; i < M; i += G) {
+        const double v = (double)col[i];
+        if (i < k) s_top += v * v;
+        else s_sub += v * v;
+      }
+      s_top = group_sum<G>(s_top, gmask);
+      s_sub = group_sum<G>(s_sub, gmask);
+      const double nrm = sqrt(s_sub), full = sqrt(s_top + s_sub);
+      const double a = (double)col[k];
+      const double beta = a >= 0.0 ? -nrm : nrm;
+      if (!(isfinite(beta) && fabs(beta) > tol * full)) {
+        if (lane == 0) atomicMin(st, (long long)t);
+        return;
+      }
+      const double scale = 1.0 / (a - beta);
+      const double tau = (beta - a) / beta;
+      __syncwarp(gmask);
+      for (int i = k + 1 + lane; i < M; i += G) col[i] = T((double)col[i] * scale);
+      __syncwarp(gmask);
+      if (lane == 0) col[k] = T(beta);
+      // apply I - tau v v' (v = [1; col[k+1:]]) to every column outside the eliminated columns ce..ce+k
+      for (int j = lane; j < C; j += G) {
+        if (j >= ce && j <= ce + k) continue;
+        T* y = A + j * M;
+        // v'y in four independent partial sums (the FMA chain is the latency of this loop), in the storage type: the
+        // panel update is FP32 in the mixed form, the reflector's tau (its scaling) FP64
+        T p0 = y[k], p1 = T(0), p2 = T(0), p3 = T(0);
+        int i = k + 1;
+        for (; i + 3 < M; i += 4) {
+          p0 += col[i] * y[i];
+          p1 += col[i + 1] * y[i + 1];
+          p2 += col[i + 2] * y[i + 2];
+          p3 += col[i + 3] * y[i + 3];
+        }
+        for (; i < M; ++i) p0 += col[i] * y[i];
+        const T sj = T((double)((p0 + p1) + (p2 + p3)) * tau);
+        y[k] = y[k] - sj;
+        for (int i = k + 1; i < M; ++i) y[i] = y[i] - sj * col[i];
+      }
+      // and to the FP64 residual
+      double sr = 0.0;
+      for (int i = k + 1 + lane; i < M; i += G) sr += (double)col[i] * res[i];
+      sr = group_sum<G>(sr, gmask) + res[k];
+      sr *= tau;
+      __syncwarp(gmask);
+      if (lane == 0) res[k] -= sr;
+      for (int i = k + 1 + lane; i < M; i += G) res[i] -= sr * (double)col[i];
+      __syncwarp(gmask);
+      for (int i = k + 1 + lane; i < M; i += G) col[i] = T(0);
+      __syncwarp(gmask);
+    }
   }
-  for (int i = lane; i < M * C; i += G) F[off + i] = A[i];
+  __syncwarp(gmask);
+  if (bulk & 2) {
+    // the factored table out by one bulk copy of its aligned interior (F at the same 16-byte offset as the raw table)
+    fence_proxy_async_shared();
+    __syncwarp(gmask);
+    if (lane == 0) span_store(F + off, A, (int64_t)M * C);
+  } else {
+    for (int i = lane; i < M * C; i += G) F[off + i] = A[i];
+  }
   for (int i = lane; i < M; i += G) Fr[rq + i] = res[i];
 }
 
@@ -1040,8 +1288,13 @@ static QRPlan* qr_plan_create(bls_ctx* ctx, const bls_qr_plan_desc* d) {
     if (t < neb) {
       // the warp's mbarrier, the residual and the table, each with room for a bulk copy's 16-byte alignment
       const int64_t rb = (8 * M + 32 + 15) & ~int64_t(15);
-      const int64_t b64 = 16 + rb + 8 * M * C + 32, b32 = 16 + rb + 4 * M * C + 32;
+      int64_t b64 = 16 + rb + 8 * M * C + 32, b32 = 16 + rb + 4 * M * C + 32;
       if (b64 > QR_SMEM_LIMIT) throw Error(BLS_EUNSUPPORTED, "table " + std::to_string(t + 1) + " exceeds the shared-memory capacity of this build");
+      // and the packed reflectors of the compact form, where they fit (the kernel checks the room it was given)
+      if (d->e_dims[t] <= QR_WY_MAX && b64 + 8 * QR_WY_MAX * M <= QR_SMEM_LIMIT) {
+        b64 += 8 * QR_WY_MAX * M;
+        b32 += 4 * QR_WY_MAX * M;
+      }
       const int c = cls_of(b64);
       cls_tables[c].push_back((int32_t)t);
       P->classes[c].bytes_f64 = std::max(P->classes[c].bytes_f64, b64);
@@ -1253,13 +1506,19 @@ static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr,
   // bulk copies need the buffers' starts on 16-byte boundaries (the device allocators give 256); otherwise the tables
   // are staged element by element
   const bool bulk = P->bulk && (reinterpret_cast<uintptr_t>(Rw) & 15) == 0 && (reinterpret_cast<uintptr_t>(Rr) & 15) == 0;
-  for (int c = 0; c < 8; ++c) {
+  // the factored tables go out by bulk copies too when F keeps the raw tables' 16-byte offsets
+  const int bulk_mode = bulk ? 1 | ((reinterpret_cast<uintptr_t>(F) & 15) == 0 ? 2 : 0) : 0;
+  fork_sides(P, s);
+  for (int c = 0, q = 0; c < 8; ++c) {
     const auto& k = P->classes[c];
     if (k.n == 0) continue;
+    cudaStream_t cs = class_stream(P, s, q++);
     const int64_t wb = ((std::is_same<T, double>::value ? k.bytes_f64 : k.bytes_f32) + 15) & ~int64_t(15);
     // lanes per table from the widest table of the class: a lane per column in the reflector updates
     int G = k.maxc <= 24 ? 8 : k.maxc <= 48 ? 16 : 32;
-    int tpc = tables_per_cta(wb, G);
+    const void* kg = G == 8 ? reinterpret_cast<const void*>(k_qr_tables<T, 8>) : G == 16 ? reinterpret_cast<const void*>(k_qr_tables<T, 16>)
+                                                                                          : reinterpret_cast<const void*>(k_qr_tables<T, 32>);
+    int tpc = tables_per_cta(wb, G, warp_cap(kg));
     if (tpc == 0) {
       G = 32;
       tpc = warps_per_cta(wb);
@@ -1267,17 +1526,18 @@ static int reduce_qr(QRPlan* P, T* F, double* Fr, const T* Rw, const double* Rr,
     const size_t smem = (size_t)(wb * tpc);
     auto launch = [&](auto kern) {
       set_smem(reinterpret_cast<const void*>(kern), smem);
-      kern<<<(unsigned)((k.n + tpc - 1) / tpc), tpc * G, smem, s>>>(
+      kern<<<(unsigned)((k.n + tpc - 1) / tpc), tpc * G, smem, cs>>>(
           k.n, (int)wb, k.tables.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(),
           P->t_ptr.as<int32_t>(), P->u_col.as<int32_t>(), P->u_ret.as<int32_t>(), P->boff_r.as<int32_t>(), P->r_dims.as<int32_t>(),
           P->e_dims.as<int32_t>(), P->boff_e.as<int32_t>(), (int)P->nr, Rw, Rr, sc_e, lambda, sv, F, Fr, Rw + P->raw_len, Rr + P->res_len,
-          bulk ? 1 : 0, st);
+          bulk_mode, st);
     };
     if (G == 8) launch(k_qr_tables<T, 8>);
     else if (G == 16) launch(k_qr_tables<T, 16>);
     else launch(k_qr_tables<T, 32>);
     P->launches += 1;
   }
+  join_sides(P, s);
   if (P->ntables > P->neblocks) {
     k_qr_free<T><<<(unsigned)(P->ntables - P->neblocks), 128, 0, s>>>(P->neblocks, P->ntables, P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(),
                                                                        P->t_raw.as<int64_t>(), P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(),
@@ -1296,15 +1556,17 @@ template <class T, int MODE>
 static void gram(QRPlan* P, T* S, bool dense, double* g, const T* F, const double* Fr, bool from_raw = false) {
   cudaStream_t s = P->ctx->stream;
   const bool bulk = P->bulk && (reinterpret_cast<uintptr_t>(F) & 15) == 0 && (reinterpret_cast<uintptr_t>(Fr) & 15) == 0;
-  for (int c = 0; c < 8; ++c) {
+  fork_sides(P, s);
+  for (int c = 0, q = 0; c < 8; ++c) {
     const auto& k = P->gram_classes[c];
     if (k.n == 0) continue;
+    cudaStream_t cs = class_stream(P, s, q++);
     const int64_t wb = ((std::is_same<T, double>::value ? k.bytes_f64 : k.bytes_f32) + 15) & ~int64_t(15);
-    const int wpc = warps_per_cta(wb);
-    const size_t smem = (size_t)(wb * wpc);
     auto kern = P->all6 ? k_qr_gram<T, MODE, true> : k_qr_gram<T, MODE, false>;
+    const int wpc = std::max(1, tables_per_cta(wb, 32, warp_cap(reinterpret_cast<const void*>(kern))));
+    const size_t smem = (size_t)(wb * wpc);
     set_smem(reinterpret_cast<const void*>(kern), smem);
-    kern<<<(unsigned)((k.n + wpc - 1) / wpc), 32 * wpc, smem, s>>>(
+    kern<<<(unsigned)((k.n + wpc - 1) / wpc), 32 * wpc, smem, cs>>>(
         k.n, (int)wb, k.tables.as<int32_t>(), P->t_rows.as<int32_t>(), P->t_cols.as<int32_t>(), P->t_top.as<int32_t>(), P->t_raw.as<int64_t>(),
         P->t_res.as<int64_t>(), P->t_ptr.as<int32_t>(), P->u_ret.as<int32_t>(), P->u_col.as<int32_t>(), P->r_dims.as<int32_t>(),
         P->boff_r.as<int32_t>(), P->tp_ptr.as<int32_t>(), P->tp_blk.as<int32_t>(),
@@ -1313,6 +1575,7 @@ static void gram(QRPlan* P, T* S, bool dense, double* g, const T* F, const doubl
         P->status.as<long long>());
     P->launches += 1;
   }
+  join_sides(P, s);
   BLS_CUDA(cudaGetLastError());
 }
 
