@@ -205,6 +205,14 @@ __device__ __forceinline__ double group_sum(double v, unsigned gmask) {
   for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
   return v;
 }
+// N independent sums over the group at once (each the same butterfly as group_sum; the N shuffles of a round overlap)
+template <int G, int N>
+__device__ __forceinline__ void group_sum_n(double (&v)[N], unsigned gmask) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1)
+#pragma unroll
+    for (int n = 0; n < N; ++n) v[n] += __shfl_xor_sync(gmask, v[n], o);
+}
 
 // Scale of table column j (the variable it belongs to): s over all variables [s_r; s_e]; 1 when s is null.
 __device__ __forceinline__ double col_scale(const double* s, int j, int t, int ncols_f, int de, const int32_t* t_ptr, const int32_t* u_col,
@@ -296,6 +304,111 @@ __device__ __forceinline__ bool wy_columns(T* A, const T* __restrict__ Vp, int n
   return check && isnan((double)chk);
 }
 
+// The compact factorisation of a table whose eliminated block has ND <= QR_WY_MAX variables (its last ND columns, from
+// ce): the eliminated columns' reflectors one after the other, each applied to the later eliminated columns (their dot
+// products reduced together); then one pass over the rows packs V and forms the products g_kl = v_k'v_l and the
+// residual's a = V'r (reduced together), a second updates the residual and clears the eliminated columns below their
+// diagonal, and the retained columns take the compact update. Returns false when the table fails: a singular
+// eliminated block, or a non-finite retained entry when `check`.
+template <class T, int G, int ND>
+__device__ __forceinline__ bool factor_wy(T* A, double* res, T* Vp, int M, int me, int ce, double tol, bool check, int lane,
+                                          unsigned gmask) {
+  double tau[ND];
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    T* col = A + (ce + k) * M;
+    // the column's norm above its diagonal (fewer than ND rows, read by every lane) and from its diagonal down
+    double s_top = 0.0, s_sub = 0.0;
+#pragma unroll
+    for (int i = 0; i < k; ++i) {
+      const double v = (double)col[i];
+      s_top += v * v;
+    }
+    for (int i = k + lane; i < M; i += G) {
+      const double v = (double)col[i];
+      s_sub += v * v;
+    }
+    s_sub = group_sum<G>(s_sub, gmask);
+    const double nrm = sqrt(s_sub), full = sqrt(s_top + s_sub);
+    const double a = (double)col[k];
+    const double beta = a >= 0.0 ? -nrm : nrm;
+    if (!(isfinite(beta) && fabs(beta) > tol * full)) return false;
+    const double scale = 1.0 / (a - beta);
+    tau[k] = (beta - a) / beta;
+    __syncwarp(gmask);   // every lane has read the column
+    // the reflector's vector in place, and its products with the later eliminated columns
+    double p[ND > 1 ? ND - 1 : 1];
+#pragma unroll
+    for (int n = 0; n < (ND > 1 ? ND - 1 : 1); ++n) p[n] = 0.0;
+    for (int i = k + 1 + lane; i < M; i += G) {
+      const T vt = T((double)col[i] * scale);
+      col[i] = vt;
+#pragma unroll
+      for (int jj = k + 1; jj < ND; ++jj) p[jj - k - 1] += (double)vt * (double)A[(ce + jj) * M + i];
+    }
+    if (lane == 0) col[k] = T(beta);
+    if (k + 1 < ND) {
+      group_sum_n<G, (ND > 1 ? ND - 1 : 1)>(p, gmask);
+      double q[ND > 1 ? ND - 1 : 1];
+#pragma unroll
+      for (int jj = k + 1; jj < ND; ++jj) q[jj - k - 1] = (p[jj - k - 1] + (double)A[(ce + jj) * M + k]) * tau[k];
+      __syncwarp(gmask);   // every lane has read row k of the later columns
+#pragma unroll
+      for (int jj = k + 1; jj < ND; ++jj) {
+        T* y = A + (ce + jj) * M;
+        if (lane == 0) y[k] = T((double)y[k] - q[jj - k - 1]);
+        for (int i = k + 1 + lane; i < M; i += G) y[i] = T((double)y[i] - q[jj - k - 1] * (double)col[i]);
+      }
+      __syncwarp(gmask);
+    }
+  }
+  // V (v_k: zero above row k, one at row k, the stored vector below), g_kl and a = V'r
+  constexpr int NG = ND * (ND - 1) / 2;
+  double acc[NG + ND];
+#pragma unroll
+  for (int n = 0; n < NG + ND; ++n) acc[n] = 0.0;
+  for (int i = lane; i < M; i += G) {
+    T v[QR_WY_MAX];
+#pragma unroll
+    for (int k = 0; k < QR_WY_MAX; ++k) v[k] = k < ND ? (i < k ? T(0) : i == k ? T(1) : A[(ce + k) * M + i]) : T(0);
+    if constexpr (sizeof(T) == 4) {
+      reinterpret_cast<float4*>(Vp)[i] = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+      reinterpret_cast<double2*>(Vp)[2 * i] = make_double2(v[0], v[1]);
+      reinterpret_cast<double2*>(Vp)[2 * i + 1] = make_double2(v[2], v[3]);
+    }
+    const double r = res[i];
+#pragma unroll
+    for (int k = 0; k < ND; ++k) {
+#pragma unroll
+      for (int l = 0; l < k; ++l) acc[k * (k - 1) / 2 + l] += (double)v[k] * (double)v[l];
+      acc[NG + k] += (double)v[k] * r;
+    }
+  }
+  group_sum_n<G, NG + ND>(acc, gmask);
+  double sd[ND];
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    double x = acc[NG + k];
+#pragma unroll
+    for (int l = 0; l < k; ++l) x -= sd[l] * acc[k * (k - 1) / 2 + l];
+    sd[k] = tau[k] * x;
+  }
+  // the residual (rows over lanes, V from this lane's own rows) and the eliminated columns below their diagonal
+  for (int i = lane; i < M; i += G) {
+    double r = res[i];
+#pragma unroll
+    for (int k = 0; k < ND; ++k) {
+      r -= sd[k] * (double)Vp[QR_WY_MAX * i + k];
+      if (i > k) A[(ce + k) * M + i] = T(0);
+    }
+    res[i] = r;
+  }
+  __syncwarp(gmask);   // V complete
+  const bool bad = wy_columns<T, ND>(A, Vp, ce, M, me, tau, acc, check, lane, G);
+  return !__any_sync(gmask, bad);
+}
+
 // qr_table! for the listed eliminated tables, a group of G lanes per table (G = 8 or 16 for narrow tables, so that a
 // warp factors several tables at once and its lanes are not left idle over a few columns; 32 otherwise); the group's
 // shared-memory region holds the table (M x C, column-major) and the FP64 residual (M). Tables are assigned by
@@ -382,113 +495,30 @@ __global__ void __launch_bounds__(32 * QR_MAX_WARPS, 8) k_qr_tables(int64_t ntab
     return;
   }
   __syncwarp(gmask);
-  // damping rows: zero, then sqrt(lambda * scaling_e) * s_e on their diagonal (formed in FP64); the compact form writes
-  // the retained columns' damping rows whole, so only the eliminated columns' are cleared for it
+  // damping rows: zero, with sqrt(lambda * scaling_e) * s_e (formed in FP64) on the eliminated columns' diagonal; the
+  // compact form writes the retained columns' damping rows whole, so only the eliminated columns' are set for it
   const int z0 = wy ? ce : 0;
   for (int i = lane; i < de * (C - z0); i += G) {
-    const int jj = i / de, r = me + (i - jj * de);
-    A[(z0 + jj) * M + r] = T(0);
+    const int jj = i / de, r = i - jj * de, j = z0 + jj;
+    T x = T(0);
+    if (j - ce == r) {
+      const int so = boff_e[t];
+      x = T(sqrt(lambda * sc_e[so + r]) * (s ? s[nr + so + r] : 1.0));
+    }
+    A[j * M + me + r] = x;
   }
   for (int l = lane; l < de; l += G) res[me + l] = 0.0;
   __syncwarp(gmask);
-  for (int l = lane; l < de; l += G) {
-    const int so = boff_e[t];
-    const double sv = s ? s[nr + so + l] : 1.0;
-    A[(ce + l) * M + me + l] = T(sqrt(lambda * sc_e[so + l]) * sv);
-  }
-  __syncwarp(gmask);
   const double tol = (double)M * eps_of<T>();
   if (wy) {
-    // the eliminated columns first (each reflector applied to the later ones, lanes over rows, FP64 sums), keeping
-    // the reflectors' vectors below the diagonal
-    double tau[QR_WY_MAX] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int k = 0; k < QR_WY_MAX; ++k) {
-      if (k >= de) break;   // unrolled, so that tau and gkl stay in registers
-      T* col = A + (ce + k) * M;
-      double s_top = 0.0, s_sub = 0.0;
-      for (int i = lane; i < M; i += G) {
-        const double v = (double)col[i];
-        if (i < k) s_top += v * v;
-        else s_sub += v * v;
-      }
-      s_top = group_sum<G>(s_top, gmask);
-      s_sub = group_sum<G>(s_sub, gmask);
-      const double nrm = sqrt(s_sub), full = sqrt(s_top + s_sub);
-      const double a = (double)col[k];
-      const double beta = a >= 0.0 ? -nrm : nrm;
-      if (!(isfinite(beta) && fabs(beta) > tol * full)) {
-        if (lane == 0) atomicMin(st, (long long)t);
-        return;
-      }
-      const double scale = 1.0 / (a - beta);
-      tau[k] = (beta - a) / beta;
-      __syncwarp(gmask);
-      for (int i = k + 1 + lane; i < M; i += G) col[i] = T((double)col[i] * scale);
-      __syncwarp(gmask);
-      if (lane == 0) col[k] = T(beta);
-      for (int jj = k + 1; jj < de; ++jj) {
-        T* y = A + (ce + jj) * M;
-        double p = 0.0;
-        for (int i = k + 1 + lane; i < M; i += G) p += (double)col[i] * (double)y[i];
-        p = group_sum<G>(p, gmask);
-        p = (p + (double)y[k]) * tau[k];
-        __syncwarp(gmask);
-        if (lane == 0) y[k] = T((double)y[k] - p);
-        for (int i = k + 1 + lane; i < M; i += G) y[i] = T((double)y[i] - p * (double)col[i]);
-        __syncwarp(gmask);
-      }
-    }
-    // the packed reflectors V (v_k: zero above row k, one at row k, the column's stored vector below) and the
-    // products g_kl = v_k' v_l, l < k, in FP64
-    for (int i = lane; i < M; i += G)
-#pragma unroll
-      for (int k = 0; k < QR_WY_MAX; ++k)
-        Vp[QR_WY_MAX * i + k] = k < de ? (i < k ? T(0) : i == k ? T(1) : A[(ce + k) * M + i]) : T(0);
-    double gkl[QR_WY_MAX * (QR_WY_MAX - 1) / 2] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int k = 1; k < QR_WY_MAX; ++k)
-#pragma unroll
-      for (int l = 0; l < k; ++l) {
-        if (k >= de) break;
-        double p = 0.0;
-        for (int i = k + 1 + lane; i < M; i += G) p += (double)A[(ce + k) * M + i] * (double)A[(ce + l) * M + i];
-        gkl[k * (k - 1) / 2 + l] = group_sum<G>(p, gmask) + (double)A[(ce + l) * M + k];
-      }
-    __syncwarp(gmask);
-    // the factored eliminated columns are zero below their diagonal
-    for (int k = 0; k < de; ++k)
-      for (int i = k + 1 + lane; i < M; i += G) A[(ce + k) * M + i] = T(0);
-    // the retained columns
-    bool badr = false;
-    if (de == 1) badr = wy_columns<T, 1>(A, Vp, ce, M, me, tau, gkl, fused, lane, G);
-    else if (de == 2) badr = wy_columns<T, 2>(A, Vp, ce, M, me, tau, gkl, fused, lane, G);
-    else if (de == 3) badr = wy_columns<T, 3>(A, Vp, ce, M, me, tau, gkl, fused, lane, G);
-    else badr = wy_columns<T, 4>(A, Vp, ce, M, me, tau, gkl, fused, lane, G);
-    if (__any_sync(gmask, badr)) {
+    bool ok;
+    if (de == 1) ok = factor_wy<T, G, 1>(A, res, Vp, M, me, ce, tol, fused, lane, gmask);
+    else if (de == 2) ok = factor_wy<T, G, 2>(A, res, Vp, M, me, ce, tol, fused, lane, gmask);
+    else if (de == 3) ok = factor_wy<T, G, 3>(A, res, Vp, M, me, ce, tol, fused, lane, gmask);
+    else ok = factor_wy<T, G, 4>(A, res, Vp, M, me, ce, tol, fused, lane, gmask);
+    if (!ok) {
       if (lane == 0) atomicMin(st, (long long)t);
       return;
-    }
-    // and the FP64 residual (lanes over rows; its damping rows are zero)
-    double ar[QR_WY_MAX] = {0.0, 0.0, 0.0, 0.0};
-    for (int i = lane; i < M; i += G) {
-      const double r = res[i];
-#pragma unroll
-      for (int k = 0; k < QR_WY_MAX; ++k) ar[k] += (double)Vp[QR_WY_MAX * i + k] * r;
-    }
-    double sd[QR_WY_MAX];
-#pragma unroll
-    for (int k = 0; k < QR_WY_MAX; ++k) {
-      double x = group_sum<G>(ar[k], gmask);
-#pragma unroll
-      for (int l = 0; l < k; ++l) x -= sd[l] * gkl[k * (k - 1) / 2 + l];
-      sd[k] = tau[k] * x;
-    }
-    for (int i = lane; i < M; i += G) {
-      double r = res[i];
-#pragma unroll
-      for (int k = 0; k < QR_WY_MAX; ++k) r -= sd[k] * (double)Vp[QR_WY_MAX * i + k];
-      res[i] = r;
     }
   } else {
     for (int k = 0; k < de; ++k) {
