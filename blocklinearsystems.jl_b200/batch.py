@@ -131,7 +131,7 @@ class BatchedReduction:
         return reduce_schur_sparse(self.S, self.g, self.b_r, self.b_e, self.sc_e, 1.0, self.U, self.E, self.C, None, None, None, None,
                                    self.ws, sync=sync)
 
-    STAGE_UNITS = (8, 16, 32)
+    STAGE_UNITS = (8, 16, 24, 32)
 
     def autotune(self, reps: int = 5) -> dict:
         """Time the phase-2 schedules that keep per-problem failure on the batch, after a warm-up run each, and keep

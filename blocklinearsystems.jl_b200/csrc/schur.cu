@@ -68,7 +68,7 @@ struct SchurPlan {
   // fast36, sparse: the column-owned schedule (k_stage36). Work items are runs of a block column's visits (most
   // columns are one item); per item {r2, first visit, visit count, items of its column} (stg_items) and its first
   // batch (stg_ibat, nitems + 1). Each item's first batch holds its diagonal block's pairs, its visits cut into 32 runs;
-  // its off-diagonal pairs are cut into units (one S block, at most stage_unit pairs, in visit order), and those units,
+  // its off-diagonal pairs are cut into units (one S block, at most stage_unit[sd] pairs, in visit order), and those units,
   // longest first, into the following batches of 32, one unit per lane of the warp that takes the batch: per batch
   // {first pair, iterations} (stg_bat), per batch and lane {the block's row offset in the column | unit length << 16 |
   // (the block's only unit in the item) << 31} (stg_lane); pairs batch by batch, iteration-major (lane fastest),
@@ -76,7 +76,9 @@ struct SchurPlan {
   // One schedule per storage type (index 0 FP32, 1 FP64): FP32 items fit two 256-thread CTAs per SM, FP64 items (half
   // the visits) two 128-thread CTAs.
   bool stage_ok = false;
-  int stage_unit = 16;
+  // per schedule, the unit size (measured on the 1M-point scene: FP32 1.81 ms at 16, 1.65 at 24; FP64 3.18 ms at 16,
+  // 3.47 at 24, and 16 the best FP64 size on the 200k-point scene)
+  int stage_unit[2] = {24, 16};
   struct StageSchedule {
     int64_t items = 0, max_nv = 0, units = 0, batches = 0, slots = 0;
     DevBuf stg_items, stg_ibat, stg_bat, stg_lane, stg_pairs;
@@ -1727,7 +1729,7 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
 // visit point's first coupling; sized in FP64 bytes this must fit the schedule's STAGE_BUDGET, so a column with more
 // visits is cut into several items (their tiles are added to S with atomics). Items stay in column order: neighbouring columns read the couplings of
 // overlapping sets of points, which then stay in L2 while the columns in flight move along the cameras.
-// A block's pairs of one item are cut into units of at most stage_unit pairs, except the diagonal block's, which make
+// A block's pairs of one item are cut into units of at most stage_unit[sd] pairs, except the diagonal block's, which make
 // the item's first batch (the item's visits cut into 32 runs, one per lane). The item's other units, longest first,
 // are cut into batches of 32 consecutive ones, a lane per unit: the lanes of a batch run units of about the same
 // length and write them to the tile at the same time (a warp-wide shared-memory store or atomic costs the same for
@@ -1743,7 +1745,7 @@ static bool build_stage_schedule(SchurPlan* P, int sd, cudaStream_t s, int64_t n
   // schedule (whose FP32 items then take about 110 KB, two 256-thread CTAs per SM), 96 KB for the FP64 one (two
   // 128-thread CTAs per SM)
   const int64_t STAGE_BUDGET = sd == 0 ? 200 * 1024 : 96 * 1024;
-  const int U = P->stage_unit;
+  const int U = P->stage_unit[sd];
   struct ColOut {
     std::vector<int4> items;
     std::vector<int32_t> nbat;   // per item its number of batches
@@ -3013,7 +3015,7 @@ int bls_schur_plan_set_stage_unit(bls_schur_plan* P, int unit) {
   if (!P || unit < 1 || unit > 4096) return BLS_EINVAL;
   BLS_GUARD({
     if (!P->fast36 || !P->has_sparse || !P->stage_ok) throw Error(BLS_EUNSUPPORTED, "the plan has no column-owned schedule");
-    if (unit == P->stage_unit) return BLS_OK;
+    if (unit == P->stage_unit[0] && unit == P->stage_unit[1]) return BLS_OK;
     cudaStream_t s = P->ctx->stream;
     const int64_t nrb = P->nrblocks, neb = P->neblocks, nc = P->ncoup;
     const int64_t nb = P->nblocks;
@@ -3038,15 +3040,16 @@ int bls_schur_plan_set_stage_unit(bls_schur_plan* P, int unit) {
       brow_off[k] = b_base[k] - cbase[b_r2[k]];
     }
     for (int64_t r = 0; r < nrb; ++r) bcolptr[r + 1] += bcolptr[r];
-    const int old = P->stage_unit;
-    P->stage_unit = unit;
+    const int old0 = P->stage_unit[0], old1 = P->stage_unit[1];
+    P->stage_unit[0] = P->stage_unit[1] = unit;
     // each schedule is replaced only when its rebuild succeeds (a schedule with the old unit size stays valid)
     bool ok = true;
     for (int sd = 0; sd < 2; ++sd)
       ok = build_stage_schedule(P, sd, s, nrb, rptr, rentry, entry_elim, eptr.data(), eret.data(), bcolptr, browval, brow_off,
                                 col_h) && ok;
     if (!ok) {
-      P->stage_unit = old;
+      P->stage_unit[0] = old0;
+      P->stage_unit[1] = old1;
       throw Error(BLS_EUNSUPPORTED, "the schedule does not fit this unit size");
     }
     P->stage_grid[0] = P->stage_grid[1] = 0;

@@ -124,8 +124,9 @@ class SchurReductionWorkspace:
                                                              "stage": 5}[which]))
 
     def set_stage_unit(self, unit: int) -> None:
-        """Rebuild the "stage" schedule with units of at most `unit` pairs (one thread's run of one S block's pairs
-        between two writes to the column tile); 16 at plan creation."""
+        """Rebuild the "stage" schedule of both storage types with units of at most `unit` pairs (one thread's run of
+        one S block's pairs between two writes to the column tile); 24 for FP32 storage and 16 for FP64 at plan
+        creation."""
         check(_lib.gpu().bls_schur_plan_set_stage_unit(self._h, int(unit)))
 
     def phase2_kernel_name(self, dtype=torch.float32, *, dense: bool = False, scaled: bool = False) -> str:
