@@ -296,7 +296,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         "mixed_over_fp64": value / v64,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": measured_traffic(args.workload, kernel), "kernel": kernel, "kernel_ms": pair_ms,
-                     "stage_unit": args.stage_unit or "24 (FP32) / 16 (FP64)",
+                     "stage_unit": args.stage_unit or "20 (FP32) / 16 (FP64)",
                      "algorithmic_bytes": bytes32, "peak_source": "measured" if peaks else "fallback",
                      "flops": algorithmic_flops(p), "achieved_tflops": algorithmic_flops(p) / (pair_ms / 1e3) / 1e12},
         "e2e": {"value": world * nobs * args.steps / (e2e_ms / 1e3), "unit": "obs/s", "h2d_bytes_per_step": h2d,

@@ -67,8 +67,8 @@ struct SchurPlan {
   bool points_ok = false;
   // fast36, sparse: the column-owned schedule (k_stage36). Work items are runs of a block column's visits (most
   // columns are one item); per item {r2, first visit, visit count, items of its column} (stg_items) and its first
-  // batch (stg_ibat, nitems + 1). Each item's first batch holds its diagonal block's pairs, its visits cut into 32 runs;
-  // its off-diagonal pairs are cut into units (one S block, at most stage_unit[sd] pairs, in visit order), and those units,
+  // batch (stg_ibat, nitems + 1). The diagonal block is formed by the staging pass (no batch);
+  // the item's off-diagonal pairs are cut into units (one S block, at most stage_unit[sd] pairs, in visit order), and those units,
   // longest first, into the following batches of 32, one unit per lane of the warp that takes the batch: per batch
   // {first pair, iterations} (stg_bat), per batch and lane {the block's row offset in the column | unit length << 16 |
   // (the block's only unit in the item) << 31} (stg_lane); pairs batch by batch, iteration-major (lane fastest),
@@ -76,9 +76,9 @@ struct SchurPlan {
   // One schedule per storage type (index 0 FP32, 1 FP64): FP32 items fit two 256-thread CTAs per SM, FP64 items (half
   // the visits) two 128-thread CTAs.
   bool stage_ok = false;
-  // per schedule, the unit size (measured on the 1M-point scene: FP32 1.81 ms at 16, 1.65 at 24; FP64 3.18 ms at 16,
-  // 3.47 at 24, and 16 the best FP64 size on the 200k-point scene)
-  int stage_unit[2] = {24, 16};
+  // per schedule, the unit size (measured on the 1M-point scene: FP32 1.73 ms at 16, 1.62 at 20, 1.68 at 24; FP64
+  // 3.07 ms at 16, 3.30 at 20; on the 200k-point scene FP32 0.318 / 0.303 / 0.300 ms and FP64 0.468 ms at 16)
+  int stage_unit[2] = {20, 16};
   struct StageSchedule {
     int64_t items = 0, max_nv = 0, units = 0, batches = 0, slots = 0;
     DevBuf stg_items, stg_ibat, stg_bat, stg_lane, stg_pairs;
@@ -1448,8 +1448,8 @@ __global__ void k_gather(T* __restrict__ dest, const T* __restrict__ src, const 
 //    this item, in visit order. The lane owns the whole 6 x 6 block: acc += C_c1' W_c2 (C_c1 from global memory, the
 //    next pair's in flight; W_c2 from shared memory), 108 multiply-adds per pair in registers, then the block goes
 //    into the column's tile in shared memory (stored when it is its block's only unit, added with atomics otherwise).
-//    The item's first batch is the diagonal block's pairs (c2, c2), the visits cut into 32 runs: its lanes' blocks
-//    are summed over the warp and the upper triangle stored into the tile's last six rows.
+//    The diagonal block's pairs (c2, c2) need no batch: step 1 forms C_c2' W of each visit from the operands it holds
+//    and stores the sums' upper triangle into the tile's last six rows.
 // 3. The tile, times the conditioning scales s_r of its rows, is subtracted from the column of S (contiguous: the
 //    column's six scalar columns of H entries each), with atomics when the column is split into several items;
 //    g_S[r2] -= s_r .* sum C_c2' z'.
@@ -1466,7 +1466,7 @@ static size_t stage_smem(int64_t max_h, int64_t max_nv) {
   const size_t tile = ((size_t)6 * max_h * sizeof(T) + 15) & ~size_t(15);
   const size_t w = (size_t)max_nv * stage_wr<T>() * sizeof(T);
   const size_t p0 = ((size_t)max_nv * 4 + 15) & ~size_t(15);
-  return tile + w + p0 + (stage_nt<T>() / 32) * 6 * sizeof(double);
+  return tile + w + p0 + (stage_nt<T>() / 32) * (6 * sizeof(double) + 21 * sizeof(T));
 }
 
 // 18 entries of one coupling block of C, read with 32-byte loads from the 32-byte boundary at or below the block (C on
@@ -1587,16 +1587,22 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
   T* W = reinterpret_cast<T*>(sm + (((size_t)6 * H * sizeof(T) + 15) & ~size_t(15)));
   int* p0s = reinterpret_cast<int*>(W + (size_t)nv * WR);
   double* gp = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(p0s) + (((size_t)nv * 4 + 15) & ~size_t(15)));
+  T* dgp = reinterpret_cast<T*>(gp + 6 * (NT / 32));   // per warp, its sums of the diagonal block's upper triangle
   for (int i = tid; i < 6 * H; i += NT) tile[i] = T(0);
   // the column's conditioning scales s_r, folded into W (the rows' scales are applied when the tile is written to S)
   double fc[6];
 #pragma unroll
   for (int w = 0; w < 6; ++w) fc[w] = s_r ? s_r[6 * r2 + w] : 1.0;
-  // 1. W and the gradient sums, a thread per visit ({first coupling, point | index of c2 << 24} per visit); the next
-  //    visit's record is loaded while the current one is formed
+  // 1. W, the gradient sums and the diagonal block, a thread per visit ({first coupling, point | index of c2 << 24} per
+  //    visit); the next visit's record is loaded while the current one is formed. The diagonal block (c2, c2) takes
+  //    C_c2' W of every visit, the product a batch would form, from the operands already in registers: its upper
+  //    triangle (dg[c (c + 1) / 2 + rho], rho <= c) is summed per thread, then per warp and over the warps.
   double ga[6];
 #pragma unroll
   for (int w = 0; w < 6; ++w) ga[w] = 0.0;
+  T dg[21];
+#pragma unroll
+  for (int i = 0; i < 21; ++i) dg[i] = T(0);
   {
     int2 vr = tid < nv ? __ldg(vis_rec + q0 + tid) : make_int2(0, 0);
     for (int v = tid; v < nv; v += NT) {
@@ -1617,6 +1623,18 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
         for (int t = 0; t < 3; ++t) wv[3 * w + t] = T(fc[w] * (Ep[t] * c0 + Ep[t + 3] * c1 + Ep[t + 6] * c2v));
         ga[w] += c0 * Ep[9] + c1 * Ep[10] + c2v * Ep[11];
       }
+      T wr[18];
+      load_w18(wv, wr);   // this thread's own W row, back from shared memory (vector loads) rather than held
+#pragma unroll
+      for (int cc = 0; cc < 6; ++cc)
+#pragma unroll
+        for (int rho = 0; rho <= cc; ++rho) {
+          T x = dg[cc * (cc + 1) / 2 + rho];
+          x = fma(c[3 * rho], wr[3 * cc], x);
+          x = fma(c[3 * rho + 1], wr[3 * cc + 1], x);
+          x = fma(c[3 * rho + 2], wr[3 * cc + 2], x);
+          dg[cc * (cc + 1) / 2 + rho] = x;
+        }
       vr = vn;
     }
   }
@@ -1627,7 +1645,22 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     if (lane == 0) gp[6 * (tid >> 5) + w] = x;
   }
+#pragma unroll
+  for (int i = 0; i < 21; ++i) {
+    T x = dg[i];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) dgp[21 * (tid >> 5) + i] = x;
+  }
   __syncthreads();
+  // the diagonal block into the tile's last six rows (no batch writes there), the warps' sums in warp order
+  if (tid < 21) {
+    int cc = 0;
+    while ((cc + 1) * (cc + 2) / 2 <= tid) ++cc;
+    const int rho = tid - cc * (cc + 1) / 2;
+    T x = dgp[tid];
+    for (int w = 1; w < NT / 32; ++w) x += dgp[21 * w + tid];
+    tile[cc * H + (H - 6) + rho] = x;
+  }
   // 2. the item's batches, taken by the warps from a counter, longest first; a lane per unit of the batch
   {
     const int bb = __ldg(ibat + item), nb = __ldg(ibat + item + 1) - bb;
@@ -1668,17 +1701,7 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
         cur = nxt;
         if (it + 2 < iters) nxt = __ldg(pc + (int64_t)(it + 2) * 32);
       }
-      if (b == 0) {
-        // the diagonal batch: the lanes' blocks summed over the warp, the upper triangle into the tile's last six rows
-#pragma unroll
-        for (int c = 0; c < 6; ++c)
-#pragma unroll
-          for (int rho = 0; rho <= c; ++rho) {
-            T x = acc[6 * rho + c];
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-            if (lane == 0) tile[c * H + (H - 6) + rho] = x;
-          }
-      } else if (len > 0) {
+      if (len > 0) {
         // the unit's block into the tile: a plain store when it is its block's only unit in the item
         T* tb = tile + (lr & 0xffff);
         if (lr >> 31) {
@@ -1729,8 +1752,8 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
 // visit point's first coupling; sized in FP64 bytes this must fit the schedule's STAGE_BUDGET, so a column with more
 // visits is cut into several items (their tiles are added to S with atomics). Items stay in column order: neighbouring columns read the couplings of
 // overlapping sets of points, which then stay in L2 while the columns in flight move along the cameras.
-// A block's pairs of one item are cut into units of at most stage_unit[sd] pairs, except the diagonal block's, which make
-// the item's first batch (the item's visits cut into 32 runs, one per lane). The item's other units, longest first,
+// A block's pairs of one item are cut into units of at most stage_unit[sd] pairs (the diagonal block's pairs are formed
+// by the kernel's staging pass and have no units). The units, longest first,
 // are cut into batches of 32 consecutive ones, a lane per unit: the lanes of a batch run units of about the same
 // length and write them to the tile at the same time (a warp-wide shared-memory store or atomic costs the same for
 // one lane as for 32), and the CTA's warps take batches from a counter in shared memory, longest first, so that they
@@ -1832,28 +1855,8 @@ static bool build_stage_schedule(SchurPlan* P, int sd, cudaStream_t s, int64_t n
         return x.pr.size() != y.pr.size() ? x.pr.size() > y.pr.size() : x.j < y.j;
       });
       o.items.push_back(make_int4((int32_t)r2, (int32_t)(rptr[r2] + bnd[g]), (int32_t)(bnd[g + 1] - bnd[g]), (int32_t)nseg));
-      o.nbat.push_back((int32_t)((us.size() + 31) / 32) + 1);
-      o.nunits += (int64_t)us.size() + 32;
-      // the item's first batch: the diagonal block's pairs (c2, c2), the item's visits cut into 32 runs, one per lane
-      // (the kernel sums the lanes' blocks over the warp)
-      {
-        const int64_t n = bnd[g + 1] - bnd[g];
-        const int32_t iters = (int32_t)((n + 31) / 32);
-        o.bat.push_back(make_int2((int32_t)o.pairs.size(), iters));
-        for (int L = 0; L < 32; ++L)
-          o.lane.push_back((uint32_t)(col_h[r2] - 6) | ((uint32_t)((L + 1) * n / 32 - L * n / 32) << 16) | 0x80000000u);
-        for (int32_t it = 0; it < iters; ++it)
-          for (int L = 0; L < 32; ++L) {
-            const int64_t lo = L * n / 32, hi = (L + 1) * n / 32;
-            uint32_t code = 0u;
-            if (lo + it < hi) {
-              const int64_t v = lo + it;
-              const int32_t c2 = rentry[rptr[r2] + bnd[g] + v];
-              code = (uint32_t)v | ((uint32_t)(c2 - eptr[entry_elim[c2]]) << 16);
-            }
-            o.pairs.push_back(code);
-          }
-      }
+      o.nbat.push_back((int32_t)((us.size() + 31) / 32));
+      o.nunits += (int64_t)us.size();
       // batches of 32 consecutive units: a lane per unit, as many iterations as the batch's first (longest) unit
       for (size_t b0 = 0; b0 < us.size(); b0 += 32) {
         const int32_t iters = (int32_t)us[b0].pr.size();

@@ -125,7 +125,7 @@ class SchurReductionWorkspace:
 
     def set_stage_unit(self, unit: int) -> None:
         """Rebuild the "stage" schedule of both storage types with units of at most `unit` pairs (one thread's run of
-        one S block's pairs between two writes to the column tile); 24 for FP32 storage and 16 for FP64 at plan
+        one S block's pairs between two writes to the column tile); 20 for FP32 storage and 16 for FP64 at plan
         creation."""
         check(_lib.gpu().bls_schur_plan_set_stage_unit(self._h, int(unit)))
 

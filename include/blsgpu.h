@@ -197,7 +197,7 @@ int bls_schur_plan_instrument(bls_schur_plan* plan, int timing);
  * blocks). All compute the same reduction; the choice is kept for comparisons and for autotuning. */
 int bls_schur_plan_set_kernel(bls_schur_plan* plan, int which);
 /* No counterpart in the reference (a tuning knob of this build's schedule): rebuild the column-owned schedule (which = 5)
- * with units of at most `unit` pairs for both storage types (1..4096; at plan creation 24 for FP32 storage and 16 for
+ * with units of at most `unit` pairs for both storage types (1..4096; at plan creation 20 for FP32 storage and 16 for
  * FP64), a unit being one thread's run of one S block's
  * pairs between two writes to the column tile. Sparse plans on the 6/3 fast path only (BLS_EUNSUPPORTED otherwise);
  * on failure the previous schedule stays. Synchronises. */
