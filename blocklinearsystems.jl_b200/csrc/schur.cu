@@ -1441,17 +1441,18 @@ __global__ void k_gather(T* __restrict__ dest, const T* __restrict__ src, const 
 // ------------------------------------------------------------------------------------------------------------------
 // Phase 2 for d_r = 6, d_e = 3 and a sparse S, column-owned (the "stage" schedule): one CTA per work item, a run of
 // the visits of block column r2 (the points that observe camera r2, in the reference's retained_entry order).
-// 1. Each visit's point-side operand W = E' C_c2 diag(s_r[r2]) (3 x 6, E' = s_e E^-1 s_e from the factor kernel, formed
-//    in FP64 and rounded to the storage type) goes to shared memory, with the visit point's first coupling index; the
-//    same pass adds C_c2' z' (z' = s_e .* z, FP64) to the column's gradient sums.
+// 1. Each visit's point-side operand W = E' C_c2 (3 x 6, E' = s_e E^-1 s_e from the factor kernel, formed in FP64 and
+//    rounded to the storage type) goes to shared memory, with the visit point's first coupling index; the same pass
+//    adds C_c2' z' (z' = s_e .* z, FP64) to the column's gradient sums.
 // 2. The warps take batches of 32 units, a lane per unit: one S block (r1, r2) and a run of its pairs (c1, c2) of
 //    this item, in visit order. The lane owns the whole 6 x 6 block: acc += C_c1' W_c2 (C_c1 from global memory, the
 //    next pair's in flight; W_c2 from shared memory), 108 multiply-adds per pair in registers, then the block goes
 //    into the column's tile in shared memory (stored when it is its block's only unit, added with atomics otherwise).
 //    The diagonal block's pairs (c2, c2) need no batch: step 1 forms C_c2' W of each visit from the operands it holds
 //    and stores the sums' upper triangle into the tile's last six rows.
-// 3. The tile, times the conditioning scales s_r of its rows, is subtracted from the column of S (contiguous: the
-//    column's six scalar columns of H entries each), with atomics when the column is split into several items;
+// 3. The tile, times the conditioning scales s_r of its rows and of column r2, is subtracted from the column of S
+//    (contiguous: the column's six scalar columns of H entries each), with atomics when the column is split into
+//    several items;
 //    g_S[r2] -= s_r .* sum C_c2' z'.
 // The reference's accumulate_sparse_columns! (src/schur_reduction.jl:315-387) walks the same pairs of each column; W
 // is its W_c2 = E^-1 scaled(C_c2) with the point scales folded in, and the pair product C_c1' W_c2 its W_c1' C_c2
@@ -1589,10 +1590,6 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
   double* gp = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(p0s) + (((size_t)nv * 4 + 15) & ~size_t(15)));
   T* dgp = reinterpret_cast<T*>(gp + 6 * (NT / 32));   // per warp, its sums of the diagonal block's upper triangle
   for (int i = tid; i < 6 * H; i += NT) tile[i] = T(0);
-  // the column's conditioning scales s_r, folded into W (the rows' scales are applied when the tile is written to S)
-  double fc[6];
-#pragma unroll
-  for (int w = 0; w < 6; ++w) fc[w] = s_r ? s_r[6 * r2 + w] : 1.0;
   // 1. W, the gradient sums and the diagonal block, a thread per visit ({first coupling, point | index of c2 << 24} per
   //    visit); the next visit's record is loaded while the current one is formed. The diagonal block (c2, c2) takes
   //    C_c2' W of every visit, the product a batch would form, from the operands already in registers: its upper
@@ -1620,7 +1617,7 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
       for (int w = 0; w < 6; ++w) {
         const double c0 = (double)c[3 * w], c1 = (double)c[3 * w + 1], c2v = (double)c[3 * w + 2];
 #pragma unroll
-        for (int t = 0; t < 3; ++t) wv[3 * w + t] = T(fc[w] * (Ep[t] * c0 + Ep[t + 3] * c1 + Ep[t + 6] * c2v));
+        for (int t = 0; t < 3; ++t) wv[3 * w + t] = T(Ep[t] * c0 + Ep[t + 3] * c1 + Ep[t + 6] * c2v);
         ga[w] += c0 * Ep[9] + c1 * Ep[10] + c2v * Ep[11];
       }
       T wr[18];
@@ -1719,10 +1716,13 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
     }
   }
   __syncthreads();
-  // 3. the column of S (times the rows' conditioning scales) and the gradient
+  // 3. the column of S (times the conditioning scales of the tile's rows and of the column) and the gradient
   // a thread per tile row: its conditioning scale once, then the row's six entries (one per scalar column), all six
   // loads of S in flight together
   const int64_t cb = __ldg(col_base + r2);
+  double fc[6];
+#pragma unroll
+  for (int w = 0; w < 6; ++w) fc[w] = s_r ? s_r[6 * r2 + w] : 1.0;
   for (int rr = tid; rr < H; rr += NT) {
     const double f = s_r ? s_r[__ldg(S_rowval + cb + rr)] : 1.0;
     T* Sr = S + cb + rr;
@@ -1731,10 +1731,10 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
 #pragma unroll
       for (int w = 0; w < 6; ++w) old[w] = Sr[(int64_t)w * H];
 #pragma unroll
-      for (int w = 0; w < 6; ++w) Sr[(int64_t)w * H] = old[w] - T((double)tile[w * H + rr] * f);
+      for (int w = 0; w < 6; ++w) Sr[(int64_t)w * H] = old[w] - T((double)tile[w * H + rr] * (f * fc[w]));
     } else {
 #pragma unroll
-      for (int w = 0; w < 6; ++w) atomicAdd(Sr + (int64_t)w * H, -T((double)tile[w * H + rr] * f));
+      for (int w = 0; w < 6; ++w) atomicAdd(Sr + (int64_t)w * H, -T((double)tile[w * H + rr] * (f * fc[w])));
     }
   }
   if (tid < 6) {
