@@ -1601,16 +1601,31 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
 #pragma unroll
   for (int i = 0; i < 21; ++i) dg[i] = T(0);
   {
+    // FP64 also has the current visit's coupling block in flight from the previous iteration (and the next visit's
+    // record from the one before); FP32 has no registers left for it (it would spill)
+    constexpr bool PF = sizeof(T) == 8;
     int2 vr = tid < nv ? __ldg(vis_rec + q0 + tid) : make_int2(0, 0);
+    int2 vn = make_int2(0, 0);
+    Raw rc;
+    if constexpr (PF) {
+      if (tid + NT < nv) vn = __ldg(vis_rec + q0 + tid + NT);
+      if (tid < nv) load_raw(C, vr.x + (int)((unsigned)vr.y >> 24), ncoup, rc);
+    }
     for (int v = tid; v < nv; v += NT) {
       const double2* ez = reinterpret_cast<const double2*>(EZ + 12 * (int64_t)(vr.y & 0xffffff));
       double Ep[12];
 #pragma unroll
       for (int i = 0; i < 6; ++i) { double2 x = __ldg(ez + i); Ep[2 * i] = x.x; Ep[2 * i + 1] = x.y; }
       T c[18];
-      load_block18(C, vr.x + (int)((unsigned)vr.y >> 24), ncoup, c);
-      int2 vn = make_int2(0, 0);
-      if (v + NT < nv) vn = __ldg(vis_rec + q0 + v + NT);
+      int2 vf = make_int2(0, 0);   // the record fetched in this iteration
+      if constexpr (PF) {
+        take18(rc, c);
+        if (v + NT < nv) load_raw(C, vn.x + (int)((unsigned)vn.y >> 24), ncoup, rc);
+        if (v + 2 * NT < nv) vf = __ldg(vis_rec + q0 + v + 2 * NT);
+      } else {
+        load_block18(C, vr.x + (int)((unsigned)vr.y >> 24), ncoup, c);
+        if (v + NT < nv) vf = __ldg(vis_rec + q0 + v + NT);
+      }
       p0s[v] = vr.x;
       T* wv = W + (size_t)v * WR;
 #pragma unroll
@@ -1632,7 +1647,12 @@ __global__ void __launch_bounds__(stage_nt<T>(), 2) k_stage36(
           x = fma(c[3 * rho + 2], wr[3 * cc + 2], x);
           dg[cc * (cc + 1) / 2 + rho] = x;
         }
-      vr = vn;
+      if constexpr (PF) {
+        vr = vn;
+        vn = vf;
+      } else {
+        vr = vf;
+      }
     }
   }
   // the gradient sums, per warp into shared memory (added up after phase 2)
