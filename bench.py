@@ -53,7 +53,7 @@ def load_package():
 
 def algorithmic_bytes(p, dtype_bytes: int) -> float:
     """Bytes the reduction must move: per point 9 E + 18k C entries in the storage type, b_e and scaling_e (FP64), a
-    4-byte camera index per observation; plus S read and written once (SURVEY's per-point model)."""
+    4-byte camera index per observation; plus S read and written once."""
     st = p.structure
     per_point = dtype_bytes * (9 * st.neblocks + 18 * p.nobs) + 8 * (3 + 3) * st.neblocks + 4 * p.nobs
     return float(per_point + 2 * dtype_bytes * p.pattern.nnz)
