@@ -1459,7 +1459,7 @@ __global__ void k_gather(T* __restrict__ dest, const T* __restrict__ src, const 
 // transposed (E^-1 is symmetric).
 template <class T>
 __host__ __device__ constexpr int stage_wr() { return sizeof(T) == 4 ? 20 : 18; }   // W record stride (16-byte multiple)
-// threads per CTA of k_stage36: 256 in FP32 (two CTAs per SM at 128 registers), 128 in FP64 (two per SM at ~200)
+// threads per CTA of k_stage36: 256 in FP32 (two CTAs per SM at 128 registers), 128 in FP64 (two per SM at ~240)
 template <class T>
 __host__ __device__ constexpr int stage_nt() { return sizeof(T) == 4 ? 256 : 128; }
 template <class T>
